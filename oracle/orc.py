@@ -1,0 +1,230 @@
+"""ctypes binding of the FP64 CPU oracle (oracle/revsim_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` as the checker.  The product path never imports it.
+"""
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liborc_revsim.so")
+_lib = None
+
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI32 = ctypes.POINTER(ctypes.c_int32)
+_PU64 = ctypes.POINTER(ctypes.c_uint64)
+
+
+class OrcSystem(ctypes.Structure):
+    _fields_ = [("n_mol", _I32), ("box", _D), ("m_O", _D), ("m_H", _D), ("inter_type", _I32),
+                ("coulomb_const", _D), ("crf_const", _D), ("cutoff", _D), ("nl_cutoff", _D),
+                ("n_steps_nf", _I32), ("kB", _D), ("temp", _D)]
+
+
+class OrcRdfTerm(ctypes.Structure):
+    _fields_ = [("sel1", _I32), ("sel2", _I32), ("x_min", _D), ("step", _D), ("width", _D),
+                ("exp_cutoff", _D), ("n_grid", _I32), ("slice_start", _I32),
+                ("slice_stride", _I32), ("n_target", _I32), ("target", _PD), ("norm", _I32),
+                ("weight", _D)]
+
+
+class OrcLoss(ctypes.Structure):
+    _fields_ = [("n_terms", _I32), ("terms", ctypes.POINTER(OrcRdfTerm))]
+
+
+def build(force=False):
+    """Compile the oracle with its Makefile (gcc, OpenMP, no FMA contraction)."""
+    if force or not os.path.exists(_LIB_PATH) or (
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "revsim_oracle.c"))):
+        subprocess.run(["make", "-s", "-C", _HERE, "-B" if force else "liborc_revsim.so"],
+                       check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_n_params.restype = _I32
+        L.orc_neighbor_pairs.restype = _I64
+        L.orc_neighbor_pairs.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PI32, _I64]
+        L.orc_forces.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64, _PD]
+        L.orc_forces_grads.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64, _PD,
+                                       _PD, _PD, _PD]
+        L.orc_energy.restype = _D
+        L.orc_energy.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64]
+        L.orc_noise.argtypes = [ctypes.POINTER(OrcSystem), ctypes.c_uint64, _D, _PD]
+        L.orc_rdf.argtypes = [ctypes.POINTER(OrcSystem), ctypes.POINTER(OrcRdfTerm), _PD, _PD]
+        L.orc_loss_grad.restype = _D
+        L.orc_loss_grad.argtypes = [ctypes.POINTER(OrcSystem), ctypes.POINTER(OrcLoss), _PD, _PD]
+        L.orc_forward_sim.restype = _D
+        L.orc_forward_sim.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PU64, _D, _I32,
+                                      _I32, _D, _I32, ctypes.POINTER(OrcLoss), _I32, _PD, _PD]
+        L.orc_reverse_sim.restype = _D
+        L.orc_reverse_sim.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PU64, _D, _I32,
+                                      _I32, _I32, _D, _I32, _PD, _PD, _D,
+                                      ctypes.POINTER(OrcLoss), _PD]
+        L.orc_num_threads.restype = _I32
+        L.orc_set_num_threads.argtypes = [_I32]
+        L.orc_vec1d.restype = _D
+        L.orc_vec1d.argtypes = [_D, _D, _D]
+        _lib = L
+    return _lib
+
+
+def _pd(a):
+    return a.ctypes.data_as(_PD)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+INTER = {"lj": 0, "dexp": 1, "buck": 2, "ljsc": 3, "buff": 4}
+
+
+def make_system(n_mol, box, inter_type="lj", temp=295.15, *, m_O=15.99943, m_H=1.007947,
+                coulomb_const=138.93545764438196, crf_const=None, cutoff=1.0, nl_cutoff=1.2,
+                n_steps_nf=20, kB=0.00831446261815324):
+    if crf_const is None:
+        crf_const = (1.0 / cutoff**3) * ((78.3 - 1) / (2 * 78.3 + 1))
+    return OrcSystem(n_mol, box, m_O, m_H, INTER[inter_type], coulomb_const, crf_const, cutoff,
+                     nl_cutoff, n_steps_nf, kB, temp)
+
+
+@dataclass
+class RdfTerm:
+    """One smoothed-RDF loss term (see orc_rdf_term in revsim_oracle.h)."""
+    sel1: int
+    sel2: int
+    x_min: float
+    step: float
+    width: float
+    exp_cutoff: float
+    n_grid: int
+    slice_start: int
+    slice_stride: int
+    target: np.ndarray
+    norm: int = 2
+    weight: float = 1.0
+    _keep: list = field(default_factory=list, repr=False)
+
+    def c(self):
+        t = _f64(self.target)
+        self._keep = [t]
+        return OrcRdfTerm(self.sel1, self.sel2, self.x_min, self.step, self.width,
+                          self.exp_cutoff, self.n_grid, self.slice_start, self.slice_stride,
+                          len(t), _pd(t), self.norm, self.weight)
+
+
+class Loss:
+    def __init__(self, terms):
+        self.terms = list(terms)
+        self._arr = (OrcRdfTerm * len(self.terms))(*[t.c() for t in self.terms])
+        self.c = OrcLoss(len(self.terms), self._arr)
+
+
+def n_params(s):
+    return lib().orc_n_params(s.inter_type)
+
+
+def neighbor_pairs(s, x):
+    x = _f64(x)
+    cap = 400 * 3 * s.n_mol + 16
+    out = np.zeros((cap, 2), dtype=np.int32)
+    n = lib().orc_neighbor_pairs(ctypes.byref(s), _pd(x), out.ctypes.data_as(_PI32), cap)
+    if n > cap:
+        out = np.zeros((n, 2), dtype=np.int32)
+        n = lib().orc_neighbor_pairs(ctypes.byref(s), _pd(x), out.ctypes.data_as(_PI32), n)
+    return out[:n].copy()
+
+
+def forces(s, params, x, pairs):
+    x, p = _f64(x), _f64(params)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    F = np.zeros(x.size)
+    lib().orc_forces(ctypes.byref(s), _pd(p), _pd(x), pairs.ctypes.data_as(_PI32), len(pairs), _pd(F))
+    return F.reshape(-1, 3)
+
+
+def forces_grads(s, params, x, pairs, w, jac=True):
+    x, p, w = _f64(x), _f64(params), _f64(w)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    P = n_params(s)
+    F = np.zeros(x.size)
+    G = np.zeros(x.size)
+    J = np.zeros(x.size * P) if jac else None
+    lib().orc_forces_grads(ctypes.byref(s), _pd(p), _pd(x), pairs.ctypes.data_as(_PI32),
+                           len(pairs), _pd(w), _pd(F), _pd(G), _pd(J) if jac else None)
+    return F.reshape(-1, 3), G.reshape(-1, 3), (J.reshape(-1, P) if jac else None)
+
+
+def energy(s, params, x, pairs):
+    x, p = _f64(x), _f64(params)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    return lib().orc_energy(ctypes.byref(s), _pd(p), _pd(x), pairs.ctypes.data_as(_PI32), len(pairs))
+
+
+def noise(s, seed, temp=None):
+    xi = np.zeros(9 * s.n_mol)
+    lib().orc_noise(ctypes.byref(s), ctypes.c_uint64(int(seed)), s.temp if temp is None else temp,
+                    _pd(xi))
+    return xi.reshape(-1, 3)
+
+
+def rdf(s, term, x):
+    x = _f64(x)
+    h = np.zeros(term.n_grid)
+    t = term.c()
+    lib().orc_rdf(ctypes.byref(s), ctypes.byref(t), _pd(x), _pd(h))
+    return h
+
+
+def loss_grad(s, loss, x, grad=True):
+    x = _f64(x)
+    g = np.zeros(x.size) if grad else None
+    val = lib().orc_loss_grad(ctypes.byref(s), ctypes.byref(loss.c), _pd(x), _pd(g) if grad else None)
+    return val, (g.reshape(-1, 3) if grad else None)
+
+
+def forward_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss=None,
+                calc_loss=True, n_steps_log=1000):
+    x, v, p = _f64(x).copy(), _f64(v).copy(), _f64(params)
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    n_snap = n_steps // n_steps_log + 1
+    sx = np.zeros((n_snap, x.size))
+    sv = np.zeros((n_snap, x.size))
+    val = lib().orc_forward_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v), seeds.ctypes.data_as(_PU64),
+                                gamma, n_steps, n_steps_loss, dt, n_steps_log,
+                                ctypes.byref(loss.c) if loss is not None else None,
+                                1 if (calc_loss and loss is not None) else 0, _pd(sx), _pd(sv))
+    return x.reshape(-1, 3), v.reshape(-1, 3), val, sx, sv
+
+
+def reverse_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
+                snaps_x, snaps_v, loss, clip=float("inf"), n_steps_log=1000):
+    x, v, p = _f64(x).copy(), _f64(v).copy(), _f64(params)
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    sx, sv = _f64(snaps_x), _f64(snaps_v)
+    g = np.zeros(n_params(s))
+    val = lib().orc_reverse_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v), seeds.ctypes.data_as(_PU64),
+                                gamma, n_steps, n_steps_loss, n_steps_trunc, dt, n_steps_log,
+                                _pd(sx), _pd(sv), clip, ctypes.byref(loss.c), _pd(g))
+    return x.reshape(-1, 3), v.reshape(-1, 3), val, g
+
+
+def set_threads(n):
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads():
+    return lib().orc_num_threads()

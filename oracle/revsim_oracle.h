@@ -1,0 +1,140 @@
+/*
+ * revsim_oracle.h -- CPU FP64 restatement of the reversible-simulation gradient
+ * of greener-group/rev-sim `water/water.jl` (3-site flexible water, LJ-family pair
+ * term + reaction-field Coulomb, harmonic bonds/angles, Langevin B-A-O-A steps,
+ * reverse-time reconstruction with the A-D adjoint accumulators, smoothed-RDF loss).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker: only tests/, the smoke
+ * check and the CPU-baseline leg of bench.py load it.  The product path (the CUDA
+ * library behind include/revsim.h) never calls into it.
+ *
+ * Parity status: the reference is Julia on Molly v0.21.1 / Enzyme / Zygote, and no
+ * Julia toolchain exists on either machine, so the reference cannot be run and it
+ * ships no golden vectors.  Absolute values are therefore "parity unpinned"; the
+ * restatement is pinned instead by the reference's own self-consistency assertions
+ * (water.jl:1613-1615: reconstruction < 1e-9 in FP64, |L_rev - L_fwd| < 1e-7),
+ * by central finite differences of every derivative (the diffusion.jl:1659-1667
+ * pattern) and by energy/force consistency (F = -dU/dx).
+ *
+ * Conventions restated from third-party Molly v0.21.1 (not vendored in the reference):
+ *   vector(c1, c2): per-dimension minimum image, returns c2 - c1 (see orc_vec1d);
+ *   wrap_coords: c - floor(c / L) * L;
+ *   random_velocity_3D(m, T, k): three N(0, sqrt(k T / m)) draws;
+ *   coulomb_const: passed in by the caller (Molly's coulombconst, kJ mol^-1 nm e^-2);
+ *   neighbour set: pairs i<j of different molecules with min-image d^2 <= rc_nl^2.
+ * All arithmetic is FP64 and compiled with -ffp-contract=off so that no fused
+ * multiply-add changes the rounding of the reference's expressions.
+ */
+#ifndef REVSIM_ORACLE_H
+#define REVSIM_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Pair forms, in the order of water.jl:121-150 (generate_inter). */
+enum { ORC_LJ = 0, ORC_DEXP = 1, ORC_BUCK = 2, ORC_LJSC = 3, ORC_BUFF = 4 };
+
+/* A water system: atoms ordered O, H1, H2 per molecule (tip3p.pdb order), bonds
+ * (O,H1), (O,H2), angle (H1, O, H2) with O central.  Parameter vector layout
+ * follows water.jl:1572-1582: [pair-form params..., q_O, k_b, r0, k_a, theta0]. */
+typedef struct {
+    int32_t n_mol;
+    double box;            /* cubic side, nm */
+    double m_O, m_H;       /* u */
+    int32_t inter_type;    /* ORC_* */
+    double coulomb_const;  /* kJ mol^-1 nm e^-2 */
+    double crf_const;      /* reaction-field k_rf, water.jl:41 */
+    double cutoff;         /* interaction cutoff, nm (1.0) */
+    double nl_cutoff;      /* neighbour-list cutoff, nm (1.2) */
+    int32_t n_steps_nf;    /* neighbour rebuild period (20) */
+    double kB;             /* u nm^2 ps^-2 K^-1 */
+    double temp;           /* K */
+} orc_system;
+
+/* One smoothed-RDF loss term (water.jl:631-711).  The grid is
+ * x_k = x_min + step*k (k = 0..n_grid-1); each distance is smeared with
+ * exp(-(x-d)^2 / width) truncated at |x-d| <= exp_cutoff and normalised per
+ * distance; h_k = V / (4 pi n1 n2 step) * sum / x_k^2.
+ * loss = weight * sum_t |h[slice_start + t*slice_stride] - target[t]|^norm. */
+typedef struct {
+    int32_t sel1, sel2;    /* 0 = O atoms, 1 = H atoms */
+    double x_min, step, width, exp_cutoff;
+    int32_t n_grid;
+    int32_t slice_start, slice_stride, n_target;
+    const double *target;
+    int32_t norm;          /* 1 = L1 (reference), 2 = squared error */
+    double weight;
+} orc_rdf_term;
+
+typedef struct {
+    int32_t n_terms;
+    const orc_rdf_term *terms;
+} orc_loss;
+
+int32_t orc_n_form_params(int32_t inter_type);
+int32_t orc_n_params(int32_t inter_type);
+
+/* Minimum-image component of Molly's vector(c1, c2): c2 - c1 folded by one box. */
+double orc_vec1d(double c1, double c2, double L);
+double orc_wrap1d(double c, double L);
+
+/* Neighbour pairs (i<j, different molecules, d^2 <= nl_cutoff^2), sorted by (i, j).
+ * Writes up to max_pairs pairs into pairs[2*k], pairs[2*k+1]; returns the count
+ * (which may exceed max_pairs: then only max_pairs are written). */
+int64_t orc_neighbor_pairs(const orc_system *s, const double *x, int32_t *pairs, int64_t max_pairs);
+
+/* calc_F! (water.jl:877-975): total force F[3N] over the given pair list. */
+void orc_forces(const orc_system *s, const double *params, const double *x,
+                const int32_t *pairs, int64_t n_pairs, double *F);
+
+/* calc_F_and_grads! (water.jl:1212-1433): forces F[3N], the force VJP
+ * dl_dfi[b] = sum_a (w[a]/m_a) . dF_a/dx_b with w = dl_dfi_prev, and the full
+ * parameter Jacobian dF_dp[3N * P] (row-major, index (3a+u)*P + p). dF_dp may be NULL. */
+void orc_forces_grads(const orc_system *s, const double *params, const double *x,
+                      const int32_t *pairs, int64_t n_pairs, const double *w,
+                      double *F, double *dl_dfi, double *dF_dp);
+
+/* Potential energy (pair form + reaction-field Coulomb + bonds + angles). */
+double orc_energy(const orc_system *s, const double *params, const double *x,
+                  const int32_t *pairs, int64_t n_pairs);
+
+/* Per-step Langevin noise: xi[3a+u] = sqrt(kB T / m_a) * z, z ~ N(0,1) from
+ * Philox4x32-10 keyed by the 64-bit step seed, counter (a, 0/1, 0, 0), Box-Muller. */
+void orc_noise(const orc_system *s, uint64_t seed, double temp, double *xi);
+
+/* RDF histogram of one term at positions x: writes h[n_grid]. */
+void orc_rdf(const orc_system *s, const orc_rdf_term *t, const double *x, double *h);
+
+/* Loss and dL/dx[3N] (dLdx may be NULL). */
+double orc_loss_grad(const orc_system *s, const orc_loss *L, const double *x, double *dLdx);
+
+/* forward_sim (water.jl:977-1105, loop 1029-1045).  x, v are updated in place
+ * (final state).  Snapshots of x and v are written every n_steps_log steps,
+ * including step 0, into snap_x/snap_v [(n_steps/n_steps_log + 1) * 3N] if not NULL.
+ * Returns the block-averaged loss (0 when calc_loss == 0). */
+double orc_forward_sim(const orc_system *s, const double *params, double *x, double *v,
+                       const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, double dt, int32_t n_steps_log,
+                       const orc_loss *loss, int32_t calc_loss,
+                       double *snap_x, double *snap_v);
+
+/* reverse_sim (water.jl:1435-1558).  x, v: final forward state on entry,
+ * reconstructed initial state on exit.  dl_dp[P] receives the gradient.
+ * Returns the block-averaged loss; returns NaN on bad arguments. */
+double orc_reverse_sim(const orc_system *s, const double *params, double *x, double *v,
+                       const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                       int32_t n_steps_log, const double *snap_x, const double *snap_v,
+                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp);
+
+/* Number of OpenMP threads used by the force loops (1 when built without OpenMP). */
+int32_t orc_num_threads(void);
+void orc_set_num_threads(int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
