@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark: forward+reverse atom-steps/s of the reversible-simulation gradient.
+
+Workload (default): 3,000 flexible 3-site waters (9,000 atoms) in a 4.5 nm periodic box,
+mixed precision (FP32 pair/bonded arithmetic, FP64 state, reconstruction and gradient
+sum), LJ + reaction-field Coulomb, dt = 1 fs, velocity Verlet (gamma = 0), 5,000 steps
+forward then 5,000 reverse; loss = squared error of the smoothed O-O RDF (200 bins,
+0-1 nm) every 1,000 steps against a target from the same code with sigma x 1.02,
+eps x 0.95; gradient w.r.t. the 7 parameters.  One bench "step" = one full gradient
+(forward_sim + reverse_sim).  One atom-step = one atom advanced one step forward and
+one step back.  Seeded synthetic input (jittered lattice, random orientations,
+Maxwell-Boltzmann velocities, equilibrated on the GPU before timing).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the CPU restatement of the reference (the FP64 oracle, OpenMP on
+all host cores; the Julia reference cannot run on these machines) on bounded samples of
+the same workload.  N > 1 (torchrun): independent replicas, one per GPU, no collective
+on the data path (weak scaling); timing is the max over ranks.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "rev-sim_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "fwd+rev atom-steps/s"
+UNIT = "atom-steps/s"
+# Algorithmic work per interacting pair (r <= 1.0 nm, unordered), counted from the
+# reference expressions (add/mul = 1, FMA = 2, sqrt/div/exp = 1): forward 40 (+15 for
+# an O-O LJ pair), reverse 170 (force + 3x3 VJP with mass scaling + dF/dtheta).
+FLOPS_FWD_IPAIR, FLOPS_FWD_OO_EXTRA, FLOPS_REV_IPAIR = 40, 15, 170
+# DRAM traffic per reverse-step launch of the default workload, from ncu
+# (profiles/rev_step_ncu.md); None until measured.
+REV_STEP_DRAM_BYTES = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-mol", type=int, default=3000)
+    ap.add_argument("--box", type=float, default=4.5)
+    ap.add_argument("--n-steps", type=int, default=5000)
+    ap.add_argument("--n-steps-loss", type=int, default=1000)
+    ap.add_argument("--gamma", type=float, default=0.0)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--form", default="lj")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64-GPU comparison run")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=10)
+    ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
+    ap.add_argument("--profile", action="store_true",
+                    help="one untimed gradient and exit (the command profiled under ncu)")
+    return ap.parse_args()
+
+
+def workload_name(a):
+    return (f"water_{a.n_mol}mol_{a.box:g}nm_{a.form}_{a.precision}_"
+            f"{a.n_steps}fwd+{a.n_steps}rev")
+
+
+def config(a, extra=None):
+    c = {"workload": workload_name(a), "n_atoms": 3 * a.n_mol, "box_nm": a.box,
+         "n_steps": a.n_steps, "n_steps_loss": a.n_steps_loss, "n_steps_trunc": a.n_steps_loss,
+         "n_steps_log": 1000, "dt_ps": 0.001, "gamma_per_ps": a.gamma, "pair_form": a.form,
+         "precision": a.precision,
+         "loss": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs sigma x1.02 / eps x0.95 target",
+         "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------ system set-up
+def prepare(a, device, equil_ps=3):
+    """Equilibrated start state and RDF target, both made on the GPU by the engine."""
+    from revsim import Engine, constants as C, oo_l2_term, systems
+    x = systems.water_coords(a.n_mol, a.box, seed=0)
+    v = systems.mb_velocities(a.n_mol, seed=1)
+    p = np.array(C.default_params(a.form))
+    eq = Engine(a.n_mol, a.box, inter_type=a.form, precision="mixed", device=device)
+    eq.set_params(p)
+    eq.set_state(x, v)
+    for blk in range(equil_ps):   # Langevin dynamics (gamma = 5/ps) from the lattice
+        eq.forward(systems.noise_seeds(1000, seed=10 + blk), 5.0, 1000, 1000, 0.001, calc_loss=False)
+    x0, v0 = eq.get_state()
+    # target: the same code with sigma x 1.02, eps x 0.95
+    pt = p.copy()
+    pt[0] *= 1.02
+    pt[1] *= 0.95
+    eq.set_params(pt)
+    eq.forward(systems.noise_seeds(1000, seed=20), 5.0, 1000, 1000, 0.001, calc_loss=False)
+    eq.set_loss([oo_l2_term(np.zeros(200))])
+    target = eq.rdf(0, 0)
+    eq.close()
+    return x0, v0, p, target
+
+
+def count_ipairs(x, box, pairs, cutoff=1.0):
+    d = x[pairs[:, 1]] - x[pairs[:, 0]]
+    d -= box * np.round(d / box)
+    r2 = (d * d).sum(1)
+    inter = r2 <= cutoff * cutoff
+    oo = inter & (pairs[:, 0] % 3 == 0) & (pairs[:, 1] % 3 == 0)
+    return int(inter.sum()), int(oo.sum())
+
+
+# ------------------------------------------------------------------- clocks
+class Clocks:
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.f:
+            return None
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [t.strip() for t in line.split(",")]
+                if len(parts) == 7:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_sample(a, x0, v0, p, target, n_s):
+    """The FP64 oracle on n_s forward + n_s reverse steps of the same system (all host
+    threads).  Returns (atom-steps/s, threads, description)."""
+    from oracle import orc
+    from revsim import systems
+    s = orc.make_system(a.n_mol, a.box, a.form)
+    t = orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, target, 2, 1.0)
+    loss = orc.Loss([t])
+    seeds = systems.noise_seeds(n_s, seed=99)
+    t0 = time.perf_counter()
+    xf, vf, _, sx, sv = orc.forward_sim(s, p, x0, v0, seeds, a.gamma, n_s, n_s, 0.001, loss, False)
+    t1 = time.perf_counter()
+    orc.reverse_sim(s, p, xf, vf, seeds, a.gamma, n_s, n_s, n_s, 0.001, sx, sv, loss)
+    t2 = time.perf_counter()
+    orc.loss_grad(s, loss, xf)
+    t3 = time.perf_counter()
+    t_loss = t3 - t2
+    # steps only, plus the loss amortised at one evaluation per n_steps_loss in each pass
+    t_steps = (t1 - t0) + (t2 - t1 - t_loss) + 2 * t_loss * n_s / a.n_steps_loss
+    return 3 * a.n_mol * n_s / t_steps, orc.num_threads(), (
+        f"{n_s} forward + {n_s} reverse steps of the {3 * a.n_mol}-atom box, FP64 oracle, "
+        f"loss cost amortised at one evaluation per {a.n_steps_loss} steps")
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import orc
+    from revsim import constants as C, systems
+    orc.build()
+    # same seeded start as the GPU arm, relaxed on the CPU (the arm is CPU-only)
+    x = systems.water_coords(a.n_mol, a.box, seed=0)
+    v = systems.mb_velocities(a.n_mol, seed=1)
+    p = np.array(C.default_params(a.form))
+    s = orc.make_system(a.n_mol, a.box, a.form)
+    x, v, _, _, _ = orc.forward_sim(s, p, x, v, systems.noise_seeds(50, seed=10), 5.0, 50, 50,
+                                    0.001, None, False)
+    t = orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, np.zeros(200), 2, 1.0)
+    target = orc.rdf(s, t, x)
+    vals = []
+    for i in range(a.warmup + a.steps):
+        val, cores, desc = cpu_sample(a, x, v, p, target, a.cpu_sample_steps)
+        if i >= a.warmup:
+            vals.append(val)
+    value = statistics.mean(vals)
+    ms = 1e3 * 3 * a.n_mol * a.n_steps / value
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+           "config": config(a, {"precision": "fp64"}),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                            "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "the reference is Julia (Molly/Enzyme); no Julia toolchain exists on these "
+                   "machines, so this arm times the FP64 C restatement of its algorithm"}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------- GPU arm
+def run_ours(a):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import build as _build
+    _build.build()
+    from revsim import Engine, _lib, oo_l2_term, systems
+
+    x0, v0, p, target = prepare(a, local, a.equil_ps)
+    eng = Engine(a.n_mol, a.box, inter_type=a.form, precision=a.precision, device=local)
+    eng.set_params(p)
+    eng.set_loss([oo_l2_term(target)])
+    eng.set_state(x0, v0)
+    seeds = systems.noise_seeds(a.n_steps, seed=100 + rank)
+    if a.profile:
+        eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+        eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+        torch.cuda.synchronize()
+        eng.close()
+        return
+    shape = eng.autotune()
+    eng.set_state(x0, v0)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def gradient():
+        lf = eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+        lr, g = eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+        return lf, lr, g
+
+    for _ in range(a.warmup):
+        gradient()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lf, lr, g = gradient()
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    clocks = clk.summary()
+    total_ms = sum(times)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / a.steps
+    n_atoms = 3 * a.n_mol
+    value = world * n_atoms * a.n_steps / (ms_step * 1e-3)
+
+    # end to end through the public API from pinned host buffers
+    xh = torch.from_numpy(x0.copy()).pin_memory()
+    vh = torch.from_numpy(v0.copy()).pin_memory()
+    e2e_ms = []
+    for _ in range(a.steps):
+        flush.zero_()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.set_state(xh.numpy(), vh.numpy())
+        gradient()
+        e1.record(stream)
+        barrier()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * n_atoms * a.n_steps / (e2e_total / a.steps * 1e-3)
+    h2d = 2 * 3 * n_atoms * 8 + 2 * a.n_steps * 8
+    d2h = 8 + 8 + 8 * eng.n_params
+
+    # roofline of the dominant kernel (the fused reverse step), timed per launch
+    eng.set_state(x0, v0)
+    eng.set_kernel_timing(True)
+    eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+    eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+    kt_ms, kt_n = eng.kernel_time(0)
+    ft_ms, ft_n = eng.kernel_time(1)
+    eng.set_kernel_timing(False)
+    launch_ms = kt_ms / max(kt_n, 1)
+    xs, _ = eng.get_state()
+    pairs = eng.neighbor_pairs(0)
+    ipairs, oo = count_ipairs(xs, a.box, pairs)
+    flops_launch = FLOPS_REV_IPAIR * ipairs
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    import ctypes
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None,
+                "traffic": REV_STEP_DRAM_BYTES,
+                "kernel": "k_water_step<float, LJ, reverse> (fused reverse step)",
+                "launch_ms": launch_ms, "launches_timed": kt_n, "ipairs": ipairs,
+                "flops_per_launch": flops_launch,
+                "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops); "
+                               "the step kernels are scalar FP32 work, neither HBM- nor tensor-bound",
+                "shape": {"lanes_per_mol": shape[0], "mols_per_cta": shape[1], "unroll": shape[2]},
+                "forward_step_launch_ms": ft_ms / max(ft_n, 1),
+                "step_kernels_share_of_gradient": (kt_ms + ft_ms) / ms_step}
+
+    extra = {}
+    if not a.no_compare and rank == 0:
+        # the same gradient in plain FP64 on the GPU: throughput and gradient difference
+        e64 = Engine(a.n_mol, a.box, inter_type=a.form, precision="fp64", device=local)
+        e64.set_params(p)
+        e64.set_loss([oo_l2_term(target)])
+        e64.set_state(x0, v0)
+        e64.autotune()
+        e64.set_state(x0, v0)
+        e64.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+        e64.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+        torch.cuda.synchronize()
+        s64 = torch.cuda.ExternalStream(e64.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e64.set_state(x0, v0)
+        e0.record(s64)
+        e64.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+        _, g64 = e64.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+        e1.record(s64)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        eng.set_state(x0, v0)
+        eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+        _, gm = eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+        # short window: the same comparison over the first 100 steps (before chaos
+        # amplifies the FP32 rounding of the trajectory)
+        short = {}
+        for eng_, key in ((eng, "mixed"), (e64, "fp64")):
+            eng_.set_state(x0, v0)
+            eng_.forward(seeds[:100], a.gamma, 100, 100, 0.001)
+            short[key] = eng_.reverse(seeds[:100], a.gamma, 100, 100, 100, 0.001)[1][0]
+        gs = np.abs(g64[0] * p)
+
+        def rel(gx, gref):
+            sc = np.abs(gref * p)
+            return float(np.max(np.abs((gx - gref) * p) / np.maximum(sc, 0.01 * sc.max())))
+        extra = {"fp64_gpu": {"value": n_atoms * a.n_steps / (ms64 * 1e-3), "ms_per_step": ms64,
+                              "speedup_mixed_over_fp64": (ms64 / ms_step)},
+                 "grad_rel_err_vs_fp64": {
+                     "full_workload": rel(gm[0], g64[0]),
+                     "first_100_steps": rel(short["mixed"], short["fp64"]),
+                     "definition": "max over parameters of |g - g_fp64| * |theta| / max(|g_fp64 * theta|, "
+                                   "0.01 max_k |g_fp64,k * theta_k|)"}}
+        e64.close()
+        del gs
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        val, cores, desc = cpu_sample(a, x0, v0, p, target, a.cpu_sample_steps)
+        cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None,
+               "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
+               "config": config(a, {"parallelism": f"replicas{world}" if world > 1 else "single"}),
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h},
+               "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+               "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])}}
+        out.update(extra)
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)

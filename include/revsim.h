@@ -1,0 +1,186 @@
+/*
+ * revsim.h -- C ABI of the B200 (sm_100a) reversible-simulation gradient engine.
+ *
+ * The engine replaces the hot path of greener-group/rev-sim `water/water.jl`:
+ * forward_sim (water.jl:977-1105), reverse_sim (water.jl:1435-1558) and the force /
+ * force-gradient kernels they call (calc_F! water.jl:877-975, calc_F_and_grads!
+ * water.jl:1212-1433, Molly's CellListMapNeighborFinder, loss_and_grads
+ * water.jl:771-787).  Plain C types only: host arrays are FP64 AoS xyz
+ * (Julia's reinterpret(Float64, ::Vector{SVector{3,Float64}}) layout), copied in and
+ * out; the library never keeps a host pointer.  Every entry point returns an int32
+ * status (REVSIM_OK or a negative REVSIM_ERR_*); no C++ exception crosses the ABI.
+ * A handle owns all device memory and one CUDA stream; calls on one handle must come
+ * from one host thread at a time.
+ *
+ * A handle holds R >= 1 independent replicas (water boxes of their own size,
+ * box side and temperature) that are stepped together in one launch per step.
+ */
+#ifndef REVSIM_H
+#define REVSIM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define REVSIM_OK 0
+#define REVSIM_ERR_BADARG (-1)
+#define REVSIM_ERR_CUDA (-2)
+#define REVSIM_ERR_NLIST_OVERFLOW (-3)
+#define REVSIM_ERR_NAN (-4)
+#define REVSIM_ERR_TIMEOUT (-5)
+#define REVSIM_ERR_GEOMETRY (-6)
+#define REVSIM_ERR_STATE (-7)
+#define REVSIM_ERR_NOMEM (-8)
+
+/* Pair forms, same order as generate_inter (water.jl:121-150). */
+#define REVSIM_LJ 0
+#define REVSIM_DEXP 1
+#define REVSIM_BUCK 2
+#define REVSIM_LJSC 3
+#define REVSIM_BUFF 4
+
+/* Arithmetic of the pair terms.  State (x, v), reverse reconstruction, the adjoint
+ * accumulators and the parameter-gradient sum are FP64 in both modes. */
+#define REVSIM_FP64 0
+#define REVSIM_MIXED 1 /* FP32 pair / bonded-term arithmetic */
+
+/* Neighbour lists used by the reverse pass. */
+#define REVSIM_NL_CHECKPOINT 0 /* rebuilt from the forward pass's build positions */
+#define REVSIM_NL_RECONSTRUCTED 1 /* rebuilt from reconstructed positions, water.jl:1504 */
+
+typedef struct revsim_handle revsim_handle;
+
+/* System description (replaces System(structure_file, ff; ...) at water.jl:980-991
+ * and the constants of water.jl:27-48).  Water atoms are ordered O, H1, H2. */
+typedef struct {
+    int32_t n_replicas;
+    const int32_t *n_mol;   /* [n_replicas] molecules per replica */
+    const double *box;      /* [n_replicas] cubic box side, nm */
+    const double *temp;     /* [n_replicas] K */
+    int32_t inter_type;     /* REVSIM_LJ .. REVSIM_BUFF */
+    int32_t precision;      /* REVSIM_FP64 or REVSIM_MIXED */
+    double m_O, m_H;        /* u */
+    double coulomb_const;   /* kJ mol^-1 nm e^-2 */
+    double crf_const;       /* reaction-field k_rf, nm^-3 */
+    double cutoff;          /* interaction cutoff, nm */
+    double nl_cutoff;       /* neighbour-list cutoff, nm */
+    double kB;              /* u nm^2 ps^-2 K^-1 */
+    int32_t n_steps_nf;     /* neighbour rebuild period, steps */
+    int32_t n_steps_log;    /* forward snapshot period, steps */
+    int32_t nl_mode;        /* REVSIM_NL_CHECKPOINT or REVSIM_NL_RECONSTRUCTED */
+    int32_t device;         /* CUDA device ordinal */
+} revsim_system_desc;
+
+/* One smoothed-RDF loss term (rdf_differentiable + loss_rdf_part, water.jl:631-697):
+ * grid x_k = x_min + step*k, k < n_grid; Gaussian exp(-(x-d)^2/width) truncated at
+ * |x-d| <= exp_cutoff and normalised per distance; loss =
+ * weight * sum_t |h[slice_start + t*slice_stride] - target_t|^norm (norm 1 or 2).
+ * sel: 0 = O atoms, 1 = H atoms. */
+typedef struct {
+    int32_t sel1, sel2;
+    double x_min, step, width, exp_cutoff;
+    int32_t n_grid;
+    int32_t slice_start, slice_stride, n_target;
+    int32_t norm;
+    double weight;
+} revsim_rdf_term;
+
+/* Create / destroy.  Replaces System construction + inject_atom_grads (water.jl:546-569). */
+int32_t revsim_create(const revsim_system_desc *desc, revsim_handle **out);
+void revsim_destroy(revsim_handle *h);
+/* Last error message of this handle ("" when none); valid until the next call. */
+const char *revsim_last_error(const revsim_handle *h);
+/* Status of the device-side checks (bit flags) accumulated since the last call. */
+int32_t revsim_device_status(revsim_handle *h, int32_t *flags);
+
+/* Sizes: total atoms over replicas and the parameter count P of the pair form. */
+int32_t revsim_sizes(const revsim_handle *h, int64_t *n_atoms, int32_t *n_params);
+
+/* Parameters in the reference layout [pair form..., q_O, k_b, r0, k_a, theta0]
+ * (water.jl:1572-1582, inject_si_grads water.jl:528-543). */
+int32_t revsim_set_params(revsim_handle *h, const double *theta, int32_t n_params);
+
+/* State of all replicas, concatenated: x, v [3 * n_atoms]. */
+int32_t revsim_set_state(revsim_handle *h, const double *x, const double *v);
+int32_t revsim_get_state(revsim_handle *h, double *x, double *v);
+
+/* Loss terms and per-replica targets [n_replicas * n_target] for each term. */
+int32_t revsim_set_loss(revsim_handle *h, int32_t n_terms, const revsim_rdf_term *terms,
+                        const double *const *targets);
+
+/* Neighbour pair set of one replica at the current positions (Molly
+ * find_neighbors with the 1.2 nm CellListMap finder, water.jl:1025): pairs
+ * (i, j), i < j, replica-local atom indices, in no particular order.  Writes
+ * min(count, cap) pairs to pairs[2k], pairs[2k+1] and the total to *count. */
+int32_t revsim_neighbor_pairs(revsim_handle *h, int32_t replica, int32_t *pairs, int64_t cap,
+                              int64_t *count);
+
+/* calc_F! (water.jl:877-975) at the current positions: F [3 * n_atoms]. */
+int32_t revsim_forces(revsim_handle *h, double *F);
+
+/* calc_F_and_grads! (water.jl:1212-1433) at the current positions with
+ * dl_dfi_prev = w [3 n_atoms]: forces F, the force VJP dl_dfi [3 n_atoms] and the
+ * contraction dtheta[r*P + p] = sum_{a in replica r} acoef[a] . dF_a/dtheta_p
+ * (the reference's sum(A dt^2/(2m) dF_dp), water.jl:1517-1519). */
+int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef, double *F,
+                         double *dl_dfi, double *dtheta);
+
+/* generate_noise! (water.jl:867-873) for one step seed per replica: xi [3 n_atoms]. */
+int32_t revsim_noise(revsim_handle *h, const uint64_t *seeds, double *xi);
+
+/* loss_and_grads (water.jl:771-787): loss [n_replicas] and dL/dx [3 n_atoms]
+ * (dLdx may be NULL). */
+int32_t revsim_loss_grad(revsim_handle *h, double *loss, double *dLdx);
+
+/* One RDF histogram h [n_grid] of term t for one replica. */
+int32_t revsim_rdf(revsim_handle *h, int32_t term, int32_t replica, double *hist);
+
+/* forward_sim (water.jl:977-1105, loop 1029-1045) from the current state.
+ * noise_seeds [n_steps * n_replicas], step-major.  Keeps snapshots every
+ * n_steps_log steps and the neighbour-build positions on the device for the
+ * reverse pass.  loss_out [n_replicas] (block-averaged; may be NULL). */
+int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gamma,
+                       int32_t n_steps, int32_t n_steps_loss, double dt, int32_t calc_loss,
+                       double *loss_out);
+
+/* reverse_sim (water.jl:1435-1558) from the current state (the forward end state).
+ * loss_out [n_replicas], dl_dp_out [n_replicas * P]: block-averaged loss and
+ * gradient per replica.  clip_norm_threshold may be +inf. */
+int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gamma,
+                       int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                       double clip_norm_threshold, double *loss_out, double *dl_dp_out);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that time with events. */
+void *revsim_stream(revsim_handle *h);
+
+/* Launch counters: number of engine kernel launches since the handle was created. */
+int64_t revsim_launch_count(const revsim_handle *h);
+
+/* Per-kernel timing of the step kernels (which = 0: fused reverse step, 1: fused
+ * forward step): when enabled, each launch is bracketed by CUDA events on the handle's
+ * stream; the summed milliseconds and the launch count are returned by
+ * revsim_kernel_time. */
+int32_t revsim_set_kernel_timing(revsim_handle *h, int32_t enable);
+int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, int64_t *launches);
+
+/* Block shape of the step kernels: lanes per molecule (8, 16 or 32), molecules per
+ * CTA, and neighbour entries per lane per loop iteration (1 or 2); 0 keeps the
+ * current value.  revsim_autotune times the allowed shapes on the current state and
+ * keeps the fastest. */
+int32_t revsim_set_launch_shape(revsim_handle *h, int32_t lanes_per_mol, int32_t mols_per_cta,
+                                int32_t unroll);
+int32_t revsim_get_launch_shape(revsim_handle *h, int32_t *lanes_per_mol, int32_t *mols_per_cta,
+                                int32_t *unroll);
+int32_t revsim_autotune(revsim_handle *h, double dt);
+
+/* Instrumentation with no counterpart in the reference: the measured FP32 fused
+ * multiply-add throughput (TFLOP/s, 2 flops per FMA) of a device, the roofline
+ * denominator of the FP32-pipe-bound step kernels. */
+int32_t revsim_probe_fp32_tflops(int32_t device, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

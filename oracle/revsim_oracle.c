@@ -84,22 +84,38 @@ int64_t orc_neighbor_pairs(const orc_system *s, const double *x, int32_t *pairs,
     const int64_t n = 3 * (int64_t)s->n_mol;
     const double rc2 = s->nl_cutoff * s->nl_cutoff;
     const double L = s->box;
-    int64_t cnt = 0;
+    /* Rows i in parallel; per-row counts, then a prefix sum keeps the (i, j) order. */
+    int64_t *cnt = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+#pragma omp parallel for schedule(dynamic, 16)
     for (int64_t i = 0; i < n; i++) {
+        int64_t c = 0;
         for (int64_t j = i + 1; j < n; j++) {
             if (i / 3 == j / 3) continue;
             double d[3];
             vec3(x + 3 * i, x + 3 * j, L, d);
+            if (sumsq3(d) <= rc2) c++;
+        }
+        cnt[i + 1] = c;
+    }
+    for (int64_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+    const int64_t total = cnt[n];
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < n; i++) {
+        int64_t k = cnt[i];
+        if (k >= max_pairs) continue;
+        for (int64_t j = i + 1; j < n && k < max_pairs; j++) {
+            if (i / 3 == j / 3) continue;
+            double d[3];
+            vec3(x + 3 * i, x + 3 * j, L, d);
             if (sumsq3(d) <= rc2) {
-                if (cnt < max_pairs) {
-                    pairs[2 * cnt] = (int32_t)i;
-                    pairs[2 * cnt + 1] = (int32_t)j;
-                }
-                cnt++;
+                pairs[2 * k] = (int32_t)i;
+                pairs[2 * k + 1] = (int32_t)j;
+                k++;
             }
         }
     }
-    return cnt;
+    free(cnt);
+    return total;
 }
 
 /* ------------------------------------------------------------------------- */
@@ -725,27 +741,39 @@ void orc_rdf(const orc_system *s, const orc_rdf_term *t, const double *x, double
     rdf_ctx c;
     rdf_setup(s, t, &c);
     const double L = s->box;
-    double *acc = (double *)calloc((size_t)t->n_grid, sizeof(double));
-    for (int64_t a = 0; a < c.n1; a++) {
-        for (int64_t b = 0; b < c.n2; b++) {
-            double dr[3];
-            vec3(x + 3 * c.idx1[a], x + 3 * c.idx2[b], L, dr);
-            double d = sqrt(sumsq3(dr));
-            if (d == 0.0) continue;
-            int64_t lo, hi;
-            hist_window(t, d, &lo, &hi);
-            if (lo > hi) continue;
-            double den, dden;
-            rdf_den(t, c.off, d, &den, &dden);
-            for (int64_t k = lo; k <= hi; k++) {
-                double e = grid_x(t, k) - d;
-                acc[k] += exp(-(e * e) / t->width) / den;
+    const int nthr = orc_num_threads();
+    double *acc = (double *)calloc((size_t)t->n_grid * nthr, sizeof(double));
+#pragma omp parallel
+    {
+#ifdef _OPENMP
+        double *al = acc + (size_t)t->n_grid * omp_get_thread_num();
+#else
+        double *al = acc;
+#endif
+#pragma omp for schedule(static)
+        for (int64_t a = 0; a < c.n1; a++) {
+            for (int64_t b = 0; b < c.n2; b++) {
+                double dr[3];
+                vec3(x + 3 * c.idx1[a], x + 3 * c.idx2[b], L, dr);
+                double d = sqrt(sumsq3(dr));
+                if (d == 0.0) continue;
+                int64_t lo, hi;
+                hist_window(t, d, &lo, &hi);
+                if (lo > hi) continue;
+                double den, dden;
+                rdf_den(t, c.off, d, &den, &dden);
+                for (int64_t k = lo; k <= hi; k++) {
+                    double e = grid_x(t, k) - d;
+                    al[k] += exp(-(e * e) / t->width) / den;
+                }
             }
         }
     }
     for (int64_t k = 0; k < t->n_grid; k++) {
+        double sum = 0.0;
+        for (int th = 0; th < nthr; th++) sum += acc[(size_t)t->n_grid * th + k];
         double xk = grid_x(t, k);
-        h[k] = c.pre * acc[k] / (xk * xk);
+        h[k] = c.pre * sum / (xk * xk);
     }
     free(acc);
     rdf_free(&c);
@@ -777,6 +805,16 @@ double orc_loss_grad(const orc_system *s, const orc_loss *Ls, const double *x, d
         if (dLdx) {
             rdf_ctx c;
             rdf_setup(s, t, &c);
+            const int nthr = orc_num_threads();
+            double *gacc = (double *)calloc((size_t)n3 * nthr, sizeof(double));
+#pragma omp parallel
+            {
+#ifdef _OPENMP
+            double *gl = gacc + (size_t)n3 * omp_get_thread_num();
+#else
+            double *gl = gacc;
+#endif
+#pragma omp for schedule(static)
             for (int64_t a = 0; a < c.n1; a++) {
                 for (int64_t b = 0; b < c.n2; b++) {
                     int64_t ia = c.idx1[a], ib = c.idx2[b];
@@ -800,11 +838,15 @@ double orc_loss_grad(const orc_system *s, const orc_loss *Ls, const double *x, d
                     if (dLdd == 0.0) continue;
                     for (int u = 0; u < 3; u++) {
                         double gu = dLdd * dr[u] / d;
-                        dLdx[3 * ib + u] += gu;
-                        dLdx[3 * ia + u] -= gu;
+                        gl[3 * ib + u] += gu;
+                        gl[3 * ia + u] -= gu;
                     }
                 }
             }
+            }
+            for (int64_t e = 0; e < n3; e++)
+                for (int th = 0; th < nthr; th++) dLdx[e] += gacc[(size_t)n3 * th + e];
+            free(gacc);
             rdf_free(&c);
         }
         free(h);

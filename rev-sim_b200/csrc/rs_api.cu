@@ -1,0 +1,1228 @@
+// rs_api.cu -- the C ABI of include/revsim.h: handle, device memory and the
+// forward / reverse drivers.
+//
+// Driver structure (host loop on one CUDA stream, one kernel per MD step):
+//   forward_sim  (water.jl:977-1105): per step one fused force+integrate kernel; the
+//                neighbour list is rebuilt every n_steps_nf steps and the build
+//                positions are kept ("checkpoints"); snapshots of x, v every
+//                n_steps_log steps; the loss every n_steps_loss steps.
+//   reverse_sim  (water.jl:1435-1558): loss gradient at the end state, then per step
+//                one fused kernel (force + VJP + dtheta + un-kick + B/A update + the
+//                next step's un-integration); snapshot restores, loss blocks and
+//                truncation exactly as the reference orders them.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "revsim.h"
+#include "rs_internal.h"
+
+using namespace rs;
+
+namespace {
+
+constexpr double kRext = 0.15;        // bound on intramolecular O-H distance, nm
+constexpr double kTwoPow1o6 = 1.122462048309373;
+
+int form_nparams(int f) {
+    switch (f) {
+        case REVSIM_LJ: return 2;
+        case REVSIM_DEXP: return 4;
+        case REVSIM_BUCK: return 3;
+        case REVSIM_LJSC: return 4;
+        case REVSIM_BUFF: return 4;
+    }
+    return -1;
+}
+
+struct Term {
+    revsim_rdf_term t;
+    int off;
+    double *d_target = nullptr;   // [R * n_target]
+    double *d_hist = nullptr;     // [R * n_grid + R]  (histogram, then pre[R])
+    double *d_dLdh = nullptr;     // [R * n_grid]
+};
+
+}  // namespace
+
+struct revsim_handle {
+    std::string err;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+
+    int R = 0, M = 0, N = 0;
+    std::vector<int> nmol, mol0, atom0;
+    std::vector<double> box, temp;
+    int form = 0, prec = 0, nl_mode = 0, nf = 20, nlog = 1000;
+    double mO = 0, mH = 0, ke = 0, krf = 0, rc = 0, rc_nl = 0, kB = 0;
+
+    std::vector<double> theta;
+    int P = 0, NFp = 0;
+    bool have_params = false, have_state = false;
+
+    int G = 32, mpc = 8, unroll = 1, n_blk = 0;
+    bool shift_ok = false;   // one periodic image per molecule pair is exact for every box
+    int cap = 0;
+
+    // tables
+    int *d_blk_rep = nullptr, *d_blk_mol0 = nullptr, *d_blk_nmol = nullptr;
+    int *d_mol_rep = nullptr, *d_atom_rep = nullptr, *d_rep_atom0 = nullptr, *d_rep_nmol = nullptr;
+    double *d_rep_box = nullptr, *d_rep_sdO = nullptr, *d_rep_sdH = nullptr;
+    // cells
+    std::vector<int> nc, cell_off;
+    int n_cells = 0;
+    int *d_rep_nc = nullptr, *d_rep_cell_off = nullptr;
+    int *d_cell_of_mol = nullptr, *d_cell_cnt = nullptr, *d_cell_start = nullptr,
+        *d_cell_fill = nullptr, *d_cell_tmp = nullptr, *d_cell_sorted = nullptr;
+    uint32_t *d_nbr = nullptr;       // working rows [M * cap]
+    int *d_nbr_cnt = nullptr;
+    int *d_cell_rep = nullptr;
+    float band = 2e-5f;
+    // rows of every forward build, reused by the reverse pass (checkpoint mode)
+    uint32_t *d_nbr_store = nullptr;
+    int *d_cnt_store = nullptr;
+    size_t store_slots = 0, store_cap = 0;
+    // state
+    double *d_x = nullptr, *d_v = nullptr, *d_A = nullptr, *d_B = nullptr, *d_C = nullptr,
+           *d_D = nullptr, *d_G = nullptr, *d_F = nullptr, *d_x0 = nullptr, *d_v0 = nullptr;
+    void *d_pos[2] = {nullptr, nullptr}, *d_wgt[2] = {nullptr, nullptr};
+    double *d_part = nullptr, *d_norm2 = nullptr, *d_scale = nullptr;
+    int *d_status = nullptr, *d_maxcnt = nullptr;
+    unsigned long long *d_count = nullptr;
+    // trajectory store
+    double *d_snap_x = nullptr, *d_snap_v = nullptr, *d_ckpt = nullptr;
+    size_t snap_cap = 0, snapv_cap = 0, ckpt_cap = 0;
+    bool fwd_valid = false;
+    int fwd_steps = 0;
+    uint64_t *d_seeds = nullptr;
+    size_t seeds_cap = 0;
+    // loss
+    std::vector<Term> terms;
+    double *d_loss = nullptr, *d_loss_acc = nullptr, *d_dLdx = nullptr;
+    // instrumentation
+    long long launches = 0;
+    bool ktime = false;
+    std::vector<cudaEvent_t> ev[2];   // [0] reverse-step kernel, [1] forward-step kernel
+    size_t ev_used[2] = {0, 0};
+    double kt_ms[2] = {0.0, 0.0};
+    long long kt_n[2] = {0, 0};
+};
+
+namespace {
+
+int fail(revsim_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(h, REVSIM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc((void **)p, sizeof(T) * n);
+}
+
+void dfree(void *p) {
+    if (p) cudaFree(p);
+}
+
+template <typename R>
+NbConsts<R> nb_consts(const revsim_handle *h) {
+    const double *t = h->theta.data();
+    const int nfp = h->NFp;
+    const double qO = t[nfp], qH = -qO / 2;
+    NbConsts<R> nb;
+    nb.qq[0] = (R)(h->ke * qO * qO);
+    nb.qq[1] = (R)(h->ke * qO * qH);
+    nb.qq[2] = (R)(h->ke * qH * qH);
+    nb.krf = (R)h->krf;
+    nb.krf2 = (R)(2 * h->krf);
+    nb.rc2 = (R)(h->rc * h->rc);
+    nb.twoinvq = (R)(2.0 / qO);
+    FormConsts<R> &fc = nb.fc;
+    for (int i = 0; i < 4; i++) fc.p[i] = (R)(i < nfp ? t[i] : 0.0);
+    for (int i = 0; i < 8; i++) fc.c[i] = (R)0;
+    switch (h->form) {
+        case REVSIM_LJ: {
+            const double s = t[0], e = t[1];
+            fc.on = e != 0.0;
+            fc.c[0] = (R)(s * s);
+            fc.c[1] = (R)(24 * e);
+            fc.c[2] = (R)(144 * e / s);
+            fc.c[3] = (R)(e != 0.0 ? 1.0 / e : 0.0);
+            break;
+        }
+        case REVSIM_BUCK: {
+            const double A = t[0], B = t[1], C = t[2];
+            fc.on = A != 0.0;
+            fc.c[0] = (R)(A * B);
+            fc.c[1] = (R)(6 * C);
+            fc.c[2] = (R)(A * B * B);
+            fc.c[3] = (R)(42 * C);
+            break;
+        }
+        case REVSIM_DEXP: {
+            const double s = t[0], e = t[1], al = t[2], be = t[3];
+            const double rm = s * kTwoPow1o6;
+            fc.on = e != 0.0;
+            fc.c[0] = (R)(1.0 / rm);
+            fc.c[1] = (R)(e * al * be);
+            fc.c[2] = (R)(1.0 / (al - be));
+            fc.c[3] = (R)rm;
+            fc.c[4] = (R)kTwoPow1o6;
+            break;
+        }
+        case REVSIM_LJSC: {
+            const double s = t[0], e = t[1], al = t[2], la = t[3];
+            const double s6 = s * s * s * s * s * s;
+            const double u = s6 * al * la * la;
+            fc.on = e != 0.0;
+            fc.c[0] = (R)s6;
+            fc.c[1] = (R)u;
+            fc.c[2] = (R)(24 * e);
+            fc.c[3] = (R)(s6 * s6);
+            fc.c[4] = (R)(e != 0.0 ? 1.0 / e : 0.0);
+            fc.c[5] = (R)(6 * u / s);
+            fc.c[6] = (R)(s6 * la * la);
+            fc.c[7] = (R)(2 * s6 * al * la);
+            break;
+        }
+        case REVSIM_BUFF: {
+            fc.on = t[1] != 0.0;
+            fc.c[0] = (R)kTwoPow1o6;
+            break;
+        }
+    }
+    return nb;
+}
+
+BondConsts bond_consts(const revsim_handle *h) {
+    const double *t = h->theta.data() + h->NFp;
+    return BondConsts{t[1], t[2], t[3], t[4]};
+}
+
+StepArgs base_args(revsim_handle *h) {
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.blk_rep = h->d_blk_rep;
+    a.blk_mol0 = h->d_blk_mol0;
+    a.blk_nmol = h->d_blk_nmol;
+    a.rep_box = h->d_rep_box;
+    a.rep_sdO = h->d_rep_sdO;
+    a.rep_sdH = h->d_rep_sdH;
+    a.rep_atom0 = h->d_rep_atom0;
+    a.nbr = h->d_nbr;
+    a.nbr_cnt = h->d_nbr_cnt;
+    a.cap = h->cap;
+    a.x = h->d_x;
+    a.v = h->d_v;
+    a.A = h->d_A;
+    a.B = h->d_B;
+    a.C = h->d_C;
+    a.D = h->d_D;
+    a.G = h->d_G;
+    a.part = h->d_part;
+    a.P = h->P;
+    a.status = h->d_status;
+    a.mO = h->mO;
+    a.mH = h->mH;
+    return a;
+}
+
+int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a) {
+    const int threads = h->G * h->mpc;
+    const BondConsts bc = bond_consts(h);
+    const bool timed = h->ktime && !(a.mode & MODE_FORCES_ONLY);
+    const int which = rev ? 0 : 1;
+    if (timed) {
+        while (h->ev[which].size() < h->ev_used[which] + 2) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            h->ev[which].push_back(e);
+        }
+        CK(cudaEventRecord(h->ev[which][h->ev_used[which]], h->st));
+    }
+    cudaError_t e;
+    if (h->prec == REVSIM_MIXED)
+        e = launch_step<float>(rev, h->form, h->G, h->unroll, h->shift_ok, h->n_blk, threads, a,
+                               nb_consts<float>(h), bc, h->st);
+    else
+        e = launch_step<double>(rev, h->form, h->G, h->unroll, h->shift_ok, h->n_blk, threads, a,
+                                nb_consts<double>(h), bc, h->st);
+    h->launches++;
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("step kernel: ") + cudaGetErrorString(e));
+    if (timed) {
+        CK(cudaEventRecord(h->ev[which][h->ev_used[which] + 1], h->st));
+        h->ev_used[which] += 2;
+    }
+    return REVSIM_OK;
+}
+
+int build_block_table(revsim_handle *h) {
+    std::vector<int> br, bm, bn;
+    for (int r = 0; r < h->R; r++)
+        for (int m = 0; m < h->nmol[r]; m += h->mpc) {
+            br.push_back(r);
+            bm.push_back(h->mol0[r] + m);
+            bn.push_back(std::min(h->mpc, h->nmol[r] - m));
+        }
+    h->n_blk = (int)br.size();
+    dfree(h->d_blk_rep);
+    dfree(h->d_blk_mol0);
+    dfree(h->d_blk_nmol);
+    dfree(h->d_part);
+    dfree(h->d_norm2);
+    h->d_blk_rep = h->d_blk_mol0 = h->d_blk_nmol = nullptr;
+    h->d_part = h->d_norm2 = nullptr;
+    CK(dalloc(&h->d_blk_rep, br.size()));
+    CK(dalloc(&h->d_blk_mol0, br.size()));
+    CK(dalloc(&h->d_blk_nmol, br.size()));
+    CK(dalloc(&h->d_part, br.size() * (size_t)std::max(h->P, 1)));
+    CK(dalloc(&h->d_norm2, br.size()));
+    CK(cudaMemcpy(h->d_blk_rep, br.data(), sizeof(int) * br.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_blk_mol0, bm.data(), sizeof(int) * bm.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_blk_nmol, bn.data(), sizeof(int) * bn.size(), cudaMemcpyHostToDevice));
+    return REVSIM_OK;
+}
+
+int alloc_nbr(revsim_handle *h, int cap) {
+    dfree(h->d_nbr);
+    h->d_nbr = nullptr;
+    dfree(h->d_nbr_store);
+    dfree(h->d_cnt_store);
+    h->d_nbr_store = nullptr;
+    h->d_cnt_store = nullptr;
+    h->store_slots = 0;
+    h->cap = cap;
+    CK(dalloc(&h->d_nbr, (size_t)h->M * cap));
+    return REVSIM_OK;
+}
+
+// Rows of every forward build (n slots), kept for the reverse pass when memory allows.
+void ensure_list_store(revsim_handle *h, size_t slots) {
+    if (slots <= 1) return;
+    if (h->d_nbr_store && h->store_slots >= slots && h->store_cap == (size_t)h->cap) return;
+    dfree(h->d_nbr_store);
+    dfree(h->d_cnt_store);
+    h->d_nbr_store = nullptr;
+    h->d_cnt_store = nullptr;
+    h->store_slots = 0;
+    uint32_t *p = nullptr;
+    int *c = nullptr;
+    if (cudaMalloc((void **)&p, sizeof(uint32_t) * (size_t)h->M * h->cap * slots) != cudaSuccess ||
+        cudaMalloc((void **)&c, sizeof(int) * (size_t)h->M * slots) != cudaSuccess) {
+        cudaGetLastError();   // clear the failed allocation; fall back to rebuilding
+        dfree(p);
+        dfree(c);
+        return;
+    }
+    h->d_nbr_store = p;
+    h->d_cnt_store = c;
+    h->store_slots = slots;
+    h->store_cap = h->cap;
+}
+
+// Neighbour list from positions xsrc (d_x or a checkpoint) into rows nbr / counts cnt
+// (the working list when null).
+int build_nlist(revsim_handle *h, const double *xsrc, uint32_t *nbr = nullptr, int *cnt = nullptr) {
+    NlistArgs a;
+    a.M = h->M;
+    a.n_cells = h->n_cells;
+    a.x = xsrc;
+    a.mol_rep = h->d_mol_rep;
+    a.rep_nc = h->d_rep_nc;
+    a.rep_cell_off = h->d_rep_cell_off;
+    a.rep_box = h->d_rep_box;
+    a.cell_of_mol = h->d_cell_of_mol;
+    a.cell_cnt = h->d_cell_cnt;
+    a.cell_start = h->d_cell_start;
+    a.cell_fill = h->d_cell_fill;
+    a.cell_tmp = h->d_cell_tmp;
+    a.cell_sorted = h->d_cell_sorted;
+    a.nbr = nbr ? nbr : h->d_nbr;
+    a.nbr_cnt = cnt ? cnt : h->d_nbr_cnt;
+    a.cap = h->cap;
+    a.cell_rep = h->d_cell_rep;
+    a.band = h->band;
+    a.rc_nl2 = h->rc_nl * h->rc_nl;
+    const double rcand = h->rc_nl + 2 * kRext;
+    a.rcand2 = rcand * rcand;
+    a.rext2 = kRext * kRext;
+    a.status = h->d_status;
+    a.max_cnt = h->d_maxcnt;
+    cudaError_t e = launch_nlist(a, h->st);
+    h->launches += 6;
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("nlist: ") + cudaGetErrorString(e));
+    return REVSIM_OK;
+}
+
+int read_status(revsim_handle *h, int *flags) {
+    int s = 0;
+    CK(cudaMemcpyAsync(&s, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
+    *flags = s;
+    return REVSIM_OK;
+}
+
+int status_code(revsim_handle *h, int s) {
+    if (s & ST_NLIST_OVERFLOW) return fail(h, REVSIM_ERR_NLIST_OVERFLOW, "neighbour row capacity exceeded");
+    if (s & ST_GEOMETRY)
+        return fail(h, REVSIM_ERR_GEOMETRY, "an O-H distance exceeds the 0.15 nm molecule bound");
+    if (s & ST_NAN) return fail(h, REVSIM_ERR_NAN, "non-finite force");
+    return REVSIM_OK;
+}
+
+// Grow the row capacity from the largest row seen (after a synchronising read).
+int grow_cap(revsim_handle *h) {
+    int mx = 0;
+    CK(cudaMemcpy(&mx, h->d_maxcnt, sizeof(int), cudaMemcpyDeviceToHost));
+    int ncap = std::max(h->cap * 5 / 4, (mx * 5 / 4 + 31) / 32 * 32);
+    return alloc_nbr(h, ncap);
+}
+
+// Build at the current positions and make sure the rows fit.
+int build_nlist_checked(revsim_handle *h, const double *xsrc) {
+    for (int attempt = 0; attempt < 4; attempt++) {
+        int rc = build_nlist(h, xsrc);
+        if (rc) return rc;
+        int s;
+        rc = read_status(h, &s);
+        if (rc) return rc;
+        if (!(s & ST_NLIST_OVERFLOW)) return status_code(h, s);
+        rc = grow_cap(h);
+        if (rc) return rc;
+    }
+    return fail(h, REVSIM_ERR_NLIST_OVERFLOW, "neighbour rows keep overflowing");
+}
+
+int pack(revsim_handle *h, int buf, bool with_w) {
+    cudaError_t e = launch_pack(h->N, h->prec, h->d_x, with_w ? h->d_C : nullptr, h->mO, h->mH,
+                                h->d_atom_rep, h->d_rep_box, h->d_pos[buf], h->d_wgt[buf], h->st);
+    h->launches++;
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("pack: ") + cudaGetErrorString(e));
+    return REVSIM_OK;
+}
+
+// loss_fn / loss_and_grads at the current positions: adds the per-replica loss to
+// acc (device [R]) and, if grad, writes dL/dx into d_dLdx.
+int loss_dev(revsim_handle *h, bool grad, double *acc) {
+    if (grad) CK(cudaMemsetAsync(h->d_dLdx, 0, sizeof(double) * 3 * (size_t)h->N, h->st));
+    for (Term &T : h->terms) {
+        const revsim_rdf_term &t = T.t;
+        RdfArgs a;
+        a.x = h->d_x;
+        a.rep_atom0 = h->d_rep_atom0;
+        a.rep_nmol = h->d_rep_nmol;
+        a.rep_box = h->d_rep_box;
+        a.sel1 = t.sel1;
+        a.sel2 = t.sel2;
+        a.x_min = t.x_min;
+        a.step = t.step;
+        a.width = t.width;
+        a.cutoff = t.exp_cutoff;
+        a.n_grid = t.n_grid;
+        a.off = T.off;
+        a.hist = T.d_hist;
+        a.dLdh = T.d_dLdh;
+        a.dLdx = h->d_dLdx;
+        int mx = *std::max_element(h->nmol.begin(), h->nmol.end());
+        const int n1 = t.sel1 == 0 ? mx : 2 * mx, n2 = t.sel2 == 0 ? mx : 2 * mx;
+        CK(cudaMemsetAsync(T.d_hist, 0, sizeof(double) * (size_t)h->R * t.n_grid, h->st));
+        CK(launch_rdf(a, h->R, n1, n2, false, h->st));
+        CK(launch_rdf_finalize(a, h->R, T.d_hist + (size_t)h->R * t.n_grid, T.d_target, t.slice_start,
+                               t.slice_stride, t.n_target, t.norm, t.weight, acc, T.d_dLdh, h->st));
+        h->launches += 2;
+        if (grad) {
+            CK(launch_rdf(a, h->R, n1, n2, true, h->st));
+            h->launches++;
+        }
+    }
+    return REVSIM_OK;
+}
+
+int upload_seeds(revsim_handle *h, const uint64_t *seeds, size_t n) {
+    if (n > h->seeds_cap) {
+        dfree(h->d_seeds);
+        h->d_seeds = nullptr;
+        CK(dalloc(&h->d_seeds, n));
+        h->seeds_cap = n;
+    }
+    if (n) CK(cudaMemcpyAsync(h->d_seeds, seeds, sizeof(uint64_t) * n, cudaMemcpyHostToDevice, h->st));
+    return REVSIM_OK;
+}
+
+int ensure_store(revsim_handle *h, double **p, size_t *cap, size_t n) {
+    if (n > *cap) {
+        dfree(*p);
+        *p = nullptr;
+        CK(dalloc(p, n));
+        *cap = n;
+    }
+    return REVSIM_OK;
+}
+
+int check_ready(revsim_handle *h) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (!h->have_params) return fail(h, REVSIM_ERR_STATE, "parameters not set");
+    if (!h->have_state) return fail(h, REVSIM_ERR_STATE, "state not set");
+    CK(cudaSetDevice(h->dev));
+    return REVSIM_OK;
+}
+
+int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, double dt, int calc_loss) {
+    const double c = std::exp(-gamma * dt), s = std::sqrt(1 - c * c);
+    const size_t n3 = 3 * (size_t)h->N;
+    const int R = h->R;
+    int rc;
+    if ((rc = pack(h, 0, false))) return rc;
+    int cur = 0;
+    const bool store = h->d_nbr_store != nullptr;
+    uint32_t *nbr = store ? h->d_nbr_store : h->d_nbr;
+    int *ncnt = store ? h->d_cnt_store : h->d_nbr_cnt;
+    CK(cudaMemcpyAsync(h->d_ckpt, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    if ((rc = build_nlist(h, h->d_x, nbr, ncnt))) return rc;
+    CK(cudaMemcpyAsync(h->d_snap_x, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_snap_v, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
+    StepArgs a = base_args(h);
+    a.dt = dt;
+    a.c = c;
+    a.s = s;
+    for (int step = 1; step <= n_steps; step++) {
+        a.cap = h->cap;
+        a.nbr = nbr;
+        a.nbr_cnt = ncnt;
+        a.pos_in = h->d_pos[cur];
+        a.pos_out = h->d_pos[cur ^ 1];
+        a.seed_cur = h->d_seeds + (size_t)(step - 1) * R;
+        if ((rc = launch_step_k(h, false, a))) return rc;
+        cur ^= 1;
+        if (step % h->nf == 0 && step < n_steps) {
+            const size_t k = (size_t)(step / h->nf);
+            CK(cudaMemcpyAsync(h->d_ckpt + k * n3, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                               h->st));
+            if (store) {
+                nbr = h->d_nbr_store + k * (size_t)h->M * h->cap;
+                ncnt = h->d_cnt_store + k * (size_t)h->M;
+            }
+            if ((rc = build_nlist(h, h->d_x, nbr, ncnt))) return rc;
+        }
+        if (h->nlog > 0 && step % h->nlog == 0) {
+            const size_t si = (size_t)(step / h->nlog) * n3;
+            CK(cudaMemcpyAsync(h->d_snap_x + si, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+            CK(cudaMemcpyAsync(h->d_snap_v + si, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+        }
+        if (calc_loss && !h->terms.empty() && step % n_steps_loss == 0)
+            if ((rc = loss_dev(h, false, h->d_loss_acc))) return rc;
+    }
+    return REVSIM_OK;
+}
+
+int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, int n_steps_trunc,
+                 double dt, double clip) {
+    const double c = std::exp(-gamma * dt), s = std::sqrt(1 - c * c);
+    const size_t n3 = 3 * (size_t)h->N;
+    const int R = h->R;
+    const bool clipping = std::isfinite(clip);
+    int rc;
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * h->P, h->st));
+    CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
+    if ((rc = loss_dev(h, true, h->d_loss_acc))) return rc;
+    CK(launch_init_adjoint(h->N, h->d_dLdx, c, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->st));
+    h->launches++;
+
+    StepArgs a = base_args(h);
+    a.dt = dt;
+    a.c = c;
+    a.s = s;
+    const double dt2 = dt * dt;
+    a.acoefO = dt2 / (2 * h->mO);
+    a.acoefH = dt2 / (2 * h->mH);
+    a.norm2 = clipping ? h->d_norm2 : nullptr;
+
+    int cur = 0;
+    long group = -1;
+    bool pending = true;
+    int trunc = 0;
+    if (h->nl_mode == REVSIM_NL_RECONSTRUCTED)
+        if ((rc = build_nlist(h, h->d_x))) return rc;
+    std::vector<double> scale(2 * R);
+    for (int step_n = n_steps; step_n >= 1; step_n--) {
+        trunc++;
+        const bool restore = h->nlog > 0 && (step_n - 1) % h->nlog == 0 && step_n > 1;
+        const bool lossb = (step_n - 1) % n_steps_loss == 0 && step_n > 1;
+        if (trunc <= n_steps_trunc) {
+            const int m = step_n - 1;
+            if (pending) {
+                StepArgs u = a;
+                u.seed_cur = h->d_seeds + (size_t)(step_n - 1) * R;
+                u.pos_out = h->d_pos[cur];
+                u.wgt_out = h->d_wgt[cur];
+                CK(launch_unintegrate(h->M, h->prec, u, h->d_mol_rep, h->st));
+                h->launches++;
+            }
+            if (h->nl_mode == REVSIM_NL_CHECKPOINT) {
+                const long g = m / h->nf;
+                if (g != group) {
+                    if (h->d_nbr_store && (size_t)g < h->store_slots) {
+                        a.nbr = h->d_nbr_store + (size_t)g * h->M * h->cap;
+                        a.nbr_cnt = h->d_cnt_store + (size_t)g * h->M;
+                    } else {
+                        if ((rc = build_nlist(h, h->d_ckpt + (size_t)g * n3))) return rc;
+                        a.nbr = h->d_nbr;
+                        a.nbr_cnt = h->d_nbr_cnt;
+                    }
+                    group = g;
+                }
+            } else if (step_n % h->nf == 0) {
+                if ((rc = build_nlist(h, h->d_x))) return rc;
+            }
+            const bool next_active = step_n > 1 && trunc + 1 <= n_steps_trunc && !restore && !lossb;
+            const bool fuse = next_active && !clipping;
+            a.cap = h->cap;
+            if (h->nl_mode != REVSIM_NL_CHECKPOINT) {
+                a.nbr = h->d_nbr;
+                a.nbr_cnt = h->d_nbr_cnt;
+            }
+            a.pos_in = h->d_pos[cur];
+            a.wgt_in = h->d_wgt[cur];
+            a.pos_out = h->d_pos[cur ^ 1];
+            a.wgt_out = h->d_wgt[cur ^ 1];
+            a.seed_next = fuse ? h->d_seeds + (size_t)(step_n - 2) * R : nullptr;
+            a.mode = (fuse ? MODE_FUSE_NEXT : 0) | (clipping ? MODE_DEFER_BA : 0);
+            if ((rc = launch_step_k(h, true, a))) return rc;
+            if (clipping) {
+                // Per-replica norm of dl_dfi from the block partials (fixed order).
+                std::vector<double> n2(h->n_blk);
+                std::vector<int> br(h->n_blk);
+                CK(cudaMemcpyAsync(n2.data(), h->d_norm2, sizeof(double) * h->n_blk, cudaMemcpyDeviceToHost, h->st));
+                CK(cudaMemcpyAsync(br.data(), h->d_blk_rep, sizeof(int) * h->n_blk, cudaMemcpyDeviceToHost, h->st));
+                CK(cudaStreamSynchronize(h->st));
+                std::vector<double> acc(R, 0.0);
+                for (int b = 0; b < h->n_blk; b++) acc[br[b]] += n2[b];
+                for (int r = 0; r < R; r++) {
+                    scale[2 * r] = std::sqrt(acc[r]);
+                    scale[2 * r + 1] = clip;
+                }
+                CK(cudaMemcpyAsync(h->d_scale, scale.data(), sizeof(double) * 2 * R, cudaMemcpyHostToDevice, h->st));
+                CK(launch_clip_post(h->N, a, h->d_atom_rep, h->d_scale, h->st));
+                h->launches++;
+            }
+            if (fuse) {
+                cur ^= 1;
+                pending = false;
+            } else {
+                pending = true;
+            }
+        }
+        if (restore && (trunc <= n_steps_trunc || lossb)) {
+            const size_t si = (size_t)((step_n - 1) / h->nlog) * n3;
+            CK(cudaMemcpyAsync(h->d_x, h->d_snap_x + si, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+            CK(cudaMemcpyAsync(h->d_v, h->d_snap_v + si, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+            pending = true;
+        }
+        if (lossb) {
+            trunc = 0;
+            if ((rc = loss_dev(h, true, h->d_loss_acc))) return rc;
+            CK(launch_init_adjoint(h->N, h->d_dLdx, c, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->st));
+            h->launches++;
+            pending = true;
+        }
+    }
+    return REVSIM_OK;
+}
+
+// Fold the per-launch event pairs recorded since the last call into the totals.
+int collect_kernel_times(revsim_handle *h) {
+    for (int w = 0; w < 2; w++) {
+        for (size_t i = 0; i + 1 < h->ev_used[w]; i += 2) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->ev[w][i], h->ev[w][i + 1]));
+            h->kt_ms[w] += ms;
+            h->kt_n[w]++;
+        }
+        h->ev_used[w] = 0;
+    }
+    return REVSIM_OK;
+}
+
+// Sum the dtheta block partials per replica (FP64, block order).
+int reduce_part(revsim_handle *h, std::vector<double> &out) {
+    std::vector<double> part((size_t)h->n_blk * h->P);
+    std::vector<int> br(h->n_blk);
+    CK(cudaMemcpyAsync(part.data(), h->d_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(br.data(), h->d_blk_rep, sizeof(int) * h->n_blk, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    out.assign((size_t)h->R * h->P, 0.0);
+    for (int b = 0; b < h->n_blk; b++)
+        for (int p = 0; p < h->P; p++) out[(size_t)br[b] * h->P + p] += part[(size_t)b * h->P + p];
+    return REVSIM_OK;
+}
+
+void free_all(revsim_handle *h) {
+    void *ptrs[] = {h->d_blk_rep, h->d_blk_mol0, h->d_blk_nmol, h->d_mol_rep, h->d_atom_rep,
+                    h->d_rep_atom0, h->d_rep_nmol, h->d_rep_box, h->d_rep_sdO, h->d_rep_sdH,
+                    h->d_rep_nc, h->d_rep_cell_off, h->d_cell_of_mol, h->d_cell_cnt, h->d_cell_start,
+                    h->d_cell_fill, h->d_cell_tmp, h->d_cell_sorted, h->d_nbr, h->d_nbr_cnt, h->d_x,
+                    h->d_v, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->d_F, h->d_x0, h->d_v0,
+                    h->d_pos[0], h->d_pos[1], h->d_wgt[0], h->d_wgt[1], h->d_part, h->d_norm2,
+                    h->d_scale, h->d_status, h->d_maxcnt, h->d_count, h->d_snap_x, h->d_snap_v,
+                    h->d_ckpt, h->d_seeds, h->d_loss, h->d_loss_acc, h->d_dLdx,
+                    h->d_cell_rep, h->d_nbr_store, h->d_cnt_store};
+    for (void *p : ptrs) dfree(p);
+    for (Term &T : h->terms) {
+        dfree(T.d_target);
+        dfree(T.d_hist);
+        dfree(T.d_dLdh);
+    }
+    for (int w = 0; w < 2; w++)
+        for (cudaEvent_t e : h->ev[w]) cudaEventDestroy(e);
+    if (h->st) cudaStreamDestroy(h->st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
+    if (!d || !out) return REVSIM_ERR_BADARG;
+    *out = nullptr;
+    revsim_handle *h = new (std::nothrow) revsim_handle();
+    if (!h) return REVSIM_ERR_NOMEM;
+    auto bad = [&](const char *m) {
+        delete h;
+        (void)m;
+        return REVSIM_ERR_BADARG;
+    };
+    if (d->n_replicas < 1 || !d->n_mol || !d->box || !d->temp) return bad("replicas");
+    if (form_nparams(d->inter_type) < 0) return bad("inter_type");
+    if (d->precision != REVSIM_FP64 && d->precision != REVSIM_MIXED) return bad("precision");
+    if (!(d->m_O > 0 && d->m_H > 0 && d->cutoff > 0 && d->nl_cutoff >= d->cutoff && d->kB > 0))
+        return bad("constants");
+    if (d->n_steps_nf < 1 || d->n_steps_log < 0) return bad("periods");
+    h->R = d->n_replicas;
+    long long M = 0;
+    for (int r = 0; r < h->R; r++) {
+        if (d->n_mol[r] < 1 || !(d->box[r] > 2 * d->nl_cutoff) || !(d->temp[r] >= 0)) return bad("replica");
+        h->nmol.push_back(d->n_mol[r]);
+        h->mol0.push_back((int)M);
+        h->atom0.push_back((int)(3 * M));
+        h->box.push_back(d->box[r]);
+        h->temp.push_back(d->temp[r]);
+        M += d->n_mol[r];
+    }
+    if (M >= (1LL << 23)) return bad("too many molecules");
+    h->M = (int)M;
+    h->N = 3 * h->M;
+    h->form = d->inter_type;
+    h->prec = d->precision;
+    h->nl_mode = d->nl_mode;
+    h->nf = d->n_steps_nf;
+    h->nlog = d->n_steps_log;
+    h->mO = d->m_O;
+    h->mH = d->m_H;
+    h->ke = d->coulomb_const;
+    h->krf = d->crf_const;
+    h->rc = d->cutoff;
+    h->rc_nl = d->nl_cutoff;
+    h->kB = d->kB;
+    h->dev = d->device;
+    h->NFp = form_nparams(h->form);
+    h->P = h->NFp + 5;
+    h->shift_ok = true;
+    for (int r = 0; r < h->R; r++)
+        if (!(h->box[r] > 2 * (h->rc + 2 * kRext) + 0.02)) h->shift_ok = false;
+
+    if (cudaSetDevice(h->dev) != cudaSuccess || cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return REVSIM_ERR_CUDA;
+    }
+    auto cfail = [&](const char *what) {
+        free_all(h);
+        delete h;
+        (void)what;
+        return REVSIM_ERR_CUDA;
+    };
+    // replica tables
+    const double rcand = h->rc_nl + 2 * kRext;
+    std::vector<int> mol_rep(h->M), atom_rep(h->N), rep_nc(h->R), rep_coff(h->R);
+    std::vector<double> sdO(h->R), sdH(h->R);
+    int ncell = 0, cap = 32;
+    for (int r = 0; r < h->R; r++) {
+        for (int m = 0; m < h->nmol[r]; m++) mol_rep[h->mol0[r] + m] = r;
+        for (int a = 0; a < 3 * h->nmol[r]; a++) atom_rep[h->atom0[r] + a] = r;
+        int nc = std::max(1, (int)std::floor(h->box[r] / (rcand / 2)));
+        nc = std::min(nc, 64);
+        rep_nc[r] = nc;
+        rep_coff[r] = ncell;
+        ncell += nc * nc * nc;
+        sdO[r] = std::sqrt(h->kB * h->temp[r] / h->mO);
+        sdH[r] = std::sqrt(h->kB * h->temp[r] / h->mH);
+        const double rho = h->nmol[r] / (h->box[r] * h->box[r] * h->box[r]);
+        const double rr = h->rc_nl + 0.25;
+        const double expect = 4.0 / 3.0 * 3.14159265358979 * rr * rr * rr * rho;
+        cap = std::max(cap, (int)((expect * 1.5 + 32 + 31) / 32) * 32);
+    }
+    cap = std::min(cap, h->M);
+    cap = std::max(cap, 32);
+    h->nc = rep_nc;
+    h->cell_off = rep_coff;
+    h->n_cells = ncell;
+    std::vector<int> cell_rep(ncell);
+    double lmax = 0;
+    for (int r = 0; r < h->R; r++) {
+        for (int c = 0; c < rep_nc[r] * rep_nc[r] * rep_nc[r]; c++) cell_rep[rep_coff[r] + c] = r;
+        lmax = std::max(lmax, h->box[r]);
+    }
+    // FP32 coordinates of a box of side L round to within L * 2^-24; the FP32 distance^2
+    // near the 1.2 nm cutoff is then within ~6e-6 (L/8) of the FP64 value.
+    h->band = (float)(2e-5 * std::max(1.0, lmax / 4.0));
+    const size_t n3 = 3 * (size_t)h->N;
+    const size_t v4 = h->prec == REVSIM_MIXED ? sizeof(float4) : sizeof(double4);
+    bool ok = dalloc(&h->d_mol_rep, h->M) == cudaSuccess && dalloc(&h->d_atom_rep, h->N) == cudaSuccess &&
+              dalloc(&h->d_rep_atom0, h->R) == cudaSuccess && dalloc(&h->d_rep_nmol, h->R) == cudaSuccess &&
+              dalloc(&h->d_rep_box, h->R) == cudaSuccess && dalloc(&h->d_rep_sdO, h->R) == cudaSuccess &&
+              dalloc(&h->d_rep_sdH, h->R) == cudaSuccess && dalloc(&h->d_rep_nc, h->R) == cudaSuccess &&
+              dalloc(&h->d_rep_cell_off, h->R) == cudaSuccess &&
+              dalloc(&h->d_cell_of_mol, h->M) == cudaSuccess && dalloc(&h->d_cell_cnt, ncell) == cudaSuccess &&
+              dalloc(&h->d_cell_start, ncell) == cudaSuccess && dalloc(&h->d_cell_fill, ncell) == cudaSuccess &&
+              dalloc(&h->d_cell_tmp, h->M) == cudaSuccess && dalloc(&h->d_cell_sorted, h->M) == cudaSuccess &&
+              dalloc(&h->d_nbr_cnt, h->M) == cudaSuccess && dalloc(&h->d_x, n3) == cudaSuccess &&
+              dalloc(&h->d_v, n3) == cudaSuccess && dalloc(&h->d_A, n3) == cudaSuccess &&
+              dalloc(&h->d_B, n3) == cudaSuccess && dalloc(&h->d_C, n3) == cudaSuccess &&
+              dalloc(&h->d_D, n3) == cudaSuccess && dalloc(&h->d_G, n3) == cudaSuccess &&
+              dalloc(&h->d_F, n3) == cudaSuccess && dalloc(&h->d_x0, n3) == cudaSuccess &&
+              dalloc(&h->d_v0, n3) == cudaSuccess && dalloc(&h->d_dLdx, n3) == cudaSuccess &&
+              cudaMalloc(&h->d_pos[0], v4 * h->N) == cudaSuccess && cudaMalloc(&h->d_pos[1], v4 * h->N) == cudaSuccess &&
+              cudaMalloc(&h->d_wgt[0], v4 * h->N) == cudaSuccess && cudaMalloc(&h->d_wgt[1], v4 * h->N) == cudaSuccess &&
+              dalloc(&h->d_scale, 2 * h->R) == cudaSuccess && dalloc(&h->d_status, 1) == cudaSuccess &&
+              dalloc(&h->d_maxcnt, 1) == cudaSuccess && dalloc(&h->d_count, 1) == cudaSuccess &&
+              dalloc(&h->d_loss, h->R) == cudaSuccess && dalloc(&h->d_loss_acc, h->R) == cudaSuccess &&
+              dalloc(&h->d_cell_rep, ncell) == cudaSuccess;
+    if (!ok) return cfail("alloc");
+    std::vector<int> rep_nmol(h->nmol.begin(), h->nmol.end());
+    ok = cudaMemcpy(h->d_mol_rep, mol_rep.data(), sizeof(int) * h->M, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_atom_rep, atom_rep.data(), sizeof(int) * h->N, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_atom0, h->atom0.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_nmol, rep_nmol.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_box, h->box.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_sdO, sdO.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_sdH, sdH.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_nc, rep_nc.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_rep_cell_off, rep_coff.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(h->d_cell_rep, cell_rep.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(h->d_status, 0, sizeof(int)) == cudaSuccess && cudaMemset(h->d_maxcnt, 0, sizeof(int)) == cudaSuccess &&
+         cudaMemset(h->d_C, 0, sizeof(double) * n3) == cudaSuccess &&
+         cudaMemset(h->d_A, 0, sizeof(double) * n3) == cudaSuccess;
+    if (!ok) return cfail("upload");
+    if (build_block_table(h) != REVSIM_OK || alloc_nbr(h, cap) != REVSIM_OK) return cfail("tables");
+    *out = h;
+    return REVSIM_OK;
+}
+
+void revsim_destroy(revsim_handle *h) {
+    if (!h) return;
+    cudaSetDevice(h->dev);
+    if (h->st) cudaStreamSynchronize(h->st);
+    free_all(h);
+    delete h;
+}
+
+const char *revsim_last_error(const revsim_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int32_t revsim_device_status(revsim_handle *h, int32_t *flags) {
+    if (!h || !flags) return REVSIM_ERR_BADARG;
+    int s = 0;
+    int rc = read_status(h, &s);
+    *flags = s;
+    return rc;
+}
+
+int32_t revsim_sizes(const revsim_handle *h, int64_t *n_atoms, int32_t *n_params) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (n_atoms) *n_atoms = h->N;
+    if (n_params) *n_params = h->P;
+    return REVSIM_OK;
+}
+
+int32_t revsim_set_params(revsim_handle *h, const double *theta, int32_t n) {
+    if (!h || !theta) return REVSIM_ERR_BADARG;
+    if (n != h->P) return fail(h, REVSIM_ERR_BADARG, "wrong parameter count");
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(theta[i])) return fail(h, REVSIM_ERR_BADARG, "non-finite parameter");
+    if (theta[h->NFp] == 0.0) return fail(h, REVSIM_ERR_BADARG, "q_O must be non-zero");
+    h->theta.assign(theta, theta + n);
+    h->have_params = true;
+    return REVSIM_OK;
+}
+
+int32_t revsim_set_state(revsim_handle *h, const double *x, const double *v) {
+    if (!h || !x || !v) return REVSIM_ERR_BADARG;
+    CK(cudaSetDevice(h->dev));
+    const size_t n3 = 3 * (size_t)h->N;
+    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->have_state = true;
+    return REVSIM_OK;
+}
+
+int32_t revsim_get_state(revsim_handle *h, double *x, double *v) {
+    if (!h) return REVSIM_ERR_BADARG;
+    CK(cudaSetDevice(h->dev));
+    const size_t n3 = 3 * (size_t)h->N;
+    if (x) CK(cudaMemcpyAsync(x, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->st));
+    if (v) CK(cudaMemcpyAsync(v, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
+int32_t revsim_set_loss(revsim_handle *h, int32_t n_terms, const revsim_rdf_term *terms,
+                        const double *const *targets) {
+    if (!h || n_terms < 0 || (n_terms > 0 && (!terms || !targets))) return REVSIM_ERR_BADARG;
+    CK(cudaSetDevice(h->dev));
+    for (Term &T : h->terms) {
+        dfree(T.d_target);
+        dfree(T.d_hist);
+        dfree(T.d_dLdh);
+    }
+    h->terms.clear();
+    for (int i = 0; i < n_terms; i++) {
+        const revsim_rdf_term &t = terms[i];
+        if (t.n_grid < 1 || !(t.step > 0) || !(t.width > 0) || !(t.exp_cutoff >= 0) || t.n_target < 0 ||
+            t.slice_start < 0 || (t.n_target > 0 && (t.slice_stride < 1 ||
+                                                     t.slice_start + (long long)(t.n_target - 1) * t.slice_stride >= t.n_grid)) ||
+            (t.norm != 1 && t.norm != 2) || (t.sel1 != 0 && t.sel1 != 1) || (t.sel2 != 0 && t.sel2 != 1) ||
+            !targets[i])
+            return fail(h, REVSIM_ERR_BADARG, "bad loss term");
+        const double q = t.x_min / t.step;
+        if (std::fabs(q - std::llround(q)) > 1e-6)
+            return fail(h, REVSIM_ERR_BADARG, "x_min must be a multiple of step (water.jl:660)");
+        Term T;
+        T.t = t;
+        T.off = (int)std::llround(q) - 1;
+        if (dalloc(&T.d_target, (size_t)h->R * std::max(t.n_target, 1)) != cudaSuccess ||
+            dalloc(&T.d_hist, (size_t)h->R * t.n_grid + h->R) != cudaSuccess ||
+            dalloc(&T.d_dLdh, (size_t)h->R * t.n_grid) != cudaSuccess) {
+            dfree(T.d_target);
+            dfree(T.d_hist);
+            dfree(T.d_dLdh);
+            return fail(h, REVSIM_ERR_NOMEM, "loss buffers");
+        }
+        h->terms.push_back(T);
+        if (t.n_target > 0)
+            CK(cudaMemcpy(T.d_target, targets[i], sizeof(double) * (size_t)h->R * t.n_target, cudaMemcpyHostToDevice));
+        std::vector<double> pre(h->R);
+        for (int r = 0; r < h->R; r++) {
+            const double n1 = t.sel1 == 0 ? h->nmol[r] : 2.0 * h->nmol[r];
+            const double n2 = t.sel2 == 0 ? h->nmol[r] : 2.0 * h->nmol[r];
+            const double V = h->box[r] * h->box[r] * h->box[r];
+            pre[r] = V / (4 * 3.14159265358979323846 * n1 * n2 * t.step);
+        }
+        CK(cudaMemcpy(T.d_hist + (size_t)h->R * t.n_grid, pre.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice));
+    }
+    return REVSIM_OK;
+}
+
+int32_t revsim_neighbor_pairs(revsim_handle *h, int32_t replica, int32_t *pairs, int64_t cap,
+                              int64_t *count) {
+    if (!h || !count || replica < 0 || replica >= h->R || cap < 0 || (cap > 0 && !pairs)) return REVSIM_ERR_BADARG;
+    if (!h->have_state) return fail(h, REVSIM_ERR_STATE, "state not set");
+    CK(cudaSetDevice(h->dev));
+    int rc = build_nlist_checked(h, h->d_x);
+    if (rc) return rc;
+    int32_t *d_pairs = nullptr;
+    CK(dalloc(&d_pairs, 2 * (size_t)std::max<int64_t>(cap, 1)));
+    CK(cudaMemsetAsync(h->d_count, 0, sizeof(unsigned long long), h->st));
+    cudaError_t e = launch_export_pairs(h->d_nbr, h->d_nbr_cnt, h->cap, h->mol0[replica], h->nmol[replica],
+                                        d_pairs, h->d_count, cap, h->st);
+    h->launches++;
+    unsigned long long n = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&n, h->d_count, sizeof(n), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    const int64_t w = std::min<int64_t>((int64_t)n, cap);
+    if (e == cudaSuccess && w > 0) e = cudaMemcpy(pairs, d_pairs, sizeof(int32_t) * 2 * w, cudaMemcpyDeviceToHost);
+    cudaFree(d_pairs);
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, cudaGetErrorString(e));
+    *count = (int64_t)n;
+    return REVSIM_OK;
+}
+
+int32_t revsim_forces(revsim_handle *h, double *F) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!F) return fail(h, REVSIM_ERR_BADARG, "F is null");
+    if ((rc = build_nlist_checked(h, h->d_x))) return rc;
+    if ((rc = pack(h, 0, false))) return rc;
+    StepArgs a = base_args(h);
+    a.pos_in = h->d_pos[0];
+    a.F_out = h->d_F;
+    a.mode = MODE_FORCES_ONLY;
+    if ((rc = launch_step_k(h, false, a))) return rc;
+    CK(cudaMemcpyAsync(F, h->d_F, sizeof(double) * 3 * (size_t)h->N, cudaMemcpyDeviceToHost, h->st));
+    int s;
+    if ((rc = read_status(h, &s))) return rc;
+    return status_code(h, s);
+}
+
+int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef, double *F,
+                         double *dl_dfi, double *dtheta) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!w || !acoef) return fail(h, REVSIM_ERR_BADARG, "null input");
+    const size_t n3 = 3 * (size_t)h->N;
+    CK(cudaMemcpyAsync(h->d_C, w, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_A, acoef, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
+    if ((rc = build_nlist_checked(h, h->d_x))) return rc;
+    if ((rc = pack(h, 0, true))) return rc;
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * h->P, h->st));
+    StepArgs a = base_args(h);
+    a.pos_in = h->d_pos[0];
+    a.wgt_in = h->d_wgt[0];
+    a.F_out = h->d_F;
+    a.acoefO = 1.0;
+    a.acoefH = 1.0;
+    a.mode = MODE_FORCES_ONLY;
+    if ((rc = launch_step_k(h, true, a))) return rc;
+    if (F) CK(cudaMemcpyAsync(F, h->d_F, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->st));
+    if (dl_dfi) CK(cudaMemcpyAsync(dl_dfi, h->d_G, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->st));
+    std::vector<double> th;
+    if ((rc = reduce_part(h, th))) return rc;
+    if (dtheta) std::memcpy(dtheta, th.data(), sizeof(double) * th.size());
+    int s;
+    if ((rc = read_status(h, &s))) return rc;
+    return status_code(h, s);
+}
+
+int32_t revsim_noise(revsim_handle *h, const uint64_t *seeds, double *xi) {
+    if (!h || !seeds || !xi) return REVSIM_ERR_BADARG;
+    CK(cudaSetDevice(h->dev));
+    int rc = upload_seeds(h, seeds, h->R);
+    if (rc) return rc;
+    CK(launch_noise(h->N, h->d_atom_rep, h->d_rep_atom0, h->d_rep_sdO, h->d_rep_sdH, h->d_seeds, h->d_F, h->st));
+    h->launches++;
+    CK(cudaMemcpyAsync(xi, h->d_F, sizeof(double) * 3 * (size_t)h->N, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
+int32_t revsim_loss_grad(revsim_handle *h, double *loss, double *dLdx) {
+    if (!h || !loss) return REVSIM_ERR_BADARG;
+    if (!h->have_state) return fail(h, REVSIM_ERR_STATE, "state not set");
+    CK(cudaSetDevice(h->dev));
+    CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double) * h->R, h->st));
+    int rc = loss_dev(h, dLdx != nullptr, h->d_loss);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(loss, h->d_loss, sizeof(double) * h->R, cudaMemcpyDeviceToHost, h->st));
+    if (dLdx) CK(cudaMemcpyAsync(dLdx, h->d_dLdx, sizeof(double) * 3 * (size_t)h->N, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
+int32_t revsim_rdf(revsim_handle *h, int32_t term, int32_t replica, double *hist) {
+    if (!h || !hist || term < 0 || term >= (int)h->terms.size() || replica < 0 || replica >= h->R)
+        return REVSIM_ERR_BADARG;
+    if (!h->have_state) return fail(h, REVSIM_ERR_STATE, "state not set");
+    CK(cudaSetDevice(h->dev));
+    std::vector<Term> keep = h->terms;
+    h->terms.assign(1, keep[term]);
+    CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double) * h->R, h->st));
+    int rc = loss_dev(h, false, h->d_loss);
+    h->terms = keep;
+    if (rc) return rc;
+    const Term &T = h->terms[term];
+    CK(cudaMemcpyAsync(hist, T.d_hist + (size_t)replica * T.t.n_grid, sizeof(double) * T.t.n_grid,
+                       cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
+int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, double dt, int32_t calc_loss, double *loss_out) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (n_steps < 0 || (n_steps > 0 && !noise_seeds) || !(dt > 0) || !(gamma >= 0))
+        return fail(h, REVSIM_ERR_BADARG, "bad forward arguments");
+    if (calc_loss && n_steps > 0 && n_steps_loss < 1) return fail(h, REVSIM_ERR_BADARG, "n_steps_loss < 1");
+    const size_t n3 = 3 * (size_t)h->N;
+    if ((rc = upload_seeds(h, noise_seeds, (size_t)n_steps * h->R))) return rc;
+    const size_t n_snap = (h->nlog > 0 ? (size_t)n_steps / h->nlog : 0) + 1;
+    const size_t n_ckpt = n_steps > 0 ? (size_t)(n_steps - 1) / h->nf + 1 : 1;
+    if ((rc = ensure_store(h, &h->d_snap_x, &h->snap_cap, n_snap * n3))) return rc;
+    if ((rc = ensure_store(h, &h->d_snap_v, &h->snapv_cap, n_snap * n3))) return rc;
+    if ((rc = ensure_store(h, &h->d_ckpt, &h->ckpt_cap, n_ckpt * n3))) return rc;
+    CK(cudaMemcpyAsync(h->d_x0, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_v0, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemsetAsync(h->d_maxcnt, 0, sizeof(int), h->st));
+    for (int attempt = 0; attempt < 3; attempt++) {
+        if (h->nl_mode == REVSIM_NL_CHECKPOINT) ensure_list_store(h, n_ckpt);
+        if ((rc = forward_impl(h, gamma, n_steps, n_steps_loss, dt, calc_loss))) return rc;
+        int s;
+        if ((rc = read_status(h, &s))) return rc;
+        if (!(s & ST_NLIST_OVERFLOW)) {
+            if ((rc = status_code(h, s))) return rc;
+            break;
+        }
+        if (attempt == 2) return status_code(h, s);
+        if ((rc = grow_cap(h))) return rc;
+        CK(cudaMemcpyAsync(h->d_x, h->d_x0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+        CK(cudaMemcpyAsync(h->d_v, h->d_v0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    }
+    if (loss_out) {
+        const int n_blocks = n_steps == 0 ? 1 : std::max(1, n_steps / std::max(1, n_steps_loss));
+        std::vector<double> l(h->R);
+        CK(cudaMemcpy(l.data(), h->d_loss_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));
+        for (int r = 0; r < h->R; r++) loss_out[r] = calc_loss ? l[r] / n_blocks : 0.0;
+    }
+    if (h->ktime && (rc = collect_kernel_times(h))) return rc;
+    h->fwd_valid = true;
+    h->fwd_steps = n_steps;
+    return REVSIM_OK;
+}
+
+int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                       double clip_norm_threshold, double *loss_out, double *dl_dp_out) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (n_steps_trunc > n_steps_loss)
+        return fail(h, REVSIM_ERR_BADARG, "n_steps_trunc must not be greater than n_steps_loss");
+    if (n_steps < 1 || n_steps_loss < 1 || !noise_seeds || !(dt > 0) || !(gamma >= 0) || !(clip_norm_threshold > 0))
+        return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
+    if (h->terms.empty()) return fail(h, REVSIM_ERR_STATE, "no loss set");
+    const bool need_store = h->nl_mode == REVSIM_NL_CHECKPOINT || (h->nlog > 0 && n_steps > h->nlog);
+    if (need_store && !(h->fwd_valid && h->fwd_steps == n_steps))
+        return fail(h, REVSIM_ERR_STATE, "reverse needs the forward pass of the same n_steps");
+    if ((rc = upload_seeds(h, noise_seeds, (size_t)n_steps * h->R))) return rc;
+    if ((rc = reverse_impl(h, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip_norm_threshold))) return rc;
+    int s;
+    if ((rc = read_status(h, &s))) return rc;
+    if ((rc = status_code(h, s))) return rc;
+    const int n_blocks = n_steps / n_steps_loss;
+    std::vector<double> th;
+    if ((rc = reduce_part(h, th))) return rc;
+    if (dl_dp_out)
+        for (size_t i = 0; i < th.size(); i++) dl_dp_out[i] = th[i] / n_blocks;
+    if (loss_out) {
+        std::vector<double> l(h->R);
+        CK(cudaMemcpy(l.data(), h->d_loss_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));
+        for (int r = 0; r < h->R; r++) loss_out[r] = l[r] / n_blocks;
+    }
+    if (h->ktime && (rc = collect_kernel_times(h))) return rc;
+    return REVSIM_OK;
+}
+
+void *revsim_stream(revsim_handle *h) { return h ? (void *)h->st : nullptr; }
+
+int64_t revsim_launch_count(const revsim_handle *h) { return h ? h->launches : 0; }
+
+int32_t revsim_set_kernel_timing(revsim_handle *h, int32_t enable) {
+    if (!h) return REVSIM_ERR_BADARG;
+    h->ktime = enable != 0;
+    for (int w = 0; w < 2; w++) {
+        h->kt_ms[w] = 0.0;
+        h->kt_n[w] = 0;
+        h->ev_used[w] = 0;
+    }
+    return REVSIM_OK;
+}
+
+int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, int64_t *launches) {
+    if (!h || which < 0 || which > 1) return REVSIM_ERR_BADARG;
+    if (total_ms) *total_ms = h->kt_ms[which];
+    if (launches) *launches = h->kt_n[which];
+    return REVSIM_OK;
+}
+
+int32_t revsim_set_launch_shape(revsim_handle *h, int32_t lanes, int32_t mpc, int32_t unroll) {
+    if (!h) return REVSIM_ERR_BADARG;
+    const int G = lanes ? lanes : h->G, m = mpc ? mpc : h->mpc, U = unroll ? unroll : h->unroll;
+    if ((G != 8 && G != 16 && G != 32) || m < 1 || G * m > 512 || (G * m) % 32 != 0 || (U != 1 && U != 2))
+        return fail(h, REVSIM_ERR_BADARG, "unsupported launch shape");
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->st));
+    h->G = G;
+    h->unroll = U;
+    if (m != h->mpc) {
+        h->mpc = m;
+        int rc = build_block_table(h);
+        if (rc) return rc;
+    }
+    return REVSIM_OK;
+}
+
+int32_t revsim_get_launch_shape(revsim_handle *h, int32_t *lanes, int32_t *mpc, int32_t *unroll) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (lanes) *lanes = h->G;
+    if (mpc) *mpc = h->mpc;
+    if (unroll) *unroll = h->unroll;
+    return REVSIM_OK;
+}
+
+// Project autotuner: times the forward and reverse step kernels (forces-only mode, on
+// the current state) for every allowed (lanes per molecule, molecules per CTA, unroll)
+// and keeps the fastest combined time.
+int32_t revsim_autotune(revsim_handle *h, double dt) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if ((rc = build_nlist_checked(h, h->d_x))) return rc;
+    if ((rc = pack(h, 0, true))) return rc;
+    double best = std::numeric_limits<double>::infinity();
+    int bg = h->G, bm = h->mpc, bu = h->unroll;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int G : {8, 16, 32}) {
+        for (int threads : {64, 128, 256, 512}) {
+            if (threads < G || threads % G) continue;
+            for (int U : {1, 2}) {
+                if ((rc = revsim_set_launch_shape(h, G, threads / G, U))) break;
+                StepArgs a = base_args(h);
+                a.pos_in = h->d_pos[0];
+                a.wgt_in = h->d_wgt[0];
+                a.F_out = h->d_F;
+                a.acoefO = dt * dt / (2 * h->mO);
+                a.acoefH = dt * dt / (2 * h->mH);
+                a.mode = MODE_FORCES_ONLY;
+                for (int it = 0; it < 2 && !rc; it++)
+                    if ((rc = launch_step_k(h, false, a)) == 0) rc = launch_step_k(h, true, a);
+                if (rc) break;
+                CK(cudaEventRecord(e0, h->st));
+                for (int it = 0; it < 8 && !rc; it++)
+                    if ((rc = launch_step_k(h, false, a)) == 0) rc = launch_step_k(h, true, a);
+                if (rc) break;
+                CK(cudaEventRecord(e1, h->st));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    bg = G;
+                    bm = threads / G;
+                    bu = U;
+                }
+            }
+            if (rc) break;
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc2 = revsim_set_launch_shape(h, bg, bm, bu);
+    return rc ? rc : rc2;
+}
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+// rs_internal.h -- host-side interface between the C-ABI layer (rs_api.cu) and the
+// kernel launchers (rs_nlist.cu, rs_step.cu, rs_loss.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rs_device.cuh"
+
+namespace rs {
+
+// Per-launch constants of the non-bonded terms, in pair precision R.
+template <typename R>
+struct NbConsts {
+    R qq[3];      // k_e q_a q_b for (O,O), (O,H), (H,H)
+    R krf;        // reaction-field k_rf
+    R krf2;       // 2 k_rf
+    R rc2;        // cutoff^2
+    R twoinvq;    // 2 / q_O  (dF_c/dq_O = 2 F_c / q_O, water.jl:1247)
+    FormConsts<R> fc;
+};
+
+struct BondConsts {
+    double kb, r0, ka, th0;
+};
+
+// Everything the step kernels read or write.
+struct StepArgs {
+    const int *blk_rep, *blk_mol0, *blk_nmol;
+    const double *rep_box, *rep_sdO, *rep_sdH;
+    const int *rep_atom0;
+    const uint32_t *nbr;
+    const int *nbr_cnt;
+    int cap;
+    double *x, *v, *A, *B, *C, *D, *G;
+    const void *pos_in, *wgt_in;
+    void *pos_out, *wgt_out;
+    double *part;      // [n_blk * P] dtheta partials (accumulated)
+    double *norm2;     // [n_blk] sum of dl_dfi^2 (deferred / clipped mode)
+    int P;
+    int *status;
+    double *F_out;     // forces-only mode
+    double dt, c, s, mO, mH, acoefO, acoefH;
+    const uint64_t *seed_cur, *seed_next;   // [n_replicas]
+    int mode;
+};
+
+enum StepMode {
+    MODE_FORCES_ONLY = 1,   // write F_out (and G / part in reverse), no integration
+    MODE_FUSE_NEXT = 2,     // reverse: also run part 1 of the next reverse step
+    MODE_DEFER_BA = 4,      // reverse: leave B, A for the clip pass, write norm2
+};
+
+struct NlistArgs {
+    int M, n_cells;
+    const double *x;
+    const int *mol_rep, *rep_nc, *rep_cell_off, *cell_rep;
+    const double *rep_box;
+    int *cell_of_mol, *cell_cnt, *cell_start, *cell_fill, *cell_tmp, *cell_sorted;
+    uint32_t *nbr;
+    int *nbr_cnt;
+    int cap;
+    double rc_nl2;     // neighbour-list cutoff^2
+    double rcand2;     // O-O candidate radius^2
+    double rext2;      // max intramolecular O-H distance^2
+    float band;        // |FP32 d^2 - rc_nl^2| at or below which FP64 decides membership
+    int *status;
+    int *max_cnt;      // [1] running maximum of the row counts
+};
+
+struct RdfArgs {
+    const double *x;
+    const int *rep_atom0, *rep_nmol;
+    const double *rep_box;
+    int sel1, sel2;
+    double x_min, step, width, cutoff;
+    int n_grid, off;
+    double *hist;      // [R * n_grid] raw sums, then h
+    const double *dLdh; // [R * n_grid]
+    double *dLdx;      // [3N]
+};
+
+// Launchers (return cudaError_t of the launch).
+cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st);
+cudaError_t launch_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap, int mol0,
+                                int nmol, int32_t *pairs, unsigned long long *count,
+                                long long max_pairs, cudaStream_t st);
+
+// Fused step kernels: lanes per molecule G (8/16/32), entries per iteration unroll (1/2),
+// shift = one periodic image per molecule pair (valid when every box side exceeds
+// 2 (cutoff + 2 * max O-H distance)).
+template <typename R>
+cudaError_t launch_step(bool rev, int form, int G, int unroll, bool shift, int n_blk, int threads,
+                        const StepArgs &a, const NbConsts<R> &nb, const BondConsts &bc,
+                        cudaStream_t st);
+template <typename R, int FORM>
+cudaError_t launch_form(bool rev, int G, int unroll, bool shift, int n_blk, int threads,
+                        const StepArgs &a, const NbConsts<R> &nb, const BondConsts &bc,
+                        cudaStream_t st);
+
+cudaError_t launch_pack(int N, int prec, const double *x, const double *C, double mO, double mH,
+                        const int *atom_rep, const double *rep_box, void *pos, void *wgt,
+                        cudaStream_t st);
+cudaError_t launch_unintegrate(int M, int prec, const StepArgs &a, const int *mol_rep,
+                               cudaStream_t st);
+cudaError_t launch_clip_post(int N, const StepArgs &a, const int *atom_rep, const double *scale,
+                             cudaStream_t st);
+cudaError_t launch_init_adjoint(int N, const double *g, double c, double *A, double *B, double *C,
+                                double *D, double *G, cudaStream_t st);
+cudaError_t launch_noise(int N, const int *atom_rep, const int *rep_atom0, const double *rep_sdO,
+                         const double *rep_sdH, const uint64_t *seeds, double *xi,
+                         cudaStream_t st);
+
+cudaError_t launch_rdf(const RdfArgs &a, int R, int max_n1, int max_n2, bool grad,
+                       cudaStream_t st);
+cudaError_t launch_rdf_finalize(const RdfArgs &a, int R, const double *pre, const double *target,
+                                int slice_start, int slice_stride, int n_target, int norm,
+                                double weight, double *loss, double *dLdh, cudaStream_t st);
+
+}  // namespace rs

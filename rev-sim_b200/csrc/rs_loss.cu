@@ -1,0 +1,198 @@
+// rs_loss.cu -- smoothed-RDF loss and its gradient on the device.
+//
+// rdf_differentiable (water.jl:631-691): every (set1, set2) atom pair at minimum-image
+// distance d != 0 is smeared over the grid x_k = x_min + step*k with
+// g_k(d) = exp(-(x_k - d)^2 / width), restricted to the window |x_k - d| <= cutoff and
+// normalised by den(d) = sum of g_k over the index window [ceil((d-c)/step) - off,
+// floor((d+c)/step) - off] (water.jl:660-667); h_k = V / (4 pi n1 n2 step) * sum / x_k^2.
+// The loss (loss_rdf_part, water.jl:693-697) compares a strided slice of h with a
+// target; the gradient is the analytic derivative of the same windowed sums (the
+// quantity Enzyme differentiates in the reference's pullback, water.jl:715-736).
+// Runs once per loss block, so it is written for clarity: one thread per ordered
+// atom pair, shared-memory histogram, FP64 throughout.
+#include "rs_internal.h"
+
+namespace rs {
+
+namespace {
+
+__device__ __forceinline__ int rdf_atom(int sel, int atom0, int i) {
+    return sel == 0 ? atom0 + 3 * i : atom0 + 3 * (i >> 1) + 1 + (i & 1);
+}
+
+__device__ __forceinline__ double grid_x(const RdfArgs &a, int k) {
+    return __dadd_rn(a.x_min, __dmul_rn(a.step, (double)k));
+}
+
+// Normaliser window, 0-based inclusive.
+__device__ __forceinline__ void den_window(const RdfArgs &a, double d, int &lo, int &hi) {
+    long long s = (long long)ceil(__ddiv_rn(__dsub_rn(d, a.cutoff), a.step)) - a.off;
+    long long e = (long long)floor(__ddiv_rn(__dadd_rn(d, a.cutoff), a.step)) - a.off;
+    if (s < 1) s = 1;
+    if (e > a.n_grid) e = a.n_grid;
+    lo = (int)(s - 1);
+    hi = (int)(e - 1);
+}
+
+// Histogram window: grid points with x - c <= d <= x + c.
+__device__ __forceinline__ void hist_window(const RdfArgs &a, double d, int &lo, int &hi) {
+    long long s = (long long)floor(__ddiv_rn(__dsub_rn(__dsub_rn(d, a.cutoff), a.x_min), a.step)) - 1;
+    long long e = (long long)ceil(__ddiv_rn(__dsub_rn(__dadd_rn(d, a.cutoff), a.x_min), a.step)) + 1;
+    if (s < 0) s = 0;
+    if (e > a.n_grid - 1) e = a.n_grid - 1;
+    int l = (int)s, h = (int)e;
+    while (l <= h && !(d <= __dadd_rn(grid_x(a, l), a.cutoff))) l++;
+    while (h >= l && !(d >= __dsub_rn(grid_x(a, h), a.cutoff))) h--;
+    lo = l;
+    hi = h;
+}
+
+__device__ __forceinline__ void den_sums(const RdfArgs &a, double d, double &den, double &dden) {
+    int lo, hi;
+    den_window(a, d, lo, hi);
+    double s = 0.0, ds = 0.0;
+    for (int k = lo; k <= hi; k++) {
+        const double e = __dsub_rn(grid_x(a, k), d);
+        const double g = exp(__ddiv_rn(-__dmul_rn(e, e), a.width));
+        s = __dadd_rn(s, g);
+        ds = __dadd_rn(ds, __ddiv_rn(__dmul_rn(__dmul_rn(g, 2.0), e), a.width));
+    }
+    den = s;
+    dden = ds;
+}
+
+template <bool GRAD>
+__global__ void k_rdf(RdfArgs a, const double *pre) {
+    extern __shared__ double s_hist[];
+    const int r = blockIdx.y;
+    const int nm = a.rep_nmol[r];
+    const int atom0 = a.rep_atom0[r];
+    const long long n1 = a.sel1 == 0 ? nm : 2LL * nm;
+    const long long n2 = a.sel2 == 0 ? nm : 2LL * nm;
+    const double L = a.rep_box[r];
+    const bool use_smem = !GRAD && a.n_grid <= 6144;
+    double *hist = a.hist + (size_t)r * a.n_grid;
+    if (use_smem) {
+        for (int k = threadIdx.x; k < a.n_grid; k += blockDim.x) s_hist[k] = 0.0;
+        __syncthreads();
+    }
+    const double dmin = __dsub_rn(__dsub_rn(a.x_min, a.cutoff), a.step);
+    const double dmax = __dadd_rn(__dadd_rn(grid_x(a, a.n_grid - 1), a.cutoff), a.step);
+    const long long total = n1 * n2;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(p / n2), i2 = (int)(p % n2);
+        const int ia = rdf_atom(a.sel1, atom0, i1), ib = rdf_atom(a.sel2, atom0, i2);
+        const double *xa = a.x + 3 * (size_t)ia, *xb = a.x + 3 * (size_t)ib;
+        double dr[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) dr[u] = vec1d(xa[u], xb[u], L);
+        const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dr[0], dr[0]), __dmul_rn(dr[1], dr[1])),
+                                              __dmul_rn(dr[2], dr[2])));
+        if (d == 0.0 || d < dmin || d > dmax) continue;
+        int lo, hi;
+        hist_window(a, d, lo, hi);
+        if (lo > hi) continue;
+        double den, dden;
+        den_sums(a, d, den, dden);
+        if (!GRAD) {
+            for (int k = lo; k <= hi; k++) {
+                const double e = __dsub_rn(grid_x(a, k), d);
+                const double g = __ddiv_rn(exp(__ddiv_rn(-__dmul_rn(e, e), a.width)), den);
+                if (use_smem)
+                    atomicAdd(s_hist + k, g);
+                else
+                    atomicAdd(hist + k, g);
+            }
+        } else {
+            const double *dLdh = a.dLdh + (size_t)r * a.n_grid;
+            double dLdd = 0.0;
+            for (int k = lo; k <= hi; k++) {
+                const double w = dLdh[k];
+                if (w == 0.0) continue;
+                const double xk = grid_x(a, k), e = __dsub_rn(xk, d);
+                const double g = exp(__ddiv_rn(-__dmul_rn(e, e), a.width));
+                const double gp = __ddiv_rn(__dmul_rn(__dmul_rn(g, 2.0), e), a.width);
+                const double t = __dsub_rn(__ddiv_rn(gp, den), __ddiv_rn(__dmul_rn(g, dden), __dmul_rn(den, den)));
+                dLdd = __dadd_rn(dLdd, __dmul_rn(__ddiv_rn(__dmul_rn(w, pre[r]), __dmul_rn(xk, xk)), t));
+            }
+            if (dLdd != 0.0) {
+#pragma unroll
+                for (int u = 0; u < 3; u++) {
+                    const double gu = __ddiv_rn(__dmul_rn(dLdd, dr[u]), d);
+                    atomicAdd(a.dLdx + 3 * (size_t)ib + u, gu);
+                    atomicAdd(a.dLdx + 3 * (size_t)ia + u, -gu);
+                }
+            }
+        }
+    }
+    if (use_smem) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < a.n_grid; k += blockDim.x)
+            if (s_hist[k] != 0.0) atomicAdd(hist + k, s_hist[k]);
+    }
+}
+
+// h_k = pre * sum_k / x_k^2; loss += weight * sum |h - target|^norm over the slice;
+// dL/dh at the slice points.  One CTA per replica.
+__global__ void k_rdf_finalize(RdfArgs a, const double *pre, const double *target, int s0, int sd,
+                               int nt, int norm, double weight, double *loss, double *dLdh) {
+    const int r = blockIdx.x;
+    double *h = a.hist + (size_t)r * a.n_grid;
+    double *gh = dLdh + (size_t)r * a.n_grid;
+    for (int k = threadIdx.x; k < a.n_grid; k += blockDim.x) {
+        const double xk = grid_x(a, k);
+        h[k] = __ddiv_rn(__dmul_rn(pre[r], h[k]), __dmul_rn(xk, xk));
+        gh[k] = 0.0;
+    }
+    __syncthreads();
+    __shared__ double s_l[256];
+    double l = 0.0;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        const int k = s0 + t * sd;
+        const double e = __dsub_rn(h[k], target[(size_t)r * nt + t]);
+        if (norm == 1) {
+            l = __dadd_rn(l, fabs(e));
+            gh[k] = weight * (e > 0.0 ? 1.0 : (e < 0.0 ? -1.0 : 0.0));
+        } else {
+            l = __dadd_rn(l, __dmul_rn(e, e));
+            gh[k] = __dmul_rn(weight, __dmul_rn(2.0, e));
+        }
+    }
+    s_l[threadIdx.x] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int t = 0; t < blockDim.x; t++) s = __dadd_rn(s, s_l[t]);
+        loss[r] = __dadd_rn(loss[r], __dmul_rn(weight, s));
+    }
+}
+
+}  // namespace
+
+// pre [R] is stashed by the caller at a.hist + R*n_grid (scratch behind the histogram).
+cudaError_t launch_rdf(const RdfArgs &a, int R, int max_n1, int max_n2, bool grad,
+                       cudaStream_t st) {
+    const long long pairs = (long long)max_n1 * max_n2;
+    long long blocks = (pairs + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    const double *pre = a.hist + (size_t)R * a.n_grid;
+    if (grad) {
+        k_rdf<true><<<dim3((unsigned)blocks, R), 256, 0, st>>>(a, pre);
+    } else {
+        const size_t smem = a.n_grid <= 6144 ? sizeof(double) * a.n_grid : 0;
+        k_rdf<false><<<dim3((unsigned)blocks, R), 256, smem, st>>>(a, pre);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rdf_finalize(const RdfArgs &a, int R, const double *pre, const double *target,
+                                int slice_start, int slice_stride, int n_target, int norm,
+                                double weight, double *loss, double *dLdh, cudaStream_t st) {
+    k_rdf_finalize<<<R, 256, 0, st>>>(a, pre, target, slice_start, slice_stride, n_target, norm,
+                                      weight, loss, dLdh);
+    return cudaGetLastError();
+}
+
+}  // namespace rs

@@ -1,0 +1,280 @@
+// rs_nlist.cu -- cell-list neighbour build for water (replaces Molly's
+// CellListMapNeighborFinder, configured at water.jl:980-991 and rebuilt every
+// n_steps_nf steps at water.jl:1025,1038,1504).
+//
+// The reference keeps an atom-pair list: pairs i<j of different molecules whose
+// minimum-image distance is <= 1.2 nm (eligible matrix of diffusion.jl:1133-1147).
+// Here the same pair set is stored blocked by molecule: row I lists every molecule
+// J != I with at least one listed atom pair, as a 32-bit entry J | mask << 23 whose
+// 9-bit mask marks which of the 3x3 atom pairs (own atom a, neighbour atom b; bit
+// 3a+b) are in the reference's set.  Rows hold both directions, so each step kernel
+// gathers a whole molecule (3 positions) per entry and accumulates the forces of its
+// own molecule with no atomics.  Membership distances are FP64, each product and sum
+// rounded separately, exactly as the CPU restatement computes them.
+#include "rs_internal.h"
+
+namespace rs {
+
+namespace {
+
+__device__ __forceinline__ double dist2_fp64(const double *xa, const double *xb, double L) {
+    const double dx = vec1d(xa[0], xb[0], L);
+    const double dy = vec1d(xa[1], xb[1], L);
+    const double dz = vec1d(xa[2], xb[2], L);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Cell of each molecule (by its O atom) and the per-cell counts.
+__global__ void k_cell_count(NlistArgs a) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= a.M) return;
+    const int r = a.mol_rep[I];
+    const int nc = a.rep_nc[r];
+    const double L = a.rep_box[r];
+    const double *xo = a.x + 9 * (size_t)I;
+    int ci[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        int c = (int)floor(xo[u] / L * nc);
+        ci[u] = c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+    }
+    const int cell = a.rep_cell_off[r] + (ci[2] * nc + ci[1]) * nc + ci[0];
+    a.cell_of_mol[I] = cell;
+    atomicAdd(a.cell_cnt + cell, 1);
+    // Molecules are matched by O-O distance with a margin of two O-H lengths.
+    if (dist2_fp64(xo, xo + 3, L) > a.rext2 || dist2_fp64(xo, xo + 6, L) > a.rext2)
+        atomicOr(a.status, ST_GEOMETRY);
+}
+
+// Exclusive scan of the cell counts (one CTA; cells are few).
+__global__ void k_cell_scan(NlistArgs a) {
+    __shared__ int s_part[1024];
+    __shared__ int s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < a.n_cells; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < a.n_cells ? a.cell_cnt[i] : 0;
+        s_part[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < blockDim.x; off <<= 1) {
+            const int t = threadIdx.x >= off ? s_part[threadIdx.x - off] : 0;
+            __syncthreads();
+            s_part[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < a.n_cells) {
+            a.cell_start[i] = s_carry + s_part[threadIdx.x] - v;
+            a.cell_fill[i] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry += s_part[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void k_cell_fill(NlistArgs a) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= a.M) return;
+    const int c = a.cell_of_mol[I];
+    a.cell_tmp[a.cell_start[c] + atomicAdd(a.cell_fill + c, 1)] = I;
+}
+
+// Order each cell by molecule index, so that the rows are a deterministic
+// function of the positions (the forward and reverse passes rebuild identical lists).
+__global__ void k_cell_sort(NlistArgs a) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= a.M) return;
+    const int c = a.cell_of_mol[I];
+    const int s = a.cell_start[c], n = a.cell_cnt[c];
+    int rank = 0;
+    for (int t = 0; t < n; t++) rank += a.cell_tmp[s + t] < I;
+    a.cell_sorted[s + rank] = I;
+}
+
+// Rows of every molecule of one home cell (one CTA per cell).  The CTA stages the
+// neighbourhood -- the members of the surrounding cells, in the canonical cell order
+// and index order within a cell -- with all three atoms in FP32 in shared memory, in
+// chunks of up to kRowChunk molecules.  Each warp takes one home molecule at a time:
+// an FP32 O-O test against the candidate radius (with a margin far above FP32 error)
+// selects candidate molecules, an FP32 test classifies each of the nine atom pairs as
+// clearly inside / clearly outside the list cutoff, and the few pairs within `band` of
+// the cutoff are decided by the exact FP64 Molly arithmetic (dist2_fp64), so the set
+// is bit-identical to the all-FP64 test.  Entries are appended in candidate order.
+constexpr int kRowChunk = 2048;
+
+__device__ __forceinline__ float mi_f(float d, float L, float hL) {
+    return d > hL ? d - L : (d < -hL ? d + L : d);
+}
+
+__global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
+    extern __shared__ float s_c[];              // [9][kRowChunk] coordinates
+    int *s_idx = (int *)(s_c + 9 * kRowChunk);   // [kRowChunk] molecule ids
+    __shared__ int s_cell[125], s_off[126];
+    const int c_home = blockIdx.x;
+    const int r = a.cell_rep[c_home];
+    const int nc = a.rep_nc[r];
+    const int off0 = a.rep_cell_off[r];
+    const double Ld = a.rep_box[r];
+    const float L = (float)Ld, hL = 0.5f * (float)Ld;
+    const int hs = a.cell_start[c_home], hn = a.cell_cnt[c_home];
+    if (hn == 0) return;
+    const int cl = c_home - off0;
+    const int cx = cl % nc, cy = (cl / nc) % nc, cz = cl / (nc * nc);
+    const int span = nc >= 5 ? 5 : nc;
+    const int ncell = span * span * span;
+    // neighbourhood cells in canonical order and their member counts
+    if (threadIdx.x < ncell) {
+        const int t = threadIdx.x;
+        const int dz = t / (span * span), dy = (t / span) % span, dx = t % span;
+        const int z = nc >= 5 ? (cz + dz - 2 + nc) % nc : dz;
+        const int y = nc >= 5 ? (cy + dy - 2 + nc) % nc : dy;
+        const int x = nc >= 5 ? (cx + dx - 2 + nc) % nc : dx;
+        s_cell[t] = off0 + (z * nc + y) * nc + x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int t = 0; t < ncell; t++) {
+            s_off[t] = acc;
+            acc += a.cell_cnt[s_cell[t]];
+        }
+        s_off[ncell] = acc;
+    }
+    __syncthreads();
+    const int total = s_off[ncell];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const float rcand2 = (float)a.rcand2 + 1e-3f;
+    const float rc2f = (float)a.rc_nl2;
+    const float band = a.band;
+    // per home molecule state kept across chunks (a warp owns the same molecules in
+    // every chunk: home members warp, warp + nwarp, ...)
+    constexpr int kMaxHome = 8;   // home molecules per warp per pass
+    for (int h0 = 0; h0 < hn; h0 += nwarp * kMaxHome) {
+        int cnt[kMaxHome];
+#pragma unroll
+        for (int q = 0; q < kMaxHome; q++) cnt[q] = 0;
+        for (int c0 = 0; c0 < total; c0 += kRowChunk) {
+            const int cn = min(kRowChunk, total - c0);
+            __syncthreads();
+            int t = 0;   // cell of candidate g (g grows with k, so t only moves forward)
+            for (int k = threadIdx.x; k < cn; k += blockDim.x) {
+                const int g = c0 + k;
+                while (s_off[t + 1] <= g) t++;
+                const int J = a.cell_sorted[a.cell_start[s_cell[t]] + (g - s_off[t])];
+                s_idx[k] = J;
+                const double *xj = a.x + 9 * (size_t)J;
+#pragma unroll
+                for (int u = 0; u < 9; u++) s_c[u * kRowChunk + k] = (float)xj[u];
+            }
+            __syncthreads();
+#pragma unroll 1
+            for (int q = 0; q < kMaxHome; q++) {
+                const int hi = h0 + q * nwarp + warp;
+                if (hi >= hn) break;
+                const int I = a.cell_sorted[hs + hi];
+                float xi[9];
+#pragma unroll
+                for (int u = 0; u < 9; u++) xi[u] = (float)a.x[9 * (size_t)I + u];
+                uint32_t *row = a.nbr + (size_t)I * a.cap;
+                for (int base = 0; base < cn; base += 32) {
+                    const int k = base + lane;
+                    uint32_t ent = 0;
+                    if (k < cn) {
+                        const int J = s_idx[k];
+                        const float ox = mi_f(s_c[k] - xi[0], L, hL);
+                        const float oy = mi_f(s_c[kRowChunk + k] - xi[1], L, hL);
+                        const float oz = mi_f(s_c[2 * kRowChunk + k] - xi[2], L, hL);
+                        if (J != I && ox * ox + oy * oy + oz * oz <= rcand2) {
+                            uint32_t mask = 0;
+#pragma unroll
+                            for (int ka = 0; ka < 3; ka++)
+#pragma unroll
+                                for (int kb = 0; kb < 3; kb++) {
+                                    const float dx = mi_f(s_c[(3 * kb) * kRowChunk + k] - xi[3 * ka], L, hL);
+                                    const float dy = mi_f(s_c[(3 * kb + 1) * kRowChunk + k] - xi[3 * ka + 1], L, hL);
+                                    const float dz = mi_f(s_c[(3 * kb + 2) * kRowChunk + k] - xi[3 * ka + 2], L, hL);
+                                    const float d2 = dx * dx + dy * dy + dz * dz;
+                                    bool in = d2 < rc2f;
+                                    if (fabsf(d2 - rc2f) <= band)
+                                        in = dist2_fp64(a.x + 9 * (size_t)I + 3 * ka,
+                                                        a.x + 9 * (size_t)J + 3 * kb, Ld) <= a.rc_nl2;
+                                    if (in) mask |= 1u << (3 * ka + kb);
+                                }
+                            if (mask) ent = (uint32_t)J | (mask << 23);
+                        }
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, ent != 0);
+                    if (ent) {
+                        const int pos = cnt[q] + __popc(bal & ((1u << lane) - 1u));
+                        if (pos < a.cap) row[pos] = ent;
+                    }
+                    cnt[q] += __popc(bal);
+                }
+            }
+        }
+#pragma unroll 1
+        for (int q = 0; q < kMaxHome; q++) {
+            const int hi = h0 + q * nwarp + warp;
+            if (hi >= hn) break;
+            if (lane == 0) {
+                const int I = a.cell_sorted[hs + hi];
+                a.nbr_cnt[I] = cnt[q];
+                if (cnt[q] > a.cap) atomicOr(a.status, ST_NLIST_OVERFLOW);
+                atomicMax(a.max_cnt, cnt[q]);
+            }
+        }
+    }
+}
+
+// Atom pairs (i < j, replica-local indices) of one replica's rows.
+__global__ void k_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap, int mol0,
+                               int nmol, int32_t *pairs, unsigned long long *count,
+                               long long max_pairs) {
+    const int I = blockIdx.y * gridDim.x + blockIdx.x;
+    if (I >= nmol) return;
+    const int Ig = mol0 + I;
+    const int n = min(nbr_cnt[Ig], cap);
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const uint32_t ent = nbr[(size_t)Ig * cap + e];
+        const int J = (int)(ent & 0x7FFFFFu) - mol0;
+        if (J <= I) continue;
+        const uint32_t mask = ent >> 23;
+        for (int b = 0; b < 9; b++) {
+            if (!((mask >> b) & 1u)) continue;
+            const unsigned long long k = atomicAdd(count, 1ull);
+            if ((long long)k < max_pairs) {
+                pairs[2 * k] = 3 * I + b / 3;
+                pairs[2 * k + 1] = 3 * J + b % 3;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
+    cudaMemsetAsync(a.cell_cnt, 0, sizeof(int) * a.n_cells, st);
+    const int t = 256, b = (a.M + t - 1) / t;
+    k_cell_count<<<b, t, 0, st>>>(a);
+    k_cell_scan<<<1, 1024, 0, st>>>(a);
+    k_cell_fill<<<b, t, 0, st>>>(a);
+    k_cell_sort<<<b, t, 0, st>>>(a);
+    const size_t smem = (9 * sizeof(float) + sizeof(int)) * kRowChunk;
+    cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rows<<<a.n_cells, 256, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap, int mol0,
+                                int nmol, int32_t *pairs, unsigned long long *count,
+                                long long max_pairs, cudaStream_t st) {
+    if (nmol <= 0) return cudaSuccess;
+    const int gx = nmol < 65535 ? nmol : 65535;
+    const int gy = (nmol + gx - 1) / gx;
+    k_export_pairs<<<dim3(gx, gy), 128, 0, st>>>(nbr, nbr_cnt, cap, mol0, nmol, pairs, count,
+                                                 max_pairs);
+    return cudaGetLastError();
+}
+
+}  // namespace rs

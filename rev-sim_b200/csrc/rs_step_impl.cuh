@@ -1,0 +1,615 @@
+// rs_step_impl.cuh -- fused forward and reverse step kernels for flexible 3-site water
+// (included by the per-precision, per-pair-form instantiation files rs_step_*.cu).
+//
+// Forward step (water.jl:1030-1037): calc_F! (non-bonded water.jl:892-913, bonds
+// 915-934, angles 936-968) followed by the B-A-O-A update and the wrap.
+// Reverse step (water.jl:1505-1521 and, fused, 1496-1502 of the next step):
+// calc_F_and_grads! (water.jl:1212-1433) with the force VJP against
+// dl_dfi_prev = accum_C, the contraction of dF/dtheta with A dt^2 / (2m)
+// (water.jl:1517-1519, never materialised as a 3N x P matrix), the velocity
+// un-kick, the B/A adjoint updates and the un-integration of the next step.
+//
+// Work decomposition: a group of G lanes owns one molecule; the lanes stride over
+// the molecule's neighbour row (entries of 3 atoms each), accumulate the forces of
+// the 3 own atoms in registers, and reduce them with a fixed xor butterfly.  Lanes
+// 0..2 then finish one atom each (bonded terms in FP64, integrator in FP64).  Every
+// atom's force is computed by exactly one group in a fixed order, so there are no
+// atomics and the forward and reverse kernels produce bit-identical forces.
+#pragma once
+
+#include "rs_internal.h"
+
+namespace rs {
+
+namespace {
+
+template <typename R>
+__device__ __forceinline__ DualN<R, 1> d1(R v, R t) {
+    DualN<R, 1> r;
+    r.v = v;
+    r.d[0] = t;
+    return r;
+}
+template <typename R>
+__device__ __forceinline__ DualN<R, 1> d1_sqrt(const DualN<R, 1> &a) {
+    const R s = xsqrt(a.v);
+    return d1(s, xdiv(a.d[0], xadd(s, s)));
+}
+__device__ __forceinline__ float r_acos(float c) { return acosf(c); }
+__device__ __forceinline__ double r_acos(double c) { return acos(c); }
+template <typename R>
+__device__ __forceinline__ DualN<R, 1> d1_acos(const DualN<R, 1> &a) {
+    return d1(r_acos(a.v), -xdiv(a.d[0], xsqrt(xsub(R(1), xmul(a.v, a.v)))));
+}
+
+// Harmonic angle H1-O-H2 (O central) of water.jl:936-968 / 1316-1356 on dual numbers:
+// value = the reference's force construction (p1 = a x (a x b) / |.|, p3 = -b x (a x b) / |.|,
+// F = k_a (theta0 - theta)), tangent along (w_H1 - w_O, w_H2 - w_O) = J w, which equals
+// the reference's J^T w because the Hessian is symmetric.  Returns false when a x b = 0.
+template <typename R>
+__device__ __forceinline__ bool angle_term(const R a_[3], const R b_[3], const R ta[3],
+                                           const R tb[3], R ka, R th0, DualN<R, 1> Fi[3],
+                                           DualN<R, 1> Fk[3], R p1d[3], R p3d[3], R &disp) {
+    using D = DualN<R, 1>;
+    D a[3], b[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        a[u] = d1(a_[u], ta[u]);
+        b[u] = d1(b_[u], tb[u]);
+    }
+    const D ra = d1_sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    const D rb = d1_sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    D cr[3], p1[3], p3[3];
+    cr[0] = a[1] * b[2] - a[2] * b[1];
+    cr[1] = a[2] * b[0] - a[0] * b[2];
+    cr[2] = a[0] * b[1] - a[1] * b[0];
+    if (cr[0].v == R(0) && cr[1].v == R(0) && cr[2].v == R(0)) return false;
+    p1[0] = a[1] * cr[2] - a[2] * cr[1];
+    p1[1] = a[2] * cr[0] - a[0] * cr[2];
+    p1[2] = a[0] * cr[1] - a[1] * cr[0];
+    const D zero = d1(R(0), R(0));
+    p3[0] = zero - (b[1] * cr[2] - b[2] * cr[1]);
+    p3[1] = zero - (b[2] * cr[0] - b[0] * cr[2]);
+    p3[2] = zero - (b[0] * cr[1] - b[1] * cr[0]);
+    const D n1 = d1_sqrt(p1[0] * p1[0] + p1[1] * p1[1] + p1[2] * p1[2]);
+    const D n3 = d1_sqrt(p3[0] * p3[0] + p3[1] * p3[1] + p3[2] * p3[2]);
+    const D cth = (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]) / (ra * rb);
+    const D th = d1_acos(cth);
+    const D F = d1(ka, R(0)) * (d1(th0, R(0)) - th);
+    const D s1 = n1 * ra, s3 = n3 * rb;
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const D q1 = p1[u] / s1;
+        const D q3 = p3[u] / s3;
+        Fi[u] = F * q1;
+        Fk[u] = F * q3;
+        p1d[u] = q1.v;
+        p3d[u] = q3.v;
+    }
+    disp = xsub(th0, th.v);
+    return true;
+}
+
+// Bonded terms of one molecule in pair precision R: forces Fb on (O, H1, H2); in
+// reverse also the VJP Gb against w = C/m and the bonded dtheta contraction with
+// acoef.  Intramolecular vectors and bond lengths come from the FP64 state (the
+// displacement r - r0 is formed in FP64, so FP32 mode does not lose it to cancellation).
+template <typename R, bool REV>
+__device__ __forceinline__ void bonded(const double xm[9], double L, const BondConsts &bc,
+                                       const R w[9], const R ac[9], R Fb[9], R Gb[9], R tb[4]) {
+#pragma unroll
+    for (int u = 0; u < 9; u++) {
+        Fb[u] = R(0);
+        Gb[u] = R(0);
+    }
+    tb[0] = tb[1] = tb[2] = tb[3] = R(0);
+    const R kb = (R)bc.kb;
+    R av[2][3];
+    // Bonds (O, H1), (O, H2): radial pair with F(r) = -k_b (r - r0), F' = -k_b.
+#pragma unroll
+    for (int h = 1; h <= 2; h++) {
+        double dd[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) dd[u] = vec1d(xm[u], xm[3 * h + u], L);
+        const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dd[0], dd[0]), __dmul_rn(dd[1], dd[1])),
+                                     __dmul_rn(dd[2], dd[2]));
+        const double rd = __dsqrt_rn(r2d);
+        const R disp = (R)__dsub_rn(rd, bc.r0);
+        R dr[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            dr[u] = (R)dd[u];
+            av[h - 1][u] = dr[u];
+        }
+        const R rinv = xrsqrt((R)r2d);
+        const R F = -xmul(kb, disp);
+        const R Fr = xmul(F, rinv);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const R f = xmul(Fr, dr[u]);
+            Fb[u] = xsub(Fb[u], f);
+            Fb[3 * h + u] = xadd(Fb[3 * h + u], f);
+        }
+        if (REV) {
+            // M delta with delta = w_H - w_O: -(F' - F/r) s n - (F/r) delta, s = n . delta
+            R dl[3];
+#pragma unroll
+            for (int u = 0; u < 3; u++) dl[u] = xsub(w[3 * h + u], w[u]);
+            const R s = xmul(rinv, xfma(dr[2], dl[2], xfma(dr[1], dl[1], xmul(dr[0], dl[0]))));
+            const R k1 = xmul(xmul(xsub(-kb, Fr), s), rinv);
+            R t = R(0);
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                const R m = -xfma(k1, dr[u], xmul(Fr, dl[u]));
+                Gb[u] = xadd(Gb[u], m);
+                Gb[3 * h + u] = xsub(Gb[3 * h + u], m);
+                t = xfma(xsub(ac[u], ac[3 * h + u]), dr[u], t);
+            }
+            t = xmul(t, rinv);
+            // dF_O/dk_b = disp n, dF_O/dr0 = -k_b n (water.jl:1298-1301)
+            tb[0] = xfma(disp, t, tb[0]);
+            tb[1] = xfma(-kb, t, tb[1]);
+        }
+    }
+    // Angle H1-O-H2.
+    R ta[3], tb3[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        ta[u] = REV ? xsub(w[3 + u], w[u]) : R(0);
+        tb3[u] = REV ? xsub(w[6 + u], w[u]) : R(0);
+    }
+    DualN<R, 1> Fi[3], Fk[3];
+    R p1d[3], p3d[3], disp;
+    if (angle_term<R>(av[0], av[1], ta, tb3, (R)bc.ka, (R)bc.th0, Fi, Fk, p1d, p3d, disp)) {
+        R t = R(0);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            Fb[3 + u] = xadd(Fb[3 + u], Fi[u].v);
+            Fb[6 + u] = xadd(Fb[6 + u], Fk[u].v);
+            Fb[u] = xsub(Fb[u], xadd(Fi[u].v, Fk[u].v));
+            if (REV) {
+                Gb[3 + u] = xadd(Gb[3 + u], Fi[u].d[0]);
+                Gb[6 + u] = xadd(Gb[6 + u], Fk[u].d[0]);
+                Gb[u] = xsub(Gb[u], xadd(Fi[u].d[0], Fk[u].d[0]));
+                t = xadd(t, xsub(xfma(ac[3 + u], p1d[u], xmul(ac[6 + u], p3d[u])),
+                                 xmul(ac[u], xadd(p1d[u], p3d[u]))));
+            }
+        }
+        if (REV) {
+            tb[2] = xmul(disp, t);           // dF/dk_a
+            tb[3] = xmul((R)bc.ka, t);       // dF/dtheta0
+        }
+    }
+}
+
+template <int G>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T pick3(int k, T a, T b, T c) {
+    return k == 0 ? a : (k == 1 ? b : c);
+}
+
+__device__ __forceinline__ float r_rint(float v) { return rintf(v); }
+__device__ __forceinline__ double r_rint(double v) { return rint(v); }
+
+// Minimum-image component for the step kernels: d - L rint(d / L).  For every pair
+// within the cutoff (|d| < L/2 - margin) it returns the same bits as Molly's rule
+// (vec1d), one rounding of (c2 - c1) -/+ L; it differs only for pairs near L/2,
+// which are far outside the cutoff.  Branch-free, unlike vec1d.
+template <typename R>
+__device__ __forceinline__ R vec_mi(R c1, R c2, R L, R invL) {
+    const R d = xsub(c2, c1);
+    return xfma(-r_rint(xmul(d, invL)), L, d);
+}
+
+// One (own atom KA, neighbour atom KB) interaction with displacement (dx, dy, dz),
+// evaluated unconditionally: pairs outside the neighbour mask or the cutoff
+// contribute exact zeros, so the nine slots of an entry run as straight-line code with
+// no divergence between the lanes of a warp (each lane holds a different neighbour).
+template <typename R, int FORM, bool REV, int KA, int KB>
+__device__ __forceinline__ void pair_term(bool bit, R dx, R dy, R dz,
+                                          const typename V4T<R>::T &wa,
+                                          const typename V4T<R>::T &wb, const R ca[3],
+                                          const NbConsts<R> &nb, R f[3], R g[3], R *th) {
+    constexpr int NF = FormInfo<FORM>::NP;
+    const R r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
+    const bool on = bit && r2 <= nb.rc2;
+    const R z = on ? R(1) : R(0);
+    const R r2s = on ? r2 : R(1);
+    const R rinv = xrsqrt(r2s);
+    const R r = xmul(r2s, rinv);
+    const R invr2 = xmul(rinv, rinv);
+    constexpr int QI = (KA > 0) + (KB > 0);
+    const R qq = nb.qq[QI];
+    const R Fc = xmul(qq, xsub(invr2, xmul(nb.krf2, r)));
+    R F = Fc;
+    R dF = R(0);
+    R gf[4];
+    if (REV) dF = -xmul(xadd(qq, qq), xadd(xmul(invr2, rinv), nb.krf));
+    if (KA == 0 && KB == 0) {
+        if (nb.fc.on) {
+            R Ff, dFf = R(0);
+            pair_form<R, FORM, REV>(nb.fc, r, rinv, invr2, Ff, dFf, gf);
+            F = xadd(F, Ff);
+            if (REV) dF = xadd(dF, dFf);
+        }
+    }
+    const R Fr = xmul(xmul(F, rinv), z);
+    // force on the own atom: -F n = -(F/r) dr
+    f[0] = xfma(-Fr, dx, f[0]);
+    f[1] = xfma(-Fr, dy, f[1]);
+    f[2] = xfma(-Fr, dz, f[2]);
+    if (REV) {
+        // VJP: M delta, delta = w_b - w_a, M = -[F' n n + (F/r)(I - n n)]
+        const R ex = xsub(wb.x, wa.x), ey = xsub(wb.y, wa.y), ez = xsub(wb.z, wa.z);
+        const R s = xmul(rinv, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
+        const R k1 = xmul(xmul(xsub(xmul(dF, z), Fr), s), rinv);
+        g[0] = xsub(g[0], xfma(k1, dx, xmul(Fr, ex)));
+        g[1] = xsub(g[1], xfma(k1, dy, xmul(Fr, ey)));
+        g[2] = xsub(g[2], xfma(k1, dz, xmul(Fr, ez)));
+        // dtheta: acoef_a . dF_a/dtheta_p = -(dF/dtheta_p) (n . acoef_a)
+        const R na = xmul(xmul(rinv, xfma(dz, ca[2], xfma(dy, ca[1], xmul(dx, ca[0])))), z);
+        th[NF] = xfma(-xmul(Fc, nb.twoinvq), na, th[NF]);
+        if (KA == 0 && KB == 0) {
+            if (nb.fc.on) {
+#pragma unroll
+                for (int p = 0; p < NF; p++) th[p] = xfma(-gf[p], na, th[p]);
+            }
+        }
+    }
+}
+
+// Displacement of one slot.  SHIFT: one periodic image per molecule pair (chosen from
+// the O-O vector) is applied to all nine atom pairs; d + s rounds exactly as Molly's
+// (c2 - c1) -/+ L, and the image is the minimum one for every pair within the cutoff
+// whenever L > 2 (cutoff + 2 * max O-H distance).  Otherwise per-slot vec_mi.
+template <typename R, bool SHIFT>
+__device__ __forceinline__ R slot_d(R ca_, R cb_, R s, R L, R invL) {
+    if (SHIFT) return xadd(xsub(cb_, ca_), s);
+    return vec_mi(ca_, cb_, L, invL);
+}
+
+template <typename R, bool SHIFT>
+__device__ __forceinline__ R image_shift(R d, R L, R hL) {
+    return d > hL ? -L : (d < -hL ? L : R(0));
+}
+
+template <typename R, int FORM, bool REV, bool SHIFT, int KA>
+__device__ __forceinline__ void pair_row(uint32_t mask, const typename V4T<R>::T &pa,
+                                         const typename V4T<R>::T pb[3],
+                                         const typename V4T<R>::T &wa,
+                                         const typename V4T<R>::T wb[3], const R ca[3],
+                                         const R sh[3], R L, R invL, const NbConsts<R> &nb,
+                                         R f[3], R g[3], R *th) {
+#define RS_SLOT(KB)                                                                             \
+    pair_term<R, FORM, REV, KA, KB>((mask >> (3 * KA + KB)) & 1u,                               \
+                                    slot_d<R, SHIFT>(pa.x, pb[KB].x, sh[0], L, invL),           \
+                                    slot_d<R, SHIFT>(pa.y, pb[KB].y, sh[1], L, invL),           \
+                                    slot_d<R, SHIFT>(pa.z, pb[KB].z, sh[2], L, invL), wa, wb[KB], \
+                                    ca, nb, f, g, th)
+    RS_SLOT(0);
+    RS_SLOT(1);
+    RS_SLOT(2);
+#undef RS_SLOT
+}
+
+template <typename R, int FORM, int G, bool REV, bool SHIFT, int U>
+__global__ void __launch_bounds__(512) k_water_step(StepArgs a, NbConsts<R> nb, BondConsts bc) {
+    using V4 = typename V4T<R>::T;
+    constexpr int NF = FormInfo<FORM>::NP;
+    constexpr int NTH = NF + 1;
+    // dynamic shared memory: [groups][P] dtheta (double), [groups] |dl_dfi|^2 (double),
+    // then [groups][22] bonded results (R): forces (9), VJP (9), dtheta (4)
+    extern __shared__ double s_th[];
+
+    const int grp = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    const int ngrp = blockDim.x / G;
+    const int blk = blockIdx.x;
+    const int rep = a.blk_rep[blk];
+    const int I = a.blk_mol0[blk] + grp;
+    const bool active = grp < a.blk_nmol[blk];
+    const double Ld = a.rep_box[rep];
+    const R L = (R)Ld;
+    const R invL = (R)(1.0 / Ld);
+    const V4 *__restrict__ pos = (const V4 *)a.pos_in;
+    const V4 *__restrict__ wgt = (const V4 *)a.wgt_in;
+
+    R f[3][3], g[3][3], th[NTH];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            f[k][u] = R(0);
+            g[k][u] = R(0);
+        }
+#pragma unroll
+    for (int p = 0; p < NTH; p++) th[p] = R(0);
+
+    V4 pa[3], wa[3];
+    R ca[3][3];
+    // Bonded terms first, by lane 0 of each group into shared memory, so that their
+    // latency overlaps the neighbour loops of the other lanes and warps.
+    R *s_bond = (R *)(s_th + ngrp * (a.P + 1)) + 22 * grp;
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            pa[k] = pos[3 * I + k];
+            if (REV) {
+                wa[k] = wgt[3 * I + k];
+                const double sc = k == 0 ? a.acoefO : a.acoefH;
+#pragma unroll
+                for (int u = 0; u < 3; u++) ca[k][u] = (R)__dmul_rn(a.A[9 * (size_t)I + 3 * k + u], sc);
+            }
+        }
+        if (lane == 0) {
+            double xm[9];
+#pragma unroll
+            for (int u = 0; u < 9; u++) xm[u] = a.x[9 * (size_t)I + u];
+            R w[9], ac[9];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                w[3 * k] = REV ? wa[k].x : R(0);
+                w[3 * k + 1] = REV ? wa[k].y : R(0);
+                w[3 * k + 2] = REV ? wa[k].z : R(0);
+#pragma unroll
+                for (int u = 0; u < 3; u++) ac[3 * k + u] = REV ? ca[k][u] : R(0);
+            }
+            R Fb[9], Gb[9], tb[4];
+            bonded<R, REV>(xm, Ld, bc, w, ac, Fb, Gb, tb);
+#pragma unroll
+            for (int u = 0; u < 9; u++) {
+                s_bond[u] = Fb[u];
+                s_bond[9 + u] = Gb[u];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) s_bond[18 + q] = tb[q];
+        }
+        const uint32_t *__restrict__ row = a.nbr + (size_t)I * a.cap;
+        const int cnt = min(a.nbr_cnt[I], a.cap);
+        const R hL = xmul(L, R(0.5));
+        for (int e0 = lane; e0 < cnt; e0 += U * G) {
+            // U entries per lane per iteration: all their loads are issued first.
+            uint32_t ent[U];
+#pragma unroll
+            for (int q = 0; q < U; q++) {
+                const int e = e0 + q * G;
+                ent[q] = e < cnt ? __ldg(row + e) : 0u;   // padding: molecule 0, empty mask
+            }
+            V4 pb[U][3], wb[U][3];
+#pragma unroll
+            for (int q = 0; q < U; q++) {
+                const int J = (int)(ent[q] & 0x7FFFFFu);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    pb[q][k] = pos[3 * J + k];
+                    if (REV) wb[q][k] = wgt[3 * J + k];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < U; q++) {
+                const uint32_t mask = ent[q] >> 23;
+                R sh[3] = {R(0), R(0), R(0)};
+                if (SHIFT) {
+                    sh[0] = image_shift<R, SHIFT>(xsub(pb[q][0].x, pa[0].x), L, hL);
+                    sh[1] = image_shift<R, SHIFT>(xsub(pb[q][0].y, pa[0].y), L, hL);
+                    sh[2] = image_shift<R, SHIFT>(xsub(pb[q][0].z, pa[0].z), L, hL);
+                }
+                pair_row<R, FORM, REV, SHIFT, 0>(mask, pa[0], pb[q], wa[0], wb[q], ca[0], sh, L, invL, nb,
+                                                 f[0], g[0], th);
+                pair_row<R, FORM, REV, SHIFT, 1>(mask, pa[1], pb[q], wa[1], wb[q], ca[1], sh, L, invL, nb,
+                                                 f[1], g[1], th);
+                pair_row<R, FORM, REV, SHIFT, 2>(mask, pa[2], pb[q], wa[2], wb[q], ca[2], sh, L, invL, nb,
+                                                 f[2], g[2], th);
+            }
+        }
+    }
+
+    // Fixed butterfly over the group: every lane ends with the same totals.
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            f[k][u] = group_sum<G>(f[k][u]);
+            if (REV) g[k][u] = group_sum<G>(g[k][u]);
+        }
+    if (REV) {
+#pragma unroll
+        for (int p = 0; p < NTH; p++) th[p] = group_sum<G>(th[p]);
+    }
+    // Every read of the molecule's FP64 state (bonded terms above) precedes the
+    // per-atom writes below, and lane 0's bonded results are visible to lanes 1, 2.
+    __syncwarp();
+
+    double n2 = 0.0;
+    double xn[3] = {0.0, 0.0, 0.0};   // new FP64 position of the lane's atom
+    bool wpos = false;
+    if (active && lane < 3) {
+        const int k = lane;
+        const size_t ia = 3 * (size_t)I + k;
+        const double m = k == 0 ? a.mO : a.mH;
+        double F[3], Gv[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            F[u] = __dadd_rn((double)pick3(k, f[0][u], f[1][u], f[2][u]), (double)s_bond[3 * k + u]);
+            if (REV)
+                Gv[u] = __dadd_rn((double)pick3(k, g[0][u], g[1][u], g[2][u]), (double)s_bond[9 + 3 * k + u]);
+        }
+        if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) atomicOr(a.status, ST_NAN);
+        const double xk[3] = {a.x[3 * ia], a.x[3 * ia + 1], a.x[3 * ia + 2]};
+        if (a.mode & MODE_FORCES_ONLY) {
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                a.F_out[3 * ia + u] = F[u];
+                if (REV) a.G[3 * ia + u] = Gv[u];
+            }
+        } else if (!REV) {
+            // B-A-O-A (water.jl:1032-1037)
+            const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
+            double xi[3] = {0.0, 0.0, 0.0};
+            if (a.s != 0.0) atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                double v = a.v[3 * ia + u], x = xk[u];
+                v = __dadd_rn(v, __ddiv_rn(__dmul_rn(F[u], a.dt), m));
+                x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
+                x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                x = wrap1d(x, Ld);
+                a.v[3 * ia + u] = v;
+                a.x[3 * ia + u] = x;
+                xn[u] = x;
+            }
+            wpos = true;
+        } else {
+            const double dt2 = __dmul_rn(a.dt, a.dt);
+            const bool fuse = (a.mode & MODE_FUSE_NEXT) != 0;
+            const bool defer = (a.mode & MODE_DEFER_BA) != 0;
+            double xi[3] = {0.0, 0.0, 0.0};
+            if (fuse && a.s != 0.0) {
+                const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
+                atom_noise(a.seed_next[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+            }
+            double Cm[3];
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                const size_t e = 3 * ia + u;
+                a.G[e] = Gv[u];
+                n2 = __dadd_rn(n2, __dmul_rn(Gv[u], Gv[u]));
+                // v_{n-1} = v' - F dt / m (water.jl:1516)
+                double v = __dsub_rn(a.v[e], __ddiv_rn(__dmul_rn(F[u], a.dt), m));
+                if (!defer) {
+                    // water.jl:1520-1521
+                    const double B = __dadd_rn(__dmul_rn(a.c, a.B[e]), __dmul_rn(dt2, Gv[u]));
+                    a.B[e] = B;
+                    a.A[e] = __dadd_rn(a.A[e], B);
+                }
+                if (fuse) {
+                    // part 1 of the next reverse step (water.jl:1496-1502)
+                    double x = xk[u];
+                    x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                    v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
+                    x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                    x = wrap1d(x, Ld);
+                    const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
+                                               __ddiv_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]),
+                                                                   __dadd_rn(1.0, a.c)),
+                                                         2.0));
+                    const double C = __dadd_rn(a.C[e], D);
+                    a.D[e] = D;
+                    a.C[e] = C;
+                    a.x[e] = x;
+                    xn[u] = x;
+                    Cm[u] = __ddiv_rn(C, m);
+                }
+                a.v[e] = v;
+            }
+            if (fuse) {
+                V4 wo;
+                wo.x = (R)Cm[0];
+                wo.y = (R)Cm[1];
+                wo.z = (R)Cm[2];
+                wo.w = R(0);
+                ((V4 *)a.wgt_out)[ia] = wo;
+                wpos = true;
+            }
+        }
+    }
+
+    // Gather buffer of the next step: H atoms are written next to their O (lane 0 of
+    // the group), so that molecules are contiguous (gather_coord).
+    {
+        const int src = (threadIdx.x & 31) - lane;
+        const double o0 = __shfl_sync(0xffffffffu, xn[0], src);
+        const double o1 = __shfl_sync(0xffffffffu, xn[1], src);
+        const double o2 = __shfl_sync(0xffffffffu, xn[2], src);
+        if (wpos) {
+            const bool is_h = lane != 0;
+            V4 po;
+            po.x = (R)gather_coord(o0, xn[0], is_h, Ld);
+            po.y = (R)gather_coord(o1, xn[1], is_h, Ld);
+            po.z = (R)gather_coord(o2, xn[2], is_h, Ld);
+            po.w = R(0);
+            ((V4 *)a.pos_out)[3 * (size_t)I + lane] = po;
+        }
+    }
+
+    if (REV) {
+        // Block reduction of the dtheta contributions (fixed order) and of |dl_dfi|^2.
+        const int P = a.P;
+        double *sth = s_th;
+        double *sn2 = s_th + ngrp * P;
+        if (lane == 0) {
+#pragma unroll
+            for (int p = 0; p < NTH; p++) sth[grp * P + p] = active ? (double)th[p] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) sth[grp * P + NF + 1 + q] = active ? (double)s_bond[18 + q] : 0.0;
+        }
+        // lanes 0..2 hold per-atom |G|^2; fold them into lane 0's slot in order
+        const double n2a = __shfl_sync(0xffffffffu, n2, (threadIdx.x & 31) - lane + 1);
+        const double n2b = __shfl_sync(0xffffffffu, n2, (threadIdx.x & 31) - lane + 2);
+        if (lane == 0) sn2[grp] = __dadd_rn(__dadd_rn(n2, n2a), n2b);
+        __syncthreads();
+        if (threadIdx.x < P) {
+            double s = 0.0;
+            for (int q = 0; q < ngrp; q++) s = __dadd_rn(s, sth[q * P + threadIdx.x]);
+            a.part[(size_t)blk * P + threadIdx.x] = __dadd_rn(a.part[(size_t)blk * P + threadIdx.x], s);
+        }
+        if (threadIdx.x == 0 && a.norm2) {
+            double s = 0.0;
+            for (int q = 0; q < ngrp; q++) s = __dadd_rn(s, sn2[q]);
+            a.norm2[blk] = s;
+        }
+    }
+}
+
+// Launch of one (precision, pair form): dispatch on lanes per molecule, image mode
+// and entries per iteration.
+template <typename R, int FORM, int G, bool SHIFT, int U>
+cudaError_t launch_one(bool rev, int n_blk, int threads, const StepArgs &a, const NbConsts<R> &nb,
+                       const BondConsts &bc, cudaStream_t st) {
+    const int ngrp = threads / G;
+    const size_t smem = sizeof(double) * (size_t)ngrp * (a.P + 1) + sizeof(R) * 22 * (size_t)ngrp;
+    if (rev)
+        k_water_step<R, FORM, G, true, SHIFT, U><<<n_blk, threads, smem, st>>>(a, nb, bc);
+    else
+        k_water_step<R, FORM, G, false, SHIFT, U><<<n_blk, threads, smem, st>>>(a, nb, bc);
+    return cudaGetLastError();
+}
+
+template <typename R, int FORM, int G>
+cudaError_t launch_g(bool rev, bool shift, int unroll, int n_blk, int threads, const StepArgs &a,
+                     const NbConsts<R> &nb, const BondConsts &bc, cudaStream_t st) {
+    if (shift)
+        return unroll == 2 ? launch_one<R, FORM, G, true, 2>(rev, n_blk, threads, a, nb, bc, st)
+                           : launch_one<R, FORM, G, true, 1>(rev, n_blk, threads, a, nb, bc, st);
+    return unroll == 2 ? launch_one<R, FORM, G, false, 2>(rev, n_blk, threads, a, nb, bc, st)
+                       : launch_one<R, FORM, G, false, 1>(rev, n_blk, threads, a, nb, bc, st);
+}
+
+}  // namespace
+
+template <typename R, int FORM>
+cudaError_t launch_form(bool rev, int G, int unroll, bool shift, int n_blk, int threads,
+                        const StepArgs &a, const NbConsts<R> &nb, const BondConsts &bc,
+                        cudaStream_t st) {
+    switch (G) {
+        case 8: return launch_g<R, FORM, 8>(rev, shift, unroll, n_blk, threads, a, nb, bc, st);
+        case 16: return launch_g<R, FORM, 16>(rev, shift, unroll, n_blk, threads, a, nb, bc, st);
+        case 32: return launch_g<R, FORM, 32>(rev, shift, unroll, n_blk, threads, a, nb, bc, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace rs

@@ -1,0 +1,20 @@
+"""revsim: B200 (sm_100a) engine for the reversible-simulation gradient of
+greener-group/rev-sim's flexible-water model.
+
+The compute runs in librevsim.so (CUDA, C ABI in include/revsim.h); this package
+is the host side: a ctypes binding (``Engine``), the reference's
+``forward_sim`` / ``reverse_sim`` signatures (``water``), loss builders (``loss``)
+and seeded system generators (``systems``).
+"""
+
+from . import constants, systems
+from ._lib import EXPORTS, LIB_PATH, RevsimError, load
+from .engine import Engine, RdfTerm
+from .loss import oo_l2_term, read_rdf_data, reference_rdf_terms
+from .water import SimSystem, forward_sim, reverse_sim
+
+__all__ = [
+    "Engine", "RdfTerm", "RevsimError", "SimSystem", "forward_sim", "reverse_sim", "load",
+    "constants", "systems", "oo_l2_term", "reference_rdf_terms", "read_rdf_data", "EXPORTS",
+    "LIB_PATH",
+]

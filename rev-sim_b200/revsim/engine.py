@@ -1,0 +1,231 @@
+"""Engine: an owning Python wrapper of one revsim_handle (one or more water replicas)."""
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from . import constants as C
+from ._lib import RevsimError, as_f64, f64p, u64p
+
+PRECISION = {"fp64": 0, "mixed": 1}
+NL_MODE = {"checkpoint": 0, "reconstructed": 1}
+
+
+@dataclass
+class RdfTerm:
+    """One smoothed-RDF loss term (revsim_rdf_term).  sel: 0 = O, 1 = H.
+    ``target`` is [n_target] (shared by all replicas) or [n_replicas, n_target]."""
+    sel1: int
+    sel2: int
+    x_min: float
+    step: float
+    width: float
+    exp_cutoff: float
+    n_grid: int
+    slice_start: int
+    slice_stride: int
+    target: np.ndarray
+    norm: int = 2
+    weight: float = 1.0
+
+
+class Engine:
+    """Owns device state for R replicas of a flexible 3-site water box.
+
+    n_mol, box, temp: scalars (one replica) or sequences (one entry per replica).
+    """
+
+    def __init__(self, n_mol, box, temp=C.TEMP, inter_type="lj", precision="fp64",
+                 nl_mode="checkpoint", device=0, n_steps_log=C.N_STEPS_LOG,
+                 n_steps_nf=C.N_STEPS_NF, cutoff=C.DIST_CUTOFF, nl_cutoff=C.DIST_NEIGHBORS,
+                 coulomb_const=C.COULOMB_CONST, crf_const=None):
+        self._L = _lib.load()
+        n_mol = np.atleast_1d(np.asarray(n_mol, dtype=np.int32))
+        R = len(n_mol)
+        box = np.broadcast_to(np.asarray(box, dtype=np.float64), (R,)).copy()
+        temp = np.broadcast_to(np.asarray(temp, dtype=np.float64), (R,)).copy()
+        if crf_const is None:
+            crf_const = (1.0 / cutoff**3) * ((78.3 - 1) / (2 * 78.3 + 1))
+        self.n_mol, self.box, self.temp = n_mol, box, temp
+        self.R = R
+        self.inter_type = inter_type
+        self.precision = precision
+        self._keep = (n_mol, box, temp)
+        desc = _lib.SystemDesc(
+            R, n_mol.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), f64p(box), f64p(temp),
+            C.INTER_TYPES[inter_type], PRECISION[precision], C.O_MASS, C.H_MASS, coulomb_const,
+            crf_const, cutoff, nl_cutoff, C.KB, n_steps_nf, n_steps_log, NL_MODE[nl_mode], device)
+        h = ctypes.c_void_p()
+        rc = self._L.revsim_create(ctypes.byref(desc), ctypes.byref(h))
+        if rc != 0:
+            raise RevsimError(rc, "revsim_create failed (bad description or no CUDA device)")
+        self._h = h
+        n_atoms = ctypes.c_int64()
+        n_params = ctypes.c_int32()
+        self._check(self._L.revsim_sizes(h, ctypes.byref(n_atoms), ctypes.byref(n_params)))
+        self.n_atoms = n_atoms.value
+        self.n_params = n_params.value
+        self.atom0 = np.concatenate([[0], np.cumsum(3 * n_mol)[:-1]]).astype(np.int64)
+        self.terms = []
+
+    # ------------------------------------------------------------------ basics
+    def _check(self, rc):
+        if rc != 0:
+            msg = self._L.revsim_last_error(self._h).decode() if getattr(self, "_h", None) else ""
+            raise RevsimError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.revsim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stream(self):
+        return self._L.revsim_stream(self._h)
+
+    def launch_count(self):
+        return self._L.revsim_launch_count(self._h)
+
+    # ------------------------------------------------------------------ state
+    def set_params(self, theta):
+        theta = as_f64(theta)
+        self._check(self._L.revsim_set_params(self._h, f64p(theta), len(theta)))
+
+    def set_state(self, x, v):
+        x = as_f64(x, (self.n_atoms, 3))
+        v = as_f64(v, (self.n_atoms, 3))
+        self._check(self._L.revsim_set_state(self._h, f64p(x), f64p(v)))
+
+    def get_state(self):
+        x = np.zeros((self.n_atoms, 3))
+        v = np.zeros((self.n_atoms, 3))
+        self._check(self._L.revsim_get_state(self._h, f64p(x), f64p(v)))
+        return x, v
+
+    def set_loss(self, terms):
+        self.terms = list(terms)
+        arr = (_lib.RdfTermC * max(1, len(terms)))()
+        tg = []
+        for i, t in enumerate(terms):
+            target = np.asarray(t.target, dtype=np.float64)
+            if target.ndim == 1:
+                target = np.broadcast_to(target, (self.R, target.size))
+            target = np.ascontiguousarray(target)
+            tg.append(target)
+            arr[i] = _lib.RdfTermC(t.sel1, t.sel2, t.x_min, t.step, t.width, t.exp_cutoff,
+                                   t.n_grid, t.slice_start, t.slice_stride, target.shape[1],
+                                   t.norm, t.weight)
+        ptrs = (ctypes.POINTER(ctypes.c_double) * max(1, len(tg)))(*[f64p(a) for a in tg])
+        self._check(self._L.revsim_set_loss(self._h, len(terms), arr, ptrs))
+
+    # ------------------------------------------------------------ primitives
+    def forces(self):
+        F = np.zeros((self.n_atoms, 3))
+        self._check(self._L.revsim_forces(self._h, f64p(F)))
+        return F
+
+    def force_vjp(self, w, acoef):
+        w = as_f64(w, (self.n_atoms, 3))
+        acoef = as_f64(acoef, (self.n_atoms, 3))
+        F = np.zeros((self.n_atoms, 3))
+        G = np.zeros((self.n_atoms, 3))
+        th = np.zeros((self.R, self.n_params))
+        self._check(self._L.revsim_force_vjp(self._h, f64p(w), f64p(acoef), f64p(F), f64p(G),
+                                             f64p(th)))
+        return F, G, th
+
+    def noise(self, seeds):
+        seeds = np.ascontiguousarray(np.broadcast_to(np.asarray(seeds, dtype=np.uint64), (self.R,)))
+        xi = np.zeros((self.n_atoms, 3))
+        self._check(self._L.revsim_noise(self._h, u64p(seeds), f64p(xi)))
+        return xi
+
+    def neighbor_pairs(self, replica=0):
+        n = ctypes.c_int64()
+        cap = 400 * 3 * int(self.n_mol[replica]) + 64
+        out = np.zeros((cap, 2), dtype=np.int32)
+        pi = out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        self._check(self._L.revsim_neighbor_pairs(self._h, replica, pi, cap, ctypes.byref(n)))
+        if n.value > cap:
+            cap = n.value
+            out = np.zeros((cap, 2), dtype=np.int32)
+            pi = out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            self._check(self._L.revsim_neighbor_pairs(self._h, replica, pi, cap, ctypes.byref(n)))
+        p = out[: n.value]
+        return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+    def loss_grad(self, grad=True):
+        loss = np.zeros(self.R)
+        g = np.zeros((self.n_atoms, 3)) if grad else None
+        self._check(self._L.revsim_loss_grad(self._h, f64p(loss), f64p(g) if grad else None))
+        return loss, g
+
+    def rdf(self, term=0, replica=0):
+        h = np.zeros(self.terms[term].n_grid)
+        self._check(self._L.revsim_rdf(self._h, term, replica, f64p(h)))
+        return h
+
+    # --------------------------------------------------------------- drivers
+    def _seeds(self, seeds, n_steps):
+        s = np.asarray(seeds, dtype=np.uint64)
+        if s.ndim == 1:
+            s = np.repeat(s[:, None], self.R, axis=1)
+        if s.shape != (n_steps, self.R):
+            raise ValueError(f"noise seeds must be [n_steps] or [n_steps, n_replicas], got {s.shape}")
+        return np.ascontiguousarray(s)
+
+    def forward(self, seeds, gamma, n_steps, n_steps_loss, dt, calc_loss=True):
+        s = self._seeds(seeds, n_steps)
+        loss = np.zeros(self.R)
+        self._check(self._L.revsim_forward(self._h, u64p(s), gamma, n_steps, n_steps_loss, dt,
+                                           1 if calc_loss else 0, f64p(loss)))
+        return loss
+
+    def reverse(self, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip=np.inf):
+        s = self._seeds(seeds, n_steps)
+        loss = np.zeros(self.R)
+        g = np.zeros((self.R, self.n_params))
+        self._check(self._L.revsim_reverse(self._h, u64p(s), gamma, n_steps, n_steps_loss,
+                                           n_steps_trunc, dt, clip, f64p(loss), f64p(g)))
+        return loss, g
+
+    # --------------------------------------------------------- instrumentation
+    def set_kernel_timing(self, on):
+        self._check(self._L.revsim_set_kernel_timing(self._h, 1 if on else 0))
+
+    def kernel_time(self, which=0):
+        """(total ms, launches) of the reverse (which=0) or forward (1) step kernel."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        self._check(self._L.revsim_kernel_time(self._h, which, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def set_launch_shape(self, lanes=0, mols_per_cta=0, unroll=0):
+        self._check(self._L.revsim_set_launch_shape(self._h, lanes, mols_per_cta, unroll))
+
+    def launch_shape(self):
+        g, m, u = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._L.revsim_get_launch_shape(self._h, ctypes.byref(g), ctypes.byref(m),
+                                                    ctypes.byref(u)))
+        return g.value, m.value, u.value
+
+    def autotune(self, dt=0.001):
+        self._check(self._L.revsim_autotune(self._h, dt))
+        return self.launch_shape()

@@ -1,0 +1,111 @@
+"""The reference's gradient entry points, with the reference's signatures.
+
+``forward_sim`` mirrors water.jl:977-1105 and ``reverse_sim`` water.jl:1435-1558:
+same positional arguments, same meaning, same return tuples, so a caller of the
+reference (the self-check block water.jl:1592-1621, ``train()`` water.jl:1662-1669)
+switches by changing the import.  The work runs in librevsim.so on the GPU.
+
+Differences, each deliberate:
+* coordinates/velocities are numpy arrays [N, 3] (nm, nm/ps); ``boundary`` is the
+  cubic box side in nm (``None``: keep the engine's);
+* the loss targets are explicit (``loss_terms``): the reference reads the Soper
+  2013 file at load time (water.jl:629); ``loss.read_rdf_data`` + ``loss.reference_rdf_terms``
+  rebuild exactly that loss from the file;
+* ``run_grads=True`` (the Zygote unrolled-RAD check, water.jl:1052-1099),
+  ``use_barostat=True`` and the enthalpy-of-vaporisation loss are not part of the
+  engine and raise ``NotImplementedError``;
+* ``n_threads`` is accepted and ignored;
+* noise: per-step seeds drive a counter-based Philox generator, regenerated
+  identically in the reverse pass (the reference uses Xoshiro(seed) + randn).
+"""
+
+import numpy as np
+
+from . import constants as C
+from .engine import Engine
+
+
+class SimSystem:
+    """What forward_sim / reverse_sim return in place of Molly's System."""
+
+    def __init__(self, engine, coords, velocities, boundary):
+        self.engine = engine
+        self.coords = coords
+        self.velocities = velocities
+        self.boundary = boundary
+
+    @property
+    def loggers(self):
+        # The forward snapshots (every n_steps_log steps) and neighbour-build positions
+        # live on the device inside the engine; reverse_sim takes the engine itself.
+        return self.engine
+
+
+def _engine_for(coords, boundary, inter_type, engine, precision):
+    n_atoms = np.asarray(coords).shape[0]
+    if n_atoms % 3:
+        raise ValueError("water systems have 3 atoms per molecule")
+    if engine is not None:
+        return engine
+    return Engine(n_atoms // 3, boundary, inter_type=inter_type, precision=precision)
+
+
+def _check_loss(loss_type):
+    if loss_type not in ("rdf",):
+        raise NotImplementedError(f"loss_type {loss_type!r}: the engine implements the RDF loss")
+
+
+def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss, params,
+                dt, n_threads, inter_type, loss_type, run_grads=False, calc_loss=True,
+                use_barostat=False, *, loss_terms=None, engine=None, precision="fp64"):
+    """water.jl:977.  Returns (sys, loss, grads); grads is [None] * P as in the
+    reference's run_grads=false branch (water.jl:1100-1102)."""
+    if run_grads:
+        raise NotImplementedError("run_grads (Zygote unrolled RAD) is not part of the engine")
+    if use_barostat:
+        raise NotImplementedError("the Monte-Carlo barostat is not part of the engine")
+    if calc_loss:
+        _check_loss(loss_type)
+    eng = _engine_for(coords, boundary, inter_type, engine, precision)
+    eng.set_params(params)
+    eng.set_state(coords, velocities)
+    if calc_loss:
+        if loss_terms is None and not eng.terms:
+            raise ValueError("calc_loss needs loss_terms")
+        if loss_terms is not None:
+            eng.set_loss(loss_terms)
+    loss = eng.forward(noise_seeds, gamma, n_steps, n_steps_loss if n_steps_loss else max(n_steps, 1),
+                       dt, calc_loss)
+    x, v = eng.get_state()
+    sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
+    return sys, (float(loss[0]) if eng.R == 1 else loss), [None] * eng.n_params
+
+
+def reverse_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss,
+                n_steps_trunc, params, dt, n_threads, fwd_loggers, clip_norm_threshold, inter_type,
+                loss_type, *, loss_terms=None):
+    """water.jl:1435.  ``fwd_loggers`` is ``sys.loggers`` of the forward_sim result.
+    Returns (sys, l, dl_dp, l_rdf, l_ev)."""
+    if n_steps_trunc > n_steps_loss:
+        raise ValueError("n_steps_trunc must not be greater than n_steps_loss")
+    _check_loss(loss_type)
+    eng = fwd_loggers
+    if not isinstance(eng, Engine):
+        raise TypeError("fwd_loggers must be the loggers of a forward_sim result")
+    eng.set_params(params)
+    eng.set_state(coords, velocities)
+    if loss_terms is not None:
+        eng.set_loss(loss_terms)
+    clip = np.inf if clip_norm_threshold is None else float(clip_norm_threshold)
+    loss, g = eng.reverse(noise_seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip)
+    x, v = eng.get_state()
+    sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
+    if eng.R == 1:
+        l, dl_dp = float(loss[0]), g[0]
+    else:
+        l, dl_dp = loss, g
+    return sys, l, dl_dp, l, 0.0 * l
+
+
+def default_params(inter_type="lj"):
+    return np.array(C.default_params(inter_type))
