@@ -43,8 +43,8 @@ UNIT = "atom-steps/s"
 # an O-O LJ pair), reverse 170 (force + 3x3 VJP with mass scaling + dF/dtheta).
 FLOPS_FWD_IPAIR, FLOPS_FWD_OO_EXTRA, FLOPS_REV_IPAIR = 40, 15, 170
 # DRAM traffic per reverse-step launch of the default workload, from ncu
-# (profiles/rev_step_ncu.md); None until measured.
-REV_STEP_DRAM_BYTES = None
+# (profiles/rev_step_ncu_water3000.md: dram__bytes_read.sum 5.395 MB, write 0).
+REV_STEP_DRAM_BYTES = 5.395e6
 
 
 def parse():
