@@ -175,6 +175,22 @@ int32_t revsim_get_launch_shape(revsim_handle *h, int32_t *lanes_per_mol, int32_
                                 int32_t *unroll);
 int32_t revsim_autotune(revsim_handle *h, double dt);
 
+/* Allocation-free loss and dL/dx for one water box, for callers that cannot let the
+ * library allocate device memory (a host whose pool allocator owns all device
+ * memory, a loop that must avoid the synchronisation cudaMalloc implies, a fully
+ * pre-budgeted service).  No counterpart in the reference: it is the loss of
+ * revsim_loss_grad for one term and one box, computed on caller-owned device
+ * buffers: d_x [3 * 3 n_mol] positions (FP64, O H H per molecule), d_target
+ * [n_target], outputs d_loss [1] and d_dLdx [3 * 3 n_mol], all on the current device,
+ * ordered on `stream` (a cudaStream_t; NULL = legacy default stream).  Its scratch is
+ * a fixed array inside the library (grids of at most 8192 points; a larger n_grid
+ * returns REVSIM_ERR_BADARG); it calls no cudaMalloc or cudaFree.  The first call on
+ * a device looks up that array's device address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+int32_t revsim_rdf_loss_grad_noalloc(const double *d_x, int32_t n_mol, double box,
+                                     const revsim_rdf_term *term, const double *d_target,
+                                     double *d_loss, double *d_dLdx, void *stream);
+
 /* Instrumentation with no counterpart in the reference: the measured FP32 fused
  * multiply-add throughput (TFLOP/s, 2 flops per FMA) of a device, the roofline
  * denominator of the FP32-pipe-bound step kernels. */

@@ -10,6 +10,10 @@
 // quantity Enzyme differentiates in the reference's pullback, water.jl:715-736).
 // Runs once per loss block, so it is written for clarity: one thread per ordered
 // atom pair, shared-memory histogram, FP64 throughout.
+#include <cmath>
+#include <mutex>
+
+#include "revsim.h"
 #include "rs_internal.h"
 
 namespace rs {
@@ -195,4 +199,104 @@ cudaError_t launch_rdf_finalize(const RdfArgs &a, int R, const double *pre, cons
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free RDF loss and gradient for one water box.
+//
+// Some callers cannot let this library call cudaMalloc: a host that owns every byte
+// of device memory through its own pool allocator (a Julia or Python framework that
+// hands out device pointers), a loop that must not hit the device-wide
+// synchronisation cudaMalloc/cudaFree imply, or a service whose memory is budgeted
+// in full before it starts.  For them this entry point takes the caller's device
+// buffers and keeps its scratch (the histogram, dL/dh, the normalisation constant
+// and a one-box table, at most kNoallocMaxGrid grid points) in the file-scope
+// array g_rdf_scratch, which every GPU that loads the library holds until the
+// process exits.  Host code cannot use the array's name as a device address: the
+// address is looked up once per device with cudaGetSymbolAddress, with that device
+// current, on the first call that device sees (make that first call before any
+// stream capture).  All calls share the one array and leave the last call's values
+// in it; each call clears what must start at zero, and calls that overlap on the GPU
+// (concurrent streams, or several host threads on one device) race on it.
+namespace {
+
+constexpr int kNoallocMaxGrid = 8192;
+// layout (doubles): hist [kNoallocMaxGrid + 1] (the normaliser V / (4 pi n1 n2 step)
+// sits right after the n_grid used entries) | dL/dh [kNoallocMaxGrid] | box [1] |
+// {atom0, n_mol} as two ints [1]
+constexpr int kNoallocDLdh = kNoallocMaxGrid + 1;
+constexpr int kNoallocBox = 2 * kNoallocMaxGrid + 1;
+constexpr int kNoallocInts = 2 * kNoallocMaxGrid + 2;
+constexpr int kNoallocDoubles = 2 * kNoallocMaxGrid + 3;
+static __device__ __align__(256) double g_rdf_scratch[kNoallocDoubles];
+
+__global__ void k_noalloc_tables(double *s, int n_grid, double pre, double box, int n_mol) {
+    s[n_grid] = pre;
+    s[kNoallocBox] = box;
+    int *t = reinterpret_cast<int *>(s + kNoallocInts);
+    t[0] = 0;
+    t[1] = n_mol;
+}
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_addr[256] = {};
+
+}  // namespace
+
 }  // namespace rs
+
+extern "C" int32_t revsim_rdf_loss_grad_noalloc(const double *d_x, int32_t n_mol, double box,
+                                                const revsim_rdf_term *t, const double *d_target,
+                                                double *d_loss, double *d_dLdx, void *stream) {
+    using namespace rs;
+    if (!d_x || !t || !d_target || !d_loss || !d_dLdx || n_mol < 1 || !(box > 0)) return REVSIM_ERR_BADARG;
+    if (t->n_grid < 1 || t->n_grid > kNoallocMaxGrid) return REVSIM_ERR_BADARG;   // beyond the scratch size
+    if (!(t->step > 0) || !(t->width > 0) || !(t->exp_cutoff >= 0) || t->n_target < 1 || t->slice_start < 0 ||
+        t->slice_stride < 1 || t->slice_start + (long long)(t->n_target - 1) * t->slice_stride >= t->n_grid ||
+        (t->norm != 1 && t->norm != 2) || (t->sel1 != 0 && t->sel1 != 1) || (t->sel2 != 0 && t->sel2 != 1))
+        return REVSIM_ERR_BADARG;
+    const double q = t->x_min / t->step;
+    if (std::fabs(q - std::llround(q)) > 1e-6) return REVSIM_ERR_BADARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return REVSIM_ERR_CUDA;
+    double *s = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_rdf_scratch) != cudaSuccess || !p) return REVSIM_ERR_CUDA;
+            g_noalloc_addr[dev] = static_cast<double *>(p);
+        }
+        s = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double n1 = t->sel1 == 0 ? n_mol : 2.0 * n_mol;
+    const double n2 = t->sel2 == 0 ? n_mol : 2.0 * n_mol;
+    const double pre = box * box * box / (4 * 3.14159265358979323846 * n1 * n2 * t->step);
+    k_noalloc_tables<<<1, 1, 0, st>>>(s, t->n_grid, pre, box, n_mol);
+    if (cudaMemsetAsync(s, 0, sizeof(double) * t->n_grid, st) != cudaSuccess ||
+        cudaMemsetAsync(d_loss, 0, sizeof(double), st) != cudaSuccess ||
+        cudaMemsetAsync(d_dLdx, 0, sizeof(double) * 9 * (size_t)n_mol, st) != cudaSuccess)
+        return REVSIM_ERR_CUDA;
+    RdfArgs a;
+    a.x = d_x;
+    a.rep_atom0 = reinterpret_cast<const int *>(s + kNoallocInts);
+    a.rep_nmol = a.rep_atom0 + 1;
+    a.rep_box = s + kNoallocBox;
+    a.sel1 = t->sel1;
+    a.sel2 = t->sel2;
+    a.x_min = t->x_min;
+    a.step = t->step;
+    a.width = t->width;
+    a.cutoff = t->exp_cutoff;
+    a.n_grid = t->n_grid;
+    a.off = (int)std::llround(q) - 1;
+    a.hist = s;
+    a.dLdh = s + kNoallocDLdh;
+    a.dLdx = d_dLdx;
+    if (launch_rdf(a, 1, (int)n1, (int)n2, false, st) != cudaSuccess ||
+        launch_rdf_finalize(a, 1, s + t->n_grid, d_target, t->slice_start, t->slice_stride, t->n_target,
+                            t->norm, t->weight, d_loss, s + kNoallocDLdh, st) != cudaSuccess ||
+        launch_rdf(a, 1, (int)n1, (int)n2, true, st) != cudaSuccess)
+        return REVSIM_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? REVSIM_OK : REVSIM_ERR_CUDA;
+}
+

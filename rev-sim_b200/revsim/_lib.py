@@ -33,7 +33,7 @@ EXPORTS = [
     "revsim_noise", "revsim_loss_grad", "revsim_rdf", "revsim_forward", "revsim_reverse",
     "revsim_stream", "revsim_launch_count", "revsim_set_kernel_timing", "revsim_kernel_time",
     "revsim_set_launch_shape", "revsim_get_launch_shape", "revsim_autotune",
-    "revsim_probe_fp32_tflops",
+    "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc",
 ]
 
 
@@ -115,6 +115,7 @@ def load(path=LIB_PATH):
         "revsim_get_launch_shape": (i32, [vp, pi32, pi32, pi32]),
         "revsim_autotune": (i32, [vp, d]),
         "revsim_probe_fp32_tflops": (i32, [i32, pd]),
+        "revsim_rdf_loss_grad_noalloc": (i32, [vp, i32, d, P(RdfTermC), vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
