@@ -348,7 +348,8 @@ def run_ours(a):
                 "flops_per_launch": flops_launch,
                 "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops); "
                                "the step kernels are scalar FP32 work, neither HBM- nor tensor-bound",
-                "shape": {"lanes_per_mol": shape[0], "mols_per_cta": shape[1], "unroll": shape[2]},
+                "shape": {"reverse": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[0])),
+                          "forward": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[1]))},
                 "forward_step_launch_ms": ft_ms / max(ft_n, 1),
                 "step_kernels_share_of_gradient": (kt_ms + ft_ms) / ms_step}
 

@@ -165,14 +165,15 @@ int64_t revsim_launch_count(const revsim_handle *h);
 int32_t revsim_set_kernel_timing(revsim_handle *h, int32_t enable);
 int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, int64_t *launches);
 
-/* Block shape of the step kernels: lanes per molecule (8, 16 or 32), molecules per
- * CTA, and neighbour entries per lane per loop iteration (1 or 2); 0 keeps the
- * current value.  revsim_autotune times the allowed shapes on the current state and
- * keeps the fastest. */
-int32_t revsim_set_launch_shape(revsim_handle *h, int32_t lanes_per_mol, int32_t mols_per_cta,
-                                int32_t unroll);
-int32_t revsim_get_launch_shape(revsim_handle *h, int32_t *lanes_per_mol, int32_t *mols_per_cta,
-                                int32_t *unroll);
+/* Block shape of the step kernels (which = 0: reverse step, 1: forward step, -1: both):
+ * lanes per molecule (8, 16 or 32), molecules per CTA, and the neighbour loop form
+ * (1: one entry per lane per iteration, 2: two, 3: one with the next entry prefetched;
+ * 3 allows at most 256 threads per CTA); 0 keeps the current value.  revsim_autotune times the
+ * allowed shapes of each kernel on the current state and keeps the fastest. */
+int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes_per_mol,
+                                int32_t mols_per_cta, int32_t unroll);
+int32_t revsim_get_launch_shape(revsim_handle *h, int32_t which, int32_t *lanes_per_mol,
+                                int32_t *mols_per_cta, int32_t *unroll);
 int32_t revsim_autotune(revsim_handle *h, double dt);
 
 /* Allocation-free loss and dL/dx for one water box, for callers that cannot let the

@@ -65,12 +65,16 @@ struct revsim_handle {
     int P = 0, NFp = 0;
     bool have_params = false, have_state = false;
 
-    int G = 32, mpc = 8, unroll = 1, n_blk = 0;
+    // Launch shapes of the step kernels, [0] reverse and [1] forward, each with its own
+    // CTA -> (replica, first molecule, molecule count) table.
+    struct Shape {
+        int G = 32, mpc = 8, U = 1, n_blk = 0;
+        int *d_blk_rep = nullptr, *d_blk_mol0 = nullptr, *d_blk_nmol = nullptr;
+    } shp[2];
     bool shift_ok = false;   // one periodic image per molecule pair is exact for every box
     int cap = 0;
 
     // tables
-    int *d_blk_rep = nullptr, *d_blk_mol0 = nullptr, *d_blk_nmol = nullptr;
     int *d_mol_rep = nullptr, *d_atom_rep = nullptr, *d_rep_atom0 = nullptr, *d_rep_nmol = nullptr;
     double *d_rep_box = nullptr, *d_rep_sdO = nullptr, *d_rep_sdH = nullptr;
     // cells
@@ -213,12 +217,13 @@ BondConsts bond_consts(const revsim_handle *h) {
     return BondConsts{t[1], t[2], t[3], t[4]};
 }
 
-StepArgs base_args(revsim_handle *h) {
+StepArgs base_args(revsim_handle *h, bool rev) {
     StepArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.blk_rep = h->d_blk_rep;
-    a.blk_mol0 = h->d_blk_mol0;
-    a.blk_nmol = h->d_blk_nmol;
+    const revsim_handle::Shape &sh = h->shp[rev ? 0 : 1];
+    a.blk_rep = sh.d_blk_rep;
+    a.blk_mol0 = sh.d_blk_mol0;
+    a.blk_nmol = sh.d_blk_nmol;
     a.rep_box = h->d_rep_box;
     a.rep_sdO = h->d_rep_sdO;
     a.rep_sdH = h->d_rep_sdH;
@@ -241,8 +246,13 @@ StepArgs base_args(revsim_handle *h) {
     return a;
 }
 
-int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a) {
-    const int threads = h->G * h->mpc;
+int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a_in) {
+    const revsim_handle::Shape &sh = h->shp[rev ? 0 : 1];
+    StepArgs a = a_in;
+    a.blk_rep = sh.d_blk_rep;
+    a.blk_mol0 = sh.d_blk_mol0;
+    a.blk_nmol = sh.d_blk_nmol;
+    const int threads = sh.G * sh.mpc;
     const BondConsts bc = bond_consts(h);
     const bool timed = h->ktime && !(a.mode & MODE_FORCES_ONLY);
     const int which = rev ? 0 : 1;
@@ -256,10 +266,10 @@ int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a) {
     }
     cudaError_t e;
     if (h->prec == REVSIM_MIXED)
-        e = launch_step<float>(rev, h->form, h->G, h->unroll, h->shift_ok, h->n_blk, threads, a,
+        e = launch_step<float>(rev, h->form, sh.G, sh.U, h->shift_ok, sh.n_blk, threads, a,
                                nb_consts<float>(h), bc, h->st);
     else
-        e = launch_step<double>(rev, h->form, h->G, h->unroll, h->shift_ok, h->n_blk, threads, a,
+        e = launch_step<double>(rev, h->form, sh.G, sh.U, h->shift_ok, sh.n_blk, threads, a,
                                 nb_consts<double>(h), bc, h->st);
     h->launches++;
     if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("step kernel: ") + cudaGetErrorString(e));
@@ -270,30 +280,35 @@ int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a) {
     return REVSIM_OK;
 }
 
-int build_block_table(revsim_handle *h) {
+// CTA table of one direction (0 reverse, 1 forward): CTAs never straddle replicas, so
+// the reverse kernel's per-CTA dtheta partials are per replica.
+int build_block_table(revsim_handle *h, int dir) {
+    revsim_handle::Shape &sh = h->shp[dir];
     std::vector<int> br, bm, bn;
     for (int r = 0; r < h->R; r++)
-        for (int m = 0; m < h->nmol[r]; m += h->mpc) {
+        for (int m = 0; m < h->nmol[r]; m += sh.mpc) {
             br.push_back(r);
             bm.push_back(h->mol0[r] + m);
-            bn.push_back(std::min(h->mpc, h->nmol[r] - m));
+            bn.push_back(std::min(sh.mpc, h->nmol[r] - m));
         }
-    h->n_blk = (int)br.size();
-    dfree(h->d_blk_rep);
-    dfree(h->d_blk_mol0);
-    dfree(h->d_blk_nmol);
-    dfree(h->d_part);
-    dfree(h->d_norm2);
-    h->d_blk_rep = h->d_blk_mol0 = h->d_blk_nmol = nullptr;
-    h->d_part = h->d_norm2 = nullptr;
-    CK(dalloc(&h->d_blk_rep, br.size()));
-    CK(dalloc(&h->d_blk_mol0, br.size()));
-    CK(dalloc(&h->d_blk_nmol, br.size()));
-    CK(dalloc(&h->d_part, br.size() * (size_t)std::max(h->P, 1)));
-    CK(dalloc(&h->d_norm2, br.size()));
-    CK(cudaMemcpy(h->d_blk_rep, br.data(), sizeof(int) * br.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_blk_mol0, bm.data(), sizeof(int) * bm.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_blk_nmol, bn.data(), sizeof(int) * bn.size(), cudaMemcpyHostToDevice));
+    sh.n_blk = (int)br.size();
+    dfree(sh.d_blk_rep);
+    dfree(sh.d_blk_mol0);
+    dfree(sh.d_blk_nmol);
+    sh.d_blk_rep = sh.d_blk_mol0 = sh.d_blk_nmol = nullptr;
+    CK(dalloc(&sh.d_blk_rep, br.size()));
+    CK(dalloc(&sh.d_blk_mol0, br.size()));
+    CK(dalloc(&sh.d_blk_nmol, br.size()));
+    CK(cudaMemcpy(sh.d_blk_rep, br.data(), sizeof(int) * br.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sh.d_blk_mol0, bm.data(), sizeof(int) * bm.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sh.d_blk_nmol, bn.data(), sizeof(int) * bn.size(), cudaMemcpyHostToDevice));
+    if (dir == 0) {
+        dfree(h->d_part);
+        dfree(h->d_norm2);
+        h->d_part = h->d_norm2 = nullptr;
+        CK(dalloc(&h->d_part, br.size() * (size_t)std::max(h->P, 1)));
+        CK(dalloc(&h->d_norm2, br.size()));
+    }
     return REVSIM_OK;
 }
 
@@ -497,7 +512,7 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     CK(cudaMemcpyAsync(h->d_snap_x, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemcpyAsync(h->d_snap_v, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
-    StepArgs a = base_args(h);
+    StepArgs a = base_args(h, false);
     a.dt = dt;
     a.c = c;
     a.s = s;
@@ -538,13 +553,13 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     const int R = h->R;
     const bool clipping = std::isfinite(clip);
     int rc;
-    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * h->P, h->st));
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
     if ((rc = loss_dev(h, true, h->d_loss_acc))) return rc;
     CK(launch_init_adjoint(h->N, h->d_dLdx, c, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->st));
     h->launches++;
 
-    StepArgs a = base_args(h);
+    StepArgs a = base_args(h, true);
     a.dt = dt;
     a.c = c;
     a.s = s;
@@ -606,13 +621,13 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
             if ((rc = launch_step_k(h, true, a))) return rc;
             if (clipping) {
                 // Per-replica norm of dl_dfi from the block partials (fixed order).
-                std::vector<double> n2(h->n_blk);
-                std::vector<int> br(h->n_blk);
-                CK(cudaMemcpyAsync(n2.data(), h->d_norm2, sizeof(double) * h->n_blk, cudaMemcpyDeviceToHost, h->st));
-                CK(cudaMemcpyAsync(br.data(), h->d_blk_rep, sizeof(int) * h->n_blk, cudaMemcpyDeviceToHost, h->st));
+                std::vector<double> n2(h->shp[0].n_blk);
+                std::vector<int> br(h->shp[0].n_blk);
+                CK(cudaMemcpyAsync(n2.data(), h->d_norm2, sizeof(double) * h->shp[0].n_blk, cudaMemcpyDeviceToHost, h->st));
+                CK(cudaMemcpyAsync(br.data(), h->shp[0].d_blk_rep, sizeof(int) * h->shp[0].n_blk, cudaMemcpyDeviceToHost, h->st));
                 CK(cudaStreamSynchronize(h->st));
                 std::vector<double> acc(R, 0.0);
-                for (int b = 0; b < h->n_blk; b++) acc[br[b]] += n2[b];
+                for (int b = 0; b < h->shp[0].n_blk; b++) acc[br[b]] += n2[b];
                 for (int r = 0; r < R; r++) {
                     scale[2 * r] = std::sqrt(acc[r]);
                     scale[2 * r + 1] = clip;
@@ -661,19 +676,24 @@ int collect_kernel_times(revsim_handle *h) {
 
 // Sum the dtheta block partials per replica (FP64, block order).
 int reduce_part(revsim_handle *h, std::vector<double> &out) {
-    std::vector<double> part((size_t)h->n_blk * h->P);
-    std::vector<int> br(h->n_blk);
+    std::vector<double> part((size_t)h->shp[0].n_blk * h->P);
+    std::vector<int> br(h->shp[0].n_blk);
     CK(cudaMemcpyAsync(part.data(), h->d_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaMemcpyAsync(br.data(), h->d_blk_rep, sizeof(int) * h->n_blk, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(br.data(), h->shp[0].d_blk_rep, sizeof(int) * h->shp[0].n_blk, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     out.assign((size_t)h->R * h->P, 0.0);
-    for (int b = 0; b < h->n_blk; b++)
+    for (int b = 0; b < h->shp[0].n_blk; b++)
         for (int p = 0; p < h->P; p++) out[(size_t)br[b] * h->P + p] += part[(size_t)b * h->P + p];
     return REVSIM_OK;
 }
 
 void free_all(revsim_handle *h) {
-    void *ptrs[] = {h->d_blk_rep, h->d_blk_mol0, h->d_blk_nmol, h->d_mol_rep, h->d_atom_rep,
+    for (auto &sh : h->shp) {
+        dfree(sh.d_blk_rep);
+        dfree(sh.d_blk_mol0);
+        dfree(sh.d_blk_nmol);
+    }
+    void *ptrs[] = {h->d_mol_rep, h->d_atom_rep,
                     h->d_rep_atom0, h->d_rep_nmol, h->d_rep_box, h->d_rep_sdO, h->d_rep_sdH,
                     h->d_rep_nc, h->d_rep_cell_off, h->d_cell_of_mol, h->d_cell_cnt, h->d_cell_start,
                     h->d_cell_fill, h->d_cell_tmp, h->d_cell_sorted, h->d_nbr, h->d_nbr_cnt, h->d_x,
@@ -828,7 +848,9 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
          cudaMemset(h->d_C, 0, sizeof(double) * n3) == cudaSuccess &&
          cudaMemset(h->d_A, 0, sizeof(double) * n3) == cudaSuccess;
     if (!ok) return cfail("upload");
-    if (build_block_table(h) != REVSIM_OK || alloc_nbr(h, cap) != REVSIM_OK) return cfail("tables");
+    if (build_block_table(h, 0) != REVSIM_OK || build_block_table(h, 1) != REVSIM_OK ||
+        alloc_nbr(h, cap) != REVSIM_OK)
+        return cfail("tables");
     *out = h;
     return REVSIM_OK;
 }
@@ -967,7 +989,7 @@ int32_t revsim_forces(revsim_handle *h, double *F) {
     if (!F) return fail(h, REVSIM_ERR_BADARG, "F is null");
     if ((rc = build_nlist_checked(h, h->d_x))) return rc;
     if ((rc = pack(h, 0, false))) return rc;
-    StepArgs a = base_args(h);
+    StepArgs a = base_args(h, false);
     a.pos_in = h->d_pos[0];
     a.F_out = h->d_F;
     a.mode = MODE_FORCES_ONLY;
@@ -988,8 +1010,8 @@ int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef,
     CK(cudaMemcpyAsync(h->d_A, acoef, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
     if ((rc = build_nlist_checked(h, h->d_x))) return rc;
     if ((rc = pack(h, 0, true))) return rc;
-    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * h->P, h->st));
-    StepArgs a = base_args(h);
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
+    StepArgs a = base_args(h, true);
     a.pos_in = h->d_pos[0];
     a.wgt_in = h->d_wgt[0];
     a.F_out = h->d_F;
@@ -1147,82 +1169,91 @@ int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, in
     return REVSIM_OK;
 }
 
-int32_t revsim_set_launch_shape(revsim_handle *h, int32_t lanes, int32_t mpc, int32_t unroll) {
-    if (!h) return REVSIM_ERR_BADARG;
-    const int G = lanes ? lanes : h->G, m = mpc ? mpc : h->mpc, U = unroll ? unroll : h->unroll;
-    if ((G != 8 && G != 16 && G != 32) || m < 1 || G * m > 512 || (G * m) % 32 != 0 || (U != 1 && U != 2))
-        return fail(h, REVSIM_ERR_BADARG, "unsupported launch shape");
+int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes, int32_t mpc,
+                                int32_t unroll) {
+    if (!h || which < -1 || which > 1) return REVSIM_ERR_BADARG;
     CK(cudaSetDevice(h->dev));
     CK(cudaStreamSynchronize(h->st));
-    h->G = G;
-    h->unroll = U;
-    if (m != h->mpc) {
-        h->mpc = m;
-        int rc = build_block_table(h);
-        if (rc) return rc;
+    for (int dir = 0; dir < 2; dir++) {
+        if (which >= 0 && which != dir) continue;
+        revsim_handle::Shape &sh = h->shp[dir];
+        const int G = lanes ? lanes : sh.G, m = mpc ? mpc : sh.mpc, U = unroll ? unroll : sh.U;
+        if ((G != 8 && G != 16 && G != 32) || m < 1 || G * m > 512 || (G * m) % 32 != 0 || U < 1 || U > 3 ||
+            (U == 3 && G * m > 256))
+            return fail(h, REVSIM_ERR_BADARG, "unsupported launch shape");
+        sh.G = G;
+        sh.U = U;
+        if (m != sh.mpc || !sh.d_blk_rep) {
+            sh.mpc = m;
+            int rc = build_block_table(h, dir);
+            if (rc) return rc;
+        }
     }
     return REVSIM_OK;
 }
 
-int32_t revsim_get_launch_shape(revsim_handle *h, int32_t *lanes, int32_t *mpc, int32_t *unroll) {
-    if (!h) return REVSIM_ERR_BADARG;
-    if (lanes) *lanes = h->G;
-    if (mpc) *mpc = h->mpc;
-    if (unroll) *unroll = h->unroll;
+int32_t revsim_get_launch_shape(revsim_handle *h, int32_t which, int32_t *lanes, int32_t *mpc,
+                                int32_t *unroll) {
+    if (!h || which < 0 || which > 1) return REVSIM_ERR_BADARG;
+    if (lanes) *lanes = h->shp[which].G;
+    if (mpc) *mpc = h->shp[which].mpc;
+    if (unroll) *unroll = h->shp[which].U;
     return REVSIM_OK;
 }
 
-// Project autotuner: times the forward and reverse step kernels (forces-only mode, on
-// the current state) for every allowed (lanes per molecule, molecules per CTA, unroll)
-// and keeps the fastest combined time.
+// Project autotuner: times the reverse and the forward step kernel separately
+// (forces-only mode, on the current state) for every allowed (lanes per molecule,
+// molecules per CTA, entries per iteration) and keeps the fastest shape of each.
 int32_t revsim_autotune(revsim_handle *h, double dt) {
     int rc = check_ready(h);
     if (rc) return rc;
     if ((rc = build_nlist_checked(h, h->d_x))) return rc;
     if ((rc = pack(h, 0, true))) return rc;
-    double best = std::numeric_limits<double>::infinity();
-    int bg = h->G, bm = h->mpc, bu = h->unroll;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    for (int G : {8, 16, 32}) {
-        for (int threads : {64, 128, 256, 512}) {
-            if (threads < G || threads % G) continue;
-            for (int U : {1, 2}) {
-                if ((rc = revsim_set_launch_shape(h, G, threads / G, U))) break;
-                StepArgs a = base_args(h);
-                a.pos_in = h->d_pos[0];
-                a.wgt_in = h->d_wgt[0];
-                a.F_out = h->d_F;
-                a.acoefO = dt * dt / (2 * h->mO);
-                a.acoefH = dt * dt / (2 * h->mH);
-                a.mode = MODE_FORCES_ONLY;
-                for (int it = 0; it < 2 && !rc; it++)
-                    if ((rc = launch_step_k(h, false, a)) == 0) rc = launch_step_k(h, true, a);
-                if (rc) break;
-                CK(cudaEventRecord(e0, h->st));
-                for (int it = 0; it < 8 && !rc; it++)
-                    if ((rc = launch_step_k(h, false, a)) == 0) rc = launch_step_k(h, true, a);
-                if (rc) break;
-                CK(cudaEventRecord(e1, h->st));
-                CK(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                CK(cudaEventElapsedTime(&ms, e0, e1));
-                if (ms < best) {
-                    best = ms;
-                    bg = G;
-                    bm = threads / G;
-                    bu = U;
+    for (int dir = 0; dir < 2 && !rc; dir++) {
+        const bool rev = dir == 0;
+        double best = std::numeric_limits<double>::infinity();
+        int bg = h->shp[dir].G, bm = h->shp[dir].mpc, bu = h->shp[dir].U;
+        for (int G : {8, 16, 32}) {
+            for (int threads : {64, 128, 256, 512}) {
+                if (threads < G || threads % G) continue;
+                for (int U : {1, 2, 3}) {
+                    if (U == 3 && threads > 256) continue;
+                    if ((rc = revsim_set_launch_shape(h, dir, G, threads / G, U))) break;
+                    StepArgs a = base_args(h, rev);
+                    a.pos_in = h->d_pos[0];
+                    a.wgt_in = h->d_wgt[0];
+                    a.F_out = h->d_F;
+                    a.acoefO = dt * dt / (2 * h->mO);
+                    a.acoefH = dt * dt / (2 * h->mH);
+                    a.mode = MODE_FORCES_ONLY;
+                    for (int it = 0; it < 2 && !rc; it++) rc = launch_step_k(h, rev, a);
+                    if (rc) break;
+                    CK(cudaEventRecord(e0, h->st));
+                    for (int it = 0; it < 10 && !rc; it++) rc = launch_step_k(h, rev, a);
+                    if (rc) break;
+                    CK(cudaEventRecord(e1, h->st));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    if (ms < best) {
+                        best = ms;
+                        bg = G;
+                        bm = threads / G;
+                        bu = U;
+                    }
                 }
+                if (rc) break;
             }
             if (rc) break;
         }
-        if (rc) break;
+        if (!rc) rc = revsim_set_launch_shape(h, dir, bg, bm, bu);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    int rc2 = revsim_set_launch_shape(h, bg, bm, bu);
-    return rc ? rc : rc2;
+    return rc;
 }
 
 }  // extern "C"

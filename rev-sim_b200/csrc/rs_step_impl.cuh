@@ -304,8 +304,13 @@ __device__ __forceinline__ void pair_row(uint32_t mask, const typename V4T<R>::T
 #undef RS_SLOT
 }
 
+// U = 1: one neighbour entry per lane per iteration; 2: two entries, all loads issued
+// first; 3: one entry, with the next entry's index and coordinates loaded while the
+// current one is computed (software pipelining; launched with at most 256 threads so
+// the compiler may use more registers).
 template <typename R, int FORM, int G, bool REV, bool SHIFT, int U>
-__global__ void __launch_bounds__(512) k_water_step(StepArgs a, NbConsts<R> nb, BondConsts bc) {
+__global__ void __launch_bounds__(U == 3 ? 256 : 512) k_water_step(StepArgs a, NbConsts<R> nb,
+                                                                   BondConsts bc) {
     using V4 = typename V4T<R>::T;
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int NTH = NF + 1;
@@ -379,39 +384,61 @@ __global__ void __launch_bounds__(512) k_water_step(StepArgs a, NbConsts<R> nb, 
         const uint32_t *__restrict__ row = a.nbr + (size_t)I * a.cap;
         const int cnt = min(a.nbr_cnt[I], a.cap);
         const R hL = xmul(L, R(0.5));
-        for (int e0 = lane; e0 < cnt; e0 += U * G) {
-            // U entries per lane per iteration: all their loads are issued first.
-            uint32_t ent[U];
-#pragma unroll
-            for (int q = 0; q < U; q++) {
-                const int e = e0 + q * G;
-                ent[q] = e < cnt ? __ldg(row + e) : 0u;   // padding: molecule 0, empty mask
+        // one neighbour entry: displacement image and the nine slots
+        auto entry = [&](uint32_t ent, const V4 pbq[3], const V4 wbq[3]) {
+            const uint32_t mask = ent >> 23;
+            R sh[3] = {R(0), R(0), R(0)};
+            if (SHIFT) {
+                sh[0] = image_shift<R, SHIFT>(xsub(pbq[0].x, pa[0].x), L, hL);
+                sh[1] = image_shift<R, SHIFT>(xsub(pbq[0].y, pa[0].y), L, hL);
+                sh[2] = image_shift<R, SHIFT>(xsub(pbq[0].z, pa[0].z), L, hL);
             }
-            V4 pb[U][3], wb[U][3];
+            pair_row<R, FORM, REV, SHIFT, 0>(mask, pa[0], pbq, wa[0], wbq, ca[0], sh, L, invL, nb, f[0],
+                                             g[0], th);
+            pair_row<R, FORM, REV, SHIFT, 1>(mask, pa[1], pbq, wa[1], wbq, ca[1], sh, L, invL, nb, f[1],
+                                             g[1], th);
+            pair_row<R, FORM, REV, SHIFT, 2>(mask, pa[2], pbq, wa[2], wbq, ca[2], sh, L, invL, nb, f[2],
+                                             g[2], th);
+        };
+        auto fetch = [&](uint32_t ent, V4 pbq[3], V4 wbq[3]) {
+            const int J = (int)(ent & 0x7FFFFFu);
 #pragma unroll
-            for (int q = 0; q < U; q++) {
-                const int J = (int)(ent[q] & 0x7FFFFFu);
+            for (int k = 0; k < 3; k++) {
+                pbq[k] = pos[3 * J + k];
+                if (REV) wbq[k] = wgt[3 * J + k];
+            }
+        };
+        if (U == 3) {
+            // padding entries (past the row end) read molecule 0 with an empty mask
+            uint32_t ent_n = lane < cnt ? __ldg(row + lane) : 0u;
+            V4 pbn[3], wbn[3];
+            fetch(ent_n, pbn, wbn);
+            for (int e = lane; e < cnt; e += G) {
+                const uint32_t ent = ent_n;
+                V4 pbq[3], wbq[3];
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    pb[q][k] = pos[3 * J + k];
-                    if (REV) wb[q][k] = wgt[3 * J + k];
+                    pbq[k] = pbn[k];
+                    if (REV) wbq[k] = wbn[k];
                 }
+                ent_n = e + G < cnt ? __ldg(row + e + G) : 0u;
+                if (e + G < cnt) fetch(ent_n, pbn, wbn);
+                entry(ent, pbq, wbq);
             }
+        } else {
+            for (int e0 = lane; e0 < cnt; e0 += U * G) {
+                // U entries per lane per iteration: all their loads are issued first.
+                uint32_t ent[U == 3 ? 1 : U];
 #pragma unroll
-            for (int q = 0; q < U; q++) {
-                const uint32_t mask = ent[q] >> 23;
-                R sh[3] = {R(0), R(0), R(0)};
-                if (SHIFT) {
-                    sh[0] = image_shift<R, SHIFT>(xsub(pb[q][0].x, pa[0].x), L, hL);
-                    sh[1] = image_shift<R, SHIFT>(xsub(pb[q][0].y, pa[0].y), L, hL);
-                    sh[2] = image_shift<R, SHIFT>(xsub(pb[q][0].z, pa[0].z), L, hL);
+                for (int q = 0; q < U; q++) {
+                    const int e = e0 + q * G;
+                    ent[q] = e < cnt ? __ldg(row + e) : 0u;   // padding: molecule 0, empty mask
                 }
-                pair_row<R, FORM, REV, SHIFT, 0>(mask, pa[0], pb[q], wa[0], wb[q], ca[0], sh, L, invL, nb,
-                                                 f[0], g[0], th);
-                pair_row<R, FORM, REV, SHIFT, 1>(mask, pa[1], pb[q], wa[1], wb[q], ca[1], sh, L, invL, nb,
-                                                 f[1], g[1], th);
-                pair_row<R, FORM, REV, SHIFT, 2>(mask, pa[2], pb[q], wa[2], wb[q], ca[2], sh, L, invL, nb,
-                                                 f[2], g[2], th);
+                V4 pb[U == 3 ? 1 : U][3], wb[U == 3 ? 1 : U][3];
+#pragma unroll
+                for (int q = 0; q < U; q++) fetch(ent[q], pb[q], wb[q]);
+#pragma unroll
+                for (int q = 0; q < U; q++) entry(ent[q], pb[q], wb[q]);
             }
         }
     }
@@ -588,14 +615,24 @@ cudaError_t launch_one(bool rev, int n_blk, int threads, const StepArgs &a, cons
     return cudaGetLastError();
 }
 
+template <typename R, int FORM, int G, bool SHIFT>
+cudaError_t launch_u(bool rev, int unroll, int n_blk, int threads, const StepArgs &a,
+                     const NbConsts<R> &nb, const BondConsts &bc, cudaStream_t st) {
+    switch (unroll) {
+        case 1: return launch_one<R, FORM, G, SHIFT, 1>(rev, n_blk, threads, a, nb, bc, st);
+        case 2: return launch_one<R, FORM, G, SHIFT, 2>(rev, n_blk, threads, a, nb, bc, st);
+        case 3:
+            if (threads > 256) return cudaErrorInvalidValue;
+            return launch_one<R, FORM, G, SHIFT, 3>(rev, n_blk, threads, a, nb, bc, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
 template <typename R, int FORM, int G>
 cudaError_t launch_g(bool rev, bool shift, int unroll, int n_blk, int threads, const StepArgs &a,
                      const NbConsts<R> &nb, const BondConsts &bc, cudaStream_t st) {
-    if (shift)
-        return unroll == 2 ? launch_one<R, FORM, G, true, 2>(rev, n_blk, threads, a, nb, bc, st)
-                           : launch_one<R, FORM, G, true, 1>(rev, n_blk, threads, a, nb, bc, st);
-    return unroll == 2 ? launch_one<R, FORM, G, false, 2>(rev, n_blk, threads, a, nb, bc, st)
-                       : launch_one<R, FORM, G, false, 1>(rev, n_blk, threads, a, nb, bc, st);
+    if (shift) return launch_u<R, FORM, G, true>(rev, unroll, n_blk, threads, a, nb, bc, st);
+    return launch_u<R, FORM, G, false>(rev, unroll, n_blk, threads, a, nb, bc, st);
 }
 
 }  // namespace

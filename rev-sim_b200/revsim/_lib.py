@@ -111,8 +111,8 @@ def load(path=LIB_PATH):
         "revsim_launch_count": (i64, [vp]),
         "revsim_set_kernel_timing": (i32, [vp, i32]),
         "revsim_kernel_time": (i32, [vp, i32, pd, pi64]),
-        "revsim_set_launch_shape": (i32, [vp, i32, i32, i32]),
-        "revsim_get_launch_shape": (i32, [vp, pi32, pi32, pi32]),
+        "revsim_set_launch_shape": (i32, [vp, i32, i32, i32, i32]),
+        "revsim_get_launch_shape": (i32, [vp, i32, pi32, pi32, pi32]),
         "revsim_autotune": (i32, [vp, d]),
         "revsim_probe_fp32_tflops": (i32, [i32, pd]),
         "revsim_rdf_loss_grad_noalloc": (i32, [vp, i32, d, P(RdfTermC), vp, vp, vp, vp]),

@@ -217,15 +217,17 @@ class Engine:
         self._check(self._L.revsim_kernel_time(self._h, which, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
 
-    def set_launch_shape(self, lanes=0, mols_per_cta=0, unroll=0):
-        self._check(self._L.revsim_set_launch_shape(self._h, lanes, mols_per_cta, unroll))
+    def set_launch_shape(self, lanes=0, mols_per_cta=0, unroll=0, which=-1):
+        """which: 0 reverse step, 1 forward step, -1 both."""
+        self._check(self._L.revsim_set_launch_shape(self._h, which, lanes, mols_per_cta, unroll))
 
-    def launch_shape(self):
+    def launch_shape(self, which=0):
         g, m, u = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        self._check(self._L.revsim_get_launch_shape(self._h, ctypes.byref(g), ctypes.byref(m),
+        self._check(self._L.revsim_get_launch_shape(self._h, which, ctypes.byref(g), ctypes.byref(m),
                                                     ctypes.byref(u)))
         return g.value, m.value, u.value
 
     def autotune(self, dt=0.001):
+        """Returns the chosen (lanes, molecules per CTA, unroll) of the reverse and forward kernels."""
         self._check(self._L.revsim_autotune(self._h, dt))
-        return self.launch_shape()
+        return self.launch_shape(0), self.launch_shape(1)
