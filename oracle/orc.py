@@ -40,10 +40,19 @@ class OrcLoss(ctypes.Structure):
     _fields_ = [("n_terms", _I32), ("terms", ctypes.POINTER(OrcRdfTerm))]
 
 
+class OrcSwSystem(ctypes.Structure):
+    _fields_ = [("n_atoms", _I32), ("box", _D), ("mass", _D), ("kB", _D), ("temp", _D)]
+
+
+class OrcSwLoss(ctypes.Structure):
+    _fields_ = [("weight", _D), ("target", _D * 9), ("vel_term", _I32)]
+
+
 def build(force=False):
     """Compile the oracle with its Makefile (gcc, OpenMP, no FMA contraction)."""
-    if force or not os.path.exists(_LIB_PATH) or (
-            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "revsim_oracle.c"))):
+    srcs = ["revsim_oracle.c", "revsim_oracle.h", "sw_oracle.c", "sw_oracle.h"]
+    if force or not os.path.exists(_LIB_PATH) or any(
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, f)) for f in srcs):
         subprocess.run(["make", "-s", "-C", _HERE, "-B" if force else "liborc_revsim.so"],
                        check=True)
     return _LIB_PATH
@@ -77,6 +86,21 @@ def lib():
         L.orc_set_num_threads.argtypes = [_I32]
         L.orc_vec1d.restype = _D
         L.orc_vec1d.argtypes = [_D, _D, _D]
+        PS, PL = ctypes.POINTER(OrcSwSystem), ctypes.POINTER(OrcSwLoss)
+        L.orc_sw_energy.restype = _D
+        L.orc_sw_energy.argtypes = [PS, _PD, _PD]
+        L.orc_sw_forces.argtypes = [PS, _PD, _PD, _PD]
+        L.orc_sw_forces_grads.argtypes = [PS, _PD, _PD, _PD, _PD, _PD, _PD]
+        L.orc_sw_stress.argtypes = [PS, _PD, _PD, _PD, _I32, _PD]
+        L.orc_sw_loss_grad.restype = _D
+        L.orc_sw_loss_grad.argtypes = [PS, _PD, PL, _PD, _PD, _PD, _PD, _PD]
+        L.orc_sw_noise.argtypes = [PS, ctypes.c_uint64, _PD]
+        L.orc_sw_forward_sim.restype = _D
+        L.orc_sw_forward_sim.argtypes = [PS, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _I32, _D, PL,
+                                         _I32, _PD, _PD]
+        L.orc_sw_reverse_sim.restype = _D
+        L.orc_sw_reverse_sim.argtypes = [PS, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _I32, _I32, _D,
+                                         _PD, _PD, PL, _PD]
         _lib = L
     return _lib
 
@@ -228,3 +252,90 @@ def set_threads(n):
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+# --------------------------------------------------------------------------------------
+# Stillinger-Weber diamond path (sw_oracle.c)
+
+SW_NP = 7
+
+
+def make_sw_system(n_atoms, box, temp=298.0, *, mass=12.011, kB=0.00831446261815324):
+    return OrcSwSystem(n_atoms, box, mass, kB, temp)
+
+
+def make_sw_loss(weight=5e-8, target=None, vel_term=True):
+    t = np.zeros(9) if target is None else np.asarray(target, dtype=np.float64).reshape(9)
+    return OrcSwLoss(weight, (_D * 9)(*t), 1 if vel_term else 0)
+
+
+def sw_energy(s, theta, x):
+    return lib().orc_sw_energy(ctypes.byref(s), _pd(_f64(theta)), _pd(_f64(x)))
+
+
+def sw_forces(s, theta, x):
+    x = _f64(x)
+    F = np.zeros(x.size)
+    lib().orc_sw_forces(ctypes.byref(s), _pd(_f64(theta)), _pd(x), _pd(F))
+    return F.reshape(-1, 3)
+
+
+def sw_forces_grads(s, theta, x, w, jac=True):
+    x, w = _f64(x), _f64(w)
+    F, G = np.zeros(x.size), np.zeros(x.size)
+    J = np.zeros(x.size * SW_NP) if jac else None
+    lib().orc_sw_forces_grads(ctypes.byref(s), _pd(_f64(theta)), _pd(x), _pd(w), _pd(F), _pd(G),
+                              _pd(J) if jac else None)
+    return F.reshape(-1, 3), G.reshape(-1, 3), (J.reshape(-1, SW_NP) if jac else None)
+
+
+def sw_stress(s, theta, x, v, vel_term=True):
+    sig = np.zeros(9)
+    lib().orc_sw_stress(ctypes.byref(s), _pd(_f64(theta)), _pd(_f64(x)), _pd(_f64(v)),
+                        1 if vel_term else 0, _pd(sig))
+    return sig.reshape(3, 3)
+
+
+def sw_loss_grad(s, theta, loss, x, v):
+    x, v = _f64(x), _f64(v)
+    gx, gv, gp = np.zeros(x.size), np.zeros(x.size), np.zeros(SW_NP)
+    val = lib().orc_sw_loss_grad(ctypes.byref(s), _pd(_f64(theta)), ctypes.byref(loss), _pd(x),
+                                 _pd(v), _pd(gx), _pd(gv), _pd(gp))
+    return val, gx.reshape(-1, 3), gv.reshape(-1, 3), gp
+
+
+def sw_noise(s, seed):
+    xi = np.zeros(3 * s.n_atoms)
+    lib().orc_sw_noise(ctypes.byref(s), ctypes.c_uint64(int(seed)), _pd(xi))
+    return xi.reshape(-1, 3)
+
+
+def sw_forward_sim(s, theta, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss=None,
+                   n_steps_buffer=0, calc_loss=True):
+    """Forward pass; returns (x, v, loss, snap_x, snap_v) with one snapshot per loss point."""
+    x, v = _f64(x).copy(), _f64(v).copy()
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    n_pts = sum(1 for k in range(1, n_steps + 1)
+                if (n_steps - k) % n_steps_loss == 0 and k >= n_steps_buffer)
+    sx = np.zeros((max(n_pts, 1), x.size))
+    sv = np.zeros((max(n_pts, 1), x.size))
+    val = lib().orc_sw_forward_sim(ctypes.byref(s), _pd(_f64(theta)), _pd(x), _pd(v),
+                                   seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss,
+                                   n_steps_buffer, dt,
+                                   ctypes.byref(loss) if loss is not None else None,
+                                   1 if (calc_loss and loss is not None) else 0, _pd(sx), _pd(sv))
+    return x.reshape(-1, 3), v.reshape(-1, 3), val, sx[:n_pts], sv[:n_pts]
+
+
+def sw_reverse_sim(s, theta, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
+                   snaps_x, snaps_v, loss):
+    """Reverse pass over the forward pass's loss points; returns (x, v, loss, dL/dtheta)."""
+    x, v = _f64(x).copy(), _f64(v).copy()
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    sx, sv = _f64(snaps_x), _f64(snaps_v)
+    g = np.zeros(SW_NP)
+    val = lib().orc_sw_reverse_sim(ctypes.byref(s), _pd(_f64(theta)), _pd(x), _pd(v),
+                                   seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss,
+                                   n_steps_trunc, len(sx), dt, _pd(sx), _pd(sv),
+                                   ctypes.byref(loss), _pd(g))
+    return x.reshape(-1, 3), v.reshape(-1, 3), val, g

@@ -655,6 +655,11 @@ static void normals2(uint64_t seed, uint32_t atom, uint32_t blk, double z[2]) {
     z[1] = rr * sin(2.0 * ORC_PI * u2);
 }
 
+void orc_philox_normals(uint64_t seed, uint32_t atom, double z[4]) {
+    normals2(seed, atom, 0u, z);
+    normals2(seed, atom, 1u, z + 2);
+}
+
 void orc_noise(const orc_system *s, uint64_t seed, double temp, double *xi) {
     const int64_t n = 3 * (int64_t)s->n_mol;
     for (int64_t a = 0; a < n; a++) {

@@ -104,6 +104,8 @@ double orc_energy(const orc_system *s, const double *params, const double *x,
 /* Per-step Langevin noise: xi[3a+u] = sqrt(kB T / m_a) * z, z ~ N(0,1) from
  * Philox4x32-10 keyed by the 64-bit step seed, counter (a, 0/1, 0, 0), Box-Muller. */
 void orc_noise(const orc_system *s, uint64_t seed, double temp, double *xi);
+/* Four N(0,1) draws for (seed, atom): Philox blocks 0 and 1 (the per-atom draw of orc_noise). */
+void orc_philox_normals(uint64_t seed, uint32_t atom, double z[4]);
 
 /* RDF histogram of one term at positions x: writes h[n_grid]. */
 void orc_rdf(const orc_system *s, const orc_rdf_term *t, const double *x, double *h);
