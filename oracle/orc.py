@@ -90,6 +90,8 @@ def lib():
         L.orc_sw_energy.restype = _D
         L.orc_sw_energy.argtypes = [PS, _PD, _PD]
         L.orc_sw_forces.argtypes = [PS, _PD, _PD, _PD]
+        L.orc_sw_pairs.restype = _I64
+        L.orc_sw_pairs.argtypes = [PS, _PD, _PD, _PI32, _I64]
         L.orc_sw_forces_grads.argtypes = [PS, _PD, _PD, _PD, _PD, _PD, _PD]
         L.orc_sw_stress.argtypes = [PS, _PD, _PD, _PD, _I32, _PD]
         L.orc_sw_loss_grad.restype = _D
@@ -271,6 +273,15 @@ def make_sw_loss(weight=5e-8, target=None, vel_term=True):
 
 def sw_energy(s, theta, x):
     return lib().orc_sw_energy(ctypes.byref(s), _pd(_f64(theta)), _pd(_f64(x)))
+
+
+def sw_pairs(s, theta, x):
+    """[n, 2] pairs i < j with r / sigma < a, ascending."""
+    x = _f64(x)
+    cap = 64 * s.n_atoms
+    out = np.zeros((cap, 2), dtype=np.int32)
+    n = lib().orc_sw_pairs(ctypes.byref(s), _pd(_f64(theta)), _pd(x), out.ctypes.data_as(_PI32), cap)
+    return out[:min(n, cap)].copy()
 
 
 def sw_forces(s, theta, x):

@@ -219,6 +219,25 @@ double orc_sw_energy(const orc_sw_system *s, const double *theta, const double *
     return E;
 }
 
+int64_t orc_sw_pairs(const orc_sw_system *s, const double *theta, const double *x,
+                     int32_t *pairs, int64_t max_pairs) {
+    nbrs nb;
+    build_nbrs(s, theta, x, &nb);
+    int64_t n = 0;
+    for (int i = 0; i < nb.n; i++)
+        for (int q = 0; q < nb.cnt[i]; q++) {
+            const int j = nb.idx[i * nb.cap + q];
+            if (j <= i) continue;
+            if (n < max_pairs) {
+                pairs[2 * n] = i;
+                pairs[2 * n + 1] = j;
+            }
+            n++;
+        }
+    free_nbrs(&nb);
+    return n;
+}
+
 void orc_sw_forces(const orc_sw_system *s, const double *theta, const double *x, double *F) {
     orc_sw_forces_grads(s, theta, x, NULL, F, NULL, NULL);
 }

@@ -41,6 +41,9 @@ typedef struct {
 } orc_sw_loss;
 
 double orc_sw_energy(const orc_sw_system *s, const double *theta, const double *x);
+/* Pairs i < j with r / sigma < a (the 2-body terms), ascending; returns the count. */
+int64_t orc_sw_pairs(const orc_sw_system *s, const double *theta, const double *x,
+                     int32_t *pairs, int64_t max_pairs);
 void orc_sw_forces(const orc_sw_system *s, const double *theta, const double *x, double *F);
 /* F, dl_dfi[b] = sum_a (w_a/m) . dF_a/dx_b, dF_dp [3N * 7] (may be NULL). */
 void orc_sw_forces_grads(const orc_sw_system *s, const double *theta, const double *x,

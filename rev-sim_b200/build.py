@@ -19,7 +19,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 # library lives in-tree).
 BUILD = os.path.join(tempfile.gettempdir(), "revsim_build_" + hashlib.sha1(HERE.encode()).hexdigest()[:10])
 LIB = os.path.join(HERE, "librevsim.so")
-SOURCES = ["rs_api.cu", "rs_step.cu", "rs_nlist.cu", "rs_loss.cu", "rs_probe.cu"] + [
+SOURCES = ["rs_api.cu", "rs_step.cu", "rs_nlist.cu", "rs_loss.cu", "rs_probe.cu", "sw_kernels.cu",
+           "sw_api.cu"] + [
     f"rs_step_{p}_{f}.cu" for p in "fd" for f in ("lj", "dexp", "buck", "ljsc", "buff")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -29,7 +30,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE,
 
 def _deps():
     files = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    files.append(os.path.join(INCLUDE, "revsim.h"))
+    files += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
     return max(os.path.getmtime(f) for f in files)
 
 

@@ -1,0 +1,834 @@
+// sw_kernels.cu -- Stillinger-Weber diamond kernels (sm_100a): candidate-list build,
+// per-centre terms with forward-mode tangents, deterministic gather + integrators,
+// stress reductions.  Follows diamond/diamond.jl: SW terms 348-381 and 444-532, the
+// Enzyme VJP and parameter pullback of sw_force_and_grads! 1658-1697, the stress
+// tensor and loss 753-786, the forward step 1462-1467 and the reverse step 1801-1846.
+// The decomposition into per-centre slot gradients is described in sw_internal.h.
+#include "sw_internal.h"
+
+namespace rs {
+namespace sw {
+
+namespace {
+
+// ------------------------------------------------------------------ duals
+// Forward-mode dual with K tangents (K = 0: a plain value).  Tangent 0 is the
+// position direction (w or S d), tangents 1..3 are a, gamma, sigma.  Every value
+// operation is the same rounding intrinsic whatever K is, so value parts are
+// bit-identical between the forward (K = 0) and reverse (K = 4) kernels.
+template <typename R, int K>
+struct SD {
+    R v;
+    R d[K > 0 ? K : 1];
+};
+
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> sdc(R v) {
+    SD<R, K> r;
+    r.v = v;
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = R(0);
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> operator+(const SD<R, K> &a, const SD<R, K> &b) {
+    SD<R, K> r;
+    r.v = xadd(a.v, b.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xadd(a.d[k], b.d[k]);
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> operator-(const SD<R, K> &a, const SD<R, K> &b) {
+    SD<R, K> r;
+    r.v = xsub(a.v, b.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xsub(a.d[k], b.d[k]);
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> operator*(const SD<R, K> &a, const SD<R, K> &b) {
+    SD<R, K> r;
+    r.v = xmul(a.v, b.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xfma(a.d[k], b.v, xmul(a.v, b.d[k]));
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> operator*(R a, const SD<R, K> &b) {
+    SD<R, K> r;
+    r.v = xmul(a, b.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xmul(a, b.d[k]);
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> operator/(const SD<R, K> &a, const SD<R, K> &b) {
+    SD<R, K> r;
+    r.v = xdiv(a.v, b.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xdiv(xsub(a.d[k], xmul(r.v, b.d[k])), b.v);
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> sd_exp(const SD<R, K> &a) {
+    SD<R, K> r;
+    r.v = xexp(a.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xmul(r.v, a.d[k]);
+    return r;
+}
+template <typename R, int K>
+__device__ __forceinline__ SD<R, K> sd_neg(const SD<R, K> &a) {
+    SD<R, K> r;
+    r.v = -a.v;
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = -a.d[k];
+    return r;
+}
+
+__device__ __forceinline__ double dist2(const double *xa, const double *xb, double L, double d[3]) {
+    d[0] = vec1d(xa[0], xb[0], L);
+    d[1] = vec1d(xa[1], xb[1], L);
+    d[2] = vec1d(xa[2], xb[2], L);
+    return __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2]));
+}
+
+// Sum NV per-thread doubles over the CTA in a fixed order; thread k < NV then adds (or
+// writes) the total to out[k].
+template <int NV>
+__device__ __forceinline__ void cta_sum(double (*s_red)[9], const double *val, double *out,
+                                        bool accumulate) {
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        v[k] = val[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] = __dadd_rn(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    }
+    const int warp = threadIdx.x / 32, nw = blockDim.x / 32;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) s_red[warp][k] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double t = 0.0;
+        for (int w = 0; w < nw; w++) t = __dadd_rn(t, s_red[w][threadIdx.x]);
+        out[threadIdx.x] = accumulate ? __dadd_rn(out[threadIdx.x], t) : t;
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ candidate list
+__global__ void k_cell_count(SwNlArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.N) return;
+    const int r = a.atom_rep[e];
+    const int nc = a.rep_nc[r];
+    const double L = a.rep_box[r];
+    int ci[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const double xu = a.x[3 * (size_t)e + u];
+        a.x_nl[3 * (size_t)e + u] = xu;
+        int cc = (int)floor(xu / L * nc);
+        ci[u] = cc < 0 ? 0 : (cc >= nc ? nc - 1 : cc);
+    }
+    const int cell = a.rep_cell_off[r] + (ci[2] * nc + ci[1]) * nc + ci[0];
+    a.cell_of[e] = cell;
+    atomicAdd(a.cell_cnt + cell, 1);
+}
+
+__global__ void k_cell_scan(SwNlArgs a) {
+    __shared__ int s_part[1024];
+    __shared__ int s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < a.n_cells; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < a.n_cells ? a.cell_cnt[i] : 0;
+        s_part[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < blockDim.x; off <<= 1) {
+            const int t = threadIdx.x >= off ? s_part[threadIdx.x - off] : 0;
+            __syncthreads();
+            s_part[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < a.n_cells) {
+            a.cell_start[i] = s_carry + s_part[threadIdx.x] - v;
+            a.cell_fill[i] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry += s_part[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void k_cell_fill(SwNlArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.N) return;
+    const int c = a.cell_of[e];
+    a.cell_atoms[a.cell_start[c] + atomicAdd(a.cell_fill + c, 1)] = e;
+}
+
+// Candidate row of atom e: every other atom of its replica within a sigma + skin (FP64
+// minimum-image distance), ascending index.  Cells are at least that wide and number at
+// least 3 per side, so the 27 cells around e are distinct and hold every candidate.
+__global__ void k_rows(SwNlArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.N) return;
+    const int r = a.atom_rep[e];
+    const int nc = a.rep_nc[r], off = a.rep_cell_off[r];
+    const double L = a.rep_box[r];
+    const int loc = a.cell_of[e] - off;
+    const int cx = loc % nc, cy = (loc / nc) % nc, cz = loc / (nc * nc);
+    const double *xe = a.x + 3 * (size_t)e;
+    int row[CAND];
+    int cnt = 0;
+    for (int dz = -1; dz <= 1; dz++) {
+        const int z = (cz + dz + nc) % nc;
+        for (int dy = -1; dy <= 1; dy++) {
+            const int y = (cy + dy + nc) % nc;
+            for (int dx = -1; dx <= 1; dx++) {
+                const int xx = (cx + dx + nc) % nc;
+                const int cell = off + (z * nc + y) * nc + xx;
+                const int s0 = a.cell_start[cell], s1 = s0 + a.cell_cnt[cell];
+                for (int s = s0; s < s1; s++) {
+                    const int j = a.cell_atoms[s];
+                    if (j == e) continue;
+                    double d[3];
+                    if (dist2(xe, a.x + 3 * (size_t)j, L, d) < a.rl2) {
+                        if (cnt < CAND) {
+                            // insertion into the ascending row
+                            int p = cnt;
+                            while (p > 0 && row[p - 1] > j) {
+                                row[p] = row[p - 1];
+                                p--;
+                            }
+                            row[p] = j;
+                        }
+                        cnt++;
+                    }
+                }
+            }
+        }
+    }
+    if (cnt > CAND) {
+        atomicOr(a.status, ST_NLIST_OVERFLOW);
+        cnt = CAND;
+    }
+    int *out = a.cand + (size_t)e * CAND;
+    for (int k = 0; k < cnt; k++) out[k] = row[k];
+    a.cand_n[e] = cnt;
+    atomicMax(a.max_cnt, cnt);
+}
+
+// ------------------------------------------------------------------ terms
+// One group of G lanes per centre c.  Phase 1: the candidates are tested in FP64
+// (r / sigma < a, as diamond.jl:351) and the active ones compacted into slots in
+// ascending index order.  Phase 2: lane q prepares slot q (unit vector, 3-body radial
+// factor h = exp(gamma / (s - a)), its derivative factors, the 2-body radial
+// derivative).  Phase 3: lane q sums over the other slots q' the 3-body gradient with
+// respect to d_q; with u = d / r, cos = u_q . u_q', c3 = cos + 1/3,
+//   dE3/dd_q = eps lambda h_q' c3 [ (c3 alpha_q - cos beta_q) u_q + beta_q u_q' ],
+//   alpha_q = dh_q/ds / sigma,  beta_q = 2 h_q / r_q,
+// so T_q = u_q (eps A g2_q / 2 + eps lambda S1) + eps lambda beta_q V with
+// S1 = sum h_q' c3 (c3 alpha_q - cos beta_q), V = sum h_q' c3 u_q'.
+template <typename R, int G, int MODE>
+__global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R> p) {
+    constexpr int K = MODE == TM_VALUE ? 0 : 4;
+    constexpr int GPB = TERM_THREADS / G;
+    using D = SD<R, K>;
+    __shared__ double s_d[GPB][G][3];
+    __shared__ R s_dd[GPB][G][3];
+    __shared__ int s_j[GPB][G];
+    __shared__ D s_u[GPB][G][3];
+    __shared__ D s_h[GPB][G];
+    __shared__ double s_red[TERM_THREADS / 32][9];
+
+    const int lane = threadIdx.x % G, grp = threadIdx.x / G;
+    const int gshift = (threadIdx.x % 32) / G * G;
+    const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
+    const unsigned gmask = gbits << gshift;
+    const int b = blockIdx.x;
+    const int rep = t.blk_rep[b];
+    const bool live = grp < t.blk_n[b];
+    const int c = t.blk_atom0[b] + grp;
+    const double L = t.rep_box[rep];
+
+    double xc[3] = {0.0, 0.0, 0.0}, wc[3] = {0.0, 0.0, 0.0}, ac[3] = {0.0, 0.0, 0.0};
+    int nc = 0;
+    if (live) {
+#pragma unroll
+        for (int u = 0; u < 3; u++) xc[u] = t.x[3 * (size_t)c + u];
+        nc = t.cand_n[c];
+        if (lane == 0) {
+            double d[3];
+            if (dist2(t.x_nl + 3 * (size_t)c, xc, L, d) > t.half_skin2) atomicOr(t.status, ST_SKIN);
+        }
+        if (MODE == TM_REV) {
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                wc[u] = __dmul_rn(t.C[3 * (size_t)c + u], t.inv_m);
+                ac[u] = __dmul_rn(t.A[3 * (size_t)c + u], t.acoef_scale);
+            }
+        }
+    }
+    const double *S = MODE == TM_LOSS ? t.S + 9 * rep : nullptr;
+    const double invV = MODE == TM_LOSS ? 1.0 / t.rep_vol[rep] : 0.0;
+
+    // Phase 1: active slots.
+    int n = 0;
+    for (int k0 = 0; k0 < nc; k0 += G) {
+        const int k = k0 + lane;
+        bool act = false;
+        double d[3] = {0.0, 0.0, 0.0};
+        int j = -1;
+        if (k < nc) {
+            j = t.cand[(size_t)c * CAND + k];
+            const double r2 = dist2(xc, t.x + 3 * (size_t)j, L, d);
+            act = __ddiv_rn(__dsqrt_rn(r2), p.sig64) < p.a64;
+        }
+        const unsigned bal = (__ballot_sync(gmask, act) >> gshift) & gbits;
+        if (act) {
+            const int q = n + __popc(bal & ((1u << lane) - 1u));
+            if (q < G) {
+                s_j[grp][q] = j;
+#pragma unroll
+                for (int u = 0; u < 3; u++) s_d[grp][q][u] = d[u];
+                if (MODE == TM_REV) {
+#pragma unroll
+                    for (int u = 0; u < 3; u++)
+                        s_dd[grp][q][u] = (R)__dsub_rn(__dmul_rn(t.C[3 * (size_t)j + u], t.inv_m), wc[u]);
+                } else if (MODE == TM_LOSS) {
+#pragma unroll
+                    for (int u = 0; u < 3; u++)
+                        s_dd[grp][q][u] = (R)__dadd_rn(__dadd_rn(__dmul_rn(S[3 * u], d[0]),
+                                                                  __dmul_rn(S[3 * u + 1], d[1])),
+                                                       __dmul_rn(S[3 * u + 2], d[2]));
+                }
+            }
+        }
+        n += __popc(bal);
+    }
+    if (n > G) {
+        if (lane == 0) atomicOr(t.status, ST_NLIST_OVERFLOW);
+        n = G;
+    }
+    if (live && lane == 0) {
+        t.act_n[c] = n;
+        atomicMax(t.max_act, n);
+    }
+    __syncwarp(gmask);
+
+    // Phase 2: per-slot quantities.
+    const bool own = lane < n;
+    D u[3], alpha = sdc<R, K>(R(0)), beta = sdc<R, K>(R(0)), g2 = sdc<R, K>(R(0));
+#pragma unroll
+    for (int k = 0; k < 3; k++) u[k] = sdc<R, K>(R(0));
+    R gB = R(0);
+    double d64[3] = {0.0, 0.0, 0.0};
+    if (own) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) d64[k] = s_d[grp][lane][k];
+        t.act_idx[(size_t)c * G + lane] = s_j[grp][lane];
+        const double r64 = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d64[0], d64[0]), __dmul_rn(d64[1], d64[1])),
+                                                __dmul_rn(d64[2], d64[2])));
+        const double s64 = __ddiv_rn(r64, p.sig64);
+        R dd[3] = {R(0), R(0), R(0)};
+        if constexpr (K > 0) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) dd[k] = s_dd[grp][lane][k];
+        }
+        const R r = (R)r64, s = (R)s64, tv = (R)__dsub_rn(s64, p.a64);
+        D rD = sdc<R, K>(r), sig = sdc<R, K>(p.sig), gam = sdc<R, K>(p.gam), sD, tD;
+        D dD[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            dD[k] = sdc<R, K>((R)d64[k]);
+            if constexpr (K > 0) dD[k].d[0] = dd[k];
+        }
+        if constexpr (K > 0) {
+            // r' = d . d' / r along the position tangent; ds/dsigma = -s / sigma; dt/da = -1
+            rD.d[0] = xdiv(xfma(dD[0].v, dd[0], xfma(dD[1].v, dd[1], xmul(dD[2].v, dd[2]))), r);
+            sig.d[3] = R(1);
+            gam.d[2] = R(1);
+        }
+        sD = sdc<R, K>(s);
+        tD = sdc<R, K>(tv);
+        if constexpr (K > 0) {
+            sD.d[0] = xdiv(rD.d[0], p.sig);
+            sD.d[3] = -xdiv(s, p.sig);
+            tD.d[0] = sD.d[0];
+            tD.d[1] = R(-1);
+            tD.d[3] = sD.d[3];
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) u[k] = dD[k] / rD;
+        const D h = sd_exp(gam / tD);
+        const D t2 = tD * tD;
+        alpha = sd_neg((gam * h) / (sig * t2));
+        beta = (R(2) * h) / rD;
+        const D e1 = sd_exp(sdc<R, K>(R(1)) / tD);
+        const D s2 = sD * sD, s4 = s2 * s2;
+        const D is4 = sdc<R, K>(R(1)) / s4;
+        // dE2/dr / (eps A) = e^{1/t} (-4 B s^-5 - (B s^-4 - 1) / t^2) / sigma   (diamond.jl:453)
+        g2 = (e1 * sd_neg((R(4) * p.B) * (is4 / sD) + ((p.B * is4) - sdc<R, K>(R(1))) / t2)) / sig;
+        gB = xdiv(xmul(e1.v, -xadd(xmul(R(4), xdiv(is4.v, sD.v)), xdiv(is4.v, t2.v))), p.sig);
+#pragma unroll
+        for (int k = 0; k < 3; k++) s_u[grp][lane][k] = u[k];
+        s_h[grp][lane] = h;
+    }
+    __syncwarp(gmask);
+
+    // Phase 3: 3-body sums over the other slots.
+    D S1 = sdc<R, K>(R(0)), V[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) V[k] = sdc<R, K>(R(0));
+    if (own) {
+        const R third = R(1) / R(3);
+        for (int q2 = 0; q2 < n; q2++) {
+            if (q2 == lane) continue;
+            const D u2x = s_u[grp][q2][0], u2y = s_u[grp][q2][1], u2z = s_u[grp][q2][2];
+            const D h2 = s_h[grp][q2];
+            const D cs = u[0] * u2x + u[1] * u2y + u[2] * u2z;
+            const D c3 = cs + sdc<R, K>(third);
+            const D w = h2 * c3;
+            S1 = S1 + w * (c3 * alpha - cs * beta);
+            V[0] = V[0] + w * u2x;
+            V[1] = V[1] + w * u2y;
+            V[2] = V[2] + w * u2z;
+        }
+    }
+    D T[3];
+    const D coef = p.half_eA * g2 + p.el * S1;
+    const D elb = p.el * beta;
+#pragma unroll
+    for (int k = 0; k < 3; k++) T[k] = u[k] * coef + elb * V[k];
+    if (own) {
+        R *Tv = (R *)t.Tv;
+        const size_t o = ((size_t)c * G + lane) * 3;
+#pragma unroll
+        for (int k = 0; k < 3; k++) Tv[o + k] = T[k].v;
+        if constexpr (K > 0) {
+            R *Tt = (R *)t.Tt;
+#pragma unroll
+            for (int k = 0; k < 3; k++) Tt[o + k] = T[k].d[0];
+        }
+    }
+
+    // Parameter contraction sum_q z_q . dT_q/dtheta (theta order A, B, a, lambda, gamma,
+    // sigma, eps); the linear parameters from the value parts.
+    if constexpr (MODE != TM_VALUE) {
+      if (t.part) {
+        double con[NP] = {0, 0, 0, 0, 0, 0, 0};
+        if (own) {
+            R z[3];
+            const int j = s_j[grp][lane];
+            if (MODE == TM_REV) {
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    z[k] = (R)__dsub_rn(__dmul_rn(t.A[3 * (size_t)j + k], t.acoef_scale), ac[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    z[k] = (R)__dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(S[3 * k], d64[0]),
+                                                            __dmul_rn(S[3 * k + 1], d64[1])),
+                                                  __dmul_rn(S[3 * k + 2], d64[2])),
+                                        invV);
+            }
+            R zu = R(0), zT3 = R(0), zd[3] = {R(0), R(0), R(0)};
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                zu = xfma(z[k], u[k].v, zu);
+                zT3 = xfma(z[k], xfma(u[k].v, S1.v, xmul(beta.v, V[k].v)), zT3);
+#pragma unroll
+                for (int m = 0; m < 3; m++) zd[m] = xfma(z[k], T[k].d[1 + m], zd[m]);
+            }
+            const double sgn = MODE == TM_REV ? -1.0 : 1.0;
+            const double half_g2zu = 0.5 * (double)g2.v * (double)zu;
+            con[0] = sgn * (double)p.eps * half_g2zu;
+            con[1] = sgn * (double)p.half_eA * (double)gB * (double)zu;
+            con[2] = sgn * (double)zd[0];
+            con[3] = sgn * (double)p.eps * (double)zT3;
+            con[4] = sgn * (double)zd[1];
+            con[5] = sgn * (double)zd[2];
+            con[6] = sgn * ((double)p.A * half_g2zu + (double)p.lam * (double)zT3);
+        }
+        cta_sum<NP>(s_red, con, t.part + (size_t)b * NP, true);
+      }
+    }
+    // Virial sum_q T_q (x) d_q (diamond.jl:757-769, as the strain derivative of the energy).
+    if (t.wpart) {
+        double w9[9];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int bb = 0; bb < 3; bb++) w9[3 * a + bb] = own ? __dmul_rn((double)T[a].v, d64[bb]) : 0.0;
+        cta_sum<9>(s_red, w9, t.wpart + (size_t)b * 9, false);
+    }
+}
+
+// ------------------------------------------------------------------ gather
+__device__ __forceinline__ void part1(const SwGatherArgs &g, int e, int rep, const uint64_t *seeds) {
+    // Un-integration of diamond.jl:1806-1812: x -= v dt/2; v = (v - xi s) / c; x -= v dt/2;
+    // wrap; D = c D + dt^2 dl_dfi (1 + c) / 2; C += D.
+    const double L = g.rep_box[rep];
+    double xi[3] = {0.0, 0.0, 0.0};
+    if (seeds) atom_noise(seeds[rep], (uint32_t)(e - g.rep_atom0[rep]), g.rep_sd[rep], xi);
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const size_t i = 3 * (size_t)e + u;
+        double x = g.x[i], v = g.v[i];
+        x = __dsub_rn(x, __ddiv_rn(__dmul_rn(v, g.dt), 2.0));
+        v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], g.s)), g.c);
+        x = __dsub_rn(x, __ddiv_rn(__dmul_rn(v, g.dt), 2.0));
+        g.x[i] = wrap1d(x, L);
+        g.v[i] = v;
+        const double Dn = __dadd_rn(__dmul_rn(g.c, g.D[i]),
+                                    __ddiv_rn(__dmul_rn(__dmul_rn(g.dt2, g.G[i]), __dadd_rn(1.0, g.c)), 2.0));
+        g.D[i] = Dn;
+        g.C[i] = __dadd_rn(g.C[i], Dn);
+    }
+}
+
+template <typename R, int G, int MODE, bool TAN>
+__global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= g.N) return;
+    const R *Tv = (const R *)g.Tv;
+    const R *Tt = (const R *)g.Tt;
+    const int n = g.act_n[e];
+    double f[3] = {0.0, 0.0, 0.0}, tg[3] = {0.0, 0.0, 0.0};
+    bool ok = true;
+    for (int q = 0; q < n; q++) {
+        const int j = g.act_idx[(size_t)e * G + q];
+        const int nj = g.act_n[j];
+        const int *rj = g.act_idx + (size_t)j * G;
+        int pos = -1;
+        for (int k = 0; k < nj; k++)
+            if (rj[k] == e) {
+                pos = k;
+                break;
+            }
+        if (pos < 0) {
+            ok = false;
+            continue;
+        }
+        const size_t ie = ((size_t)e * G + q) * 3, ij = ((size_t)j * G + pos) * 3;
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            f[u] = __dadd_rn(f[u], __dsub_rn((double)Tv[ij + u], (double)Tv[ie + u]));
+            if (TAN) tg[u] = __dadd_rn(tg[u], __dsub_rn((double)Tt[ij + u], (double)Tt[ie + u]));
+        }
+    }
+    if (!ok) atomicOr(g.status, ST_NLIST_OVERFLOW);
+    const int rep = g.atom_rep[e];
+    // f = dE/dx_e, tg = its derivative along the tangent (H w or H u).
+    if (MODE == GM_FORCES) {
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            g.F[3 * (size_t)e + u] = -f[u];
+            if (TAN && g.G) g.G[3 * (size_t)e + u] = -tg[u];
+        }
+        if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]))) atomicOr(g.status, ST_NAN);
+        return;
+    }
+    if (MODE == GM_FWD) {
+        // diamond.jl:1462-1467
+        const double L = g.rep_box[rep];
+        double xi[3] = {0.0, 0.0, 0.0};
+        if (g.seed_cur) atom_noise(g.seed_cur[rep], (uint32_t)(e - g.rep_atom0[rep]), g.rep_sd[rep], xi);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const size_t i = 3 * (size_t)e + u;
+            const double F = -f[u];
+            double v = __dadd_rn(g.v[i], __ddiv_rn(__dmul_rn(F, g.dt), g.m));
+            double x = __dadd_rn(g.x[i], __ddiv_rn(__dmul_rn(v, g.dt), 2.0));
+            v = __dadd_rn(__dmul_rn(v, g.c), __dmul_rn(xi[u], g.s));
+            x = __dadd_rn(x, __ddiv_rn(__dmul_rn(v, g.dt), 2.0));
+            g.x[i] = wrap1d(x, L);
+            g.v[i] = v;
+        }
+        if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]))) atomicOr(g.status, ST_NAN);
+        return;
+    }
+    if (MODE == GM_REV) {
+        // diamond.jl:1838-1846: v -= F dt / m; B = c B + dt^2 dl_dfi; A += B
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const size_t i = 3 * (size_t)e + u;
+            const double F = -f[u], Gn = -tg[u];
+            g.v[i] = __dsub_rn(g.v[i], __ddiv_rn(__dmul_rn(F, g.dt), g.m));
+            const double Bn = __dadd_rn(__dmul_rn(g.c, g.B[i]), __dmul_rn(g.dt2, Gn));
+            g.B[i] = Bn;
+            g.A[i] = __dadd_rn(g.A[i], Bn);
+            g.G[i] = Gn;
+        }
+        if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]) && isfinite(tg[0]) &&
+              isfinite(tg[1]) && isfinite(tg[2])))
+            atomicOr(g.status, ST_NAN);
+        if (g.fuse_next) part1(g, e, rep, g.seed_next);
+        return;
+    }
+    if (MODE == GM_LOSS) {
+        // dL/dx = (H u + S^T dE/dx) / V,  dL/dv = -(m / V) (S + S^T)(v - vbar)
+        const double *S = g.S + 9 * rep;
+        const double V = g.rep_vol[rep];
+        double gx[3], gv[3];
+#pragma unroll
+        for (int gm = 0; gm < 3; gm++) {
+            double st = 0.0;
+#pragma unroll
+            for (int al = 0; al < 3; al++) st = __dadd_rn(st, __dmul_rn(S[3 * al + gm], f[al]));
+            gx[gm] = __ddiv_rn(__dadd_rn(tg[gm], st), V);
+            double tv = 0.0;
+            if (g.vel_term) {
+#pragma unroll
+                for (int bb = 0; bb < 3; bb++)
+                    tv = __dadd_rn(tv, __dmul_rn(__dadd_rn(S[3 * gm + bb], S[3 * bb + gm]),
+                                                 __dsub_rn(g.v[3 * (size_t)e + bb], g.vbar[3 * rep + bb])));
+            }
+            gv[gm] = g.vel_term ? __ddiv_rn(__dmul_rn(-g.m, tv), V) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const size_t i = 3 * (size_t)e + u;
+            if (g.dLdx) g.dLdx[i] = gx[u];
+            if (g.dLdv) g.dLdv[i] = gv[u];
+            if (g.init_adjoint) {
+                // diamond.jl:1789-1793
+                const double c = g.c, dt = g.dt;
+                g.A[i] = __dadd_rn(__dmul_rn(gx[u], __dadd_rn(1.0, c)), __ddiv_rn(__dmul_rn(__dmul_rn(gv[u], c), 2.0), dt));
+                g.B[i] = __dadd_rn(__dmul_rn(gx[u], __dadd_rn(1.0, c)),
+                                   __ddiv_rn(__dmul_rn(__dmul_rn(gv[u], __dsub_rn(c, 1.0)), 2.0), dt));
+                g.C[i] = __ddiv_rn(__dmul_rn(gv[u], __dadd_rn(1.0, c)), dt);
+                g.D[i] = __dadd_rn(__ddiv_rn(__dmul_rn(gx[u], __dadd_rn(__dadd_rn(1.0, __dmul_rn(2.0, c)), __dmul_rn(c, c))),
+                                             __dmul_rn(2.0, c)),
+                                   __ddiv_rn(__dmul_rn(gv[u], __dsub_rn(c, __ddiv_rn(1.0, c))), dt));
+                g.G[i] = 0.0;
+            }
+        }
+        if (!(isfinite(gx[0]) && isfinite(gx[1]) && isfinite(gx[2]))) atomicOr(g.status, ST_NAN);
+    }
+}
+
+__global__ void k_part1(SwGatherArgs g) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= g.N) return;
+    part1(g, e, g.atom_rep[e], g.seed_cur);
+}
+
+__global__ void k_noise(int N, const int *atom_rep, const int *rep_atom0, const double *rep_sd,
+                        const uint64_t *seeds, double *xi) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= N) return;
+    const int r = atom_rep[e];
+    atom_noise(seeds[r], (uint32_t)(e - rep_atom0[r]), rep_sd[r], xi + 3 * (size_t)e);
+}
+
+// ------------------------------------------------------------- reductions
+template <int NV>
+__device__ __forceinline__ void block_sum256(double (*s)[256], double *v, double *out) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) s[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+#pragma unroll
+            for (int k = 0; k < NV; k++) s[k][threadIdx.x] = __dadd_rn(s[k][threadIdx.x], s[k][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < NV) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(256) k_vsum(SwRedArgs a) {
+    __shared__ double s[3][256];
+    const int b = blockIdx.x;
+    const int i = threadIdx.x;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i < a.ablk_n[b]) {
+        const size_t e = (size_t)a.ablk_atom0[b] + i;
+#pragma unroll
+        for (int u = 0; u < 3; u++) v[u] = a.v[3 * e + u];
+    }
+    block_sum256<3>(s, v, a.vpart + 3 * (size_t)b);
+}
+
+__global__ void k_vbar(SwRedArgs a) {
+    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+        double t[3] = {0.0, 0.0, 0.0};
+        long long n = 0;
+        for (int b = 0; b < a.n_ablk; b++) {
+            if (a.ablk_rep[b] != r) continue;
+            n += a.ablk_n[b];
+#pragma unroll
+            for (int u = 0; u < 3; u++) t[u] = __dadd_rn(t[u], a.vpart[3 * (size_t)b + u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 3; u++) a.vbar[3 * r + u] = __ddiv_rn(t[u], (double)n);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_kin(SwRedArgs a) {
+    __shared__ double s[9][256];
+    const int b = blockIdx.x;
+    const int i = threadIdx.x;
+    double k9[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) k9[k] = 0.0;
+    if (i < a.ablk_n[b]) {
+        const size_t e = (size_t)a.ablk_atom0[b] + i;
+        const int r = a.ablk_rep[b];
+        double dv[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) dv[u] = __dsub_rn(a.v[3 * e + u], a.vbar[3 * r + u]);
+#pragma unroll
+        for (int al = 0; al < 3; al++)
+#pragma unroll
+            for (int be = 0; be < 3; be++) k9[3 * al + be] = __dmul_rn(dv[al], dv[be]);
+    }
+    block_sum256<9>(s, k9, a.kpart + 9 * (size_t)b);
+}
+
+// sigma = (K + W) / V (diamond.jl:753-770); loss = weight sum (sigma - target)^2 / 9
+// (diamond.jl:772-775); S = dL/dsigma.
+__global__ void k_loss_final(SwRedArgs a) {
+    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+        double W[9], Kt[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) W[k] = Kt[k] = 0.0;
+        for (int b = 0; b < a.n_blk; b++) {
+            if (a.blk_rep[b] != r) continue;
+#pragma unroll
+            for (int k = 0; k < 9; k++) W[k] = __dadd_rn(W[k], a.wpart[9 * (size_t)b + k]);
+        }
+        if (a.vel_term) {
+            for (int b = 0; b < a.n_ablk; b++) {
+                if (a.ablk_rep[b] != r) continue;
+#pragma unroll
+                for (int k = 0; k < 9; k++) Kt[k] = __dadd_rn(Kt[k], a.kpart[9 * (size_t)b + k]);
+            }
+        }
+        const double V = a.rep_vol[r];
+        double l = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const double K = a.vel_term ? __dmul_rn(-a.m, Kt[k]) : 0.0;
+            const double sg = __ddiv_rn(__dadd_rn(K, W[k]), V);
+            if (a.sigma) a.sigma[9 * r + k] = sg;
+            const double e = __dsub_rn(sg, a.target[9 * r + k]);
+            l = __dadd_rn(l, __dmul_rn(e, e));
+            if (a.S) a.S[9 * r + k] = __ddiv_rn(__dmul_rn(__dmul_rn(2.0, a.weight), e), 9.0);
+        }
+        l = __dmul_rn(l, __ddiv_rn(a.weight, 9.0));
+        if (a.loss) a.loss[r] = l;
+        if (a.loss_acc) a.loss_acc[r] = __dadd_rn(a.loss_acc[r], l);
+    }
+}
+
+__global__ void k_active_pairs(int N, int G, const int *act_idx, const int *act_n, int32_t *pairs,
+                               unsigned long long *count, long long max_pairs) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= N) return;
+    for (int q = 0; q < act_n[e]; q++) {
+        const int j = act_idx[(size_t)e * G + q];
+        if (j <= e) continue;
+        const unsigned long long k = atomicAdd(count, 1ull);
+        if ((long long)k < max_pairs) {
+            pairs[2 * k] = e;
+            pairs[2 * k + 1] = j;
+        }
+    }
+}
+
+inline int nblk(int n, int t) { return (n + t - 1) / t; }
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+cudaError_t launch_sw_nlist(const SwNlArgs &a, cudaStream_t st) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(a.cell_cnt, 0, sizeof(int) * a.n_cells, st))) return e;
+    k_cell_count<<<nblk(a.N, 256), 256, 0, st>>>(a);
+    k_cell_scan<<<1, 1024, 0, st>>>(a);
+    k_cell_fill<<<nblk(a.N, 256), 256, 0, st>>>(a);
+    k_rows<<<nblk(a.N, 128), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_sw_terms(int mode, int G, int n_blk, const SwTermArgs &a, const SwConsts<R> &p,
+                            cudaStream_t st) {
+#define RS_TERMS(GG, MM) k_terms<R, GG, MM><<<n_blk, TERM_THREADS, 0, st>>>(a, p)
+    if (G == 16) {
+        if (mode == TM_VALUE) RS_TERMS(16, TM_VALUE);
+        else if (mode == TM_REV) RS_TERMS(16, TM_REV);
+        else RS_TERMS(16, TM_LOSS);
+    } else if (G == 32) {
+        if (mode == TM_VALUE) RS_TERMS(32, TM_VALUE);
+        else if (mode == TM_REV) RS_TERMS(32, TM_REV);
+        else RS_TERMS(32, TM_LOSS);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+#undef RS_TERMS
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_sw_gather(int mode, int G, bool tangent, const SwGatherArgs &a, cudaStream_t st) {
+    const int nb = nblk(a.N, 256);
+#define RS_G(GG)                                                                              \
+    do {                                                                                      \
+        if (mode == GM_FORCES && tangent) k_gather<R, GG, GM_FORCES, true><<<nb, 256, 0, st>>>(a);  \
+        else if (mode == GM_FORCES) k_gather<R, GG, GM_FORCES, false><<<nb, 256, 0, st>>>(a); \
+        else if (mode == GM_FWD) k_gather<R, GG, GM_FWD, false><<<nb, 256, 0, st>>>(a);       \
+        else if (mode == GM_REV) k_gather<R, GG, GM_REV, true><<<nb, 256, 0, st>>>(a);        \
+        else k_gather<R, GG, GM_LOSS, true><<<nb, 256, 0, st>>>(a);                           \
+    } while (0)
+    if (G == 16) RS_G(16);
+    else if (G == 32) RS_G(32);
+    else return cudaErrorInvalidValue;
+#undef RS_G
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_stress(const SwRedArgs &a, cudaStream_t st) {
+    k_vsum<<<a.n_ablk, 256, 0, st>>>(a);
+    k_vbar<<<1, 64, 0, st>>>(a);
+    k_kin<<<a.n_ablk, 256, 0, st>>>(a);
+    k_loss_final<<<1, 64, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_part1(int N, const SwGatherArgs &a, cudaStream_t st) {
+    k_part1<<<nblk(N, 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_noise(int N, const int *atom_rep, const int *rep_atom0, const double *rep_sd,
+                            const uint64_t *seeds, double *xi, cudaStream_t st) {
+    k_noise<<<nblk(N, 256), 256, 0, st>>>(N, atom_rep, rep_atom0, rep_sd, seeds, xi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_active_pairs(int N, int G, const int *act_idx, const int *act_n,
+                                   int32_t *pairs, unsigned long long *count, long long max_pairs,
+                                   cudaStream_t st) {
+    k_active_pairs<<<nblk(N, 256), 256, 0, st>>>(N, G, act_idx, act_n, pairs, count, max_pairs);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_sw_terms<float>(int, int, int, const SwTermArgs &, const SwConsts<float> &,
+                                            cudaStream_t);
+template cudaError_t launch_sw_terms<double>(int, int, int, const SwTermArgs &,
+                                             const SwConsts<double> &, cudaStream_t);
+template cudaError_t launch_sw_gather<float>(int, int, bool, const SwGatherArgs &, cudaStream_t);
+template cudaError_t launch_sw_gather<double>(int, int, bool, const SwGatherArgs &, cudaStream_t);
+
+}  // namespace sw
+}  // namespace rs

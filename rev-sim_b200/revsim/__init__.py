@@ -4,17 +4,19 @@ greener-group/rev-sim's flexible-water model.
 The compute runs in librevsim.so (CUDA, C ABI in include/revsim.h); this package
 is the host side: a ctypes binding (``Engine``), the reference's
 ``forward_sim`` / ``reverse_sim`` signatures (``water``), loss builders (``loss``)
-and seeded system generators (``systems``).
+and seeded system generators (``systems``); the Stillinger-Weber diamond engine
+(``SwEngine``, C ABI in include/revsim_sw.h) with the diamond entry points in ``sw``.
 """
 
-from . import constants, systems
-from ._lib import EXPORTS, LIB_PATH, RevsimError, load
+from . import constants, diamond, systems
+from ._lib import EXPORTS, LIB_PATH, SW_EXPORTS, RevsimError, load
 from .engine import Engine, RdfTerm
 from .loss import oo_l2_term, read_rdf_data, reference_rdf_terms
+from .sw import SwEngine
 from .water import SimSystem, forward_sim, reverse_sim
 
 __all__ = [
     "Engine", "RdfTerm", "RevsimError", "SimSystem", "forward_sim", "reverse_sim", "load",
     "constants", "systems", "oo_l2_term", "reference_rdf_terms", "read_rdf_data", "EXPORTS",
-    "LIB_PATH",
+    "LIB_PATH", "SW_EXPORTS", "SwEngine", "diamond",
 ]

@@ -36,6 +36,16 @@ EXPORTS = [
     "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc",
 ]
 
+# Every symbol include/revsim_sw.h declares.
+SW_EXPORTS = [
+    "revsim_sw_create", "revsim_sw_destroy", "revsim_sw_last_error", "revsim_sw_set_params",
+    "revsim_sw_set_state", "revsim_sw_get_state", "revsim_sw_set_loss", "revsim_sw_forces",
+    "revsim_sw_force_vjp", "revsim_sw_stress", "revsim_sw_loss_grad", "revsim_sw_noise",
+    "revsim_sw_active_pairs", "revsim_sw_forward", "revsim_sw_reverse", "revsim_sw_stream",
+    "revsim_sw_launch_count", "revsim_sw_set_kernel_timing", "revsim_sw_kernel_time",
+    "revsim_sw_set_lanes",
+]
+
 
 class RevsimError(RuntimeError):
     def __init__(self, code, msg):
@@ -63,6 +73,26 @@ class SystemDesc(ctypes.Structure):
         ("nl_mode", ctypes.c_int32),
         ("device", ctypes.c_int32),
     ]
+
+
+class SwDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_replicas", ctypes.c_int32),
+        ("n_atoms", ctypes.POINTER(ctypes.c_int32)),
+        ("box", ctypes.POINTER(ctypes.c_double)),
+        ("temp", ctypes.POINTER(ctypes.c_double)),
+        ("precision", ctypes.c_int32),
+        ("mass", ctypes.c_double),
+        ("kB", ctypes.c_double),
+        ("skin", ctypes.c_double),
+        ("n_steps_nf", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class SwLossC(ctypes.Structure):
+    _fields_ = [("weight", ctypes.c_double), ("vel_term", ctypes.c_int32),
+                ("target", ctypes.POINTER(ctypes.c_double))]
 
 
 class RdfTermC(ctypes.Structure):
@@ -116,6 +146,26 @@ def load(path=LIB_PATH):
         "revsim_autotune": (i32, [vp, d]),
         "revsim_probe_fp32_tflops": (i32, [i32, pd]),
         "revsim_rdf_loss_grad_noalloc": (i32, [vp, i32, d, P(RdfTermC), vp, vp, vp, vp]),
+        "revsim_sw_create": (i32, [P(SwDesc), P(vp)]),
+        "revsim_sw_destroy": (None, [vp]),
+        "revsim_sw_last_error": (ctypes.c_char_p, [vp]),
+        "revsim_sw_set_params": (i32, [vp, pd, i32]),
+        "revsim_sw_set_state": (i32, [vp, pd, pd]),
+        "revsim_sw_get_state": (i32, [vp, pd, pd]),
+        "revsim_sw_set_loss": (i32, [vp, P(SwLossC)]),
+        "revsim_sw_forces": (i32, [vp, pd]),
+        "revsim_sw_force_vjp": (i32, [vp, pd, pd, pd, pd, pd]),
+        "revsim_sw_stress": (i32, [vp, i32, pd]),
+        "revsim_sw_loss_grad": (i32, [vp, pd, pd, pd, pd]),
+        "revsim_sw_noise": (i32, [vp, pu64, pd]),
+        "revsim_sw_active_pairs": (i32, [vp, pi32, i64, pi64]),
+        "revsim_sw_forward": (i32, [vp, pu64, d, i32, i32, i32, d, i32, pd, pi32]),
+        "revsim_sw_reverse": (i32, [vp, pu64, d, i32, i32, i32, d, pd, pd]),
+        "revsim_sw_stream": (i32, [vp, P(vp)]),
+        "revsim_sw_launch_count": (i32, [vp, pi64]),
+        "revsim_sw_set_kernel_timing": (i32, [vp, i32]),
+        "revsim_sw_kernel_time": (i32, [vp, i32, pd, pi64]),
+        "revsim_sw_set_lanes": (i32, [vp, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

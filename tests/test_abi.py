@@ -11,10 +11,11 @@ import pytest
 from conftest import PKG, ROOT
 
 HEADER = os.path.join(ROOT, "include", "revsim.h")
+SW_HEADER = os.path.join(ROOT, "include", "revsim_sw.h")
 
 
-def declared_symbols():
-    src = open(HEADER).read()
+def declared_symbols(header=HEADER):
+    src = open(header).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(revsim_[a-z_0-9]+)\s*\(", src)))
 
@@ -34,13 +35,14 @@ def test_header_declares_entry_points():
 
 
 def test_library_exports_every_declared_symbol(lib):
-    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    missing = [s for s in declared_symbols() + declared_symbols(SW_HEADER) if not hasattr(lib, s)]
     assert not missing, missing
 
 
 def test_python_binding_covers_every_symbol():
-    from revsim import EXPORTS
+    from revsim import EXPORTS, SW_EXPORTS
     assert sorted(EXPORTS) == declared_symbols()
+    assert sorted(SW_EXPORTS) == declared_symbols(SW_HEADER)
 
 
 def test_error_paths_without_device(lib):
@@ -52,3 +54,13 @@ def test_error_paths_without_device(lib):
     assert L.revsim_set_params(None, None, 0) == -1
     assert L.revsim_forward(None, None, 0.0, 0, 0, 0.0, 0, None) == -1
     assert L.revsim_last_error(None) == b"null handle"
+
+
+def test_sw_error_paths_without_device(lib):
+    from revsim import _lib
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    assert L.revsim_sw_create(None, ctypes.byref(h)) == -1
+    assert L.revsim_sw_set_params(None, None, 0) == -1
+    assert L.revsim_sw_forward(None, None, 0.0, 0, 1, 0, 0.0, 0, None, None) == -1
+    assert L.revsim_sw_last_error(None) == b"null handle"
