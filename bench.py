@@ -64,6 +64,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=10)
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
+    ap.add_argument("--workload", default="water", choices=["water", "diamond"],
+                    help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
+                         "carbon, 16 replicas of 8,000 atoms")
+    ap.add_argument("--replicas", type=int, default=16, help="diamond replicas")
+    ap.add_argument("--cells", type=int, default=10, help="diamond conventional cells per side")
+    ap.add_argument("--sw-steps", type=int, default=2000)
+    ap.add_argument("--sw-steps-loss", type=int, default=500)
     ap.add_argument("--profile", action="store_true",
                     help="one untimed gradient and exit (the command profiled under ncu)")
     return ap.parse_args()
@@ -422,9 +429,300 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------ diamond workload
+# Algorithmic work of the Stillinger-Weber reverse terms kernel, counted from its
+# arithmetic (add/mul = 1, FMA = 2, div/exp = 1) with 4 tangents (the position direction
+# and a, gamma, sigma): per ordered pair of active neighbours (q, q') of a centre 97 flops
+# (the 3-body gradient with respect to d_q: 18 for the value, 79 for the tangents), per
+# active neighbour 440 flops (unit vector, radial factors, 2-body term, slot assembly,
+# parameter contraction).  Forward kernel (values only): 18 and 40.
+SW_FLOPS_REV_PAIR, SW_FLOPS_REV_SLOT = 97, 440
+SW_FLOPS_FWD_PAIR, SW_FLOPS_FWD_SLOT = 18, 40
+SW_DT, SW_GAMMA, SW_NOISE = 0.0005, 4.0, 0.005
+
+
+def diamond_name(a):
+    return (f"diamond_sw_{a.replicas}x{8 * a.cells ** 3}atoms_{a.precision}_"
+            f"{a.sw_steps}fwd+{a.sw_steps}rev")
+
+
+def diamond_config(a, extra=None):
+    from revsim import diamond as D
+    c = {"workload": diamond_name(a), "replicas": a.replicas, "n_atoms_per_replica": 8 * a.cells ** 3,
+         "box_nm": a.cells * D.LATTICE_A, "lattice_nm": D.LATTICE_A, "noise_nm": SW_NOISE,
+         "temp_K": 300.0, "n_steps": a.sw_steps, "n_steps_loss": a.sw_steps_loss,
+         "n_steps_trunc": a.sw_steps_loss, "dt_ps": SW_DT, "gamma_per_ps": SW_GAMMA,
+         "precision": a.precision,
+         "loss": "stress tensor squared error (weight 5e-8) vs the mean stress of a run with "
+                 "A x1.05, lambda x0.95",
+         "equilibration": "1 ps Langevin (gamma 4/ps) from the noisy lattice, untimed",
+         "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def diamond_prepare(a, device):
+    """Equilibrated replicas and the stress target, made on the GPU by the engine."""
+    from revsim import SwEngine, diamond as D, systems
+    xs, vs, boxes = [], [], []
+    for r in range(a.replicas):
+        x, box = D.diamond_coords(a.cells, noise=SW_NOISE, seed=4 + r)
+        xs.append(x)
+        vs.append(D.mb_velocities(len(x), temp=300.0, seed=1000 + r))
+        boxes.append(box)
+    n = len(xs[0])
+    p = D.default_params()
+    eq = SwEngine([n] * a.replicas, boxes, temp=300.0, precision="mixed", device=device)
+    eq.set_params(p)
+    eq.set_state(np.concatenate(xs), np.concatenate(vs))
+    eq.set_loss()
+    eq.forward(systems.noise_seeds(2000 * a.replicas, seed=30).reshape(2000, a.replicas),
+               SW_GAMMA, 2000, 2000, SW_DT, calc_loss=False)
+    x0, v0 = eq.get_state()
+    pt = p.copy()
+    pt[0] *= 1.05
+    pt[3] *= 0.95
+    eq.set_params(pt)
+    eq.forward(systems.noise_seeds(200 * a.replicas, seed=31).reshape(200, a.replicas),
+               SW_GAMMA, 200, 200, SW_DT, calc_loss=False)
+    target = eq.stress().mean(axis=0)
+    eq.close()
+    return x0, v0, boxes, p, target
+
+
+def diamond_cpu_sample(a, x0, v0, box, p, target, n_s=2):
+    """The FP64 oracle on n_s forward + n_s reverse steps of one replica (all host threads)."""
+    from oracle import orc
+    from revsim import systems
+    n = len(x0)
+    s = orc.make_sw_system(n, box, 300.0)
+    L = orc.make_sw_loss(5e-8, target)
+    seeds = systems.noise_seeds(n_s, seed=98)
+    t0 = time.perf_counter()
+    xf, vf, _, sx, sv = orc.sw_forward_sim(s, p, x0, v0, seeds, SW_GAMMA, n_s, n_s, SW_DT, L, 0,
+                                           False)
+    orc.sw_reverse_sim(s, p, xf, vf, seeds, SW_GAMMA, n_s, n_s, n_s, SW_DT, sx, sv, L)
+    t1 = time.perf_counter()
+    return n * n_s / (t1 - t0), orc.num_threads(), (
+        f"{n_s} forward + {n_s} reverse steps of one {n}-atom replica, FP64 oracle "
+        f"(its loss evaluations included)")
+
+
+def run_reference_diamond(a):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import orc
+    from revsim import diamond as D
+    orc.build()
+    x, box = D.diamond_coords(a.cells, noise=SW_NOISE, seed=4)
+    v = D.mb_velocities(len(x), temp=300.0, seed=1000)
+    p = D.default_params()
+    vals = []
+    for i in range(a.warmup + a.steps):
+        val, cores, desc = diamond_cpu_sample(a, x, v, box, p, np.zeros(9))
+        if i >= a.warmup:
+            vals.append(val)
+    value = statistics.mean(vals)
+    n_tot = a.replicas * len(x)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1e3 * n_tot * a.sw_steps / value,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "impl": "reference", "config": diamond_config(a, {"precision": "fp64"}),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "the reference is Julia (Molly/Enzyme/JAX); no Julia toolchain exists on these "
+                   "machines, so this arm times the FP64 C restatement of its algorithm"}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours_diamond(a):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import build as _build
+    _build.build()
+    import ctypes
+    from revsim import SwEngine, _lib, systems
+
+    x0, v0, boxes, p, target = diamond_prepare(a, local)
+    R, n = a.replicas, len(x0) // a.replicas
+    N = R * n
+    K, NL = a.sw_steps, a.sw_steps_loss
+
+    def make(prec):
+        e = SwEngine([n] * R, boxes, temp=300.0, precision=prec, device=local)
+        e.set_params(p)
+        e.set_loss(5e-8, target)
+        e.set_state(x0, v0)
+        return e
+
+    eng = make(a.precision)
+    seeds = systems.noise_seeds(K * R, seed=200 + rank).reshape(K, R)
+    if a.profile:
+        eng.forward(seeds, SW_GAMMA, K, NL, SW_DT)
+        eng.reverse(seeds, SW_GAMMA, K, NL, NL, SW_DT)
+        torch.cuda.synchronize()
+        eng.close()
+        return
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def gradient(e=eng):
+        lf, _ = e.forward(seeds, SW_GAMMA, K, NL, SW_DT)
+        lr, g = e.reverse(seeds, SW_GAMMA, K, NL, NL, SW_DT)
+        return lf, lr, g
+
+    for _ in range(a.warmup):
+        eng.set_state(x0, v0)
+        gradient()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            eng.set_state(x0, v0)
+            flush.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lf, lr, g = gradient()
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    clocks = clk.summary()
+    total_ms = sum(times)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / a.steps
+    value = world * N * K / (ms_step * 1e-3)
+
+    # end to end through the public API from pinned host buffers
+    xh = torch.from_numpy(x0.copy()).pin_memory()
+    vh = torch.from_numpy(v0.copy()).pin_memory()
+    e2e_ms = []
+    for _ in range(a.steps):
+        flush.zero_()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.set_state(xh.numpy(), vh.numpy())
+        gradient()
+        e1.record(stream)
+        barrier()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * N * K / (e2e_total / a.steps * 1e-3)
+    h2d = 2 * 3 * N * 8 + 2 * K * R * 8
+    d2h = 2 * R * 8 + R * 7 * 8 + 2 * 3 * N * 8
+
+    # roofline of the dominant kernel (the reverse terms kernel), timed per launch
+    eng.set_state(x0, v0)
+    eng.set_kernel_timing(True)
+    gradient()
+    rt_ms, rt_n = eng.kernel_time(0)
+    ft_ms, ft_n = eng.kernel_time(1)
+    rg_ms, rg_n = eng.kernel_time(2)
+    fg_ms, fg_n = eng.kernel_time(3)
+    eng.set_kernel_timing(False)
+    launch_ms = rt_ms / max(rt_n, 1)
+    pairs = eng.active_pairs()
+    deg = np.bincount(pairs.ravel(), minlength=N).astype(np.int64)
+    flops_launch = int(SW_FLOPS_REV_PAIR * (deg * (deg - 1)).sum() + SW_FLOPS_REV_SLOT * deg.sum())
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "kernel": "k_terms<float, 16, TM_REV> (Stillinger-Weber reverse terms)",
+                "launch_ms": launch_ms, "launches_timed": rt_n, "flops_per_launch": flops_launch,
+                "mean_active_neighbours": float(deg.mean()),
+                "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)",
+                "kernel_ms_per_launch": {"rev_terms": launch_ms, "fwd_terms": ft_ms / max(ft_n, 1),
+                                         "rev_gather": rg_ms / max(rg_n, 1),
+                                         "fwd_gather": fg_ms / max(fg_n, 1)},
+                "step_kernels_share_of_gradient": (rt_ms + ft_ms + rg_ms + fg_ms) / ms_step}
+
+    extra = {}
+    if not a.no_compare and rank == 0:
+        e64 = make("fp64")
+        gradient(e64)
+        s64 = torch.cuda.ExternalStream(e64.stream())
+        e64.set_state(x0, v0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s64)
+        _, _, g64 = gradient(e64)
+        e1.record(s64)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        eng.set_state(x0, v0)
+        _, _, gm = gradient()
+        short = {}
+        for eng_, key in ((eng, "mixed"), (e64, "fp64")):
+            eng_.set_state(x0, v0)
+            eng_.forward(seeds[:100], SW_GAMMA, 100, 100, SW_DT)
+            short[key] = eng_.reverse(seeds[:100], SW_GAMMA, 100, 100, 100, SW_DT)[1].mean(axis=0)
+
+        def rel(gx, gref):
+            sc = np.abs(gref * p)
+            return float(np.max(np.abs((gx - gref) * p) / np.maximum(sc, 0.01 * sc.max())))
+        extra = {"fp64_gpu": {"value": N * K / (ms64 * 1e-3), "ms_per_step": ms64,
+                              "speedup_mixed_over_fp64": ms64 / ms_step},
+                 "grad_rel_err_vs_fp64": {
+                     "full_workload": rel(gm.mean(axis=0), g64.mean(axis=0)),
+                     "first_100_steps": rel(short["mixed"], short["fp64"]),
+                     "definition": "replica-mean gradient; max over parameters of |g - g_fp64| * "
+                                   "|theta| / max(|g_fp64 * theta|, 0.01 max_k |g_fp64,k * theta_k|)"}}
+        e64.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        val, cores, desc = diamond_cpu_sample(a, x0[:n], v0[:n], boxes[0], p, target)
+        cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None,
+               "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
+               "config": diamond_config(a, {"parallelism": f"replicas{world}" if world > 1 else "single"}),
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h},
+               "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+               "clocks": clocks,
+               "loss": {"forward": float(lf.mean()), "reverse": float(lr.mean())}}
+        out.update(extra)
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 if __name__ == "__main__":
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "diamond":
+        run_reference_diamond(args) if args.impl == "reference" else run_ours_diamond(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -371,7 +371,7 @@ int gather(revsim_sw_handle *h, int mode, bool tangent, const SwGatherArgs &g, i
     RC(ev_begin(h, which));
     cudaError_t e = h->prec == REVSIM_MIXED ? launch_sw_gather<float>(mode, h->G, tangent, g, h->st)
                                             : launch_sw_gather<double>(mode, h->G, tangent, g, h->st);
-    h->launches++;
+    h->launches += mode == GM_FORCES ? 1 : 2;
     if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("gather kernel: ") + cudaGetErrorString(e));
     return ev_end(h, which);
 }

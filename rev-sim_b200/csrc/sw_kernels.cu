@@ -244,8 +244,12 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
     __shared__ double s_d[GPB][G][3];
     __shared__ R s_dd[GPB][G][3];
     __shared__ int s_j[GPB][G];
-    __shared__ D s_u[GPB][G][3];
-    __shared__ D s_h[GPB][G];
+    // slot data read by the other lanes: unit vector and its position tangent (it does not
+    // depend on theta), 3-body radial factor h with all tangents
+    __shared__ R s_uv[GPB][G][3];
+    __shared__ R s_ud[GPB][G][3];
+    __shared__ R s_hv[GPB][G];
+    __shared__ R s_hd[GPB][G][K > 0 ? K : 1];
     __shared__ double s_red[TERM_THREADS / 32][9];
 
     const int lane = threadIdx.x % G, grp = threadIdx.x / G;
@@ -378,28 +382,63 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
         g2 = (e1 * sd_neg((R(4) * p.B) * (is4 / sD) + ((p.B * is4) - sdc<R, K>(R(1))) / t2)) / sig;
         gB = xdiv(xmul(e1.v, -xadd(xmul(R(4), xdiv(is4.v, sD.v)), xdiv(is4.v, t2.v))), p.sig);
 #pragma unroll
-        for (int k = 0; k < 3; k++) s_u[grp][lane][k] = u[k];
-        s_h[grp][lane] = h;
+        for (int k = 0; k < 3; k++) {
+            s_uv[grp][lane][k] = u[k].v;
+            if constexpr (K > 0) s_ud[grp][lane][k] = u[k].d[0];
+        }
+        s_hv[grp][lane] = h.v;
+        if constexpr (K > 0) {
+#pragma unroll
+            for (int kk = 0; kk < K; kk++) s_hd[grp][lane][kk] = h.d[kk];
+        }
     }
     __syncwarp(gmask);
 
-    // Phase 3: 3-body sums over the other slots.
+    // Phase 3: 3-body sums over the other slots.  The value arithmetic is the same
+    // sequence of rounded operations for every K; the tangents use that u and cos
+    // depend on the position direction only (tangent 0), not on the parameters.
     D S1 = sdc<R, K>(R(0)), V[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) V[k] = sdc<R, K>(R(0));
     if (own) {
         const R third = R(1) / R(3);
+        R ud[3] = {R(0), R(0), R(0)};
+        if constexpr (K > 0) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) ud[k] = u[k].d[0];
+        }
         for (int q2 = 0; q2 < n; q2++) {
             if (q2 == lane) continue;
-            const D u2x = s_u[grp][q2][0], u2y = s_u[grp][q2][1], u2z = s_u[grp][q2][2];
-            const D h2 = s_h[grp][q2];
-            const D cs = u[0] * u2x + u[1] * u2y + u[2] * u2z;
-            const D c3 = cs + sdc<R, K>(third);
-            const D w = h2 * c3;
-            S1 = S1 + w * (c3 * alpha - cs * beta);
-            V[0] = V[0] + w * u2x;
-            V[1] = V[1] + w * u2y;
-            V[2] = V[2] + w * u2z;
+            const R u2[3] = {s_uv[grp][q2][0], s_uv[grp][q2][1], s_uv[grp][q2][2]};
+            const R h2 = s_hv[grp][q2];
+            const R cs = xadd(xadd(xmul(u[0].v, u2[0]), xmul(u[1].v, u2[1])), xmul(u[2].v, u2[2]));
+            const R c3 = xadd(cs, third);
+            const R w = xmul(h2, c3);
+            const R X = xsub(xmul(c3, alpha.v), xmul(cs, beta.v));
+            S1.v = xadd(S1.v, xmul(w, X));
+#pragma unroll
+            for (int k = 0; k < 3; k++) V[k].v = xadd(V[k].v, xmul(w, u2[k]));
+            if constexpr (K > 0) {
+                const R u2d[3] = {s_ud[grp][q2][0], s_ud[grp][q2][1], s_ud[grp][q2][2]};
+                const R csd = xfma(ud[0], u2[0], xfma(u[0].v, u2d[0], xfma(ud[1], u2[1], xfma(u[1].v, u2d[1],
+                                   xfma(ud[2], u2[2], xmul(u[2].v, u2d[2]))))));
+                R wd[K], Xd[K];
+                wd[0] = xfma(s_hd[grp][q2][0], c3, xmul(h2, csd));
+                Xd[0] = xsub(xfma(csd, alpha.v, xmul(c3, alpha.d[0])), xfma(csd, beta.v, xmul(cs, beta.d[0])));
+#pragma unroll
+                for (int kk = 1; kk < K; kk++) {
+                    wd[kk] = xmul(s_hd[grp][q2][kk], c3);
+                    Xd[kk] = xsub(xmul(c3, alpha.d[kk]), xmul(cs, beta.d[kk]));
+                }
+#pragma unroll
+                for (int kk = 0; kk < K; kk++) S1.d[kk] = xfma(wd[kk], X, xfma(w, Xd[kk], S1.d[kk]));
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    V[k].d[0] = xfma(wd[0], u2[k], xfma(w, u2d[k], V[k].d[0]));
+#pragma unroll
+                    for (int kk = 1; kk < K; kk++) V[k].d[kk] = xfma(wd[kk], u2[k], V[k].d[kk]);
+                }
+            }
         }
     }
     D T[3];
@@ -494,48 +533,74 @@ __device__ __forceinline__ void part1(const SwGatherArgs &g, int e, int rep, con
     }
 }
 
-template <typename R, int G, int MODE, bool TAN>
+template <typename R, int G, bool TAN>
 __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= g.N) return;
+    // G lanes per atom e: lane q reads slot q (T_{e,q}) and the matching slot of its
+    // neighbour (T_{j_q, slot of e}); a butterfly sum over the lanes (every lane ends
+    // with the same bits: each level adds two equal-order pairs) gives f = dE/dx_e and
+    // tg, its derivative along the tangent (H w or H u).  Lane 0 writes F = -f and
+    // G = -tg; k_finish integrates.
+    const int lane = threadIdx.x % G;
+    const int e = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G);
+    const int gshift = (threadIdx.x % 32) / G * G;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gshift;
     const R *Tv = (const R *)g.Tv;
     const R *Tt = (const R *)g.Tt;
-    const int n = g.act_n[e];
+    const bool live = e < g.N;
     double f[3] = {0.0, 0.0, 0.0}, tg[3] = {0.0, 0.0, 0.0};
-    bool ok = true;
-    for (int q = 0; q < n; q++) {
-        const int j = g.act_idx[(size_t)e * G + q];
-        const int nj = g.act_n[j];
-        const int *rj = g.act_idx + (size_t)j * G;
-        int pos = -1;
-        for (int k = 0; k < nj; k++)
-            if (rj[k] == e) {
-                pos = k;
-                break;
-            }
-        if (pos < 0) {
-            ok = false;
-            continue;
-        }
-        const size_t ie = ((size_t)e * G + q) * 3, ij = ((size_t)j * G + pos) * 3;
+    if (live) {
+        const int n = g.act_n[e];
+        if (lane < n) {
+            const int j = g.act_idx[(size_t)e * G + lane];
+            const int nj = g.act_n[j];
+            const int *rj = g.act_idx + (size_t)j * G;
+            int pos = -1;
+            for (int k = 0; k < nj; k++)
+                if (rj[k] == e) pos = k;
+            if (pos < 0) {
+                atomicOr(g.status, ST_NLIST_OVERFLOW);
+            } else {
+                const size_t ie = ((size_t)e * G + lane) * 3, ij = ((size_t)j * G + pos) * 3;
 #pragma unroll
-        for (int u = 0; u < 3; u++) {
-            f[u] = __dadd_rn(f[u], __dsub_rn((double)Tv[ij + u], (double)Tv[ie + u]));
-            if (TAN) tg[u] = __dadd_rn(tg[u], __dsub_rn((double)Tt[ij + u], (double)Tt[ie + u]));
+                for (int u = 0; u < 3; u++) {
+                    f[u] = __dsub_rn((double)Tv[ij + u], (double)Tv[ie + u]);
+                    if (TAN) tg[u] = __dsub_rn((double)Tt[ij + u], (double)Tt[ie + u]);
+                }
+            }
         }
     }
-    if (!ok) atomicOr(g.status, ST_NLIST_OVERFLOW);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            f[u] = __dadd_rn(f[u], __shfl_xor_sync(gmask, f[u], o));
+            if (TAN) tg[u] = __dadd_rn(tg[u], __shfl_xor_sync(gmask, tg[u], o));
+        }
+    }
+    if (!live || lane != 0) return;
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        g.F[3 * (size_t)e + u] = -f[u];
+        if (TAN) g.G[3 * (size_t)e + u] = -tg[u];
+    }
+    if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]) && isfinite(tg[0]) && isfinite(tg[1]) &&
+          isfinite(tg[2])))
+        atomicOr(g.status, ST_NAN);
+}
+
+// One thread per atom: the step (or loss) arithmetic after the gather.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_finish(SwGatherArgs g) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= g.N) return;
+    double f[3], tg[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        f[u] = -g.F[3 * (size_t)e + u];
+        tg[u] = MODE == GM_FWD ? 0.0 : -g.G[3 * (size_t)e + u];
+    }
     const int rep = g.atom_rep[e];
     // f = dE/dx_e, tg = its derivative along the tangent (H w or H u).
-    if (MODE == GM_FORCES) {
-#pragma unroll
-        for (int u = 0; u < 3; u++) {
-            g.F[3 * (size_t)e + u] = -f[u];
-            if (TAN && g.G) g.G[3 * (size_t)e + u] = -tg[u];
-        }
-        if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]))) atomicOr(g.status, ST_NAN);
-        return;
-    }
     if (MODE == GM_FWD) {
         // diamond.jl:1462-1467
         const double L = g.rep_box[rep];
@@ -552,7 +617,6 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
             g.x[i] = wrap1d(x, L);
             g.v[i] = v;
         }
-        if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]))) atomicOr(g.status, ST_NAN);
         return;
     }
     if (MODE == GM_REV) {
@@ -565,11 +629,7 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
             const double Bn = __dadd_rn(__dmul_rn(g.c, g.B[i]), __dmul_rn(g.dt2, Gn));
             g.B[i] = Bn;
             g.A[i] = __dadd_rn(g.A[i], Bn);
-            g.G[i] = Gn;
         }
-        if (!(isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]) && isfinite(tg[0]) &&
-              isfinite(tg[1]) && isfinite(tg[2])))
-            atomicOr(g.status, ST_NAN);
         if (g.fuse_next) part1(g, e, rep, g.seed_next);
         return;
     }
@@ -611,7 +671,6 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
                 g.G[i] = 0.0;
             }
         }
-        if (!(isfinite(gx[0]) && isfinite(gx[1]) && isfinite(gx[2]))) atomicOr(g.status, ST_NAN);
     }
 }
 
@@ -781,19 +840,21 @@ cudaError_t launch_sw_terms(int mode, int G, int n_blk, const SwTermArgs &a, con
 
 template <typename R>
 cudaError_t launch_sw_gather(int mode, int G, bool tangent, const SwGatherArgs &a, cudaStream_t st) {
-    const int nb = nblk(a.N, 256);
-#define RS_G(GG)                                                                              \
-    do {                                                                                      \
-        if (mode == GM_FORCES && tangent) k_gather<R, GG, GM_FORCES, true><<<nb, 256, 0, st>>>(a);  \
-        else if (mode == GM_FORCES) k_gather<R, GG, GM_FORCES, false><<<nb, 256, 0, st>>>(a); \
-        else if (mode == GM_FWD) k_gather<R, GG, GM_FWD, false><<<nb, 256, 0, st>>>(a);       \
-        else if (mode == GM_REV) k_gather<R, GG, GM_REV, true><<<nb, 256, 0, st>>>(a);        \
-        else k_gather<R, GG, GM_LOSS, true><<<nb, 256, 0, st>>>(a);                           \
-    } while (0)
-    if (G == 16) RS_G(16);
-    else if (G == 32) RS_G(32);
-    else return cudaErrorInvalidValue;
-#undef RS_G
+    const int nb = (int)(((size_t)a.N * G + 255) / 256);
+    const bool tan = tangent || mode == GM_REV || mode == GM_LOSS;
+    if (G == 16) {
+        if (tan) k_gather<R, 16, true><<<nb, 256, 0, st>>>(a);
+        else k_gather<R, 16, false><<<nb, 256, 0, st>>>(a);
+    } else if (G == 32) {
+        if (tan) k_gather<R, 32, true><<<nb, 256, 0, st>>>(a);
+        else k_gather<R, 32, false><<<nb, 256, 0, st>>>(a);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    const int na = nblk(a.N, 256);
+    if (mode == GM_FWD) k_finish<GM_FWD><<<na, 256, 0, st>>>(a);
+    else if (mode == GM_REV) k_finish<GM_REV><<<na, 256, 0, st>>>(a);
+    else if (mode == GM_LOSS) k_finish<GM_LOSS><<<na, 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
