@@ -262,9 +262,13 @@ def run_ours(a):
     eng.set_state(x0, v0)
     seeds = systems.noise_seeds(a.n_steps, seed=100 + rank)
     if a.profile:
+        # one gradient between cudaProfilerStart/Stop (ncu --profile-from-start off)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
         eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
         eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         eng.close()
         return
     shape = eng.autotune()
@@ -567,9 +571,13 @@ def run_ours_diamond(a):
     eng = make(a.precision)
     seeds = systems.noise_seeds(K * R, seed=200 + rank).reshape(K, R)
     if a.profile:
+        # one gradient between cudaProfilerStart/Stop (ncu --profile-from-start off)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
         eng.forward(seeds, SW_GAMMA, K, NL, SW_DT)
         eng.reverse(seeds, SW_GAMMA, K, NL, NL, SW_DT)
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         eng.close()
         return
     stream = torch.cuda.ExternalStream(eng.stream())

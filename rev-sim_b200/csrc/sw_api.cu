@@ -44,6 +44,7 @@ struct revsim_sw_handle {
     int n_blk = 0, n_ablk = 0;
     int *d_blk_rep = nullptr, *d_blk_atom0 = nullptr, *d_blk_n = nullptr;
     int *d_ablk_rep = nullptr, *d_ablk_atom0 = nullptr, *d_ablk_n = nullptr;
+    int *d_rep_blk0 = nullptr, *d_rep_ablk0 = nullptr;   // [R + 1] block ranges per replica
     // cells and candidate rows
     std::vector<int> nc, cell_off;
     int n_cells = 0;
@@ -123,8 +124,12 @@ SwConsts<R> consts(const revsim_sw_handle *h) {
     p.eps = (R)t[6];
     p.half_eA = (R)(0.5 * t[6] * t[0]);
     p.el = (R)(t[6] * t[3]);
+    p.isig = (R)(1.0 / t[5]);
     p.a64 = t[2];
     p.sig64 = t[5];
+    const double lim = t[2] * t[5];
+    p.lo2 = (lim * (1 - 1e-9)) * (lim * (1 - 1e-9));
+    p.hi2 = (lim * (1 + 1e-9)) * (lim * (1 + 1e-9));
     return p;
 }
 
@@ -138,6 +143,12 @@ int set_blocks(revsim_sw_handle *h) {
             bn.push_back(std::min(gpb, h->nat[r] - i));
         }
     h->n_blk = (int)br.size();
+    std::vector<int> r0(h->R + 1, 0);
+    for (int b = 0; b < h->n_blk; b++) r0[br[b] + 1] = b + 1;
+    for (int r = 0; r < h->R; r++) r0[r + 1] = std::max(r0[r + 1], r0[r]);
+    dfree(h->d_rep_blk0);
+    CK(dalloc(&h->d_rep_blk0, h->R + 1));
+    CK(cudaMemcpy(h->d_rep_blk0, r0.data(), sizeof(int) * (h->R + 1), cudaMemcpyHostToDevice));
     dfree(h->d_blk_rep);
     dfree(h->d_blk_atom0);
     dfree(h->d_blk_n);
@@ -188,7 +199,8 @@ int set_cells(revsim_sw_handle *h) {
 void free_all(revsim_sw_handle *h) {
     void *ptrs[] = {h->d_atom_rep, h->d_rep_atom0, h->d_rep_n, h->d_rep_box, h->d_rep_vol,
                     h->d_rep_sd, h->d_target, h->d_blk_rep, h->d_blk_atom0, h->d_blk_n,
-                    h->d_ablk_rep, h->d_ablk_atom0, h->d_ablk_n, h->d_rep_nc, h->d_rep_cell_off,
+                    h->d_ablk_rep, h->d_ablk_atom0, h->d_ablk_n, h->d_rep_blk0, h->d_rep_ablk0,
+                    h->d_rep_nc, h->d_rep_cell_off,
                     h->d_cell_of, h->d_cell_cnt, h->d_cell_start, h->d_cell_fill, h->d_cell_atoms,
                     h->d_cand, h->d_cand_n, h->d_x_nl, h->d_act_idx, h->d_act_n, h->d_Tv, h->d_Tt,
                     h->d_x, h->d_v, h->d_F, h->d_G, h->d_A, h->d_B, h->d_C, h->d_D, h->d_dLdx,
@@ -388,6 +400,9 @@ int stress(revsim_sw_handle *h, int vel_term, bool accumulate) {
     a.n_ablk = h->n_ablk;
     a.blk_rep = h->d_blk_rep;
     a.n_blk = h->n_blk;
+    a.rep_blk0 = h->d_rep_blk0;
+    a.rep_ablk0 = h->d_rep_ablk0;
+    a.rep_n = h->d_rep_n;
     a.v = h->d_v;
     a.vpart = h->d_vpart;
     a.kpart = h->d_kpart;
@@ -668,6 +683,11 @@ int32_t revsim_sw_create(const revsim_sw_desc *d, revsim_sw_handle **out) {
                 an.push_back(std::min(256, h->nat[r] - i));
             }
         h->n_ablk = (int)ar.size();
+        std::vector<int> ra(R + 1, 0);
+        for (int b = 0; b < h->n_ablk; b++) ra[ar[b] + 1] = b + 1;
+        for (int r = 0; r < R; r++) ra[r + 1] = std::max(ra[r + 1], ra[r]);
+        CK(dalloc(&h->d_rep_ablk0, R + 1));
+        CK(cudaMemcpy(h->d_rep_ablk0, ra.data(), sizeof(int) * (R + 1), cudaMemcpyHostToDevice));
         CK(dalloc(&h->d_ablk_rep, ar.size()));
         CK(dalloc(&h->d_ablk_atom0, ar.size()));
         CK(dalloc(&h->d_ablk_n, ar.size()));

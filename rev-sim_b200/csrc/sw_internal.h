@@ -10,7 +10,8 @@
 //   T_{c,q} = dE_c / dd_q   (and its directional derivative along a tangent),
 // and the gather kernel forms the gradient of atom e as
 //   dE/dx_e = sum_q ( T_{j_q, slot of e in j_q} - T_{e,q} ),
-// summed in ascending q: a deterministic order that depends only on the positions,
+// summed in a fixed order over the slots (a butterfly over the lanes that hold them;
+// slots ascend with the neighbour index): an order that depends only on the positions,
 // not on when the candidate list was built, so forward and reverse forces are
 // bit-identical without storing the lists.
 #pragma once
@@ -34,7 +35,9 @@ struct SwConsts {
     R A, B, a, lam, gam, sig, eps;
     R half_eA;   // eps * A / 2
     R el;        // eps * lambda
+    R isig;      // 1 / sigma
     double a64, sig64;
+    double lo2, hi2;   // (a sigma)^2 (1 -+ 1e-9)^2: r^2 below lo2 is active, above hi2 not
 };
 
 struct SwNlArgs {
@@ -100,6 +103,7 @@ struct SwRedArgs {
     int n_ablk;
     const int *blk_rep;                          // term CTAs
     int n_blk;
+    const int *rep_blk0, *rep_ablk0, *rep_n;     // [R + 1] first term / atom block per replica, [R] atoms
     const double *v;
     double *vpart, *kpart;                       // [n_ablk * 3], [n_ablk * 9]
     double *vbar;                                // [R * 3]

@@ -79,6 +79,15 @@ __device__ __forceinline__ SD<R, K> sd_exp(const SD<R, K> &a) {
     return r;
 }
 template <typename R, int K>
+__device__ __forceinline__ SD<R, K> sd_inv(const SD<R, K> &a) {
+    SD<R, K> r;
+    r.v = xdiv(R(1), a.v);
+    const R m = -xmul(r.v, r.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = xmul(m, a.d[k]);
+    return r;
+}
+template <typename R, int K>
 __device__ __forceinline__ SD<R, K> sd_neg(const SD<R, K> &a) {
     SD<R, K> r;
     r.v = -a.v;
@@ -176,8 +185,14 @@ __global__ void k_cell_fill(SwNlArgs a) {
 // Candidate row of atom e: every other atom of its replica within a sigma + skin (FP64
 // minimum-image distance), ascending index.  Cells are at least that wide and number at
 // least 3 per side, so the 27 cells around e are distinct and hold every candidate.
-__global__ void k_rows(SwNlArgs a) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per atom: lane l < 27 scans cell l, hits are collected in shared memory in
+// any order, then each hit is written at its rank (the hits are distinct atoms).
+constexpr int ROWS_WARPS = 8;
+__global__ void __launch_bounds__(32 * ROWS_WARPS) k_rows(SwNlArgs a) {
+    __shared__ int s_list[ROWS_WARPS][CAND];
+    __shared__ int s_cnt[ROWS_WARPS];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int e = blockIdx.x * ROWS_WARPS + warp;
     if (e >= a.N) return;
     const int r = a.atom_rep[e];
     const int nc = a.rep_nc[r], off = a.rep_cell_off[r];
@@ -185,44 +200,39 @@ __global__ void k_rows(SwNlArgs a) {
     const int loc = a.cell_of[e] - off;
     const int cx = loc % nc, cy = (loc / nc) % nc, cz = loc / (nc * nc);
     const double *xe = a.x + 3 * (size_t)e;
-    int row[CAND];
-    int cnt = 0;
-    for (int dz = -1; dz <= 1; dz++) {
-        const int z = (cz + dz + nc) % nc;
-        for (int dy = -1; dy <= 1; dy++) {
-            const int y = (cy + dy + nc) % nc;
-            for (int dx = -1; dx <= 1; dx++) {
-                const int xx = (cx + dx + nc) % nc;
-                const int cell = off + (z * nc + y) * nc + xx;
-                const int s0 = a.cell_start[cell], s1 = s0 + a.cell_cnt[cell];
-                for (int s = s0; s < s1; s++) {
-                    const int j = a.cell_atoms[s];
-                    if (j == e) continue;
-                    double d[3];
-                    if (dist2(xe, a.x + 3 * (size_t)j, L, d) < a.rl2) {
-                        if (cnt < CAND) {
-                            // insertion into the ascending row
-                            int p = cnt;
-                            while (p > 0 && row[p - 1] > j) {
-                                row[p] = row[p - 1];
-                                p--;
-                            }
-                            row[p] = j;
-                        }
-                        cnt++;
-                    }
-                }
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncwarp();
+    if (lane < 27) {
+        const int z = (cz + lane / 9 - 1 + nc) % nc;
+        const int y = (cy + (lane / 3) % 3 - 1 + nc) % nc;
+        const int xx = (cx + lane % 3 - 1 + nc) % nc;
+        const int cell = off + (z * nc + y) * nc + xx;
+        const int s0 = a.cell_start[cell], s1 = s0 + a.cell_cnt[cell];
+        for (int q = s0; q < s1; q++) {
+            const int j = a.cell_atoms[q];
+            if (j == e) continue;
+            double d[3];
+            if (dist2(xe, a.x + 3 * (size_t)j, L, d) < a.rl2) {
+                const int k = atomicAdd(&s_cnt[warp], 1);
+                if (k < CAND) s_list[warp][k] = j;
             }
         }
     }
-    if (cnt > CAND) {
-        atomicOr(a.status, ST_NLIST_OVERFLOW);
-        cnt = CAND;
-    }
+    __syncwarp();
+    const int cnt = s_cnt[warp];
+    const int m = cnt < CAND ? cnt : CAND;
     int *out = a.cand + (size_t)e * CAND;
-    for (int k = 0; k < cnt; k++) out[k] = row[k];
-    a.cand_n[e] = cnt;
-    atomicMax(a.max_cnt, cnt);
+    for (int it = lane; it < m; it += 32) {
+        const int v = s_list[warp][it];
+        int rank = 0;
+        for (int k = 0; k < m; k++) rank += s_list[warp][k] < v ? 1 : 0;
+        out[rank] = v;
+    }
+    if (lane == 0) {
+        if (cnt > CAND) atomicOr(a.status, ST_NLIST_OVERFLOW);
+        a.cand_n[e] = m;
+        atomicMax(a.max_cnt, cnt);
+    }
 }
 
 // ------------------------------------------------------------------ terms
@@ -293,7 +303,9 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
         if (k < nc) {
             j = t.cand[(size_t)c * CAND + k];
             const double r2 = dist2(xc, t.x + 3 * (size_t)j, L, d);
-            act = __ddiv_rn(__dsqrt_rn(r2), p.sig64) < p.a64;
+            // r / sigma < a decided in FP64 as the reference rounds it; r^2 outside a
+            // 1e-9 relative band around (a sigma)^2 decides it without the root.
+            act = r2 < p.lo2 || (r2 <= p.hi2 && __ddiv_rn(__dsqrt_rn(r2), p.sig64) < p.a64);
         }
         const unsigned bal = (__ballot_sync(gmask, act) >> gshift) & gbits;
         if (act) {
@@ -327,60 +339,63 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
     }
     __syncwarp(gmask);
 
-    // Phase 2: per-slot quantities.
+    // Phase 2: per-slot quantities (u = d / r, h = exp(gamma / t), alpha = dh/ds / sigma,
+    // beta = 2 h / r with s = r / sigma, t = s - a; t from FP64 to keep its digits near
+    // the cutoff).  Divisions are three reciprocals.
     const bool own = lane < n;
-    D u[3], alpha = sdc<R, K>(R(0)), beta = sdc<R, K>(R(0)), g2 = sdc<R, K>(R(0));
+    D u[3], alpha = sdc<R, K>(R(0)), beta = sdc<R, K>(R(0)), sD = sdc<R, K>(R(1)),
+            itD = sdc<R, K>(R(0)), it2 = sdc<R, K>(R(0)), g2 = sdc<R, K>(R(0));
+    R gB = R(0);
 #pragma unroll
     for (int k = 0; k < 3; k++) u[k] = sdc<R, K>(R(0));
-    R gB = R(0);
-    double d64[3] = {0.0, 0.0, 0.0};
+    D gam = sdc<R, K>(p.gam), isig = sdc<R, K>(p.isig);
+    if constexpr (K > 0) {
+        gam.d[2] = R(1);
+        isig.d[3] = -xmul(p.isig, p.isig);
+    }
     if (own) {
+        double d64[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) d64[k] = s_d[grp][lane][k];
         t.act_idx[(size_t)c * G + lane] = s_j[grp][lane];
         const double r64 = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d64[0], d64[0]), __dmul_rn(d64[1], d64[1])),
                                                 __dmul_rn(d64[2], d64[2])));
         const double s64 = __ddiv_rn(r64, p.sig64);
-        R dd[3] = {R(0), R(0), R(0)};
+        const R r = (R)r64, ir = xdiv(R(1), r);
+        R rdot = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) u[k].v = xmul((R)d64[k], ir);
+        sD.v = (R)s64;
+        D tD = sdc<R, K>((R)__dsub_rn(s64, p.a64));
+        D irD = sdc<R, K>(ir);
         if constexpr (K > 0) {
+            // position tangent: r' = u . d'; u' = (d' - u r') / r; s' = r' / sigma;
+            // parameter tangents: dt/da = -1, ds/dsigma = dt/dsigma = -s / sigma
+            R dd[3];
 #pragma unroll
             for (int k = 0; k < 3; k++) dd[k] = s_dd[grp][lane][k];
-        }
-        const R r = (R)r64, s = (R)s64, tv = (R)__dsub_rn(s64, p.a64);
-        D rD = sdc<R, K>(r), sig = sdc<R, K>(p.sig), gam = sdc<R, K>(p.gam), sD, tD;
-        D dD[3];
+            rdot = xfma(u[0].v, dd[0], xfma(u[1].v, dd[1], xmul(u[2].v, dd[2])));
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            dD[k] = sdc<R, K>((R)d64[k]);
-            if constexpr (K > 0) dD[k].d[0] = dd[k];
-        }
-        if constexpr (K > 0) {
-            // r' = d . d' / r along the position tangent; ds/dsigma = -s / sigma; dt/da = -1
-            rD.d[0] = xdiv(xfma(dD[0].v, dd[0], xfma(dD[1].v, dd[1], xmul(dD[2].v, dd[2]))), r);
-            sig.d[3] = R(1);
-            gam.d[2] = R(1);
-        }
-        sD = sdc<R, K>(s);
-        tD = sdc<R, K>(tv);
-        if constexpr (K > 0) {
-            sD.d[0] = xdiv(rD.d[0], p.sig);
-            sD.d[3] = -xdiv(s, p.sig);
+            for (int k = 0; k < 3; k++) u[k].d[0] = xmul(xsub(dd[k], xmul(u[k].v, rdot)), ir);
+            sD.d[0] = xmul(rdot, p.isig);
+            sD.d[3] = -xmul(sD.v, p.isig);
             tD.d[0] = sD.d[0];
             tD.d[1] = R(-1);
             tD.d[3] = sD.d[3];
+            irD.d[0] = -xmul(rdot, xmul(ir, ir));
         }
-#pragma unroll
-        for (int k = 0; k < 3; k++) u[k] = dD[k] / rD;
-        const D h = sd_exp(gam / tD);
-        const D t2 = tD * tD;
-        alpha = sd_neg((gam * h) / (sig * t2));
-        beta = (R(2) * h) / rD;
-        const D e1 = sd_exp(sdc<R, K>(R(1)) / tD);
-        const D s2 = sD * sD, s4 = s2 * s2;
-        const D is4 = sdc<R, K>(R(1)) / s4;
-        // dE2/dr / (eps A) = e^{1/t} (-4 B s^-5 - (B s^-4 - 1) / t^2) / sigma   (diamond.jl:453)
-        g2 = (e1 * sd_neg((R(4) * p.B) * (is4 / sD) + ((p.B * is4) - sdc<R, K>(R(1))) / t2)) / sig;
-        gB = xdiv(xmul(e1.v, -xadd(xmul(R(4), xdiv(is4.v, sD.v)), xdiv(is4.v, t2.v))), p.sig);
+        itD = sd_inv(tD);
+        it2 = itD * itD;
+        const D h = sd_exp(gam * itD);
+        alpha = sd_neg(((gam * h) * it2) * isig);
+        beta = R(2) * (h * irD);
+        // 2-body: dE2/dr / (eps A) = e^{1/t} (-4 B s^-5 - (B s^-4 - 1) / t^2) / sigma
+        // (diamond.jl:453), and its B derivative.
+        const D e1 = sd_exp(itD);
+        const D is = sd_inv(sD);
+        const D is2 = is * is, is4 = is2 * is2, is5 = is4 * is;
+        g2 = (e1 * sd_neg((R(4) * p.B) * is5 + ((p.B * is4) - sdc<R, K>(R(1))) * it2)) * isig;
+        gB = xmul(xmul(e1.v, -xadd(xmul(R(4), is5.v), xmul(is4.v, it2.v))), p.isig);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             s_uv[grp][lane][k] = u[k].v;
@@ -408,9 +423,11 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
             for (int k = 0; k < 3; k++) ud[k] = u[k].d[0];
         }
         for (int q2 = 0; q2 < n; q2++) {
-            if (q2 == lane) continue;
+            // the slot itself enters with weight 0 (its terms are finite), which keeps the
+            // lanes of a group on one path
+            const R one = q2 == lane ? R(0) : R(1);
             const R u2[3] = {s_uv[grp][q2][0], s_uv[grp][q2][1], s_uv[grp][q2][2]};
-            const R h2 = s_hv[grp][q2];
+            const R h2 = xmul(s_hv[grp][q2], one);
             const R cs = xadd(xadd(xmul(u[0].v, u2[0]), xmul(u[1].v, u2[1])), xmul(u[2].v, u2[2]));
             const R c3 = xadd(cs, third);
             const R w = xmul(h2, c3);
@@ -423,11 +440,11 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
                 const R csd = xfma(ud[0], u2[0], xfma(u[0].v, u2d[0], xfma(ud[1], u2[1], xfma(u[1].v, u2d[1],
                                    xfma(ud[2], u2[2], xmul(u[2].v, u2d[2]))))));
                 R wd[K], Xd[K];
-                wd[0] = xfma(s_hd[grp][q2][0], c3, xmul(h2, csd));
+                wd[0] = xfma(xmul(s_hd[grp][q2][0], one), c3, xmul(h2, csd));
                 Xd[0] = xsub(xfma(csd, alpha.v, xmul(c3, alpha.d[0])), xfma(csd, beta.v, xmul(cs, beta.d[0])));
 #pragma unroll
                 for (int kk = 1; kk < K; kk++) {
-                    wd[kk] = xmul(s_hd[grp][q2][kk], c3);
+                    wd[kk] = xmul(xmul(s_hd[grp][q2][kk], one), c3);
                     Xd[kk] = xsub(xmul(c3, alpha.d[kk]), xmul(cs, beta.d[kk]));
                 }
 #pragma unroll
@@ -440,6 +457,11 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
                 }
             }
         }
+    }
+    double d64[3] = {0.0, 0.0, 0.0};
+    if (own) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) d64[k] = s_d[grp][lane][k];
     }
     D T[3];
     const D coef = p.half_eA * g2 + p.el * S1;
@@ -553,10 +575,19 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
         if (lane < n) {
             const int j = g.act_idx[(size_t)e * G + lane];
             const int nj = g.act_n[j];
-            const int *rj = g.act_idx + (size_t)j * G;
+            // the neighbour's whole slot row in G/4 16-byte loads, then compare
+            const int4 *rj = reinterpret_cast<const int4 *>(g.act_idx + (size_t)j * G);
+            int4 row[G / 4];
+#pragma unroll
+            for (int k = 0; k < G / 4; k++) row[k] = rj[k];
             int pos = -1;
-            for (int k = 0; k < nj; k++)
-                if (rj[k] == e) pos = k;
+#pragma unroll
+            for (int k = 0; k < G / 4; k++) {
+                if (4 * k + 0 < nj && row[k].x == e) pos = 4 * k + 0;
+                if (4 * k + 1 < nj && row[k].y == e) pos = 4 * k + 1;
+                if (4 * k + 2 < nj && row[k].z == e) pos = 4 * k + 2;
+                if (4 * k + 3 < nj && row[k].w == e) pos = 4 * k + 3;
+            }
             if (pos < 0) {
                 atomicOr(g.status, ST_NLIST_OVERFLOW);
             } else {
@@ -717,19 +748,28 @@ __global__ void __launch_bounds__(256) k_vsum(SwRedArgs a) {
     block_sum256<3>(s, v, a.vpart + 3 * (size_t)b);
 }
 
-__global__ void k_vbar(SwRedArgs a) {
-    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
-        double t[3] = {0.0, 0.0, 0.0};
-        long long n = 0;
-        for (int b = 0; b < a.n_ablk; b++) {
-            if (a.ablk_rep[b] != r) continue;
-            n += a.ablk_n[b];
+// Per-replica sums of block partials: thread t adds blocks b0 + t, b0 + t + 256, ... in
+// order, then a fixed tree over the threads.
+template <int NV>
+__device__ __forceinline__ void range_sum256(double (*s)[256], const double *part, int b0, int b1,
+                                             double *out) {
+    double v[NV];
 #pragma unroll
-            for (int u = 0; u < 3; u++) t[u] = __dadd_rn(t[u], a.vpart[3 * (size_t)b + u]);
-        }
+    for (int k = 0; k < NV; k++) v[k] = 0.0;
+    for (int b = b0 + threadIdx.x; b < b1; b += 256) {
 #pragma unroll
-        for (int u = 0; u < 3; u++) a.vbar[3 * r + u] = __ddiv_rn(t[u], (double)n);
+        for (int k = 0; k < NV; k++) v[k] = __dadd_rn(v[k], part[(size_t)b * NV + k]);
     }
+    block_sum256<NV>(s, v, out);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_vbar(SwRedArgs a) {
+    __shared__ double s[3][256];
+    __shared__ double tot[3];
+    const int r = blockIdx.x;
+    range_sum256<3>(s, a.vpart, a.rep_ablk0[r], a.rep_ablk0[r + 1], tot);
+    if (threadIdx.x < 3) a.vbar[3 * r + threadIdx.x] = __ddiv_rn(tot[threadIdx.x], (double)a.rep_n[r]);
 }
 
 __global__ void __launch_bounds__(256) k_kin(SwRedArgs a) {
@@ -755,38 +795,26 @@ __global__ void __launch_bounds__(256) k_kin(SwRedArgs a) {
 
 // sigma = (K + W) / V (diamond.jl:753-770); loss = weight sum (sigma - target)^2 / 9
 // (diamond.jl:772-775); S = dL/dsigma.
-__global__ void k_loss_final(SwRedArgs a) {
-    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
-        double W[9], Kt[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) W[k] = Kt[k] = 0.0;
-        for (int b = 0; b < a.n_blk; b++) {
-            if (a.blk_rep[b] != r) continue;
-#pragma unroll
-            for (int k = 0; k < 9; k++) W[k] = __dadd_rn(W[k], a.wpart[9 * (size_t)b + k]);
-        }
-        if (a.vel_term) {
-            for (int b = 0; b < a.n_ablk; b++) {
-                if (a.ablk_rep[b] != r) continue;
-#pragma unroll
-                for (int k = 0; k < 9; k++) Kt[k] = __dadd_rn(Kt[k], a.kpart[9 * (size_t)b + k]);
-            }
-        }
-        const double V = a.rep_vol[r];
-        double l = 0.0;
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-            const double K = a.vel_term ? __dmul_rn(-a.m, Kt[k]) : 0.0;
-            const double sg = __ddiv_rn(__dadd_rn(K, W[k]), V);
-            if (a.sigma) a.sigma[9 * r + k] = sg;
-            const double e = __dsub_rn(sg, a.target[9 * r + k]);
-            l = __dadd_rn(l, __dmul_rn(e, e));
-            if (a.S) a.S[9 * r + k] = __ddiv_rn(__dmul_rn(__dmul_rn(2.0, a.weight), e), 9.0);
-        }
-        l = __dmul_rn(l, __ddiv_rn(a.weight, 9.0));
-        if (a.loss) a.loss[r] = l;
-        if (a.loss_acc) a.loss_acc[r] = __dadd_rn(a.loss_acc[r], l);
+__global__ void __launch_bounds__(256) k_loss_final(SwRedArgs a) {
+    __shared__ double s[9][256];
+    __shared__ double W[9], Kt[9];
+    const int r = blockIdx.x;
+    range_sum256<9>(s, a.wpart, a.rep_blk0[r], a.rep_blk0[r + 1], W);
+    if (a.vel_term) range_sum256<9>(s, a.kpart, a.rep_ablk0[r], a.rep_ablk0[r + 1], Kt);
+    if (threadIdx.x != 0) return;
+    const double V = a.rep_vol[r];
+    double l = 0.0;
+    for (int k = 0; k < 9; k++) {
+        const double K = a.vel_term ? __dmul_rn(-a.m, Kt[k]) : 0.0;
+        const double sg = __ddiv_rn(__dadd_rn(K, W[k]), V);
+        if (a.sigma) a.sigma[9 * r + k] = sg;
+        const double e = __dsub_rn(sg, a.target[9 * r + k]);
+        l = __dadd_rn(l, __dmul_rn(e, e));
+        if (a.S) a.S[9 * r + k] = __ddiv_rn(__dmul_rn(__dmul_rn(2.0, a.weight), e), 9.0);
     }
+    l = __dmul_rn(l, __ddiv_rn(a.weight, 9.0));
+    if (a.loss) a.loss[r] = l;
+    if (a.loss_acc) a.loss_acc[r] = __dadd_rn(a.loss_acc[r], l);
 }
 
 __global__ void k_active_pairs(int N, int G, const int *act_idx, const int *act_n, int32_t *pairs,
@@ -815,7 +843,7 @@ cudaError_t launch_sw_nlist(const SwNlArgs &a, cudaStream_t st) {
     k_cell_count<<<nblk(a.N, 256), 256, 0, st>>>(a);
     k_cell_scan<<<1, 1024, 0, st>>>(a);
     k_cell_fill<<<nblk(a.N, 256), 256, 0, st>>>(a);
-    k_rows<<<nblk(a.N, 128), 128, 0, st>>>(a);
+    k_rows<<<nblk(a.N, ROWS_WARPS), 32 * ROWS_WARPS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -860,9 +888,9 @@ cudaError_t launch_sw_gather(int mode, int G, bool tangent, const SwGatherArgs &
 
 cudaError_t launch_sw_stress(const SwRedArgs &a, cudaStream_t st) {
     k_vsum<<<a.n_ablk, 256, 0, st>>>(a);
-    k_vbar<<<1, 64, 0, st>>>(a);
+    k_vbar<<<a.R, 256, 0, st>>>(a);
     k_kin<<<a.n_ablk, 256, 0, st>>>(a);
-    k_loss_final<<<1, 64, 0, st>>>(a);
+    k_loss_final<<<a.R, 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
