@@ -49,7 +49,8 @@ struct revsim_sw_handle {
     std::vector<int> nc, cell_off;
     int n_cells = 0;
     int *d_rep_nc = nullptr, *d_rep_cell_off = nullptr, *d_cell_of = nullptr, *d_cell_cnt = nullptr,
-        *d_cell_start = nullptr, *d_cell_fill = nullptr, *d_cell_atoms = nullptr;
+        *d_cell_start = nullptr, *d_cell_fill = nullptr;
+    float4 *d_cell_pos = nullptr;
     int *d_cand = nullptr, *d_cand_n = nullptr;
     double *d_x_nl = nullptr;
     // active slots and slot gradients (sized for 32 lanes in FP64)
@@ -128,6 +129,8 @@ SwConsts<R> consts(const revsim_sw_handle *h) {
     p.a64 = t[2];
     p.sig64 = t[5];
     const double lim = t[2] * t[5];
+    p.asig = (R)lim;
+    p.lim2 = lim * lim;
     p.lo2 = (lim * (1 - 1e-9)) * (lim * (1 - 1e-9));
     p.hi2 = (lim * (1 + 1e-9)) * (lim * (1 + 1e-9));
     return p;
@@ -201,7 +204,7 @@ void free_all(revsim_sw_handle *h) {
                     h->d_rep_sd, h->d_target, h->d_blk_rep, h->d_blk_atom0, h->d_blk_n,
                     h->d_ablk_rep, h->d_ablk_atom0, h->d_ablk_n, h->d_rep_blk0, h->d_rep_ablk0,
                     h->d_rep_nc, h->d_rep_cell_off,
-                    h->d_cell_of, h->d_cell_cnt, h->d_cell_start, h->d_cell_fill, h->d_cell_atoms,
+                    h->d_cell_of, h->d_cell_cnt, h->d_cell_start, h->d_cell_fill, h->d_cell_pos,
                     h->d_cand, h->d_cand_n, h->d_x_nl, h->d_act_idx, h->d_act_n, h->d_Tv, h->d_Tt,
                     h->d_x, h->d_v, h->d_F, h->d_G, h->d_A, h->d_B, h->d_C, h->d_D, h->d_dLdx,
                     h->d_dLdv, h->d_x0, h->d_v0, h->d_part, h->d_wpart, h->d_vpart, h->d_kpart,
@@ -261,12 +264,12 @@ int build_list(revsim_sw_handle *h) {
     a.cell_cnt = h->d_cell_cnt;
     a.cell_start = h->d_cell_start;
     a.cell_fill = h->d_cell_fill;
-    a.cell_atoms = h->d_cell_atoms;
+    a.cell_pos = h->d_cell_pos;
     a.cand = h->d_cand;
     a.cand_n = h->d_cand_n;
     a.x_nl = h->d_x_nl;
-    const double rl = h->theta[2] * h->theta[5] + h->skin;
-    a.rl2 = rl * rl;
+    const double rl = h->theta[2] * h->theta[5] + h->skin + 1e-4;
+    a.rl2f = (float)(rl * rl);
     a.status = h->d_status;
     a.max_cnt = h->d_maxcnt;
     cudaError_t e = launch_sw_nlist(a, h->st);
@@ -702,14 +705,14 @@ int32_t revsim_sw_create(const revsim_sw_desc *d, revsim_sw_handle **out) {
         CK(dalloc(&h->d_loss, R));
         CK(dalloc(&h->d_loss_acc, R));
         CK(dalloc(&h->d_cell_of, h->N));
-        CK(dalloc(&h->d_cell_atoms, h->N));
+        CK(dalloc(&h->d_cell_pos, h->N));
         CK(dalloc(&h->d_cand, (size_t)h->N * CAND));
         CK(dalloc(&h->d_cand_n, h->N));
         CK(dalloc(&h->d_x_nl, n3));
         CK(dalloc(&h->d_act_idx, (size_t)h->N * 32));
         CK(dalloc(&h->d_act_n, h->N));
-        CK(dalloc((char **)&h->d_Tv, (size_t)h->N * 32 * 3 * sizeof(double)));
-        CK(dalloc((char **)&h->d_Tt, (size_t)h->N * 32 * 3 * sizeof(double)));
+        CK(dalloc((char **)&h->d_Tv, (size_t)h->N * 32 * 4 * sizeof(double)));
+        CK(dalloc((char **)&h->d_Tt, (size_t)h->N * 32 * 4 * sizeof(double)));
         double **st[] = {&h->d_x, &h->d_v, &h->d_F, &h->d_G, &h->d_A, &h->d_B, &h->d_C,
                          &h->d_D, &h->d_dLdx, &h->d_dLdv, &h->d_x0, &h->d_v0};
         for (double **p : st) {

@@ -36,7 +36,8 @@ struct SwConsts {
     R half_eA;   // eps * A / 2
     R el;        // eps * lambda
     R isig;      // 1 / sigma
-    double a64, sig64;
+    R asig;      // a sigma
+    double a64, sig64, lim2;   // lim2 = (a sigma)^2
     double lo2, hi2;   // (a sigma)^2 (1 -+ 1e-9)^2: r^2 below lo2 is active, above hi2 not
 };
 
@@ -45,10 +46,11 @@ struct SwNlArgs {
     const double *x;
     const int *atom_rep, *rep_nc, *rep_cell_off, *rep_atom0, *rep_n;
     const double *rep_box;
-    int *cell_of, *cell_cnt, *cell_start, *cell_fill, *cell_atoms;
+    int *cell_of, *cell_cnt, *cell_start, *cell_fill;
+    float4 *cell_pos;    // [N] cell-ordered FP32 positions, atom index in .w
     int *cand, *cand_n;
     double *x_nl;
-    double rl2;          // (a sigma + skin)^2
+    float rl2f;          // (a sigma + skin + 1e-4)^2
     int *status, *max_cnt;
 };
 
@@ -68,7 +70,7 @@ struct SwTermArgs {
     const double *S;       // TM_LOSS: [R * 9] dL/dsigma per replica
     double inv_m, acoef_scale;
     int *act_idx, *act_n;
-    void *Tv, *Tt;         // [N * G * 3] in R
+    void *Tv, *Tt;         // [N * G] 4-vectors in R (x, y, z, unused)
     double *part;          // [n_blk * NP] dtheta partials, accumulated (may be null)
     double *wpart;         // [n_blk * 9] virial partials, written (may be null)
     double half_skin2;

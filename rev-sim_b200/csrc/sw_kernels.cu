@@ -78,10 +78,13 @@ __device__ __forceinline__ SD<R, K> sd_exp(const SD<R, K> &a) {
     for (int k = 0; k < K; k++) r.d[k] = xmul(r.v, a.d[k]);
     return r;
 }
+__device__ __forceinline__ float xrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double xrcp(double a) { return __drcp_rn(a); }
+
 template <typename R, int K>
 __device__ __forceinline__ SD<R, K> sd_inv(const SD<R, K> &a) {
     SD<R, K> r;
-    r.v = xdiv(R(1), a.v);
+    r.v = xrcp(a.v);
     const R m = -xmul(r.v, r.v);
 #pragma unroll
     for (int k = 0; k < K; k++) r.d[k] = xmul(m, a.d[k]);
@@ -175,18 +178,23 @@ __global__ void k_cell_scan(SwNlArgs a) {
     }
 }
 
+// Cell-ordered FP32 copy of the positions with the atom index in .w: the candidate test
+// streams one 16-byte load per atom.
 __global__ void k_cell_fill(SwNlArgs a) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.N) return;
     const int c = a.cell_of[e];
-    a.cell_atoms[a.cell_start[c] + atomicAdd(a.cell_fill + c, 1)] = e;
+    const double *x = a.x + 3 * (size_t)e;
+    a.cell_pos[a.cell_start[c] + atomicAdd(a.cell_fill + c, 1)] =
+        make_float4((float)x[0], (float)x[1], (float)x[2], __int_as_float(e));
 }
 
-// Candidate row of atom e: every other atom of its replica within a sigma + skin (FP64
-// minimum-image distance), ascending index.  Cells are at least that wide and number at
-// least 3 per side, so the 27 cells around e are distinct and hold every candidate.
-// One warp per atom: lane l < 27 scans cell l, hits are collected in shared memory in
-// any order, then each hit is written at its rank (the hits are distinct atoms).
+// Candidate row of atom e: every other atom of its replica within a sigma + skin, ascending
+// index.  The rows only need to hold every active pair (the terms kernel decides activity
+// exactly, in FP64), so the test is FP32 with a 1e-4 nm margin.  Cells are at least that
+// wide and number at least 3 per side, so the 27 cells around e are distinct and hold
+// every candidate.  One warp per atom: lane l < 27 scans cell l, hits are collected in
+// shared memory in any order, then each hit is written at its rank (distinct atoms).
 constexpr int ROWS_WARPS = 8;
 __global__ void __launch_bounds__(32 * ROWS_WARPS) k_rows(SwNlArgs a) {
     __shared__ int s_list[ROWS_WARPS][CAND];
@@ -199,7 +207,9 @@ __global__ void __launch_bounds__(32 * ROWS_WARPS) k_rows(SwNlArgs a) {
     const double L = a.rep_box[r];
     const int loc = a.cell_of[e] - off;
     const int cx = loc % nc, cy = (loc / nc) % nc, cz = loc / (nc * nc);
-    const double *xe = a.x + 3 * (size_t)e;
+    const float xe0 = (float)a.x[3 * (size_t)e], xe1 = (float)a.x[3 * (size_t)e + 1],
+                xe2 = (float)a.x[3 * (size_t)e + 2];
+    const float Lf = (float)L, iLf = (float)(1.0 / L), rl2 = a.rl2f;
     if (lane == 0) s_cnt[warp] = 0;
     __syncwarp();
     if (lane < 27) {
@@ -209,10 +219,13 @@ __global__ void __launch_bounds__(32 * ROWS_WARPS) k_rows(SwNlArgs a) {
         const int cell = off + (z * nc + y) * nc + xx;
         const int s0 = a.cell_start[cell], s1 = s0 + a.cell_cnt[cell];
         for (int q = s0; q < s1; q++) {
-            const int j = a.cell_atoms[q];
-            if (j == e) continue;
-            double d[3];
-            if (dist2(xe, a.x + 3 * (size_t)j, L, d) < a.rl2) {
+            const float4 pj = a.cell_pos[q];
+            const int j = __float_as_int(pj.w);
+            float dx = pj.x - xe0, dy = pj.y - xe1, dz = pj.z - xe2;
+            dx -= Lf * rintf(dx * iLf);
+            dy -= Lf * rintf(dy * iLf);
+            dz -= Lf * rintf(dz * iLf);
+            if (j != e && dx * dx + dy * dy + dz * dz < rl2) {
                 const int k = atomicAdd(&s_cnt[warp], 1);
                 if (k < CAND) s_list[warp][k] = j;
             }
@@ -254,12 +267,13 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
     __shared__ double s_d[GPB][G][3];
     __shared__ R s_dd[GPB][G][3];
     __shared__ int s_j[GPB][G];
-    // slot data read by the other lanes: unit vector and its position tangent (it does not
-    // depend on theta), 3-body radial factor h with all tangents
-    __shared__ R s_uv[GPB][G][3];
-    __shared__ R s_ud[GPB][G][3];
-    __shared__ R s_hv[GPB][G];
-    __shared__ R s_hd[GPB][G][K > 0 ? K : 1];
+    // slot data read by the other lanes, in 4-vectors: (u, h), (u', h'_pos), (h'_a, h'_gamma,
+    // h'_sigma, -) -- the unit vector, its position tangent (u does not depend on theta)
+    // and the 3-body radial factor h with its tangents
+    using V4 = typename V4T<R>::T;
+    __shared__ V4 s_uh[GPB][G];
+    __shared__ V4 s_ut[GPB][K > 0 ? G : 1];
+    __shared__ V4 s_ht[GPB][K > 0 ? G : 1];
     __shared__ double s_red[TERM_THREADS / 32][9];
 
     const int lane = threadIdx.x % G, grp = threadIdx.x / G;
@@ -340,8 +354,8 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
     __syncwarp(gmask);
 
     // Phase 2: per-slot quantities (u = d / r, h = exp(gamma / t), alpha = dh/ds / sigma,
-    // beta = 2 h / r with s = r / sigma, t = s - a; t from FP64 to keep its digits near
-    // the cutoff).  Divisions are three reciprocals.
+    // beta = 2 h / r with s = r / sigma, t = s - a; t from an FP64 difference to keep its
+    // digits near the cutoff).  Divisions are reciprocals.
     const bool own = lane < n;
     D u[3], alpha = sdc<R, K>(R(0)), beta = sdc<R, K>(R(0)), sD = sdc<R, K>(R(1)),
             itD = sdc<R, K>(R(0)), it2 = sdc<R, K>(R(0)), g2 = sdc<R, K>(R(0));
@@ -358,15 +372,15 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
 #pragma unroll
         for (int k = 0; k < 3; k++) d64[k] = s_d[grp][lane][k];
         t.act_idx[(size_t)c * G + lane] = s_j[grp][lane];
-        const double r64 = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d64[0], d64[0]), __dmul_rn(d64[1], d64[1])),
-                                                __dmul_rn(d64[2], d64[2])));
-        const double s64 = __ddiv_rn(r64, p.sig64);
-        const R r = (R)r64, ir = xdiv(R(1), r);
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d64[0], d64[0]), __dmul_rn(d64[1], d64[1])),
+                                    __dmul_rn(d64[2], d64[2]));
+        const R r = xsqrt((R)r2), ir = xrcp(r);
         R rdot = R(0);
 #pragma unroll
         for (int k = 0; k < 3; k++) u[k].v = xmul((R)d64[k], ir);
-        sD.v = (R)s64;
-        D tD = sdc<R, K>((R)__dsub_rn(s64, p.a64));
+        sD.v = xmul(r, p.isig);
+        // t = s - a = (r^2 - (a sigma)^2) / (sigma (r + a sigma)), the difference in FP64
+        D tD = sdc<R, K>(xmul((R)__dsub_rn(r2, p.lim2), xrcp(xmul(p.sig, xadd(r, p.asig)))));
         D irD = sdc<R, K>(ir);
         if constexpr (K > 0) {
             // position tangent: r' = u . d'; u' = (d' - u r') / r; s' = r' / sigma;
@@ -396,15 +410,24 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
         const D is2 = is * is, is4 = is2 * is2, is5 = is4 * is;
         g2 = (e1 * sd_neg((R(4) * p.B) * is5 + ((p.B * is4) - sdc<R, K>(R(1))) * it2)) * isig;
         gB = xmul(xmul(e1.v, -xadd(xmul(R(4), is5.v), xmul(is4.v, it2.v))), p.isig);
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            s_uv[grp][lane][k] = u[k].v;
-            if constexpr (K > 0) s_ud[grp][lane][k] = u[k].d[0];
-        }
-        s_hv[grp][lane] = h.v;
+        V4 uh;
+        uh.x = u[0].v;
+        uh.y = u[1].v;
+        uh.z = u[2].v;
+        uh.w = h.v;
+        s_uh[grp][lane] = uh;
         if constexpr (K > 0) {
-#pragma unroll
-            for (int kk = 0; kk < K; kk++) s_hd[grp][lane][kk] = h.d[kk];
+            V4 ut, ht;
+            ut.x = u[0].d[0];
+            ut.y = u[1].d[0];
+            ut.z = u[2].d[0];
+            ut.w = h.d[0];
+            ht.x = h.d[1];
+            ht.y = h.d[2];
+            ht.z = h.d[3];
+            ht.w = R(0);
+            s_ut[grp][lane] = ut;
+            s_ht[grp][lane] = ht;
         }
     }
     __syncwarp(gmask);
@@ -426,8 +449,9 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
             // the slot itself enters with weight 0 (its terms are finite), which keeps the
             // lanes of a group on one path
             const R one = q2 == lane ? R(0) : R(1);
-            const R u2[3] = {s_uv[grp][q2][0], s_uv[grp][q2][1], s_uv[grp][q2][2]};
-            const R h2 = xmul(s_hv[grp][q2], one);
+            const V4 uh2 = s_uh[grp][q2];
+            const R u2[3] = {uh2.x, uh2.y, uh2.z};
+            const R h2 = xmul(uh2.w, one);
             const R cs = xadd(xadd(xmul(u[0].v, u2[0]), xmul(u[1].v, u2[1])), xmul(u[2].v, u2[2]));
             const R c3 = xadd(cs, third);
             const R w = xmul(h2, c3);
@@ -436,15 +460,17 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
 #pragma unroll
             for (int k = 0; k < 3; k++) V[k].v = xadd(V[k].v, xmul(w, u2[k]));
             if constexpr (K > 0) {
-                const R u2d[3] = {s_ud[grp][q2][0], s_ud[grp][q2][1], s_ud[grp][q2][2]};
+                const V4 ut2 = s_ut[grp][q2], ht2 = s_ht[grp][q2];
+                const R u2d[3] = {ut2.x, ut2.y, ut2.z};
+                const R h2d[4] = {ut2.w, ht2.x, ht2.y, ht2.z};
                 const R csd = xfma(ud[0], u2[0], xfma(u[0].v, u2d[0], xfma(ud[1], u2[1], xfma(u[1].v, u2d[1],
                                    xfma(ud[2], u2[2], xmul(u[2].v, u2d[2]))))));
                 R wd[K], Xd[K];
-                wd[0] = xfma(xmul(s_hd[grp][q2][0], one), c3, xmul(h2, csd));
+                wd[0] = xfma(xmul(h2d[0], one), c3, xmul(h2, csd));
                 Xd[0] = xsub(xfma(csd, alpha.v, xmul(c3, alpha.d[0])), xfma(csd, beta.v, xmul(cs, beta.d[0])));
 #pragma unroll
                 for (int kk = 1; kk < K; kk++) {
-                    wd[kk] = xmul(xmul(s_hd[grp][q2][kk], one), c3);
+                    wd[kk] = xmul(xmul(h2d[kk], one), c3);
                     Xd[kk] = xsub(xmul(c3, alpha.d[kk]), xmul(cs, beta.d[kk]));
                 }
 #pragma unroll
@@ -469,14 +495,20 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
 #pragma unroll
     for (int k = 0; k < 3; k++) T[k] = u[k] * coef + elb * V[k];
     if (own) {
-        R *Tv = (R *)t.Tv;
-        const size_t o = ((size_t)c * G + lane) * 3;
-#pragma unroll
-        for (int k = 0; k < 3; k++) Tv[o + k] = T[k].v;
+        using V4 = typename V4T<R>::T;
+        V4 tv;
+        tv.x = T[0].v;
+        tv.y = T[1].v;
+        tv.z = T[2].v;
+        tv.w = R(0);
+        reinterpret_cast<V4 *>(t.Tv)[(size_t)c * G + lane] = tv;
         if constexpr (K > 0) {
-            R *Tt = (R *)t.Tt;
-#pragma unroll
-            for (int k = 0; k < 3; k++) Tt[o + k] = T[k].d[0];
+            V4 tt;
+            tt.x = T[0].d[0];
+            tt.y = T[1].d[0];
+            tt.z = T[2].d[0];
+            tt.w = R(0);
+            reinterpret_cast<V4 *>(t.Tt)[(size_t)c * G + lane] = tt;
         }
     }
 
@@ -566,8 +598,9 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
     const int e = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G);
     const int gshift = (threadIdx.x % 32) / G * G;
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gshift;
-    const R *Tv = (const R *)g.Tv;
-    const R *Tt = (const R *)g.Tt;
+    using V4 = typename V4T<R>::T;
+    const V4 *Tv = reinterpret_cast<const V4 *>(g.Tv);
+    const V4 *Tt = reinterpret_cast<const V4 *>(g.Tt);
     const bool live = e < g.N;
     double f[3] = {0.0, 0.0, 0.0}, tg[3] = {0.0, 0.0, 0.0};
     if (live) {
@@ -591,11 +624,16 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
             if (pos < 0) {
                 atomicOr(g.status, ST_NLIST_OVERFLOW);
             } else {
-                const size_t ie = ((size_t)e * G + lane) * 3, ij = ((size_t)j * G + pos) * 3;
-#pragma unroll
-                for (int u = 0; u < 3; u++) {
-                    f[u] = __dsub_rn((double)Tv[ij + u], (double)Tv[ie + u]);
-                    if (TAN) tg[u] = __dsub_rn((double)Tt[ij + u], (double)Tt[ie + u]);
+                const size_t ie = (size_t)e * G + lane, ij = (size_t)j * G + pos;
+                const V4 a = Tv[ij], b = Tv[ie];
+                f[0] = __dsub_rn((double)a.x, (double)b.x);
+                f[1] = __dsub_rn((double)a.y, (double)b.y);
+                f[2] = __dsub_rn((double)a.z, (double)b.z);
+                if (TAN) {
+                    const V4 at = Tt[ij], bt = Tt[ie];
+                    tg[0] = __dsub_rn((double)at.x, (double)bt.x);
+                    tg[1] = __dsub_rn((double)at.y, (double)bt.y);
+                    tg[2] = __dsub_rn((double)at.z, (double)bt.z);
                 }
             }
         }
