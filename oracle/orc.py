@@ -26,7 +26,7 @@ _PU64 = ctypes.POINTER(ctypes.c_uint64)
 class OrcSystem(ctypes.Structure):
     _fields_ = [("n_mol", _I32), ("box", _D), ("m_O", _D), ("m_H", _D), ("inter_type", _I32),
                 ("coulomb_const", _D), ("crf_const", _D), ("cutoff", _D), ("nl_cutoff", _D),
-                ("n_steps_nf", _I32), ("kB", _D), ("temp", _D)]
+                ("n_steps_nf", _I32), ("kB", _D), ("temp", _D), ("mlp", _I32)]
 
 
 class OrcRdfTerm(ctypes.Structure):
@@ -50,7 +50,8 @@ class OrcSwLoss(ctypes.Structure):
 
 def build(force=False):
     """Compile the oracle with its Makefile (gcc, OpenMP, no FMA contraction)."""
-    srcs = ["revsim_oracle.c", "revsim_oracle.h", "sw_oracle.c", "sw_oracle.h"]
+    srcs = ["revsim_oracle.c", "revsim_oracle.h", "sw_oracle.c", "sw_oracle.h", "mlp_oracle.c",
+            "mlp_oracle.h"]
     if force or not os.path.exists(_LIB_PATH) or any(
             os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, f)) for f in srcs):
         subprocess.run(["make", "-s", "-C", _HERE, "-B" if force else "liborc_revsim.so"],
@@ -84,6 +85,14 @@ def lib():
                                       ctypes.POINTER(OrcLoss), _PD]
         L.orc_num_threads.restype = _I32
         L.orc_set_num_threads.argtypes = [_I32]
+        L.orc_system_n_params.restype = _I32
+        L.orc_system_n_params.argtypes = [ctypes.POINTER(OrcSystem)]
+        L.orc_contract.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64, _PD, _PD]
+        L.orc_mlp_nodes.argtypes = [_PD, _D, _PD, _PD]
+        L.orc_mlp_table.argtypes = [_PD, _D, _PD]
+        L.orc_mlp_pair.argtypes = [_PD, _I32, _D, _D, _PD, _PD, _PD]
+        L.orc_mlp_backprop.argtypes = [_PD, _D, _PD, _PD]
+        L.orc_mlp_init.argtypes = [ctypes.c_uint64, _PD]
         L.orc_vec1d.restype = _D
         L.orc_vec1d.argtypes = [_D, _D, _D]
         PS, PL = ctypes.POINTER(OrcSwSystem), ctypes.POINTER(OrcSwLoss)
@@ -120,11 +129,11 @@ INTER = {"lj": 0, "dexp": 1, "buck": 2, "ljsc": 3, "buff": 4}
 
 def make_system(n_mol, box, inter_type="lj", temp=295.15, *, m_O=15.99943, m_H=1.007947,
                 coulomb_const=138.93545764438196, crf_const=None, cutoff=1.0, nl_cutoff=1.2,
-                n_steps_nf=20, kB=0.00831446261815324):
+                n_steps_nf=20, kB=0.00831446261815324, mlp=False):
     if crf_const is None:
         crf_const = (1.0 / cutoff**3) * ((78.3 - 1) / (2 * 78.3 + 1))
     return OrcSystem(n_mol, box, m_O, m_H, INTER[inter_type], coulomb_const, crf_const, cutoff,
-                     nl_cutoff, n_steps_nf, kB, temp)
+                     nl_cutoff, n_steps_nf, kB, temp, 1 if mlp else 0)
 
 
 @dataclass
@@ -160,6 +169,10 @@ class Loss:
 
 
 def n_params(s):
+    return lib().orc_system_n_params(ctypes.byref(s))
+
+
+def n_classical_params(s):
     return lib().orc_n_params(s.inter_type)
 
 
@@ -183,9 +196,10 @@ def forces(s, params, x, pairs):
 
 
 def forces_grads(s, params, x, pairs, w, jac=True):
+    """F, the VJP and the Jacobian of the classical parameters."""
     x, p, w = _f64(x), _f64(params), _f64(w)
     pairs = np.ascontiguousarray(pairs, dtype=np.int32)
-    P = n_params(s)
+    P = n_classical_params(s)
     F = np.zeros(x.size)
     G = np.zeros(x.size)
     J = np.zeros(x.size * P) if jac else None
@@ -350,3 +364,52 @@ def sw_reverse_sim(s, theta, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_
                                    n_steps_trunc, len(sx), dt, _pd(sx), _pd(sv),
                                    ctypes.byref(loss), _pd(g))
     return x.reshape(-1, 3), v.reshape(-1, 3), val, g
+
+
+# --------------------------------------------------------------------------------------
+# Learned pair correction (mlp_oracle.c)
+
+MLP_NG, MLP_NT, MLP_H, MLP_NRBF = 1024, 3, 64, 16
+MLP_PER_TYPE = MLP_H * MLP_NRBF + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1
+MLP_NPARAMS = MLP_NT * MLP_PER_TYPE
+
+
+def contract(s, params, x, pairs, acoef):
+    """sum_a acoef_a . dF_a/dtheta for every parameter (classical, then MLP)."""
+    x, p, a = _f64(x), _f64(params), _f64(acoef)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    out = np.zeros(n_params(s))
+    lib().orc_contract(ctypes.byref(s), _pd(p), _pd(x), pairs.ctypes.data_as(_PI32), len(pairs),
+                       _pd(a), _pd(out))
+    return out
+
+
+def mlp_init(seed=3):
+    th = np.zeros(MLP_NPARAMS)
+    lib().orc_mlp_init(ctypes.c_uint64(seed), _pd(th))
+    return th
+
+
+def mlp_nodes(theta, rc=1.0):
+    u = np.zeros((MLP_NT, MLP_NG + 1))
+    du = np.zeros((MLP_NT, MLP_NG + 1))
+    lib().orc_mlp_nodes(_pd(_f64(theta)), rc, _pd(u), _pd(du))
+    return u, du
+
+
+def mlp_table(theta, rc=1.0):
+    c = np.zeros((MLP_NT, MLP_NG, 4))
+    lib().orc_mlp_table(_pd(_f64(theta)), rc, _pd(c))
+    return c
+
+
+def mlp_pair(coef, t, r, rc=1.0):
+    u, F, dF = _D(), _D(), _D()
+    lib().orc_mlp_pair(_pd(_f64(coef)), t, rc, r, ctypes.byref(u), ctypes.byref(F), ctypes.byref(dF))
+    return u.value, F.value, dF.value
+
+
+def mlp_backprop(theta, coef_adj, rc=1.0):
+    out = np.zeros(MLP_NPARAMS)
+    lib().orc_mlp_backprop(_pd(_f64(theta)), rc, _pd(_f64(coef_adj)), _pd(out))
+    return out

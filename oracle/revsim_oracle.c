@@ -10,6 +10,7 @@
  * Build: gcc -O2 -fPIC -shared -fopenmp -ffp-contract=off (oracle/Makefile).
  */
 #include "revsim_oracle.h"
+#include "mlp_oracle.h"
 
 #include <complex.h>
 #include <math.h>
@@ -54,6 +55,19 @@ int32_t orc_n_form_params(int32_t t) {
 int32_t orc_n_params(int32_t t) {
     int32_t n = orc_n_form_params(t);
     return n < 0 ? -1 : n + 5;
+}
+
+int32_t orc_system_n_params(const orc_system *s) {
+    int32_t n = orc_n_params(s->inter_type);
+    return n < 0 ? -1 : n + (s->mlp ? ORC_MLP_NPARAMS : 0);
+}
+
+/* The MLP's interval table for the parameters (NULL when the system has no MLP). */
+static double *mlp_table(const orc_system *s, const double *params) {
+    if (!s->mlp) return NULL;
+    double *coef = (double *)malloc(sizeof(double) * ORC_MLP_NT * ORC_MLP_NG * 4);
+    orc_mlp_table(params + orc_n_params(s->inter_type), s->cutoff, coef);
+    return coef;
 }
 
 /* Molly vector_1D: displacement c2 - c1 folded to the nearer image. */
@@ -360,7 +374,7 @@ static inline double mass(const orc_system *s, int64_t a) { return is_O(a) ? s->
 static void forces_core(const orc_system *s, const double *params, const double *x,
                         const int32_t *pairs, int64_t n_pairs, const double *wvec, int grads,
                         double *F, double *dl_dfi, double *dF_dp, const double *acoef,
-                        double *dl_dp) {
+                        double *dl_dp, const double *mlp_coef, double *mlp_adj) {
     const int64_t n = 3 * (int64_t)s->n_mol, n3 = 3 * n;
     const double L = s->box, rc2 = s->cutoff * s->cutoff;
     const double kc = s->coulomb_const, crf = s->crf_const;
@@ -373,6 +387,9 @@ static void forces_core(const orc_system *s, const double *params, const double 
     double *Gt = wvec ? (double *)calloc((size_t)n3 * nthr, sizeof(double)) : NULL;
     double *Pt = (double *)calloc((size_t)P * nthr, sizeof(double));
     double *Jt = dF_dp ? (double *)calloc((size_t)n3 * P * nthr, sizeof(double)) : NULL;
+    const size_t NA = (size_t)ORC_MLP_NT * ORC_MLP_NG * 4;
+    double *At = (mlp_coef && mlp_adj && acoef) ? (double *)calloc(NA * nthr, sizeof(double)) : NULL;
+    const double mlp_hinv = ORC_MLP_NG / s->cutoff;
 
 #pragma omp parallel
     {
@@ -385,6 +402,7 @@ static void forces_core(const orc_system *s, const double *params, const double 
         double *Gl = Gt ? Gt + (size_t)n3 * tid : NULL;
         double *Pl = Pt + (size_t)P * tid;
         double *Jl = Jt ? Jt + (size_t)n3 * P * tid : NULL;
+        double *Al = At ? At + NA * tid : NULL;
 
         /* Non-bonded: water.jl:892-913 (forces) and 1232-1277 (grads). */
 #pragma omp for schedule(static)
@@ -405,6 +423,20 @@ static void forces_core(const orc_system *s, const double *params, const double 
                 double Fp = 0.0, dFp = 0.0;
                 on = pair_form(s->inter_type, params, r, invr2, grads, &Fp, &dFp, g);
                 if (on) { Ftot += Fp; dFdr += dFp; }
+            }
+            int mt = 0, mg = 0;
+            double ms = 0.0;
+            if (mlp_coef) {
+                /* learned pair correction (mlp_oracle.h): types O-O, O-H, H-H */
+                double Fm, dFm;
+                mt = (is_O(i) ? 0 : 1) + (is_O(j) ? 0 : 1);
+                orc_mlp_pair(mlp_coef, mt, s->cutoff, r, NULL, &Fm, &dFm);
+                Ftot += Fm;
+                dFdr += dFm;
+                const double q = r * mlp_hinv;
+                mg = (int)floor(q);
+                if (mg > ORC_MLP_NG - 1) mg = ORC_MLP_NG - 1;
+                ms = q - mg;
             }
             double *Fi = Fl + 3 * i, *Fj = Fl + 3 * j;
             for (int u = 0; u < 3; u++) {
@@ -434,6 +466,13 @@ static void forces_core(const orc_system *s, const double *params, const double 
                 if (on)
                     for (int p = 0; p < nf; p++) Pl[p] += g[p] * t;
                 Pl[iq] += gq * t;
+                if (Al) {
+                    /* F = -(c1 + 2 c2 s + 3 c3 s^2) / h on interval mg */
+                    double *ca = Al + ((size_t)mt * ORC_MLP_NG + mg) * 4;
+                    ca[1] += -mlp_hinv * t;
+                    ca[2] += -2.0 * ms * mlp_hinv * t;
+                    ca[3] += -3.0 * ms * ms * mlp_hinv * t;
+                }
             }
             if (Jl) {
                 for (int u = 0; u < 3; u++) {
@@ -570,6 +609,10 @@ static void forces_core(const orc_system *s, const double *params, const double 
     if (dl_dp)
         for (int t = 0; t < nthr; t++)
             for (int p = 0; p < P; p++) dl_dp[p] += Pt[(size_t)P * t + p];
+    if (At)
+        for (int t = 0; t < nthr; t++)
+            for (size_t k = 0; k < NA; k++) mlp_adj[k] += At[NA * t + k];
+    free(At);
     free(Ft);
     free(Gt);
     free(Pt);
@@ -578,13 +621,31 @@ static void forces_core(const orc_system *s, const double *params, const double 
 
 void orc_forces(const orc_system *s, const double *params, const double *x,
                 const int32_t *pairs, int64_t n_pairs, double *F) {
-    forces_core(s, params, x, pairs, n_pairs, NULL, 0, F, NULL, NULL, NULL, NULL);
+    double *coef = mlp_table(s, params);
+    forces_core(s, params, x, pairs, n_pairs, NULL, 0, F, NULL, NULL, NULL, NULL, coef, NULL);
+    free(coef);
 }
 
 void orc_forces_grads(const orc_system *s, const double *params, const double *x,
                       const int32_t *pairs, int64_t n_pairs, const double *w,
                       double *F, double *dl_dfi, double *dF_dp) {
-    forces_core(s, params, x, pairs, n_pairs, w, 1, F, dl_dfi, dF_dp, NULL, NULL);
+    double *coef = mlp_table(s, params);
+    forces_core(s, params, x, pairs, n_pairs, w, 1, F, dl_dfi, dF_dp, NULL, NULL, coef, NULL);
+    free(coef);
+}
+
+void orc_contract(const orc_system *s, const double *params, const double *x,
+                  const int32_t *pairs, int64_t n_pairs, const double *acoef, double *dtheta) {
+    const int Pc = orc_n_params(s->inter_type), Pt = orc_system_n_params(s);
+    double *coef = mlp_table(s, params);
+    double *adj = coef ? (double *)calloc((size_t)ORC_MLP_NT * ORC_MLP_NG * 4, sizeof(double)) : NULL;
+    double *F = (double *)malloc(sizeof(double) * 9 * (size_t)s->n_mol);
+    for (int p = 0; p < Pt; p++) dtheta[p] = 0.0;
+    forces_core(s, params, x, pairs, n_pairs, NULL, 1, F, NULL, NULL, acoef, dtheta, coef, adj);
+    if (coef) orc_mlp_backprop(params + Pc, s->cutoff, adj, dtheta + Pc);
+    free(F);
+    free(coef);
+    free(adj);
 }
 
 /* Potential energy: pair form + reaction-field Coulomb (Molly CoulombReactionField:
@@ -594,6 +655,7 @@ double orc_energy(const orc_system *s, const double *params, const double *x,
     const double L = s->box, rc = s->cutoff, rc2 = rc * rc;
     const double crf = s->crf_const, c_rf = 1.0 / rc + crf * rc * rc;
     const wparams w = unpack(s, params);
+    double *coef = mlp_table(s, params);
     double E = 0.0;
     for (int64_t ni = 0; ni < n_pairs; ni++) {
         int64_t i = pairs[2 * ni], j = pairs[2 * ni + 1];
@@ -604,7 +666,13 @@ double orc_energy(const orc_system *s, const double *params, const double *x,
         double r = sqrt(r2);
         E += s->coulomb_const * charge(&w, i) * charge(&w, j) * (1.0 / r + crf * r2 - c_rf);
         if (is_O(i) && is_O(j)) E += pair_form_energy(s->inter_type, params, r);
+        if (coef) {
+            double um;
+            orc_mlp_pair(coef, (is_O(i) ? 0 : 1) + (is_O(j) ? 0 : 1), rc, r, &um, NULL, NULL);
+            E += um;
+        }
     }
+    free(coef);
     for (int64_t m = 0; m < s->n_mol; m++) {
         const double *xo = x + 9 * m;
         for (int h = 1; h <= 2; h++) {
@@ -886,6 +954,7 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
     int64_t cap = 16 * n + 1024;
     int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * (size_t)cap);
     int64_t np = rebuild_pairs(s, x, &pairs, &cap);
+    double *coef = mlp_table(s, params);
     if (snap_x) {
         memcpy(snap_x, x, sizeof(double) * (size_t)n3);
         memcpy(snap_v, v, sizeof(double) * (size_t)n3);
@@ -893,7 +962,7 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
     double loss_accum = 0.0;
     /* water.jl:1029-1045 */
     for (int32_t step = 1; step <= n_steps; step++) {
-        orc_forces(s, params, x, pairs, np, F);
+        forces_core(s, params, x, pairs, np, NULL, 0, F, NULL, NULL, NULL, NULL, coef, NULL);
         for (int64_t a = 0; a < n; a++) {
             double m = mass(s, a);
             for (int u = 0; u < 3; u++) v[3 * a + u] = v[3 * a + u] + F[3 * a + u] * dt / m;
@@ -911,6 +980,7 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
         }
         if (calc_loss && loss && step % n_steps_loss == 0) loss_accum += orc_loss_grad(s, loss, x, NULL);
     }
+    free(coef);
     free(F);
     free(xi);
     free(pairs);
@@ -940,7 +1010,9 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
     const double c = exp(-gamma * dt), sn = sqrt(1 - c * c);
     const double dt2 = dt * dt;
     const int32_t n_blocks = n_steps / n_steps_loss;
-    const int P = orc_n_params(s->inter_type);
+    const int P = orc_system_n_params(s), Pc = orc_n_params(s->inter_type);
+    double *coef = mlp_table(s, params);
+    double *adj = coef ? (double *)calloc((size_t)ORC_MLP_NT * ORC_MLP_NG * 4, sizeof(double)) : NULL;
     double *buf = (double *)calloc((size_t)n3 * 9, sizeof(double));
     double *F = buf, *xi = buf + n3, *g = buf + 2 * n3, *A = buf + 3 * n3, *B = buf + 4 * n3;
     double *C = buf + 5 * n3, *Dd = buf + 6 * n3, *dl_dfi = buf + 7 * n3, *acoef = buf + 8 * n3;
@@ -970,7 +1042,7 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
                 double m = mass(s, a);
                 for (int u = 0; u < 3; u++) acoef[3 * a + u] = A[3 * a + u] * (dt2 / (2 * m));
             }
-            forces_core(s, params, x, pairs, np, C, 1, F, dl_dfi, NULL, acoef, dl_dp);
+            forces_core(s, params, x, pairs, np, C, 1, F, dl_dfi, NULL, acoef, dl_dp, coef, adj);
             /* part 2, water.jl:1511-1521 */
             double nrm = 0.0;
             for (int64_t e = 0; e < n3; e++) nrm += dl_dfi[e] * dl_dfi[e];
@@ -998,7 +1070,10 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
             reset_accums(n3, c, g, A, B, C, Dd, dl_dfi);
         }
     }
+    if (coef) orc_mlp_backprop(params + Pc, s->cutoff, adj, dl_dp + Pc);
     for (int p = 0; p < P; p++) dl_dp[p] /= n_blocks;
+    free(coef);
+    free(adj);
     free(buf);
     free(pairs);
     return loss_accum / n_blocks;

@@ -52,6 +52,8 @@ typedef struct {
     int32_t n_steps_nf;    /* neighbour rebuild period (20) */
     double kB;             /* u nm^2 ps^-2 K^-1 */
     double temp;           /* K */
+    int32_t mlp;           /* 1: add the learned pair correction of mlp_oracle.h; its
+                              ORC_MLP_NPARAMS parameters follow the classical ones */
 } orc_system;
 
 /* One smoothed-RDF loss term (water.jl:631-711).  The grid is
@@ -76,6 +78,8 @@ typedef struct {
 
 int32_t orc_n_form_params(int32_t inter_type);
 int32_t orc_n_params(int32_t inter_type);
+/* Classical parameters plus the MLP's when s->mlp. */
+int32_t orc_system_n_params(const orc_system *s);
 
 /* Minimum-image component of Molly's vector(c1, c2): c2 - c1 folded by one box. */
 double orc_vec1d(double c1, double c2, double L);
@@ -91,11 +95,16 @@ void orc_forces(const orc_system *s, const double *params, const double *x,
                 const int32_t *pairs, int64_t n_pairs, double *F);
 
 /* calc_F_and_grads! (water.jl:1212-1433): forces F[3N], the force VJP
- * dl_dfi[b] = sum_a (w[a]/m_a) . dF_a/dx_b with w = dl_dfi_prev, and the full
- * parameter Jacobian dF_dp[3N * P] (row-major, index (3a+u)*P + p). dF_dp may be NULL. */
+ * dl_dfi[b] = sum_a (w[a]/m_a) . dF_a/dx_b with w = dl_dfi_prev, and the parameter
+ * Jacobian of the classical parameters dF_dp[3N * P] (row-major, index (3a+u)*P + p,
+ * P = orc_n_params).  dF_dp may be NULL. */
 void orc_forces_grads(const orc_system *s, const double *params, const double *x,
                       const int32_t *pairs, int64_t n_pairs, const double *w,
                       double *F, double *dl_dfi, double *dF_dp);
+
+/* sum_a acoef_a . dF_a/dtheta for every parameter (classical and MLP): dtheta[P]. */
+void orc_contract(const orc_system *s, const double *params, const double *x,
+                  const int32_t *pairs, int64_t n_pairs, const double *acoef, double *dtheta);
 
 /* Potential energy (pair form + reaction-field Coulomb + bonds + angles). */
 double orc_energy(const orc_system *s, const double *params, const double *x,
