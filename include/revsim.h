@@ -71,7 +71,18 @@ typedef struct {
     int32_t n_steps_log;    /* forward snapshot period, steps */
     int32_t nl_mode;        /* REVSIM_NL_CHECKPOINT or REVSIM_NL_RECONSTRUCTED */
     int32_t device;         /* CUDA device ordinal */
+    int32_t mlp;            /* 1: add the learned pair correction (REVSIM_LJ only); its
+                               REVSIM_MLP_NPARAMS parameters follow the classical ones */
 } revsim_system_desc;
+
+/* The learned pair correction (no reference counterpart; it takes the place of the
+ * reference's PyTorch / JAX learned terms, water_maceoff.jl:147-163): per element pair
+ * (O-O, O-H, H-H) of different molecules within the cutoff, u(r) = MLP(phi(r)) fc(r) with
+ * 16 Gaussian radial basis functions (centres k rc/15, width 0.05 nm), 64 -> 64 SiLU ->
+ * scalar, fc(r) = (cos(pi r / rc) + 1) / 2, tabulated on 1,024 intervals of [0, rc] and
+ * interpolated with cubic Hermite segments.  Parameters per type: W1[64][16], b1[64],
+ * W2[64][64], b2[64], w3[64], b3. */
+#define REVSIM_MLP_NPARAMS 15939
 
 /* One smoothed-RDF loss term (rdf_differentiable + loss_rdf_part, water.jl:631-697):
  * grid x_k = x_min + step*k, k < n_grid; Gaussian exp(-(x-d)^2/width) truncated at

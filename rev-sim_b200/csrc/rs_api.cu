@@ -62,7 +62,12 @@ struct revsim_handle {
     double mO = 0, mH = 0, ke = 0, krf = 0, rc = 0, rc_nl = 0, kB = 0;
 
     std::vector<double> theta;
-    int P = 0, NFp = 0;
+    int P = 0, NFp = 0;   // classical parameter count (the step kernels' partials)
+    int Pt = 0;           // all parameters: classical, then the MLP's when mlp
+    bool mlp = false;
+    double *d_mlp_theta = nullptr, *d_mlp_adj = nullptr, *d_mlp_scratch = nullptr,
+           *d_mlp_grad = nullptr;
+    void *d_mlp_tab = nullptr;
     bool have_params = false, have_state = false;
 
     // Launch shapes of the step kernels, [0] reverse and [1] forward, each with its own
@@ -209,6 +214,9 @@ NbConsts<R> nb_consts(const revsim_handle *h) {
             break;
         }
     }
+    nb.mlp_tab = h->d_mlp_tab;
+    nb.mlp_adj = h->d_mlp_adj;
+    nb.mlp_hinv = (R)(MLP_NG / h->rc);
     return nb;
 }
 
@@ -266,11 +274,11 @@ int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a_in) {
     }
     cudaError_t e;
     if (h->prec == REVSIM_MIXED)
-        e = launch_step<float>(rev, h->form, sh.G, sh.U, h->shift_ok, sh.n_blk, threads, a,
-                               nb_consts<float>(h), bc, h->st);
+        e = launch_step<float>(rev, h->mlp ? (int)F_LJ_MLP : h->form, sh.G, sh.U, h->shift_ok, sh.n_blk,
+                               threads, a, nb_consts<float>(h), bc, h->st);
     else
-        e = launch_step<double>(rev, h->form, sh.G, sh.U, h->shift_ok, sh.n_blk, threads, a,
-                                nb_consts<double>(h), bc, h->st);
+        e = launch_step<double>(rev, h->mlp ? (int)F_LJ_MLP : h->form, sh.G, sh.U, h->shift_ok, sh.n_blk,
+                                threads, a, nb_consts<double>(h), bc, h->st);
     h->launches++;
     if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("step kernel: ") + cudaGetErrorString(e));
     if (timed) {
@@ -546,6 +554,12 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     return REVSIM_OK;
 }
 
+int mlp_zero_adj(revsim_handle *h) {
+    if (!h->mlp || !h->d_mlp_adj) return REVSIM_OK;
+    CK(cudaMemsetAsync(h->d_mlp_adj, 0, sizeof(double) * (size_t)h->R * MLP_NT * MLP_NG * 4, h->st));
+    return REVSIM_OK;
+}
+
 int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, int n_steps_trunc,
                  double dt, double clip) {
     const double c = std::exp(-gamma * dt), s = std::sqrt(1 - c * c);
@@ -554,6 +568,7 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     const bool clipping = std::isfinite(clip);
     int rc;
     CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
+    if (int rc_ = mlp_zero_adj(h)) return rc_;
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
     if ((rc = loss_dev(h, true, h->d_loss_acc))) return rc;
     CK(launch_init_adjoint(h->N, h->d_dLdx, c, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->st));
@@ -693,6 +708,8 @@ void free_all(revsim_handle *h) {
         dfree(sh.d_blk_mol0);
         dfree(sh.d_blk_nmol);
     }
+    void *mptrs[] = {h->d_mlp_theta, h->d_mlp_adj, h->d_mlp_scratch, h->d_mlp_grad, h->d_mlp_tab};
+    for (void *p : mptrs) dfree(p);
     void *ptrs[] = {h->d_mol_rep, h->d_atom_rep,
                     h->d_rep_atom0, h->d_rep_nmol, h->d_rep_box, h->d_rep_sdO, h->d_rep_sdH,
                     h->d_rep_nc, h->d_rep_cell_off, h->d_cell_of_mol, h->d_cell_cnt, h->d_cell_start,
@@ -762,6 +779,9 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
     h->dev = d->device;
     h->NFp = form_nparams(h->form);
     h->P = h->NFp + 5;
+    h->mlp = d->mlp != 0;
+    if (h->mlp && h->form != REVSIM_LJ) return bad("the learned pair correction needs REVSIM_LJ");
+    h->Pt = h->P + (h->mlp ? MLP_NPARAMS : 0);
     h->shift_ok = true;
     for (int r = 0; r < h->R; r++)
         if (!(h->box[r] > 2 * (h->rc + 2 * kRext) + 0.02)) h->shift_ok = false;
@@ -876,17 +896,68 @@ int32_t revsim_device_status(revsim_handle *h, int32_t *flags) {
 int32_t revsim_sizes(const revsim_handle *h, int64_t *n_atoms, int32_t *n_params) {
     if (!h) return REVSIM_ERR_BADARG;
     if (n_atoms) *n_atoms = h->N;
-    if (n_params) *n_params = h->P;
+    if (n_params) *n_params = h->Pt;
     return REVSIM_OK;
 }
 
+namespace {
+// Upload the MLP parameters and rebuild the interval table.
+int set_mlp(revsim_handle *h, const double *theta_mlp) {
+    const size_t adj = (size_t)h->R * MLP_NT * MLP_NG * 4;
+    if (!h->d_mlp_theta) {
+        CK(dalloc(&h->d_mlp_theta, MLP_NPARAMS));
+        CK(dalloc(&h->d_mlp_adj, adj));
+        CK(dalloc(&h->d_mlp_scratch, mlp_scratch_doubles()));
+        CK(dalloc(&h->d_mlp_grad, (size_t)h->R * MLP_NPARAMS));
+        CK(dalloc((double **)&h->d_mlp_tab, (size_t)MLP_NT * MLP_NG * 4));
+        CK(cudaMemset(h->d_mlp_adj, 0, sizeof(double) * adj));
+    }
+    CK(cudaMemcpyAsync(h->d_mlp_theta, theta_mlp, sizeof(double) * MLP_NPARAMS, cudaMemcpyHostToDevice, h->st));
+    cudaError_t e = launch_mlp_table(h->prec, h->d_mlp_theta, h->rc, h->d_mlp_scratch, h->d_mlp_tab, h->st);
+    h->launches += 2;
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP table: ") + cudaGetErrorString(e));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
+// The accumulated interval-coefficient adjoints of every replica -> dtheta_mlp [R][MLP_NPARAMS].
+int mlp_grads(revsim_handle *h, std::vector<double> &out) {
+    for (int r = 0; r < h->R; r++) {
+        cudaError_t e = launch_mlp_backprop(h->d_mlp_theta, h->rc, h->d_mlp_adj + (size_t)r * MLP_NT * MLP_NG * 4,
+                                            h->d_mlp_scratch, h->d_mlp_grad + (size_t)r * MLP_NPARAMS, h->st);
+        h->launches += 3;
+        if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP backprop: ") + cudaGetErrorString(e));
+    }
+    out.resize((size_t)h->R * MLP_NPARAMS);
+    CK(cudaMemcpyAsync(out.data(), h->d_mlp_grad, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
+// Classical sums [R][P] and MLP gradients [R][MLP_NPARAMS] -> out [R][Pt], times scale.
+void join_grads(const revsim_handle *h, const std::vector<double> &cl, const std::vector<double> &ml,
+                double scale, double *out) {
+    for (int r = 0; r < h->R; r++) {
+        for (int p = 0; p < h->P; p++) out[(size_t)r * h->Pt + p] = cl[(size_t)r * h->P + p] * scale;
+        if (h->mlp)
+            for (int p = 0; p < MLP_NPARAMS; p++)
+                out[(size_t)r * h->Pt + h->P + p] = ml[(size_t)r * MLP_NPARAMS + p] * scale;
+    }
+}
+}  // namespace
+
 int32_t revsim_set_params(revsim_handle *h, const double *theta, int32_t n) {
     if (!h || !theta) return REVSIM_ERR_BADARG;
-    if (n != h->P) return fail(h, REVSIM_ERR_BADARG, "wrong parameter count");
+    if (n != h->Pt) return fail(h, REVSIM_ERR_BADARG, "wrong parameter count");
     for (int i = 0; i < n; i++)
         if (!std::isfinite(theta[i])) return fail(h, REVSIM_ERR_BADARG, "non-finite parameter");
     if (theta[h->NFp] == 0.0) return fail(h, REVSIM_ERR_BADARG, "q_O must be non-zero");
-    h->theta.assign(theta, theta + n);
+    if (h->mlp) {
+        CK(cudaSetDevice(h->dev));
+        int rc = set_mlp(h, theta + h->P);
+        if (rc) return rc;
+    }
+    h->theta.assign(theta, theta + h->P);
     h->have_params = true;
     return REVSIM_OK;
 }
@@ -1011,6 +1082,7 @@ int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef,
     if ((rc = build_nlist_checked(h, h->d_x))) return rc;
     if ((rc = pack(h, 0, true))) return rc;
     CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
+    if ((rc = mlp_zero_adj(h))) return rc;
     StepArgs a = base_args(h, true);
     a.pos_in = h->d_pos[0];
     a.wgt_in = h->d_wgt[0];
@@ -1021,9 +1093,10 @@ int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef,
     if ((rc = launch_step_k(h, true, a))) return rc;
     if (F) CK(cudaMemcpyAsync(F, h->d_F, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->st));
     if (dl_dfi) CK(cudaMemcpyAsync(dl_dfi, h->d_G, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->st));
-    std::vector<double> th;
+    std::vector<double> th, thm;
     if ((rc = reduce_part(h, th))) return rc;
-    if (dtheta) std::memcpy(dtheta, th.data(), sizeof(double) * th.size());
+    if (h->mlp && (rc = mlp_grads(h, thm))) return rc;
+    if (dtheta) join_grads(h, th, thm, 1.0, dtheta);
     int s;
     if ((rc = read_status(h, &s))) return rc;
     return status_code(h, s);
@@ -1134,10 +1207,10 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
     if ((rc = read_status(h, &s))) return rc;
     if ((rc = status_code(h, s))) return rc;
     const int n_blocks = n_steps / n_steps_loss;
-    std::vector<double> th;
+    std::vector<double> th, thm;
     if ((rc = reduce_part(h, th))) return rc;
-    if (dl_dp_out)
-        for (size_t i = 0; i < th.size(); i++) dl_dp_out[i] = th[i] / n_blocks;
+    if (h->mlp && (rc = mlp_grads(h, thm))) return rc;
+    if (dl_dp_out) join_grads(h, th, thm, 1.0 / n_blocks, dl_dp_out);
     if (loss_out) {
         std::vector<double> l(h->R);
         CK(cudaMemcpy(l.data(), h->d_loss_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));

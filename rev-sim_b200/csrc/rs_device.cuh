@@ -115,7 +115,8 @@ __device__ __forceinline__ void atom_noise(uint64_t seed, uint32_t atom, double 
 // Radial pair force F(r) (positive = repulsive), dF/dr and dF/dtheta_p for the
 // O-O pair term (water.jl:160-407).  Only O carries the pair term in the water
 // model, so the mixing rules reduce to the O parameters themselves.
-enum Form { F_LJ = 0, F_DEXP = 1, F_BUCK = 2, F_LJSC = 3, F_BUFF = 4 };
+enum Form { F_LJ = 0, F_DEXP = 1, F_BUCK = 2, F_LJSC = 3, F_BUFF = 4,
+            F_LJ_MLP = 5 /* LJ plus the tabulated learned pair correction (rs_mlp.cu) */ };
 
 template <int FORM> struct FormInfo;
 template <> struct FormInfo<F_LJ> { static constexpr int NP = 2; };
@@ -123,6 +124,7 @@ template <> struct FormInfo<F_DEXP> { static constexpr int NP = 4; };
 template <> struct FormInfo<F_BUCK> { static constexpr int NP = 3; };
 template <> struct FormInfo<F_LJSC> { static constexpr int NP = 4; };
 template <> struct FormInfo<F_BUFF> { static constexpr int NP = 4; };
+template <> struct FormInfo<F_LJ_MLP> { static constexpr int NP = 2; };
 
 // Precomputed per-launch constants of a pair form (host fills them from theta).
 template <typename R>

@@ -9,6 +9,13 @@
 
 namespace rs {
 
+// Learned pair correction (rs_mlp.cu): 16 radial basis functions -> 64 -> 64 SiLU -> 1
+// per element pair (O-O, O-H, H-H), tabulated on MLP_NG intervals of [0, cutoff].
+constexpr int MLP_NRBF = 16, MLP_H = 64, MLP_NG = 1024, MLP_NT = 3;
+constexpr int MLP_PER_TYPE = MLP_H * MLP_NRBF + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1;
+constexpr int MLP_NPARAMS = MLP_NT * MLP_PER_TYPE;
+constexpr double MLP_WIDTH = 0.05;
+
 // Per-launch constants of the non-bonded terms, in pair precision R.
 template <typename R>
 struct NbConsts {
@@ -18,6 +25,11 @@ struct NbConsts {
     R rc2;        // cutoff^2
     R twoinvq;    // 2 / q_O  (dF_c/dq_O = 2 F_c / q_O, water.jl:1247)
     FormConsts<R> fc;
+    // F_LJ_MLP: interval table [MLP_NT][MLP_NG] of 4-vectors (cubic coefficients), the
+    // accumulators of their adjoints [R][MLP_NT][MLP_NG][4] (reverse), and MLP_NG / cutoff
+    const void *mlp_tab;
+    double *mlp_adj;
+    R mlp_hinv;
 };
 
 struct BondConsts {
@@ -97,6 +109,15 @@ template <typename R, int FORM>
 cudaError_t launch_form(bool rev, int G, int unroll, bool shift, int n_blk, int threads,
                         const StepArgs &a, const NbConsts<R> &nb, const BondConsts &bc,
                         cudaStream_t st);
+
+size_t mlp_scratch_doubles();
+// Node evaluation and interval table of the MLP for parameters theta (device, FP64).
+cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *scratch, void *tab,
+                             cudaStream_t st);
+// Interval-coefficient adjoints -> dtheta [MLP_NPARAMS] (after launch_mlp_table with the
+// same theta and scratch).
+cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, double *scratch,
+                                double *dtheta, cudaStream_t st);
 
 cudaError_t launch_pack(int N, int prec, const double *x, const double *C, double mO, double mH,
                         const int *atom_rep, const double *rep_box, void *pos, void *wgt,

@@ -152,6 +152,7 @@ cudaError_t launch_step(bool rev, int form, int G, int unroll, bool shift, int n
         case F_BUCK: return launch_form<R, F_BUCK>(rev, G, unroll, shift, n_blk, threads, a, nb, bc, st);
         case F_LJSC: return launch_form<R, F_LJSC>(rev, G, unroll, shift, n_blk, threads, a, nb, bc, st);
         case F_BUFF: return launch_form<R, F_BUFF>(rev, G, unroll, shift, n_blk, threads, a, nb, bc, st);
+        case F_LJ_MLP: return launch_form<R, F_LJ_MLP>(rev, G, unroll, shift, n_blk, threads, a, nb, bc, st);
     }
     return cudaErrorInvalidValue;
 }

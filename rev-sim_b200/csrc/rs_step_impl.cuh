@@ -221,8 +221,10 @@ template <typename R, int FORM, bool REV, int KA, int KB>
 __device__ __forceinline__ void pair_term(bool bit, R dx, R dy, R dz,
                                           const typename V4T<R>::T &wa,
                                           const typename V4T<R>::T &wb, const R ca[3],
-                                          const NbConsts<R> &nb, R f[3], R g[3], R *th) {
+                                          const NbConsts<R> &nb, R f[3], R g[3], R *th,
+                                          double *madj) {
     constexpr int NF = FormInfo<FORM>::NP;
+    constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
     const R r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
     const bool on = bit && r2 <= nb.rc2;
     const R z = on ? R(1) : R(0);
@@ -240,9 +242,26 @@ __device__ __forceinline__ void pair_term(bool bit, R dx, R dy, R dz,
     if (KA == 0 && KB == 0) {
         if (nb.fc.on) {
             R Ff, dFf = R(0);
-            pair_form<R, FORM, REV>(nb.fc, r, rinv, invr2, Ff, dFf, gf);
+            pair_form<R, PF, REV>(nb.fc, r, rinv, invr2, Ff, dFf, gf);
             F = xadd(F, Ff);
             if (REV) dF = xadd(dF, dFf);
+        }
+    }
+    // Learned pair correction: the cubic segment of interval gi of type QI (O-O, O-H,
+    // H-H), F = -u'(r) = -(c1 + 2 c2 s + 3 c3 s^2) / h, dF/dr = -(2 c2 + 6 c3 s) / h^2.
+    int gi = 0;
+    R sm = R(0);
+    if constexpr (FORM == F_LJ_MLP) {
+        using V4m = typename V4T<R>::T;
+        const R q = xmul(r, nb.mlp_hinv);
+        gi = min((int)q, MLP_NG - 1);
+        sm = xsub(q, (R)gi);
+        const V4m cf = reinterpret_cast<const V4m *>(nb.mlp_tab)[QI * MLP_NG + gi];
+        const R d1 = xmul(xfma(sm, xfma(xmul(R(3), sm), cf.w, xmul(R(2), cf.z)), cf.y), nb.mlp_hinv);
+        F = xsub(F, d1);
+        if (REV) {
+            const R d2 = xmul(xmul(xfma(xmul(R(6), sm), cf.w, xmul(R(2), cf.z)), nb.mlp_hinv), nb.mlp_hinv);
+            dF = xsub(dF, d2);
         }
     }
     const R Fr = xmul(xmul(F, rinv), z);
@@ -265,6 +284,16 @@ __device__ __forceinline__ void pair_term(bool bit, R dx, R dy, R dz,
             if (nb.fc.on) {
 #pragma unroll
                 for (int p = 0; p < NF; p++) th[p] = xfma(-gf[p], na, th[p]);
+            }
+        }
+        if constexpr (FORM == F_LJ_MLP) {
+            // -(dF/dc_k) (n . acoef_a) for the interval's coefficients c1, c2, c3
+            if (on) {
+                const double v = (double)na * (double)nb.mlp_hinv, s1 = (double)sm;
+                double *adj = madj + ((size_t)QI * MLP_NG + gi) * 4;
+                atomicAdd(adj + 1, v);
+                atomicAdd(adj + 2, 2.0 * s1 * v);
+                atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
             }
         }
     }
@@ -291,13 +320,13 @@ __device__ __forceinline__ void pair_row(uint32_t mask, const typename V4T<R>::T
                                          const typename V4T<R>::T &wa,
                                          const typename V4T<R>::T wb[3], const R ca[3],
                                          const R sh[3], R L, R invL, const NbConsts<R> &nb,
-                                         R f[3], R g[3], R *th) {
+                                         R f[3], R g[3], R *th, double *madj) {
 #define RS_SLOT(KB)                                                                             \
     pair_term<R, FORM, REV, KA, KB>((mask >> (3 * KA + KB)) & 1u,                               \
                                     slot_d<R, SHIFT>(pa.x, pb[KB].x, sh[0], L, invL),           \
                                     slot_d<R, SHIFT>(pa.y, pb[KB].y, sh[1], L, invL),           \
                                     slot_d<R, SHIFT>(pa.z, pb[KB].z, sh[2], L, invL), wa, wb[KB], \
-                                    ca, nb, f, g, th)
+                                    ca, nb, f, g, th, madj)
     RS_SLOT(0);
     RS_SLOT(1);
     RS_SLOT(2);
@@ -330,6 +359,8 @@ __global__ void __launch_bounds__(U == 3 ? 256 : 512) k_water_step(StepArgs a, N
     const R invL = (R)(1.0 / Ld);
     const V4 *__restrict__ pos = (const V4 *)a.pos_in;
     const V4 *__restrict__ wgt = (const V4 *)a.wgt_in;
+    // this replica's accumulator of the learned term's interval-coefficient adjoints
+    double *madj = FORM == F_LJ_MLP && REV ? nb.mlp_adj + (size_t)rep * MLP_NT * MLP_NG * 4 : nullptr;
 
     R f[3][3], g[3][3], th[NTH];
 #pragma unroll
@@ -394,11 +425,11 @@ __global__ void __launch_bounds__(U == 3 ? 256 : 512) k_water_step(StepArgs a, N
                 sh[2] = image_shift<R, SHIFT>(xsub(pbq[0].z, pa[0].z), L, hL);
             }
             pair_row<R, FORM, REV, SHIFT, 0>(mask, pa[0], pbq, wa[0], wbq, ca[0], sh, L, invL, nb, f[0],
-                                             g[0], th);
+                                             g[0], th, madj);
             pair_row<R, FORM, REV, SHIFT, 1>(mask, pa[1], pbq, wa[1], wbq, ca[1], sh, L, invL, nb, f[1],
-                                             g[1], th);
+                                             g[1], th, madj);
             pair_row<R, FORM, REV, SHIFT, 2>(mask, pa[2], pbq, wa[2], wbq, ca[2], sh, L, invL, nb, f[2],
-                                             g[2], th);
+                                             g[2], th, madj);
         };
         auto fetch = [&](uint32_t ent, V4 pbq[3], V4 wbq[3]) {
             const int J = (int)(ent & 0x7FFFFFu);

@@ -72,6 +72,7 @@ class SystemDesc(ctypes.Structure):
         ("n_steps_log", ctypes.c_int32),
         ("nl_mode", ctypes.c_int32),
         ("device", ctypes.c_int32),
+        ("mlp", ctypes.c_int32),
     ]
 
 

@@ -40,7 +40,7 @@ class Engine:
     def __init__(self, n_mol, box, temp=C.TEMP, inter_type="lj", precision="fp64",
                  nl_mode="checkpoint", device=0, n_steps_log=C.N_STEPS_LOG,
                  n_steps_nf=C.N_STEPS_NF, cutoff=C.DIST_CUTOFF, nl_cutoff=C.DIST_NEIGHBORS,
-                 coulomb_const=C.COULOMB_CONST, crf_const=None):
+                 coulomb_const=C.COULOMB_CONST, crf_const=None, mlp=False):
         self._L = _lib.load()
         n_mol = np.atleast_1d(np.asarray(n_mol, dtype=np.int32))
         R = len(n_mol)
@@ -52,11 +52,13 @@ class Engine:
         self.R = R
         self.inter_type = inter_type
         self.precision = precision
+        self.mlp = bool(mlp)
         self._keep = (n_mol, box, temp)
         desc = _lib.SystemDesc(
             R, n_mol.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), f64p(box), f64p(temp),
             C.INTER_TYPES[inter_type], PRECISION[precision], C.O_MASS, C.H_MASS, coulomb_const,
-            crf_const, cutoff, nl_cutoff, C.KB, n_steps_nf, n_steps_log, NL_MODE[nl_mode], device)
+            crf_const, cutoff, nl_cutoff, C.KB, n_steps_nf, n_steps_log, NL_MODE[nl_mode], device,
+            1 if mlp else 0)
         h = ctypes.c_void_p()
         rc = self._L.revsim_create(ctypes.byref(desc), ctypes.byref(h))
         if rc != 0:
