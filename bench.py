@@ -64,9 +64,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=10)
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
-    ap.add_argument("--workload", default="water", choices=["water", "diamond"],
+    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp"],
                     help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
-                         "carbon, 16 replicas of 8,000 atoms")
+                         "carbon, 16 replicas of 8,000 atoms; mlp: 895 waters with the learned "
+                         "pair correction, gradient throughput and a training comparison")
+    ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
+    ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
+    ap.add_argument("--train-steps-loss", type=int, default=500)
+    ap.add_argument("--train-trunc", type=int, default=200)
     ap.add_argument("--replicas", type=int, default=16, help="diamond replicas")
     ap.add_argument("--cells", type=int, default=10, help="diamond conventional cells per side")
     ap.add_argument("--sw-steps", type=int, default=2000)
@@ -726,9 +731,168 @@ def run_ours_diamond(a):
         dist.destroy_process_group()
 
 
+# ----------------------------------------------------------------- MLP workload
+# Extra work of the learned pair correction per interacting pair (interval index and
+# coordinate, cubic derivative; reverse also the second derivative and the coefficient
+# adjoints): forward 12, reverse 24 flops.
+MLP_FLOPS_FWD_EXTRA, MLP_FLOPS_REV_EXTRA = 12, 24
+
+
+def mlp_config(a, extra=None):
+    c = {"workload": f"water_895mol_3nm_lj+mlp_{a.precision}_1000fwd+1000rev",
+         "n_atoms": 2685, "box_nm": 3.0, "n_steps": 1000, "n_steps_loss": 1000,
+         "n_steps_trunc": 1000, "dt_ps": 0.001, "gamma_per_ps": 0.0,
+         "learned_term": "per element pair (O-O, O-H, H-H) MLP 16 RBF (0-1 nm, width 0.05 nm) "
+                         "-> 64 -> 64 SiLU -> 1, cosine cutoff, 15,939 parameters, seeded "
+                         "Xavier init; tabulated on 1,024 intervals, cubic Hermite per pair",
+         "loss": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs sigma x1.02 / eps x0.95 target",
+         "training": f"{a.updates} Adam updates per arm, {a.train_steps} steps per update, loss "
+                     f"every {a.train_steps_loss}, truncation {a.train_trunc}, gamma 1/ps; "
+                     "classical lr 2e-3 x |theta_0| (the reference's scaled Adam), MLP lr 1e-3",
+         "precision": a.precision, "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_ours_mlp(a):
+    """Config 4: the 895-water system with the learned pair correction.  Timed: the full
+    gradient (1,000 forward + 1,000 reverse steps) with the MLP on.  Then a training
+    comparison, wall-clock timed: the classical + MLP model and the classical model alone,
+    each trained for the same number of Adam updates from the same start."""
+    import ctypes
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    import build as _build
+    _build.build()
+    from revsim import Engine, _lib, mlp, oo_l2_term, systems
+    a.n_mol, a.box, a.form = 895, 3.0, "lj"
+    x0, v0, p, target = prepare(a, local, a.equil_ps)
+    theta0 = np.concatenate([p, mlp.init_params(3)])
+    eng = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=True)
+    eng.set_params(theta0)
+    eng.set_loss([oo_l2_term(target)])
+    seeds = systems.noise_seeds(1000, seed=300 + rank)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def gradient(e=eng):
+        e.set_state(x0, v0)
+        lf = e.forward(seeds, 0.0, 1000, 1000, 0.001)
+        lr, g = e.reverse(seeds, 0.0, 1000, 1000, 1000, 0.001)
+        return lf, lr, g
+
+    for _ in range(a.warmup):
+        gradient()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lf, lr, g = gradient()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    clocks = clk.summary()
+    ms_step = sum(times) / a.steps
+    value = world * 2685 * 1000 / (ms_step * 1e-3)
+    h2d = 2 * 3 * 2685 * 8 + 2 * 1000 * 8
+    d2h = 8 * 2 + 8 * len(theta0)
+
+    # roofline: the reverse step kernel with the learned term
+    eng.set_kernel_timing(True)
+    gradient()
+    kt_ms, kt_n = eng.kernel_time(0)
+    eng.set_kernel_timing(False)
+    launch_ms = kt_ms / max(kt_n, 1)
+    xs, _ = eng.get_state()
+    pairs = eng.neighbor_pairs(0)
+    ipairs, _ = count_ipairs(xs, 3.0, pairs)
+    flops_launch = (FLOPS_REV_IPAIR + MLP_FLOPS_REV_EXTRA) * ipairs
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "kernel": "k_water_step<float, LJ_MLP, reverse>", "launch_ms": launch_ms,
+                "ipairs": ipairs, "flops_per_launch": flops_launch,
+                "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)"}
+
+    # accuracy: mixed vs FP64 GPU gradient over the first 100 steps
+    e64 = Engine(895, 3.0, inter_type="lj", precision="fp64", device=local, mlp=True)
+    e64.set_params(theta0)
+    e64.set_loss([oo_l2_term(target)])
+    short = {}
+    for e_, key in ((eng, "mixed"), (e64, "fp64")):
+        e_.set_state(x0, v0)
+        e_.forward(seeds[:100], 0.0, 100, 100, 0.001)
+        short[key] = e_.reverse(seeds[:100], 0.0, 100, 100, 100, 0.001)[1][0]
+    gm, g64 = short["mixed"], short["fp64"]
+    nc = len(p)
+    scl = np.abs(g64[:nc] * p)
+    err_cl = float(np.max(np.abs((gm[:nc] - g64[:nc]) * p) / np.maximum(scl, 0.01 * scl.max())))
+    err_mlp = float(np.abs(gm[nc:] - g64[nc:]).max() / np.abs(g64[nc:]).max())
+    e64.close()
+
+    # training comparison (same start, same seeds per update)
+    train = {}
+    for arm, use_mlp in (("classical", False), ("classical+mlp", True)):
+        e_ = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=use_mlp)
+        th = np.array(theta0 if use_mlp else p)
+        e_.set_loss([oo_l2_term(target)])
+        state = {"x": x0, "v": v0}
+        # the dynamics continue across updates (the forward end state starts the next one)
+        losses = []
+        scale = np.full(len(th), 1e-3)
+        scale[:len(p)] = 2e-3 * np.abs(p)
+        opt = mlp.Adam(len(th), lr=scale)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for u in range(a.updates):
+            e_.set_params(th)
+            e_.set_state(state["x"], state["v"])
+            sd = systems.noise_seeds(a.train_steps, seed=5000 + u)
+            l_u = e_.forward(sd, 1.0, a.train_steps, a.train_steps_loss, 0.001)
+            state["x"], state["v"] = e_.get_state()
+            _, gr = e_.reverse(sd, 1.0, a.train_steps, a.train_steps_loss, a.train_trunc, 0.001)
+            losses.append(float(l_u[0]))
+            th = opt.step(th, gr[0])
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e_.close()
+        k = max(1, a.updates // 10)
+        train[arm] = {"wall_s": wall, "loss_first": float(np.mean(losses[:k])),
+                      "loss_last": float(np.mean(losses[-k:])), "updates": a.updates,
+                      "loss_curve_every_10": [float(np.mean(losses[i:i + 10]))
+                                              for i in range(0, len(losses), 10)]}
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+           "data": "synthetic", "config": mlp_config(a),
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None,
+           "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])},
+           "grad_rel_err_vs_fp64_first_100_steps": {"classical": err_cl, "mlp": err_mlp},
+           "training": train,
+           "e2e_note": "every timed gradient starts from host arrays (set_state), so value is "
+                       "end to end"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    eng.close()
+
+
 if __name__ == "__main__":
     args = parse()
-    if args.workload == "diamond":
+    if args.workload == "mlp":
+        run_ours_mlp(args)
+    elif args.workload == "diamond":
         run_reference_diamond(args) if args.impl == "reference" else run_ours_diamond(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -556,7 +556,7 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
 
 int mlp_zero_adj(revsim_handle *h) {
     if (!h->mlp || !h->d_mlp_adj) return REVSIM_OK;
-    CK(cudaMemsetAsync(h->d_mlp_adj, 0, sizeof(double) * (size_t)h->R * MLP_NT * MLP_NG * 4, h->st));
+    CK(cudaMemsetAsync(h->d_mlp_adj, 0, sizeof(double) * (size_t)h->R * MLP_NCOPY * MLP_NT * MLP_NG * 4, h->st));
     return REVSIM_OK;
 }
 
@@ -903,7 +903,7 @@ int32_t revsim_sizes(const revsim_handle *h, int64_t *n_atoms, int32_t *n_params
 namespace {
 // Upload the MLP parameters and rebuild the interval table.
 int set_mlp(revsim_handle *h, const double *theta_mlp) {
-    const size_t adj = (size_t)h->R * MLP_NT * MLP_NG * 4;
+    const size_t adj = (size_t)h->R * MLP_NCOPY * MLP_NT * MLP_NG * 4;
     if (!h->d_mlp_theta) {
         CK(dalloc(&h->d_mlp_theta, MLP_NPARAMS));
         CK(dalloc(&h->d_mlp_adj, adj));
@@ -923,7 +923,8 @@ int set_mlp(revsim_handle *h, const double *theta_mlp) {
 // The accumulated interval-coefficient adjoints of every replica -> dtheta_mlp [R][MLP_NPARAMS].
 int mlp_grads(revsim_handle *h, std::vector<double> &out) {
     for (int r = 0; r < h->R; r++) {
-        cudaError_t e = launch_mlp_backprop(h->d_mlp_theta, h->rc, h->d_mlp_adj + (size_t)r * MLP_NT * MLP_NG * 4,
+        cudaError_t e = launch_mlp_backprop(h->d_mlp_theta, h->rc,
+                                            h->d_mlp_adj + (size_t)r * MLP_NCOPY * MLP_NT * MLP_NG * 4, MLP_NCOPY,
                                             h->d_mlp_scratch, h->d_mlp_grad + (size_t)r * MLP_NPARAMS, h->st);
         h->launches += 3;
         if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP backprop: ") + cudaGetErrorString(e));

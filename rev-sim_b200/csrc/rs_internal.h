@@ -15,6 +15,9 @@ constexpr int MLP_NRBF = 16, MLP_H = 64, MLP_NG = 1024, MLP_NT = 3;
 constexpr int MLP_PER_TYPE = MLP_H * MLP_NRBF + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1;
 constexpr int MLP_NPARAMS = MLP_NT * MLP_PER_TYPE;
 constexpr double MLP_WIDTH = 0.05;
+// Copies of the coefficient-adjoint accumulator per replica; CTA b adds into copy
+// b % MLP_NCOPY, which spreads the atomics of the many pairs that share an interval.
+constexpr int MLP_NCOPY = 16;
 
 // Per-launch constants of the non-bonded terms, in pair precision R.
 template <typename R>
@@ -26,7 +29,8 @@ struct NbConsts {
     R twoinvq;    // 2 / q_O  (dF_c/dq_O = 2 F_c / q_O, water.jl:1247)
     FormConsts<R> fc;
     // F_LJ_MLP: interval table [MLP_NT][MLP_NG] of 4-vectors (cubic coefficients), the
-    // accumulators of their adjoints [R][MLP_NT][MLP_NG][4] (reverse), and MLP_NG / cutoff
+    // accumulators of their adjoints [R][MLP_NCOPY][MLP_NT][MLP_NG][4] (reverse), and
+    // MLP_NG / cutoff
     const void *mlp_tab;
     double *mlp_adj;
     R mlp_hinv;
@@ -114,10 +118,10 @@ size_t mlp_scratch_doubles();
 // Node evaluation and interval table of the MLP for parameters theta (device, FP64).
 cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *scratch, void *tab,
                              cudaStream_t st);
-// Interval-coefficient adjoints -> dtheta [MLP_NPARAMS] (after launch_mlp_table with the
-// same theta and scratch).
-cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, double *scratch,
-                                double *dtheta, cudaStream_t st);
+// Interval-coefficient adjoints (the sum of ncopy accumulators) -> dtheta [MLP_NPARAMS]
+// (after launch_mlp_table with the same theta and scratch).
+cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, int ncopy,
+                                double *scratch, double *dtheta, cudaStream_t st);
 
 cudaError_t launch_pack(int N, int prec, const double *x, const double *C, double mO, double mH,
                         const int *atom_rep, const double *rep_box, void *pos, void *wgt,

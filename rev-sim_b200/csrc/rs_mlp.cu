@@ -120,20 +120,32 @@ __global__ void k_mlp_coef(const double *u, const double *du, double rc, V4 *tab
     tab[k] = c;
 }
 
-// Coefficient adjoints -> node value / derivative adjoints (the transpose of k_mlp_coef).
-__global__ void k_mlp_adj_nodes(const double *cadj, double rc, double *au, double *ad) {
+// Coefficient adjoints (summed over the ncopy accumulators in order) -> node value /
+// derivative adjoints (the transpose of k_mlp_coef).
+__device__ __forceinline__ void sum_copies(const double *cadj, int ncopy, size_t off, double c[4]) {
+    c[0] = c[1] = c[2] = c[3] = 0.0;
+    for (int q = 0; q < ncopy; q++) {
+        const double *p = cadj + (size_t)q * MLP_NT * NG * 4 + off;
+        c[0] += p[0];
+        c[1] += p[1];
+        c[2] += p[2];
+        c[3] += p[3];
+    }
+}
+
+__global__ void k_mlp_adj_nodes(const double *cadj, int ncopy, double rc, double *au, double *ad) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= MLP_NT * (NG + 1)) return;
     const int t = k / (NG + 1), g = k % (NG + 1);
     const double h = rc / NG;
-    double a = 0.0, d = 0.0;
+    double a = 0.0, d = 0.0, c[4];
     if (g < NG) {
-        const double *c = cadj + ((size_t)t * NG + g) * 4;
+        sum_copies(cadj, ncopy, ((size_t)t * NG + g) * 4, c);
         a += c[0] - 3.0 * c[2] + 2.0 * c[3];
         d += h * (c[1] - 2.0 * c[2] + c[3]);
     }
     if (g > 0) {
-        const double *c = cadj + ((size_t)t * NG + g - 1) * 4;
+        sum_copies(cadj, ncopy, ((size_t)t * NG + g - 1) * 4, c);
         a += 3.0 * c[2] - 2.0 * c[3];
         d += h * (c[3] - c[2]);
     }
@@ -232,12 +244,12 @@ cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *s
     return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, double *scratch,
-                                double *dtheta, cudaStream_t st) {
+cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, int ncopy,
+                                double *scratch, double *dtheta, cudaStream_t st) {
     const size_t S = (size_t)MLP_NT * (NG + 1) * NA, NN = (size_t)MLP_NT * (NG + 1);
     double *act = scratch, *bwd = scratch + S;
     double *au = scratch + 2 * S + 2 * NN, *ad = au + NN;
-    k_mlp_adj_nodes<<<(int)((NN + 255) / 256), 256, 0, st>>>(cadj, rc, au, ad);
+    k_mlp_adj_nodes<<<(int)((NN + 255) / 256), 256, 0, st>>>(cadj, ncopy, rc, au, ad);
     k_mlp_node_bwd<<<dim3(NG + 1, MLP_NT), 64, 0, st>>>(theta, act, au, ad, bwd);
     k_mlp_wgrad<<<(MLP_NPARAMS + 127) / 128, 128, 0, st>>>(rc, act, bwd, dtheta);
     return cudaGetLastError();

@@ -360,7 +360,9 @@ __global__ void __launch_bounds__(U == 3 ? 256 : 512) k_water_step(StepArgs a, N
     const V4 *__restrict__ pos = (const V4 *)a.pos_in;
     const V4 *__restrict__ wgt = (const V4 *)a.wgt_in;
     // this replica's accumulator of the learned term's interval-coefficient adjoints
-    double *madj = FORM == F_LJ_MLP && REV ? nb.mlp_adj + (size_t)rep * MLP_NT * MLP_NG * 4 : nullptr;
+    double *madj = FORM == F_LJ_MLP && REV
+                       ? nb.mlp_adj + ((size_t)rep * MLP_NCOPY + (blk % MLP_NCOPY)) * MLP_NT * MLP_NG * 4
+                       : nullptr;
 
     R f[3][3], g[3][3], th[NTH];
 #pragma unroll
