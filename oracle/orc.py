@@ -85,6 +85,8 @@ def lib():
                                       ctypes.POINTER(OrcLoss), _PD]
         L.orc_num_threads.restype = _I32
         L.orc_set_num_threads.argtypes = [_I32]
+        L.orc_energy_grads.restype = _D
+        L.orc_energy_grads.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64, _PD]
         L.orc_system_n_params.restype = _I32
         L.orc_system_n_params.argtypes = [ctypes.POINTER(OrcSystem)]
         L.orc_contract.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64, _PD, _PD]
@@ -212,6 +214,16 @@ def energy(s, params, x, pairs):
     x, p = _f64(x), _f64(params)
     pairs = np.ascontiguousarray(pairs, dtype=np.int32)
     return lib().orc_energy(ctypes.byref(s), _pd(p), _pd(x), pairs.ctypes.data_as(_PI32), len(pairs))
+
+
+def energy_grads(s, params, x, pairs):
+    """(E, dE/dtheta [P]) at x."""
+    x, p = _f64(x), _f64(params)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    g = np.zeros(n_params(s))
+    E = lib().orc_energy_grads(ctypes.byref(s), _pd(p), _pd(x), pairs.ctypes.data_as(_PI32),
+                               len(pairs), _pd(g))
+    return E, g
 
 
 def noise(s, seed, temp=None):

@@ -286,6 +286,41 @@ static double pair_form_energy(int type, const double *p, double r) {
     return 0.0;
 }
 
+/* The pair-form energies on complex parameters (the same expressions as
+ * pair_form_energy): dE/dtheta_k = Im E(theta + i h e_k) / h, exact to rounding. */
+static double complex cpow6(double complex z) {
+    double complex z2 = z * z;
+    return z2 * z2 * z2;
+}
+
+static double complex pair_form_energy_c(int type, const double complex *p, double r) {
+    switch (type) {
+        case ORC_LJ: {
+            double complex sr6 = cpow6(p[0] / r);
+            return 4 * p[1] * (sr6 * sr6 - sr6);
+        }
+        case ORC_DEXP: {
+            double complex rm = p[0] * two_pow_1o6, al = p[2], be = p[3];
+            double complex k1 = be * cexp(al) / (al - be), k2 = al * cexp(be) / (al - be);
+            return p[1] * (k1 * cexp(-al * r / rm) - k2 * cexp(-be * r / rm));
+        }
+        case ORC_BUCK:
+            return p[0] * cexp(-p[1] * r) - p[2] / pow(r, 6);
+        case ORC_LJSC: {
+            double complex s6 = cpow6(p[0]);
+            double complex six = s6 / (pow(r, 6) + s6 * p[2] * p[3] * p[3]);
+            return 4 * p[1] * (six * six - six);
+        }
+        case ORC_BUFF: {
+            double complex rm = p[0] * two_pow_1o6, d = p[2], gm = p[3];
+            double complex s = r / rm, b = (1 + d) / (s + d);
+            double complex b7 = cpow6(b) * b, s7 = cpow6(s) * s;
+            return p[1] * b7 * ((1 + gm) / (s7 + gm) - 2);
+        }
+    }
+    return 0.0;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Forward-mode dual numbers for the angle-term Jacobian-vector product.  The
  * Hessian of a potential is symmetric, so J w (tangent of the force along w)
@@ -650,6 +685,78 @@ void orc_contract(const orc_system *s, const double *params, const double *x,
 
 /* Potential energy: pair form + reaction-field Coulomb (Molly CoulombReactionField:
  * k q_i q_j (1/r + k_rf r^2 - c_rf), c_rf = 1/rc + k_rf rc^2) + bonds + angles. */
+double orc_energy_grads(const orc_system *s, const double *params, const double *x,
+                        const int32_t *pairs, int64_t n_pairs, double *dEdp) {
+    const double L = s->box, rc = s->cutoff, rc2 = rc * rc;
+    const double crf = s->crf_const, c_rf = 1.0 / rc + crf * rc * rc;
+    const wparams w = unpack(s, params);
+    const int Pc = w.P, Pt = orc_system_n_params(s), nf = w.nf;
+    double *coef = mlp_table(s, params);
+    double *adj = coef ? (double *)calloc((size_t)ORC_MLP_NT * ORC_MLP_NG * 4, sizeof(double)) : NULL;
+    const double hinv = ORC_MLP_NG / rc, ch = 1e-30;
+    for (int p = 0; p < Pt; p++) dEdp[p] = 0.0;
+    double E = 0.0;
+    for (int64_t ni = 0; ni < n_pairs; ni++) {
+        int64_t i = pairs[2 * ni], j = pairs[2 * ni + 1];
+        double dr[3];
+        vec3(x + 3 * i, x + 3 * j, L, dr);
+        double r2 = sumsq3(dr);
+        if (!(r2 <= rc2)) continue;
+        double r = sqrt(r2);
+        double Ec = s->coulomb_const * charge(&w, i) * charge(&w, j) * (1.0 / r + crf * r2 - c_rf);
+        E += Ec;
+        dEdp[nf] += 2.0 * Ec / w.qO;
+        if (is_O(i) && is_O(j)) {
+            E += pair_form_energy(s->inter_type, params, r);
+            /* the reference's iszero gate (eps, or A for Buckingham) switches the form off */
+            if (params[s->inter_type == ORC_BUCK ? 0 : 1] != 0.0)
+                for (int k = 0; k < nf; k++) {
+                    double complex pc[4];
+                    for (int q = 0; q < nf; q++) pc[q] = params[q] + (q == k ? I * ch : 0.0);
+                    dEdp[k] += cimag(pair_form_energy_c(s->inter_type, pc, r)) / ch;
+                }
+        }
+        if (coef) {
+            const int t = (is_O(i) ? 0 : 1) + (is_O(j) ? 0 : 1);
+            double um;
+            orc_mlp_pair(coef, t, rc, r, &um, NULL, NULL);
+            E += um;
+            const double q = r * hinv;
+            int g = (int)floor(q);
+            if (g > ORC_MLP_NG - 1) g = ORC_MLP_NG - 1;
+            const double sv = q - g;
+            double *ca = adj + ((size_t)t * ORC_MLP_NG + g) * 4;
+            ca[0] += 1.0;
+            ca[1] += sv;
+            ca[2] += sv * sv;
+            ca[3] += sv * sv * sv;
+        }
+    }
+    for (int64_t m = 0; m < s->n_mol; m++) {
+        const double *xo = x + 9 * m;
+        for (int h = 1; h <= 2; h++) {
+            double dr[3];
+            vec3(xo, xo + 3 * h, L, dr);
+            double d = sqrt(sumsq3(dr)) - w.r0;
+            E += 0.5 * w.kb * d * d;
+            dEdp[nf + 1] += 0.5 * d * d;
+            dEdp[nf + 2] += -w.kb * d;
+        }
+        double a[3], b[3];
+        vec3(xo, xo + 3, L, a);
+        vec3(xo, xo + 6, L, b);
+        double c = (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]) / (sqrt(sumsq3(a)) * sqrt(sumsq3(b)));
+        double th = acos(c) - w.th0;
+        E += 0.5 * w.ka * th * th;
+        dEdp[nf + 3] += 0.5 * th * th;
+        dEdp[nf + 4] += -w.ka * th;
+    }
+    if (coef) orc_mlp_backprop(params + Pc, rc, adj, dEdp + Pc);
+    free(coef);
+    free(adj);
+    return E;
+}
+
 double orc_energy(const orc_system *s, const double *params, const double *x,
                   const int32_t *pairs, int64_t n_pairs) {
     const double L = s->box, rc = s->cutoff, rc2 = rc * rc;

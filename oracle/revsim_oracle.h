@@ -106,6 +106,11 @@ void orc_forces_grads(const orc_system *s, const double *params, const double *x
 void orc_contract(const orc_system *s, const double *params, const double *x,
                   const int32_t *pairs, int64_t n_pairs, const double *acoef, double *dtheta);
 
+/* Potential energy and its parameter gradient dEdp[P] (classical, then the MLP's): the
+ * per-snapshot dE/dtheta of the reweighting estimator (water.jl:1176-1183). */
+double orc_energy_grads(const orc_system *s, const double *params, const double *x,
+                        const int32_t *pairs, int64_t n_pairs, double *dEdp);
+
 /* Potential energy (pair form + reaction-field Coulomb + bonds + angles). */
 double orc_energy(const orc_system *s, const double *params, const double *x,
                   const int32_t *pairs, int64_t n_pairs);
