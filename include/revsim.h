@@ -138,6 +138,11 @@ int32_t revsim_forces(revsim_handle *h, double *F);
 int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef, double *F,
                          double *dl_dfi, double *dtheta);
 
+/* The potential energy energy[n_replicas] and its parameter gradient dEdtheta
+ * [n_replicas * P] at the current state (the Zygote gradient of potential_energy in
+ * reweighting_sim, water.jl:1176-1183).  Either output may be NULL. */
+int32_t revsim_energy_grad(revsim_handle *h, double *energy, double *dEdtheta);
+
 /* generate_noise! (water.jl:867-873) for one step seed per replica: xi [3 n_atoms]. */
 int32_t revsim_noise(revsim_handle *h, const uint64_t *seeds, double *xi);
 

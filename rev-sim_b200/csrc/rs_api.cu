@@ -68,6 +68,7 @@ struct revsim_handle {
     double *d_mlp_theta = nullptr, *d_mlp_adj = nullptr, *d_mlp_scratch = nullptr,
            *d_mlp_grad = nullptr;
     void *d_mlp_tab = nullptr;
+    double *d_epart = nullptr;   // [M][P + 1] energy-gradient partials
     bool have_params = false, have_state = false;
 
     // Launch shapes of the step kernels, [0] reverse and [1] forward, each with its own
@@ -708,7 +709,8 @@ void free_all(revsim_handle *h) {
         dfree(sh.d_blk_mol0);
         dfree(sh.d_blk_nmol);
     }
-    void *mptrs[] = {h->d_mlp_theta, h->d_mlp_adj, h->d_mlp_scratch, h->d_mlp_grad, h->d_mlp_tab};
+    void *mptrs[] = {h->d_mlp_theta, h->d_mlp_adj, h->d_mlp_scratch, h->d_mlp_grad, h->d_mlp_tab,
+                     h->d_epart};
     for (void *p : mptrs) dfree(p);
     void *ptrs[] = {h->d_mol_rep, h->d_atom_rep,
                     h->d_rep_atom0, h->d_rep_nmol, h->d_rep_box, h->d_rep_sdO, h->d_rep_sdH,
@@ -1098,6 +1100,59 @@ int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef,
     if ((rc = reduce_part(h, th))) return rc;
     if (h->mlp && (rc = mlp_grads(h, thm))) return rc;
     if (dtheta) join_grads(h, th, thm, 1.0, dtheta);
+    int s;
+    if ((rc = read_status(h, &s))) return rc;
+    return status_code(h, s);
+}
+
+int32_t revsim_energy_grad(revsim_handle *h, double *energy, double *dEdtheta) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    CK(cudaSetDevice(h->dev));
+    if ((rc = build_nlist_checked(h, h->d_x))) return rc;
+    if ((rc = mlp_zero_adj(h))) return rc;
+    if (!h->d_epart) CK(dalloc(&h->d_epart, (size_t)h->M * (h->P + 1)));
+    EnergyArgs a;
+    a.M = h->M;
+    a.P = h->P;
+    a.cap = h->cap;
+    a.x = h->d_x;
+    a.mol_rep = h->d_mol_rep;
+    a.rep_box = h->d_rep_box;
+    a.nbr = h->d_nbr;
+    a.nbr_cnt = h->d_nbr_cnt;
+    a.rc2 = h->rc * h->rc;
+    a.ke = h->ke;
+    a.krf = h->krf;
+    a.crf_shift = 1.0 / h->rc + h->krf * h->rc * h->rc;
+    const double *t = h->theta.data();
+    a.qO = t[h->NFp];
+    a.kb = t[h->NFp + 1];
+    a.r0 = t[h->NFp + 2];
+    a.ka = t[h->NFp + 3];
+    a.th0 = t[h->NFp + 4];
+    for (int k = 0; k < 4; k++) a.form_p[k] = k < h->NFp ? t[k] : 0.0;
+    a.mlp_tab = h->d_mlp_tab;
+    a.mlp_adj = h->mlp ? h->d_mlp_adj : nullptr;
+    a.mlp_hinv = MLP_NG / h->rc;
+    a.part = h->d_epart;
+    cudaError_t e = launch_energy_grads(h->mlp ? (int)F_LJ_MLP : h->form, h->prec, a, h->st);
+    h->launches++;
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("energy gradient: ") + cudaGetErrorString(e));
+    std::vector<double> part((size_t)h->M * (h->P + 1));
+    std::vector<int> mol_rep(h->M);
+    CK(cudaMemcpyAsync(part.data(), h->d_epart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(mol_rep.data(), h->d_mol_rep, sizeof(int) * h->M, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    std::vector<double> E(h->R, 0.0), cl((size_t)h->R * h->P, 0.0), ml;
+    for (int I = 0; I < h->M; I++) {
+        const int r = mol_rep[I];
+        E[r] += part[(size_t)I * (h->P + 1)];
+        for (int p = 0; p < h->P; p++) cl[(size_t)r * h->P + p] += part[(size_t)I * (h->P + 1) + 1 + p];
+    }
+    if (h->mlp && (rc = mlp_grads(h, ml))) return rc;
+    if (energy) std::memcpy(energy, E.data(), sizeof(double) * h->R);
+    if (dEdtheta) join_grads(h, cl, ml, 1.0, dEdtheta);
     int s;
     if ((rc = read_status(h, &s))) return rc;
     return status_code(h, s);

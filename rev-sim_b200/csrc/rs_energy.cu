@@ -1,0 +1,180 @@
+// rs_energy.cu -- potential energy and its parameter gradient at the current state: the
+// per-snapshot dE/dtheta of the reweighting estimator (reweighting_sim, water.jl:1107-1210;
+// the Zygote gradient of potential_energy at water.jl:1176-1183).  FP64, once per loss point.
+//
+// One thread per molecule I sums the molecule pairs (I, J > I) of its neighbour row (each
+// unordered pair once; the row's 9-bit mask gives the listed atom pairs), the pair-form
+// energy on dual numbers whose tangents are the form's parameters, the reaction-field
+// Coulomb energy (dE/dq_O = 2 E_c / q_O), its own two bonds and angle, and -- with the
+// learned term -- the interval-coefficient adjoints (1, s, s^2, s^3) of each pair's Hermite
+// segment, which the MLP backpropagation turns into dE/dtheta_mlp.  Per-molecule partials
+// [E, dE/dtheta...] are summed per replica on the host in molecule order.
+#include "rs_internal.h"
+
+namespace rs {
+
+namespace {
+
+template <int K>
+using DN = DualN<double, K>;
+
+template <int K>
+__device__ __forceinline__ DN<K> dexp_(const DN<K> &a) {
+    DN<K> r;
+    r.v = exp(a.v);
+#pragma unroll
+    for (int k = 0; k < K; k++) r.d[k] = r.v * a.d[k];
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ DN<K> pow6(const DN<K> &a) {
+    const DN<K> a2 = a * a;
+    return a2 * a2 * a2;
+}
+
+// Pair-form energy (the expressions of Molly's LennardJones, water.jl's DoubleExponential,
+// Buckingham, LennardJonesSoftCore and Buffered147 energies) with tangents = form parameters.
+template <int FORM>
+__device__ DN<4> form_energy(const double *p, double r) {
+    DN<4> P[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) P[k] = dn_var<double, 4>(p[k], k);
+    const DN<4> one = dn_const<double, 4>(1.0), R = dn_const<double, 4>(r);
+    constexpr double c216 = 1.122462048309373;
+    if (FORM == F_LJ || FORM == F_LJ_MLP) {
+        const DN<4> sr6 = pow6(P[0] / R);
+        return dn_const<double, 4>(4.0) * P[1] * (sr6 * sr6 - sr6);
+    } else if (FORM == F_DEXP) {
+        const DN<4> rm = P[0] * dn_const<double, 4>(c216);
+        const DN<4> k1 = P[3] * dexp_(P[2]) / (P[2] - P[3]), k2 = P[2] * dexp_(P[3]) / (P[2] - P[3]);
+        const DN<4> x = R / rm;
+        DN<4> na = P[2] * x, nb = P[3] * x;
+        na.v = -na.v;
+        nb.v = -nb.v;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            na.d[k] = -na.d[k];
+            nb.d[k] = -nb.d[k];
+        }
+        return P[1] * (k1 * dexp_(na) - k2 * dexp_(nb));
+    } else if (FORM == F_BUCK) {
+        DN<4> e = P[1] * R;
+        e.v = -e.v;
+#pragma unroll
+        for (int k = 0; k < 4; k++) e.d[k] = -e.d[k];
+        const double r6 = r * r * r * r * r * r;
+        return P[0] * dexp_(e) - P[2] / dn_const<double, 4>(r6);
+    } else if (FORM == F_LJSC) {
+        const double r6 = r * r * r * r * r * r;
+        const DN<4> s6 = pow6(P[0]);
+        const DN<4> six = s6 / (dn_const<double, 4>(r6) + s6 * P[2] * P[3] * P[3]);
+        return dn_const<double, 4>(4.0) * P[1] * (six * six - six);
+    } else {   // F_BUFF
+        const DN<4> rm = P[0] * dn_const<double, 4>(c216);
+        const DN<4> s = R / rm, b = (one + P[2]) / (s + P[2]);
+        const DN<4> b7 = pow6(b) * b, s7 = pow6(s) * s;
+        return P[1] * b7 * ((one + P[3]) / (s7 + P[3]) - dn_const<double, 4>(2.0));
+    }
+}
+
+template <int FORM, typename V4>
+__global__ void k_energy_grads(EnergyArgs a) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= a.M) return;
+    constexpr int NFm = FormInfo<FORM>::NP;
+    const int rep = a.mol_rep[I];
+    const double L = a.rep_box[rep];
+    const double *x = a.x;
+    const int P = a.P;   // classical parameters
+    double acc[1 + 16];
+#pragma unroll
+    for (int k = 0; k < 17; k++) acc[k] = 0.0;
+    const bool gate = a.form_p[FORM == F_BUCK ? 0 : 1] != 0.0;
+    const double qq[3] = {a.qO * a.qO, a.qO * (-0.5 * a.qO), 0.25 * a.qO * a.qO};
+    double *madj = a.mlp_adj ? a.mlp_adj + ((size_t)rep * MLP_NCOPY + (I % MLP_NCOPY)) * MLP_NT * MLP_NG * 4
+                             : nullptr;
+    const uint32_t *row = a.nbr + (size_t)I * a.cap;
+    const int cnt = min(a.nbr_cnt[I], a.cap);
+    for (int e = 0; e < cnt; e++) {
+        const uint32_t ent = row[e];
+        const int J = (int)(ent & 0x7FFFFFu);
+        if (J <= I) continue;
+        const uint32_t mask = ent >> 23;
+        for (int ka = 0; ka < 3; ka++)
+            for (int kb = 0; kb < 3; kb++) {
+                if (!((mask >> (3 * ka + kb)) & 1u)) continue;
+                const double *xi = x + 3 * (size_t)(3 * I + ka), *xj = x + 3 * (size_t)(3 * J + kb);
+                const double d0 = vec1d(xi[0], xj[0], L), d1 = vec1d(xi[1], xj[1], L), d2 = vec1d(xi[2], xj[2], L);
+                const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+                if (!(r2 <= a.rc2)) continue;
+                const double r = sqrt(r2);
+                const int QI = (ka > 0) + (kb > 0);
+                const double Ec = a.ke * qq[QI] * (1.0 / r + a.krf * r2 - a.crf_shift);
+                acc[0] += Ec;
+                acc[1 + NFm] += 2.0 * Ec / a.qO;
+                if (ka == 0 && kb == 0 && gate) {
+                    const DN<4> Ef = form_energy<FORM>(a.form_p, r);
+                    acc[0] += Ef.v;
+#pragma unroll
+                    for (int k = 0; k < NFm; k++) acc[1 + k] += Ef.d[k];
+                }
+                if (FORM == F_LJ_MLP && madj) {
+                    const double q = r * a.mlp_hinv;
+                    const int g = min((int)q, MLP_NG - 1);
+                    const double s = q - g;
+                    const V4 c = reinterpret_cast<const V4 *>(a.mlp_tab)[QI * MLP_NG + g];
+                    acc[0] += (double)c.x + s * ((double)c.y + s * ((double)c.z + s * (double)c.w));
+                    double *ad = madj + ((size_t)QI * MLP_NG + g) * 4;
+                    atomicAdd(ad, 1.0);
+                    atomicAdd(ad + 1, s);
+                    atomicAdd(ad + 2, s * s);
+                    atomicAdd(ad + 3, s * s * s);
+                }
+            }
+    }
+    // bonds (O, H1), (O, H2) and the angle H1-O-H2 (water.jl:915-968 energies)
+    const double *xo = x + 9 * (size_t)I;
+    double b[2][3];
+    for (int h = 0; h < 2; h++) {
+        for (int u = 0; u < 3; u++) b[h][u] = vec1d(xo[u], xo[3 * (h + 1) + u], L);
+        const double d = sqrt(b[h][0] * b[h][0] + b[h][1] * b[h][1] + b[h][2] * b[h][2]) - a.r0;
+        acc[0] += 0.5 * a.kb * d * d;
+        acc[1 + NFm + 1] += 0.5 * d * d;
+        acc[1 + NFm + 2] += -a.kb * d;
+    }
+    const double c = (b[0][0] * b[1][0] + b[0][1] * b[1][1] + b[0][2] * b[1][2]) /
+                     (sqrt(b[0][0] * b[0][0] + b[0][1] * b[0][1] + b[0][2] * b[0][2]) *
+                      sqrt(b[1][0] * b[1][0] + b[1][1] * b[1][1] + b[1][2] * b[1][2]));
+    const double th = acos(fmin(1.0, fmax(-1.0, c))) - a.th0;
+    acc[0] += 0.5 * a.ka * th * th;
+    acc[1 + NFm + 3] += 0.5 * th * th;
+    acc[1 + NFm + 4] += -a.ka * th;
+    for (int k = 0; k <= P; k++) a.part[(size_t)I * (P + 1) + k] = acc[k];
+}
+
+template <int FORM>
+cudaError_t launch_f(int prec, const EnergyArgs &a, cudaStream_t st) {
+    const int t = 128, b = (a.M + t - 1) / t;
+    if (prec == 1)
+        k_energy_grads<FORM, float4><<<b, t, 0, st>>>(a);
+    else
+        k_energy_grads<FORM, double4><<<b, t, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_energy_grads(int form, int prec, const EnergyArgs &a, cudaStream_t st) {
+    switch (form) {
+        case F_LJ: return launch_f<F_LJ>(prec, a, st);
+        case F_DEXP: return launch_f<F_DEXP>(prec, a, st);
+        case F_BUCK: return launch_f<F_BUCK>(prec, a, st);
+        case F_LJSC: return launch_f<F_LJSC>(prec, a, st);
+        case F_BUFF: return launch_f<F_BUFF>(prec, a, st);
+        case F_LJ_MLP: return launch_f<F_LJ_MLP>(prec, a, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace rs

@@ -114,6 +114,24 @@ cudaError_t launch_form(bool rev, int G, int unroll, bool shift, int n_blk, int 
                         const StepArgs &a, const NbConsts<R> &nb, const BondConsts &bc,
                         cudaStream_t st);
 
+// Potential energy and its parameter gradient (rs_energy.cu), one thread per molecule.
+struct EnergyArgs {
+    int M, P, cap;
+    const double *x;
+    const int *mol_rep;
+    const double *rep_box;
+    const uint32_t *nbr;
+    const int *nbr_cnt;
+    double rc2, ke, krf, crf_shift;   // crf_shift = 1/rc + k_rf rc^2
+    double qO, kb, r0, ka, th0;
+    double form_p[4];                 // pair-form parameters, zero-padded
+    const void *mlp_tab;              // F_LJ_MLP: interval table, adjoint accumulators, NG / rc
+    double *mlp_adj;
+    double mlp_hinv;
+    double *part;                     // [M][P + 1]: energy, then dE/dtheta (classical)
+};
+cudaError_t launch_energy_grads(int form, int prec, const EnergyArgs &a, cudaStream_t st);
+
 size_t mlp_scratch_doubles();
 // Node evaluation and interval table of the MLP for parameters theta (device, FP64).
 cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *scratch, void *tab,

@@ -13,10 +13,11 @@ from ._lib import EXPORTS, LIB_PATH, SW_EXPORTS, RevsimError, load
 from .engine import Engine, RdfTerm
 from .loss import oo_l2_term, read_rdf_data, reference_rdf_terms
 from .sw import SwEngine
-from .water import SimSystem, forward_sim, reverse_sim
+from .water import SimSystem, forward_sim, reverse_sim, reweighting_sim
 
 __all__ = [
-    "Engine", "RdfTerm", "RevsimError", "SimSystem", "forward_sim", "reverse_sim", "load",
+    "Engine", "RdfTerm", "RevsimError", "SimSystem", "forward_sim", "reverse_sim",
+    "reweighting_sim", "load",
     "constants", "systems", "oo_l2_term", "reference_rdf_terms", "read_rdf_data", "EXPORTS",
     "LIB_PATH", "SW_EXPORTS", "SwEngine", "diamond",
 ]

@@ -33,7 +33,7 @@ EXPORTS = [
     "revsim_noise", "revsim_loss_grad", "revsim_rdf", "revsim_forward", "revsim_reverse",
     "revsim_stream", "revsim_launch_count", "revsim_set_kernel_timing", "revsim_kernel_time",
     "revsim_set_launch_shape", "revsim_get_launch_shape", "revsim_autotune",
-    "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc",
+    "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc", "revsim_energy_grad",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -134,6 +134,7 @@ def load(path=LIB_PATH):
         "revsim_forces": (i32, [vp, pd]),
         "revsim_force_vjp": (i32, [vp, pd, pd, pd, pd, pd]),
         "revsim_noise": (i32, [vp, pu64, pd]),
+        "revsim_energy_grad": (i32, [vp, pd, pd]),
         "revsim_loss_grad": (i32, [vp, pd, pd]),
         "revsim_rdf": (i32, [vp, i32, i32, pd]),
         "revsim_forward": (i32, [vp, pu64, d, i32, i32, d, i32, pd]),

@@ -153,6 +153,13 @@ class Engine:
                                              f64p(th)))
         return F, G, th
 
+    def energy_grad(self):
+        """(E [R], dE/dtheta [R, n_params]) at the current state."""
+        E = np.zeros(self.R)
+        g = np.zeros((self.R, self.n_params))
+        self._check(self._L.revsim_energy_grad(self._h, f64p(E), f64p(g)))
+        return E, g
+
     def noise(self, seeds):
         seeds = np.ascontiguousarray(np.broadcast_to(np.asarray(seeds, dtype=np.uint64), (self.R,)))
         xi = np.zeros((self.n_atoms, 3))

@@ -1,6 +1,7 @@
 """The reference's gradient entry points, with the reference's signatures.
 
-``forward_sim`` mirrors water.jl:977-1105 and ``reverse_sim`` water.jl:1435-1558:
+``forward_sim`` mirrors water.jl:977-1105, ``reverse_sim`` water.jl:1435-1558 and
+``reweighting_sim`` water.jl:1107-1210:
 same positional arguments, same meaning, same return tuples, so a caller of the
 reference (the self-check block water.jl:1592-1621, ``train()`` water.jl:1662-1669)
 switches by changing the import.  The work runs in librevsim.so on the GPU.
@@ -105,6 +106,48 @@ def reverse_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
     else:
         l, dl_dp = loss, g
     return sys, l, dl_dp, l, 0.0 * l
+
+
+def reweighting_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss, params,
+                    dt, n_threads, inter_type, loss_type, use_barostat=False, *, loss_terms=None,
+                    engine=None, precision="fp64", temp=C.TEMP):
+    """water.jl:1107-1210: the ensemble-reweighting gradient estimator,
+    dL/dtheta = <dl/dtheta> - beta (<L dE/dtheta> - <L> <dE/dtheta>), averages over the loss
+    points (every n_steps_loss steps) of one forward run, beta = 1 / (k_B T).  The RDF loss has
+    no direct parameter dependence (dl/dtheta = 0).  Returns (sys, loss, grads, l_rdf, l_ev)."""
+    if use_barostat:
+        raise NotImplementedError("the Monte-Carlo barostat is not part of the engine")
+    _check_loss(loss_type)
+    eng = _engine_for(coords, boundary, inter_type, engine, precision)
+    eng.set_params(params)
+    eng.set_state(coords, velocities)
+    if loss_terms is not None:
+        eng.set_loss(loss_terms)
+    if not eng.terms:
+        raise ValueError("reweighting_sim needs loss_terms")
+    seeds = np.asarray(noise_seeds, dtype=np.uint64)
+    n_blocks = 1 if n_steps == 0 else n_steps // n_steps_loss
+    loss_acc = np.zeros(eng.R)
+    dE_acc = np.zeros((eng.R, eng.n_params))
+    l_dE_acc = np.zeros((eng.R, eng.n_params))
+    for b in range(n_steps // n_steps_loss):
+        # the forward run in blocks of n_steps_loss: the loss at each block's end is the
+        # reference's loss at step_n % n_steps_loss == 0 (water.jl:1168)
+        lb = eng.forward(seeds[b * n_steps_loss:(b + 1) * n_steps_loss], gamma, n_steps_loss,
+                         n_steps_loss, dt)
+        _, dE = eng.energy_grad()
+        loss_acc += lb
+        dE_acc += dE
+        l_dE_acc += lb[:, None] * dE
+    loss = loss_acc / n_blocks
+    beta = 1.0 / (C.KB * np.asarray(temp, dtype=np.float64))
+    beta = np.broadcast_to(beta, (eng.R,))[:, None]
+    grads = -beta * (l_dE_acc / n_blocks - loss[:, None] * dE_acc / n_blocks)
+    x, v = eng.get_state()
+    sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
+    if eng.R == 1:
+        return sys, float(loss[0]), grads[0], float(loss[0]), 0.0
+    return sys, loss, grads, loss, 0.0 * loss
 
 
 def default_params(inter_type="lj"):
