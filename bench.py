@@ -64,10 +64,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=10)
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
-    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp"],
+    ap.add_argument("--n-replicas", type=int, default=64, help="replicas workload: boxes")
+    ap.add_argument("--rep-steps", type=int, default=2000, help="replicas workload: steps")
+    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas"],
                     help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
                          "carbon, 16 replicas of 8,000 atoms; mlp: 895 waters with the learned "
-                         "pair correction, gradient throughput and a training comparison")
+                         "pair correction, gradient throughput and a training comparison; "
+                         "replicas: 64 water boxes of 300-3,000 molecules at 280-320 K in one launch")
     ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
@@ -775,6 +778,8 @@ def run_ours_mlp(a):
     eng = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=True)
     eng.set_params(theta0)
     eng.set_loss([oo_l2_term(target)])
+    eng.set_state(x0, v0)
+    shape = eng.autotune()
     seeds = systems.noise_seeds(1000, seed=300 + rank)
     stream = torch.cuda.ExternalStream(eng.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -832,6 +837,8 @@ def run_ours_mlp(a):
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value if peak.value else None, "traffic": None,
                 "kernel": "k_water_step<float, LJ_MLP, reverse>", "launch_ms": launch_ms,
+                "shape": {"reverse": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[0])),
+                          "forward": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[1]))},
                 "ipairs": ipairs, "flops_per_launch": flops_launch,
                 "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)"}
 
@@ -857,6 +864,9 @@ def run_ours_mlp(a):
         e_ = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=use_mlp)
         th = np.array(theta0 if use_mlp else p)
         e_.set_loss([oo_l2_term(target)])
+        e_.set_params(th)
+        e_.set_state(x0, v0)
+        e_.autotune()
         state = {"x": x0, "v": v0}
         # the dynamics continue across updates (the forward end state starts the next one)
         losses = []
@@ -898,9 +908,156 @@ def run_ours_mlp(a):
     eng.close()
 
 
+# ------------------------------------------------------------ replicas workload
+def replica_systems(n_rep, seed=2):
+    """Config 3: molecule counts log-uniform in [300, 3000] and temperatures uniform in
+    [280, 320] K from a seed; boxes at liquid density, at least 2.45 nm (the minimum image
+    of the 1.2 nm neighbour cutoff needs a side above 2.4 nm, so replicas under ~480
+    molecules are less dense)."""
+    from revsim import systems
+    rng = np.random.default_rng(seed)
+    n_mol = np.round(np.exp(rng.uniform(np.log(300), np.log(3000), n_rep))).astype(int)
+    temps = rng.uniform(280.0, 320.0, n_rep)
+    boxes = np.array([max(systems.box_for_density(n), 2.45) for n in n_mol])
+    return n_mol, boxes, temps
+
+
+def replicas_config(a, n_mol, extra=None):
+    c = {"workload": f"water_{a.n_replicas}replicas_{int(n_mol.sum())}mol_lj_{a.precision}_"
+                     f"{a.rep_steps}fwd+{a.rep_steps}rev",
+         "replicas": a.n_replicas, "n_mol_range": [int(n_mol.min()), int(n_mol.max())],
+         "n_atoms": int(3 * n_mol.sum()), "temp_K_range": [280, 320], "n_steps": a.rep_steps,
+         "n_steps_loss": 1000, "n_steps_trunc": 1000, "dt_ps": 0.001, "gamma_per_ps": 1.0,
+         "loss": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs the replica-mean RDF of a "
+                 "sigma x1.02 / eps x0.95 run; per-replica gradients averaged",
+         "launch": "all replicas in one launch per step (per-CTA replica table); not captured "
+                   "in a CUDA graph (the step kernels are GPU-bound)",
+         "precision": a.precision, "l2": "inputs larger than L2 are not guaranteed; flushed "
+                                         "(256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_ours_replicas(a):
+    """Config 3: 64 water boxes of uneven size and temperature in one handle; one bench step
+    = one batched gradient (forward + reverse) whose per-replica gradients are averaged."""
+    import ctypes
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    import build as _build
+    _build.build()
+    from revsim import Engine, _lib, constants as C, oo_l2_term, systems
+    n_mol, boxes, temps = replica_systems(a.n_replicas)
+    R, K = a.n_replicas, a.rep_steps
+    p = np.array(C.default_params("lj"))
+    x = np.concatenate([systems.water_coords(n, b, seed=10 + r) for r, (n, b) in enumerate(zip(n_mol, boxes))])
+    v = np.concatenate([systems.mb_velocities(n, t, seed=100 + r) for r, (n, t) in enumerate(zip(n_mol, temps))])
+    eq = Engine(n_mol, boxes, temp=temps, precision="mixed", device=local)
+    eq.set_params(p)
+    eq.set_state(x, v)
+    for blk in range(2):
+        eq.forward(systems.noise_seeds(1000 * R, seed=20 + blk).reshape(1000, R), 5.0, 1000, 1000,
+                   0.001, calc_loss=False)
+    x0, v0 = eq.get_state()
+    pt = p.copy()
+    pt[0] *= 1.02
+    pt[1] *= 0.95
+    eq.set_params(pt)
+    eq.forward(systems.noise_seeds(1000 * R, seed=30).reshape(1000, R), 5.0, 1000, 1000, 0.001,
+               calc_loss=False)
+    eq.set_loss([oo_l2_term(np.zeros(200))])
+    target = np.mean([eq.rdf(0, r) for r in range(R)], axis=0)
+    eq.close()
+    eng = Engine(n_mol, boxes, temp=temps, precision=a.precision, device=local)
+    eng.set_params(p)
+    eng.set_loss([oo_l2_term(target)])
+    eng.set_state(x0, v0)
+    shape = eng.autotune()
+    seeds = systems.noise_seeds(K * R, seed=400 + rank).reshape(K, R)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def gradient():
+        eng.set_state(x0, v0)
+        lf = eng.forward(seeds, 1.0, K, 1000, 0.001)
+        lr, g = eng.reverse(seeds, 1.0, K, 1000, 1000, 0.001)
+        return lf, lr, g.mean(axis=0)
+
+    if a.profile:
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        gradient()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        eng.close()
+        return
+    for _ in range(a.warmup):
+        gradient()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lf, lr, g = gradient()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    clocks = clk.summary()
+    ms_step = sum(times) / a.steps
+    n_atoms = int(3 * n_mol.sum())
+    value = world * n_atoms * K / (ms_step * 1e-3)
+    eng.set_kernel_timing(True)
+    gradient()
+    kt_ms, kt_n = eng.kernel_time(0)
+    ft_ms, ft_n = eng.kernel_time(1)
+    eng.set_kernel_timing(False)
+    launch_ms = kt_ms / max(kt_n, 1)
+    xs, _ = eng.get_state()
+    ipairs = 0
+    for r in range(R):
+        sl = slice(int(3 * n_mol[:r].sum()), int(3 * n_mol[:r + 1].sum()))
+        ipairs += count_ipairs(xs[sl], boxes[r], eng.neighbor_pairs(r))[0]
+    flops_launch = FLOPS_REV_IPAIR * ipairs
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "kernel": "k_water_step<float, LJ, reverse> over all 64 replicas",
+                "launch_ms": launch_ms, "ipairs": ipairs, "flops_per_launch": flops_launch,
+                "forward_step_launch_ms": ft_ms / max(ft_n, 1),
+                "shape": {"reverse": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[0])),
+                          "forward": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[1]))},
+                "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)"}
+    h2d = 2 * 3 * n_atoms * 8 + 2 * K * R * 8
+    d2h = 2 * R * 8 + R * len(p) * 8
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+           "data": "synthetic", "config": replicas_config(a, n_mol),
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None, "clocks": clocks,
+           "loss": {"forward_mean": float(lf.mean()), "reverse_mean": float(lr.mean())},
+           "mean_gradient": [float(t) for t in g],
+           "e2e_note": "every timed gradient starts from host arrays (set_state), so value is end to end"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    eng.close()
+
+
 if __name__ == "__main__":
     args = parse()
-    if args.workload == "mlp":
+    if args.workload == "replicas":
+        run_ours_replicas(args)
+    elif args.workload == "mlp":
         run_ours_mlp(args)
     elif args.workload == "diamond":
         run_reference_diamond(args) if args.impl == "reference" else run_ours_diamond(args)
