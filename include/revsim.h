@@ -150,6 +150,29 @@ int32_t revsim_noise(revsim_handle *h, const uint64_t *seeds, double *xi);
  * (dLdx may be NULL). */
 int32_t revsim_loss_grad(revsim_handle *h, double *loss, double *dLdx);
 
+/* The enthalpy-of-vaporisation loss term of loss_fn's loss_type :enth_vap and :both
+ * (enthalpy_vaporization / loss_enth_vap, water.jl:738-769): per replica
+ * l_ev = (u_gas - U / n_molecules + rt - target)^2, U the potential energy over a neighbour
+ * list built from the current positions, added to the RDF terms' loss (revsim_set_loss; no
+ * terms = :enth_vap) at every loss point of revsim_forward, revsim_reverse, revsim_loss_grad
+ * and revsim_loss_and_grads.  Its dL/dx is (2 e / n) F and its direct parameter gradient
+ * -(2 e / n) dU/dtheta, e = u_gas - U/n + rt - target, which revsim_reverse adds at every
+ * loss point (water.jl:1471, 1540).  enable 0 removes the term.  The reference's constants:
+ * u_gas 3.69, rt 2.45, target 44.12 + 2.8 kJ/mol.  No counterpart function in the
+ * reference, whose loss_type argument selects the same terms. */
+int32_t revsim_set_enth_vap(revsim_handle *h, int32_t enable, double u_gas, double rt, double target);
+
+/* The RDF and enthalpy parts [n_replicas] of the loss the last revsim_forward or
+ * revsim_reverse returned (loss_accum_rdf and loss_accum_ev over n_blocks, water.jl:1548-1551);
+ * zeros after a forward pass without loss.  Either output may be NULL. */
+int32_t revsim_loss_parts(revsim_handle *h, double *l_rdf, double *l_ev);
+
+/* loss_and_grads (water.jl:771-786) at the current state, all of its outputs: loss, l_rdf and
+ * l_ev [n_replicas], dl_dc = dL/dx [3 n_atoms] and the direct parameter gradient
+ * dl_dp [n_replicas][n_params] (zero without the enthalpy term).  Any output may be NULL. */
+int32_t revsim_loss_and_grads(revsim_handle *h, double *loss, double *l_rdf, double *l_ev,
+                              double *dLdx, double *dl_dp);
+
 /* One RDF histogram h [n_grid] of term t for one replica. */
 int32_t revsim_rdf(revsim_handle *h, int32_t term, int32_t replica, double *hist);
 

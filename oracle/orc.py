@@ -37,7 +37,8 @@ class OrcRdfTerm(ctypes.Structure):
 
 
 class OrcLoss(ctypes.Structure):
-    _fields_ = [("n_terms", _I32), ("terms", ctypes.POINTER(OrcRdfTerm))]
+    _fields_ = [("n_terms", _I32), ("terms", ctypes.POINTER(OrcRdfTerm)), ("enth_vap", _I32),
+                ("u_gas", _D), ("rt", _D), ("target", _D)]
 
 
 class OrcSwSystem(ctypes.Structure):
@@ -78,11 +79,15 @@ def lib():
         L.orc_loss_grad.argtypes = [ctypes.POINTER(OrcSystem), ctypes.POINTER(OrcLoss), _PD, _PD]
         L.orc_forward_sim.restype = _D
         L.orc_forward_sim.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PU64, _D, _I32,
-                                      _I32, _D, _I32, ctypes.POINTER(OrcLoss), _I32, _PD, _PD]
+                                      _I32, _D, _I32, ctypes.POINTER(OrcLoss), _I32, _PD, _PD,
+                                      _PD]
         L.orc_reverse_sim.restype = _D
         L.orc_reverse_sim.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PU64, _D, _I32,
                                       _I32, _I32, _D, _I32, _PD, _PD, _D,
-                                      ctypes.POINTER(OrcLoss), _PD]
+                                      ctypes.POINTER(OrcLoss), _PD, _PD]
+        L.orc_loss_and_grads.restype = _D
+        L.orc_loss_and_grads.argtypes = [ctypes.POINTER(OrcSystem), _PD, ctypes.POINTER(OrcLoss),
+                                         _PD, _PD, _PD, _PD]
         L.orc_num_threads.restype = _I32
         L.orc_set_num_threads.argtypes = [_I32]
         L.orc_energy_grads.restype = _D
@@ -163,11 +168,17 @@ class RdfTerm:
                           len(t), _pd(t), self.norm, self.weight)
 
 
+# loss_enth_vap constants (water.jl:740-753), kJ/mol
+ENTH_U_GAS, ENTH_RT, ENTH_TARGET = 3.69, 2.45, 44.12 + 2.8
+
+
 class Loss:
-    def __init__(self, terms):
+    """RDF terms plus, with ``enth_vap``, the enthalpy-of-vaporisation term."""
+
+    def __init__(self, terms, enth_vap=False, u_gas=ENTH_U_GAS, rt=ENTH_RT, target=ENTH_TARGET):
         self.terms = list(terms)
-        self._arr = (OrcRdfTerm * len(self.terms))(*[t.c() for t in self.terms])
-        self.c = OrcLoss(len(self.terms), self._arr)
+        self._arr = (OrcRdfTerm * max(len(self.terms), 1))(*[t.c() for t in self.terms])
+        self.c = OrcLoss(len(self.terms), self._arr, 1 if enth_vap else 0, u_gas, rt, target)
 
 
 def n_params(s):
@@ -248,30 +259,46 @@ def loss_grad(s, loss, x, grad=True):
     return val, (g.reshape(-1, 3) if grad else None)
 
 
+def loss_and_grads(s, params, loss, x):
+    """(loss, (l_rdf, l_ev), dL/dx [N, 3], direct dl/dtheta [P]) at x (water.jl:771-786)."""
+    x, p = _f64(x), _f64(params)
+    parts, g, dp = np.zeros(2), np.zeros(x.size), np.zeros(n_params(s))
+    val = lib().orc_loss_and_grads(ctypes.byref(s), _pd(p), ctypes.byref(loss.c), _pd(x),
+                                   _pd(parts), _pd(g), _pd(dp))
+    return val, (parts[0], parts[1]), g.reshape(-1, 3), dp
+
+
 def forward_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss=None,
-                calc_loss=True, n_steps_log=1000):
+                calc_loss=True, n_steps_log=1000, parts=False):
+    """(x, v, loss, snaps_x, snaps_v), plus (l_rdf, l_ev) when ``parts``."""
     x, v, p = _f64(x).copy(), _f64(v).copy(), _f64(params)
     seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
     n_snap = n_steps // n_steps_log + 1
     sx = np.zeros((n_snap, x.size))
     sv = np.zeros((n_snap, x.size))
+    lp = np.zeros(2)
     val = lib().orc_forward_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v), seeds.ctypes.data_as(_PU64),
                                 gamma, n_steps, n_steps_loss, dt, n_steps_log,
                                 ctypes.byref(loss.c) if loss is not None else None,
-                                1 if (calc_loss and loss is not None) else 0, _pd(sx), _pd(sv))
-    return x.reshape(-1, 3), v.reshape(-1, 3), val, sx, sv
+                                1 if (calc_loss and loss is not None) else 0, _pd(sx), _pd(sv),
+                                _pd(lp))
+    out = (x.reshape(-1, 3), v.reshape(-1, 3), val, sx, sv)
+    return out + ((lp[0], lp[1]),) if parts else out
 
 
 def reverse_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
-                snaps_x, snaps_v, loss, clip=float("inf"), n_steps_log=1000):
+                snaps_x, snaps_v, loss, clip=float("inf"), n_steps_log=1000, parts=False):
+    """(x0, v0, loss, dl/dtheta), plus (l_rdf, l_ev) when ``parts``."""
     x, v, p = _f64(x).copy(), _f64(v).copy(), _f64(params)
     seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
     sx, sv = _f64(snaps_x), _f64(snaps_v)
     g = np.zeros(n_params(s))
+    lp = np.zeros(2)
     val = lib().orc_reverse_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v), seeds.ctypes.data_as(_PU64),
                                 gamma, n_steps, n_steps_loss, n_steps_trunc, dt, n_steps_log,
-                                _pd(sx), _pd(sv), clip, ctypes.byref(loss.c), _pd(g))
-    return x.reshape(-1, 3), v.reshape(-1, 3), val, g
+                                _pd(sx), _pd(sv), clip, ctypes.byref(loss.c), _pd(g), _pd(lp))
+    out = (x.reshape(-1, 3), v.reshape(-1, 3), val, g)
+    return out + ((lp[0], lp[1]),) if parts else out
 
 
 def set_threads(n):

@@ -1035,6 +1035,48 @@ double orc_loss_grad(const orc_system *s, const orc_loss *Ls, const double *x, d
     return loss;
 }
 
+double orc_loss_and_grads(const orc_system *s, const double *params, const orc_loss *Ls,
+                          const double *x, double *l_parts, double *dLdx, double *dl_dp) {
+    const int64_t n3 = 9 * (int64_t)s->n_mol;
+    const int P = orc_system_n_params(s);
+    /* loss_fn, water.jl:757-769 */
+    const double l_rdf = orc_loss_grad(s, Ls, x, dLdx);
+    double l_ev = 0.0;
+    if (dl_dp)
+        for (int p = 0; p < P; p++) dl_dp[p] = 0.0;
+    if (Ls->enth_vap) {
+        /* enthalpy_vaporization / loss_enth_vap, water.jl:738-755 */
+        int64_t cap = 16 * (3 * (int64_t)s->n_mol) + 1024;
+        int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * (size_t)cap);
+        int64_t np = orc_neighbor_pairs(s, x, pairs, cap);
+        if (np > cap) {
+            cap = np;
+            pairs = (int32_t *)realloc(pairs, sizeof(int32_t) * 2 * (size_t)cap);
+            np = orc_neighbor_pairs(s, x, pairs, cap);
+        }
+        double *dU = (double *)malloc(sizeof(double) * (size_t)P);
+        const double U = orc_energy_grads(s, params, x, pairs, np, dU);
+        const double e = Ls->u_gas - U / s->n_mol + Ls->rt - Ls->target;
+        const double k = 2.0 * e / s->n_mol;   /* dl_ev/dU = -k */
+        l_ev = e * e;
+        if (dl_dp)
+            for (int p = 0; p < P; p++) dl_dp[p] = -k * dU[p];
+        if (dLdx) {
+            double *F = (double *)malloc(sizeof(double) * (size_t)n3);
+            orc_forces(s, params, x, pairs, np, F);
+            for (int64_t i = 0; i < n3; i++) dLdx[i] += k * F[i];
+            free(F);
+        }
+        free(dU);
+        free(pairs);
+    }
+    if (l_parts) {
+        l_parts[0] = l_rdf;
+        l_parts[1] = l_ev;
+    }
+    return l_rdf + l_ev;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Rebuild the pair list into a growable buffer; returns the pair count. */
 static int64_t rebuild_pairs(const orc_system *s, const double *x, int32_t **pairs, int64_t *cap) {
@@ -1051,7 +1093,7 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
                        const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                        int32_t n_steps_loss, double dt, int32_t n_steps_log,
                        const orc_loss *loss, int32_t calc_loss,
-                       double *snap_x, double *snap_v) {
+                       double *snap_x, double *snap_v, double *l_parts) {
     const int64_t n = 3 * (int64_t)s->n_mol, n3 = 3 * n;
     const double L = s->box;
     const double c = exp(-gamma * dt), sn = sqrt(1 - c * c);   /* water.jl:1019-1020 */
@@ -1066,7 +1108,7 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
         memcpy(snap_x, x, sizeof(double) * (size_t)n3);
         memcpy(snap_v, v, sizeof(double) * (size_t)n3);
     }
-    double loss_accum = 0.0;
+    double loss_accum = 0.0, parts_accum[2] = {0.0, 0.0};
     /* water.jl:1029-1045 */
     for (int32_t step = 1; step <= n_steps; step++) {
         forces_core(s, params, x, pairs, np, NULL, 0, F, NULL, NULL, NULL, NULL, coef, NULL);
@@ -1085,7 +1127,16 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
             memcpy(snap_x + si * n3, x, sizeof(double) * (size_t)n3);
             memcpy(snap_v + si * n3, v, sizeof(double) * (size_t)n3);
         }
-        if (calc_loss && loss && step % n_steps_loss == 0) loss_accum += orc_loss_grad(s, loss, x, NULL);
+        if (calc_loss && loss && step % n_steps_loss == 0) {
+            double lp[2];
+            loss_accum += orc_loss_and_grads(s, params, loss, x, lp, NULL, NULL);
+            parts_accum[0] += lp[0];
+            parts_accum[1] += lp[1];
+        }
+    }
+    if (l_parts) {
+        l_parts[0] = parts_accum[0] / n_blocks;
+        l_parts[1] = parts_accum[1] / n_blocks;
     }
     free(coef);
     free(F);
@@ -1110,7 +1161,8 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
                        const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                        int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
                        int32_t n_steps_log, const double *snap_x, const double *snap_v,
-                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp) {
+                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
+                       double *l_parts) {
     if (n_steps_trunc > n_steps_loss || n_steps_loss <= 0) return NAN;  /* water.jl:1437-1439 */
     const int64_t n = 3 * (int64_t)s->n_mol, n3 = 3 * n;
     const double L = s->box;
@@ -1127,7 +1179,14 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
     int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * (size_t)cap);
 
     for (int p = 0; p < P; p++) dl_dp[p] = 0.0;
-    double loss_accum = orc_loss_grad(s, loss, x, g);   /* water.jl:1471 */
+    /* direct dl/dtheta of every loss point (water.jl:1471, 1540) */
+    double *ddirect = (double *)calloc((size_t)P, sizeof(double));
+    double *dblock = (double *)malloc(sizeof(double) * (size_t)P);
+    double lp[2], parts_accum[2];
+    double loss_accum = orc_loss_and_grads(s, params, loss, x, lp, g, dblock);   /* water.jl:1471 */
+    parts_accum[0] = lp[0];
+    parts_accum[1] = lp[1];
+    for (int p = 0; p < P; p++) ddirect[p] += dblock[p];
     reset_accums(n3, c, g, A, B, C, Dd, dl_dfi);
     int64_t np = rebuild_pairs(s, x, &pairs, &cap);
 
@@ -1173,12 +1232,21 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
         }
         if ((step_n - 1) % n_steps_loss == 0 && step_n > 1) {
             trunc_count = 0;
-            loss_accum += orc_loss_grad(s, loss, x, g);
+            loss_accum += orc_loss_and_grads(s, params, loss, x, lp, g, dblock);
+            parts_accum[0] += lp[0];
+            parts_accum[1] += lp[1];
+            for (int p = 0; p < P; p++) ddirect[p] += dblock[p];
             reset_accums(n3, c, g, A, B, C, Dd, dl_dfi);
         }
     }
     if (coef) orc_mlp_backprop(params + Pc, s->cutoff, adj, dl_dp + Pc);
-    for (int p = 0; p < P; p++) dl_dp[p] /= n_blocks;
+    for (int p = 0; p < P; p++) dl_dp[p] = (dl_dp[p] + ddirect[p]) / n_blocks;
+    if (l_parts) {
+        l_parts[0] = parts_accum[0] / n_blocks;
+        l_parts[1] = parts_accum[1] / n_blocks;
+    }
+    free(ddirect);
+    free(dblock);
     free(coef);
     free(adj);
     free(buf);

@@ -71,9 +71,15 @@ typedef struct {
     double weight;
 } orc_rdf_term;
 
+/* The loss of loss_fn (water.jl:757-769): the RDF terms, plus -- when enth_vap is set -- the
+ * enthalpy-of-vaporisation term of loss_enth_vap (water.jl:738-755),
+ * l_ev = (u_gas - U / n_mol + rt - target)^2, U the potential energy (the reference's values:
+ * u_gas 3.69, rt 2.45, target 44.12 + 2.8 kJ/mol). */
 typedef struct {
     int32_t n_terms;
     const orc_rdf_term *terms;
+    int32_t enth_vap;
+    double u_gas, rt, target;
 } orc_loss;
 
 int32_t orc_n_form_params(int32_t inter_type);
@@ -124,27 +130,39 @@ void orc_philox_normals(uint64_t seed, uint32_t atom, double z[4]);
 /* RDF histogram of one term at positions x: writes h[n_grid]. */
 void orc_rdf(const orc_system *s, const orc_rdf_term *t, const double *x, double *h);
 
-/* Loss and dL/dx[3N] (dLdx may be NULL). */
+/* The RDF terms' loss and dL/dx[3N] (dLdx may be NULL); ignores the enthalpy term. */
 double orc_loss_grad(const orc_system *s, const orc_loss *L, const double *x, double *dLdx);
+
+/* loss_and_grads (water.jl:771-786) at x: returns the loss; l_parts[2] (may be NULL) receives
+ * its RDF and enthalpy parts, dLdx[3N] (may be NULL) dL/dx, and dl_dp[P] (may be NULL) the
+ * direct parameter gradient.  With the enthalpy term, e = u_gas - U/n_mol + rt - target gives
+ * dl_ev/dx = (2 e / n_mol) F and dl_ev/dtheta = -(2 e / n_mol) dU/dtheta (the RDF terms have
+ * no direct parameter dependence).  U sums over a fresh neighbour list, as
+ * enthalpy_vaporization's find_neighbors does (water.jl:743). */
+double orc_loss_and_grads(const orc_system *s, const double *params, const orc_loss *L,
+                          const double *x, double *l_parts, double *dLdx, double *dl_dp);
 
 /* forward_sim (water.jl:977-1105, loop 1029-1045).  x, v are updated in place
  * (final state).  Snapshots of x and v are written every n_steps_log steps,
  * including step 0, into snap_x/snap_v [(n_steps/n_steps_log + 1) * 3N] if not NULL.
- * Returns the block-averaged loss (0 when calc_loss == 0). */
+ * Returns the block-averaged loss (0 when calc_loss == 0); l_parts[2] (may be NULL) receives
+ * its block-averaged RDF and enthalpy parts. */
 double orc_forward_sim(const orc_system *s, const double *params, double *x, double *v,
                        const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                        int32_t n_steps_loss, double dt, int32_t n_steps_log,
                        const orc_loss *loss, int32_t calc_loss,
-                       double *snap_x, double *snap_v);
+                       double *snap_x, double *snap_v, double *l_parts);
 
 /* reverse_sim (water.jl:1435-1558).  x, v: final forward state on entry,
- * reconstructed initial state on exit.  dl_dp[P] receives the gradient.
- * Returns the block-averaged loss; returns NaN on bad arguments. */
+ * reconstructed initial state on exit.  dl_dp[P] receives the gradient (the adjoint terms
+ * plus, with the enthalpy term, the direct dl/dtheta of every loss point, water.jl:1540).
+ * Returns the block-averaged loss (l_parts as for orc_forward_sim); NaN on bad arguments. */
 double orc_reverse_sim(const orc_system *s, const double *params, double *x, double *v,
                        const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                        int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
                        int32_t n_steps_log, const double *snap_x, const double *snap_v,
-                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp);
+                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
+                       double *l_parts);
 
 /* Number of OpenMP threads used by the force loops (1 when built without OpenMP). */
 int32_t orc_num_threads(void);

@@ -114,6 +114,15 @@ struct revsim_handle {
     // loss
     std::vector<Term> terms;
     double *d_loss = nullptr, *d_loss_acc = nullptr, *d_dLdx = nullptr;
+    // enthalpy-of-vaporisation term: per-replica l_ev sums, 2 e / n, direct dl/dtheta sums
+    // [R][P], and the neighbour rows of its energy (built at each loss point)
+    bool ev_on = false;
+    double ev_ugas = 3.69, ev_rt = 2.45, ev_target = 44.12 + 2.8;
+    double *d_ev_acc = nullptr, *d_ev_k = nullptr, *d_ev_grad = nullptr;
+    uint32_t *d_nbr_ev = nullptr;
+    int *d_cnt_ev = nullptr;
+    int ev_cap = 0;
+    int last_blocks = 1;   // loss points of the last forward / reverse (0: no loss computed)
     // instrumentation
     long long launches = 0;
     bool ktime = false;
@@ -440,9 +449,105 @@ int pack(revsim_handle *h, int buf, bool with_w) {
     return REVSIM_OK;
 }
 
-// loss_fn / loss_and_grads at the current positions: adds the per-replica loss to
-// acc (device [R]) and, if grad, writes dL/dx into d_dLdx.
-int loss_dev(revsim_handle *h, bool grad, double *acc) {
+EnergyArgs energy_args(revsim_handle *h, const uint32_t *nbr, const int *cnt) {
+    EnergyArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.M = h->M;
+    a.P = h->P;
+    a.cap = h->cap;
+    a.x = h->d_x;
+    a.mol_rep = h->d_mol_rep;
+    a.rep_box = h->d_rep_box;
+    a.nbr = nbr;
+    a.nbr_cnt = cnt;
+    a.rc2 = h->rc * h->rc;
+    a.ke = h->ke;
+    a.krf = h->krf;
+    a.crf_shift = 1.0 / h->rc + h->krf * h->rc * h->rc;
+    const double *t = h->theta.data();
+    a.qO = t[h->NFp];
+    a.kb = t[h->NFp + 1];
+    a.r0 = t[h->NFp + 2];
+    a.ka = t[h->NFp + 3];
+    a.th0 = t[h->NFp + 4];
+    for (int k = 0; k < 4; k++) a.form_p[k] = k < h->NFp ? t[k] : 0.0;
+    a.mlp_tab = h->d_mlp_tab;
+    a.mlp_hinv = MLP_NG / h->rc;
+    a.part = h->d_epart;
+    a.grads = 1;
+    a.adj_mul = 1.0;
+    return a;
+}
+
+// The enthalpy-of-vaporisation term at the current positions (enthalpy_vaporization and
+// loss_enth_vap, water.jl:738-755): adds l_ev to acc and d_ev_acc; with grad_p adds the
+// direct -(2 e / n) dU/dtheta to d_ev_grad (classical) and d_mlp_adj (MLP coefficient
+// adjoints); with grad_x adds (2 e / n) F to d_dLdx.  U sums over rows built here from the
+// current positions, as the reference's find_neighbors does (water.jl:743).
+int enth_dev(revsim_handle *h, double *acc, double *ev_acc, bool grad_x, bool grad_p) {
+    if (h->ev_cap != h->cap) {
+        dfree(h->d_nbr_ev);
+        dfree(h->d_cnt_ev);
+        h->d_nbr_ev = nullptr;
+        h->d_cnt_ev = nullptr;
+        h->ev_cap = 0;
+        CK(dalloc(&h->d_nbr_ev, (size_t)h->M * h->cap));
+        CK(dalloc(&h->d_cnt_ev, (size_t)h->M));
+        h->ev_cap = h->cap;
+    }
+    if (!h->d_epart) CK(dalloc(&h->d_epart, (size_t)h->M * (h->P + 1)));
+    int rc = build_nlist(h, h->d_x, h->d_nbr_ev, h->d_cnt_ev);
+    if (rc) return rc;
+    const int form = h->mlp ? (int)F_LJ_MLP : h->form;
+    EnergyArgs a = energy_args(h, h->d_nbr_ev, h->d_cnt_ev);
+    a.grads = grad_p ? 1 : 0;
+    CK(launch_energy_grads(form, h->prec, a, h->st));
+    EnthArgs f;
+    f.R = h->R;
+    f.P = h->P;
+    f.grads = grad_p ? 1 : 0;
+    f.rep_atom0 = h->d_rep_atom0;
+    f.rep_nmol = h->d_rep_nmol;
+    f.part = h->d_epart;
+    f.u_gas = h->ev_ugas;
+    f.rt = h->ev_rt;
+    f.target = h->ev_target;
+    f.acc = acc;
+    f.ev_acc = ev_acc;
+    f.k = h->d_ev_k;
+    f.dgrad = h->d_ev_grad;
+    CK(launch_enth_finalize(f, h->st));
+    h->launches += 2;
+    if (grad_p && h->mlp) {
+        // dU/dcoef scaled per replica by -(2 e / n) into the MLP coefficient adjoints
+        a.grads = 0;
+        a.mlp_adj = h->d_mlp_adj;
+        a.adj_scale = h->d_ev_k;
+        a.adj_mul = -1.0;
+        CK(launch_energy_grads(form, h->prec, a, h->st));
+        h->launches++;
+    }
+    if (grad_x) {
+        if ((rc = pack(h, 0, false))) return rc;
+        StepArgs s = base_args(h, false);
+        s.nbr = h->d_nbr_ev;
+        s.nbr_cnt = h->d_cnt_ev;
+        s.cap = h->cap;
+        s.pos_in = h->d_pos[0];
+        s.F_out = h->d_F;
+        s.mode = MODE_FORCES_ONLY;
+        if ((rc = launch_step_k(h, false, s))) return rc;
+        CK(launch_enth_dldx(h->N, h->d_atom_rep, h->d_ev_k, h->d_F, h->d_dLdx, h->st));
+        h->launches++;
+    }
+    return REVSIM_OK;
+}
+
+// loss_fn / loss_and_grads at the current positions: adds the per-replica loss to acc
+// (device [R]) and the enthalpy part to ev_acc (may be null); if grad writes dL/dx into
+// d_dLdx; if grad_p adds the enthalpy term's direct parameter gradient to d_ev_grad /
+// d_mlp_adj.
+int loss_dev(revsim_handle *h, bool grad, double *acc, double *ev_acc = nullptr, bool grad_p = false) {
     if (grad) CK(cudaMemsetAsync(h->d_dLdx, 0, sizeof(double) * 3 * (size_t)h->N, h->st));
     for (Term &T : h->terms) {
         const revsim_rdf_term &t = T.t;
@@ -474,8 +579,11 @@ int loss_dev(revsim_handle *h, bool grad, double *acc) {
             h->launches++;
         }
     }
+    if (h->ev_on) return enth_dev(h, acc, ev_acc, grad, grad_p);
     return REVSIM_OK;
 }
+
+bool has_loss(const revsim_handle *h) { return !h->terms.empty() || h->ev_on; }
 
 int upload_seeds(revsim_handle *h, const uint64_t *seeds, size_t n) {
     if (n > h->seeds_cap) {
@@ -521,6 +629,7 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     CK(cudaMemcpyAsync(h->d_snap_x, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemcpyAsync(h->d_snap_v, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
+    if (h->ev_on) CK(cudaMemsetAsync(h->d_ev_acc, 0, sizeof(double) * R, h->st));
     StepArgs a = base_args(h, false);
     a.dt = dt;
     a.c = c;
@@ -549,8 +658,8 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
             CK(cudaMemcpyAsync(h->d_snap_x + si, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
             CK(cudaMemcpyAsync(h->d_snap_v + si, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
         }
-        if (calc_loss && !h->terms.empty() && step % n_steps_loss == 0)
-            if ((rc = loss_dev(h, false, h->d_loss_acc))) return rc;
+        if (calc_loss && has_loss(h) && step % n_steps_loss == 0)
+            if ((rc = loss_dev(h, false, h->d_loss_acc, h->d_ev_acc))) return rc;
     }
     return REVSIM_OK;
 }
@@ -571,7 +680,11 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
     if (int rc_ = mlp_zero_adj(h)) return rc_;
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
-    if ((rc = loss_dev(h, true, h->d_loss_acc))) return rc;
+    if (h->ev_on) {
+        CK(cudaMemsetAsync(h->d_ev_acc, 0, sizeof(double) * R, h->st));
+        CK(cudaMemsetAsync(h->d_ev_grad, 0, sizeof(double) * R * h->P, h->st));
+    }
+    if ((rc = loss_dev(h, true, h->d_loss_acc, h->d_ev_acc, true))) return rc;
     CK(launch_init_adjoint(h->N, h->d_dLdx, c, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->st));
     h->launches++;
 
@@ -667,7 +780,7 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
         }
         if (lossb) {
             trunc = 0;
-            if ((rc = loss_dev(h, true, h->d_loss_acc))) return rc;
+            if ((rc = loss_dev(h, true, h->d_loss_acc, h->d_ev_acc, true))) return rc;
             CK(launch_init_adjoint(h->N, h->d_dLdx, c, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->st));
             h->launches++;
             pending = true;
@@ -720,7 +833,8 @@ void free_all(revsim_handle *h) {
                     h->d_pos[0], h->d_pos[1], h->d_wgt[0], h->d_wgt[1], h->d_part, h->d_norm2,
                     h->d_scale, h->d_status, h->d_maxcnt, h->d_count, h->d_snap_x, h->d_snap_v,
                     h->d_ckpt, h->d_seeds, h->d_loss, h->d_loss_acc, h->d_dLdx,
-                    h->d_cell_rep, h->d_nbr_store, h->d_cnt_store};
+                    h->d_cell_rep, h->d_nbr_store, h->d_cnt_store, h->d_ev_acc, h->d_ev_k,
+                    h->d_ev_grad, h->d_nbr_ev, h->d_cnt_ev};
     for (void *p : ptrs) dfree(p);
     for (Term &T : h->terms) {
         dfree(T.d_target);
@@ -1112,30 +1226,8 @@ int32_t revsim_energy_grad(revsim_handle *h, double *energy, double *dEdtheta) {
     if ((rc = build_nlist_checked(h, h->d_x))) return rc;
     if ((rc = mlp_zero_adj(h))) return rc;
     if (!h->d_epart) CK(dalloc(&h->d_epart, (size_t)h->M * (h->P + 1)));
-    EnergyArgs a;
-    a.M = h->M;
-    a.P = h->P;
-    a.cap = h->cap;
-    a.x = h->d_x;
-    a.mol_rep = h->d_mol_rep;
-    a.rep_box = h->d_rep_box;
-    a.nbr = h->d_nbr;
-    a.nbr_cnt = h->d_nbr_cnt;
-    a.rc2 = h->rc * h->rc;
-    a.ke = h->ke;
-    a.krf = h->krf;
-    a.crf_shift = 1.0 / h->rc + h->krf * h->rc * h->rc;
-    const double *t = h->theta.data();
-    a.qO = t[h->NFp];
-    a.kb = t[h->NFp + 1];
-    a.r0 = t[h->NFp + 2];
-    a.ka = t[h->NFp + 3];
-    a.th0 = t[h->NFp + 4];
-    for (int k = 0; k < 4; k++) a.form_p[k] = k < h->NFp ? t[k] : 0.0;
-    a.mlp_tab = h->d_mlp_tab;
+    EnergyArgs a = energy_args(h, h->d_nbr, h->d_nbr_cnt);
     a.mlp_adj = h->mlp ? h->d_mlp_adj : nullptr;
-    a.mlp_hinv = MLP_NG / h->rc;
-    a.part = h->d_epart;
     cudaError_t e = launch_energy_grads(h->mlp ? (int)F_LJ_MLP : h->form, h->prec, a, h->st);
     h->launches++;
     if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("energy gradient: ") + cudaGetErrorString(e));
@@ -1183,16 +1275,90 @@ int32_t revsim_loss_grad(revsim_handle *h, double *loss, double *dLdx) {
     return REVSIM_OK;
 }
 
+int32_t revsim_set_enth_vap(revsim_handle *h, int32_t enable, double u_gas, double rt, double target) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (enable && !(std::isfinite(u_gas) && std::isfinite(rt) && std::isfinite(target)))
+        return fail(h, REVSIM_ERR_BADARG, "enthalpy constants must be finite");
+    CK(cudaSetDevice(h->dev));
+    if (enable && !h->d_ev_acc) {
+        CK(dalloc(&h->d_ev_acc, 2 * (size_t)h->R));   // [0, R) runs, [R, 2R) revsim_loss_and_grads
+        CK(dalloc(&h->d_ev_k, (size_t)h->R));
+        CK(dalloc(&h->d_ev_grad, (size_t)h->R * h->P));
+        CK(cudaMemset(h->d_ev_acc, 0, sizeof(double) * 2 * h->R));
+    }
+    h->ev_on = enable != 0;
+    h->ev_ugas = u_gas;
+    h->ev_rt = rt;
+    h->ev_target = target;
+    return REVSIM_OK;
+}
+
+int32_t revsim_loss_parts(revsim_handle *h, double *l_rdf, double *l_ev) {
+    if (!h) return REVSIM_ERR_BADARG;
+    CK(cudaSetDevice(h->dev));
+    std::vector<double> tot(h->R, 0.0), ev(h->R, 0.0);
+    if (h->last_blocks > 0) {
+        CK(cudaMemcpy(tot.data(), h->d_loss_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));
+        if (h->ev_on) CK(cudaMemcpy(ev.data(), h->d_ev_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));
+    }
+    const double nb = std::max(1, h->last_blocks);
+    for (int r = 0; r < h->R; r++) {
+        if (l_rdf) l_rdf[r] = h->last_blocks > 0 ? (tot[r] - ev[r]) / nb : 0.0;
+        if (l_ev) l_ev[r] = h->last_blocks > 0 ? ev[r] / nb : 0.0;
+    }
+    return REVSIM_OK;
+}
+
+int32_t revsim_loss_and_grads(revsim_handle *h, double *loss, double *l_rdf, double *l_ev, double *dLdx,
+                              double *dl_dp) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double) * h->R, h->st));
+    if (h->ev_on) {
+        CK(cudaMemsetAsync(h->d_ev_acc + h->R, 0, sizeof(double) * h->R, h->st));
+        CK(cudaMemsetAsync(h->d_ev_grad, 0, sizeof(double) * h->R * h->P, h->st));
+    }
+    if (h->ev_on && dl_dp && (rc = mlp_zero_adj(h))) return rc;
+    double *ev1 = h->ev_on ? h->d_ev_acc + h->R : nullptr;   // this call's slot
+    if ((rc = loss_dev(h, dLdx != nullptr, h->d_loss, ev1, dl_dp != nullptr))) return rc;
+    std::vector<double> tot(h->R), ev(h->R, 0.0);
+    CK(cudaMemcpyAsync(tot.data(), h->d_loss, sizeof(double) * h->R, cudaMemcpyDeviceToHost, h->st));
+    if (h->ev_on) CK(cudaMemcpyAsync(ev.data(), h->d_ev_acc + h->R, sizeof(double) * h->R, cudaMemcpyDeviceToHost, h->st));
+    if (dLdx) CK(cudaMemcpyAsync(dLdx, h->d_dLdx, sizeof(double) * 3 * (size_t)h->N, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int r = 0; r < h->R; r++) {
+        if (loss) loss[r] = tot[r];
+        if (l_rdf) l_rdf[r] = tot[r] - ev[r];
+        if (l_ev) l_ev[r] = ev[r];
+    }
+    if (dl_dp) {
+        std::vector<double> cl((size_t)h->R * h->P, 0.0), ml;
+        if (h->ev_on) {
+            CK(cudaMemcpy(cl.data(), h->d_ev_grad, sizeof(double) * cl.size(), cudaMemcpyDeviceToHost));
+            if (h->mlp && (rc = mlp_grads(h, ml))) return rc;
+        } else if (h->mlp) {
+            ml.assign((size_t)h->R * (h->Pt - h->P), 0.0);
+        }
+        join_grads(h, cl, ml, 1.0, dl_dp);
+    }
+    int s;
+    if ((rc = read_status(h, &s))) return rc;
+    return status_code(h, s);
+}
+
 int32_t revsim_rdf(revsim_handle *h, int32_t term, int32_t replica, double *hist) {
     if (!h || !hist || term < 0 || term >= (int)h->terms.size() || replica < 0 || replica >= h->R)
         return REVSIM_ERR_BADARG;
     if (!h->have_state) return fail(h, REVSIM_ERR_STATE, "state not set");
     CK(cudaSetDevice(h->dev));
     std::vector<Term> keep = h->terms;
+    const bool ev = h->ev_on;
     h->terms.assign(1, keep[term]);
+    h->ev_on = false;
     CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double) * h->R, h->st));
     int rc = loss_dev(h, false, h->d_loss);
     h->terms = keep;
+    h->ev_on = ev;
     if (rc) return rc;
     const Term &T = h->terms[term];
     CK(cudaMemcpyAsync(hist, T.d_hist + (size_t)replica * T.t.n_grid, sizeof(double) * T.t.n_grid,
@@ -1232,6 +1398,7 @@ int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gam
         CK(cudaMemcpyAsync(h->d_x, h->d_x0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
         CK(cudaMemcpyAsync(h->d_v, h->d_v0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     }
+    h->last_blocks = calc_loss ? (n_steps == 0 ? 1 : std::max(1, n_steps / std::max(1, n_steps_loss))) : 0;
     if (loss_out) {
         const int n_blocks = n_steps == 0 ? 1 : std::max(1, n_steps / std::max(1, n_steps_loss));
         std::vector<double> l(h->R);
@@ -1253,7 +1420,7 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
         return fail(h, REVSIM_ERR_BADARG, "n_steps_trunc must not be greater than n_steps_loss");
     if (n_steps < 1 || n_steps_loss < 1 || !noise_seeds || !(dt > 0) || !(gamma >= 0) || !(clip_norm_threshold > 0))
         return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
-    if (h->terms.empty()) return fail(h, REVSIM_ERR_STATE, "no loss set");
+    if (!has_loss(h)) return fail(h, REVSIM_ERR_STATE, "no loss set");
     const bool need_store = h->nl_mode == REVSIM_NL_CHECKPOINT || (h->nlog > 0 && n_steps > h->nlog);
     if (need_store && !(h->fwd_valid && h->fwd_steps == n_steps))
         return fail(h, REVSIM_ERR_STATE, "reverse needs the forward pass of the same n_steps");
@@ -1265,8 +1432,15 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
     const int n_blocks = n_steps / n_steps_loss;
     std::vector<double> th, thm;
     if ((rc = reduce_part(h, th))) return rc;
+    if (h->ev_on) {
+        // the enthalpy term's direct dl/dtheta of every loss point (water.jl:1471, 1540)
+        std::vector<double> d((size_t)h->R * h->P);
+        CK(cudaMemcpy(d.data(), h->d_ev_grad, sizeof(double) * d.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < d.size(); i++) th[i] += d[i];
+    }
     if (h->mlp && (rc = mlp_grads(h, thm))) return rc;
     if (dl_dp_out) join_grads(h, th, thm, 1.0 / n_blocks, dl_dp_out);
+    h->last_blocks = n_blocks;
     if (loss_out) {
         std::vector<double> l(h->R);
         CK(cudaMemcpy(l.data(), h->d_loss_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));

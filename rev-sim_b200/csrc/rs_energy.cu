@@ -8,7 +8,9 @@
 // Coulomb energy (dE/dq_O = 2 E_c / q_O), its own two bonds and angle, and -- with the
 // learned term -- the interval-coefficient adjoints (1, s, s^2, s^3) of each pair's Hermite
 // segment, which the MLP backpropagation turns into dE/dtheta_mlp.  Per-molecule partials
-// [E, dE/dtheta...] are summed per replica on the host in molecule order.
+// [E, dE/dtheta...] are summed per replica on the host in molecule order, or -- for the
+// enthalpy-of-vaporisation loss term (loss_enth_vap, water.jl:738-755) -- on the device by
+// k_enth_finalize, which also turns U into the loss and its coefficient 2 e / n.
 #include "rs_internal.h"
 
 namespace rs {
@@ -91,6 +93,7 @@ __global__ void k_energy_grads(EnergyArgs a) {
 #pragma unroll
     for (int k = 0; k < 17; k++) acc[k] = 0.0;
     const bool gate = a.form_p[FORM == F_BUCK ? 0 : 1] != 0.0;
+    const double aw = a.adj_scale ? a.adj_mul * a.adj_scale[rep] : 1.0;
     const double qq[3] = {a.qO * a.qO, a.qO * (-0.5 * a.qO), 0.25 * a.qO * a.qO};
     double *madj = a.mlp_adj ? a.mlp_adj + ((size_t)rep * MLP_NCOPY + (I % MLP_NCOPY)) * MLP_NT * MLP_NG * 4
                              : nullptr;
@@ -114,22 +117,28 @@ __global__ void k_energy_grads(EnergyArgs a) {
                 acc[0] += Ec;
                 acc[1 + NFm] += 2.0 * Ec / a.qO;
                 if (ka == 0 && kb == 0 && gate) {
-                    const DN<4> Ef = form_energy<FORM>(a.form_p, r);
-                    acc[0] += Ef.v;
+                    if (a.grads) {
+                        const DN<4> Ef = form_energy<FORM>(a.form_p, r);
+                        acc[0] += Ef.v;
 #pragma unroll
-                    for (int k = 0; k < NFm; k++) acc[1 + k] += Ef.d[k];
+                        for (int k = 0; k < NFm; k++) acc[1 + k] += Ef.d[k];
+                    } else {
+                        acc[0] += form_energy<FORM>(a.form_p, r).v;
+                    }
                 }
-                if (FORM == F_LJ_MLP && madj) {
+                if (FORM == F_LJ_MLP) {
                     const double q = r * a.mlp_hinv;
                     const int g = min((int)q, MLP_NG - 1);
                     const double s = q - g;
                     const V4 c = reinterpret_cast<const V4 *>(a.mlp_tab)[QI * MLP_NG + g];
                     acc[0] += (double)c.x + s * ((double)c.y + s * ((double)c.z + s * (double)c.w));
-                    double *ad = madj + ((size_t)QI * MLP_NG + g) * 4;
-                    atomicAdd(ad, 1.0);
-                    atomicAdd(ad + 1, s);
-                    atomicAdd(ad + 2, s * s);
-                    atomicAdd(ad + 3, s * s * s);
+                    if (madj) {
+                        double *ad = madj + ((size_t)QI * MLP_NG + g) * 4;
+                        atomicAdd(ad, aw);
+                        atomicAdd(ad + 1, aw * s);
+                        atomicAdd(ad + 2, aw * s * s);
+                        atomicAdd(ad + 3, aw * s * s * s);
+                    }
                 }
             }
     }
@@ -150,7 +159,45 @@ __global__ void k_energy_grads(EnergyArgs a) {
     acc[0] += 0.5 * a.ka * th * th;
     acc[1 + NFm + 3] += 0.5 * th * th;
     acc[1 + NFm + 4] += -a.ka * th;
-    for (int k = 0; k <= P; k++) a.part[(size_t)I * (P + 1) + k] = acc[k];
+    for (int k = 0; k <= (a.grads ? P : 0); k++) a.part[(size_t)I * (P + 1) + k] = acc[k];
+}
+
+constexpr int kEnthThreads = 256;
+
+__global__ void __launch_bounds__(kEnthThreads) k_enth_finalize(EnthArgs a) {
+    __shared__ double red[kEnthThreads];
+    __shared__ double kr;
+    const int r = blockIdx.x, t = threadIdx.x;
+    const int m0 = a.rep_atom0[r] / 3, n = a.rep_nmol[r];
+    const int ncol = a.grads ? a.P + 1 : 1;
+    for (int col = 0; col < ncol; col++) {
+        double s = 0.0;
+        for (int I = t; I < n; I += kEnthThreads) s += a.part[(size_t)(m0 + I) * (a.P + 1) + col];
+        red[t] = s;
+        __syncthreads();
+        for (int w = kEnthThreads / 2; w > 0; w >>= 1) {
+            if (t < w) red[t] += red[t + w];
+            __syncthreads();
+        }
+        if (t == 0) {
+            if (col == 0) {
+                // enthalpy_vaporization and loss_enth_vap, water.jl:738-755
+                const double e = a.u_gas - red[0] / n + a.rt - a.target;
+                a.acc[r] += e * e;
+                if (a.ev_acc) a.ev_acc[r] += e * e;
+                kr = 2.0 * e / n;
+                a.k[r] = kr;
+            } else {
+                a.dgrad[(size_t)r * a.P + col - 1] += -kr * red[0];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_enth_dldx(int n3, const int *atom_rep, const double *k, const double *F, double *dLdx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n3) dLdx[i] += k[atom_rep[i / 3]] * F[i];
 }
 
 template <int FORM>
@@ -164,6 +211,18 @@ cudaError_t launch_f(int prec, const EnergyArgs &a, cudaStream_t st) {
 }
 
 }  // namespace
+
+cudaError_t launch_enth_finalize(const EnthArgs &a, cudaStream_t st) {
+    if (a.R > 0) k_enth_finalize<<<a.R, kEnthThreads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_enth_dldx(int N, const int *atom_rep, const double *k, const double *F, double *dLdx,
+                             cudaStream_t st) {
+    const int n3 = 3 * N, t = 256;
+    if (n3 > 0) k_enth_dldx<<<(n3 + t - 1) / t, t, 0, st>>>(n3, atom_rep, k, F, dLdx);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_energy_grads(int form, int prec, const EnergyArgs &a, cudaStream_t st) {
     switch (form) {

@@ -129,8 +129,27 @@ struct EnergyArgs {
     double *mlp_adj;
     double mlp_hinv;
     double *part;                     // [M][P + 1]: energy, then dE/dtheta (classical)
+    int grads;                        // 0: energy column only, no classical partials
+    const double *adj_scale;          // per replica: MLP adjoints scaled by adj_mul adj_scale[r]
+    double adj_mul;                   // (adj_scale null: unscaled)
 };
 cudaError_t launch_energy_grads(int form, int prec, const EnergyArgs &a, cudaStream_t st);
+
+// The enthalpy-of-vaporisation loss term (loss_enth_vap, water.jl:738-755) from the energy
+// partials: per replica U = sum of part[I][0] over its molecules (fixed-order tree),
+// e = u_gas - U / n + rt - target, acc[r] += e^2, ev_acc[r] += e^2, k[r] = 2 e / n and, when
+// grads, dgrad[r][p] += -k[r] * sum part[I][1 + p].
+struct EnthArgs {
+    int R, P, grads;
+    const int *rep_atom0, *rep_nmol;
+    const double *part;
+    double u_gas, rt, target;
+    double *acc, *ev_acc, *k, *dgrad;
+};
+cudaError_t launch_enth_finalize(const EnthArgs &a, cudaStream_t st);
+// dLdx[i] += k[replica of atom i / 3] * F[i], i < 3N (dl_ev/dx = (2 e / n) F).
+cudaError_t launch_enth_dldx(int N, const int *atom_rep, const double *k, const double *F, double *dLdx,
+                             cudaStream_t st);
 
 size_t mlp_scratch_doubles();
 // Node evaluation and interval table of the MLP for parameters theta (device, FP64).

@@ -34,6 +34,7 @@ EXPORTS = [
     "revsim_stream", "revsim_launch_count", "revsim_set_kernel_timing", "revsim_kernel_time",
     "revsim_set_launch_shape", "revsim_get_launch_shape", "revsim_autotune",
     "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc", "revsim_energy_grad",
+    "revsim_set_enth_vap", "revsim_loss_parts", "revsim_loss_and_grads",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -136,6 +137,9 @@ def load(path=LIB_PATH):
         "revsim_noise": (i32, [vp, pu64, pd]),
         "revsim_energy_grad": (i32, [vp, pd, pd]),
         "revsim_loss_grad": (i32, [vp, pd, pd]),
+        "revsim_set_enth_vap": (i32, [vp, i32, d, d, d]),
+        "revsim_loss_parts": (i32, [vp, pd, pd]),
+        "revsim_loss_and_grads": (i32, [vp, pd, pd, pd, pd, pd]),
         "revsim_rdf": (i32, [vp, i32, i32, pd]),
         "revsim_forward": (i32, [vp, pu64, d, i32, i32, d, i32, pd]),
         "revsim_reverse": (i32, [vp, pu64, d, i32, i32, i32, d, d, pd, pd]),

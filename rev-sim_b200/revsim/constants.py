@@ -8,6 +8,8 @@ Values follow greener-group/rev-sim ``water/water.jl``:
   snapshot every 1000 steps: ``water.jl:37-40,42``
 * test parameters (sigma, eps, alpha, beta, A, B, C, q_O, k_b, r0, k_a, theta0):
   ``water.jl:1562-1582``
+* enthalpy-of-vaporisation loss: mean gas-phase energy 3.69, RT 2.45 and the target
+  44.12 + 2.8 kJ/mol: ``water.jl:738-755``
 
 Units are nm, ps, u (g/mol), kJ/mol, K and elementary charges.  The Coulomb constant
 and Boltzmann constant come from the CODATA 2018 SI definitions (the reference reads
@@ -27,6 +29,8 @@ DIST_NEIGHBORS = 1.2
 N_STEPS_NF = 20
 N_STEPS_LOG = 1000
 CRF_CONST = (1.0 / DIST_CUTOFF**3) * ((78.3 - 1) / (2 * 78.3 + 1))
+
+ENTH_U_GAS, ENTH_RT, ENTH_TARGET = 3.69, 2.45, 44.12 + 2.8
 
 # Pair forms in the order of water.jl:121-150 (generate_inter).
 INTER_TYPES = {"lj": 0, "dexp": 1, "buck": 2, "ljsc": 3, "buff": 4}

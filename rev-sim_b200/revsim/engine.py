@@ -71,6 +71,8 @@ class Engine:
         self.n_params = n_params.value
         self.atom0 = np.concatenate([[0], np.cumsum(3 * n_mol)[:-1]]).astype(np.int64)
         self.terms = []
+        self.rdf_terms = []      # the RDF terms loss_type :rdf / :both use (water.py)
+        self.enth_vap = False
 
     # ------------------------------------------------------------------ basics
     def _check(self, rc):
@@ -185,6 +187,27 @@ class Engine:
         g = np.zeros((self.n_atoms, 3)) if grad else None
         self._check(self._L.revsim_loss_grad(self._h, f64p(loss), f64p(g) if grad else None))
         return loss, g
+
+    def set_enth_vap(self, enable=True, u_gas=C.ENTH_U_GAS, rt=C.ENTH_RT, target=C.ENTH_TARGET):
+        """Add (or with enable=False remove) the enthalpy-of-vaporisation loss term
+        (loss_enth_vap, water.jl:738-755) to the RDF terms of set_loss."""
+        self._check(self._L.revsim_set_enth_vap(self._h, 1 if enable else 0, u_gas, rt, target))
+        self.enth_vap = bool(enable)
+
+    def loss_parts(self):
+        """(l_rdf [R], l_ev [R]) of the loss the last forward / reverse returned."""
+        lr, le = np.zeros(self.R), np.zeros(self.R)
+        self._check(self._L.revsim_loss_parts(self._h, f64p(lr), f64p(le)))
+        return lr, le
+
+    def loss_and_grads(self):
+        """loss_and_grads (water.jl:771-786) at the current state: (loss [R], l_rdf [R],
+        l_ev [R], dL/dx [N, 3], direct dl/dtheta [R, n_params])."""
+        out = [np.zeros(self.R) for _ in range(3)]
+        g = np.zeros((self.n_atoms, 3))
+        dp = np.zeros((self.R, self.n_params))
+        self._check(self._L.revsim_loss_and_grads(self._h, *[f64p(a) for a in out], f64p(g), f64p(dp)))
+        return out[0], out[1], out[2], g, dp
 
     def rdf(self, term=0, replica=0):
         h = np.zeros(self.terms[term].n_grid)

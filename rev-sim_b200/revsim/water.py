@@ -12,9 +12,10 @@ Differences, each deliberate:
 * the loss targets are explicit (``loss_terms``): the reference reads the Soper
   2013 file at load time (water.jl:629); ``loss.read_rdf_data`` + ``loss.reference_rdf_terms``
   rebuild exactly that loss from the file;
-* ``run_grads=True`` (the Zygote unrolled-RAD check, water.jl:1052-1099),
-  ``use_barostat=True`` and the enthalpy-of-vaporisation loss are not part of the
-  engine and raise ``NotImplementedError``;
+* ``loss_type`` is ``"rdf"``, ``"enth_vap"`` or ``"both"`` as in loss_fn (water.jl:757-769);
+  the RDF terms stay on the engine between calls, so ``loss_terms`` is needed once;
+* ``run_grads=True`` (the Zygote unrolled-RAD check, water.jl:1052-1099) and
+  ``use_barostat=True`` are not part of the engine and raise ``NotImplementedError``;
 * ``n_threads`` is accepted and ignored;
 * noise: per-step seeds drive a counter-based Philox generator, regenerated
   identically in the reverse pass (the reference uses Xoshiro(seed) + randn).
@@ -51,9 +52,21 @@ def _engine_for(coords, boundary, inter_type, engine, precision):
     return Engine(n_atoms // 3, boundary, inter_type=inter_type, precision=precision)
 
 
-def _check_loss(loss_type):
-    if loss_type not in ("rdf",):
-        raise NotImplementedError(f"loss_type {loss_type!r}: the engine implements the RDF loss")
+LOSS_TYPES = {"rdf": (True, False), "enth_vap": (False, True), "both": (True, True)}
+
+
+def _set_loss(eng, loss_type, loss_terms):
+    """loss_fn's loss_type (water.jl:757-769): the RDF terms, the enthalpy term, or both."""
+    loss_type = str(loss_type).lstrip(":")
+    if loss_type not in LOSS_TYPES:
+        raise ValueError("loss_type not recognised")
+    use_rdf, use_ev = LOSS_TYPES[loss_type]
+    if loss_terms is not None:
+        eng.rdf_terms = list(loss_terms)
+    if use_rdf and not eng.rdf_terms:
+        raise ValueError(f"loss_type {loss_type!r} needs loss_terms")
+    eng.set_loss(eng.rdf_terms if use_rdf else [])
+    eng.set_enth_vap(use_ev)
 
 
 def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss, params,
@@ -65,16 +78,11 @@ def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
         raise NotImplementedError("run_grads (Zygote unrolled RAD) is not part of the engine")
     if use_barostat:
         raise NotImplementedError("the Monte-Carlo barostat is not part of the engine")
-    if calc_loss:
-        _check_loss(loss_type)
     eng = _engine_for(coords, boundary, inter_type, engine, precision)
     eng.set_params(params)
     eng.set_state(coords, velocities)
     if calc_loss:
-        if loss_terms is None and not eng.terms:
-            raise ValueError("calc_loss needs loss_terms")
-        if loss_terms is not None:
-            eng.set_loss(loss_terms)
+        _set_loss(eng, loss_type, loss_terms)
     loss = eng.forward(noise_seeds, gamma, n_steps, n_steps_loss if n_steps_loss else max(n_steps, 1),
                        dt, calc_loss)
     x, v = eng.get_state()
@@ -89,23 +97,20 @@ def reverse_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
     Returns (sys, l, dl_dp, l_rdf, l_ev)."""
     if n_steps_trunc > n_steps_loss:
         raise ValueError("n_steps_trunc must not be greater than n_steps_loss")
-    _check_loss(loss_type)
     eng = fwd_loggers
     if not isinstance(eng, Engine):
         raise TypeError("fwd_loggers must be the loggers of a forward_sim result")
+    _set_loss(eng, loss_type, loss_terms)
     eng.set_params(params)
     eng.set_state(coords, velocities)
-    if loss_terms is not None:
-        eng.set_loss(loss_terms)
     clip = np.inf if clip_norm_threshold is None else float(clip_norm_threshold)
     loss, g = eng.reverse(noise_seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip)
     x, v = eng.get_state()
     sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
+    l_rdf, l_ev = eng.loss_parts()
     if eng.R == 1:
-        l, dl_dp = float(loss[0]), g[0]
-    else:
-        l, dl_dp = loss, g
-    return sys, l, dl_dp, l, 0.0 * l
+        return sys, float(loss[0]), g[0], float(l_rdf[0]), float(l_ev[0])
+    return sys, loss, g, l_rdf, l_ev
 
 
 def reweighting_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss, params,
@@ -113,41 +118,41 @@ def reweighting_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n
                     engine=None, precision="fp64", temp=C.TEMP):
     """water.jl:1107-1210: the ensemble-reweighting gradient estimator,
     dL/dtheta = <dl/dtheta> - beta (<L dE/dtheta> - <L> <dE/dtheta>), averages over the loss
-    points (every n_steps_loss steps) of one forward run, beta = 1 / (k_B T).  The RDF loss has
-    no direct parameter dependence (dl/dtheta = 0).  Returns (sys, loss, grads, l_rdf, l_ev)."""
+    points (every n_steps_loss steps) of one forward run, beta = 1 / (k_B T); dl/dtheta is the
+    enthalpy term's direct gradient (zero for the RDF loss).  Returns
+    (sys, loss, grads, l_rdf, l_ev)."""
     if use_barostat:
         raise NotImplementedError("the Monte-Carlo barostat is not part of the engine")
-    _check_loss(loss_type)
     eng = _engine_for(coords, boundary, inter_type, engine, precision)
     eng.set_params(params)
     eng.set_state(coords, velocities)
-    if loss_terms is not None:
-        eng.set_loss(loss_terms)
-    if not eng.terms:
-        raise ValueError("reweighting_sim needs loss_terms")
+    _set_loss(eng, loss_type, loss_terms)
     seeds = np.asarray(noise_seeds, dtype=np.uint64)
     n_blocks = 1 if n_steps == 0 else n_steps // n_steps_loss
-    loss_acc = np.zeros(eng.R)
+    acc = np.zeros((3, eng.R))   # loss, l_rdf, l_ev
+    dl_acc = np.zeros((eng.R, eng.n_params))
     dE_acc = np.zeros((eng.R, eng.n_params))
     l_dE_acc = np.zeros((eng.R, eng.n_params))
     for b in range(n_steps // n_steps_loss):
-        # the forward run in blocks of n_steps_loss: the loss at each block's end is the
-        # reference's loss at step_n % n_steps_loss == 0 (water.jl:1168)
-        lb = eng.forward(seeds[b * n_steps_loss:(b + 1) * n_steps_loss], gamma, n_steps_loss,
-                         n_steps_loss, dt)
+        # the forward run in blocks of n_steps_loss; loss_and_grads at each block's end is the
+        # reference's at step_n % n_steps_loss == 0 (water.jl:1176)
+        eng.forward(seeds[b * n_steps_loss:(b + 1) * n_steps_loss], gamma, n_steps_loss,
+                    n_steps_loss, dt, calc_loss=False)
+        lb, lrb, leb, _, dlb = eng.loss_and_grads()
         _, dE = eng.energy_grad()
-        loss_acc += lb
+        acc += np.stack([lb, lrb, leb])
+        dl_acc += dlb
         dE_acc += dE
         l_dE_acc += lb[:, None] * dE
-    loss = loss_acc / n_blocks
+    loss, l_rdf, l_ev = acc / n_blocks
     beta = 1.0 / (C.KB * np.asarray(temp, dtype=np.float64))
     beta = np.broadcast_to(beta, (eng.R,))[:, None]
-    grads = -beta * (l_dE_acc / n_blocks - loss[:, None] * dE_acc / n_blocks)
+    grads = dl_acc / n_blocks - beta * (l_dE_acc / n_blocks - loss[:, None] * dE_acc / n_blocks)
     x, v = eng.get_state()
     sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
     if eng.R == 1:
-        return sys, float(loss[0]), grads[0], float(loss[0]), 0.0
-    return sys, loss, grads, loss, 0.0 * loss
+        return sys, float(loss[0]), grads[0], float(l_rdf[0]), float(l_ev[0])
+    return sys, loss, grads, l_rdf, l_ev
 
 
 def default_params(inter_type="lj"):
