@@ -39,8 +39,7 @@ typedef struct {
     double y, dy, fc, dfc;
 } node_act;
 
-static void node_forward(const mlp_view *m, double r, double rc, node_act *a) {
-    const double w = ORC_MLP_WIDTH;
+static void node_forward(const mlp_view *m, double r, double rc, double w, node_act *a) {
     for (int k = 0; k < NR; k++) {
         const double mu = k * rc / (NR - 1), e = r - mu;
         a->phi[k] = exp(-e * e / (2 * w * w));
@@ -80,13 +79,13 @@ static void node_forward(const mlp_view *m, double r, double rc, node_act *a) {
     a->dfc = -0.5 * M_PI / rc * sin(x);
 }
 
-void orc_mlp_nodes(const double *theta, double rc, double *u, double *du) {
-    for (int t = 0; t < ORC_MLP_NT; t++) {
+void orc_mlp_nodes_n(const double *theta, int32_t nt, double rc, double w, double *u, double *du) {
+    for (int t = 0; t < nt; t++) {
         const mlp_view m = view(theta, t);
 #pragma omp parallel for schedule(static)
         for (int g = 0; g <= NG; g++) {
             node_act a;
-            node_forward(&m, g * (rc / NG), rc, &a);
+            node_forward(&m, g * (rc / NG), rc, w, &a);
             u[t * (NG + 1) + g] = a.y * a.fc;
             du[t * (NG + 1) + g] = a.dy * a.fc + a.y * a.dfc;
         }
@@ -101,12 +100,16 @@ static void hermite(double y0, double d0, double y1, double d1, double h, double
     c[3] = 2.0 * (y0 - y1) + h * (d0 + d1);
 }
 
-void orc_mlp_table(const double *theta, double rc, double *coef) {
-    double *u = (double *)malloc(sizeof(double) * ORC_MLP_NT * (NG + 1));
-    double *du = (double *)malloc(sizeof(double) * ORC_MLP_NT * (NG + 1));
-    orc_mlp_nodes(theta, rc, u, du);
+void orc_mlp_nodes(const double *theta, double rc, double *u, double *du) {
+    orc_mlp_nodes_n(theta, ORC_MLP_NT, rc, ORC_MLP_WIDTH, u, du);
+}
+
+void orc_mlp_table_n(const double *theta, int32_t nt, double rc, double w, double *coef) {
+    double *u = (double *)malloc(sizeof(double) * nt * (NG + 1));
+    double *du = (double *)malloc(sizeof(double) * nt * (NG + 1));
+    orc_mlp_nodes_n(theta, nt, rc, w, u, du);
     const double h = rc / NG;
-    for (int t = 0; t < ORC_MLP_NT; t++)
+    for (int t = 0; t < nt; t++)
         for (int g = 0; g < NG; g++) {
             const int b = t * (NG + 1) + g;
             hermite(u[b], du[b], u[b + 1], du[b + 1], h, coef + ((size_t)t * NG + g) * 4);
@@ -131,9 +134,18 @@ void orc_mlp_pair(const double *coef, int32_t type, double rc, double r, double 
     if (dF) *dF = -d2;
 }
 
+void orc_mlp_table(const double *theta, double rc, double *coef) {
+    orc_mlp_table_n(theta, ORC_MLP_NT, rc, ORC_MLP_WIDTH, coef);
+}
+
 void orc_mlp_backprop(const double *theta, double rc, const double *coef_adj, double *dtheta) {
+    orc_mlp_backprop_n(theta, ORC_MLP_NT, rc, ORC_MLP_WIDTH, coef_adj, dtheta);
+}
+
+void orc_mlp_backprop_n(const double *theta, int32_t nt, double rc, double w, const double *coef_adj,
+                        double *dtheta) {
     const double h = rc / NG;
-    for (int t = 0; t < ORC_MLP_NT; t++) {
+    for (int t = 0; t < nt; t++) {
         const mlp_view m = view(theta, t);
         /* coefficient adjoints -> node value / derivative adjoints */
         double *au = (double *)calloc(NG + 1, sizeof(double));
@@ -151,7 +163,7 @@ void orc_mlp_backprop(const double *theta, double rc, const double *coef_adj, do
         for (int g = 0; g <= NG; g++) {
             if (au[g] == 0.0 && ad[g] == 0.0) continue;
             node_act a;
-            node_forward(&m, g * h, rc, &a);
+            node_forward(&m, g * h, rc, w, &a);
             /* u = y fc, u' = y' fc + y fc' */
             const double yb = au[g] * a.fc + ad[g] * a.dfc, dyb = ad[g] * a.fc;
             double z2b[H], dz2b[H], h1b[H], dh1b[H];

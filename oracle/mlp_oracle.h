@@ -40,6 +40,12 @@ void orc_mlp_pair(const double *coef, int32_t type, double rc, double r, double 
 /* Adjoint of the interval coefficients -> dtheta (accumulated): the chain rule through the
  * Hermite coefficients, the node values and derivatives, and the MLP. */
 void orc_mlp_backprop(const double *theta, double rc, const double *coef_adj, double *dtheta);
+/* The same three for the first nt types of theta and RBF width w (the functions above are
+ * nt = ORC_MLP_NT, w = ORC_MLP_WIDTH); the Stillinger-Weber path uses one type. */
+void orc_mlp_nodes_n(const double *theta, int32_t nt, double rc, double w, double *u, double *du);
+void orc_mlp_table_n(const double *theta, int32_t nt, double rc, double w, double *coef);
+void orc_mlp_backprop_n(const double *theta, int32_t nt, double rc, double w, const double *coef_adj,
+                        double *dtheta);
 /* Xavier-uniform W1, W2; w3 Xavier-uniform times 0.01; zero biases; seeded. */
 void orc_mlp_init(uint64_t seed, double *theta);
 

@@ -42,7 +42,8 @@ class OrcLoss(ctypes.Structure):
 
 
 class OrcSwSystem(ctypes.Structure):
-    _fields_ = [("n_atoms", _I32), ("box", _D), ("mass", _D), ("kB", _D), ("temp", _D)]
+    _fields_ = [("n_atoms", _I32), ("box", _D), ("mass", _D), ("kB", _D), ("temp", _D),
+                ("mlp", _I32)]
 
 
 class OrcSwLoss(ctypes.Structure):
@@ -103,6 +104,12 @@ def lib():
         L.orc_vec1d.restype = _D
         L.orc_vec1d.argtypes = [_D, _D, _D]
         PS, PL = ctypes.POINTER(OrcSwSystem), ctypes.POINTER(OrcSwLoss)
+        L.orc_sw_n_params.restype = _I32
+        L.orc_sw_n_params.argtypes = [PS]
+        L.orc_sw_contract.argtypes = [PS, _PD, _PD, _PD, _PD]
+        L.orc_mlp_nodes_n.argtypes = [_PD, _I32, _D, _D, _PD, _PD]
+        L.orc_mlp_table_n.argtypes = [_PD, _I32, _D, _D, _PD]
+        L.orc_mlp_backprop_n.argtypes = [_PD, _I32, _D, _D, _PD, _PD]
         L.orc_sw_energy.restype = _D
         L.orc_sw_energy.argtypes = [PS, _PD, _PD]
         L.orc_sw_forces.argtypes = [PS, _PD, _PD, _PD]
@@ -315,8 +322,22 @@ def num_threads():
 SW_NP = 7
 
 
-def make_sw_system(n_atoms, box, temp=298.0, *, mass=12.011, kB=0.00831446261815324):
-    return OrcSwSystem(n_atoms, box, mass, kB, temp)
+SW_MLP_RC, SW_MLP_WIDTH = 0.25, 0.0125   # the learned radial term (sw_oracle.h)
+
+
+def make_sw_system(n_atoms, box, temp=298.0, *, mass=12.011, kB=0.00831446261815324, mlp=False):
+    return OrcSwSystem(n_atoms, box, mass, kB, temp, 1 if mlp else 0)
+
+
+def sw_n_params(s):
+    return lib().orc_sw_n_params(ctypes.byref(s))
+
+
+def sw_contract(s, theta, x, acoef):
+    """sum_a acoef_a . dF_a/dtheta for every parameter (SW, then the learned term's)."""
+    out = np.zeros(sw_n_params(s))
+    lib().orc_sw_contract(ctypes.byref(s), _pd(_f64(theta)), _pd(_f64(x)), _pd(_f64(acoef)), _pd(out))
+    return out
 
 
 def make_sw_loss(weight=5e-8, target=None, vel_term=True):
@@ -362,7 +383,7 @@ def sw_stress(s, theta, x, v, vel_term=True):
 
 def sw_loss_grad(s, theta, loss, x, v):
     x, v = _f64(x), _f64(v)
-    gx, gv, gp = np.zeros(x.size), np.zeros(x.size), np.zeros(SW_NP)
+    gx, gv, gp = np.zeros(x.size), np.zeros(x.size), np.zeros(sw_n_params(s))
     val = lib().orc_sw_loss_grad(ctypes.byref(s), _pd(_f64(theta)), ctypes.byref(loss), _pd(x),
                                  _pd(v), _pd(gx), _pd(gv), _pd(gp))
     return val, gx.reshape(-1, 3), gv.reshape(-1, 3), gp
@@ -397,7 +418,7 @@ def sw_reverse_sim(s, theta, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_
     x, v = _f64(x).copy(), _f64(v).copy()
     seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
     sx, sv = _f64(snaps_x), _f64(snaps_v)
-    g = np.zeros(SW_NP)
+    g = np.zeros(sw_n_params(s))
     val = lib().orc_sw_reverse_sim(ctypes.byref(s), _pd(_f64(theta)), _pd(x), _pd(v),
                                    seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss,
                                    n_steps_trunc, len(sx), dt, _pd(sx), _pd(sv),
@@ -452,3 +473,9 @@ def mlp_backprop(theta, coef_adj, rc=1.0):
     out = np.zeros(MLP_NPARAMS)
     lib().orc_mlp_backprop(_pd(_f64(theta)), rc, _pd(_f64(coef_adj)), _pd(out))
     return out
+
+
+def mlp_table_n(theta, nt, rc, width):
+    c = np.zeros((nt, MLP_NG, 4))
+    lib().orc_mlp_table_n(_pd(_f64(theta)), nt, rc, width, _pd(c))
+    return c

@@ -14,10 +14,55 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "mlp_oracle.h"
 #include "revsim_oracle.h"
 
 typedef double complex cplx;
 static const double kH = 1e-30;   /* complex-step size */
+
+int32_t orc_sw_n_params(const orc_sw_system *s) { return ORC_SW_NP + (s->mlp ? ORC_MLP_PER_TYPE : 0); }
+
+/* ---------------------------------------------------------- learned radial term */
+static const double kMlpHinv = ORC_MLP_NG / ORC_SW_MLP_RC;
+
+/* Interval coefficients [NG][4] of the learned term, or NULL without it. */
+static double *mlp_coef(const orc_sw_system *s, const double *theta) {
+    if (!s->mlp) return NULL;
+    double *c = (double *)malloc(sizeof(double) * ORC_MLP_NG * 4);
+    orc_mlp_table_n(theta + ORC_SW_NP, 1, ORC_SW_MLP_RC, ORC_SW_MLP_WIDTH, c);
+    return c;
+}
+
+static inline int mlp_seg(double r) {
+    int g = (int)floor(r * kMlpHinv);
+    return g < 0 ? 0 : (g > ORC_MLP_NG - 1 ? ORC_MLP_NG - 1 : g);
+}
+
+static double mlp_e(const double *coef, double r) {
+    const int g = mlp_seg(r);
+    const double sv = r * kMlpHinv - g, *c = coef + 4 * g;
+    return c[0] + sv * (c[1] + sv * (c[2] + sv * c[3]));
+}
+
+/* g_j = u'(r) d / r for d = x_j - x_i: u' is a cubic in r on the interval of the real
+ * distance, so the complex step through it is exact. */
+static void mlp_g(const cplx d[3], const double *coef, cplx gj[3]) {
+    const cplx r = csqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const int g = mlp_seg(creal(r));
+    const cplx sv = r * kMlpHinv - g;
+    const double *c = coef + 4 * g;
+    const cplx du = (c[1] + sv * (2.0 * c[2] + 3.0 * sv * c[3])) * kMlpHinv;
+    for (int u = 0; u < 3; u++) gj[u] = du * d[u] / r;
+}
+
+/* adj[g][k] += wgt d u'(r) / dc_k = wgt k s^(k-1) / h  (k = 1..3; c_0 does not enter u'). */
+static void mlp_adj(double r, double wgt, double *adj) {
+    const int g = mlp_seg(r);
+    const double sv = r * kMlpHinv - g, w = wgt * kMlpHinv;
+    adj[4 * g + 1] += w;
+    adj[4 * g + 2] += 2.0 * w * sv;
+    adj[4 * g + 3] += 3.0 * w * sv * sv;
+}
 
 /* ----------------------------------------------------------------- terms */
 /* 2-body gradient g_j = dE2/dx_j for d = x_j - x_i (g_i = -g_j), diamond.jl:348-356 and
@@ -119,8 +164,9 @@ static void free_nbrs(nbrs *nb) {
 typedef void (*term_cb)(void *ctx, int na, const int *atoms, const cplx (*g)[3],
                         const double (*dc)[3]);
 
-static void visit_terms(const orc_sw_system *s, const double *theta, const nbrs *nb, int mode,
-                        const double *tan, int p_idx, term_cb cb, void *ctx) {
+static void visit_terms(const orc_sw_system *s, const double *theta, const double *coef,
+                        const nbrs *nb, int mode, const double *tan, int p_idx, term_cb cb,
+                        void *ctx) {
     cplx p[ORC_SW_NP];
     for (int q = 0; q < ORC_SW_NP; q++) p[q] = theta[q] + ((mode == 2 && q == p_idx) ? I * kH : 0.0);
     const int n = nb->n;
@@ -139,6 +185,11 @@ static void visit_terms(const orc_sw_system *s, const double *theta, const nbrs 
                     d[u] = dj[u] + I * kH * t;
                 }
                 sw2_g(d, p, gj);
+                if (coef && sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]) < ORC_SW_MLP_RC) {
+                    cplx gm[3];
+                    mlp_g(d, coef, gm);
+                    for (int u = 0; u < 3; u++) gj[u] += gm[u];
+                }
                 for (int u = 0; u < 3; u++) {
                     g[0][u] = -gj[u];
                     g[1][u] = gj[u];
@@ -205,16 +256,22 @@ static void cb_vir(void *vctx, int na, const int *atoms, const cplx (*g)[3], con
 double orc_sw_energy(const orc_sw_system *s, const double *theta, const double *x) {
     nbrs nb;
     build_nbrs(s, theta, x, &nb);
+    double *coef = mlp_coef(s, theta);
     double E = 0.0;
     for (int i = 0; i < nb.n; i++) {
         for (int qa = 0; qa < nb.cnt[i]; qa++) {
             const int j = nb.idx[i * nb.cap + qa];
             const double *dj = nb.d + 3 * ((size_t)i * nb.cap + qa);
-            if (j > i) E += sw2_e(dj, theta);
+            if (j > i) {
+                E += sw2_e(dj, theta);
+                const double r = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
+                if (coef && r < ORC_SW_MLP_RC) E += mlp_e(coef, r);
+            }
             for (int qb = qa + 1; qb < nb.cnt[i]; qb++)
                 E += sw3_e(dj, nb.d + 3 * ((size_t)i * nb.cap + qb), theta);
         }
     }
+    free(coef);
     free_nbrs(&nb);
     return E;
 }
@@ -247,16 +304,17 @@ void orc_sw_forces_grads(const orc_sw_system *s, const double *theta, const doub
     const int n3 = 3 * s->n_atoms;
     nbrs nb;
     build_nbrs(s, theta, x, &nb);
+    double *coef = mlp_coef(s, theta);
     memset(F, 0, sizeof(double) * n3);
     acc_ctx c = {F, 0, -1.0};
-    visit_terms(s, theta, &nb, 0, NULL, 0, cb_acc, &c);
+    visit_terms(s, theta, coef, &nb, 0, NULL, 0, cb_acc, &c);
     if (dl_dfi && w) {
         /* J (w/m): the tangent of F along w/m; J is symmetric (a Hessian) */
         double *t = (double *)malloc(sizeof(double) * n3);
         for (int e = 0; e < n3; e++) t[e] = w[e] / s->mass;
         memset(dl_dfi, 0, sizeof(double) * n3);
         acc_ctx cg = {dl_dfi, 1, -1.0};
-        visit_terms(s, theta, &nb, 1, t, 0, cb_acc, &cg);
+        visit_terms(s, theta, coef, &nb, 1, t, 0, cb_acc, &cg);
         free(t);
     }
     if (dF_dp) {
@@ -264,12 +322,52 @@ void orc_sw_forces_grads(const orc_sw_system *s, const double *theta, const doub
         for (int p = 0; p < ORC_SW_NP; p++) {
             memset(col, 0, sizeof(double) * n3);
             acc_ctx cp = {col, 1, -1.0};
-            visit_terms(s, theta, &nb, 2, NULL, p, cb_acc, &cp);
+            visit_terms(s, theta, coef, &nb, 2, NULL, p, cb_acc, &cp);
             for (int e = 0; e < n3; e++) dF_dp[e * ORC_SW_NP + p] = col[e];
         }
         free(col);
     }
+    free(coef);
     free_nbrs(&nb);
+}
+
+/* Learned-term coefficient adjoints of sum_a acoef_a . dF_a/dc: per pair F_j = -g_j,
+ * F_i = g_j, so the weight is -(acoef_j - acoef_i) . d / r. */
+static void mlp_contract_adj(const orc_sw_system *s, const nbrs *nb, const double *acoef, double *adj) {
+    for (int i = 0; i < nb->n; i++)
+        for (int q = 0; q < nb->cnt[i]; q++) {
+            const int j = nb->idx[i * nb->cap + q];
+            if (j <= i) continue;
+            const double *d = nb->d + 3 * ((size_t)i * nb->cap + q);
+            const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (!(r < ORC_SW_MLP_RC)) continue;
+            double zu = 0.0;
+            for (int u = 0; u < 3; u++) zu += (acoef[3 * j + u] - acoef[3 * i + u]) * d[u] / r;
+            mlp_adj(r, -zu, adj);
+        }
+    (void)s;
+}
+
+void orc_sw_contract(const orc_sw_system *s, const double *theta, const double *x,
+                     const double *acoef, double *dtheta) {
+    const int n3 = 3 * s->n_atoms, P = orc_sw_n_params(s);
+    double *F = (double *)malloc(sizeof(double) * n3);
+    double *J = (double *)malloc(sizeof(double) * n3 * ORC_SW_NP);
+    orc_sw_forces_grads(s, theta, x, NULL, F, NULL, J);
+    for (int p = 0; p < P; p++) dtheta[p] = 0.0;
+    for (int p = 0; p < ORC_SW_NP; p++)
+        for (int e = 0; e < n3; e++) dtheta[p] += acoef[e] * J[e * ORC_SW_NP + p];
+    if (s->mlp) {
+        nbrs nb;
+        build_nbrs(s, theta, x, &nb);
+        double *adj = (double *)calloc(ORC_MLP_NG * 4, sizeof(double));
+        mlp_contract_adj(s, &nb, acoef, adj);
+        orc_mlp_backprop_n(theta + ORC_SW_NP, 1, ORC_SW_MLP_RC, ORC_SW_MLP_WIDTH, adj, dtheta + ORC_SW_NP);
+        free(adj);
+        free_nbrs(&nb);
+    }
+    free(F);
+    free(J);
 }
 
 /* Kinetic tensor -sum m (v - vbar)(v - vbar)^T (diamond.jl:754-756). */
@@ -290,9 +388,11 @@ void orc_sw_stress(const orc_sw_system *s, const double *theta, const double *x,
                    int32_t vel_term, double *sigma) {
     nbrs nb;
     build_nbrs(s, theta, x, &nb);
+    double *coef = mlp_coef(s, theta);
     vir_ctx c;
     memset(&c, 0, sizeof(c));
-    visit_terms(s, theta, &nb, 0, NULL, 0, cb_vir, &c);
+    visit_terms(s, theta, coef, &nb, 0, NULL, 0, cb_vir, &c);
+    free(coef);
     double K[9], vb[3];
     kinetic(s, v, K, vb);
     const double V = s->box * s->box * s->box;
@@ -331,14 +431,15 @@ double orc_sw_loss_grad(const orc_sw_system *s, const double *theta, const orc_s
     if (dLdx || dLdp) {
         nbrs nb;
         build_nbrs(s, theta, x, &nb);
+        double *coef = mlp_coef(s, theta);
         if (dLdx) {
             /* (1/V) [ H u + S^T g ], u_a = S d_a per term */
             memset(dLdx, 0, sizeof(double) * n3);
             acc_ctx ch = {dLdx, 1, 1.0 / V};
-            visit_terms(s, theta, &nb, 3, S, 0, cb_acc, &ch);
+            visit_terms(s, theta, coef, &nb, 3, S, 0, cb_acc, &ch);
             double *g = (double *)calloc((size_t)n3, sizeof(double));
             acc_ctx cg = {g, 0, 1.0};
-            visit_terms(s, theta, &nb, 0, NULL, 0, cb_acc, &cg);
+            visit_terms(s, theta, coef, &nb, 0, NULL, 0, cb_acc, &cg);
             for (int a = 0; a < n; a++)
                 for (int gm = 0; gm < 3; gm++) {
                     double t = 0.0;
@@ -352,12 +453,33 @@ double orc_sw_loss_grad(const orc_sw_system *s, const double *theta, const orc_s
                 vir_ctx c;
                 memset(&c, 0, sizeof(c));
                 c.imag = 1;
-                visit_terms(s, theta, &nb, 2, NULL, p, cb_vir, &c);
+                visit_terms(s, theta, coef, &nb, 2, NULL, p, cb_vir, &c);
                 double t = 0.0;
                 for (int q = 0; q < 9; q++) t += S[q] * c.W[q];
                 dLdp[p] = t / V;
             }
+            if (coef) {
+                /* W += g_j (x) d per pair: dL/dc = sum_ab S_ab d_a d_b / (r V) du'/dc */
+                double *adj = (double *)calloc(ORC_MLP_NG * 4, sizeof(double));
+                for (int i = 0; i < nb.n; i++)
+                    for (int q = 0; q < nb.cnt[i]; q++) {
+                        const int j = nb.idx[i * nb.cap + q];
+                        if (j <= i) continue;
+                        const double *d = nb.d + 3 * ((size_t)i * nb.cap + q);
+                        const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                        if (!(r < ORC_SW_MLP_RC)) continue;
+                        double t = 0.0;
+                        for (int al = 0; al < 3; al++)
+                            for (int be = 0; be < 3; be++) t += S[3 * al + be] * d[al] * d[be];
+                        mlp_adj(r, t / (r * V), adj);
+                    }
+                for (int p = ORC_SW_NP; p < orc_sw_n_params(s); p++) dLdp[p] = 0.0;
+                orc_mlp_backprop_n(theta + ORC_SW_NP, 1, ORC_SW_MLP_RC, ORC_SW_MLP_WIDTH, adj,
+                                   dLdp + ORC_SW_NP);
+                free(adj);
+            }
         }
+        free(coef);
         free_nbrs(&nb);
     }
     return loss;
@@ -428,10 +550,12 @@ double orc_sw_reverse_sim(const orc_sw_system *s, const double *theta, double *x
     double *F = buf, *xi = buf + n3, *g = buf + 2 * n3, *h = buf + 3 * n3, *A = buf + 4 * n3;
     double *B = buf + 5 * n3, *C = buf + 6 * n3, *D = buf + 7 * n3, *G = buf + 8 * n3;
     double *acoef = buf + 9 * n3, *w = buf + 10 * n3;
-    double dp[ORC_SW_NP];
+    const int P = orc_sw_n_params(s);
+    double *dp = (double *)malloc(sizeof(double) * P);
+    double *adj = s->mlp ? (double *)calloc(ORC_MLP_NG * 4, sizeof(double)) : NULL;
     double *dF_dp = (double *)malloc(sizeof(double) * n3 * ORC_SW_NP);
     double loss = orc_sw_loss_grad(s, theta, L, x, v, g, h, dp);
-    for (int p = 0; p < ORC_SW_NP; p++) dl_dp[p] = dp[p];
+    for (int p = 0; p < P; p++) dl_dp[p] = dp[p];
     sw_reset(n3, c, dt, g, h, A, B, C, D, G);
     for (int lc = 1; lc <= n_blocks; lc++) {   /* diamond.jl:1799-1868 */
         const int step_start = n_steps - (lc - 1) * n_steps_loss;
@@ -452,6 +576,12 @@ double orc_sw_reverse_sim(const orc_sw_system *s, const double *theta, double *x
                 for (int e = 0; e < n3; e++) t += acoef[e] * dF_dp[e * ORC_SW_NP + p];
                 dl_dp[p] += t;
             }
+            if (adj) {
+                nbrs nb;
+                build_nbrs(s, theta, x, &nb);
+                mlp_contract_adj(s, &nb, acoef, adj);
+                free_nbrs(&nb);
+            }
             for (int e = 0; e < n3; e++) v[e] = v[e] - F[e] * dt / s->mass;
             for (int e = 0; e < n3; e++) B[e] = c * B[e] + dt2 * G[e];
             for (int e = 0; e < n3; e++) A[e] = A[e] + B[e];
@@ -461,12 +591,15 @@ double orc_sw_reverse_sim(const orc_sw_system *s, const double *theta, double *x
             memcpy(x, snap_x + si, sizeof(double) * n3);
             memcpy(v, snap_v + si, sizeof(double) * n3);
             loss += orc_sw_loss_grad(s, theta, L, x, v, g, h, dp);
-            for (int p = 0; p < ORC_SW_NP; p++) dl_dp[p] += dp[p];
+            for (int p = 0; p < P; p++) dl_dp[p] += dp[p];
             sw_reset(n3, c, dt, g, h, A, B, C, D, G);
         }
     }
-    for (int p = 0; p < ORC_SW_NP; p++) dl_dp[p] /= n_blocks;
+    if (adj) orc_mlp_backprop_n(theta + ORC_SW_NP, 1, ORC_SW_MLP_RC, ORC_SW_MLP_WIDTH, adj, dl_dp + ORC_SW_NP);
+    for (int p = 0; p < P; p++) dl_dp[p] /= n_blocks;
     free(buf);
     free(dF_dp);
+    free(dp);
+    free(adj);
     return loss / n_blocks;
 }
