@@ -30,6 +30,15 @@ extern "C" {
 #endif
 
 #define REVSIM_SW_NPARAMS 7
+/* The learned radial term (desc.mlp = 1): one MLP pair function of r on [0, 0.25 nm]
+ * (16 Gaussian radial basis functions of width 0.0125 nm -> 64 -> 64 SiLU -> 1, times a
+ * cosine cutoff; the layout of revsim.h's per-type MLP), tabulated as cubic Hermite segments
+ * on 1,024 intervals and added to the 2-body term of every active pair with r < 0.25 nm.
+ * Its REVSIM_SW_MLP_NPARAMS parameters follow the 7 SW ones in every theta / gradient
+ * array (n_params = 7 + REVSIM_SW_MLP_NPARAMS).  It stands in for the reference's learned
+ * GNN term (params_gnn of diamond.jl:1394, 1757). */
+#define REVSIM_SW_MLP_NPARAMS 5313
+#define REVSIM_SW_MLP_CUTOFF 0.25
 
 typedef struct revsim_sw_handle revsim_sw_handle;
 
@@ -45,6 +54,7 @@ typedef struct {
     int32_t n_steps_nf;       /* candidate-list rebuild interval, steps; halved (and the call
                                  rerun) whenever an atom moves more than skin / 2 between builds */
     int32_t device;
+    int32_t mlp;              /* 1: add the learned radial term */
 } revsim_sw_desc;
 
 /* Stress loss weight * sum_ab (sigma_ab - target_ab)^2 / 9 per replica (diamond.jl:772-775). */
@@ -58,7 +68,8 @@ int32_t revsim_sw_create(const revsim_sw_desc *desc, revsim_sw_handle **out);
 void revsim_sw_destroy(revsim_sw_handle *h);
 const char *revsim_sw_last_error(const revsim_sw_handle *h);
 
-/* theta [7]: StillingerWeber(A, B, 4, 0, a, lambda, gamma, sigma, eps), diamond.jl:1352-1356. */
+/* theta [n_params]: StillingerWeber(A, B, 4, 0, a, lambda, gamma, sigma, eps),
+ * diamond.jl:1352-1356, then the learned term's parameters when desc.mlp. */
 int32_t revsim_sw_set_params(revsim_sw_handle *h, const double *theta, int32_t n);
 /* x, v [3 N] (x is wrapped into each replica's box by the caller, as Molly keeps it). */
 int32_t revsim_sw_set_state(revsim_sw_handle *h, const double *x, const double *v);
@@ -68,14 +79,14 @@ int32_t revsim_sw_set_loss(revsim_sw_handle *h, const revsim_sw_loss *loss);
 /* forces_sw (diamond.jl:534-541): F [3 N]. */
 int32_t revsim_sw_forces(revsim_sw_handle *h, double *F);
 /* sw_force_and_grads! (diamond.jl:1658-1697): F, dl_dfi[b] = sum_a (w_a / m) . dF_a/dx_b
- * and dtheta [n_replicas * 7] = sum_a acoef_a . dF_a/dtheta per replica (acoef may be NULL,
+ * and dtheta [n_replicas * n_params] = sum_a acoef_a . dF_a/dtheta per replica (acoef may be NULL,
  * then dtheta is not written). */
 int32_t revsim_sw_force_vjp(revsim_sw_handle *h, const double *w, const double *acoef, double *F,
                             double *dl_dfi, double *dtheta);
 /* virial_stress_tensor (diamond.jl:753-770): sigma [n_replicas * 9]. */
 int32_t revsim_sw_stress(revsim_sw_handle *h, int32_t vel_term, double *sigma);
 /* loss_and_grads for :stress (diamond.jl:1342-1350): loss [n_replicas], dL/dx, dL/dv [3 N],
- * dL/dtheta [n_replicas * 7]; any output may be NULL. */
+ * dL/dtheta [n_replicas * n_params]; any output may be NULL. */
 int32_t revsim_sw_loss_grad(revsim_sw_handle *h, double *loss, double *dLdx, double *dLdv,
                             double *dLdtheta);
 /* generate_noise! (diamond.jl:1387-1392) for one seed per replica: xi [3 N]. */
@@ -93,7 +104,7 @@ int32_t revsim_sw_forward(revsim_sw_handle *h, const uint64_t *noise_seeds, doub
                           int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_buffer, double dt,
                           int32_t calc_loss, double *loss, int32_t *n_blocks);
 /* reverse_sim (diamond.jl:1757-1878) from the handle's state (the forward end state):
- * loss [n_replicas], dl_dtheta [n_replicas * 7], each the mean over the loss blocks of
+ * loss [n_replicas], dl_dtheta [n_replicas * n_params], each the mean over the loss blocks of
  * the forward pass run last on this handle with the same n_steps and n_steps_loss. */
 int32_t revsim_sw_reverse(revsim_sw_handle *h, const uint64_t *noise_seeds, double gamma,
                           int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_trunc, double dt,

@@ -153,12 +153,15 @@ cudaError_t launch_enth_dldx(int N, const int *atom_rep, const double *k, const 
 
 size_t mlp_scratch_doubles();
 // Node evaluation and interval table of the MLP for parameters theta (device, FP64).
+// nt types (1..MLP_NT) of theta, RBF width w: the water model's three types at MLP_WIDTH by
+// default; the Stillinger-Weber radial term uses one type.
 cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *scratch, void *tab,
-                             cudaStream_t st);
+                             cudaStream_t st, int nt = MLP_NT, double w = MLP_WIDTH);
 // Interval-coefficient adjoints (the sum of ncopy accumulators) -> dtheta [MLP_NPARAMS]
 // (after launch_mlp_table with the same theta and scratch).
 cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, int ncopy,
-                                double *scratch, double *dtheta, cudaStream_t st);
+                                double *scratch, double *dtheta, cudaStream_t st, int nt = MLP_NT,
+                                double w = MLP_WIDTH);
 
 cudaError_t launch_pack(int N, int prec, const double *x, const double *C, double mO, double mH,
                         const int *atom_rep, const double *rep_box, void *pos, void *wgt,

@@ -8,6 +8,8 @@
 // kernels interpolate each pair with the cubic Hermite segment of its interval (one
 // 16- or 32-byte table load per pair).  The reverse pass accumulates the adjoints of the
 // interval coefficients; k_mlp_* below carry them back to the weights once per pass.
+// The same code serves the Stillinger-Weber path's learned radial term (one type, its own
+// cutoff and width): the type count nt and width w are arguments.
 #include "rs_internal.h"
 
 namespace rs {
@@ -43,8 +45,8 @@ __device__ __forceinline__ double silu2(double z) {
     return s * (1.0 - s) * (2.0 + z * (1.0 - 2.0 * s));
 }
 
-__device__ __forceinline__ void rbf(double r, double rc, int k, double &phi, double &dphi) {
-    const double w = MLP_WIDTH, mu = k * rc / (NR - 1), e = r - mu;
+__device__ __forceinline__ void rbf(double r, double rc, double w, int k, double &phi, double &dphi) {
+    const double mu = k * rc / (NR - 1), e = r - mu;
     phi = exp(-e * e / (2.0 * w * w));
     dphi = -e / (w * w) * phi;
 }
@@ -63,13 +65,13 @@ __device__ __forceinline__ double block_sum64(double v, double *s) {
 }
 
 // One block (64 threads = hidden units) per (node g, type t): value and r-tangent streams.
-__global__ void __launch_bounds__(64) k_mlp_nodes(const double *theta, double rc, double *act,
+__global__ void __launch_bounds__(64) k_mlp_nodes(const double *theta, double rc, double w, double *act,
                                                   double *u, double *du) {
     __shared__ double s_phi[NR], s_dphi[NR], s_h1[H], s_dh1[H], s_red[H];
     const int g = blockIdx.x, t = blockIdx.y, i = threadIdx.x;
     const View m = view(theta, t);
     const double r = g * (rc / NG);
-    if (i < NR) rbf(r, rc, i, s_phi[i], s_dphi[i]);
+    if (i < NR) rbf(r, rc, w, i, s_phi[i], s_dphi[i]);
     __syncthreads();
     double z1 = m.b1[i], dz1 = 0.0;
     for (int k = 0; k < NR; k++) {
@@ -105,9 +107,9 @@ __global__ void __launch_bounds__(64) k_mlp_nodes(const double *theta, double rc
 
 // Hermite coefficients of every interval: p(s) = c0 + c1 s + c2 s^2 + c3 s^3, s in [0, 1].
 template <typename V4>
-__global__ void k_mlp_coef(const double *u, const double *du, double rc, V4 *tab) {
+__global__ void k_mlp_coef(const double *u, const double *du, double rc, int nt, V4 *tab) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= MLP_NT * NG) return;
+    if (k >= nt * NG) return;
     const int t = k / NG, g = k % NG;
     const double h = rc / NG;
     const double y0 = u[t * (NG + 1) + g], y1 = u[t * (NG + 1) + g + 1];
@@ -122,10 +124,10 @@ __global__ void k_mlp_coef(const double *u, const double *du, double rc, V4 *tab
 
 // Coefficient adjoints (summed over the ncopy accumulators in order) -> node value /
 // derivative adjoints (the transpose of k_mlp_coef).
-__device__ __forceinline__ void sum_copies(const double *cadj, int ncopy, size_t off, double c[4]) {
+__device__ __forceinline__ void sum_copies(const double *cadj, int ncopy, int nt, size_t off, double c[4]) {
     c[0] = c[1] = c[2] = c[3] = 0.0;
     for (int q = 0; q < ncopy; q++) {
-        const double *p = cadj + (size_t)q * MLP_NT * NG * 4 + off;
+        const double *p = cadj + (size_t)q * nt * NG * 4 + off;
         c[0] += p[0];
         c[1] += p[1];
         c[2] += p[2];
@@ -133,19 +135,19 @@ __device__ __forceinline__ void sum_copies(const double *cadj, int ncopy, size_t
     }
 }
 
-__global__ void k_mlp_adj_nodes(const double *cadj, int ncopy, double rc, double *au, double *ad) {
+__global__ void k_mlp_adj_nodes(const double *cadj, int ncopy, int nt, double rc, double *au, double *ad) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= MLP_NT * (NG + 1)) return;
+    if (k >= nt * (NG + 1)) return;
     const int t = k / (NG + 1), g = k % (NG + 1);
     const double h = rc / NG;
     double a = 0.0, d = 0.0, c[4];
     if (g < NG) {
-        sum_copies(cadj, ncopy, ((size_t)t * NG + g) * 4, c);
+        sum_copies(cadj, ncopy, nt, ((size_t)t * NG + g) * 4, c);
         a += c[0] - 3.0 * c[2] + 2.0 * c[3];
         d += h * (c[1] - 2.0 * c[2] + c[3]);
     }
     if (g > 0) {
-        sum_copies(cadj, ncopy, ((size_t)t * NG + g - 1) * 4, c);
+        sum_copies(cadj, ncopy, nt, ((size_t)t * NG + g - 1) * 4, c);
         a += 3.0 * c[2] - 2.0 * c[3];
         d += h * (c[3] - c[2]);
     }
@@ -188,9 +190,10 @@ __global__ void __launch_bounds__(64) k_mlp_node_bwd(const double *theta, const 
 }
 
 // One thread per parameter: sum over the nodes in order (deterministic).
-__global__ void k_mlp_wgrad(double rc, const double *act, const double *bwd, double *dtheta) {
+__global__ void k_mlp_wgrad(double rc, double w, int nt, const double *act, const double *bwd,
+                            double *dtheta) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= MLP_NPARAMS) return;
+    if (k >= nt * MLP_PER_TYPE) return;
     const int t = k / MLP_PER_TYPE, q = k % MLP_PER_TYPE;
     const double *A = act + (size_t)t * (NG + 1) * NA;
     const double *B = bwd + (size_t)t * (NG + 1) * NA;
@@ -199,7 +202,7 @@ __global__ void k_mlp_wgrad(double rc, const double *act, const double *bwd, dou
         const int i = q / NR, kk = q % NR;
         for (int g = 0; g <= NG; g++) {
             double phi, dphi;
-            rbf(g * (rc / NG), rc, kk, phi, dphi);
+            rbf(g * (rc / NG), rc, w, kk, phi, dphi);
             s += B[g * NA + i] * phi + B[g * NA + H + i] * dphi;
         }
     } else if (q < H * NR + H) {                   // b1[i]
@@ -232,26 +235,29 @@ __global__ void k_mlp_wgrad(double rc, const double *act, const double *bwd, dou
 size_t mlp_scratch_doubles() { return (size_t)2 * MLP_NT * (NG + 1) * NA + 4 * (size_t)MLP_NT * (NG + 1); }
 
 cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *scratch, void *tab,
-                             cudaStream_t st) {
+                             cudaStream_t st, int nt, double w) {
+    if (nt < 1 || nt > MLP_NT) return cudaErrorInvalidValue;
     const size_t S = (size_t)MLP_NT * (NG + 1) * NA, NN = (size_t)MLP_NT * (NG + 1);
     double *act = scratch, *u = scratch + 2 * S, *du = u + NN;
-    k_mlp_nodes<<<dim3(NG + 1, MLP_NT), 64, 0, st>>>(theta, rc, act, u, du);
-    const int n = MLP_NT * NG;
+    k_mlp_nodes<<<dim3(NG + 1, nt), 64, 0, st>>>(theta, rc, w, act, u, du);
+    const int n = nt * NG;
     if (prec == 1)
-        k_mlp_coef<float4><<<(n + 255) / 256, 256, 0, st>>>(u, du, rc, (float4 *)tab);
+        k_mlp_coef<float4><<<(n + 255) / 256, 256, 0, st>>>(u, du, rc, nt, (float4 *)tab);
     else
-        k_mlp_coef<double4><<<(n + 255) / 256, 256, 0, st>>>(u, du, rc, (double4 *)tab);
+        k_mlp_coef<double4><<<(n + 255) / 256, 256, 0, st>>>(u, du, rc, nt, (double4 *)tab);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, int ncopy,
-                                double *scratch, double *dtheta, cudaStream_t st) {
+                                double *scratch, double *dtheta, cudaStream_t st, int nt, double w) {
+    if (nt < 1 || nt > MLP_NT) return cudaErrorInvalidValue;
     const size_t S = (size_t)MLP_NT * (NG + 1) * NA, NN = (size_t)MLP_NT * (NG + 1);
     double *act = scratch, *bwd = scratch + S;
     double *au = scratch + 2 * S + 2 * NN, *ad = au + NN;
-    k_mlp_adj_nodes<<<(int)((NN + 255) / 256), 256, 0, st>>>(cadj, ncopy, rc, au, ad);
-    k_mlp_node_bwd<<<dim3(NG + 1, MLP_NT), 64, 0, st>>>(theta, act, au, ad, bwd);
-    k_mlp_wgrad<<<(MLP_NPARAMS + 127) / 128, 128, 0, st>>>(rc, act, bwd, dtheta);
+    const int nn = nt * (NG + 1), np = nt * MLP_PER_TYPE;
+    k_mlp_adj_nodes<<<(nn + 255) / 256, 256, 0, st>>>(cadj, ncopy, nt, rc, au, ad);
+    k_mlp_node_bwd<<<dim3(NG + 1, nt), 64, 0, st>>>(theta, act, au, ad, bwd);
+    k_mlp_wgrad<<<(np + 127) / 128, 128, 0, st>>>(rc, w, nt, act, bwd, dtheta);
     return cudaGetLastError();
 }
 

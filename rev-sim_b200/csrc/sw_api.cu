@@ -24,6 +24,8 @@
 using namespace rs;
 using namespace rs::sw;
 
+static_assert(REVSIM_SW_MLP_NPARAMS == MLP_PER_TYPE, "one MLP type of rs_mlp.cu");
+
 struct revsim_sw_handle {
     std::string err;
     int dev = 0;
@@ -34,6 +36,13 @@ struct revsim_sw_handle {
     std::vector<double> box, temp;
     double mass = 0, kB = 0, skin = 0;
     double theta[NP] = {0, 0, 0, 0, 0, 0, 0};
+    // learned radial term: its MLP parameters follow the 7 SW ones (Pt in all)
+    bool mlp = false;
+    int Pt = NP;
+    std::vector<double> theta_mlp;
+    double *d_mlp_theta = nullptr, *d_mlp_adj = nullptr, *d_mlp_scratch = nullptr,
+           *d_mlp_grad = nullptr;
+    void *d_mlp_tab = nullptr;
     bool have_params = false, have_state = false, have_loss = false;
     double weight = 0;
     int vel_term = 1;
@@ -133,6 +142,10 @@ SwConsts<R> consts(const revsim_sw_handle *h) {
     p.lim2 = lim * lim;
     p.lo2 = (lim * (1 - 1e-9)) * (lim * (1 - 1e-9));
     p.hi2 = (lim * (1 + 1e-9)) * (lim * (1 + 1e-9));
+    p.mlp_hinv = (R)(MLP_NG / MLP_RC);
+    p.mlp_hhalf = (R)(MLP_NG / (2 * MLP_RC));
+    p.mlp_hinv2 = (R)((MLP_NG / MLP_RC) * (MLP_NG / MLP_RC));
+    p.mlp_rc2 = MLP_RC * MLP_RC;
     return p;
 }
 
@@ -209,7 +222,8 @@ void free_all(revsim_sw_handle *h) {
                     h->d_x, h->d_v, h->d_F, h->d_G, h->d_A, h->d_B, h->d_C, h->d_D, h->d_dLdx,
                     h->d_dLdv, h->d_x0, h->d_v0, h->d_part, h->d_wpart, h->d_vpart, h->d_kpart,
                     h->d_vbar, h->d_sigma, h->d_S, h->d_loss, h->d_loss_acc, h->d_status,
-                    h->d_maxcnt, h->d_maxact, h->d_snap_x, h->d_snap_v, h->d_seeds};
+                    h->d_maxcnt, h->d_maxact, h->d_snap_x, h->d_snap_v, h->d_seeds,
+                    h->d_mlp_theta, h->d_mlp_adj, h->d_mlp_scratch, h->d_mlp_grad, h->d_mlp_tab};
     for (void *p : ptrs) dfree(p);
     for (auto &v : h->ev)
         for (cudaEvent_t e : v) cudaEventDestroy(e);
@@ -333,6 +347,8 @@ int terms(revsim_sw_handle *h, int mode, bool with_part, bool with_w, double aco
     a.Tt = h->d_Tt;
     a.part = with_part ? h->d_part : nullptr;
     a.wpart = with_w ? h->d_wpart : nullptr;
+    a.mlp_tab = h->mlp ? h->d_mlp_tab : nullptr;
+    a.mlp_adj = (h->mlp && with_part) ? h->d_mlp_adj : nullptr;
     a.half_skin2 = 0.25 * h->skin * h->skin;
     a.status = h->d_status;
     a.max_act = h->d_maxact;
@@ -448,6 +464,44 @@ int upload_seeds(revsim_sw_handle *h, const uint64_t *seeds, size_t n) {
     return REVSIM_OK;
 }
 
+// Zero the dtheta partials (and the learned term's coefficient adjoints).
+int zero_part(revsim_sw_handle *h) {
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * NP, h->st));
+    if (h->mlp)
+        CK(cudaMemsetAsync(h->d_mlp_adj, 0, sizeof(double) * (size_t)h->R * MLP_NCOPY * MLP_NG * 4, h->st));
+    return REVSIM_OK;
+}
+
+int reduce_part(revsim_sw_handle *h, std::vector<double> &out);
+
+// Per replica: the SW partials summed in block order, then the learned term's gradient
+// backpropagated from its coefficient adjoints; out [R][Pt] = scale * (both).
+int grads_out(revsim_sw_handle *h, double scale, double *out) {
+    std::vector<double> sw;
+    RC(reduce_part(h, sw));
+    std::vector<double> ml;
+    if (h->mlp) {
+        for (int r = 0; r < h->R; r++) {
+            cudaError_t e = launch_mlp_backprop(h->d_mlp_theta, MLP_RC,
+                                                h->d_mlp_adj + (size_t)r * MLP_NCOPY * MLP_NG * 4, MLP_NCOPY,
+                                                h->d_mlp_scratch, h->d_mlp_grad + (size_t)r * MLP_PER_TYPE,
+                                                h->st, 1, MLP_W);
+            h->launches += 3;
+            if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP backprop: ") + cudaGetErrorString(e));
+        }
+        ml.resize((size_t)h->R * MLP_PER_TYPE);
+        CK(cudaMemcpyAsync(ml.data(), h->d_mlp_grad, sizeof(double) * ml.size(), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    }
+    for (int r = 0; r < h->R; r++) {
+        for (int p = 0; p < NP; p++) out[(size_t)r * h->Pt + p] = scale * sw[(size_t)r * NP + p];
+        if (h->mlp)
+            for (int p = 0; p < MLP_PER_TYPE; p++)
+                out[(size_t)r * h->Pt + NP + p] = scale * ml[(size_t)r * MLP_PER_TYPE + p];
+    }
+    return REVSIM_OK;
+}
+
 int reduce_part(revsim_sw_handle *h, std::vector<double> &out) {
     std::vector<double> part((size_t)h->n_blk * NP);
     std::vector<int> br(h->n_blk);
@@ -525,7 +579,7 @@ int reverse_impl(revsim_sw_handle *h, double gamma, int n_steps, int n_steps_los
     const int n_blocks = h->fwd_blocks;
     const double sn = std::sqrt(1 - std::exp(-2 * gamma * dt));
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * h->R, h->st));
-    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * NP, h->st));
+    RC(zero_part(h));
     CK(cudaMemsetAsync(h->d_maxact, 0, sizeof(int), h->st));
     const double acoef_scale = dt * dt / (2 * h->mass);
     RC(build_list(h));
@@ -649,6 +703,8 @@ int32_t revsim_sw_create(const revsim_sw_desc *d, revsim_sw_handle **out) {
     h->skin = d->skin;
     h->nf = d->n_steps_nf;
     h->dev = d->device;
+    h->mlp = d->mlp != 0;
+    h->Pt = NP + (h->mlp ? MLP_PER_TYPE : 0);
     int rc = [&]() -> int {
         CK(cudaSetDevice(h->dev));
         CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
@@ -726,6 +782,13 @@ int32_t revsim_sw_create(const revsim_sw_desc *d, revsim_sw_handle **out) {
         CK(cudaMemset(h->d_maxcnt, 0, sizeof(int)));
         CK(cudaMemset(h->d_maxact, 0, sizeof(int)));
         RC(set_blocks(h));
+        if (h->mlp) {
+            CK(dalloc(&h->d_mlp_theta, (size_t)MLP_PER_TYPE));
+            CK(dalloc(&h->d_mlp_adj, (size_t)R * MLP_NCOPY * MLP_NG * 4));
+            CK(dalloc(&h->d_mlp_scratch, mlp_scratch_doubles()));
+            CK(dalloc(&h->d_mlp_grad, (size_t)R * MLP_PER_TYPE));
+            CK(dalloc((char **)&h->d_mlp_tab, (size_t)MLP_NG * 4 * sizeof(double)));
+        }
         return REVSIM_OK;
     }();
     if (rc) {
@@ -748,8 +811,11 @@ void revsim_sw_destroy(revsim_sw_handle *h) {
 const char *revsim_sw_last_error(const revsim_sw_handle *h) { return h ? h->err.c_str() : "null handle"; }
 
 int32_t revsim_sw_set_params(revsim_sw_handle *h, const double *theta, int32_t n) {
-    if (!h || !theta || n != NP) return fail(h, REVSIM_ERR_BADARG, "theta must hold 7 values");
-    for (int i = 0; i < NP; i++)
+    if (!h || !theta) return REVSIM_ERR_BADARG;
+    if (n != h->Pt)
+        return fail(h, REVSIM_ERR_BADARG, h->mlp ? "theta must hold 7 + REVSIM_SW_MLP_NPARAMS values"
+                                                 : "theta must hold 7 values");
+    for (int i = 0; i < n; i++)
         if (!std::isfinite(theta[i])) return fail(h, REVSIM_ERR_BADARG, "non-finite parameter");
     if (!(theta[2] > 0) || !(theta[5] > 0)) return fail(h, REVSIM_ERR_BADARG, "a and sigma must be positive");
     CK(cudaSetDevice(h->dev));
@@ -766,6 +832,19 @@ int32_t revsim_sw_set_params(revsim_sw_handle *h, const double *theta, int32_t n
             std::memcpy(h->theta, old, sizeof(old));
             return fail(h, REVSIM_ERR_BADARG, "a sigma + skin must stay below half the box side");
         }
+    if (h->mlp) {
+        std::vector<double> tm(theta + NP, theta + n);
+        if (tm != h->theta_mlp) {
+            CK(cudaMemcpyAsync(h->d_mlp_theta, tm.data(), sizeof(double) * tm.size(), cudaMemcpyHostToDevice, h->st));
+            cudaError_t e = launch_mlp_table(h->prec, h->d_mlp_theta, MLP_RC, h->d_mlp_scratch, h->d_mlp_tab,
+                                             h->st, 1, MLP_W);
+            h->launches += 2;
+            if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+            if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP table: ") + cudaGetErrorString(e));
+            h->theta_mlp = tm;
+            h->fwd_valid = false;
+        }
+    }
     h->have_params = true;
     if (std::memcmp(old, h->theta, sizeof(old)) != 0) h->fwd_valid = false;
     return REVSIM_OK;
@@ -833,7 +912,7 @@ int32_t revsim_sw_force_vjp(revsim_sw_handle *h, const double *w, const double *
     if (acoef) CK(cudaMemcpyAsync(h->d_A, acoef, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
     else CK(cudaMemsetAsync(h->d_A, 0, sizeof(double) * n3, h->st));
     RC(with_lane_retry(h, [&]() -> int {
-        CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * NP, h->st));
+        RC(zero_part(h));
         RC(build_list(h));
         RC(terms(h, TM_REV, true, false, 1.0));
         SwGatherArgs g = gather_args(h, 1.0, 0.0);
@@ -841,11 +920,7 @@ int32_t revsim_sw_force_vjp(revsim_sw_handle *h, const double *w, const double *
     }));
     if (F) CK(cudaMemcpy(F, h->d_F, sizeof(double) * n3, cudaMemcpyDeviceToHost));
     if (dl_dfi) CK(cudaMemcpy(dl_dfi, h->d_G, sizeof(double) * n3, cudaMemcpyDeviceToHost));
-    if (dtheta && acoef) {
-        std::vector<double> out;
-        RC(reduce_part(h, out));
-        std::memcpy(dtheta, out.data(), sizeof(double) * out.size());
-    }
+    if (dtheta && acoef) RC(grads_out(h, 1.0, dtheta));
     return REVSIM_OK;
 }
 
@@ -869,7 +944,7 @@ int32_t revsim_sw_loss_grad(revsim_sw_handle *h, double *loss, double *dLdx, dou
     if (!h->have_loss) return fail(h, REVSIM_ERR_STATE, "loss not set");
     const size_t n3 = 3 * (size_t)h->N;
     RC(with_lane_retry(h, [&]() -> int {
-        CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->n_blk * NP, h->st));
+        RC(zero_part(h));
         RC(build_list(h));
         RC(stress(h, h->vel_term, false));
         return loss_grad_dev(h, 1.0, 0.0, false, h->d_dLdx, h->d_dLdv);
@@ -877,11 +952,7 @@ int32_t revsim_sw_loss_grad(revsim_sw_handle *h, double *loss, double *dLdx, dou
     if (loss) CK(cudaMemcpy(loss, h->d_loss, sizeof(double) * h->R, cudaMemcpyDeviceToHost));
     if (dLdx) CK(cudaMemcpy(dLdx, h->d_dLdx, sizeof(double) * n3, cudaMemcpyDeviceToHost));
     if (dLdv) CK(cudaMemcpy(dLdv, h->d_dLdv, sizeof(double) * n3, cudaMemcpyDeviceToHost));
-    if (dLdtheta) {
-        std::vector<double> out;
-        RC(reduce_part(h, out));
-        std::memcpy(dLdtheta, out.data(), sizeof(double) * out.size());
-    }
+    if (dLdtheta) RC(grads_out(h, 1.0, dLdtheta));
     return REVSIM_OK;
 }
 
@@ -981,11 +1052,7 @@ int32_t revsim_sw_reverse(revsim_sw_handle *h, const uint64_t *noise_seeds, doub
         CK(cudaMemcpy(loss, h->d_loss_acc, sizeof(double) * h->R, cudaMemcpyDeviceToHost));
         for (int r = 0; r < h->R; r++) loss[r] /= nb;
     }
-    if (dl_dtheta) {
-        std::vector<double> out;
-        RC(reduce_part(h, out));
-        for (size_t i = 0; i < out.size(); i++) dl_dtheta[i] = out[i] / nb;
-    }
+    if (dl_dtheta) RC(grads_out(h, 1.0 / nb, dl_dtheta));
     h->fwd_valid = false;
     return REVSIM_OK;
 }

@@ -19,7 +19,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "rs_device.cuh"
+#include "rs_internal.h"   // rs_device.cuh, the MLP table and backprop launchers
 
 namespace rs {
 namespace sw {
@@ -28,6 +28,9 @@ constexpr int CAND = 64;        // candidate-row capacity (r < a sigma + skin)
 constexpr int ST_SKIN = 16;     // an atom moved more than skin/2 since the list build
 constexpr int TERM_THREADS = 128;
 constexpr int NP = 7;           // theta = [A, B, a, lambda, gamma, sigma, eps]
+// The learned radial term: one MLP type (rs_mlp.cu) tabulated on [0, MLP_RC] with RBF width
+// MLP_W, added to the 2-body term of every active pair with r < MLP_RC.
+constexpr double MLP_RC = 0.25, MLP_W = 0.0125;
 
 // Parameters in term precision R, plus the FP64 values that decide activity.
 template <typename R>
@@ -39,6 +42,9 @@ struct SwConsts {
     R asig;      // a sigma
     double a64, sig64, lim2;   // lim2 = (a sigma)^2
     double lo2, hi2;   // (a sigma)^2 (1 -+ 1e-9)^2: r^2 below lo2 is active, above hi2 not
+    R mlp_hinv;        // learned term: NG / MLP_RC, NG / (2 MLP_RC), (NG / MLP_RC)^2
+    R mlp_hhalf, mlp_hinv2;
+    double mlp_rc2;    // MLP_RC^2 (the term is on for r^2 < mlp_rc2, decided in FP64)
 };
 
 struct SwNlArgs {
@@ -73,6 +79,8 @@ struct SwTermArgs {
     void *Tv, *Tt;         // [N * G] 4-vectors in R (x, y, z, unused)
     double *part;          // [n_blk * NP] dtheta partials, accumulated (may be null)
     double *wpart;         // [n_blk * 9] virial partials, written (may be null)
+    const void *mlp_tab;   // learned term: [MLP_NG] cubic coefficients in R (null: off)
+    double *mlp_adj;       // [R][MLP_NCOPY][MLP_NG][4] coefficient adjoints (with part)
     double half_skin2;
     int *status, *max_act;
 };

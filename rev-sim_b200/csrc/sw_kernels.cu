@@ -360,6 +360,9 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
     D u[3], alpha = sdc<R, K>(R(0)), beta = sdc<R, K>(R(0)), sD = sdc<R, K>(R(1)),
             itD = sdc<R, K>(R(0)), it2 = sdc<R, K>(R(0)), g2 = sdc<R, K>(R(0));
     R gB = R(0);
+    D gm = sdc<R, K>(R(0));   // learned term: u'(r) / 2, the slot's half of the pair
+    int mg = -1;              // its interval (-1: off) and position in it
+    R msv = R(0);
 #pragma unroll
     for (int k = 0; k < 3; k++) u[k] = sdc<R, K>(R(0));
     D gam = sdc<R, K>(p.gam), isig = sdc<R, K>(p.isig);
@@ -410,6 +413,17 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
         const D is2 = is * is, is4 = is2 * is2, is5 = is4 * is;
         g2 = (e1 * sd_neg((R(4) * p.B) * is5 + ((p.B * is4) - sdc<R, K>(R(1))) * it2)) * isig;
         gB = xmul(xmul(e1.v, -xadd(xmul(R(4), is5.v), xmul(is4.v, it2.v))), p.isig);
+        if (t.mlp_tab && r2 < p.mlp_rc2) {
+            // u'/2 = (c1 + s (2 c2 + 3 s c3)) NG / (2 rc) on the cubic segment of interval
+            // g, s = r NG / rc - g; its position tangent u''/2 r' = (c2 + 3 s c3) (NG/rc)^2 r'
+            const R q = xmul(r, p.mlp_hinv);
+            mg = min((int)q, MLP_NG - 1);
+            msv = xsub(q, (R)mg);
+            const V4 cc = reinterpret_cast<const V4 *>(t.mlp_tab)[mg];
+            const R s3 = xmul(R(3), msv);
+            gm.v = xmul(xfma(msv, xfma(s3, cc.w, xmul(R(2), cc.z)), cc.y), p.mlp_hhalf);
+            if constexpr (K > 0) gm.d[0] = xmul(xmul(xfma(s3, cc.w, cc.z), p.mlp_hinv2), rdot);
+        }
         V4 uh;
         uh.x = u[0].v;
         uh.y = u[1].v;
@@ -490,7 +504,7 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
         for (int k = 0; k < 3; k++) d64[k] = s_d[grp][lane][k];
     }
     D T[3];
-    const D coef = p.half_eA * g2 + p.el * S1;
+    const D coef = (p.half_eA * g2 + p.el * S1) + gm;
     const D elb = p.el * beta;
 #pragma unroll
     for (int k = 0; k < 3; k++) T[k] = u[k] * coef + elb * V[k];
@@ -549,6 +563,14 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
             con[4] = sgn * (double)zd[1];
             con[5] = sgn * (double)zd[2];
             con[6] = sgn * ((double)p.A * half_g2zu + (double)p.lam * (double)zT3);
+            if (t.mlp_adj && mg >= 0) {
+                // z . dT/dc_k = zu k s^(k-1) NG / (2 rc), k = 1..3, into the replica's copy
+                const double w = sgn * (double)zu * (double)p.mlp_hhalf, sv = (double)msv;
+                double *ad = t.mlp_adj + (((size_t)rep * MLP_NCOPY + (size_t)(c % MLP_NCOPY)) * MLP_NG + mg) * 4;
+                atomicAdd(ad + 1, w);
+                atomicAdd(ad + 2, 2.0 * w * sv);
+                atomicAdd(ad + 3, 3.0 * w * sv * sv);
+            }
         }
         cta_sum<NP>(s_red, con, t.part + (size_t)b * NP, true);
       }

@@ -89,6 +89,7 @@ class SwDesc(ctypes.Structure):
         ("skin", ctypes.c_double),
         ("n_steps_nf", ctypes.c_int32),
         ("device", ctypes.c_int32),
+        ("mlp", ctypes.c_int32),
     ]
 
 

@@ -22,6 +22,17 @@ LATTICE_A = 0.3567
 STRESS_WEIGHT = 5e-8
 PARAM_NAMES = ("A", "B", "a", "lambda", "gamma", "sigma", "eps")
 N_PARAMS = 7
+# The learned radial term (one MLP type of revsim.mlp on [0, 0.25 nm], RBF width 0.0125 nm):
+# its parameters follow the SW ones when the engine has it.
+MLP_CUTOFF, MLP_WIDTH = 0.25, 0.0125
+MLP_NPARAMS = 5313
+
+
+def init_mlp_params(seed=3):
+    """Seeded initialisation of the learned radial term (the first type of
+    revsim.mlp.init_params)."""
+    from . import mlp
+    return mlp.init_params(seed)[:MLP_NPARAMS]
 
 
 def default_params():

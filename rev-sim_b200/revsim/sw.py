@@ -23,7 +23,7 @@ class SwEngine:
     """Device state for R diamond replicas (n_atoms, box, temp: scalars or per replica)."""
 
     def __init__(self, n_atoms, box, temp=D.TEMP, precision="mixed", device=0, skin=0.05,
-                 n_steps_nf=10, mass=D.C_MASS):
+                 n_steps_nf=10, mass=D.C_MASS, mlp=False):
         self._L = _lib.load()
         n_atoms = np.atleast_1d(np.asarray(n_atoms, dtype=np.int32))
         R = len(n_atoms)
@@ -33,9 +33,12 @@ class SwEngine:
         self.R, self.N = R, int(n_atoms.sum())
         self.precision = precision
         self.mass = mass
+        self.mlp = bool(mlp)
+        # the 7 SW parameters, then the learned radial term's (one MLP type)
+        self.n_params = D.N_PARAMS + (D.MLP_NPARAMS if mlp else 0)
         desc = _lib.SwDesc(R, n_atoms.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                            f64p(self.box), f64p(self.temp), PRECISION[precision], mass, D.KB,
-                           skin, n_steps_nf, device)
+                           skin, n_steps_nf, device, 1 if mlp else 0)
         h = ctypes.c_void_p()
         rc = self._L.revsim_sw_create(ctypes.byref(desc), ctypes.byref(h))
         if rc != 0:
@@ -98,12 +101,12 @@ class SwEngine:
         return F
 
     def force_vjp(self, w, acoef=None):
-        """(F, dl_dfi = sum_a (w_a/m) dF_a/dx, dtheta[R, 7] = sum_a acoef_a dF_a/dtheta)."""
+        """(F, dl_dfi = sum_a (w_a/m) dF_a/dx, dtheta[R, n_params] = sum_a acoef_a dF_a/dtheta)."""
         w = self._vec(w)
         a = None if acoef is None else self._vec(acoef)
         F = np.zeros((self.N, 3))
         G = np.zeros((self.N, 3))
-        dth = np.zeros((self.R, D.N_PARAMS))
+        dth = np.zeros((self.R, self.n_params))
         self._ck(self._L.revsim_sw_force_vjp(self._h, f64p(w), f64p(a) if a is not None else None,
                                              f64p(F), f64p(G), f64p(dth)))
         return F, G, (dth if a is not None else None)
@@ -114,11 +117,11 @@ class SwEngine:
         return s.reshape(self.R, 3, 3)
 
     def loss_grad(self):
-        """(loss[R], dL/dx [N, 3], dL/dv [N, 3], dL/dtheta [R, 7]) at the current state."""
+        """(loss[R], dL/dx [N, 3], dL/dv [N, 3], dL/dtheta [R, n_params]) at the current state."""
         loss = np.zeros(self.R)
         gx = np.zeros((self.N, 3))
         gv = np.zeros((self.N, 3))
-        gp = np.zeros((self.R, D.N_PARAMS))
+        gp = np.zeros((self.R, self.n_params))
         self._ck(self._L.revsim_sw_loss_grad(self._h, f64p(loss), f64p(gx), f64p(gv), f64p(gp)))
         return loss, gx, gv, gp
 
@@ -155,10 +158,10 @@ class SwEngine:
         return loss, nb.value
 
     def reverse(self, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt):
-        """Reverse pass from the forward end state; returns (loss[R], dL/dtheta [R, 7])."""
+        """Reverse pass from the forward end state; returns (loss[R], dL/dtheta [R, n_params])."""
         s = self._seeds(seeds, n_steps)
         loss = np.zeros(self.R)
-        g = np.zeros((self.R, D.N_PARAMS))
+        g = np.zeros((self.R, self.n_params))
         self._ck(self._L.revsim_sw_reverse(self._h, u64p(s), gamma, n_steps, n_steps_loss,
                                            n_steps_trunc, dt, f64p(loss), f64p(g)))
         return loss, g
@@ -196,11 +199,21 @@ class SwSystem:
     loggers: object = None
 
 
-def _engine_for(coords, box, precision, engine):
+def _engine_for(coords, box, precision, engine, mlp):
     if engine is not None:
         return engine
     n = len(np.asarray(coords).reshape(-1, 3))
-    return SwEngine(n, box, precision=precision)
+    return SwEngine(n, box, precision=precision, mlp=mlp)
+
+
+def _theta(eng, params_sw, params_gnn):
+    """The engine's parameter vector: the SW parameters, then -- with the learned term, which
+    stands in for the reference's GNN -- params_gnn."""
+    if eng.mlp:
+        if params_gnn is None:
+            raise ValueError("an engine with the learned term needs params_gnn (its MLP parameters)")
+        return np.concatenate([np.asarray(params_sw, dtype=np.float64), np.asarray(params_gnn, dtype=np.float64)])
+    return np.asarray(params_sw, dtype=np.float64)
 
 
 def forward_sim(coords_in, velocities_in, noise_seeds, gamma, n_steps, n_steps_loss,
@@ -209,14 +222,15 @@ def forward_sim(coords_in, velocities_in, noise_seeds, gamma, n_steps, n_steps_l
                 precision="mixed", engine=None, weight=D.STRESS_WEIGHT, target=None):
     """diamond.jl:1394-1538 for :sw / :stress.  Returns (sys, loss, loss_accum_blocks,
     loss_logs, grads_sw, grads_gnn); ``run_grads`` (the forward-mode AD check of the
-    reference) is not available and must be False; params_gnn is ignored (None)."""
+    reference) is not available and must be False; params_gnn holds the learned radial term's
+    MLP parameters (None: no learned term)."""
     if inter_type != "sw" or loss_type != "stress":
         raise ValueError("the engine implements inter_type :sw with loss_type :stress")
     if run_grads:
         raise ValueError("run_grads (forward-mode AD through the whole run) is not provided; "
                          "use reverse_sim")
-    eng = _engine_for(coords_in, box, precision, engine)
-    eng.set_params(params_sw)
+    eng = _engine_for(coords_in, box, precision, engine, params_gnn is not None)
+    eng.set_params(_theta(eng, params_sw, params_gnn))
     eng.set_state(coords_in, velocities_in)
     eng.set_loss(weight, target)
     loss, nb = eng.forward(noise_seeds, gamma, n_steps, n_steps_loss, dt, n_steps_buffer,
@@ -224,7 +238,8 @@ def forward_sim(coords_in, velocities_in, noise_seeds, gamma, n_steps, n_steps_l
     x, v = eng.get_state()
     sys = SwSystem(x, v, eng)
     l = float(loss.mean()) if calc_loss else 0.0
-    return sys, l, {"stress": l * nb, "n_blocks": nb}, {"stress": l}, np.zeros(D.N_PARAMS), None
+    return (sys, l, {"stress": l * nb, "n_blocks": nb}, {"stress": l}, np.zeros(D.N_PARAMS),
+            np.zeros(D.MLP_NPARAMS) if eng.mlp else None)
 
 
 def reverse_sim(coords, velocities, noise_seeds, gamma, n_steps, n_steps_loss, n_steps_trunc,
@@ -237,8 +252,11 @@ def reverse_sim(coords, velocities, noise_seeds, gamma, n_steps, n_steps_loss, n
     eng = fwd_loggers
     if not isinstance(eng, SwEngine):
         raise ValueError("fwd_loggers must be the engine returned by forward_sim")
-    eng.set_params(params_sw)   # the forward record stays valid for unchanged parameters
+    # the forward record stays valid for unchanged parameters
+    eng.set_params(_theta(eng, params_sw, params_gnn))
     eng.set_state(coords, velocities)
     loss, g = eng.reverse(noise_seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt)
     x, v = eng.get_state()
-    return SwSystem(x, v, eng), float(loss.mean()), g.mean(axis=0), None
+    g = g.mean(axis=0)
+    return (SwSystem(x, v, eng), float(loss.mean()), g[:D.N_PARAMS],
+            g[D.N_PARAMS:] if eng.mlp else None)
