@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--cells", type=int, default=10, help="diamond conventional cells per side")
     ap.add_argument("--sw-steps", type=int, default=2000)
     ap.add_argument("--sw-steps-loss", type=int, default=500)
+    ap.add_argument("--sw-plain", action="store_true",
+                    help="diamond without the learned radial term (SW alone)")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed gradient and exit (the command profiled under ncu)")
     return ap.parse_args()
@@ -406,8 +408,14 @@ def run_ours(a):
         gs = np.abs(g64[0] * p)
 
         def rel(gx, gref):
-            sc = np.abs(gref * p)
-            return float(np.max(np.abs((gx - gref) * p) / np.maximum(sc, 0.01 * sc.max())))
+            # SW parameters in units of dL/dlog(theta); the MLP's (when present) relative to
+            # the largest MLP entry
+            q = p[:7]
+            sc = np.abs(gref[:7] * q)
+            e = float(np.max(np.abs((gx[:7] - gref[:7]) * q) / np.maximum(sc, 0.01 * sc.max())))
+            if len(p) > 7:
+                e = max(e, float(np.abs(gx[7:] - gref[7:]).max() / np.abs(gref[7:]).max()))
+            return e
         extra = {"fp64_gpu": {"value": n_atoms * a.n_steps / (ms64 * 1e-3), "ms_per_step": ms64,
                               "speedup_mixed_over_fp64": (ms64 / ms_step)},
                  "grad_rel_err_vs_fp64": {
@@ -450,12 +458,22 @@ def run_ours(a):
 # parameter contraction).  Forward kernel (values only): 18 and 40.
 SW_FLOPS_REV_PAIR, SW_FLOPS_REV_SLOT = 97, 440
 SW_FLOPS_FWD_PAIR, SW_FLOPS_FWD_SLOT = 18, 40
+# The learned radial term per active slot within its 0.25 nm cutoff: reverse 25 flops
+# (interval, u'/2 and its tangent, the coefficient-adjoint weights), forward 10.
+SW_FLOPS_REV_MLP, SW_FLOPS_FWD_MLP = 25, 10
 SW_DT, SW_GAMMA, SW_NOISE = 0.0005, 4.0, 0.005
 
 
 def diamond_name(a):
-    return (f"diamond_sw_{a.replicas}x{8 * a.cells ** 3}atoms_{a.precision}_"
-            f"{a.sw_steps}fwd+{a.sw_steps}rev")
+    return (f"diamond_sw{'' if a.sw_plain else '+mlp'}_{a.replicas}x{8 * a.cells ** 3}atoms_"
+            f"{a.precision}_{a.sw_steps}fwd+{a.sw_steps}rev")
+
+
+def diamond_params(a):
+    """SW parameters of diamond.jl:53, then (with the learned term) its seeded MLP."""
+    from revsim import diamond as D
+    p = D.default_params()
+    return p if a.sw_plain else np.concatenate([p, D.init_mlp_params(3)])
 
 
 def diamond_config(a, extra=None):
@@ -467,6 +485,10 @@ def diamond_config(a, extra=None):
          "precision": a.precision,
          "loss": "stress tensor squared error (weight 5e-8) vs the mean stress of a run with "
                  "A x1.05, lambda x0.95",
+         "learned_term": None if a.sw_plain else (
+             "one MLP pair function on the SW 2-body term: 16 RBF (0-0.25 nm, width 0.0125 nm) "
+             "-> 64 -> 64 SiLU -> 1, cosine cutoff, 5,313 parameters, seeded Xavier init; "
+             "tabulated on 1,024 intervals, cubic Hermite per active pair within 0.25 nm"),
          "equilibration": "1 ps Langevin (gamma 4/ps) from the noisy lattice, untimed",
          "l2": "flushed (256 MiB write) between timed steps"}
     if extra:
@@ -484,8 +506,9 @@ def diamond_prepare(a, device):
         vs.append(D.mb_velocities(len(x), temp=300.0, seed=1000 + r))
         boxes.append(box)
     n = len(xs[0])
-    p = D.default_params()
-    eq = SwEngine([n] * a.replicas, boxes, temp=300.0, precision="mixed", device=device)
+    p = diamond_params(a)
+    eq = SwEngine([n] * a.replicas, boxes, temp=300.0, precision="mixed", device=device,
+                  mlp=not a.sw_plain)
     eq.set_params(p)
     eq.set_state(np.concatenate(xs), np.concatenate(vs))
     eq.set_loss()
@@ -508,7 +531,7 @@ def diamond_cpu_sample(a, x0, v0, box, p, target, n_s=2):
     from oracle import orc
     from revsim import systems
     n = len(x0)
-    s = orc.make_sw_system(n, box, 300.0)
+    s = orc.make_sw_system(n, box, 300.0, mlp=len(p) > 7)
     L = orc.make_sw_loss(5e-8, target)
     seeds = systems.noise_seeds(n_s, seed=98)
     t0 = time.perf_counter()
@@ -529,7 +552,7 @@ def run_reference_diamond(a):
     orc.build()
     x, box = D.diamond_coords(a.cells, noise=SW_NOISE, seed=4)
     v = D.mb_velocities(len(x), temp=300.0, seed=1000)
-    p = D.default_params()
+    p = diamond_params(a)
     vals = []
     for i in range(a.warmup + a.steps):
         val, cores, desc = diamond_cpu_sample(a, x, v, box, p, np.zeros(9))
@@ -570,7 +593,7 @@ def run_ours_diamond(a):
     K, NL = a.sw_steps, a.sw_steps_loss
 
     def make(prec):
-        e = SwEngine([n] * R, boxes, temp=300.0, precision=prec, device=local)
+        e = SwEngine([n] * R, boxes, temp=300.0, precision=prec, device=local, mlp=not a.sw_plain)
         e.set_params(p)
         e.set_loss(5e-8, target)
         e.set_state(x0, v0)
@@ -648,7 +671,7 @@ def run_ours_diamond(a):
         e2e_total = float(t.item())
     e2e_value = world * N * K / (e2e_total / a.steps * 1e-3)
     h2d = 2 * 3 * N * 8 + 2 * K * R * 8
-    d2h = 2 * R * 8 + R * 7 * 8 + 2 * 3 * N * 8
+    d2h = 2 * R * 8 + R * len(p) * 8 + 2 * 3 * N * 8
 
     # roofline of the dominant kernel (the reverse terms kernel), timed per launch
     eng.set_state(x0, v0)
@@ -663,6 +686,15 @@ def run_ours_diamond(a):
     pairs = eng.active_pairs()
     deg = np.bincount(pairs.ravel(), minlength=N).astype(np.int64)
     flops_launch = int(SW_FLOPS_REV_PAIR * (deg * (deg - 1)).sum() + SW_FLOPS_REV_SLOT * deg.sum())
+    n_mlp_slots = 0
+    if not a.sw_plain:
+        # both slots of every active pair within the learned term's 0.25 nm cutoff
+        xs_now = eng.get_state()[0]
+        L_pair = np.asarray(boxes)[pairs[:, 0] // n][:, None]
+        d = xs_now[pairs[:, 1]] - xs_now[pairs[:, 0]]
+        d -= L_pair * np.round(d / L_pair)
+        n_mlp_slots = 2 * int((np.linalg.norm(d, axis=1) < 0.25).sum())
+        flops_launch += SW_FLOPS_REV_MLP * n_mlp_slots
     achieved = flops_launch / (launch_ms * 1e-3) / 1e12
     peak = ctypes.c_double()
     _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
@@ -671,6 +703,7 @@ def run_ours_diamond(a):
                 "kernel": "k_terms<float, 16, TM_REV> (Stillinger-Weber reverse terms)",
                 "launch_ms": launch_ms, "launches_timed": rt_n, "flops_per_launch": flops_launch,
                 "mean_active_neighbours": float(deg.mean()),
+                "learned_term_slots_per_launch": n_mlp_slots,
                 "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)",
                 "kernel_ms_per_launch": {"rev_terms": launch_ms, "fwd_terms": ft_ms / max(ft_n, 1),
                                          "rev_gather": rg_ms / max(rg_n, 1),
@@ -699,15 +732,23 @@ def run_ours_diamond(a):
             short[key] = eng_.reverse(seeds[:100], SW_GAMMA, 100, 100, 100, SW_DT)[1].mean(axis=0)
 
         def rel(gx, gref):
-            sc = np.abs(gref * p)
-            return float(np.max(np.abs((gx - gref) * p) / np.maximum(sc, 0.01 * sc.max())))
+            # SW parameters in units of dL/dlog(theta); the MLP's (when present) relative to
+            # the largest MLP entry
+            q = p[:7]
+            sc = np.abs(gref[:7] * q)
+            e = float(np.max(np.abs((gx[:7] - gref[:7]) * q) / np.maximum(sc, 0.01 * sc.max())))
+            if len(p) > 7:
+                e = max(e, float(np.abs(gx[7:] - gref[7:]).max() / np.abs(gref[7:]).max()))
+            return e
         extra = {"fp64_gpu": {"value": N * K / (ms64 * 1e-3), "ms_per_step": ms64,
                               "speedup_mixed_over_fp64": ms64 / ms_step},
                  "grad_rel_err_vs_fp64": {
                      "full_workload": rel(gm.mean(axis=0), g64.mean(axis=0)),
                      "first_100_steps": rel(short["mixed"], short["fp64"]),
-                     "definition": "replica-mean gradient; max over parameters of |g - g_fp64| * "
-                                   "|theta| / max(|g_fp64 * theta|, 0.01 max_k |g_fp64,k * theta_k|)"}}
+                     "definition": "replica-mean gradient; max over the SW parameters of "
+                                   "|g - g_fp64| |theta| / max(|g_fp64 theta|, 0.01 max_k "
+                                   "|g_fp64,k theta_k|), and over the MLP parameters of "
+                                   "|g - g_fp64| / max |g_fp64,mlp|"}}
         e64.close()
 
     cpu = None
