@@ -41,6 +41,12 @@ class OrcLoss(ctypes.Structure):
                 ("u_gas", _D), ("rt", _D), ("target", _D)]
 
 
+class OrcBarostat(ctypes.Structure):
+    _fields_ = [("pressure", _D), ("n_steps", _I32), ("volume_scale", _D), ("scale_increment", _D),
+                ("max_volume_frac", _D), ("seed", ctypes.c_uint64), ("n_attempted", _I64),
+                ("n_accepted", _I64), ("n_draws", _I64), ("n_accepted_total", _I64)]
+
+
 class OrcSwSystem(ctypes.Structure):
     _fields_ = [("n_atoms", _I32), ("box", _D), ("mass", _D), ("kB", _D), ("temp", _D),
                 ("mlp", _I32)]
@@ -89,6 +95,13 @@ def lib():
         L.orc_loss_and_grads.restype = _D
         L.orc_loss_and_grads.argtypes = [ctypes.POINTER(OrcSystem), _PD, ctypes.POINTER(OrcLoss),
                                          _PD, _PD, _PD, _PD]
+        L.orc_barostat_uniform.restype = _D
+        L.orc_barostat_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.orc_barostat_attempt.restype = _I32
+        L.orc_barostat_attempt.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PI32, _I64,
+                                           ctypes.POINTER(OrcBarostat)]
+        L.orc_forward_sim_barostat.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PU64, _D,
+                                               _I32, _D, ctypes.POINTER(OrcBarostat)]
         L.orc_num_threads.restype = _I32
         L.orc_set_num_threads.argtypes = [_I32]
         L.orc_energy_grads.restype = _D
@@ -306,6 +319,31 @@ def reverse_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_tr
                                 _pd(sx), _pd(sv), clip, ctypes.byref(loss.c), _pd(g), _pd(lp))
     out = (x.reshape(-1, 3), v.reshape(-1, 3), val, g)
     return out + ((lp[0], lp[1]),) if parts else out
+
+
+def make_barostat(box, seed, pressure=1.0, n_steps=30, scale_factor=0.01, scale_increment=1.1,
+                  max_volume_frac=0.3):
+    """MonteCarloBarostatNoUnits(P, T, boundary) with the defaults of water.jl:802-806."""
+    return OrcBarostat(pressure, n_steps, box ** 3 * scale_factor, scale_increment, max_volume_frac,
+                       int(seed), 0, 0, 0, 0)
+
+
+def barostat_attempt(s, params, x, pairs, baro):
+    """One attempt; returns (accepted, x) with s.box and baro updated in place."""
+    x = _f64(x).copy()
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    acc = lib().orc_barostat_attempt(ctypes.byref(s), _pd(_f64(params)), _pd(x),
+                                     pairs.ctypes.data_as(_PI32), len(pairs), ctypes.byref(baro))
+    return bool(acc), x.reshape(-1, 3)
+
+
+def forward_sim_barostat(s, params, x, v, seeds, gamma, n_steps, dt, baro):
+    """Equilibration run with the barostat; returns (x, v); s.box and baro are updated."""
+    x, v = _f64(x).copy(), _f64(v).copy()
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    lib().orc_forward_sim_barostat(ctypes.byref(s), _pd(_f64(params)), _pd(x), _pd(v),
+                                   seeds.ctypes.data_as(_PU64), gamma, n_steps, dt, ctypes.byref(baro))
+    return x.reshape(-1, 3), v.reshape(-1, 3)
 
 
 def set_threads(n):

@@ -1253,3 +1253,104 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
     free(pairs);
     return loss_accum / n_blocks;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Monte-Carlo barostat, water.jl:789-865 (see revsim_oracle.h). */
+static const double kBarNa = 0.0602214076;   /* 1 bar nm^3 x N_A in kJ/mol */
+
+double orc_barostat_uniform(uint64_t seed, uint64_t k) {
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (k + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* Molecule centres scaled by l about the origin, atoms moved with their molecule and
+ * wrapped into the scaled box (scale_coords!). */
+static void scale_molecules(const orc_system *s, const double *x, double l, double *xt) {
+    const double L = s->box, Ln = L * l;
+    for (int64_t m = 0; m < s->n_mol; m++) {
+        const double *xo = x + 9 * m;
+        double d1[3], d2[3], sh[3];
+        vec3(xo, xo + 3, L, d1);
+        vec3(xo, xo + 6, L, d2);
+        for (int u = 0; u < 3; u++) {
+            const double c = xo[u] + (d1[u] + d2[u]) / 3.0;
+            sh[u] = c * l - c;
+        }
+        for (int k = 0; k < 3; k++)
+            for (int u = 0; u < 3; u++) xt[9 * m + 3 * k + u] = orc_wrap1d(xo[3 * k + u] + sh[u], Ln);
+    }
+}
+
+int32_t orc_barostat_attempt(orc_system *s, const double *params, double *x, const int32_t *pairs,
+                             int64_t n_pairs, orc_barostat *b) {
+    const int64_t n3 = 9 * (int64_t)s->n_mol;
+    const double kT = s->kB * s->temp;
+    const double E = orc_energy(s, params, x, pairs, n_pairs);
+    const double L = s->box, V = L * L * L;
+    const double u1 = orc_barostat_uniform(b->seed, 2 * (uint64_t)b->n_draws);
+    const double u2 = orc_barostat_uniform(b->seed, 2 * (uint64_t)b->n_draws + 1);
+    b->n_draws++;
+    const double dV = b->volume_scale * (2 * u1 - 1);
+    const double v_scale = (V + dV) / V, l = cbrt(v_scale);
+    double *xt = (double *)malloc(sizeof(double) * (size_t)n3);
+    scale_molecules(s, x, l, xt);
+    s->box = L * l;
+    const double Et = orc_energy(s, params, xt, pairs, n_pairs);
+    const double dW = (Et - E) + b->pressure * kBarNa * dV - s->n_mol * kT * log(v_scale);
+    int32_t acc = 0;
+    if (dW <= 0.0 || u2 < exp(-dW / kT)) {
+        memcpy(x, xt, sizeof(double) * (size_t)n3);
+        b->n_accepted++;
+        b->n_accepted_total++;
+        acc = 1;
+    } else {
+        s->box = L;
+    }
+    b->n_attempted++;
+    if (b->n_attempted >= 10) {
+        if (b->n_accepted < 0.25 * b->n_attempted) {
+            b->volume_scale /= b->scale_increment;
+            b->n_attempted = b->n_accepted = 0;
+        } else if (b->n_accepted > 0.75 * b->n_attempted) {
+            const double cap = V * b->max_volume_frac, vs = b->volume_scale * b->scale_increment;
+            b->volume_scale = vs < cap ? vs : cap;
+            b->n_attempted = b->n_accepted = 0;
+        }
+    }
+    free(xt);
+    return acc;
+}
+
+void orc_forward_sim_barostat(orc_system *s, const double *params, double *x, double *v,
+                              const uint64_t *noise_seeds, double gamma, int32_t n_steps, double dt,
+                              orc_barostat *b) {
+    const int64_t n = 3 * (int64_t)s->n_mol, n3 = 3 * n;
+    const double c = exp(-gamma * dt), sn = sqrt(1 - c * c);
+    double *F = (double *)malloc(sizeof(double) * (size_t)n3);
+    double *xi = (double *)malloc(sizeof(double) * (size_t)n3);
+    int64_t cap = 16 * n + 1024;
+    int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * (size_t)cap);
+    int64_t np = rebuild_pairs(s, x, &pairs, &cap);
+    double *coef = mlp_table(s, params);
+    for (int32_t step = 1; step <= n_steps; step++) {   /* water.jl:1029-1045 */
+        forces_core(s, params, x, pairs, np, NULL, 0, F, NULL, NULL, NULL, NULL, coef, NULL);
+        for (int64_t a = 0; a < n; a++) {
+            const double m = mass(s, a);
+            for (int u = 0; u < 3; u++) v[3 * a + u] = v[3 * a + u] + F[3 * a + u] * dt / m;
+        }
+        for (int64_t e = 0; e < n3; e++) x[e] = x[e] + v[e] * dt / 2;
+        orc_noise(s, noise_seeds[step - 1], s->temp, xi);
+        for (int64_t e = 0; e < n3; e++) v[e] = v[e] * c + xi[e] * sn;
+        for (int64_t e = 0; e < n3; e++) x[e] = x[e] + v[e] * dt / 2;
+        for (int64_t e = 0; e < n3; e++) x[e] = orc_wrap1d(x[e], s->box);
+        if (step % s->n_steps_nf == 0) np = rebuild_pairs(s, x, &pairs, &cap);
+        if (b && step % b->n_steps == 0) orc_barostat_attempt(s, params, x, pairs, np, b);
+    }
+    free(coef);
+    free(F);
+    free(xi);
+    free(pairs);
+}

@@ -164,6 +164,46 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
                        double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
                        double *l_parts);
 
+/* Monte-Carlo barostat: MonteCarloBarostatNoUnits and its apply_coupling!
+ * (water.jl:789-865) as forward_sim runs it with use_barostat (water.jl:1009-1014,
+ * 1043-1044): every n_steps steps, after the step's neighbour refresh, one volume move
+ * dV = volume_scale (2 u1 - 1), molecule centres scaled by l = cbrt((V + dV) / V) with the
+ * box, the energy of the trial state over the same pair list, and acceptance if
+ * dW = dU + P dV N_A - n_mol kB T ln(v_scale) <= 0 or u2 < exp(-dW / (kB T)) (kJ/mol);
+ * after every 10 attempts volume_scale shrinks by scale_increment below 25 % acceptance
+ * and grows (up to max_volume_frac V) above 75 %.
+ * Differences, each deliberate: the two uniforms of attempt k are
+ * orc_barostat_uniform(seed, 2k) and (seed, 2k + 1), a counter-based stream, where the
+ * reference draws Julia's global rand(); the molecule centre is the mean of the O atom and
+ * the minimum-image positions of its H atoms (Molly's scale_coords! averages the stored,
+ * wrapped positions, which differs only for a molecule split across the box face). */
+typedef struct {
+    double pressure;          /* bar (1.0 in water.jl:1011) */
+    int32_t n_steps;          /* attempt period in steps (30) */
+    double volume_scale;      /* nm^3 (box volume x 0.01 at construction) */
+    double scale_increment;   /* 1.1 */
+    double max_volume_frac;   /* 0.3 */
+    uint64_t seed;
+    int64_t n_attempted, n_accepted;   /* the adaptation window */
+    int64_t n_draws;                   /* attempts so far (the draw counter) */
+    int64_t n_accepted_total;
+} orc_barostat;
+
+/* Uniform in [0, 1) from draw k of the stream `seed` (splitmix64 of seed + k). */
+double orc_barostat_uniform(uint64_t seed, uint64_t k);
+
+/* One attempt on (x, s->box) with the given pair list; updates x, s->box and b; returns 1
+ * when the move was accepted. */
+int32_t orc_barostat_attempt(orc_system *s, const double *params, double *x, const int32_t *pairs,
+                             int64_t n_pairs, orc_barostat *b);
+
+/* forward_sim with use_barostat and calc_loss = false (the equilibration runs of train(),
+ * water.jl:1642-1645): n_steps B-A-O-A steps, neighbour rebuild every n_steps_nf steps, a
+ * barostat attempt every b->n_steps steps.  Updates x, v, s->box and b. */
+void orc_forward_sim_barostat(orc_system *s, const double *params, double *x, double *v,
+                              const uint64_t *noise_seeds, double gamma, int32_t n_steps, double dt,
+                              orc_barostat *b);
+
 /* Number of OpenMP threads used by the force loops (1 when built without OpenMP). */
 int32_t orc_num_threads(void);
 void orc_set_num_threads(int32_t n);
