@@ -162,6 +162,41 @@ int32_t revsim_loss_grad(revsim_handle *h, double *loss, double *dLdx);
  * reference, whose loss_type argument selects the same terms. */
 int32_t revsim_set_enth_vap(revsim_handle *h, int32_t enable, double u_gas, double rt, double target);
 
+/* Monte-Carlo barostat of forward_sim's use_barostat (MonteCarloBarostatNoUnits and its
+ * apply_coupling!, water.jl:789-865, set up at water.jl:1009-1014): every n_steps forward
+ * steps (counted over the revsim_forward calls since it was switched on, so a run split into
+ * blocks keeps the reference's schedule), after the step's neighbour refresh, each replica
+ * tries one volume move:
+ * dV = volume_scale (2 u1 - 1), molecule centres (O plus the mean of the minimum-image O->H
+ * vectors) scaled with the box by cbrt((V + dV) / V), the energy of the trial state over the
+ * current neighbour rows, acceptance if dW = dU + P dV N_A - n_mol kB T ln((V + dV) / V) <= 0
+ * or u2 < exp(-dW / (kB T)); after every 10 attempts volume_scale is divided by
+ * scale_increment below 25 % acceptance and multiplied (up to max_volume_frac V) above 75 %.
+ * u1, u2 of replica r's attempt k are draws 2k and 2k+1 of the stream seed + r (splitmix64;
+ * the reference draws Julia's global rand()).  A forward pass with the barostat on is an
+ * equilibration run: revsim_reverse refuses its record. */
+typedef struct {
+    double pressure;          /* bar (1.0 in water.jl:1011) */
+    int32_t n_steps;          /* attempt period, steps (30) */
+    double scale_factor;      /* initial volume_scale / box volume (0.01) */
+    double scale_increment;   /* 1.1 */
+    double max_volume_frac;   /* 0.3 */
+    uint64_t seed;
+} revsim_barostat_desc;
+
+/* Switch the barostat on (desc) or off (NULL); switching it on resets volume_scale to
+ * scale_factor x the current box volume and the attempt counters. */
+int32_t revsim_set_barostat(revsim_handle *h, const revsim_barostat_desc *desc);
+
+/* Per replica: box side (nm), volume_scale (nm^3), attempts and accepted moves so far (any
+ * output may be NULL). */
+int32_t revsim_barostat_state(revsim_handle *h, double *box, double *volume_scale,
+                              int64_t *n_attempts, int64_t *n_accepted);
+
+/* The boundary argument of forward_sim / reverse_sim (water.jl:977, 1435, 1001): new cubic box
+ * sides [n_replicas], nm (each above 2 x nl_cutoff).  Invalidates the forward record. */
+int32_t revsim_set_box(revsim_handle *h, const double *box);
+
 /* The RDF and enthalpy parts [n_replicas] of the loss the last revsim_forward or
  * revsim_reverse returned (loss_accum_rdf and loss_accum_ev over n_blocks, water.jl:1548-1551);
  * zeros after a forward pass without loss.  Either output may be NULL. */

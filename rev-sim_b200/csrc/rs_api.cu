@@ -123,6 +123,17 @@ struct revsim_handle {
     int *d_cnt_ev = nullptr;
     int ev_cap = 0;
     int last_blocks = 1;   // loss points of the last forward / reverse (0: no loss computed)
+    // Monte-Carlo barostat (forward passes only): per replica volume_scale, the adaptation
+    // window, the draw counter and the accepted total; saved positions and the trial
+    // scale / acceptance per replica on the device
+    bool baro_on = false, fwd_baro = false;
+    revsim_barostat_desc baro{};
+    std::vector<double> baro_vs;
+    std::vector<long long> baro_att, baro_acc, baro_draws, baro_acc_tot;
+    long long baro_step = 0;   // forward steps since the barostat was switched on
+    double *d_bx = nullptr, *d_lsc = nullptr;
+    int *d_bacc = nullptr;
+    int cell_cap = 0;   // allocated cells (the cell grid follows the boxes)
     // instrumentation
     long long launches = 0;
     bool ktime = false;
@@ -614,6 +625,132 @@ int check_ready(revsim_handle *h) {
     return REVSIM_OK;
 }
 
+// Cell grid of every replica from its current box (cells of side >= half the candidate
+// distance, at most 64 per side), the one-image rule and the FP32 row band; the cell arrays
+// grow when a box does.
+int set_cells(revsim_handle *h) {
+    const double rcand = h->rc_nl + 2 * kRext;
+    std::vector<int> nc(h->R), coff(h->R);
+    int ncell = 0;
+    double lmax = 0;
+    h->shift_ok = true;
+    for (int r = 0; r < h->R; r++) {
+        nc[r] = std::min(64, std::max(1, (int)std::floor(h->box[r] / (rcand / 2))));
+        coff[r] = ncell;
+        ncell += nc[r] * nc[r] * nc[r];
+        lmax = std::max(lmax, h->box[r]);
+        if (!(h->box[r] > 2 * (h->rc + 2 * kRext) + 0.02)) h->shift_ok = false;
+    }
+    h->band = (float)(2e-5 * std::max(1.0, lmax / 4.0));
+    if (nc == h->nc) return REVSIM_OK;
+    if (ncell > h->cell_cap) {
+        int **arrs[] = {&h->d_cell_cnt, &h->d_cell_start, &h->d_cell_fill, &h->d_cell_rep};
+        for (int **a : arrs) {
+            dfree(*a);
+            *a = nullptr;
+        }
+        h->cell_cap = 0;
+        for (int **a : arrs) CK(dalloc(a, ncell));
+        h->cell_cap = ncell;
+    }
+    std::vector<int> cell_rep(ncell);
+    for (int r = 0; r < h->R; r++)
+        for (int c = 0; c < nc[r] * nc[r] * nc[r]; c++) cell_rep[coff[r] + c] = r;
+    CK(cudaMemcpyAsync(h->d_rep_nc, nc.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_rep_cell_off, coff.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_cell_rep, cell_rep.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->nc = nc;
+    h->cell_off = coff;
+    h->n_cells = ncell;
+    return REVSIM_OK;
+}
+
+// Potential energy per replica (FP64 kernel over the given rows, summed in molecule order).
+int replica_energies(revsim_handle *h, const uint32_t *nbr, const int *cnt, std::vector<double> &E) {
+    if (!h->d_epart) CK(dalloc(&h->d_epart, (size_t)h->M * (h->P + 1)));
+    EnergyArgs a = energy_args(h, nbr, cnt);
+    a.grads = 0;
+    CK(launch_energy_grads(h->mlp ? (int)F_LJ_MLP : h->form, h->prec, a, h->st));
+    h->launches++;
+    std::vector<double> part((size_t)h->M * (h->P + 1));
+    CK(cudaMemcpyAsync(part.data(), h->d_epart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    E.assign(h->R, 0.0);
+    for (int r = 0; r < h->R; r++)
+        for (int I = h->mol0[r]; I < h->mol0[r] + h->nmol[r]; I++) E[r] += part[(size_t)I * (h->P + 1)];
+    return REVSIM_OK;
+}
+
+uint64_t splitmix_draw(uint64_t seed, uint64_t k) {
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (k + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double uniform01(uint64_t seed, uint64_t k) { return (double)(splitmix_draw(seed, k) >> 11) * (1.0 / 9007199254740992.0); }
+
+// One volume move per replica (apply_coupling!, water.jl:820-862) on the current state with
+// the current rows; on any acceptance the gather buffer `buf` is repacked and the cell grid
+// follows the new boxes.
+int baro_attempt(revsim_handle *h, const uint32_t *nbr, const int *cnt, int buf) {
+    const int R = h->R;
+    const double kBarNa = 0.0602214076;   // 1 bar nm^3 x N_A, kJ/mol
+    std::vector<double> E, Et, lsc(R), old(h->box);
+    int rc = replica_energies(h, nbr, cnt, E);
+    if (rc) return rc;
+    std::vector<double> dV(R), u2(R);
+    for (int r = 0; r < R; r++) {
+        const uint64_t sr = h->baro.seed + (uint64_t)r, k = (uint64_t)h->baro_draws[r]++;
+        const double u1 = uniform01(sr, 2 * k);
+        u2[r] = uniform01(sr, 2 * k + 1);
+        const double V = old[r] * old[r] * old[r];
+        dV[r] = h->baro_vs[r] * (2 * u1 - 1);
+        lsc[r] = std::cbrt((V + dV[r]) / V);
+    }
+    const size_t n3 = 3 * (size_t)h->N;
+    CK(cudaMemcpyAsync(h->d_bx, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_lsc, lsc.data(), sizeof(double) * R, cudaMemcpyHostToDevice, h->st));
+    CK(launch_baro_scale(h->M, h->d_mol_rep, h->d_rep_box, h->d_lsc, h->d_x, h->st));
+    h->launches++;
+    std::vector<double> trial(R);
+    for (int r = 0; r < R; r++) trial[r] = old[r] * lsc[r];
+    CK(cudaMemcpyAsync(h->d_rep_box, trial.data(), sizeof(double) * R, cudaMemcpyHostToDevice, h->st));
+    if ((rc = replica_energies(h, nbr, cnt, Et))) return rc;
+    std::vector<int> acc(R);
+    bool any = false;
+    for (int r = 0; r < R; r++) {
+        const double kT = h->kB * h->temp[r], V = old[r] * old[r] * old[r];
+        const double dW = (Et[r] - E[r]) + h->baro.pressure * kBarNa * dV[r] -
+                          h->nmol[r] * kT * std::log((V + dV[r]) / V);
+        acc[r] = (dW <= 0.0 || u2[r] < std::exp(-dW / kT)) ? 1 : 0;
+        any = any || acc[r];
+        h->box[r] = acc[r] ? trial[r] : old[r];
+        if (acc[r]) {
+            h->baro_acc[r]++;
+            h->baro_acc_tot[r]++;
+        }
+        if (++h->baro_att[r] >= 10) {
+            if (h->baro_acc[r] < 0.25 * h->baro_att[r]) {
+                h->baro_vs[r] /= h->baro.scale_increment;
+                h->baro_att[r] = h->baro_acc[r] = 0;
+            } else if (h->baro_acc[r] > 0.75 * h->baro_att[r]) {
+                h->baro_vs[r] = std::min(h->baro_vs[r] * h->baro.scale_increment, V * h->baro.max_volume_frac);
+                h->baro_att[r] = h->baro_acc[r] = 0;
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(h->d_bacc, acc.data(), sizeof(int) * R, cudaMemcpyHostToDevice, h->st));
+    CK(launch_baro_restore(h->M, h->d_mol_rep, h->d_bacc, h->d_bx, h->d_x, h->st));
+    CK(cudaMemcpyAsync(h->d_rep_box, h->box.data(), sizeof(double) * R, cudaMemcpyHostToDevice, h->st));
+    h->launches++;
+    if (any) {
+        if ((rc = set_cells(h))) return rc;
+        if ((rc = pack(h, buf, false))) return rc;
+    }
+    return REVSIM_OK;
+}
+
 int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, double dt, int calc_loss) {
     const double c = std::exp(-gamma * dt), s = std::sqrt(1 - c * c);
     const size_t n3 = 3 * (size_t)h->N;
@@ -660,6 +797,9 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
         }
         if (calc_loss && has_loss(h) && step % n_steps_loss == 0)
             if ((rc = loss_dev(h, false, h->d_loss_acc, h->d_ev_acc))) return rc;
+        // apply_coupling! (water.jl:1043-1044) after the step's loggers and loss
+        if (h->baro_on && ++h->baro_step % h->baro.n_steps == 0)
+            if ((rc = baro_attempt(h, nbr, ncnt, cur))) return rc;
     }
     return REVSIM_OK;
 }
@@ -834,7 +974,7 @@ void free_all(revsim_handle *h) {
                     h->d_scale, h->d_status, h->d_maxcnt, h->d_count, h->d_snap_x, h->d_snap_v,
                     h->d_ckpt, h->d_seeds, h->d_loss, h->d_loss_acc, h->d_dLdx,
                     h->d_cell_rep, h->d_nbr_store, h->d_cnt_store, h->d_ev_acc, h->d_ev_k,
-                    h->d_ev_grad, h->d_nbr_ev, h->d_cnt_ev};
+                    h->d_ev_grad, h->d_nbr_ev, h->d_cnt_ev, h->d_bx, h->d_lsc, h->d_bacc};
     for (void *p : ptrs) dfree(p);
     for (Term &T : h->terms) {
         dfree(T.d_target);
@@ -937,6 +1077,7 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
     h->nc = rep_nc;
     h->cell_off = rep_coff;
     h->n_cells = ncell;
+    h->cell_cap = ncell;
     std::vector<int> cell_rep(ncell);
     double lmax = 0;
     for (int r = 0; r < h->R; r++) {
@@ -1275,6 +1416,65 @@ int32_t revsim_loss_grad(revsim_handle *h, double *loss, double *dLdx) {
     return REVSIM_OK;
 }
 
+int32_t revsim_set_barostat(revsim_handle *h, const revsim_barostat_desc *d) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (!d) {
+        h->baro_on = false;
+        return REVSIM_OK;
+    }
+    if (!(d->pressure >= 0) || d->n_steps < 1 || !(d->scale_factor > 0) || !(d->scale_increment > 1) ||
+        !(d->max_volume_frac > 0))
+        return fail(h, REVSIM_ERR_BADARG, "bad barostat description");
+    CK(cudaSetDevice(h->dev));
+    if (!h->d_bx) {
+        CK(dalloc(&h->d_bx, 3 * (size_t)h->N));
+        CK(dalloc(&h->d_lsc, (size_t)h->R));
+        CK(dalloc(&h->d_bacc, (size_t)h->R));
+    }
+    h->baro = *d;
+    h->baro_vs.resize(h->R);
+    for (int r = 0; r < h->R; r++) h->baro_vs[r] = h->box[r] * h->box[r] * h->box[r] * d->scale_factor;
+    h->baro_att.assign(h->R, 0);
+    h->baro_acc.assign(h->R, 0);
+    h->baro_draws.assign(h->R, 0);
+    h->baro_acc_tot.assign(h->R, 0);
+    h->baro_step = 0;
+    h->baro_on = true;
+    return REVSIM_OK;
+}
+
+int32_t revsim_barostat_state(revsim_handle *h, double *box, double *volume_scale, int64_t *n_attempts,
+                              int64_t *n_accepted) {
+    if (!h) return REVSIM_ERR_BADARG;
+    for (int r = 0; r < h->R; r++) {
+        const bool on = !h->baro_vs.empty();
+        if (box) box[r] = h->box[r];
+        if (volume_scale) volume_scale[r] = on ? h->baro_vs[r] : 0.0;
+        if (n_attempts) n_attempts[r] = on ? h->baro_draws[r] : 0;
+        if (n_accepted) n_accepted[r] = on ? h->baro_acc_tot[r] : 0;
+    }
+    return REVSIM_OK;
+}
+
+int32_t revsim_set_box(revsim_handle *h, const double *box) {
+    if (!h || !box) return REVSIM_ERR_BADARG;
+    for (int r = 0; r < h->R; r++)
+        if (!(box[r] > 2 * h->rc_nl) || !std::isfinite(box[r]))
+            return fail(h, REVSIM_ERR_BADARG, "box side must exceed twice the neighbour cutoff");
+    CK(cudaSetDevice(h->dev));
+    const std::vector<double> old = h->box;
+    h->box.assign(box, box + h->R);
+    int rc = set_cells(h);
+    if (rc) {
+        h->box = old;
+        return rc;
+    }
+    CK(cudaMemcpyAsync(h->d_rep_box, h->box.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->fwd_valid = false;
+    return REVSIM_OK;
+}
+
 int32_t revsim_set_enth_vap(revsim_handle *h, int32_t enable, double u_gas, double rt, double target) {
     if (!h) return REVSIM_ERR_BADARG;
     if (enable && !(std::isfinite(u_gas) && std::isfinite(rt) && std::isfinite(target)))
@@ -1384,6 +1584,11 @@ int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gam
     CK(cudaMemcpyAsync(h->d_x0, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemcpyAsync(h->d_v0, h->d_v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemsetAsync(h->d_maxcnt, 0, sizeof(int), h->st));
+    // the barostat changes the boxes: a retry starts from the boxes and barostat state of now
+    const std::vector<double> box0 = h->box, vs0 = h->baro_vs;
+    const std::vector<long long> att0 = h->baro_att, acc0 = h->baro_acc, dr0 = h->baro_draws,
+                                 tot0 = h->baro_acc_tot;
+    const long long bstep0 = h->baro_step;
     for (int attempt = 0; attempt < 3; attempt++) {
         if (h->nl_mode == REVSIM_NL_CHECKPOINT) ensure_list_store(h, n_ckpt);
         if ((rc = forward_impl(h, gamma, n_steps, n_steps_loss, dt, calc_loss))) return rc;
@@ -1397,7 +1602,19 @@ int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gam
         if ((rc = grow_cap(h))) return rc;
         CK(cudaMemcpyAsync(h->d_x, h->d_x0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
         CK(cudaMemcpyAsync(h->d_v, h->d_v0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->st));
+        if (h->baro_on) {
+            h->box = box0;
+            h->baro_vs = vs0;
+            h->baro_att = att0;
+            h->baro_acc = acc0;
+            h->baro_draws = dr0;
+            h->baro_acc_tot = tot0;
+            h->baro_step = bstep0;
+            CK(cudaMemcpyAsync(h->d_rep_box, h->box.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice, h->st));
+            if ((rc = set_cells(h))) return rc;
+        }
     }
+    h->fwd_baro = h->baro_on;
     h->last_blocks = calc_loss ? (n_steps == 0 ? 1 : std::max(1, n_steps / std::max(1, n_steps_loss))) : 0;
     if (loss_out) {
         const int n_blocks = n_steps == 0 ? 1 : std::max(1, n_steps / std::max(1, n_steps_loss));
@@ -1421,6 +1638,9 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
     if (n_steps < 1 || n_steps_loss < 1 || !noise_seeds || !(dt > 0) || !(gamma >= 0) || !(clip_norm_threshold > 0))
         return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
     if (!has_loss(h)) return fail(h, REVSIM_ERR_STATE, "no loss set");
+    if (h->fwd_baro)
+        return fail(h, REVSIM_ERR_STATE, "the forward pass ran with the barostat (an equilibration run): "
+                                         "no reverse record");
     const bool need_store = h->nl_mode == REVSIM_NL_CHECKPOINT || (h->nlog > 0 && n_steps > h->nlog);
     if (need_store && !(h->fwd_valid && h->fwd_steps == n_steps))
         return fail(h, REVSIM_ERR_STATE, "reverse needs the forward pass of the same n_steps");

@@ -151,6 +151,14 @@ cudaError_t launch_enth_finalize(const EnthArgs &a, cudaStream_t st);
 cudaError_t launch_enth_dldx(int N, const int *atom_rep, const double *k, const double *F, double *dLdx,
                              cudaStream_t st);
 
+// Monte-Carlo volume move (rs_barostat.cu): molecule centres scaled by lsc[replica] about
+// the origin, positions wrapped into the scaled box (in place); and the restore of the
+// replicas whose move was rejected.
+cudaError_t launch_baro_scale(int M, const int *mol_rep, const double *box_old, const double *lsc,
+                              double *x, cudaStream_t st);
+cudaError_t launch_baro_restore(int M, const int *mol_rep, const int *accepted, const double *xb,
+                                double *x, cudaStream_t st);
+
 size_t mlp_scratch_doubles();
 // Node evaluation and interval table of the MLP for parameters theta (device, FP64).
 // nt types (1..MLP_NT) of theta, RBF width w: the water model's three types at MLP_WIDTH by

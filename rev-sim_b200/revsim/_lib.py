@@ -34,7 +34,8 @@ EXPORTS = [
     "revsim_stream", "revsim_launch_count", "revsim_set_kernel_timing", "revsim_kernel_time",
     "revsim_set_launch_shape", "revsim_get_launch_shape", "revsim_autotune",
     "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc", "revsim_energy_grad",
-    "revsim_set_enth_vap", "revsim_loss_parts", "revsim_loss_and_grads",
+    "revsim_set_enth_vap", "revsim_loss_parts", "revsim_loss_and_grads", "revsim_set_barostat",
+    "revsim_barostat_state", "revsim_set_box",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -74,6 +75,17 @@ class SystemDesc(ctypes.Structure):
         ("nl_mode", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("mlp", ctypes.c_int32),
+    ]
+
+
+class BarostatDesc(ctypes.Structure):
+    _fields_ = [
+        ("pressure", ctypes.c_double),
+        ("n_steps", ctypes.c_int32),
+        ("scale_factor", ctypes.c_double),
+        ("scale_increment", ctypes.c_double),
+        ("max_volume_frac", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
     ]
 
 
@@ -139,6 +151,9 @@ def load(path=LIB_PATH):
         "revsim_energy_grad": (i32, [vp, pd, pd]),
         "revsim_loss_grad": (i32, [vp, pd, pd]),
         "revsim_set_enth_vap": (i32, [vp, i32, d, d, d]),
+        "revsim_set_barostat": (i32, [vp, P(BarostatDesc)]),
+        "revsim_barostat_state": (i32, [vp, pd, pd, pi64, pi64]),
+        "revsim_set_box": (i32, [vp, pd]),
         "revsim_loss_parts": (i32, [vp, pd, pd]),
         "revsim_loss_and_grads": (i32, [vp, pd, pd, pd, pd, pd]),
         "revsim_rdf": (i32, [vp, i32, i32, pd]),

@@ -188,6 +188,33 @@ class Engine:
         self._check(self._L.revsim_loss_grad(self._h, f64p(loss), f64p(g) if grad else None))
         return loss, g
 
+    def set_barostat(self, enable=True, pressure=1.0, n_steps=30, scale_factor=0.01,
+                     scale_increment=1.1, max_volume_frac=0.3, seed=0):
+        """Monte-Carlo barostat of forward passes (MonteCarloBarostatNoUnits, water.jl:789-865,
+        with its defaults of water.jl:802-806); enable=False switches it off."""
+        if not enable:
+            self._check(self._L.revsim_set_barostat(self._h, None))
+            return
+        d = _lib.BarostatDesc(pressure, n_steps, scale_factor, scale_increment, max_volume_frac,
+                              int(seed) & 0xFFFFFFFFFFFFFFFF)
+        self._check(self._L.revsim_set_barostat(self._h, ctypes.byref(d)))
+
+    def barostat_state(self):
+        """(box [R], volume_scale [R], attempts [R], accepted [R])."""
+        box, vs = np.zeros(self.R), np.zeros(self.R)
+        na, nacc = np.zeros(self.R, dtype=np.int64), np.zeros(self.R, dtype=np.int64)
+        p64 = ctypes.POINTER(ctypes.c_int64)
+        self._check(self._L.revsim_barostat_state(self._h, f64p(box), f64p(vs), na.ctypes.data_as(p64),
+                                                  nacc.ctypes.data_as(p64)))
+        self.box = box.copy()
+        return box, vs, na, nacc
+
+    def set_box(self, box):
+        """New cubic box sides [R] (the boundary argument of forward_sim / reverse_sim)."""
+        b = np.ascontiguousarray(np.broadcast_to(np.asarray(box, dtype=np.float64), (self.R,)))
+        self._check(self._L.revsim_set_box(self._h, f64p(b)))
+        self.box = b.copy()
+
     def set_enth_vap(self, enable=True, u_gas=C.ENTH_U_GAS, rt=C.ENTH_RT, target=C.ENTH_TARGET):
         """Add (or with enable=False remove) the enthalpy-of-vaporisation loss term
         (loss_enth_vap, water.jl:738-755) to the RDF terms of set_loss."""

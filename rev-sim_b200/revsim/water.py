@@ -14,8 +14,10 @@ Differences, each deliberate:
   rebuild exactly that loss from the file;
 * ``loss_type`` is ``"rdf"``, ``"enth_vap"`` or ``"both"`` as in loss_fn (water.jl:757-769);
   the RDF terms stay on the engine between calls, so ``loss_terms`` is needed once;
-* ``run_grads=True`` (the Zygote unrolled-RAD check, water.jl:1052-1099) and
-  ``use_barostat=True`` are not part of the engine and raise ``NotImplementedError``;
+* ``use_barostat=True`` runs the engine's Monte-Carlo barostat (its draws from a stream keyed
+  by the first noise seed; the returned ``sys.boundary`` is the final box); ``run_grads=True``
+  (the Zygote unrolled-RAD check, water.jl:1052-1099) is not part of the engine and raises
+  ``NotImplementedError``;
 * ``n_threads`` is accepted and ignored;
 * noise: per-step seeds drive a counter-based Philox generator, regenerated
   identically in the reverse pass (the reference uses Xoshiro(seed) + randn).
@@ -48,6 +50,9 @@ def _engine_for(coords, boundary, inter_type, engine, precision):
     if n_atoms % 3:
         raise ValueError("water systems have 3 atoms per molecule")
     if engine is not None:
+        if boundary is not None and not np.array_equal(np.broadcast_to(boundary, engine.box.shape),
+                                                       engine.box):
+            engine.set_box(boundary)   # the boundary argument (water.jl:1001)
         return engine
     return Engine(n_atoms // 3, boundary, inter_type=inter_type, precision=precision)
 
@@ -76,17 +81,25 @@ def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
     reference's run_grads=false branch (water.jl:1100-1102)."""
     if run_grads:
         raise NotImplementedError("run_grads (Zygote unrolled RAD) is not part of the engine")
-    if use_barostat:
-        raise NotImplementedError("the Monte-Carlo barostat is not part of the engine")
     eng = _engine_for(coords, boundary, inter_type, engine, precision)
     eng.set_params(params)
     eng.set_state(coords, velocities)
     if calc_loss:
         _set_loss(eng, loss_type, loss_terms)
-    loss = eng.forward(noise_seeds, gamma, n_steps, n_steps_loss if n_steps_loss else max(n_steps, 1),
-                       dt, calc_loss)
+    seeds = np.asarray(noise_seeds, dtype=np.uint64)
+    if use_barostat:
+        # MonteCarloBarostatNoUnits(1 bar, temp, boundary) (water.jl:1009-1014); its draws
+        # come from a stream keyed by the run's first noise seed
+        eng.set_barostat(True, seed=int(seeds.reshape(-1)[0]) if seeds.size else 0)
+    try:
+        loss = eng.forward(seeds, gamma, n_steps, n_steps_loss if n_steps_loss else max(n_steps, 1),
+                           dt, calc_loss)
+    finally:
+        if use_barostat:
+            eng.set_barostat(False)
     x, v = eng.get_state()
-    sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
+    box = eng.barostat_state()[0]
+    sys = SimSystem(eng, x, v, float(box[0]) if eng.R == 1 else box)
     return sys, (float(loss[0]) if eng.R == 1 else loss), [None] * eng.n_params
 
 
@@ -121,13 +134,14 @@ def reweighting_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n
     points (every n_steps_loss steps) of one forward run, beta = 1 / (k_B T); dl/dtheta is the
     enthalpy term's direct gradient (zero for the RDF loss).  Returns
     (sys, loss, grads, l_rdf, l_ev)."""
-    if use_barostat:
-        raise NotImplementedError("the Monte-Carlo barostat is not part of the engine")
     eng = _engine_for(coords, boundary, inter_type, engine, precision)
     eng.set_params(params)
     eng.set_state(coords, velocities)
     _set_loss(eng, loss_type, loss_terms)
     seeds = np.asarray(noise_seeds, dtype=np.uint64)
+    if use_barostat:
+        # one barostat over the whole run: its step count carries across the blocks
+        eng.set_barostat(True, seed=int(seeds.reshape(-1)[0]) if seeds.size else 0)
     n_blocks = 1 if n_steps == 0 else n_steps // n_steps_loss
     acc = np.zeros((3, eng.R))   # loss, l_rdf, l_ev
     dl_acc = np.zeros((eng.R, eng.n_params))
@@ -144,6 +158,8 @@ def reweighting_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n
         dl_acc += dlb
         dE_acc += dE
         l_dE_acc += lb[:, None] * dE
+    if use_barostat:
+        eng.set_barostat(False)
     loss, l_rdf, l_ev = acc / n_blocks
     beta = 1.0 / (C.KB * np.asarray(temp, dtype=np.float64))
     beta = np.broadcast_to(beta, (eng.R,))[:, None]
