@@ -333,13 +333,25 @@ __device__ __forceinline__ void pair_row(uint32_t mask, const typename V4T<R>::T
 #undef RS_SLOT
 }
 
+// Register budget per thread.  FP32: the forward kernels at 80 (no spills), the reverse
+// kernel at 104 (U = 1, no spills), 128 (U = 2) and 168 (U = 3, launched with at most 256
+// threads; software pipelining wants the registers); on the 9,000-atom box these budgets
+// took the autotuned gradient from 134.5 to 139.8 M atom-steps/s.  FP64: 128, and 255
+// for U = 3.
+template <typename R, bool REV, int U>
+constexpr int step_maxnreg() {
+    if (sizeof(R) == 8) return U == 3 ? 255 : 128;
+    if (!REV) return 80;
+    return U == 3 ? 168 : (U == 1 ? 104 : 128);
+}
+
 // U = 1: one neighbour entry per lane per iteration; 2: two entries, all loads issued
 // first; 3: one entry, with the next entry's index and coordinates loaded while the
 // current one is computed (software pipelining; launched with at most 256 threads so
 // the compiler may use more registers).
 template <typename R, int FORM, int G, bool REV, bool SHIFT, int U>
-__global__ void __launch_bounds__(U == 3 ? 256 : 512) k_water_step(StepArgs a, NbConsts<R> nb,
-                                                                   BondConsts bc) {
+__global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a, NbConsts<R> nb,
+                                                                      BondConsts bc) {
     using V4 = typename V4T<R>::T;
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int NTH = NF + 1;
