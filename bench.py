@@ -60,17 +60,20 @@ def parse():
     ap.add_argument("--gamma", type=float, default=0.0)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--form", default="lj")
+    ap.add_argument("--loss", default="rdf", choices=["rdf", "enth_vap", "both"],
+                    help="water: loss_type of loss_fn (water.jl:757-769)")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-GPU comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=10)
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
     ap.add_argument("--n-replicas", type=int, default=64, help="replicas workload: boxes")
     ap.add_argument("--rep-steps", type=int, default=2000, help="replicas workload: steps")
-    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas"],
+    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas", "equil"],
                     help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
                          "carbon, 16 replicas of 8,000 atoms; mlp: 895 waters with the learned "
                          "pair correction, gradient throughput and a training comparison; "
-                         "replicas: 64 water boxes of 300-3,000 molecules at 280-320 K in one launch")
+                         "replicas: 64 water boxes of 300-3,000 molecules at 280-320 K in one launch; "
+                         "equil: barostatted forward equilibration of the water box")
     ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
@@ -87,8 +90,30 @@ def parse():
 
 
 def workload_name(a):
+    loss = "" if a.loss == "rdf" else f"_loss-{a.loss}"
     return (f"water_{a.n_mol}mol_{a.box:g}nm_{a.form}_{a.precision}_"
-            f"{a.n_steps}fwd+{a.n_steps}rev")
+            f"{a.n_steps}fwd+{a.n_steps}rev{loss}")
+
+
+LOSS_TEXT = {
+    "rdf": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs sigma x1.02 / eps x0.95 target",
+    "enth_vap": "enthalpy of vaporisation (loss_enth_vap, water.jl:738-755): "
+                "(3.69 - U/n + 2.45 - 46.92)^2 per loss point, direct dl/dtheta included",
+    "both": "O-O smoothed RDF (as rdf) plus the enthalpy-of-vaporisation term (as enth_vap)",
+}
+
+
+def apply_loss(e, a, target):
+    """loss_type: the RDF term, the enthalpy term or both on an engine."""
+    from revsim import oo_l2_term
+    e.set_loss([oo_l2_term(target)] if a.loss in ("rdf", "both") else [])
+    e.set_enth_vap(a.loss in ("enth_vap", "both"))
+
+
+def oracle_loss(a, target):
+    from oracle import orc
+    t = orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, target, 2, 1.0)
+    return orc.Loss([t] if a.loss in ("rdf", "both") else [], enth_vap=a.loss in ("enth_vap", "both"))
 
 
 def config(a, extra=None):
@@ -96,7 +121,7 @@ def config(a, extra=None):
          "n_steps": a.n_steps, "n_steps_loss": a.n_steps_loss, "n_steps_trunc": a.n_steps_loss,
          "n_steps_log": 1000, "dt_ps": 0.001, "gamma_per_ps": a.gamma, "pair_form": a.form,
          "precision": a.precision,
-         "loss": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs sigma x1.02 / eps x0.95 target",
+         "loss": LOSS_TEXT[a.loss],
          "l2": "flushed (256 MiB write) between timed steps"}
     if extra:
         c.update(extra)
@@ -195,15 +220,14 @@ def cpu_sample(a, x0, v0, p, target, n_s):
     from oracle import orc
     from revsim import systems
     s = orc.make_system(a.n_mol, a.box, a.form)
-    t = orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, target, 2, 1.0)
-    loss = orc.Loss([t])
+    loss = oracle_loss(a, target)
     seeds = systems.noise_seeds(n_s, seed=99)
     t0 = time.perf_counter()
     xf, vf, _, sx, sv = orc.forward_sim(s, p, x0, v0, seeds, a.gamma, n_s, n_s, 0.001, loss, False)
     t1 = time.perf_counter()
     orc.reverse_sim(s, p, xf, vf, seeds, a.gamma, n_s, n_s, n_s, 0.001, sx, sv, loss)
     t2 = time.perf_counter()
-    orc.loss_grad(s, loss, xf)
+    orc.loss_and_grads(s, p, loss, xf)
     t3 = time.perf_counter()
     t_loss = t3 - t2
     # steps only, plus the loss amortised at one evaluation per n_steps_loss in each pass
@@ -268,7 +292,7 @@ def run_ours(a):
     x0, v0, p, target = prepare(a, local, a.equil_ps)
     eng = Engine(a.n_mol, a.box, inter_type=a.form, precision=a.precision, device=local)
     eng.set_params(p)
-    eng.set_loss([oo_l2_term(target)])
+    apply_loss(eng, a, target)
     eng.set_state(x0, v0)
     seeds = systems.noise_seeds(a.n_steps, seed=100 + rank)
     if a.profile:
@@ -379,7 +403,7 @@ def run_ours(a):
         # the same gradient in plain FP64 on the GPU: throughput and gradient difference
         e64 = Engine(a.n_mol, a.box, inter_type=a.form, precision="fp64", device=local)
         e64.set_params(p)
-        e64.set_loss([oo_l2_term(target)])
+        apply_loss(e64, a, target)
         e64.set_state(x0, v0)
         e64.autotune()
         e64.set_state(x0, v0)
@@ -442,6 +466,183 @@ def run_ours(a):
                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])}}
         out.update(extra)
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------- equilibration workload
+EQUIL_METRIC = "forward atom-steps/s (barostatted Langevin equilibration)"
+
+
+def equil_config(a, extra=None):
+    c = {"workload": f"water_{a.n_mol}mol_{a.box:g}nm_{a.form}_{a.precision}_equil_npt_{a.n_steps}fwd",
+         "n_atoms": 3 * a.n_mol, "box_nm": a.box, "n_steps": a.n_steps, "dt_ps": 0.001,
+         "gamma_per_ps": 1.0, "pair_form": a.form, "precision": a.precision,
+         "barostat": "Monte-Carlo, 1 bar, a volume move every 30 steps (water.jl:789-865, "
+                     "use_barostat of the train() equilibration, water.jl:1642-1645)",
+         "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def equil_cpu_sample(a, x0, v0, p, n_s=60):
+    """The FP64 oracle's barostatted forward run on n_s steps (two volume moves)."""
+    from oracle import orc
+    from revsim import systems
+    s = orc.make_system(a.n_mol, a.box, a.form)
+    b = orc.make_barostat(a.box, seed=5)
+    seeds = systems.noise_seeds(n_s, seed=97)
+    t0 = time.perf_counter()
+    orc.forward_sim_barostat(s, p, x0, v0, seeds, 1.0, n_s, 0.001, b)
+    dt = time.perf_counter() - t0
+    return 3 * a.n_mol * n_s / dt, orc.num_threads(), (
+        f"{n_s} barostatted forward steps ({n_s // 30} volume moves) of the {3 * a.n_mol}-atom box, "
+        f"FP64 oracle")
+
+
+def run_reference_equil(a):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import orc
+    from revsim import constants as C, systems
+    orc.build()
+    x = systems.water_coords(a.n_mol, a.box, seed=0)
+    v = systems.mb_velocities(a.n_mol, seed=1)
+    p = np.array(C.default_params(a.form))
+    s = orc.make_system(a.n_mol, a.box, a.form)
+    x, v, _, _, _ = orc.forward_sim(s, p, x, v, systems.noise_seeds(50, seed=10), 5.0, 50, 50,
+                                    0.001, None, False)
+    vals = []
+    for i in range(a.warmup + a.steps):
+        val, cores, desc = equil_cpu_sample(a, x, v, p)
+        if i >= a.warmup:
+            vals.append(val)
+    value = statistics.mean(vals)
+    out = {"metric": EQUIL_METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1e3 * 3 * a.n_mol * a.n_steps / value,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "impl": "reference", "config": equil_config(a, {"precision": "fp64"}),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours_equil(a):
+    """Throughput of the barostatted equilibration (forward steps with a Monte-Carlo volume
+    move every 30 steps) of the water box, on one GPU per rank (independent replicas)."""
+    import ctypes
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import build as _build
+    _build.build()
+    from revsim import Engine, _lib, systems
+    x0, v0, p, _ = prepare(a, local, a.equil_ps)
+    eng = Engine(a.n_mol, a.box, inter_type=a.form, precision=a.precision, device=local)
+    eng.set_params(p)
+    eng.set_state(x0, v0)
+    eng.autotune()
+    seeds = systems.noise_seeds(a.n_steps, seed=500 + rank)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def run(xs=x0, vs=v0):
+        eng.set_box(a.box)
+        eng.set_state(xs, vs)
+        eng.set_barostat(True, seed=7 + rank)
+        eng.forward(seeds, 1.0, a.n_steps, a.n_steps, 0.001, calc_loss=False)
+        eng.set_barostat(False)
+
+    for _ in range(a.warmup):
+        run()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    box, vs, na, nacc = eng.barostat_state()
+    total = sum(times)
+    if dist is not None:
+        t = torch.tensor([total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    ms = total / a.steps
+    n_atoms = 3 * a.n_mol
+    value = world * n_atoms * a.n_steps / (ms * 1e-3)
+    # end to end: the state from pinned host buffers, the final state and box read back
+    xh = torch.from_numpy(x0.copy()).pin_memory()
+    vh = torch.from_numpy(v0.copy()).pin_memory()
+    e2e = []
+    for _ in range(a.steps):
+        flush.zero_()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(xh.numpy(), vh.numpy())
+        eng.get_state()
+        eng.barostat_state()
+        e1.record(stream)
+        barrier()
+        e2e.append(e0.elapsed_time(e1))
+    e2e_value = world * n_atoms * a.n_steps / (sum(e2e) / a.steps * 1e-3)
+    # roofline of the dominant kernel (the fused forward step)
+    eng.set_kernel_timing(True)
+    run()
+    ft_ms, ft_n = eng.kernel_time(1)
+    eng.set_kernel_timing(False)
+    launch_ms = ft_ms / max(ft_n, 1)
+    xs, _ = eng.get_state()
+    box_now = eng.barostat_state()[0][0]
+    ipairs, oo = count_ipairs(xs, box_now, eng.neighbor_pairs(0))
+    flops_launch = FLOPS_FWD_IPAIR * ipairs + FLOPS_FWD_OO_EXTRA * oo
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "kernel": "k_water_step<float, LJ, forward> (fused forward step)",
+                "launch_ms": launch_ms, "launches_timed": ft_n, "ipairs": ipairs,
+                "flops_per_launch": flops_launch,
+                "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)",
+                "step_kernel_share": ft_ms / ms}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        val, cores, desc = equil_cpu_sample(a, x0, v0, p)
+        cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        out = {"metric": EQUIL_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+               "data": "synthetic", "config": equil_config(a),
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 3 * n_atoms * 8 + a.n_steps * 8,
+                       "d2h_bytes_per_step": 2 * 3 * n_atoms * 8 + 32},
+               "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+               "barostat": {"final_box_nm": float(box[0]), "volume_moves": int(na[0]),
+                            "accepted": int(nacc[0]), "volume_scale_nm3": float(vs[0])}}
         print(json.dumps(out), flush=True)
     eng.close()
     if dist is not None:
@@ -1102,6 +1303,8 @@ if __name__ == "__main__":
         run_ours_mlp(args)
     elif args.workload == "diamond":
         run_reference_diamond(args) if args.impl == "reference" else run_ours_diamond(args)
+    elif args.workload == "equil":
+        run_reference_equil(args) if args.impl == "reference" else run_ours_equil(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

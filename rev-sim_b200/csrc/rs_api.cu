@@ -131,7 +131,7 @@ struct revsim_handle {
     std::vector<double> baro_vs;
     std::vector<long long> baro_att, baro_acc, baro_draws, baro_acc_tot;
     long long baro_step = 0;   // forward steps since the barostat was switched on
-    double *d_bx = nullptr, *d_lsc = nullptr;
+    double *d_bx = nullptr, *d_lsc = nullptr, *d_repE = nullptr;
     int *d_bacc = nullptr;
     int cell_cap = 0;   // allocated cells (the cell grid follows the boxes)
     // instrumentation
@@ -666,19 +666,17 @@ int set_cells(revsim_handle *h) {
     return REVSIM_OK;
 }
 
-// Potential energy per replica (FP64 kernel over the given rows, summed in molecule order).
+// Potential energy per replica (FP64 kernel over the given rows, per-replica tree sums).
 int replica_energies(revsim_handle *h, const uint32_t *nbr, const int *cnt, std::vector<double> &E) {
     if (!h->d_epart) CK(dalloc(&h->d_epart, (size_t)h->M * (h->P + 1)));
     EnergyArgs a = energy_args(h, nbr, cnt);
     a.grads = 0;
     CK(launch_energy_grads(h->mlp ? (int)F_LJ_MLP : h->form, h->prec, a, h->st));
-    h->launches++;
-    std::vector<double> part((size_t)h->M * (h->P + 1));
-    CK(cudaMemcpyAsync(part.data(), h->d_epart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
+    CK(launch_rep_energy(h->R, h->d_rep_atom0, h->d_rep_nmol, h->d_epart, h->P, h->d_repE, h->st));
+    h->launches += 2;
     E.assign(h->R, 0.0);
-    for (int r = 0; r < h->R; r++)
-        for (int I = h->mol0[r]; I < h->mol0[r] + h->nmol[r]; I++) E[r] += part[(size_t)I * (h->P + 1)];
+    CK(cudaMemcpyAsync(E.data(), h->d_repE, sizeof(double) * h->R, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
     return REVSIM_OK;
 }
 
@@ -974,7 +972,7 @@ void free_all(revsim_handle *h) {
                     h->d_scale, h->d_status, h->d_maxcnt, h->d_count, h->d_snap_x, h->d_snap_v,
                     h->d_ckpt, h->d_seeds, h->d_loss, h->d_loss_acc, h->d_dLdx,
                     h->d_cell_rep, h->d_nbr_store, h->d_cnt_store, h->d_ev_acc, h->d_ev_k,
-                    h->d_ev_grad, h->d_nbr_ev, h->d_cnt_ev, h->d_bx, h->d_lsc, h->d_bacc};
+                    h->d_ev_grad, h->d_nbr_ev, h->d_cnt_ev, h->d_bx, h->d_lsc, h->d_bacc, h->d_repE};
     for (void *p : ptrs) dfree(p);
     for (Term &T : h->terms) {
         dfree(T.d_target);
@@ -1430,6 +1428,7 @@ int32_t revsim_set_barostat(revsim_handle *h, const revsim_barostat_desc *d) {
         CK(dalloc(&h->d_bx, 3 * (size_t)h->N));
         CK(dalloc(&h->d_lsc, (size_t)h->R));
         CK(dalloc(&h->d_bacc, (size_t)h->R));
+        CK(dalloc(&h->d_repE, (size_t)h->R));
     }
     h->baro = *d;
     h->baro_vs.resize(h->R);

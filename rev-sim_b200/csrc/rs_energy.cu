@@ -80,10 +80,17 @@ __device__ DN<4> form_energy(const double *p, double r) {
     }
 }
 
+// EG_LANES lanes per molecule stride its row; the per-lane sums are combined by a fixed
+// xor butterfly (deterministic), and lane 0 adds the bonded terms and writes the partials.
+constexpr int EG_LANES = 16, EG_THREADS = 128;
+
 template <int FORM, typename V4>
-__global__ void k_energy_grads(EnergyArgs a) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x;
-    if (I >= a.M) return;
+__global__ void __launch_bounds__(EG_THREADS) k_energy_grads(EnergyArgs a) {
+    const int Ig = (blockIdx.x * blockDim.x + threadIdx.x) / EG_LANES;
+    const int lane = threadIdx.x % EG_LANES;
+    // every lane of the warp reaches the butterfly: molecules past the end run empty
+    const bool live = Ig < a.M;
+    const int I = live ? Ig : a.M - 1;
     constexpr int NFm = FormInfo<FORM>::NP;
     const int rep = a.mol_rep[I];
     const double L = a.rep_box[rep];
@@ -98,8 +105,8 @@ __global__ void k_energy_grads(EnergyArgs a) {
     double *madj = a.mlp_adj ? a.mlp_adj + ((size_t)rep * MLP_NCOPY + (I % MLP_NCOPY)) * MLP_NT * MLP_NG * 4
                              : nullptr;
     const uint32_t *row = a.nbr + (size_t)I * a.cap;
-    const int cnt = min(a.nbr_cnt[I], a.cap);
-    for (int e = 0; e < cnt; e++) {
+    const int cnt = live ? min(a.nbr_cnt[I], a.cap) : 0;
+    for (int e = lane; e < cnt; e += EG_LANES) {
         const uint32_t ent = row[e];
         const int J = (int)(ent & 0x7FFFFFu);
         if (J <= I) continue;
@@ -142,6 +149,15 @@ __global__ void k_energy_grads(EnergyArgs a) {
                 }
             }
     }
+    // fixed butterfly over the molecule's lanes
+    const unsigned wmask = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < 17; k++) {
+        if (k > P) break;
+#pragma unroll
+        for (int o = EG_LANES / 2; o > 0; o >>= 1) acc[k] = __dadd_rn(acc[k], __shfl_xor_sync(wmask, acc[k], o));
+    }
+    if (lane != 0 || !live) return;
     // bonds (O, H1), (O, H2) and the angle H1-O-H2 (water.jl:915-968 energies)
     const double *xo = x + 9 * (size_t)I;
     double b[2][3];
@@ -195,6 +211,23 @@ __global__ void __launch_bounds__(kEnthThreads) k_enth_finalize(EnthArgs a) {
     }
 }
 
+// Per replica: the sum of the energy column of the partials (fixed-order tree).
+__global__ void __launch_bounds__(kEnthThreads) k_rep_energy(const int *rep_atom0, const int *rep_nmol,
+                                                             const double *part, int P, double *E) {
+    __shared__ double red[kEnthThreads];
+    const int r = blockIdx.x, t = threadIdx.x;
+    const int m0 = rep_atom0[r] / 3, n = rep_nmol[r];
+    double s = 0.0;
+    for (int I = t; I < n; I += kEnthThreads) s += part[(size_t)(m0 + I) * (P + 1)];
+    red[t] = s;
+    __syncthreads();
+    for (int w = kEnthThreads / 2; w > 0; w >>= 1) {
+        if (t < w) red[t] += red[t + w];
+        __syncthreads();
+    }
+    if (t == 0) E[r] = red[0];
+}
+
 __global__ void k_enth_dldx(int n3, const int *atom_rep, const double *k, const double *F, double *dLdx) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n3) dLdx[i] += k[atom_rep[i / 3]] * F[i];
@@ -202,11 +235,11 @@ __global__ void k_enth_dldx(int n3, const int *atom_rep, const double *k, const 
 
 template <int FORM>
 cudaError_t launch_f(int prec, const EnergyArgs &a, cudaStream_t st) {
-    const int t = 128, b = (a.M + t - 1) / t;
+    const int per = EG_THREADS / EG_LANES, b = (a.M + per - 1) / per;
     if (prec == 1)
-        k_energy_grads<FORM, float4><<<b, t, 0, st>>>(a);
+        k_energy_grads<FORM, float4><<<b, EG_THREADS, 0, st>>>(a);
     else
-        k_energy_grads<FORM, double4><<<b, t, 0, st>>>(a);
+        k_energy_grads<FORM, double4><<<b, EG_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -214,6 +247,12 @@ cudaError_t launch_f(int prec, const EnergyArgs &a, cudaStream_t st) {
 
 cudaError_t launch_enth_finalize(const EnthArgs &a, cudaStream_t st) {
     if (a.R > 0) k_enth_finalize<<<a.R, kEnthThreads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rep_energy(int R, const int *rep_atom0, const int *rep_nmol, const double *part, int P,
+                              double *E, cudaStream_t st) {
+    if (R > 0) k_rep_energy<<<R, kEnthThreads, 0, st>>>(rep_atom0, rep_nmol, part, P, E);
     return cudaGetLastError();
 }
 

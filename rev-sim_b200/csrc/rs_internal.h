@@ -147,6 +147,9 @@ struct EnthArgs {
     double *acc, *ev_acc, *k, *dgrad;
 };
 cudaError_t launch_enth_finalize(const EnthArgs &a, cudaStream_t st);
+// E[r] = the replica's sum of part[I][0] (fixed-order tree), r < R.
+cudaError_t launch_rep_energy(int R, const int *rep_atom0, const int *rep_nmol, const double *part, int P,
+                              double *E, cudaStream_t st);
 // dLdx[i] += k[replica of atom i / 3] * F[i], i < 3N (dl_ev/dx = (2 e / n) F).
 cudaError_t launch_enth_dldx(int N, const int *atom_rep, const double *k, const double *F, double *dLdx,
                              cudaStream_t st);
