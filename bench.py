@@ -86,6 +86,8 @@ def parse():
                     help="diamond without the learned radial term (SW alone)")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed gradient and exit (the command profiled under ncu)")
+    ap.add_argument("--profile-shape", default="16,8,3/32,4,1",
+                    help="water --profile: reverse/forward launch shapes (lanes,mols_per_cta,unroll)")
     return ap.parse_args()
 
 
@@ -296,13 +298,20 @@ def run_ours(a):
     eng.set_state(x0, v0)
     seeds = systems.noise_seeds(a.n_steps, seed=100 + rank)
     if a.profile:
-        # one gradient between cudaProfilerStart/Stop (ncu --profile-from-start off)
+        # the launch shapes the bench's autotuner picks on this box (fixed here: timings
+        # under the profiler would steer the tuner), then one gradient between
+        # cudaProfilerStart/Stop (ncu --profile-from-start off captures only that gradient)
+        (rg, rm, ru), (fg, fm, fu) = [tuple(int(t) for t in q.split(",")) for q in a.profile_shape.split("/")]
+        eng.set_launch_shape(rg, rm, ru, which=0)
+        eng.set_launch_shape(fg, fm, fu, which=1)
+        eng.set_state(x0, v0)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
         eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
         eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
+        print(json.dumps({"profiled_shape": eng.launch_shape(0), "forward_shape": eng.launch_shape(1)}))
         eng.close()
         return
     shape = eng.autotune()

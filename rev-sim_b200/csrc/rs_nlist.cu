@@ -102,6 +102,7 @@ __global__ void k_cell_sort(NlistArgs a) {
 // the cutoff are decided by the exact FP64 Molly arithmetic (dist2_fp64), so the set
 // is bit-identical to the all-FP64 test.  Entries are appended in candidate order.
 constexpr int kRowChunk = 2048;
+constexpr int kCandBatch = 256;
 
 __device__ __forceinline__ float mi_f(float d, float L, float hL) {
     return d > hL ? d - L : (d < -hL ? d + L : d);
@@ -110,7 +111,8 @@ __device__ __forceinline__ float mi_f(float d, float L, float hL) {
 __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     extern __shared__ float s_c[];              // [9][kRowChunk] coordinates
     int *s_idx = (int *)(s_c + 9 * kRowChunk);   // [kRowChunk] molecule ids
-    __shared__ int s_cell[125], s_off[126];
+    __shared__ int s_off[126], s_start[125];
+    __shared__ int s_kbuf[8 * kCandBatch];       // per warp: candidates passing the O-O test
     const int c_home = blockIdx.x;
     const int r = a.cell_rep[c_home];
     const int nc = a.rep_nc[r];
@@ -123,23 +125,22 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     const int cx = cl % nc, cy = (cl / nc) % nc, cz = cl / (nc * nc);
     const int span = nc >= 5 ? 5 : nc;
     const int ncell = span * span * span;
-    // neighbourhood cells in canonical order and their member counts
+    // neighbourhood cells in canonical order, their member counts and first members,
+    // loaded by one thread per cell; the exclusive prefix of the counts in shared memory
     if (threadIdx.x < ncell) {
         const int t = threadIdx.x;
         const int dz = t / (span * span), dy = (t / span) % span, dx = t % span;
         const int z = nc >= 5 ? (cz + dz - 2 + nc) % nc : dz;
         const int y = nc >= 5 ? (cy + dy - 2 + nc) % nc : dy;
         const int x = nc >= 5 ? (cx + dx - 2 + nc) % nc : dx;
-        s_cell[t] = off0 + (z * nc + y) * nc + x;
+        const int c = off0 + (z * nc + y) * nc + x;
+        s_off[t + 1] = a.cell_cnt[c];
+        s_start[t] = a.cell_start[c];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int t = 0; t < ncell; t++) {
-            s_off[t] = acc;
-            acc += a.cell_cnt[s_cell[t]];
-        }
-        s_off[ncell] = acc;
+        s_off[0] = 0;
+        for (int t = 1; t <= ncell; t++) s_off[t] += s_off[t - 1];
     }
     __syncthreads();
     const int total = s_off[ncell];
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
             for (int k = threadIdx.x; k < cn; k += blockDim.x) {
                 const int g = c0 + k;
                 while (s_off[t + 1] <= g) t++;
-                const int J = a.cell_sorted[a.cell_start[s_cell[t]] + (g - s_off[t])];
+                const int J = a.cell_sorted[s_start[t] + (g - s_off[t])];
                 s_idx[k] = J;
                 const double *xj = a.x + 9 * (size_t)J;
 #pragma unroll
@@ -177,15 +178,33 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
 #pragma unroll
                 for (int u = 0; u < 9; u++) xi[u] = (float)a.x[9 * (size_t)I + u];
                 uint32_t *row = a.nbr + (size_t)I * a.cap;
-                for (int base = 0; base < cn; base += 32) {
-                    const int k = base + lane;
-                    uint32_t ent = 0;
-                    if (k < cn) {
-                        const int J = s_idx[k];
-                        const float ox = mi_f(s_c[k] - xi[0], L, hL);
-                        const float oy = mi_f(s_c[kRowChunk + k] - xi[1], L, hL);
-                        const float oz = mi_f(s_c[2 * kRowChunk + k] - xi[2], L, hL);
-                        if (J != I && ox * ox + oy * oy + oz * oz <= rcand2) {
+                // in batches of kCandBatch candidates: the O-O test first, compacting the
+                // passing candidates (in order) for the nine-pair test, so the lanes of the
+                // second pass are all busy
+                int *s_k = s_kbuf + warp * kCandBatch;
+                for (int b0 = 0; b0 < cn; b0 += kCandBatch) {
+                    const int b1 = min(b0 + kCandBatch, cn);
+                    int nk = 0;
+                    for (int base = b0; base < b1; base += 32) {
+                        const int k = base + lane;
+                        bool pass = false;
+                        if (k < b1) {
+                            const float ox = mi_f(s_c[k] - xi[0], L, hL);
+                            const float oy = mi_f(s_c[kRowChunk + k] - xi[1], L, hL);
+                            const float oz = mi_f(s_c[2 * kRowChunk + k] - xi[2], L, hL);
+                            pass = s_idx[k] != I && ox * ox + oy * oy + oz * oz <= rcand2;
+                        }
+                        const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                        if (pass) s_k[nk + __popc(bal & ((1u << lane) - 1u))] = k;
+                        nk += __popc(bal);
+                    }
+                    __syncwarp();
+                    for (int base = 0; base < nk; base += 32) {
+                        const int idx = base + lane;
+                        uint32_t ent = 0;
+                        if (idx < nk) {
+                            const int k = s_k[idx];
+                            const int J = s_idx[k];
                             uint32_t mask = 0;
 #pragma unroll
                             for (int ka = 0; ka < 3; ka++)
@@ -203,13 +222,14 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                                 }
                             if (mask) ent = (uint32_t)J | (mask << 23);
                         }
+                        const unsigned bal = __ballot_sync(0xffffffffu, ent != 0);
+                        if (ent) {
+                            const int pos = cnt[q] + __popc(bal & ((1u << lane) - 1u));
+                            if (pos < a.cap) row[pos] = ent;
+                        }
+                        cnt[q] += __popc(bal);
                     }
-                    const unsigned bal = __ballot_sync(0xffffffffu, ent != 0);
-                    if (ent) {
-                        const int pos = cnt[q] + __popc(bal & ((1u << lane) - 1u));
-                        if (pos < a.cap) row[pos] = ent;
-                    }
-                    cnt[q] += __popc(bal);
+                    __syncwarp();
                 }
             }
         }
