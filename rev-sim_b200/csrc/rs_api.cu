@@ -1700,8 +1700,9 @@ int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes, 
         if (which >= 0 && which != dir) continue;
         revsim_handle::Shape &sh = h->shp[dir];
         const int G = lanes ? lanes : sh.G, m = mpc ? mpc : sh.mpc, U = unroll ? unroll : sh.U;
-        if ((G != 8 && G != 16 && G != 32) || m < 1 || G * m > 512 || (G * m) % 32 != 0 || U < 1 || U > 3 ||
-            (U == 3 && G * m > 256))
+        const int thr = G * m;
+        if ((G != 8 && G != 16 && G != 32) || m < 1 || thr > 512 || thr % 32 != 0 || U < 1 || U > 3 ||
+            (U == 3 && thr > 256))
             return fail(h, REVSIM_ERR_BADARG, "unsupported launch shape");
         sh.G = G;
         sh.U = U;
@@ -1739,11 +1740,12 @@ int32_t revsim_autotune(revsim_handle *h, double dt) {
         double best = std::numeric_limits<double>::infinity();
         int bg = h->shp[dir].G, bm = h->shp[dir].mpc, bu = h->shp[dir].U;
         for (int G : {8, 16, 32}) {
-            for (int threads : {64, 128, 256, 512}) {
+            for (int threads : {64, 128, 192, 256, 384, 512}) {
                 if (threads < G || threads % G) continue;
                 for (int U : {1, 2, 3}) {
+                    const int mpc = threads / G;
                     if (U == 3 && threads > 256) continue;
-                    if ((rc = revsim_set_launch_shape(h, dir, G, threads / G, U))) break;
+                    if ((rc = revsim_set_launch_shape(h, dir, G, mpc, U))) break;
                     StepArgs a = base_args(h, rev);
                     a.pos_in = h->d_pos[0];
                     a.wgt_in = h->d_wgt[0];
@@ -1763,7 +1765,7 @@ int32_t revsim_autotune(revsim_handle *h, double dt) {
                     if (ms < best) {
                         best = ms;
                         bg = G;
-                        bm = threads / G;
+                        bm = mpc;
                         bu = U;
                     }
                 }

@@ -333,6 +333,98 @@ __device__ __forceinline__ void pair_row(uint32_t mask, const typename V4T<R>::T
 #undef RS_SLOT
 }
 
+// The per-atom update of a step after the pair, bonded and reduction phases: forces F and
+// VJP Gv of atom k of molecule I (FP64 sums), then forces-only output, the forward B-A-O-A
+// update or the reverse un-kick with the adjoint updates and the next step's part 1.
+// n2 receives |Gv|^2, xn the new FP64 position when wpos.
+template <typename R, bool REV>
+__device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int rep, double Ld,
+                                            const double F[3], const double Gv[3], double &n2,
+                                            double xn[3], bool &wpos) {
+    using V4 = typename V4T<R>::T;
+    const size_t ia = 3 * (size_t)I + k;
+    const double m = k == 0 ? a.mO : a.mH;
+    if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) atomicOr(a.status, ST_NAN);
+    const double xk[3] = {a.x[3 * ia], a.x[3 * ia + 1], a.x[3 * ia + 2]};
+    if (a.mode & MODE_FORCES_ONLY) {
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            a.F_out[3 * ia + u] = F[u];
+            if (REV) a.G[3 * ia + u] = Gv[u];
+        }
+    } else if (!REV) {
+        // B-A-O-A (water.jl:1032-1037)
+        const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
+        double xi[3] = {0.0, 0.0, 0.0};
+        if (a.s != 0.0) atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            double v = a.v[3 * ia + u], x = xk[u];
+            v = __dadd_rn(v, __ddiv_rn(__dmul_rn(F[u], a.dt), m));
+            x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
+            x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            x = wrap1d(x, Ld);
+            a.v[3 * ia + u] = v;
+            a.x[3 * ia + u] = x;
+            xn[u] = x;
+        }
+        wpos = true;
+    } else {
+        const double dt2 = __dmul_rn(a.dt, a.dt);
+        const bool fuse = (a.mode & MODE_FUSE_NEXT) != 0;
+        const bool defer = (a.mode & MODE_DEFER_BA) != 0;
+        double xi[3] = {0.0, 0.0, 0.0};
+        if (fuse && a.s != 0.0) {
+            const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
+            atom_noise(a.seed_next[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+        }
+        double Cm[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const size_t e = 3 * ia + u;
+            a.G[e] = Gv[u];
+            n2 = __dadd_rn(n2, __dmul_rn(Gv[u], Gv[u]));
+            // v_{n-1} = v' - F dt / m (water.jl:1516)
+            double v = __dsub_rn(a.v[e], __ddiv_rn(__dmul_rn(F[u], a.dt), m));
+            if (!defer) {
+                // water.jl:1520-1521
+                const double B = __dadd_rn(__dmul_rn(a.c, a.B[e]), __dmul_rn(dt2, Gv[u]));
+                a.B[e] = B;
+                a.A[e] = __dadd_rn(a.A[e], B);
+            }
+            if (fuse) {
+                // part 1 of the next reverse step (water.jl:1496-1502)
+                double x = xk[u];
+                x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
+                x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                x = wrap1d(x, Ld);
+                const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
+                                           __ddiv_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]),
+                                                               __dadd_rn(1.0, a.c)),
+                                                     2.0));
+                const double C = __dadd_rn(a.C[e], D);
+                a.D[e] = D;
+                a.C[e] = C;
+                a.x[e] = x;
+                xn[u] = x;
+                Cm[u] = __ddiv_rn(C, m);
+            }
+            a.v[e] = v;
+        }
+        if (fuse) {
+            V4 wo;
+            wo.x = (R)Cm[0];
+            wo.y = (R)Cm[1];
+            wo.z = (R)Cm[2];
+            wo.w = R(0);
+            ((V4 *)a.wgt_out)[ia] = wo;
+            wpos = true;
+        }
+    }
+}
+
 // Register budget per thread.  FP32: the forward kernels at 80 (no spills), the reverse
 // kernel at 104 (U = 1, no spills), 128 (U = 2) and 168 (U = 3, launched with at most 256
 // threads; software pipelining wants the registers); on the 9,000-atom box these budgets
@@ -509,94 +601,14 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     bool wpos = false;
     if (active && lane < 3) {
         const int k = lane;
-        const size_t ia = 3 * (size_t)I + k;
-        const double m = k == 0 ? a.mO : a.mH;
-        double F[3], Gv[3];
+        double F[3], Gv[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int u = 0; u < 3; u++) {
             F[u] = __dadd_rn((double)pick3(k, f[0][u], f[1][u], f[2][u]), (double)s_bond[3 * k + u]);
             if (REV)
                 Gv[u] = __dadd_rn((double)pick3(k, g[0][u], g[1][u], g[2][u]), (double)s_bond[9 + 3 * k + u]);
         }
-        if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) atomicOr(a.status, ST_NAN);
-        const double xk[3] = {a.x[3 * ia], a.x[3 * ia + 1], a.x[3 * ia + 2]};
-        if (a.mode & MODE_FORCES_ONLY) {
-#pragma unroll
-            for (int u = 0; u < 3; u++) {
-                a.F_out[3 * ia + u] = F[u];
-                if (REV) a.G[3 * ia + u] = Gv[u];
-            }
-        } else if (!REV) {
-            // B-A-O-A (water.jl:1032-1037)
-            const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
-            double xi[3] = {0.0, 0.0, 0.0};
-            if (a.s != 0.0) atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
-#pragma unroll
-            for (int u = 0; u < 3; u++) {
-                double v = a.v[3 * ia + u], x = xk[u];
-                v = __dadd_rn(v, __ddiv_rn(__dmul_rn(F[u], a.dt), m));
-                x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-                v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
-                x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-                x = wrap1d(x, Ld);
-                a.v[3 * ia + u] = v;
-                a.x[3 * ia + u] = x;
-                xn[u] = x;
-            }
-            wpos = true;
-        } else {
-            const double dt2 = __dmul_rn(a.dt, a.dt);
-            const bool fuse = (a.mode & MODE_FUSE_NEXT) != 0;
-            const bool defer = (a.mode & MODE_DEFER_BA) != 0;
-            double xi[3] = {0.0, 0.0, 0.0};
-            if (fuse && a.s != 0.0) {
-                const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
-                atom_noise(a.seed_next[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
-            }
-            double Cm[3];
-#pragma unroll
-            for (int u = 0; u < 3; u++) {
-                const size_t e = 3 * ia + u;
-                a.G[e] = Gv[u];
-                n2 = __dadd_rn(n2, __dmul_rn(Gv[u], Gv[u]));
-                // v_{n-1} = v' - F dt / m (water.jl:1516)
-                double v = __dsub_rn(a.v[e], __ddiv_rn(__dmul_rn(F[u], a.dt), m));
-                if (!defer) {
-                    // water.jl:1520-1521
-                    const double B = __dadd_rn(__dmul_rn(a.c, a.B[e]), __dmul_rn(dt2, Gv[u]));
-                    a.B[e] = B;
-                    a.A[e] = __dadd_rn(a.A[e], B);
-                }
-                if (fuse) {
-                    // part 1 of the next reverse step (water.jl:1496-1502)
-                    double x = xk[u];
-                    x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-                    v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
-                    x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-                    x = wrap1d(x, Ld);
-                    const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
-                                               __ddiv_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]),
-                                                                   __dadd_rn(1.0, a.c)),
-                                                         2.0));
-                    const double C = __dadd_rn(a.C[e], D);
-                    a.D[e] = D;
-                    a.C[e] = C;
-                    a.x[e] = x;
-                    xn[u] = x;
-                    Cm[u] = __ddiv_rn(C, m);
-                }
-                a.v[e] = v;
-            }
-            if (fuse) {
-                V4 wo;
-                wo.x = (R)Cm[0];
-                wo.y = (R)Cm[1];
-                wo.z = (R)Cm[2];
-                wo.w = R(0);
-                ((V4 *)a.wgt_out)[ia] = wo;
-                wpos = true;
-            }
-        }
+        atom_update<R, REV>(a, I, k, rep, Ld, F, Gv, n2, xn, wpos);
     }
 
     // Gather buffer of the next step: H atoms are written next to their O (lane 0 of

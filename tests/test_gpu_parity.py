@@ -359,18 +359,22 @@ def test_launch_shapes_agree(cfg1_water):
     e = engine(n_mol, box, "lj", "fp64")
     e.set_state(x, v)
     ref = None
+    per_g = {}
     for G in (8, 16, 32):
-        for threads in (64, 256, 512):
-            for U in (1, 2, 3):
-                if U == 3 and threads > 256:
-                    continue
-                e.set_launch_shape(G, threads // G, U)
-                F, Gv, th = e.force_vjp(w, ac)
-                if ref is None:
-                    ref = (F, Gv, th)
-                    continue
-                assert nrel(F, ref[0]) < 1e-13 and nrel(Gv, ref[1]) < 1e-13
-                assert np.all(scaled_err(th[0], ref[2][0], np.array(C.default_params())) < 1e-12)
+        shapes = [(threads // G, U) for threads in (64, 256, 512) for U in (1, 2, 3)
+                  if not (U == 3 and threads > 256)]
+        for mpc, U in shapes:
+            e.set_launch_shape(G, mpc, U)
+            F, Gv, th = e.force_vjp(w, ac)
+            if ref is None:
+                ref = (F, Gv, th)
+            assert nrel(F, ref[0]) < 1e-13 and nrel(Gv, ref[1]) < 1e-13
+            assert np.all(scaled_err(th[0], ref[2][0], np.array(C.default_params())) < 1e-12)
+            # at one lane count every loop form sums each atom's slots in the same order
+            if G in per_g:
+                assert np.array_equal(F, per_g[G][0]) and np.array_equal(Gv, per_g[G][1]), (G, mpc, U)
+            else:
+                per_g[G] = (F, Gv)
     rshape, fshape = e.autotune()
     assert rshape[0] in (8, 16, 32) and rshape[2] in (1, 2, 3) and fshape[0] in (8, 16, 32)
     F2, Gv2, _ = e.force_vjp(w, ac)
