@@ -1199,9 +1199,15 @@ def run_ours_replicas(a):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import build as _build
     _build.build()
     from revsim import Engine, _lib, constants as C, oo_l2_term, systems
+    from revsim.distributed import allreduce_mean
     n_mol, boxes, temps = replica_systems(a.n_replicas)
     R, K = a.n_replicas, a.rep_steps
     p = np.array(C.default_params("lj"))
@@ -1232,11 +1238,18 @@ def run_ours_replicas(a):
     stream = torch.cuda.ExternalStream(eng.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
     def gradient():
+        # one parameter update's gradient: every rank's replicas, averaged over all ranks
+        # (the one collective of the path, P + 1 doubles)
         eng.set_state(x0, v0)
         lf = eng.forward(seeds, 1.0, K, 1000, 0.001)
         lr, g = eng.reverse(seeds, 1.0, K, 1000, 1000, 0.001)
-        return lf, lr, g.mean(axis=0)
+        return lf, lr, allreduce_mean(g)
 
     if a.profile:
         torch.cuda.synchronize()
@@ -1253,16 +1266,21 @@ def run_ours_replicas(a):
     with Clocks(local) as clk:
         for _ in range(a.steps):
             flush.zero_()
-            torch.cuda.synchronize()
+            barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             lf, lr, g = gradient()
             e1.record(stream)
-            torch.cuda.synchronize()
+            barrier()
             times.append(e0.elapsed_time(e1))
     launches = (eng.launch_count() - n0) // a.steps
     clocks = clk.summary()
-    ms_step = sum(times) / a.steps
+    total_ms = sum(times)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / a.steps
     n_atoms = int(3 * n_mol.sum())
     value = world * n_atoms * K / (ms_step * 1e-3)
     eng.set_kernel_timing(True)
@@ -1293,7 +1311,11 @@ def run_ours_replicas(a):
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
-           "data": "synthetic", "config": replicas_config(a, n_mol),
+           "data": "synthetic",
+           "config": replicas_config(a, n_mol, {
+               "parallelism": f"replicas{world}" if world > 1 else "single",
+               "gradient_exchange": "per-replica gradients averaged over all ranks by one "
+                                    "all-reduce of P + 1 doubles per update (timed)"}),
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None, "clocks": clocks,
            "loss": {"forward_mean": float(lf.mean()), "reverse_mean": float(lr.mean())},
@@ -1302,6 +1324,9 @@ def run_ours_replicas(a):
     if rank == 0:
         print(json.dumps(out), flush=True)
     eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
