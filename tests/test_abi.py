@@ -64,3 +64,37 @@ def test_sw_error_paths_without_device(lib):
     assert L.revsim_sw_set_params(None, None, 0) == -1
     assert L.revsim_sw_forward(None, None, 0.0, 0, 1, 0, 0.0, 0, None, None) == -1
     assert L.revsim_sw_last_error(None) == b"null handle"
+
+
+def test_new_entry_points_reject_a_null_handle(lib):
+    from revsim import _lib
+    L = _lib.load()
+    d = _lib.BarostatDesc(1.0, 30, 0.01, 1.1, 0.3, 0)
+    assert L.revsim_set_enth_vap(None, 1, 3.69, 2.45, 46.92) == -1
+    assert L.revsim_loss_parts(None, None, None) == -1
+    assert L.revsim_loss_and_grads(None, None, None, None, None, None) == -1
+    assert L.revsim_set_barostat(None, ctypes.byref(d)) == -1
+    assert L.revsim_barostat_state(None, None, None, None, None) == -1
+    assert L.revsim_set_box(None, None) == -1
+
+
+def test_descriptor_validation_before_any_device_call(lib):
+    """Invalid descriptions return REVSIM_ERR_BADARG before the library touches CUDA."""
+    import numpy as np
+    from revsim import _lib, constants as C
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    n = np.array([0], dtype=np.int32)            # a replica without molecules
+    box, temp = np.array([3.0]), np.array([295.0])
+    pd = ctypes.POINTER(ctypes.c_double)
+    desc = _lib.SystemDesc(1, n.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), box.ctypes.data_as(pd),
+                           temp.ctypes.data_as(pd), 0, 0, C.O_MASS, C.H_MASS, C.COULOMB_CONST,
+                           C.CRF_CONST, 1.0, 1.2, C.KB, 20, 1000, 0, 0, 0)
+    assert L.revsim_create(ctypes.byref(desc), ctypes.byref(h)) == -1
+    n[0] = 10
+    box[0] = 2.3                                  # below twice the 1.2 nm list cutoff
+    assert L.revsim_create(ctypes.byref(desc), ctypes.byref(h)) == -1
+    box[0] = 3.0
+    desc.mlp = 1
+    desc.inter_type = 2                           # the learned term needs REVSIM_LJ
+    assert L.revsim_create(ctypes.byref(desc), ctypes.byref(h)) == -1
