@@ -68,12 +68,13 @@ def parse():
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
     ap.add_argument("--n-replicas", type=int, default=64, help="replicas workload: boxes")
     ap.add_argument("--rep-steps", type=int, default=2000, help="replicas workload: steps")
-    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas", "equil"],
+    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas", "equil", "reweight"],
                     help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
                          "carbon, 16 replicas of 8,000 atoms; mlp: 895 waters with the learned "
                          "pair correction, gradient throughput and a training comparison; "
                          "replicas: 64 water boxes of 300-3,000 molecules at 280-320 K in one launch; "
-                         "equil: barostatted forward equilibration of the water box")
+                         "equil: barostatted forward equilibration of the water box; "
+                         "reweight: the reweighting gradient estimator on the water box")
     ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
@@ -653,6 +654,169 @@ def run_ours_equil(a):
                "barostat": {"final_box_nm": float(box[0]), "volume_moves": int(na[0]),
                             "accepted": int(nacc[0]), "volume_scale_nm3": float(vs[0])}}
         print(json.dumps(out), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------- reweighting workload
+REWEIGHT_METRIC = "forward atom-steps/s (reweighting gradient estimator)"
+
+
+def reweight_config(a, extra=None):
+    c = {"workload": f"water_{a.n_mol}mol_{a.box:g}nm_{a.form}_{a.precision}_reweight_{a.n_steps}fwd",
+         "n_atoms": 3 * a.n_mol, "box_nm": a.box, "n_steps": a.n_steps, "n_steps_loss": a.n_steps_loss,
+         "dt_ps": 0.001, "gamma_per_ps": 1.0, "pair_form": a.form, "precision": a.precision,
+         "estimator": "reweighting_sim (water.jl:1107-1210): at every loss point the loss, its "
+                      "direct gradient and dE/dtheta (FP64 energy kernel); "
+                      "<dl/dtheta> - beta (<L dE/dtheta> - <L><dE/dtheta>) on the host",
+         "loss": LOSS_TEXT[a.loss], "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def reweight_cpu_sample(a, x0, v0, p, target, n_s=20):
+    """The FP64 oracle: n_s forward steps, then the loss, its gradient and dE/dtheta once."""
+    from oracle import orc
+    from revsim import systems
+    s = orc.make_system(a.n_mol, a.box, a.form)
+    loss = oracle_loss(a, target)
+    seeds = systems.noise_seeds(n_s, seed=96)
+    t0 = time.perf_counter()
+    xf, _, _, _, _ = orc.forward_sim(s, p, x0, v0, seeds, 1.0, n_s, n_s, 0.001, loss, False)
+    t1 = time.perf_counter()
+    orc.loss_and_grads(s, p, loss, xf)
+    orc.energy_grads(s, p, xf, orc.neighbor_pairs(s, xf))
+    t2 = time.perf_counter()
+    per_step = (t1 - t0) / n_s + (t2 - t1) / a.n_steps_loss
+    return 3 * a.n_mol / per_step, orc.num_threads(), (
+        f"{n_s} forward steps of the {3 * a.n_mol}-atom box plus one loss point (loss, gradient, "
+        f"dE/dtheta) amortised over {a.n_steps_loss} steps, FP64 oracle")
+
+
+def run_reference_reweight(a):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import orc
+    from revsim import constants as C, systems
+    orc.build()
+    x = systems.water_coords(a.n_mol, a.box, seed=0)
+    v = systems.mb_velocities(a.n_mol, seed=1)
+    p = np.array(C.default_params(a.form))
+    s = orc.make_system(a.n_mol, a.box, a.form)
+    x, v, _, _, _ = orc.forward_sim(s, p, x, v, systems.noise_seeds(50, seed=10), 5.0, 50, 50,
+                                    0.001, None, False)
+    target = np.zeros(200)
+    vals = []
+    for i in range(a.warmup + a.steps):
+        val, cores, desc = reweight_cpu_sample(a, x, v, p, target)
+        if i >= a.warmup:
+            vals.append(val)
+    value = statistics.mean(vals)
+    out = {"metric": REWEIGHT_METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1e3 * 3 * a.n_mol * a.n_steps / value,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "impl": "reference", "config": reweight_config(a, {"precision": "fp64"}),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours_reweight(a):
+    import ctypes
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import build as _build
+    _build.build()
+    from revsim import Engine, _lib, systems
+    from revsim.water import reweighting_sim
+    x0, v0, p, target = prepare(a, local, a.equil_ps)
+    eng = Engine(a.n_mol, a.box, inter_type=a.form, precision=a.precision, device=local)
+    eng.set_params(p)
+    eng.set_state(x0, v0)
+    eng.autotune()
+    seeds = systems.noise_seeds(a.n_steps, seed=600 + rank)
+    from revsim import oo_l2_term
+    terms = [oo_l2_term(target)] if a.loss in ("rdf", "both") else []
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def run(xs=x0, vs=v0):
+        return reweighting_sim(xs, vs, None, seeds, 1.0, a.n_steps, a.n_steps_loss, p, 0.001, 1,
+                               a.form, a.loss, loss_terms=terms, engine=eng)
+
+    for _ in range(a.warmup):
+        run()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = run()
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    total = sum(times)
+    if dist is not None:
+        t = torch.tensor([total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    ms = total / a.steps
+    n_atoms = 3 * a.n_mol
+    value = world * n_atoms * a.n_steps / (ms * 1e-3)
+    eng.set_kernel_timing(True)
+    run()
+    ft_ms, ft_n = eng.kernel_time(1)
+    eng.set_kernel_timing(False)
+    launch_ms = ft_ms / max(ft_n, 1)
+    xs, _ = eng.get_state()
+    ipairs, oo = count_ipairs(xs, a.box, eng.neighbor_pairs(0))
+    flops_launch = FLOPS_FWD_IPAIR * ipairs + FLOPS_FWD_OO_EXTRA * oo
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp32_tflops(local, ctypes.byref(peak))
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "kernel": "k_water_step<float, LJ, forward> (fused forward step)",
+                "launch_ms": launch_ms, "ipairs": ipairs, "flops_per_launch": flops_launch,
+                "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)",
+                "step_kernel_share": ft_ms / ms}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        val, cores, desc = reweight_cpu_sample(a, x0, v0, p, target)
+        cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        _, loss, grads, l_rdf, l_ev = out
+        res = {"metric": REWEIGHT_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+               "data": "synthetic", "config": reweight_config(a),
+               "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 2 * 3 * n_atoms * 8 + a.n_steps * 8,
+                       "d2h_bytes_per_step": 2 * 3 * n_atoms * 8 + 8 * (3 + 2 * len(p)) * (a.n_steps // a.n_steps_loss)},
+               "e2e_note": "every timed run starts from host arrays (reweighting_sim sets the state)",
+               "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+               "loss": float(loss), "l_rdf": float(l_rdf), "l_ev": float(l_ev),
+               "gradient": [float(g) for g in grads]}
+        print(json.dumps(res), flush=True)
     eng.close()
     if dist is not None:
         dist.barrier()
@@ -1337,6 +1501,8 @@ if __name__ == "__main__":
         run_ours_mlp(args)
     elif args.workload == "diamond":
         run_reference_diamond(args) if args.impl == "reference" else run_ours_diamond(args)
+    elif args.workload == "reweight":
+        run_reference_reweight(args) if args.impl == "reference" else run_ours_reweight(args)
     elif args.workload == "equil":
         run_reference_equil(args) if args.impl == "reference" else run_ours_equil(args)
     elif args.impl == "reference":
