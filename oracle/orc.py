@@ -47,6 +47,14 @@ class OrcBarostat(ctypes.Structure):
                 ("n_accepted", _I64), ("n_draws", _I64), ("n_accepted_total", _I64)]
 
 
+class OrcGasSystem(ctypes.Structure):
+    _fields_ = [("n_water", _I32), ("n_gas", _I32), ("box", _D), ("m_O", _D), ("m_H", _D),
+                ("inter_type", _I32), ("coulomb_const", _D), ("crf_const", _D), ("cutoff", _D),
+                ("nl_cutoff", _D), ("n_steps_nf", _I32), ("kB", _D), ("temp", _D), ("kb_w", _D),
+                ("r0_w", _D), ("ka_w", _D), ("th0_w", _D), ("kb_g", _D), ("r0_g", _D),
+                ("n_mol_ev", _I32)]
+
+
 class OrcSwSystem(ctypes.Structure):
     _fields_ = [("n_atoms", _I32), ("box", _D), ("mass", _D), ("kB", _D), ("temp", _D),
                 ("mlp", _I32)]
@@ -59,7 +67,7 @@ class OrcSwLoss(ctypes.Structure):
 def build(force=False):
     """Compile the oracle with its Makefile (gcc, OpenMP, no FMA contraction)."""
     srcs = ["revsim_oracle.c", "revsim_oracle.h", "sw_oracle.c", "sw_oracle.h", "mlp_oracle.c",
-            "mlp_oracle.h"]
+            "mlp_oracle.h", "gas_oracle.c", "gas_oracle.h", "Makefile"]
     if force or not os.path.exists(_LIB_PATH) or any(
             os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, f)) for f in srcs):
         subprocess.run(["make", "-s", "-C", _HERE, "-B" if force else "liborc_revsim.so"],
@@ -139,6 +147,29 @@ def lib():
         L.orc_sw_reverse_sim.restype = _D
         L.orc_sw_reverse_sim.argtypes = [PS, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _I32, _I32, _D,
                                          _PD, _PD, PL, _PD]
+        PG = ctypes.POINTER(OrcGasSystem)
+        L.orc_gas_n_params.restype = _I32
+        L.orc_gas_n_params.argtypes = [_I32]
+        L.orc_gas_neighbor_pairs.restype = _I64
+        L.orc_gas_neighbor_pairs.argtypes = [PG, _PD, _PI32, _I64]
+        L.orc_gas_forces.argtypes = [PG, _PD, _PD, _PI32, _I64, _PD]
+        L.orc_gas_forces_grads.argtypes = [PG, _PD, _PD, _PI32, _I64, _PD, _PD, _PD, _PD, _PD]
+        L.orc_gas_energy.restype = _D
+        L.orc_gas_energy.argtypes = [PG, _PD, _PD, _PI32, _I64, _PD]
+        L.orc_gas_noise.argtypes = [PG, ctypes.c_uint64, _PD]
+        L.orc_gas_centres.argtypes = [PG, _PD, _PD]
+        L.orc_gas_diffusion_D.restype = _D
+        L.orc_gas_diffusion_D.argtypes = [_PD, _I32, _I32, _D, _D, _PD]
+        L.orc_gas_loss_final.restype = _D
+        L.orc_gas_loss_final.argtypes = [_I32, _PD, _I32, _I32, _D, _D, _D, _PD, _PD]
+        L.orc_gas_ev_point.restype = _D
+        L.orc_gas_ev_point.argtypes = [PG, _PD, _PD, _I32, _PD, _PD]
+        L.orc_gas_forward_sim.restype = _D
+        L.orc_gas_forward_sim.argtypes = [PG, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _D, _I32, _I32,
+                                          _PD, _PD, _PD, _PD]
+        L.orc_gas_reverse_sim.restype = _D
+        L.orc_gas_reverse_sim.argtypes = [PG, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _I32, _D, _I32,
+                                          _PD, _PD, _PD, _PD, _PD]
         _lib = L
     return _lib
 
@@ -517,3 +548,136 @@ def mlp_table_n(theta, nt, rc, width):
     c = np.zeros((nt, MLP_NG, 4))
     lib().orc_mlp_table_n(_pd(_f64(theta)), nt, rc, width, _pd(c))
     return c
+
+
+# ------------------------------------------------------------------ gas in water
+# diffusion.jl: O2 bond k = 1640.4 kcal/mol/A^2 in kJ/mol/nm^2 and r0 (:46, :1113-1116)
+GAS_KB, GAS_R0 = 1640.4 * 4.184 * 100, 0.12074
+GAS_LOSS = {"diff": 1, "ev": 4, "diff_ev": 5}
+
+
+def make_gas_system(n_water, n_gas, box, inter_type="lj", temp=295.15, *, m_O=15.99943,
+                    m_H=1.007947, coulomb_const=138.93545764438196, cutoff=1.0, nl_cutoff=1.2,
+                    n_steps_nf=20, kB=0.00831446261815324, kb_w=462750.4, r0_w=0.09572,
+                    ka_w=836.8, th0_w=1.82421813418, kb_g=GAS_KB, r0_g=GAS_R0, n_mol_ev=None):
+    crf = (1.0 / cutoff**3) * ((78.3 - 1) / (2 * 78.3 + 1))
+    return OrcGasSystem(n_water, n_gas, box, m_O, m_H, INTER[inter_type], coulomb_const, crf,
+                        cutoff, nl_cutoff, n_steps_nf, kB, temp, kb_w, r0_w, ka_w, th0_w, kb_g,
+                        r0_g, n_water + n_gas if n_mol_ev is None else n_mol_ev)
+
+
+def gas_n_atoms(s):
+    return 3 * s.n_water + 2 * s.n_gas
+
+
+def gas_n_params(inter_type):
+    return lib().orc_gas_n_params(INTER[inter_type] if isinstance(inter_type, str) else inter_type)
+
+
+def gas_neighbor_pairs(s, x):
+    x = _f64(x)
+    n = lib().orc_gas_neighbor_pairs(ctypes.byref(s), _pd(x), None, 0)
+    pairs = np.zeros((max(n, 1), 2), dtype=np.int32)
+    lib().orc_gas_neighbor_pairs(ctypes.byref(s), _pd(x), pairs.ctypes.data_as(_PI32), n)
+    return pairs[:n]
+
+
+def gas_forces(s, p, x, pairs=None):
+    x = _f64(x)
+    pairs = gas_neighbor_pairs(s, x) if pairs is None else np.ascontiguousarray(pairs, np.int32)
+    F = np.zeros(3 * gas_n_atoms(s))
+    lib().orc_gas_forces(ctypes.byref(s), _pd(_f64(p)), _pd(x), pairs.ctypes.data_as(_PI32),
+                         len(pairs), _pd(F))
+    return F.reshape(-1, 3)
+
+
+def gas_forces_grads(s, p, x, w, acoef, pairs=None):
+    """(F, dl_dfi, dl_dp) of calc_F_and_grads! against dl_dfi_prev = w with the contraction
+    against acoef."""
+    x = _f64(x)
+    pairs = gas_neighbor_pairs(s, x) if pairs is None else np.ascontiguousarray(pairs, np.int32)
+    n3 = 3 * gas_n_atoms(s)
+    F, G = np.zeros(n3), np.zeros(n3)
+    dp = np.zeros(gas_n_params(s.inter_type))
+    lib().orc_gas_forces_grads(ctypes.byref(s), _pd(_f64(p)), _pd(x), pairs.ctypes.data_as(_PI32),
+                               len(pairs), _pd(_f64(w)), _pd(_f64(acoef)), _pd(F), _pd(G), _pd(dp))
+    return F.reshape(-1, 3), G.reshape(-1, 3), dp
+
+
+def gas_energy(s, p, x, pairs=None, grads=False):
+    x = _f64(x)
+    pairs = gas_neighbor_pairs(s, x) if pairs is None else np.ascontiguousarray(pairs, np.int32)
+    dp = np.zeros(gas_n_params(s.inter_type)) if grads else None
+    E = lib().orc_gas_energy(ctypes.byref(s), _pd(_f64(p)), _pd(x), pairs.ctypes.data_as(_PI32),
+                             len(pairs), _pd(dp) if grads else None)
+    return (E, dp) if grads else E
+
+
+def gas_noise(s, seed):
+    xi = np.zeros(3 * gas_n_atoms(s))
+    lib().orc_gas_noise(ctypes.byref(s), ctypes.c_uint64(int(seed)), _pd(xi))
+    return xi.reshape(-1, 3)
+
+
+def gas_centres(s, x):
+    c = np.zeros(3 * s.n_gas)
+    lib().orc_gas_centres(ctypes.byref(s), _pd(_f64(x)), _pd(c))
+    return c.reshape(-1, 3)
+
+
+def gas_diffusion_D(gc, box, loss_frequency, grads=False):
+    gc = _f64(gc)
+    n_frames, n_gas = gc.shape[0], gc.shape[1]
+    g = np.zeros_like(gc) if grads else None
+    D = lib().orc_gas_diffusion_D(_pd(gc), n_frames, n_gas, box, loss_frequency,
+                                  _pd(g) if grads else None)
+    return (D, g) if grads else D
+
+
+def gas_loss_final(loss_type, gc, box, loss_frequency, ev_sum=0.0):
+    """(loss, [D m^2/s, l_diff, l_rdf, l_ev], dl_diff/dgc)."""
+    gc = _f64(gc)
+    out = np.zeros(4)
+    g = np.zeros_like(gc)
+    l = lib().orc_gas_loss_final(GAS_LOSS[loss_type], _pd(gc), gc.shape[0], gc.shape[1], box,
+                                 loss_frequency, ev_sum, _pd(out), _pd(g))
+    return l, out, g
+
+
+def gas_ev_point(s, p, x, n_blocks):
+    """(l, dl/dx, direct dl/dtheta) of one loss point's enthalpy term."""
+    g = np.zeros(3 * gas_n_atoms(s))
+    dp = np.zeros(gas_n_params(s.inter_type))
+    l = lib().orc_gas_ev_point(ctypes.byref(s), _pd(_f64(p)), _pd(_f64(x)), n_blocks, _pd(g), _pd(dp))
+    return l, g.reshape(-1, 3), dp
+
+
+def gas_forward_sim(s, p, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss_type="diff",
+                    calc_loss=True):
+    """(x, v, loss, snaps_x, snaps_v, centres, [D, l_diff, l_rdf, l_ev])."""
+    x, v = _f64(x).copy(), _f64(v).copy()
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    n_blocks = 1 if n_steps == 0 else n_steps // n_steps_loss
+    n3 = 3 * gas_n_atoms(s)
+    sx, sv = np.zeros((n_blocks + 1, n3)), np.zeros((n_blocks + 1, n3))
+    gc = np.zeros((n_blocks, s.n_gas, 3))
+    out = np.zeros(4)
+    l = lib().orc_gas_forward_sim(ctypes.byref(s), _pd(_f64(p)), _pd(x), _pd(v),
+                                  seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss, dt,
+                                  GAS_LOSS[loss_type], 1 if calc_loss else 0, _pd(sx), _pd(sv),
+                                  _pd(gc), _pd(out))
+    return x, v, l, sx, sv, gc, out
+
+
+def gas_reverse_sim(s, p, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, snaps_x,
+                    snaps_v, centres, loss_type="diff"):
+    """(x, v, loss, dl_dp, [D, l_diff, l_rdf, l_ev])."""
+    x, v = _f64(x).copy(), _f64(v).copy()
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    dp = np.zeros(gas_n_params(s.inter_type))
+    out = np.zeros(4)
+    l = lib().orc_gas_reverse_sim(ctypes.byref(s), _pd(_f64(p)), _pd(x), _pd(v),
+                                  seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss,
+                                  n_steps_trunc, dt, GAS_LOSS[loss_type], _pd(_f64(snaps_x)),
+                                  _pd(_f64(snaps_v)), _pd(_f64(centres)), _pd(dp), _pd(out))
+    return x, v, l, dp, out

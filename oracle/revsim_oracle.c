@@ -251,6 +251,11 @@ static int pair_form(int type, const double *p, double r, double invr2, int grad
     return 0;
 }
 
+int32_t orc_pair_form(int32_t type, const double *p, double r, double invr2, int32_t grads,
+                      double *F, double *dFdr, double *g) {
+    return pair_form(type, p, r, invr2, grads, F, dFdr, g);
+}
+
 /* Pair-form potential energy (Molly potential_energy for LJ / soft-core, and
  * water.jl:409-526 for the others); used by the FD consistency tests only. */
 static double pair_form_energy(int type, const double *p, double r) {
@@ -284,6 +289,10 @@ static double pair_form_energy(int type, const double *p, double r) {
         }
     }
     return 0.0;
+}
+
+double orc_pair_form_energy(int32_t type, const double *p, double r) {
+    return pair_form_energy(type, p, r);
 }
 
 /* The pair-form energies on complex parameters (the same expressions as
@@ -378,6 +387,26 @@ static int angle_term(const double *a_, const double *b_, const double *ta, cons
     }
     if (disp_out) *disp_out = th0 - th.v;
     return 1;
+}
+
+int32_t orc_angle_term(const double a[3], const double b[3], const double ta[3],
+                       const double tb[3], double ka, double th0, double Fi[3], double Fk[3],
+                       double dFi[3], double dFk[3]) {
+    dual Fid[3], Fkd[3];
+    if (!angle_term(a, b, ta, tb, ka, th0, Fid, Fkd, NULL, NULL, NULL)) return 0;
+    for (int u = 0; u < 3; u++) {
+        Fi[u] = Fid[u].v;
+        Fk[u] = Fkd[u].v;
+        dFi[u] = Fid[u].d;
+        dFk[u] = Fkd[u].d;
+    }
+    return 1;
+}
+
+/* The complex-parameter energy for callers in this library (the gas restatement's
+ * complex-step dE/dtheta through the mixing rules). */
+double complex orc_pair_form_energy_cx(int32_t type, const double complex *p, double r) {
+    return pair_form_energy_c(type, p, r);
 }
 
 /* ------------------------------------------------------------------------- */

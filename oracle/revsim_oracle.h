@@ -126,6 +126,19 @@ double orc_energy(const orc_system *s, const double *params, const double *x,
 void orc_noise(const orc_system *s, uint64_t seed, double temp, double *xi);
 /* Four N(0,1) draws for (seed, atom): Philox blocks 0 and 1 (the per-atom draw of orc_noise). */
 void orc_philox_normals(uint64_t seed, uint32_t atom, double z[4]);
+/* Building blocks shared with the gas-in-water restatement (gas_oracle.c).
+ * orc_pair_form: F(r) (positive = repulsive), dF/dr and dF/dtheta of one pair form for
+ * the per-pair parameters p (its own mixing of p with itself is exact), invr2 = 1/r2;
+ * returns 0 when the iszero gate switches the form off.  orc_pair_form_energy: its
+ * potential energy.  orc_angle_term: the harmonic angle's forces on the two outer
+ * atoms for the arms a, b from the central atom (the central atom takes minus their
+ * sum) and their tangents along (ta, tb); returns 0 when a x b = 0. */
+int32_t orc_pair_form(int32_t type, const double *p, double r, double invr2, int32_t grads,
+                      double *F, double *dFdr, double *g);
+double orc_pair_form_energy(int32_t type, const double *p, double r);
+int32_t orc_angle_term(const double a[3], const double b[3], const double ta[3],
+                       const double tb[3], double ka, double th0, double Fi[3], double Fk[3],
+                       double dFi[3], double dFk[3]);
 
 /* RDF histogram of one term at positions x: writes h[n_grid]. */
 void orc_rdf(const orc_system *s, const orc_rdf_term *t, const double *x, double *h);

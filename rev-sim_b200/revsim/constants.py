@@ -74,3 +74,36 @@ def langevin_coeffs(gamma, dt):
     """c = exp(-gamma dt), s = sqrt(1 - c^2) (water.jl:1019-1020)."""
     c = math.exp(-gamma * dt)
     return c, math.sqrt(1 - c * c)
+
+
+# ------------------------------------------------------------------ gas in water
+# diffusion.jl: 885 waters and 10 O2 in a 3.0 nm box (:30-34, :47), O2 bond
+# k = 1640.4 kcal mol^-1 A^-2 and r0 = 0.12074 nm (:46, :1113-1116), gas sites of mass m_O
+# and no charge; default sigma_gas / eps_gas and the per-form parameters (:1621-1639).
+GAS_N_WATER, GAS_N_GAS, GAS_BOX = 885, 10, 3.0
+GAS_KB_BOND, GAS_R0_BOND = 1640.4 * 4.184 * 100, 0.12074
+GAS_SIGMA, GAS_EPSILON = 0.3297, 0.438
+GAS_BUCK = (BUCK_A, BUCK_B, BUCK_C)
+GAS_LOSS_TYPES = {"diff": 1, "ev": 4, "diff_ev": 5}
+
+
+def gas_default_params(inter_type="lj"):
+    """Parameter vector of diffusion.jl:1629-1639: the water and gas pair-form parameters,
+    the form's own globals, then q_O."""
+    if inter_type == "lj":
+        head = [SIGMA, EPSILON, GAS_SIGMA, GAS_EPSILON]
+    elif inter_type == "dexp":
+        head = [SIGMA, EPSILON, GAS_SIGMA, GAS_EPSILON, DEXP_ALPHA, DEXP_BETA]
+    elif inter_type == "buck":
+        head = [BUCK_A, BUCK_B, BUCK_C, *GAS_BUCK]
+    elif inter_type == "ljsc":
+        head = [SIGMA, EPSILON, GAS_SIGMA, GAS_EPSILON, LJSC_ALPHA, LJSC_LAMBDA]
+    elif inter_type == "buff":
+        head = [SIGMA, EPSILON, GAS_SIGMA, GAS_EPSILON, BUFF_DELTA, BUFF_GAMMA]
+    else:
+        raise ValueError("inter_type not recognised")
+    return head + [O_CHARGE]
+
+
+def gas_n_params(inter_type):
+    return 5 if inter_type == "lj" else 7

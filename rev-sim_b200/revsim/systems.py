@@ -94,3 +94,32 @@ def load_pdb(path):
 def box_for_density(n_mol, mol_per_nm3=33.1):
     """Cubic box side giving liquid-water number density (~33.1 molecules/nm^3)."""
     return (n_mol / mol_per_nm3) ** (1.0 / 3.0)
+
+
+def gas_water_coords(n_water, n_gas, box, seed=0, jitter=0.02):
+    """Waters followed by O2 molecules [3 n_water + 2 n_gas, 3] (nm), wrapped.  As in
+    setup_system (diffusion.jl:1060-1118): n_water + n_gas lattice waters, n_gas of them
+    (chosen by the seed) become O2 with the first site on the water O and the second
+    0.12074 nm along O -> H1."""
+    n_mol = n_water + n_gas
+    x = water_coords(n_mol, box, seed=seed, jitter=jitter).reshape(n_mol, 3, 3)
+    rng = np.random.default_rng(seed + 1000)
+    gas = np.sort(rng.choice(n_mol, size=n_gas, replace=False))
+    keep = np.setdiff1d(np.arange(n_mol), gas)
+    xo = x[gas, 0]
+    d = x[gas, 1] - xo
+    d -= box * np.round(d / box)
+    o2 = xo + d / np.linalg.norm(d, axis=1, keepdims=True) * C.GAS_R0_BOND
+    out = np.concatenate([x[keep].reshape(-1, 3), np.stack([xo, o2], axis=1).reshape(-1, 3)])
+    return out - np.floor(out / box) * box
+
+
+def gas_water_masses(n_water, n_gas):
+    return np.concatenate([masses(n_water), np.full(2 * n_gas, C.O_MASS)])
+
+
+def gas_water_velocities(n_water, n_gas, temp=C.TEMP, seed=1):
+    """Maxwell-Boltzmann velocities of the gas-in-water system (nm/ps)."""
+    rng = np.random.default_rng(seed)
+    sd = np.sqrt(C.KB * temp / gas_water_masses(n_water, n_gas))
+    return rng.normal(size=(len(sd), 3)) * sd[:, None]
