@@ -266,10 +266,11 @@ int32_t revsim_rdf_loss_grad_noalloc(const double *d_x, int32_t n_mol, double bo
                                      const revsim_rdf_term *term, const double *d_target,
                                      double *d_loss, double *d_dLdx, void *stream);
 
-/* Instrumentation with no counterpart in the reference: the measured FP32 fused
+/* Instrumentation with no counterpart in the reference: the measured FP32 / FP64 fused
  * multiply-add throughput (TFLOP/s, 2 flops per FMA) of a device, the roofline
- * denominator of the FP32-pipe-bound step kernels. */
+ * denominators of the FP32-pipe-bound step kernels and of the FP64 gas-in-water kernels. */
 int32_t revsim_probe_fp32_tflops(int32_t device, double *tflops);
+int32_t revsim_probe_fp64_tflops(int32_t device, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,559 @@
+// gas_kernels.cu -- kernels of the gas-in-water engine (diffusion/diffusion.jl): neighbour
+// rows, the fused forward and reverse step kernels, the energy and the small helpers.
+//
+// Work decomposition: one warp per atom.  The 32 lanes stride over the atom's neighbour row
+// (every other atom within the list cutoff, both directions, ascending index), accumulate the
+// atom's force (and in reverse its VJP and the class sums of the parameter derivatives) in
+// FP64 registers and combine them with a fixed xor butterfly; lane 0 adds the bonded terms of
+// the atom's molecule and runs the atom's integrator update.  Each atom's sums are computed
+// by one warp in a fixed order: no atomics, deterministic results.  Positions for the pair
+// terms come from a double4 gather copy (pos_in) that the step writes into the other buffer
+// (pos_out), so no warp reads a position another warp has already moved.
+#include "gas_internal.h"
+#include "rs_form_energy.cuh"
+#include "rs_step_impl.cuh"
+
+namespace gs {
+
+using namespace rs;
+
+namespace {
+
+__device__ __forceinline__ double kind_mass(int k, double mO, double mH) { return k == 1 ? mH : mO; }
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Radial bond own atom -> partner (displacement d, own to partner): force on the own atom
+// -(F/r) d with F = -k (r - r0), and in reverse the VJP M (w_p - w_o).
+template <bool REV>
+__device__ __forceinline__ void o2_bond(const double d[3], double kb, double r0, const double wo[3],
+                                        const double wp[3], double f[3], double g[3]) {
+    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])),
+                                __dmul_rn(d[2], d[2]));
+    const double r = __dsqrt_rn(r2);
+    const double rinv = __drcp_rn(r);
+    const double F = -__dmul_rn(kb, __dsub_rn(r, r0));
+    const double Fr = __dmul_rn(F, rinv);
+#pragma unroll
+    for (int u = 0; u < 3; u++) f[u] = __fma_rn(-Fr, d[u], f[u]);
+    if (REV) {
+        double e[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) e[u] = __dsub_rn(wp[u], wo[u]);
+        const double s = __dmul_rn(rinv, __fma_rn(d[2], e[2], __fma_rn(d[1], e[1], __dmul_rn(d[0], e[0]))));
+        const double k1 = __dmul_rn(__dmul_rn(__dsub_rn(-kb, Fr), s), rinv);
+#pragma unroll
+        for (int u = 0; u < 3; u++) g[u] = __dsub_rn(g[u], __fma_rn(k1, d[u], __dmul_rn(Fr, e[u])));
+    }
+}
+
+// ------------------------------------------------------------------ neighbour rows
+// Row of atom i: every atom j of another molecule with min-image d^2 <= rc_nl^2 (Molly's
+// per-dimension rule), except water H - gas pairs, which carry no term (no charge on the
+// gas, no pair form on H).  Ascending j by ballot compaction.
+__global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
+    if (i >= a.N) return;
+    const double4 pa = a.pos[i];
+    const int ka = site_kind(i, a.nw3);
+    const int mi = i < a.nw3 ? i / 3 : (a.nw3 / 3) + (i - a.nw3) / 2;
+    int n = 0;
+    int *row = a.rows + (size_t)i * a.cap;
+    for (int base = 0; base < a.N; base += 32) {
+        const int j = base + lane;
+        bool ok = false;
+        if (j < a.N) {
+            const int kb = site_kind(j, a.nw3);
+            const int mj = j < a.nw3 ? j / 3 : (a.nw3 / 3) + (j - a.nw3) / 2;
+            if (mj != mi && !((ka == 1 && kb == 2) || (ka == 2 && kb == 1))) {
+                const double4 pb = a.pos[j];
+                const double d0 = vec1d(pa.x, pb.x, a.L), d1 = vec1d(pa.y, pb.y, a.L),
+                             d2 = vec1d(pa.z, pb.z, a.L);
+                const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                            __dmul_rn(d2, d2));
+                ok = r2 <= a.rc_nl2;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const int k = n + __popc(m & ((1u << lane) - 1u));
+            if (k < a.cap) row[k] = j;
+        }
+        n += __popc(m);
+    }
+    if (lane == 0) {
+        a.cnt[i] = min(n, a.cap);
+        if (n > a.cap) atomicOr(a.status, ST_NLIST_OVERFLOW);
+    }
+}
+
+// ------------------------------------------------------------------ step kernels
+template <int FORM, bool REV>
+__global__ void __launch_bounds__(kThreads) k_gas_step(const GasConsts k, const GasArgs a) {
+    constexpr int NP = FormInfo<FORM>::NP;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
+    if (i >= a.N) return;   // whole warps only
+    const int ka = site_kind(i, a.nw3);
+    const double ma = kind_mass(ka, a.mO, a.mH);
+    const double4 pa = a.pos_in[i];
+    double4 wa = make_double4(0.0, 0.0, 0.0, 0.0);
+    double ca[3] = {0.0, 0.0, 0.0};
+    if (REV) {
+        wa = a.wgt_in[i];
+        const double cf = __ddiv_rn(__dmul_rn(a.dt, a.dt), __dmul_rn(2.0, ma));
+#pragma unroll
+        for (int u = 0; u < 3; u++)
+            ca[u] = a.acoef_in ? a.acoef_in[3 * (size_t)i + u] : __dmul_rn(a.A[3 * (size_t)i + u], cf);
+    }
+    double f[3] = {0.0, 0.0, 0.0}, g[3] = {0.0, 0.0, 0.0};
+    double acc[3][NP];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int q = 0; q < NP; q++) acc[c][q] = 0.0;
+    double thq = 0.0;
+    const int n = a.cnt[i];
+    const int *row = a.rows + (size_t)i * a.cap;
+    for (int e = lane; e < n; e += 32) {
+        const int j = row[e];
+        const double4 pb = a.pos_in[j];
+        const double dx = vec_mi(pa.x, pb.x, a.L, a.invL);
+        const double dy = vec_mi(pa.y, pb.y, a.L, a.invL);
+        const double dz = vec_mi(pa.z, pb.z, a.L, a.invL);
+        const double r2 = __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+        if (!(r2 <= k.rc2)) continue;
+        const int kb = site_kind(j, a.nw3);
+        const double rinv = xrsqrt(r2);
+        const double r = __dmul_rn(r2, rinv);
+        const double invr2 = __dmul_rn(rinv, rinv);
+        double F = 0.0, dF = 0.0, Fc = 0.0;
+        const bool coul = ka != 2 && kb != 2;
+        if (coul) {
+            const double qq = k.qq[(ka == 1) + (kb == 1)];
+            Fc = __dmul_rn(qq, __dsub_rn(invr2, __dmul_rn(k.krf2, r)));
+            F = Fc;
+            if (REV) dF = -__dmul_rn(__dadd_rn(qq, qq), __dadd_rn(__dmul_rn(invr2, rinv), k.krf));
+        }
+        double gf[4] = {0.0, 0.0, 0.0, 0.0};
+        int cls = -1;
+        if (ka != 1 && kb != 1) {
+            cls = (ka == 2) + (kb == 2);
+            if (k.on[cls]) {
+                double Ff, dFf = 0.0;
+                pair_form<double, FORM, REV>(k.fc[cls], r, rinv, invr2, Ff, dFf, gf);
+                F = __dadd_rn(F, Ff);
+                if (REV) dF = __dadd_rn(dF, dFf);
+            } else {
+                cls = -1;
+            }
+        }
+        const double Fr = __dmul_rn(F, rinv);
+        f[0] = __fma_rn(-Fr, dx, f[0]);
+        f[1] = __fma_rn(-Fr, dy, f[1]);
+        f[2] = __fma_rn(-Fr, dz, f[2]);
+        if (REV) {
+            const double4 wb = a.wgt_in[j];
+            const double ex = __dsub_rn(wb.x, wa.x), ey = __dsub_rn(wb.y, wa.y),
+                         ez = __dsub_rn(wb.z, wa.z);
+            const double s = __dmul_rn(rinv, __fma_rn(dz, ez, __fma_rn(dy, ey, __dmul_rn(dx, ex))));
+            const double k1 = __dmul_rn(__dmul_rn(__dsub_rn(dF, Fr), s), rinv);
+            g[0] = __dsub_rn(g[0], __fma_rn(k1, dx, __dmul_rn(Fr, ex)));
+            g[1] = __dsub_rn(g[1], __fma_rn(k1, dy, __dmul_rn(Fr, ey)));
+            g[2] = __dsub_rn(g[2], __fma_rn(k1, dz, __dmul_rn(Fr, ez)));
+            const double na = __dmul_rn(rinv, __fma_rn(dz, ca[2], __fma_rn(dy, ca[1], __dmul_rn(dx, ca[0]))));
+            if (coul) thq = __fma_rn(-__dmul_rn(Fc, k.twoinvq), na, thq);
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                if (c == cls)
+#pragma unroll
+                    for (int q = 0; q < NP; q++) acc[c][q] = __fma_rn(-gf[q], na, acc[c][q]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        f[u] = wsum(f[u]);
+        if (REV) g[u] = wsum(g[u]);
+    }
+    if (REV) {
+        thq = wsum(thq);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int q = 0; q < NP; q++) acc[c][q] = wsum(acc[c][q]);
+    }
+    if (lane != 0) return;
+
+    // bonded terms of the atom's molecule (diffusion.jl:997-1050, 1367-1498)
+    if (ka != 2) {
+        const int m0 = i - i % 3, kk = i % 3;
+        double xm[9], w9[9], ac9[9], Fb[9], Gb[9], tb[4];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const double4 p = a.pos_in[m0 + q];
+            xm[3 * q] = p.x;
+            xm[3 * q + 1] = p.y;
+            xm[3 * q + 2] = p.z;
+            double4 w = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (REV) w = a.wgt_in[m0 + q];
+            w9[3 * q] = w.x;
+            w9[3 * q + 1] = w.y;
+            w9[3 * q + 2] = w.z;
+            ac9[3 * q] = ac9[3 * q + 1] = ac9[3 * q + 2] = 0.0;
+        }
+        bonded<double, REV>(xm, a.L, a.bw, w9, ac9, Fb, Gb, tb);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            f[u] = __dadd_rn(f[u], Fb[3 * kk + u]);
+            if (REV) g[u] = __dadd_rn(g[u], Gb[3 * kk + u]);
+        }
+    } else {
+        const int p = ((i - a.nw3) ^ 1) + a.nw3;
+        const double4 pp = a.pos_in[p];
+        const double d[3] = {vec1d(pa.x, pp.x, a.L), vec1d(pa.y, pp.y, a.L), vec1d(pa.z, pp.z, a.L)};
+        double wo[3] = {0.0, 0.0, 0.0}, wp[3] = {0.0, 0.0, 0.0};
+        if (REV) {
+            const double4 w = a.wgt_in[p];
+            wo[0] = wa.x; wo[1] = wa.y; wo[2] = wa.z;
+            wp[0] = w.x; wp[1] = w.y; wp[2] = w.z;
+        }
+        o2_bond<REV>(d, a.kb_g, a.r0_g, wo, wp, f, g);
+    }
+    if (!isfinite(f[0]) || !isfinite(f[1]) || !isfinite(f[2])) atomicOr(a.status, ST_NAN);
+
+    if (REV) {
+        double th[kMaxP];
+#pragma unroll
+        for (int p = 0; p < kMaxP; p++) th[p] = 0.0;
+#pragma unroll
+        for (int q = 0; q < NP; q++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                th[k.iw[q]] = __fma_rn(k.fw[c][q], acc[c][q], th[k.iw[q]]);
+                if (k.ig[q] >= 0) th[k.ig[q]] = __fma_rn(k.fg[c][q], acc[c][q], th[k.ig[q]]);
+            }
+        th[k.iq] = __dadd_rn(th[k.iq], thq);
+        double *pt = a.part + (size_t)i * k.P;
+        for (int p = 0; p < k.P; p++) pt[p] = __dadd_rn(pt[p], th[p]);
+    }
+    const size_t b = 3 * (size_t)i;
+    if (a.mode & MODE_FORCES_ONLY) {
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            a.F_out[b + u] = f[u];
+            if (REV) a.G[b + u] = g[u];
+        }
+        return;
+    }
+    const double sd = ka == 1 ? a.sdH : a.sdO;
+    if (!REV) {
+        // B-A-O-A (diffusion.jl:1228-1233)
+        double xi[3] = {0.0, 0.0, 0.0};
+        if (a.s != 0.0) atom_noise(a.seed_cur, (uint32_t)i, sd, xi);
+        double xn[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            double v = a.v[b + u], x = a.x[b + u];
+            v = __dadd_rn(v, __ddiv_rn(__dmul_rn(f[u], a.dt), ma));
+            x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
+            x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            x = wrap1d(x, a.L);
+            a.v[b + u] = v;
+            a.x[b + u] = x;
+            xn[u] = x;
+        }
+        a.pos_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
+        return;
+    }
+    // reverse part 2 (diffusion.jl:1580-1586) and, fused, part 1 of the next step (1566-1572)
+    const double dt2 = __dmul_rn(a.dt, a.dt);
+    const bool fuse = (a.mode & MODE_FUSE_NEXT) != 0;
+    double xi[3] = {0.0, 0.0, 0.0};
+    if (fuse && a.s != 0.0) atom_noise(a.seed_next, (uint32_t)i, sd, xi);
+    double xn[3], Cm[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const size_t e = b + u;
+        a.G[e] = g[u];
+        double v = __dsub_rn(a.v[e], __ddiv_rn(__dmul_rn(f[u], a.dt), ma));
+        const double B = __dadd_rn(__dmul_rn(a.c, a.B[e]), __dmul_rn(dt2, g[u]));
+        a.B[e] = B;
+        a.A[e] = __dadd_rn(a.A[e], B);
+        if (fuse) {
+            double x = a.x[e];
+            x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
+            x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            x = wrap1d(x, a.L);
+            const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
+                                       __ddiv_rn(__dmul_rn(__dmul_rn(dt2, g[u]), __dadd_rn(1.0, a.c)), 2.0));
+            const double C = __dadd_rn(a.C[e], D);
+            a.D[e] = D;
+            a.C[e] = C;
+            a.x[e] = x;
+            xn[u] = x;
+            Cm[u] = __ddiv_rn(C, ma);
+        }
+        a.v[e] = v;
+    }
+    if (fuse) {
+        a.pos_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
+        a.wgt_out[i] = make_double4(Cm[0], Cm[1], Cm[2], 0.0);
+    }
+}
+
+__global__ void k_gas_part1(const GasArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.N) return;
+    const int ka = site_kind(i, a.nw3);
+    const double ma = kind_mass(ka, a.mO, a.mH);
+    const double dt2 = __dmul_rn(a.dt, a.dt);
+    double xi[3] = {0.0, 0.0, 0.0};
+    if (a.s != 0.0) atom_noise(a.seed_next, (uint32_t)i, ka == 1 ? a.sdH : a.sdO, xi);
+    double xn[3], Cm[3];
+    const size_t b = 3 * (size_t)i;
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const size_t e = b + u;
+        double v = a.v[e], x = a.x[e];
+        x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+        v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
+        x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+        x = wrap1d(x, a.L);
+        const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
+                                   __ddiv_rn(__dmul_rn(__dmul_rn(dt2, a.G[e]), __dadd_rn(1.0, a.c)), 2.0));
+        const double C = __dadd_rn(a.C[e], D);
+        a.D[e] = D;
+        a.C[e] = C;
+        a.x[e] = x;
+        a.v[e] = v;
+        xn[u] = x;
+        Cm[u] = __ddiv_rn(C, ma);
+    }
+    a.pos_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
+    a.wgt_out[i] = make_double4(Cm[0], Cm[1], Cm[2], 0.0);
+}
+
+__global__ void k_gas_pack(int N, const double *x, double4 *pos) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    pos[i] = make_double4(x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2], 0.0);
+}
+
+__global__ void k_gas_pack_w(int N, int nw3, const double *w, double mO, double mH, double4 *wgt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double m = site_kind(i, nw3) == 1 ? mH : mO;
+    const size_t b = 3 * (size_t)i;
+    wgt[i] = make_double4(__ddiv_rn(w[b], m), __ddiv_rn(w[b + 1], m), __ddiv_rn(w[b + 2], m), 0.0);
+}
+
+__global__ void k_gas_reset(int n3, const double *g, double f1, double f2, double f3, double *A,
+                            double *B, double *C, double *D, double *G) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n3) return;
+    const double ge = g[e];
+    const double a = __dmul_rn(ge, f1);
+    A[e] = a;
+    B[e] = a;
+    C[e] = 0.0;
+    D[e] = __ddiv_rn(__dmul_rn(ge, f2), f3);
+    G[e] = 0.0;
+}
+
+__global__ void k_gas_axpy(int n, double k, const double *x, double *y) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) y[e] = __fma_rn(k, x[e], y[e]);
+}
+
+// ------------------------------------------------------------------ energy
+template <int FORM>
+__global__ void __launch_bounds__(kThreads) k_gas_energy(const GasConsts k, const GasArgs a,
+                                                         double *epart) {
+    constexpr int NP = FormInfo<FORM>::NP;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
+    if (i >= a.N) return;
+    const int ka = site_kind(i, a.nw3);
+    const double4 pa = a.pos_in[i];
+    double E = 0.0, eq = 0.0;
+    double acc[3][NP];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int q = 0; q < NP; q++) acc[c][q] = 0.0;
+    const int n = a.cnt[i];
+    const int *row = a.rows + (size_t)i * a.cap;
+    for (int e = lane; e < n; e += 32) {
+        const int j = row[e];
+        if (j <= i) continue;
+        const double4 pb = a.pos_in[j];
+        const double d0 = vec1d(pa.x, pb.x, a.L), d1 = vec1d(pa.y, pb.y, a.L), d2 = vec1d(pa.z, pb.z, a.L);
+        const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+        if (!(r2 <= k.rc2)) continue;
+        const double r = sqrt(r2);
+        const int kb = site_kind(j, a.nw3);
+        if (ka != 2 && kb != 2) {
+            // Molly CoulombReactionField energy; dE/dq_O = 2 E_c / q_O
+            const double Ec = k.qq[(ka == 1) + (kb == 1)] * (1.0 / r + k.krf * r2 - k.crf_shift);
+            E += Ec;
+            eq += Ec * k.twoinvq;
+        }
+        if (ka != 1 && kb != 1) {
+            const int cls = (ka == 2) + (kb == 2);
+            if (k.on[cls]) {
+                const DualN<double, 4> Ef = form_energy<FORM>(k.fc[cls].p, r);
+                E += Ef.v;
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    if (c == cls)
+#pragma unroll
+                        for (int q = 0; q < NP; q++) acc[c][q] += Ef.d[q];
+            }
+        }
+    }
+    E = wsum(E);
+    eq = wsum(eq);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int q = 0; q < NP; q++) acc[c][q] = wsum(acc[c][q]);
+    if (lane != 0) return;
+    // bonded terms on the molecule's first atom
+    if (ka == 0) {
+        double x[9];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const double4 p = a.pos_in[i + q];
+            x[3 * q] = p.x;
+            x[3 * q + 1] = p.y;
+            x[3 * q + 2] = p.z;
+        }
+        double dd[2][3];
+        for (int h = 1; h <= 2; h++) {
+            for (int u = 0; u < 3; u++) dd[h - 1][u] = vec1d(x[u], x[3 * h + u], a.L);
+            const double bl = sqrt(dd[h - 1][0] * dd[h - 1][0] + dd[h - 1][1] * dd[h - 1][1] +
+                                   dd[h - 1][2] * dd[h - 1][2]) - a.bw.r0;
+            E += 0.5 * a.bw.kb * bl * bl;
+        }
+        const double *u1 = dd[0], *u2 = dd[1];
+        const double cth = (u1[0] * u2[0] + u1[1] * u2[1] + u1[2] * u2[2]) /
+                           (sqrt(u1[0] * u1[0] + u1[1] * u1[1] + u1[2] * u1[2]) *
+                            sqrt(u2[0] * u2[0] + u2[1] * u2[1] + u2[2] * u2[2]));
+        const double th = acos(cth) - a.bw.th0;
+        E += 0.5 * a.bw.ka * th * th;
+    } else if (ka == 2 && ((i - a.nw3) & 1) == 0) {
+        const double4 pp = a.pos_in[i + 1];
+        const double d0 = vec1d(pa.x, pp.x, a.L), d1 = vec1d(pa.y, pp.y, a.L), d2 = vec1d(pa.z, pp.z, a.L);
+        const double bl = sqrt(d0 * d0 + d1 * d1 + d2 * d2) - a.r0_g;
+        E += 0.5 * a.kb_g * bl * bl;
+    }
+    double th[kMaxP];
+#pragma unroll
+    for (int p = 0; p < kMaxP; p++) th[p] = 0.0;
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            th[k.iw[q]] += k.fw[c][q] * acc[c][q];
+            if (k.ig[q] >= 0) th[k.ig[q]] += k.fg[c][q] * acc[c][q];
+        }
+    th[k.iq] += eq;
+    double *out = epart + (size_t)i * (k.P + 1);
+    out[0] = E;
+    for (int p = 0; p < k.P; p++) out[1 + p] = th[p];
+}
+
+// Single CTA: out[q] = scale * sum over atoms (strided per thread, then a fixed tree).
+__global__ void __launch_bounds__(256) k_gas_esum(int N, int P, const double *epart, double e_scale,
+                                                  double g_scale, int accumulate, double *out) {
+    __shared__ double sh[256];
+    for (int q = 0; q <= P; q++) {
+        double s = 0.0;
+        for (int a = threadIdx.x; a < N; a += 256) s += epart[(size_t)a * (P + 1) + q];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const double v = sh[0] * (q == 0 ? e_scale : g_scale);
+            out[q] = accumulate ? out[q] + v : v;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool REV>
+void step_form(int form, const GasConsts &k, const GasArgs &a, dim3 grid, cudaStream_t st) {
+    switch (form) {
+        case F_LJ: k_gas_step<F_LJ, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_DEXP: k_gas_step<F_DEXP, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_BUCK: k_gas_step<F_BUCK, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_LJSC: k_gas_step<F_LJSC, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_BUFF: k_gas_step<F_BUFF, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+    }
+}
+
+}  // namespace
+
+void launch_gas_rows(const GasRowArgs &a, cudaStream_t st) {
+    const int grid = (a.N + kWarpsPerCta - 1) / kWarpsPerCta;
+    k_gas_rows<<<grid, kThreads, 0, st>>>(a);
+}
+
+void launch_gas_step(int form, bool rev, const GasConsts &k, const GasArgs &a, cudaStream_t st) {
+    const dim3 grid((a.N + kWarpsPerCta - 1) / kWarpsPerCta);
+    if (rev)
+        step_form<true>(form, k, a, grid, st);
+    else
+        step_form<false>(form, k, a, grid, st);
+}
+
+void launch_gas_part1(const GasArgs &a, cudaStream_t st) {
+    k_gas_part1<<<(a.N + 127) / 128, 128, 0, st>>>(a);
+}
+
+void launch_gas_pack(int N, const double *x, double4 *pos, cudaStream_t st) {
+    k_gas_pack<<<(N + 127) / 128, 128, 0, st>>>(N, x, pos);
+}
+
+void launch_gas_pack_w(int N, int nw3, const double *w, double mO, double mH, double4 *wgt,
+                       cudaStream_t st) {
+    k_gas_pack_w<<<(N + 127) / 128, 128, 0, st>>>(N, nw3, w, mO, mH, wgt);
+}
+
+void launch_gas_reset(int n3, const double *g, double f1, double f2, double f3, double *A,
+                      double *B, double *C, double *D, double *G, cudaStream_t st) {
+    k_gas_reset<<<(n3 + 255) / 256, 256, 0, st>>>(n3, g, f1, f2, f3, A, B, C, D, G);
+}
+
+void launch_gas_axpy(int n, double k, const double *x, double *y, cudaStream_t st) {
+    k_gas_axpy<<<(n + 255) / 256, 256, 0, st>>>(n, k, x, y);
+}
+
+void launch_gas_energy(int form, const GasConsts &k, const GasArgs &a, double *epart,
+                       cudaStream_t st) {
+    const dim3 grid((a.N + kWarpsPerCta - 1) / kWarpsPerCta);
+    switch (form) {
+        case F_LJ: k_gas_energy<F_LJ><<<grid, kThreads, 0, st>>>(k, a, epart); break;
+        case F_DEXP: k_gas_energy<F_DEXP><<<grid, kThreads, 0, st>>>(k, a, epart); break;
+        case F_BUCK: k_gas_energy<F_BUCK><<<grid, kThreads, 0, st>>>(k, a, epart); break;
+        case F_LJSC: k_gas_energy<F_LJSC><<<grid, kThreads, 0, st>>>(k, a, epart); break;
+        case F_BUFF: k_gas_energy<F_BUFF><<<grid, kThreads, 0, st>>>(k, a, epart); break;
+    }
+}
+
+void launch_gas_esum(int N, int P, const double *epart, double e_scale, double g_scale,
+                     bool accumulate, double *out, cudaStream_t st) {
+    k_gas_esum<<<1, 256, 0, st>>>(N, P, epart, e_scale, g_scale, accumulate ? 1 : 0, out);
+}
+
+}  // namespace gs

@@ -168,23 +168,19 @@ void dfree(void *p) {
     if (p) cudaFree(p);
 }
 
+}  // namespace
+
+namespace rs {
+
+// Constants of one pair form for the per-pair parameters t[0..nfp-1] (the water engine's
+// O-O parameters, or the gas engine's mixed parameters of one site class).
 template <typename R>
-NbConsts<R> nb_consts(const revsim_handle *h) {
-    const double *t = h->theta.data();
-    const int nfp = h->NFp;
-    const double qO = t[nfp], qH = -qO / 2;
-    NbConsts<R> nb;
-    nb.qq[0] = (R)(h->ke * qO * qO);
-    nb.qq[1] = (R)(h->ke * qO * qH);
-    nb.qq[2] = (R)(h->ke * qH * qH);
-    nb.krf = (R)h->krf;
-    nb.krf2 = (R)(2 * h->krf);
-    nb.rc2 = (R)(h->rc * h->rc);
-    nb.twoinvq = (R)(2.0 / qO);
-    FormConsts<R> &fc = nb.fc;
+FormConsts<R> form_consts(int form, const double *t, int nfp) {
+    FormConsts<R> fc;
     for (int i = 0; i < 4; i++) fc.p[i] = (R)(i < nfp ? t[i] : 0.0);
     for (int i = 0; i < 8; i++) fc.c[i] = (R)0;
-    switch (h->form) {
+    fc.on = 0;
+    switch (form) {
         case REVSIM_LJ: {
             const double s = t[0], e = t[1];
             fc.on = e != 0.0;
@@ -235,6 +231,30 @@ NbConsts<R> nb_consts(const revsim_handle *h) {
             break;
         }
     }
+    return fc;
+}
+
+template FormConsts<float> form_consts<float>(int, const double *, int);
+template FormConsts<double> form_consts<double>(int, const double *, int);
+
+}  // namespace rs
+
+namespace {
+
+template <typename R>
+NbConsts<R> nb_consts(const revsim_handle *h) {
+    const double *t = h->theta.data();
+    const int nfp = h->NFp;
+    const double qO = t[nfp], qH = -qO / 2;
+    NbConsts<R> nb;
+    nb.qq[0] = (R)(h->ke * qO * qO);
+    nb.qq[1] = (R)(h->ke * qO * qH);
+    nb.qq[2] = (R)(h->ke * qH * qH);
+    nb.krf = (R)h->krf;
+    nb.krf2 = (R)(2 * h->krf);
+    nb.rc2 = (R)(h->rc * h->rc);
+    nb.twoinvq = (R)(2.0 / qO);
+    nb.fc = form_consts<R>(h->form, t, nfp);
     nb.mlp_tab = h->d_mlp_tab;
     nb.mlp_adj = h->d_mlp_adj;
     nb.mlp_hinv = (R)(MLP_NG / h->rc);

@@ -36,6 +36,10 @@ struct NbConsts {
     R mlp_hinv;
 };
 
+// Constants of one pair form for the per-pair parameters t[0..nfp-1] (rs_api.cu).
+template <typename R>
+FormConsts<R> form_consts(int form, const double *t, int nfp);
+
 struct BondConsts {
     double kb, r0, ka, th0;
 };

@@ -35,7 +35,7 @@ EXPORTS = [
     "revsim_set_launch_shape", "revsim_get_launch_shape", "revsim_autotune",
     "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc", "revsim_energy_grad",
     "revsim_set_enth_vap", "revsim_loss_parts", "revsim_loss_and_grads", "revsim_set_barostat",
-    "revsim_barostat_state", "revsim_set_box",
+    "revsim_barostat_state", "revsim_set_box", "revsim_probe_fp64_tflops",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -46,6 +46,16 @@ SW_EXPORTS = [
     "revsim_sw_active_pairs", "revsim_sw_forward", "revsim_sw_reverse", "revsim_sw_stream",
     "revsim_sw_launch_count", "revsim_sw_set_kernel_timing", "revsim_sw_kernel_time",
     "revsim_sw_set_lanes",
+]
+
+
+# Every symbol include/revsim_gas.h declares.
+GAS_EXPORTS = [
+    "revsim_gas_create", "revsim_gas_destroy", "revsim_gas_last_error", "revsim_gas_n_params",
+    "revsim_gas_set_params", "revsim_gas_set_state", "revsim_gas_get_state", "revsim_gas_forces",
+    "revsim_gas_force_vjp", "revsim_gas_energy", "revsim_gas_forward", "revsim_gas_reverse",
+    "revsim_gas_stream", "revsim_gas_launch_count", "revsim_gas_set_kernel_timing",
+    "revsim_gas_kernel_time",
 ]
 
 
@@ -102,6 +112,18 @@ class SwDesc(ctypes.Structure):
         ("n_steps_nf", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("mlp", ctypes.c_int32),
+    ]
+
+
+class GasDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_water", ctypes.c_int32), ("n_gas", ctypes.c_int32), ("box", ctypes.c_double),
+        ("inter_type", ctypes.c_int32), ("temp", ctypes.c_double), ("m_O", ctypes.c_double),
+        ("m_H", ctypes.c_double), ("coulomb_const", ctypes.c_double), ("cutoff", ctypes.c_double),
+        ("nl_cutoff", ctypes.c_double), ("n_steps_nf", ctypes.c_int32), ("kB", ctypes.c_double),
+        ("kb_w", ctypes.c_double), ("r0_w", ctypes.c_double), ("ka_w", ctypes.c_double),
+        ("th0_w", ctypes.c_double), ("kb_g", ctypes.c_double), ("r0_g", ctypes.c_double),
+        ("n_mol_ev", ctypes.c_int32), ("device", ctypes.c_int32),
     ]
 
 
@@ -167,6 +189,7 @@ def load(path=LIB_PATH):
         "revsim_get_launch_shape": (i32, [vp, i32, pi32, pi32, pi32]),
         "revsim_autotune": (i32, [vp, d]),
         "revsim_probe_fp32_tflops": (i32, [i32, pd]),
+        "revsim_probe_fp64_tflops": (i32, [i32, pd]),
         "revsim_rdf_loss_grad_noalloc": (i32, [vp, i32, d, P(RdfTermC), vp, vp, vp, vp]),
         "revsim_sw_create": (i32, [P(SwDesc), P(vp)]),
         "revsim_sw_destroy": (None, [vp]),
@@ -188,6 +211,22 @@ def load(path=LIB_PATH):
         "revsim_sw_set_kernel_timing": (i32, [vp, i32]),
         "revsim_sw_kernel_time": (i32, [vp, i32, pd, pi64]),
         "revsim_sw_set_lanes": (i32, [vp, i32]),
+        "revsim_gas_create": (i32, [P(GasDesc), P(vp)]),
+        "revsim_gas_destroy": (i32, [vp]),
+        "revsim_gas_last_error": (ctypes.c_char_p, [vp]),
+        "revsim_gas_n_params": (i32, [i32]),
+        "revsim_gas_set_params": (i32, [vp, pd, i32]),
+        "revsim_gas_set_state": (i32, [vp, pd, pd]),
+        "revsim_gas_get_state": (i32, [vp, pd, pd]),
+        "revsim_gas_forces": (i32, [vp, pd]),
+        "revsim_gas_force_vjp": (i32, [vp, pd, pd, pd, pd, pd]),
+        "revsim_gas_energy": (i32, [vp, pd, pd]),
+        "revsim_gas_forward": (i32, [vp, pu64, d, i32, i32, d, i32, i32, pd, pd, pd]),
+        "revsim_gas_reverse": (i32, [vp, pu64, d, i32, i32, i32, d, i32, pd, pd, pd]),
+        "revsim_gas_stream": (vp, [vp]),
+        "revsim_gas_launch_count": (i64, [vp]),
+        "revsim_gas_set_kernel_timing": (i32, [vp, i32]),
+        "revsim_gas_kernel_time": (i32, [vp, i32, pd, pi64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

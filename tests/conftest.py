@@ -37,6 +37,22 @@ def relaxed_water(n_mol, box, seed=0, steps=100, inter_type="lj"):
     return x, v
 
 
+def relaxed_gas(n_water, n_gas, box, inter_type="lj", seed=0, steps=60):
+    """A seeded gas-in-water box relaxed by the oracle with Langevin steps (gamma = 1/ps):
+    (oracle system, default parameters, x, v)."""
+    from oracle import orc
+    from revsim import constants as C, systems
+
+    s = orc.make_gas_system(n_water, n_gas, box, inter_type)
+    x = systems.gas_water_coords(n_water, n_gas, box, seed=seed)
+    v = systems.gas_water_velocities(n_water, n_gas, seed=seed + 1)
+    p = np.array(C.gas_default_params(inter_type))
+    if steps:
+        x, v, *_ = orc.gas_forward_sim(s, p, x, v, systems.noise_seeds(steps, seed=seed + 7), 1.0,
+                                       steps, steps, 0.001, calc_loss=False)
+    return s, p, x, v
+
+
 @pytest.fixture(scope="session")
 def small_water():
     """150 molecules in a 2.6 nm box (low density keeps the oracle fast), relaxed."""

@@ -12,6 +12,7 @@ from conftest import PKG, ROOT
 
 HEADER = os.path.join(ROOT, "include", "revsim.h")
 SW_HEADER = os.path.join(ROOT, "include", "revsim_sw.h")
+GAS_HEADER = os.path.join(ROOT, "include", "revsim_gas.h")
 
 
 def declared_symbols(header=HEADER):
@@ -35,14 +36,16 @@ def test_header_declares_entry_points():
 
 
 def test_library_exports_every_declared_symbol(lib):
-    missing = [s for s in declared_symbols() + declared_symbols(SW_HEADER) if not hasattr(lib, s)]
+    missing = [s for s in declared_symbols() + declared_symbols(SW_HEADER) + declared_symbols(GAS_HEADER)
+               if not hasattr(lib, s)]
     assert not missing, missing
 
 
 def test_python_binding_covers_every_symbol():
-    from revsim import EXPORTS, SW_EXPORTS
+    from revsim import EXPORTS, GAS_EXPORTS, SW_EXPORTS
     assert sorted(EXPORTS) == declared_symbols()
     assert sorted(SW_EXPORTS) == declared_symbols(SW_HEADER)
+    assert sorted(GAS_EXPORTS) == declared_symbols(GAS_HEADER)
 
 
 def test_error_paths_without_device(lib):
@@ -98,3 +101,25 @@ def test_descriptor_validation_before_any_device_call(lib):
     desc.mlp = 1
     desc.inter_type = 2                           # the learned term needs REVSIM_LJ
     assert L.revsim_create(ctypes.byref(desc), ctypes.byref(h)) == -1
+
+
+def test_gas_entry_points_without_device(lib):
+    """Argument checks of the gas-in-water ABI happen before any CUDA call."""
+    from revsim import _lib
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    assert L.revsim_gas_create(None, ctypes.byref(h)) == -1
+    d = _lib.GasDesc()
+    d.n_water, d.n_gas, d.box, d.inter_type = 10, 2, 2.0, 0    # box < 2 x 1.2 nm
+    assert L.revsim_gas_create(ctypes.byref(d), ctypes.byref(h)) == -6 and not h.value
+    d.box, d.inter_type = 3.0, 9
+    assert L.revsim_gas_create(ctypes.byref(d), ctypes.byref(h)) == -1
+    d.inter_type, d.n_water, d.n_gas = 0, 0, 0
+    assert L.revsim_gas_create(ctypes.byref(d), ctypes.byref(h)) == -1
+    assert [L.revsim_gas_n_params(t) for t in range(5)] == [5, 7, 7, 7, 7]
+    assert L.revsim_gas_n_params(5) == -1
+    assert L.revsim_gas_set_params(None, None, 0) == -1
+    assert L.revsim_gas_forward(None, None, 0.0, 0, 1, 0.001, 1, 1, None, None, None) == -1
+    assert L.revsim_gas_reverse(None, None, 0.0, 0, 1, 1, 0.001, 1, None, None, None) == -1
+    assert L.revsim_gas_last_error(None) == b"null handle"
+    assert L.revsim_gas_destroy(None) == 0

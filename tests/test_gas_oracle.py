@@ -5,21 +5,11 @@ loss (the reference's own checks, diffusion.jl:1659-1677)."""
 import numpy as np
 import pytest
 
+from conftest import relaxed_gas
 from oracle import orc
-from revsim import constants as C, systems
+from revsim import systems
 
 FORMS = ["lj", "dexp", "buck", "ljsc", "buff"]
-
-
-def relaxed_gas(n_water, n_gas, box, inter_type="lj", seed=0, steps=60):
-    s = orc.make_gas_system(n_water, n_gas, box, inter_type)
-    x = systems.gas_water_coords(n_water, n_gas, box, seed=seed)
-    v = systems.gas_water_velocities(n_water, n_gas, seed=seed + 1)
-    p = np.array(C.gas_default_params(inter_type))
-    if steps:
-        x, v, *_ = orc.gas_forward_sim(s, p, x, v, systems.noise_seeds(steps, seed=seed + 7), 1.0,
-                                       steps, steps, 0.001, calc_loss=False)
-    return s, p, x, v
 
 
 @pytest.fixture(scope="module")
