@@ -68,13 +68,22 @@ def parse():
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
     ap.add_argument("--n-replicas", type=int, default=64, help="replicas workload: boxes")
     ap.add_argument("--rep-steps", type=int, default=2000, help="replicas workload: steps")
-    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas", "equil", "reweight"],
+    ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas", "equil", "reweight",
+                             "diffusion"],
                     help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
                          "carbon, 16 replicas of 8,000 atoms; mlp: 895 waters with the learned "
                          "pair correction, gradient throughput and a training comparison; "
                          "replicas: 64 water boxes of 300-3,000 molecules at 280-320 K in one launch; "
                          "equil: barostatted forward equilibration of the water box; "
-                         "reweight: the reweighting gradient estimator on the water box")
+                         "reweight: the reweighting gradient estimator on the water box; "
+                         "diffusion: O2 in water, the diffusion-coefficient gradient")
+    ap.add_argument("--gas-water", type=int, default=885, help="diffusion: waters")
+    ap.add_argument("--gas-n", type=int, default=10, help="diffusion: O2 molecules")
+    ap.add_argument("--gas-box", type=float, default=3.0)
+    ap.add_argument("--gas-steps", type=int, default=50000)
+    ap.add_argument("--gas-steps-loss", type=int, default=500)
+    ap.add_argument("--gas-trunc", type=int, default=200)
+    ap.add_argument("--gas-loss", default="diff_ev", choices=["diff", "diff_ev"])
     ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
@@ -823,6 +832,226 @@ def run_ours_reweight(a):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------ diffusion workload
+DIFF_METRIC = "gas-in-water gradient atom-steps/s (forward steps of forward + truncated reverse)"
+
+
+def diffusion_config(a, extra=None):
+    c = {"workload": (f"gas_{a.gas_water}w+{a.gas_n}O2_{a.gas_box:g}nm_{a.form}_fp64_"
+                      f"{a.gas_steps}fwd_loss{a.gas_steps_loss}_trunc{a.gas_trunc}_{a.gas_loss}"),
+         "n_atoms": 3 * a.gas_water + 2 * a.gas_n, "n_water": a.gas_water, "n_gas": a.gas_n,
+         "box_nm": a.gas_box, "n_steps": a.gas_steps, "n_steps_loss": a.gas_steps_loss,
+         "n_steps_trunc": a.gas_trunc,
+         "reverse_steps": (a.gas_steps // a.gas_steps_loss) * min(a.gas_trunc, a.gas_steps_loss),
+         "dt_ps": 0.001, "gamma_per_ps": 1.0, "pair_form": a.form, "precision": "fp64",
+         "loss": {"diff": "diffusion coefficient of the O2 centres (calculate_D, diffusion.jl:861-911)",
+                  "diff_ev": "diffusion coefficient plus the enthalpy-of-vaporisation term "
+                             "(diffusion.jl:799-815, 861-911)"}[a.gas_loss],
+         "source": "train() of diffusion.jl:1683-1700 (50 ps forward, loss every 500 fs, "
+                   "reverse truncated at 200 steps per loss point)",
+         "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def gas_prepare(a, device):
+    """Seeded gas-in-water box equilibrated on the GPU (a.equil_ps ps of Langevin, gamma 1/ps)."""
+    from revsim import constants as C, systems
+    from revsim.gas import GasEngine
+    x = systems.gas_water_coords(a.gas_water, a.gas_n, a.gas_box, seed=0)
+    v = systems.gas_water_velocities(a.gas_water, a.gas_n, seed=1)
+    p = np.array(C.gas_default_params(a.form))
+    eq = GasEngine(a.gas_water, a.gas_n, a.gas_box, a.form, device=device)
+    eq.set_params(p)
+    eq.set_state(x, v)
+    n = 1000 * a.equil_ps
+    eq.forward(systems.noise_seeds(n, seed=30), 1.0, n, n, 0.001, "diff", calc_loss=False)
+    x0, v0 = eq.get_state()
+    eq.close()
+    return x0, v0, p
+
+
+def gas_count_ipairs(x, a, cutoff=1.0):
+    """Unordered pairs within the cutoff that carry a term (water-water, and pairs of non-H
+    sites), and how many of them carry the pair form."""
+    n = len(x)
+    nw3 = 3 * a.gas_water
+    kind = np.array([(0 if i % 3 == 0 else 1) if i < nw3 else 2 for i in range(n)])
+    mol = np.array([i // 3 if i < nw3 else a.gas_water + (i - nw3) // 2 for i in range(n)])
+    total = form = 0
+    for i0 in range(0, n, 512):
+        d = x[None, :, :] - x[i0:i0 + 512, None, :]
+        d -= a.gas_box * np.round(d / a.gas_box)
+        r2 = (d * d).sum(-1)
+        ii = np.arange(i0, min(i0 + 512, n))[:, None]
+        jj = np.arange(n)[None, :]
+        ki, kj = kind[ii], kind[jj]
+        ok = (jj > ii) & (mol[ii] != mol[jj]) & (r2 <= cutoff * cutoff)
+        coul = (ki != 2) & (kj != 2)
+        pf = (ki != 1) & (kj != 1)
+        total += int((ok & (coul | pf)).sum())
+        form += int((ok & pf).sum())
+    return total, form
+
+
+def gas_cpu_sample(a, x0, v0, p):
+    """The FP64 oracle on a bounded sample: 10 forward steps (two loss points) and the 4
+    reverse steps of a truncation of 2, per-step costs scaled to the workload."""
+    from oracle import orc
+    from revsim import systems
+    s = orc.make_gas_system(a.gas_water, a.gas_n, a.gas_box, a.form)
+    seeds = systems.noise_seeds(10, seed=98)
+    t0 = time.perf_counter()
+    xf, vf, _, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, 10, 5, 0.001, a.gas_loss)
+    t1 = time.perf_counter()
+    orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, 10, 5, 2, 0.001, sx, sv, gc, a.gas_loss)
+    t2 = time.perf_counter()
+    nb = a.gas_steps // a.gas_steps_loss
+    n_rev = nb * min(a.gas_trunc, a.gas_steps_loss)
+    per_grad = (t1 - t0) / 10 * a.gas_steps + (t2 - t1) / 4 * n_rev
+    n_atoms = 3 * a.gas_water + 2 * a.gas_n
+    return n_atoms * a.gas_steps / per_grad, orc.num_threads(), (
+        f"10 forward steps (2 loss points) and 4 reverse steps of the {n_atoms}-atom box, FP64 "
+        f"oracle; per-step costs scaled to {a.gas_steps} forward + {n_rev} reverse steps")
+
+
+def run_reference_diffusion(a):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import orc
+    from revsim import constants as C, systems
+    orc.build()
+    s = orc.make_gas_system(a.gas_water, a.gas_n, a.gas_box, a.form)
+    x = systems.gas_water_coords(a.gas_water, a.gas_n, a.gas_box, seed=0)
+    v = systems.gas_water_velocities(a.gas_water, a.gas_n, seed=1)
+    p = np.array(C.gas_default_params(a.form))
+    x, v, *_ = orc.gas_forward_sim(s, p, x, v, systems.noise_seeds(40, seed=30), 1.0, 40, 40, 0.001,
+                                   "diff", calc_loss=False)
+    vals = []
+    for i in range(a.warmup + a.steps):
+        val, cores, desc = gas_cpu_sample(a, x, v, p)
+        if i >= a.warmup:
+            vals.append(val)
+    value = statistics.mean(vals)
+    n_atoms = 3 * a.gas_water + 2 * a.gas_n
+    out = {"metric": DIFF_METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1e3 * n_atoms * a.gas_steps / value,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "impl": "reference", "config": diffusion_config(a),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours_diffusion(a):
+    """One gradient of the gas-in-water system per step: forward_sim then reverse_sim through
+    the host API, from host arrays, on one GPU per rank (independent replicas)."""
+    import ctypes
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import build as _build
+    _build.build()
+    from revsim import _lib, systems
+    from revsim.gas import GasEngine, forward_sim, reverse_sim
+    x0, v0, p = gas_prepare(a, local)
+    eng = GasEngine(a.gas_water, a.gas_n, a.gas_box, a.form, device=local)
+    seeds = systems.noise_seeds(a.gas_steps, seed=700 + rank)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def run():
+        sys_f, loss_f, acc, _ = forward_sim(x0, v0, seeds, 1.0, a.gas_steps, a.gas_steps_loss, p,
+                                            0.001, 1, a.form, a.gas_loss, engine=eng)
+        out = reverse_sim(sys_f.coords, sys_f.velocities, seeds, 1.0, a.gas_steps, a.gas_steps_loss,
+                          a.gas_trunc, p, 0.001, 1, sys_f.loggers, acc, a.form, a.gas_loss)
+        return loss_f, out
+
+    for _ in range(a.warmup):
+        run()
+    n0 = eng.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            loss_f, out = run()
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1))
+    launches = (eng.launch_count() - n0) // a.steps
+    total = sum(times)
+    if dist is not None:
+        t = torch.tensor([total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    ms = total / a.steps
+    n_atoms = 3 * a.gas_water + 2 * a.gas_n
+    value = world * n_atoms * a.gas_steps / (ms * 1e-3)
+    eng.set_kernel_timing(True)
+    run()
+    rev_ms, rev_n = eng.kernel_time(0)
+    fwd_ms, fwd_n = eng.kernel_time(1)
+    eng.set_kernel_timing(False)
+    ipairs, form_pairs = gas_count_ipairs(x0, a)
+    peak = ctypes.c_double()
+    _lib.load().revsim_probe_fp64_tflops(local, ctypes.byref(peak))
+    fl_fwd = FLOPS_FWD_IPAIR * ipairs + FLOPS_FWD_OO_EXTRA * form_pairs
+    fl_rev = FLOPS_REV_IPAIR * ipairs
+    k_rev, k_fwd = rev_ms / max(rev_n, 1), fwd_ms / max(fwd_n, 1)
+    rev_dominant = rev_ms >= fwd_ms
+    launch_ms = k_rev if rev_dominant else k_fwd
+    flops_launch = fl_rev if rev_dominant else fl_fwd
+    achieved = flops_launch / (launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "kernel": ("k_gas_step<LJ, reverse>" if rev_dominant else "k_gas_step<LJ, forward>"),
+                "launch_ms": launch_ms, "ipairs": ipairs, "pair_form_ipairs": form_pairs,
+                "flops_per_launch": flops_launch,
+                "peak_source": "measured FP64 FMA throughput of this GPU (revsim_probe_fp64_tflops)",
+                "reverse_step_ms": k_rev, "forward_step_ms": k_fwd,
+                "reverse_share": rev_ms / ms, "forward_share": fwd_ms / ms}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        val, cores, desc = gas_cpu_sample(a, x0, v0, p)
+        cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        sys_r, loss_r, dl_dp, D, l_diff, l_rdf, l_ev = out
+        nb = a.gas_steps // a.gas_steps_loss
+        res = {"metric": DIFF_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": diffusion_config(a, {"parallelism": f"replicas{world}" if world > 1 else "single"}),
+               "e2e": {"value": value, "unit": UNIT,
+                       "h2d_bytes_per_step": 2 * 3 * n_atoms * 8 + nb * 6 * a.gas_n * 8,
+                       "d2h_bytes_per_step": 4 * 3 * n_atoms * 8 + nb * 6 * a.gas_n * 8 + n_atoms * len(p) * 8},
+               "e2e_note": "every timed step runs forward_sim and reverse_sim of revsim.gas from host arrays",
+               "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+               "clocks": clk.summary(), "loss_fwd": float(loss_f), "loss_rev": float(loss_r),
+               "D_m2_per_s": D, "l_diff": l_diff, "l_ev": l_ev,
+               "gradient": [float(g) for g in dl_dp]}
+        print(json.dumps(res), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ------------------------------------------------------------ diamond workload
 # Algorithmic work of the Stillinger-Weber reverse terms kernel, counted from its
 # arithmetic (add/mul = 1, FMA = 2, div/exp = 1) with 4 tangents (the position direction
@@ -1501,6 +1730,8 @@ if __name__ == "__main__":
         run_ours_mlp(args)
     elif args.workload == "diamond":
         run_reference_diamond(args) if args.impl == "reference" else run_ours_diamond(args)
+    elif args.workload == "diffusion":
+        run_reference_diffusion(args) if args.impl == "reference" else run_ours_diffusion(args)
     elif args.workload == "reweight":
         run_reference_reweight(args) if args.impl == "reference" else run_ours_reweight(args)
     elif args.workload == "equil":
