@@ -2,7 +2,9 @@
 // rows, the fused forward and reverse step kernels, the energy and the small helpers.
 //
 // Work decomposition: one warp per atom.  The 32 lanes stride over the atom's neighbour row
-// (every other atom within the list cutoff, both directions, ascending index), accumulate the
+// (every other atom within the list cutoff, both directions, grouped by site kind), test the
+// entries against the cutoff, queue the ones inside per warp and evaluate them 32 at a time
+// (see k_gas_step), accumulate the
 // atom's force (and in reverse its VJP and the class sums of the parameter derivatives) in
 // FP64 registers and combine them with a fixed xor butterfly; lane 0 adds the bonded terms of
 // the atom's molecule and runs the atom's integrator update.  Each atom's sums are computed
@@ -54,7 +56,19 @@ __device__ __forceinline__ void o2_bond(const double d[3], double kb, double r0,
 // ------------------------------------------------------------------ neighbour rows
 // Row of atom i: every atom j of another molecule with min-image d^2 <= rc_nl^2 (Molly's
 // per-dimension rule), except water H - gas pairs, which carry no term (no charge on the
-// gas, no pair form on H).  Ascending j by ballot compaction.
+// gas, no pair form on H).  Grouped by site kind -- water O, then water H, then gas, each in
+// ascending order (ballot compaction over that candidate order) -- so that the 32 lanes of
+// a step kernel's warp mostly hold neighbours of one kind and take the same branches.
+__device__ __forceinline__ int kind_order(int c, int nw3) {
+    const int nw = nw3 / 3;
+    if (c < nw) return 3 * c;                        // water O
+    if (c < nw3) {                                   // water H1, H2
+        const int q = c - nw;
+        return 3 * (q >> 1) + 1 + (q & 1);
+    }
+    return c;                                        // gas
+}
+
 __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
@@ -65,7 +79,8 @@ __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
     int n = 0;
     int *row = a.rows + (size_t)i * a.cap;
     for (int base = 0; base < a.N; base += 32) {
-        const int j = base + lane;
+        const int cand = base + lane;
+        const int j = cand < a.N ? kind_order(cand, a.nw3) : a.N;
         bool ok = false;
         if (j < a.N) {
             const int kb = site_kind(j, a.nw3);
@@ -93,8 +108,14 @@ __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
 }
 
 // ------------------------------------------------------------------ step kernels
+// Register budget: the LJ reverse kernel at <= 128 registers (4 CTAs, 16 warps per SM; it
+// spills only in its lane-0 epilogue there); the other reverse forms (dual numbers, more
+// live values) and the forward kernels (76 registers) unconstrained.
 template <int FORM, bool REV>
-__global__ void __launch_bounds__(kThreads) k_gas_step(const GasConsts k, const GasArgs a) {
+constexpr int gas_min_blocks() { return (REV && FORM == F_LJ) ? 4 : 1; }
+
+template <int FORM, bool REV>
+__global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_step(const GasConsts k, const GasArgs a) {
     constexpr int NP = FormInfo<FORM>::NP;
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
@@ -120,14 +141,9 @@ __global__ void __launch_bounds__(kThreads) k_gas_step(const GasConsts k, const 
     double thq = 0.0;
     const int n = a.cnt[i];
     const int *row = a.rows + (size_t)i * a.cap;
-    for (int e = lane; e < n; e += 32) {
-        const int j = row[e];
-        const double4 pb = a.pos_in[j];
-        const double dx = vec_mi(pa.x, pb.x, a.L, a.invL);
-        const double dy = vec_mi(pa.y, pb.y, a.L, a.invL);
-        const double dz = vec_mi(pa.z, pb.z, a.L, a.invL);
-        const double r2 = __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
-        if (!(r2 <= k.rc2)) continue;
+    // Pair terms of one row entry within the cutoff (displacement d, own atom to j).
+    auto pair = [&](const int j, const double dx, const double dy, const double dz,
+                    const double r2) {
         const int kb = site_kind(j, a.nw3);
         const double rinv = xrsqrt(r2);
         const double r = __dmul_rn(r2, rinv);
@@ -135,7 +151,8 @@ __global__ void __launch_bounds__(kThreads) k_gas_step(const GasConsts k, const 
         double F = 0.0, dF = 0.0, Fc = 0.0;
         const bool coul = ka != 2 && kb != 2;
         if (coul) {
-            const double qq = k.qq[(ka == 1) + (kb == 1)];
+            const int qi = (ka == 1) + (kb == 1);
+            const double qq = qi == 0 ? k.qq[0] : qi == 1 ? k.qq[1] : k.qq[2];
             Fc = __dmul_rn(qq, __dsub_rn(invr2, __dmul_rn(k.krf2, r)));
             F = Fc;
             if (REV) dF = -__dmul_rn(__dadd_rn(qq, qq), __dadd_rn(__dmul_rn(invr2, rinv), k.krf));
@@ -144,9 +161,15 @@ __global__ void __launch_bounds__(kThreads) k_gas_step(const GasConsts k, const 
         int cls = -1;
         if (ka != 1 && kb != 1) {
             cls = (ka == 2) + (kb == 2);
-            if (k.on[cls]) {
-                double Ff, dFf = 0.0;
-                pair_form<double, FORM, REV>(k.fc[cls], r, rinv, invr2, Ff, dFf, gf);
+            if (cls == 0 ? k.on[0] : cls == 1 ? k.on[1] : k.on[2]) {
+                // constant class indices keep the constants in the parameter bank
+                double Ff = 0.0, dFf = 0.0;
+                if (cls == 0)
+                    pair_form<double, FORM, REV>(k.fc[0], r, rinv, invr2, Ff, dFf, gf);
+                else if (cls == 1)
+                    pair_form<double, FORM, REV>(k.fc[1], r, rinv, invr2, Ff, dFf, gf);
+                else
+                    pair_form<double, FORM, REV>(k.fc[2], r, rinv, invr2, Ff, dFf, gf);
                 F = __dadd_rn(F, Ff);
                 if (REV) dF = __dadd_rn(dF, dFf);
             } else {
@@ -174,7 +197,61 @@ __global__ void __launch_bounds__(kThreads) k_gas_step(const GasConsts k, const 
 #pragma unroll
                     for (int q = 0; q < NP; q++) acc[c][q] = __fma_rn(-gf[q], na, acc[c][q]);
         }
+        };
+    // Two phases per warp.  Phase 1: each lane loads GAS_U row entries (all loads issued
+    // before any is used, so GAS_U neighbour gathers per lane are in flight), tests them
+    // against the cutoff and pushes the ones inside (about 58 % at the list cutoff 1.2 nm)
+    // onto a per-warp queue in shared memory.  Phase 2: while 32 or more are queued, all
+    // lanes evaluate one each, so the pair arithmetic runs with full warps.  The queue is
+    // processed last-in first-out in a fixed order (deterministic sums).
+    constexpr int GAS_U = 4, QCAP = 32 * GAS_U + 32;
+    __shared__ double s_d[kWarpsPerCta][4][QCAP];
+    __shared__ int s_j[kWarpsPerCta][QCAP];
+    const int w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    int qn = 0;
+    for (int base = 0; base < n; base += 32 * GAS_U) {
+        int jj[GAS_U];
+        double4 pb[GAS_U];
+#pragma unroll
+        for (int u = 0; u < GAS_U; u++) {
+            const int e = base + 32 * u + lane;
+            jj[u] = e < n ? row[e] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < GAS_U; u++)
+            if (jj[u] >= 0) pb[u] = a.pos_in[jj[u]];
+#pragma unroll
+        for (int u = 0; u < GAS_U; u++) {
+            bool ok = false;
+            double dx = 0.0, dy = 0.0, dz = 0.0, r2 = 0.0;
+            if (jj[u] >= 0) {
+                dx = vec_mi(pa.x, pb[u].x, a.L, a.invL);
+                dy = vec_mi(pa.y, pb[u].y, a.L, a.invL);
+                dz = vec_mi(pa.z, pb[u].z, a.L, a.invL);
+                r2 = __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+                ok = r2 <= k.rc2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int q = qn + __popc(m & lt);
+                s_j[w][q] = jj[u];
+                s_d[w][0][q] = dx;
+                s_d[w][1][q] = dy;
+                s_d[w][2][q] = dz;
+                s_d[w][3][q] = r2;
+            }
+            qn += __popc(m);
+        }
+        __syncwarp();
+        while (qn >= 32) {
+            const int q = qn - 32 + lane;
+            pair(s_j[w][q], s_d[w][0][q], s_d[w][1][q], s_d[w][2][q], s_d[w][3][q]);
+            qn -= 32;
+        }
+        __syncwarp();
     }
+    if (lane < qn) pair(s_j[w][lane], s_d[w][0][lane], s_d[w][1][lane], s_d[w][2][lane], s_d[w][3][lane]);
 #pragma unroll
     for (int u = 0; u < 3; u++) {
         f[u] = wsum(f[u]);
@@ -408,7 +485,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_energy(const GasConsts k, cons
         if (ka != 1 && kb != 1) {
             const int cls = (ka == 2) + (kb == 2);
             if (k.on[cls]) {
-                const DualN<double, 4> Ef = form_energy<FORM>(k.fc[cls].p, r);
+                const DualN<double, 4> Ef = form_energy<FORM>(cls == 0 ? k.fc[0].p : cls == 1 ? k.fc[1].p : k.fc[2].p, r);
                 E += Ef.v;
 #pragma unroll
                 for (int c = 0; c < 3; c++)
