@@ -45,6 +45,10 @@ FLOPS_FWD_IPAIR, FLOPS_FWD_OO_EXTRA, FLOPS_REV_IPAIR = 40, 15, 170
 # DRAM traffic per reverse-step launch of the default workload, from ncu
 # (profiles/rev_step_ncu_water3000.md: dram__bytes_read.sum 5.395 MB, write 0).
 REV_STEP_DRAM_BYTES = 5.395e6
+# DRAM traffic per forward-step launch of the gas-in-water engine (2,675 atoms), from ncu
+# with cold caches (profiles/gas_step_ncu_gas2675.md: 8.11 MB read, 0.11 MB written).
+GAS_FWD_STEP_DRAM_BYTES = 8.22e6
+GAS_REV_STEP_DRAM_BYTES = 8.97e6
 
 
 def parse():
@@ -1019,7 +1023,9 @@ def run_ours_diffusion(a):
     flops_launch = fl_rev if rev_dominant else fl_fwd
     achieved = flops_launch / (launch_ms * 1e-3) / 1e12
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "frac": achieved / peak.value if peak.value else None,
+                "traffic": GAS_REV_STEP_DRAM_BYTES if rev_dominant else GAS_FWD_STEP_DRAM_BYTES,
+                "traffic_note": "ncu, cold caches (rows and positions are L2-resident live)",
                 "kernel": ("k_gas_step<LJ, reverse>" if rev_dominant else "k_gas_step<LJ, forward>"),
                 "launch_ms": launch_ms, "ipairs": ipairs, "pair_form_ipairs": form_pairs,
                 "flops_per_launch": flops_launch,
