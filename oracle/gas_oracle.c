@@ -20,6 +20,7 @@ double complex orc_pair_form_energy_cx(int32_t type, const double complex *p, do
 static const double kDiffExp = 2.0e-9;        /* D_exp, m^2 s^-1 (diffusion.jl:900) */
 static const double kDiffWeight = 1e18;       /* loss_weight, m^-4 s^2 (diffusion.jl:902) */
 static const double kLossWeightEv = 0.05;     /* loss_weighting_ev (diffusion.jl:52) */
+static const double kLossWeightRdf = 0.05;    /* loss_weighting_rdf (diffusion.jl:51) */
 static const double kUGas = 3.69, kRT = 2.45, kEvTarget = 44.12 + 2.8;   /* :800-813 */
 
 static inline void vec3(const double *xi, const double *xj, double L, double *d) {
@@ -469,8 +470,8 @@ double orc_gas_diffusion_D(const double *gc, int32_t n_frames, int32_t n_gas, do
 }
 
 double orc_gas_loss_final(int32_t loss_type, const double *gc, int32_t n_frames, int32_t n_gas,
-                          double box, double loss_frequency, double ev_sum, double *out,
-                          double *dl_dgc) {
+                          double box, double loss_frequency, double ev_sum, double rdf_sum,
+                          double *out, double *dl_dgc) {
     const double D = orc_gas_diffusion_D(gc, n_frames, n_gas, box, loss_frequency, dl_dgc);
     const double Dc = D * 1e-6;
     double l_diff = 0.0;
@@ -485,13 +486,14 @@ double orc_gas_loss_final(int32_t loss_type, const double *gc, int32_t n_frames,
         memset(dl_dgc, 0, sizeof(double) * nc);
     }
     const double l_ev = (loss_type & ORC_GAS_EV) ? kLossWeightEv * ev_sum / n_frames : 0.0;
+    const double l_rdf = (loss_type & ORC_GAS_RDF) ? kLossWeightRdf * rdf_sum / n_frames : 0.0;
     if (out) {
         out[0] = Dc;
         out[1] = l_diff;
-        out[2] = 0.0;
+        out[2] = l_rdf;
         out[3] = l_ev;
     }
-    return l_diff + l_ev;
+    return l_diff + l_rdf + l_ev;
 }
 
 static int64_t rebuild(const orc_gas_system *s, const double *x, int32_t **pairs, int64_t *cap) {
@@ -540,12 +542,24 @@ double orc_gas_ev_point(const orc_gas_system *s, const double *params, const dou
     return l;
 }
 
+/* loss_rdf of the water atoms (diffusion.jl:759-774) by the water restatement; its gradient
+ * with respect to the water coordinates into dldx [9 n_water] when non-NULL. */
+static double rdf_raw(const orc_gas_system *s, const orc_loss *rdf, const double *x, double *dldx) {
+    orc_system ws;
+    memset(&ws, 0, sizeof(ws));
+    ws.n_mol = s->n_water;
+    ws.box = s->box;
+    orc_loss L = *rdf;
+    L.enth_vap = 0;
+    return orc_loss_grad(&ws, &L, x, dldx);
+}
+
 /* ------------------------------------------------------------------------- */
 double orc_gas_forward_sim(const orc_gas_system *s, const double *params, double *x, double *v,
                            const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                            int32_t n_steps_loss, double dt, int32_t loss_type,
                            int32_t calc_loss, double *snap_x, double *snap_v, double *gc,
-                           double *out) {
+                           double *out, const orc_loss *rdf) {
     const int64_t n = n_atoms(s), n3 = 3 * n;
     const double L = s->box;
     const double c = exp(-gamma * dt), sn = sqrt(1 - c * c);   /* diffusion.jl:1216-1217 */
@@ -560,7 +574,7 @@ double orc_gas_forward_sim(const orc_gas_system *s, const double *params, double
         memcpy(snap_x, x, sizeof(double) * (size_t)n3);
         memcpy(snap_v, v, sizeof(double) * (size_t)n3);
     }
-    double ev_sum = 0.0;
+    double ev_sum = 0.0, rdf_sum = 0.0;
     /* diffusion.jl:1226-1240 */
     for (int32_t step = 1; step <= n_steps; step++) {
         orc_gas_forces(s, params, x, pairs, np, F);
@@ -582,11 +596,12 @@ double orc_gas_forward_sim(const orc_gas_system *s, const double *params, double
             }
             if (gc && k <= n_blocks) orc_gas_centres(s, x, gc + (k - 1) * 3 * (int64_t)s->n_gas);
             if (calc_loss && (loss_type & ORC_GAS_EV)) ev_sum += ev_raw(s, params, x, NULL, NULL);
+            if (calc_loss && (loss_type & ORC_GAS_RDF) && rdf) rdf_sum += rdf_raw(s, rdf, x, NULL);
         }
     }
     double loss = 0.0;
     if (calc_loss && gc)
-        loss = orc_gas_loss_final(loss_type, gc, n_blocks, s->n_gas, L, lf, ev_sum, out, NULL);
+        loss = orc_gas_loss_final(loss_type, gc, n_blocks, s->n_gas, L, lf, ev_sum, rdf_sum, out, NULL);
     free(F);
     free(xi);
     free(pairs);
@@ -609,11 +624,20 @@ static void reset_accums(int64_t n3, double c, const double *g, double *A, doubl
  * frame split half and half onto the two sites of each gas molecule (diffusion.jl:1536-1539, 1596-1598). */
 static double point_grad(const orc_gas_system *s, const double *params, const double *x,
                          int32_t loss_type, int32_t n_blocks, const double *dgc_frame,
-                         double *g, double *dl_dp) {
+                         double *g, double *dl_dp, const orc_loss *rdf, double *l_rdf) {
     const int64_t n3 = 3 * n_atoms(s);
     memset(g, 0, sizeof(double) * (size_t)n3);
     double l = 0.0;
     if (loss_type & ORC_GAS_EV) l = orc_gas_ev_point(s, params, x, n_blocks, g, dl_dp);
+    *l_rdf = 0.0;
+    if ((loss_type & ORC_GAS_RDF) && rdf) {
+        const int64_t nw9 = 9 * (int64_t)s->n_water;
+        double *t = (double *)malloc(sizeof(double) * (size_t)(nw9 ? nw9 : 1));
+        const double w = kLossWeightRdf / n_blocks;
+        *l_rdf = w * rdf_raw(s, rdf, x, t);
+        for (int64_t e = 0; e < nw9; e++) g[e] += w * t[e];
+        free(t);
+    }
     double *gg = g + 9 * (int64_t)s->n_water;
     for (int64_t q = 0; q < s->n_gas; q++)
         for (int u = 0; u < 3; u++) {
@@ -628,7 +652,7 @@ double orc_gas_reverse_sim(const orc_gas_system *s, const double *params, double
                            const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                            int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
                            int32_t loss_type, const double *snap_x, const double *snap_v,
-                           const double *gc, double *dl_dp, double *out) {
+                           const double *gc, double *dl_dp, double *out, const orc_loss *rdf) {
     const int64_t n = n_atoms(s), n3 = 3 * n;
     const double L = s->box;
     const double c = exp(-gamma * dt), sn = sqrt(1 - c * c), dt2 = dt * dt;
@@ -639,7 +663,7 @@ double orc_gas_reverse_sim(const orc_gas_system *s, const double *params, double
     double *dgc = (double *)malloc(sizeof(double) * (fsz * (size_t)n_blocks + 1));
     double parts[4];
     const double l_diff = orc_gas_loss_final(loss_type & ORC_GAS_DIFF, gc, n_blocks, s->n_gas, L, lf,
-                                             0.0, parts, dgc);
+                                             0.0, 0.0, parts, dgc);
     double *buf = (double *)calloc((size_t)n3 * 9, sizeof(double));
     double *F = buf, *xi = buf + n3, *g = buf + 2 * n3, *A = buf + 3 * n3, *B = buf + 4 * n3;
     double *C = buf + 5 * n3, *Dd = buf + 6 * n3, *dl_dfi = buf + 7 * n3, *acoef = buf + 8 * n3;
@@ -647,7 +671,10 @@ double orc_gas_reverse_sim(const orc_gas_system *s, const double *params, double
     int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * (size_t)cap);
     for (int p = 0; p < P; p++) dl_dp[p] = 0.0;
 
-    double l_ev = point_grad(s, params, x, loss_type, n_blocks, dgc + fsz * (n_blocks - 1), g, dl_dp);
+    double lr_pt = 0.0, l_rdf = 0.0;
+    double l_ev = point_grad(s, params, x, loss_type, n_blocks, dgc + fsz * (n_blocks - 1), g, dl_dp,
+                             rdf, &lr_pt);
+    l_rdf += lr_pt;
     reset_accums(n3, c, g, A, B, C, Dd, dl_dfi);
     memcpy(x, snap_x + (size_t)n_blocks * n3, sizeof(double) * (size_t)n3);
     memcpy(v, snap_v + (size_t)n_blocks * n3, sizeof(double) * (size_t)n3);
@@ -685,18 +712,20 @@ double orc_gas_reverse_sim(const orc_gas_system *s, const double *params, double
             memcpy(x, snap_x + (size_t)k * n3, sizeof(double) * (size_t)n3);
             memcpy(v, snap_v + (size_t)k * n3, sizeof(double) * (size_t)n3);
             np = rebuild(s, x, &pairs, &cap);
-            l_ev += point_grad(s, params, x, loss_type, n_blocks, dgc + fsz * (k - 1), g, dl_dp);
+            l_ev += point_grad(s, params, x, loss_type, n_blocks, dgc + fsz * (k - 1), g, dl_dp, rdf,
+                               &lr_pt);
+            l_rdf += lr_pt;
             reset_accums(n3, c, g, A, B, C, Dd, dl_dfi);
         }
     }
     if (out) {
         out[0] = parts[0];
         out[1] = l_diff;
-        out[2] = 0.0;
+        out[2] = l_rdf;
         out[3] = l_ev;
     }
     free(dgc);
     free(buf);
     free(pairs);
-    return l_diff + l_ev;
+    return l_diff + l_rdf + l_ev;
 }

@@ -31,6 +31,8 @@
 
 #include <stdint.h>
 
+#include "revsim_oracle.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -48,9 +50,12 @@ typedef struct {
     int32_t n_mol_ev;        /* molecules dividing U in the enthalpy term (all: diffusion.jl:804) */
 } orc_gas_system;
 
-/* Loss selection: bit 0 the diffusion term, bit 1 the RDF term (not restated), bit 2 the
- * enthalpy-of-vaporisation term (loss_type :diff, :ev, :diff_ev of diffusion.jl:823-834). */
-enum { ORC_GAS_DIFF = 1, ORC_GAS_EV = 4 };
+/* Loss selection: bit 0 the diffusion term, bit 1 the RDF term, bit 2 the enthalpy-of-
+ * vaporisation term (loss_type :diff, :rdf, :ev and their sums, diffusion.jl:823-834).  The
+ * RDF term is loss_rdf (diffusion.jl:759-774) over the water atoms: the terms of an orc_loss
+ * (revsim_oracle.h; e.g. the O-O and O-H L1 terms against the Soper data) evaluated as the
+ * water restatement does for a box of n_water molecules, weighted 0.05 / n_blocks. */
+enum { ORC_GAS_DIFF = 1, ORC_GAS_RDF = 2, ORC_GAS_EV = 4 };
 
 int32_t orc_gas_n_params(int32_t inter_type);
 
@@ -87,19 +92,20 @@ void orc_gas_centres(const orc_gas_system *s, const double *x, double *c);
 double orc_gas_diffusion_D(const double *gc, int32_t n_frames, int32_t n_gas, double box,
                            double loss_frequency, double *dD_dgc);
 
-/* The loss of loss_fn_final (diffusion.jl:897-911) from the frames and, when the enthalpy
- * term is on, its accumulated per-frame sum; out[0..3] = D (m^2/s), l_diff, l_rdf, l_ev.
- * dl_dgc receives the gradient of l_diff with respect to the centres when non-NULL. */
+/* The loss of loss_fn_final (diffusion.jl:897-911) from the frames and, for the RDF and
+ * enthalpy terms, their accumulated per-frame sums; out[0..3] = D (m^2/s), l_diff, l_rdf,
+ * l_ev.  dl_dgc receives the gradient of l_diff with respect to the centres when non-NULL. */
 double orc_gas_loss_final(int32_t loss_type, const double *gc, int32_t n_frames, int32_t n_gas,
-                          double box, double loss_frequency, double ev_sum, double *out,
-                          double *dl_dgc);
+                          double box, double loss_frequency, double ev_sum, double rdf_sum,
+                          double *out, double *dl_dgc);
 
 /* One loss point's enthalpy term l = 0.05 (dH - 46.92)^2 / n_blocks with its gradients
  * dl/dx (dLdx) and the direct dl/dtheta (added into dl_dp) when non-NULL. */
 double orc_gas_ev_point(const orc_gas_system *s, const double *params, const double *x,
                         int32_t n_blocks, double *dLdx, double *dl_dp);
 
-/* forward_sim (diffusion.jl:1181-1298) without the RAD gradient.  snap_x / snap_v
+/* forward_sim (diffusion.jl:1181-1298) without the RAD gradient; rdf: the RDF terms (used
+ * when loss_type has ORC_GAS_RDF).  snap_x / snap_v
  * [(n_blocks + 1) * 3N]: the state at step 0 and at every loss point; gc
  * [n_blocks * n_gas * 3] the gas centres at the loss points.  Returns the loss when
  * calc_loss, else 0; out[0..3] as orc_gas_loss_final. */
@@ -107,7 +113,7 @@ double orc_gas_forward_sim(const orc_gas_system *s, const double *params, double
                            const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                            int32_t n_steps_loss, double dt, int32_t loss_type,
                            int32_t calc_loss, double *snap_x, double *snap_v, double *gc,
-                           double *out);
+                           double *out, const orc_loss *rdf);
 
 /* reverse_sim (diffusion.jl:1511-1616) from the final state in x, v (and the forward's
  * snapshots and centres): returns the loss; dl_dp [P]; out[0..3] as above.  After a
@@ -118,7 +124,7 @@ double orc_gas_reverse_sim(const orc_gas_system *s, const double *params, double
                            const uint64_t *noise_seeds, double gamma, int32_t n_steps,
                            int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
                            int32_t loss_type, const double *snap_x, const double *snap_v,
-                           const double *gc, double *dl_dp, double *out);
+                           const double *gc, double *dl_dp, double *out, const orc_loss *rdf);
 
 #ifdef __cplusplus
 }

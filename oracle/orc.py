@@ -161,15 +161,15 @@ def lib():
         L.orc_gas_diffusion_D.restype = _D
         L.orc_gas_diffusion_D.argtypes = [_PD, _I32, _I32, _D, _D, _PD]
         L.orc_gas_loss_final.restype = _D
-        L.orc_gas_loss_final.argtypes = [_I32, _PD, _I32, _I32, _D, _D, _D, _PD, _PD]
+        L.orc_gas_loss_final.argtypes = [_I32, _PD, _I32, _I32, _D, _D, _D, _D, _PD, _PD]
         L.orc_gas_ev_point.restype = _D
         L.orc_gas_ev_point.argtypes = [PG, _PD, _PD, _I32, _PD, _PD]
         L.orc_gas_forward_sim.restype = _D
         L.orc_gas_forward_sim.argtypes = [PG, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _D, _I32, _I32,
-                                          _PD, _PD, _PD, _PD]
+                                          _PD, _PD, _PD, _PD, ctypes.POINTER(OrcLoss)]
         L.orc_gas_reverse_sim.restype = _D
         L.orc_gas_reverse_sim.argtypes = [PG, _PD, _PD, _PD, _PU64, _D, _I32, _I32, _I32, _D, _I32,
-                                          _PD, _PD, _PD, _PD, _PD]
+                                          _PD, _PD, _PD, _PD, _PD, ctypes.POINTER(OrcLoss)]
         _lib = L
     return _lib
 
@@ -553,7 +553,7 @@ def mlp_table_n(theta, nt, rc, width):
 # ------------------------------------------------------------------ gas in water
 # diffusion.jl: O2 bond k = 1640.4 kcal/mol/A^2 in kJ/mol/nm^2 and r0 (:46, :1113-1116)
 GAS_KB, GAS_R0 = 1640.4 * 4.184 * 100, 0.12074
-GAS_LOSS = {"diff": 1, "ev": 4, "diff_ev": 5}
+GAS_LOSS = {"diff": 1, "rdf": 2, "ev": 4, "diff_rdf": 3, "diff_ev": 5, "rdf_ev": 6, "diff_rdf_ev": 7}
 
 
 def make_gas_system(n_water, n_gas, box, inter_type="lj", temp=295.15, *, m_O=15.99943,
@@ -634,13 +634,13 @@ def gas_diffusion_D(gc, box, loss_frequency, grads=False):
     return (D, g) if grads else D
 
 
-def gas_loss_final(loss_type, gc, box, loss_frequency, ev_sum=0.0):
+def gas_loss_final(loss_type, gc, box, loss_frequency, ev_sum=0.0, rdf_sum=0.0):
     """(loss, [D m^2/s, l_diff, l_rdf, l_ev], dl_diff/dgc)."""
     gc = _f64(gc)
     out = np.zeros(4)
     g = np.zeros_like(gc)
     l = lib().orc_gas_loss_final(GAS_LOSS[loss_type], _pd(gc), gc.shape[0], gc.shape[1], box,
-                                 loss_frequency, ev_sum, _pd(out), _pd(g))
+                                 loss_frequency, ev_sum, rdf_sum, _pd(out), _pd(g))
     return l, out, g
 
 
@@ -653,8 +653,9 @@ def gas_ev_point(s, p, x, n_blocks):
 
 
 def gas_forward_sim(s, p, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss_type="diff",
-                    calc_loss=True):
-    """(x, v, loss, snaps_x, snaps_v, centres, [D, l_diff, l_rdf, l_ev])."""
+                    calc_loss=True, rdf=None):
+    """(x, v, loss, snaps_x, snaps_v, centres, [D, l_diff, l_rdf, l_ev]); rdf: a Loss of RDF
+    terms for the rdf loss types."""
     x, v = _f64(x).copy(), _f64(v).copy()
     seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
     n_blocks = 1 if n_steps == 0 else n_steps // n_steps_loss
@@ -665,12 +666,12 @@ def gas_forward_sim(s, p, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss_ty
     l = lib().orc_gas_forward_sim(ctypes.byref(s), _pd(_f64(p)), _pd(x), _pd(v),
                                   seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss, dt,
                                   GAS_LOSS[loss_type], 1 if calc_loss else 0, _pd(sx), _pd(sv),
-                                  _pd(gc), _pd(out))
+                                  _pd(gc), _pd(out), ctypes.byref(rdf.c) if rdf is not None else None)
     return x, v, l, sx, sv, gc, out
 
 
 def gas_reverse_sim(s, p, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, snaps_x,
-                    snaps_v, centres, loss_type="diff"):
+                    snaps_v, centres, loss_type="diff", rdf=None):
     """(x, v, loss, dl_dp, [D, l_diff, l_rdf, l_ev])."""
     x, v = _f64(x).copy(), _f64(v).copy()
     seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
@@ -679,5 +680,6 @@ def gas_reverse_sim(s, p, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_tru
     l = lib().orc_gas_reverse_sim(ctypes.byref(s), _pd(_f64(p)), _pd(x), _pd(v),
                                   seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss,
                                   n_steps_trunc, dt, GAS_LOSS[loss_type], _pd(_f64(snaps_x)),
-                                  _pd(_f64(snaps_v)), _pd(_f64(centres)), _pd(dp), _pd(out))
+                                  _pd(_f64(snaps_v)), _pd(_f64(centres)), _pd(dp), _pd(out),
+                                  ctypes.byref(rdf.c) if rdf is not None else None)
     return x, v, l, dp, out

@@ -144,15 +144,17 @@ def test_diffusion_coefficient_and_its_gradient():
         assert abs(fd - g[f, q, u]) <= 1e-6 * max(abs(fd), 1e-8)
 
 
-@pytest.mark.parametrize("loss_type", ["diff", "diff_ev"])
+@pytest.mark.parametrize("loss_type", ["diff", "diff_ev", "diff_rdf_ev"])
 def test_reverse_reconstructs_and_matches_forward(small_gas, loss_type):
     """diffusion.jl:1674-1675: reconstruction < 1e-9, |L_rev - L_fwd| < 1e-7."""
     s, p, x0, v0 = small_gas
     n, nl = 40, 10
     seeds = systems.noise_seeds(n, seed=11)
-    xf, vf, lf, sx, sv, gc, outf = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, loss_type)
+    rdf = gas_rdf_loss(2) if "rdf" in loss_type else None
+    xf, vf, lf, sx, sv, gc, outf = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, loss_type,
+                                                       rdf=rdf)
     xr, vr, lr, dp, outr = orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, n, nl, nl, 0.001, sx, sv, gc,
-                                               loss_type)
+                                               loss_type, rdf=rdf)
     d = xr - x0
     d -= s.box * np.round(d / s.box)
     assert np.abs(d).max() < 1e-9
@@ -160,13 +162,23 @@ def test_reverse_reconstructs_and_matches_forward(small_gas, loss_type):
     assert np.allclose(outr, outf, rtol=1e-12, atol=0)
 
 
-def blockwise_fd(s, p, sx, sv, seeds, nl, n_blocks, loss_type, dl_dgc, k):
+def gas_rdf_loss(seed=0):
+    """Two smooth (squared-error) RDF terms over the water atoms, O-O and O-H, against seeded
+    random targets: the shape of loss_rdf (diffusion.jl:759-774) without the Soper data."""
+    rng = np.random.default_rng(seed)
+    return orc.Loss([orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, rng.uniform(0, 2, 200), 2, 1.0),
+                     orc.RdfTerm(0, 1, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, rng.uniform(0, 2, 200), 2, 1.0)])
+
+
+def blockwise_fd(s, p, sx, sv, seeds, nl, n_blocks, loss_type, dl_dgc, k, rdf=None):
     """d/dtheta_k of the reverse pass's estimator by central differences: reverse_sim resets
     its adjoints at every loss point (diffusion.jl:1589-1605), so each loss point's gradient
     flows back through its own block only; here each block restarts from its stored snapshot
-    with theta +- h and the frame's centres (and enthalpy term) are differenced.  h is 1e-3
-    relative: the centres move by ~1e-8 nm per 1e-5 of a parameter, where rounding dominates."""
+    with theta +- h and the frame's centres (and RDF / enthalpy terms) are differenced.  h is
+    1e-3 relative: the centres move by ~1e-8 nm per 1e-5 of a parameter, where rounding
+    dominates."""
     h = 1e-3 * abs(p[k])
+    point = "_".join(t for t in ("rdf", "ev") if t in loss_type) or "ev"
     tot = 0.0
     for b in range(n_blocks):
         res = []
@@ -174,31 +186,50 @@ def blockwise_fd(s, p, sx, sv, seeds, nl, n_blocks, loss_type, dl_dgc, k):
             pk = p.copy()
             pk[k] += sgn * h
             out = orc.gas_forward_sim(s, pk, sx[b], sv[b], seeds[b * nl:(b + 1) * nl], 1.0, nl, nl,
-                                      0.001, "ev", calc_loss="ev" in loss_type)
-            res.append((out[5][0], out[6][3] / n_blocks))
+                                      0.001, point, calc_loss=point in loss_type, rdf=rdf)
+            res.append((out[5][0], (out[6][2] + out[6][3]) / n_blocks))
         d = res[0][0] - res[1][0]
         d -= s.box * np.round(d / s.box)
         tot += (dl_dgc[b] * d).sum() / (2 * h)
-        if "ev" in loss_type:
+        if point in loss_type:
             tot += (res[0][1] - res[1][1]) / (2 * h)
     return tot
 
 
 @pytest.mark.parametrize("form,loss_type", [("lj", "diff"), ("lj", "diff_ev"), ("buck", "diff"),
-                                            ("dexp", "diff")])
+                                            ("dexp", "diff"), ("lj", "diff_rdf_ev"), ("lj", "rdf")])
 def test_reverse_gradient_against_blockwise_central_differences(form, loss_type):
     """The reverse pass's gradient against central differences of the same estimator (the
     reference prints its reverse gradient beside RAD and FD ones, diffusion.jl:1656-1681)."""
     s, p, x0, v0 = relaxed_gas(60, 4, 2.5, form, seed=8, steps=30)
     n, nl = 24, 6
+    rdf = gas_rdf_loss(3) if "rdf" in loss_type else None
     seeds = systems.noise_seeds(n, seed=13)
-    xf, vf, lf, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, loss_type)
+    xf, vf, lf, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, loss_type,
+                                                    rdf=rdf)
     _, _, lr, dp, _ = orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, n, nl, nl, 0.001, sx, sv, gc,
-                                          loss_type)
+                                          loss_type, rdf=rdf)
+    assert abs(lr - lf) < 1e-7
     _, _, dl_dgc = orc.gas_loss_final("diff", gc, s.box, nl * 0.001)
-    fd = np.array([blockwise_fd(s, p, sx, sv, seeds, nl, n // nl, loss_type, dl_dgc, k)
+    if "diff" not in loss_type:
+        dl_dgc = np.zeros_like(dl_dgc)
+    fd = np.array([blockwise_fd(s, p, sx, sv, seeds, nl, n // nl, loss_type, dl_dgc, k, rdf)
                    for k in range(len(p))])
     # in units of dL/dlog(theta), floored at 1% of the largest component
     sf = np.abs(fd * p)
     err = np.abs((dp - fd) * p) / np.maximum(sf, 0.01 * sf.max())
     assert np.all(err < 1e-4), (form, err)
+
+
+def test_rdf_term_is_the_water_rdf_of_the_water_atoms():
+    """The gas system's RDF loss point is the water restatement's loss on the water atoms,
+    weighted 0.05 / n_blocks (diffusion.jl:51, 765-771)."""
+    s, p, x0, v0 = relaxed_gas(60, 4, 2.5, seed=9, steps=10)
+    rdf = gas_rdf_loss(4)
+    n, nl = 12, 6
+    seeds = systems.noise_seeds(n, seed=14)
+    _, _, lf, sx, sv, gc, out = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, "rdf", rdf=rdf)
+    ws = orc.make_system(s.n_water, s.box)
+    ref = sum(orc.loss_grad(ws, rdf, sx[b + 1].reshape(-1, 3)[:3 * s.n_water])[0] for b in range(2))
+    assert abs(out[2] - 0.05 * ref / 2) <= 1e-12 * abs(out[2]) and out[1] == out[3] == 0.0
+    assert abs(lf - out[2]) <= 1e-15 * abs(lf)
