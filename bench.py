@@ -87,7 +87,7 @@ def parse():
     ap.add_argument("--gas-steps", type=int, default=50000)
     ap.add_argument("--gas-steps-loss", type=int, default=500)
     ap.add_argument("--gas-trunc", type=int, default=200)
-    ap.add_argument("--gas-loss", default="diff_ev", choices=["diff", "diff_ev"])
+    ap.add_argument("--gas-loss", default="diff_rdf_ev", choices=["diff", "diff_ev", "diff_rdf_ev"])
     ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
@@ -850,7 +850,12 @@ def diffusion_config(a, extra=None):
          "dt_ps": 0.001, "gamma_per_ps": 1.0, "pair_form": a.form, "precision": "fp64",
          "loss": {"diff": "diffusion coefficient of the O2 centres (calculate_D, diffusion.jl:861-911)",
                   "diff_ev": "diffusion coefficient plus the enthalpy-of-vaporisation term "
-                             "(diffusion.jl:799-815, 861-911)"}[a.gas_loss],
+                             "(diffusion.jl:799-815, 861-911)",
+                  "diff_rdf_ev": "train()'s :diff_rdf_ev: diffusion coefficient, the O-O and O-H "
+                                 "L1 RDF terms of the water atoms on the reference grid and "
+                                 "slices against flat synthetic targets (g = 1; the Soper data "
+                                 "is not on the box), and the enthalpy term "
+                                 "(diffusion.jl:759-815, 861-911)"}[a.gas_loss],
          "source": "train() of diffusion.jl:1683-1700 (50 ps forward, loss every 500 fs, "
                    "reverse truncated at 200 steps per loss point)",
          "l2": "flushed (256 MiB write) between timed steps"}
@@ -899,17 +904,36 @@ def gas_count_ipairs(x, a, cutoff=1.0):
     return total, form
 
 
+def gas_rdf_terms(a):
+    """The RDF terms of the diffusion workload: loss_rdf's O-O and O-H L1 terms on the
+    reference grid and slices (diffusion.jl:759-774) against flat targets (g = 1)."""
+    from revsim.loss import reference_rdf_terms
+    return reference_rdf_terms(np.ones(248), np.ones(281)) if "rdf" in a.gas_loss else None
+
+
+def gas_oracle_rdf(a):
+    from oracle import orc
+    terms = gas_rdf_terms(a)
+    if terms is None:
+        return None
+    return orc.Loss([orc.RdfTerm(t.sel1, t.sel2, t.x_min, t.step, t.width, t.exp_cutoff, t.n_grid,
+                                 t.slice_start, t.slice_stride, t.target, t.norm, t.weight)
+                     for t in terms])
+
+
 def gas_cpu_sample(a, x0, v0, p):
     """The FP64 oracle on a bounded sample: 10 forward steps (two loss points) and the 4
     reverse steps of a truncation of 2, per-step costs scaled to the workload."""
     from oracle import orc
     from revsim import systems
     s = orc.make_gas_system(a.gas_water, a.gas_n, a.gas_box, a.form)
+    rdf = gas_oracle_rdf(a)
     seeds = systems.noise_seeds(10, seed=98)
     t0 = time.perf_counter()
-    xf, vf, _, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, 10, 5, 0.001, a.gas_loss)
+    xf, vf, _, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, 10, 5, 0.001, a.gas_loss,
+                                                   rdf=rdf)
     t1 = time.perf_counter()
-    orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, 10, 5, 2, 0.001, sx, sv, gc, a.gas_loss)
+    orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, 10, 5, 2, 0.001, sx, sv, gc, a.gas_loss, rdf=rdf)
     t2 = time.perf_counter()
     nb = a.gas_steps // a.gas_steps_loss
     n_rev = nb * min(a.gas_trunc, a.gas_steps_loss)
@@ -968,6 +992,8 @@ def run_ours_diffusion(a):
     from revsim.gas import GasEngine, forward_sim, reverse_sim
     x0, v0, p = gas_prepare(a, local)
     eng = GasEngine(a.gas_water, a.gas_n, a.gas_box, a.form, device=local)
+    if "rdf" in a.gas_loss:
+        eng.set_rdf(gas_rdf_terms(a))
     seeds = systems.noise_seeds(a.gas_steps, seed=700 + rank)
     stream = torch.cuda.ExternalStream(eng.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")

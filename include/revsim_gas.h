@@ -6,8 +6,9 @@
  * (diffusion.jl:1511-1616) and the force / force-gradient kernels they call (calc_F!
  * diffusion.jl:959-1057, calc_F_and_grads! diffusion.jl:1300-1509, the neighbour finder of
  * setup_system diffusion.jl:1133-1155), with the diffusion-coefficient loss
- * (calculate_D diffusion.jl:861-895, loss_fn_final 897-911) and the enthalpy-of-
- * vaporisation loss (diffusion.jl:799-815) at the loss points.
+ * (calculate_D diffusion.jl:861-895, loss_fn_final 897-911), the enthalpy-of-
+ * vaporisation loss (diffusion.jl:799-815) and the RDF loss of the water atoms
+ * (diffusion.jl:759-774) at the loss points.
  *
  * The system: n_water flexible 3-site waters (atoms O, H1, H2) followed by n_gas two-site
  * O2 molecules (atoms O1, O2).  Pair forms between unlike sites by Lorentz-Berthelot mixing
@@ -33,9 +34,10 @@
 extern "C" {
 #endif
 
-/* Loss terms (loss_type of diffusion.jl:823-834; the RDF term is not built):
- * :diff -> REVSIM_GAS_DIFF, :ev -> REVSIM_GAS_EV, :diff_ev -> both. */
+/* Loss terms (loss_type of diffusion.jl:823-834), bits of loss_type: :diff -> REVSIM_GAS_DIFF,
+ * :rdf -> REVSIM_GAS_RDF, :ev -> REVSIM_GAS_EV; :diff_rdf_ev -> all three. */
 #define REVSIM_GAS_DIFF 1
+#define REVSIM_GAS_RDF 2
 #define REVSIM_GAS_EV 4
 
 typedef struct revsim_gas_handle revsim_gas_handle;
@@ -73,6 +75,13 @@ int32_t revsim_gas_set_params(revsim_gas_handle *h, const double *theta, int32_t
 /* coords / velocities [3 N], N = 3 n_water + 2 n_gas. */
 int32_t revsim_gas_set_state(revsim_gas_handle *h, const double *x, const double *v);
 int32_t revsim_gas_get_state(revsim_gas_handle *h, double *x, double *v);
+
+/* The RDF term: loss_rdf (diffusion.jl:759-774) over the water atoms, n_terms smoothed-RDF
+ * terms (revsim_rdf_term of revsim.h, e.g. the O-O and O-H L1 terms against the Soper data of
+ * read_rdf_data, diffusion.jl:673-686) with their targets [n_target] each, weighted
+ * 0.05 / n_blocks (loss_weighting_rdf, diffusion.jl:51) at every loss point. */
+int32_t revsim_gas_set_rdf(revsim_gas_handle *h, int32_t n_terms, const revsim_rdf_term *terms,
+                           const double *const *targets);
 
 /* calc_F! at the current state: F [3 N]. */
 int32_t revsim_gas_forces(revsim_gas_handle *h, double *F);

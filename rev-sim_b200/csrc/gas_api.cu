@@ -51,8 +51,20 @@ struct revsim_gas_handle {
     bool fwd_valid = false;
     int fwd_steps = 0, fwd_nl = 0, fwd_blocks = 0;
     double fwd_dt = 0, fwd_gamma = 0;
-    std::vector<double> centres, Eloss;
-    bool fwd_has_E = false;
+    std::vector<double> centres, Eloss, Rloss;
+    bool fwd_has_E = false, fwd_has_R = false;
+    // RDF term of the water atoms: the terms, their targets and scratch (histogram with the
+    // normaliser behind it, dL/dh), the one-box table {atom0, n_mol} / box, dL/dx of the
+    // water atoms, and the per-loss-point losses of the forward pass
+    struct RdfDev {
+        revsim_rdf_term t;
+        int off = 0;
+        double *d_target = nullptr, *d_hist = nullptr, *d_dLdh = nullptr;
+    };
+    std::vector<RdfDev> rdf;
+    int *d_rdf_int = nullptr;
+    double *d_rdf_box = nullptr, *d_rdf_dx = nullptr, *d_rdf_tmp = nullptr, *d_rdf_loss = nullptr;
+    size_t rdf_loss_cap = 0;
     // instrumentation
     long long launches = 0;
     bool ktime = false;
@@ -66,6 +78,7 @@ namespace {
 
 constexpr double kDiffExp = 2.0e-9, kDiffWeight = 1e18;   // diffusion.jl:900-902
 constexpr double kLossWeightEv = 0.05;                    // diffusion.jl:52
+constexpr double kLossWeightRdf = 0.05;                   // diffusion.jl:51
 constexpr double kUGas = 3.69, kRT = 2.45, kEvTarget = 44.12 + 2.8;   // diffusion.jl:800-813
 
 int fail(revsim_gas_handle *h, int code, const std::string &msg) {
@@ -390,14 +403,60 @@ int ensure_eloss(revsim_gas_handle *h, size_t n) {
     return REVSIM_OK;
 }
 
+void free_rdf(revsim_gas_handle *h) {
+    for (auto &T : h->rdf) {
+        if (T.d_target) cudaFree(T.d_target);
+        if (T.d_hist) cudaFree(T.d_hist);
+        if (T.d_dLdh) cudaFree(T.d_dLdh);
+    }
+    h->rdf.clear();
+}
+
+// Every RDF term at the current state (the water atoms 0 .. 3 n_water - 1, laid out O, H1, H2
+// as the water engine's boxes): the summed term losses into *d_loss (accumulated) and, when
+// grad, dL/dx of the water atoms into d_rdf_dx (accumulated).
+int rdf_point(revsim_gas_handle *h, bool grad, double *d_loss) {
+    for (auto &T : h->rdf) {
+        const revsim_rdf_term &t = T.t;
+        CK(cudaMemsetAsync(T.d_hist, 0, sizeof(double) * t.n_grid, h->st));
+        rs::RdfArgs a;
+        a.x = h->d_x;
+        a.rep_atom0 = h->d_rdf_int;
+        a.rep_nmol = h->d_rdf_int + 1;
+        a.rep_box = h->d_rdf_box;
+        a.sel1 = t.sel1;
+        a.sel2 = t.sel2;
+        a.x_min = t.x_min;
+        a.step = t.step;
+        a.width = t.width;
+        a.cutoff = t.exp_cutoff;
+        a.n_grid = t.n_grid;
+        a.off = T.off;
+        a.hist = T.d_hist;
+        a.dLdh = T.d_dLdh;
+        a.dLdx = h->d_rdf_dx;
+        const int n1 = t.sel1 == 0 ? h->nw : 2 * h->nw, n2 = t.sel2 == 0 ? h->nw : 2 * h->nw;
+        CK(rs::launch_rdf(a, 1, n1, n2, false, h->st));
+        CK(rs::launch_rdf_finalize(a, 1, T.d_hist + t.n_grid, T.d_target, t.slice_start, t.slice_stride,
+                                   t.n_target, t.norm, t.weight, d_loss, T.d_dLdh, h->st));
+        h->launches += 2;
+        if (grad) {
+            CK(rs::launch_rdf(a, 1, n1, n2, true, h->st));
+            h->launches++;
+        }
+    }
+    return REVSIM_OK;
+}
+
 // dl/dx of one loss point into d_g (enthalpy term, then the centre gradient of the frame
 // halved onto the two sites of each gas molecule, diffusion.jl:1536-1539), the direct
 // enthalpy dl/dtheta into d_direct; l_ev receives the point's enthalpy loss.
-int point_grad(revsim_gas_handle *h, int loss_type, int n_blocks, double E, const double *dgc_frame,
-               double *l_ev) {
+int point_grad(revsim_gas_handle *h, int loss_type, int n_blocks, double E, double R,
+               const double *dgc_frame, double *l_ev, double *l_rdf) {
     const size_t n3 = 3 * (size_t)h->N;
     CK(cudaMemsetAsync(h->d_g, 0, n3 * sizeof(double), h->st));
     *l_ev = 0.0;
+    *l_rdf = 0.0;
     if (loss_type & REVSIM_GAS_EV) {
         const double e = ev_err(h, E);
         *l_ev = e * e * kLossWeightEv / n_blocks;
@@ -411,6 +470,18 @@ int point_grad(revsim_gas_handle *h, int loss_type, int n_blocks, double E, cons
         rc = energy_partials(h);
         if (rc) return rc;
         launch_gas_esum(h->N, h->P, h->d_epart, 0.0, -kk, true, h->d_direct, h->st);
+        h->launches++;
+        CK(cudaGetLastError());
+    }
+    if ((loss_type & REVSIM_GAS_RDF) && h->nw > 0) {
+        // loss_and_grads_rdf_ev (diffusion.jl:922-947): 0.05 loss_rdf / n_blocks
+        const double wr = kLossWeightRdf / n_blocks;
+        *l_rdf = wr * R;
+        CK(cudaMemsetAsync(h->d_rdf_dx, 0, 9 * (size_t)h->nw * sizeof(double), h->st));
+        CK(cudaMemsetAsync(h->d_rdf_tmp, 0, sizeof(double), h->st));
+        int rc = rdf_point(h, true, h->d_rdf_tmp);
+        if (rc) return rc;
+        launch_gas_axpy(9 * h->nw, wr, h->d_rdf_dx, h->d_g, h->st);
         h->launches++;
         CK(cudaGetLastError());
     }
@@ -462,6 +533,10 @@ int32_t revsim_gas_destroy(revsim_gas_handle *h) {
                     h->d_direct, h->d_gtail, h->d_Eloss, h->d_pos[0], h->d_pos[1], h->d_wgt[0],
                     h->d_wgt[1], h->d_snap_x, h->d_snap_v};
     for (void *p : bufs)
+        if (p) cudaFree(p);
+    free_rdf(h);
+    void *rbufs[] = {h->d_rdf_int, h->d_rdf_box, h->d_rdf_dx, h->d_rdf_tmp, h->d_rdf_loss};
+    for (void *p : rbufs)
         if (p) cudaFree(p);
     for (int w = 0; w < 2; w++)
         for (cudaEvent_t e : h->ev[w]) cudaEventDestroy(e);
@@ -526,14 +601,65 @@ int32_t revsim_gas_create(const revsim_gas_desc *d, revsim_gas_handle **out) {
         bad(dalloc(&h->d_part, N * kMaxP)) || bad(dalloc(&h->d_epart, N * (kMaxP + 1))) ||
         bad(dalloc(&h->d_direct, kMaxP + 1)) || bad(dalloc(&h->d_gtail, 6 * (size_t)h->ng)) ||
         bad(dalloc(&h->d_pos[0], N)) || bad(dalloc(&h->d_pos[1], N)) || bad(dalloc(&h->d_wgt[0], N)) ||
-        bad(dalloc(&h->d_wgt[1], N)) || bad(cudaMemset(h->d_status, 0, sizeof(int))) ||
+        bad(dalloc(&h->d_wgt[1], N)) || bad(dalloc(&h->d_rdf_int, 2)) ||
+        bad(dalloc(&h->d_rdf_box, 1)) || bad(dalloc(&h->d_rdf_dx, 9 * (size_t)h->nw)) ||
+        bad(dalloc(&h->d_rdf_tmp, 1)) || bad(cudaMemset(h->d_status, 0, sizeof(int))) ||
         bad(cudaMemset(h->d_wgt[0], 0, N * sizeof(double4))) ||
         bad(cudaMemset(h->d_wgt[1], 0, N * sizeof(double4)))) {
         cudaGetLastError();
         revsim_gas_destroy(h);
         return REVSIM_ERR_NOMEM;
     }
+    const int tab[2] = {0, h->nw};
+    if (bad(cudaMemcpy(h->d_rdf_int, tab, sizeof(tab), cudaMemcpyHostToDevice)) ||
+        bad(cudaMemcpy(h->d_rdf_box, &h->L, sizeof(double), cudaMemcpyHostToDevice))) {
+        cudaGetLastError();
+        revsim_gas_destroy(h);
+        return REVSIM_ERR_CUDA;
+    }
     *out = h;
+    return REVSIM_OK;
+}
+
+int32_t revsim_gas_set_rdf(revsim_gas_handle *h, int32_t n_terms, const revsim_rdf_term *terms,
+                           const double *const *targets) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (n_terms < 0 || (n_terms > 0 && (!terms || !targets))) return fail(h, REVSIM_ERR_BADARG, "bad RDF terms");
+    for (int i = 0; i < n_terms; i++) {
+        const revsim_rdf_term &t = terms[i];
+        if (t.n_grid < 1 || !(t.step > 0) || !(t.width > 0) || !(t.exp_cutoff >= 0) || t.n_target < 1 ||
+            t.slice_start < 0 || t.slice_stride < 1 ||
+            t.slice_start + (long long)(t.n_target - 1) * t.slice_stride >= t.n_grid ||
+            (t.norm != 1 && t.norm != 2) || (t.sel1 != 0 && t.sel1 != 1) || (t.sel2 != 0 && t.sel2 != 1) ||
+            !targets[i])
+            return fail(h, REVSIM_ERR_BADARG, "bad RDF term");
+        const double q = t.x_min / t.step;
+        if (std::fabs(q - std::llround(q)) > 1e-6)
+            return fail(h, REVSIM_ERR_BADARG, "x_min must be a multiple of step (diffusion.jl:709)");
+    }
+    if (n_terms > 0 && h->nw < 1) return fail(h, REVSIM_ERR_BADARG, "the RDF term needs water molecules");
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->st));
+    free_rdf(h);
+    const double pi = 3.14159265358979323846;
+    for (int i = 0; i < n_terms; i++) {
+        const revsim_rdf_term &t = terms[i];
+        revsim_gas_handle::RdfDev T;
+        T.t = t;
+        T.off = (int)std::llround(t.x_min / t.step) - 1;
+        h->rdf.push_back(T);
+        auto &D = h->rdf.back();
+        if (dalloc(&D.d_target, t.n_target) != cudaSuccess || dalloc(&D.d_hist, (size_t)t.n_grid + 1) != cudaSuccess ||
+            dalloc(&D.d_dLdh, t.n_grid) != cudaSuccess) {
+            free_rdf(h);
+            return fail(h, REVSIM_ERR_NOMEM, "RDF scratch");
+        }
+        // the normaliser V / (4 pi n1 n2 step) behind the histogram (rdf_differentiable, 725)
+        const double n1 = t.sel1 == 0 ? h->nw : 2.0 * h->nw, n2 = t.sel2 == 0 ? h->nw : 2.0 * h->nw;
+        const double pre = h->L * h->L * h->L / (4 * pi * n1 * n2 * t.step);
+        CK(cudaMemcpy(D.d_target, targets[i], sizeof(double) * t.n_target, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(D.d_hist + t.n_grid, &pre, sizeof(double), cudaMemcpyHostToDevice));
+    }
     return REVSIM_OK;
 }
 
@@ -651,7 +777,10 @@ int32_t revsim_gas_forward(revsim_gas_handle *h, const uint64_t *seeds, double g
     if (!h->have_params || !h->have_state) return fail(h, REVSIM_ERR_STATE, "set parameters and state first");
     if (n_steps < 0 || n_steps_loss < 1 || !(dt > 0) || !(gamma >= 0) || (n_steps > 0 && !seeds))
         return fail(h, REVSIM_ERR_BADARG, "bad step arguments");
-    if (loss_type & ~(REVSIM_GAS_DIFF | REVSIM_GAS_EV)) return fail(h, REVSIM_ERR_BADARG, "unknown loss_type bits");
+    if (loss_type & ~(REVSIM_GAS_DIFF | REVSIM_GAS_RDF | REVSIM_GAS_EV))
+        return fail(h, REVSIM_ERR_BADARG, "unknown loss_type bits");
+    if ((loss_type & REVSIM_GAS_RDF) && h->rdf.empty())
+        return fail(h, REVSIM_ERR_STATE, "the RDF loss needs revsim_gas_set_rdf first");
     const int n_blocks = n_steps == 0 ? 1 : n_steps / n_steps_loss;
     if (calc_loss && (loss_type & REVSIM_GAS_DIFF) && n_blocks < 2)
         return fail(h, REVSIM_ERR_BADARG, "the diffusion loss needs at least two loss points");
@@ -662,6 +791,16 @@ int32_t revsim_gas_forward(revsim_gas_handle *h, const uint64_t *seeds, double g
     int rc = ensure_snapshots(h, (size_t)n_blocks + 1);
     if (!rc && calc_loss && (loss_type & REVSIM_GAS_EV)) rc = ensure_eloss(h, (size_t)n_blocks);
     if (rc) return rc;
+    const bool want_R = calc_loss && (loss_type & REVSIM_GAS_RDF);
+    if (want_R && h->rdf_loss_cap < (size_t)n_blocks) {
+        if (h->d_rdf_loss) cudaFree(h->d_rdf_loss);
+        h->d_rdf_loss = nullptr;
+        h->rdf_loss_cap = 0;
+        if (dalloc(&h->d_rdf_loss, (size_t)n_blocks) != cudaSuccess)
+            return fail(h, REVSIM_ERR_NOMEM, "loss-point RDF losses");
+        h->rdf_loss_cap = n_blocks;
+    }
+    if (want_R) CK(cudaMemsetAsync(h->d_rdf_loss, 0, sizeof(double) * n_blocks, h->st));
     h->fwd_valid = false;
     const double c = std::exp(-gamma * dt), sn = std::sqrt(1 - c * c);   // diffusion.jl:1216-1217
     h->cur = 0;
@@ -698,6 +837,10 @@ int32_t revsim_gas_forward(revsim_gas_handle *h, const uint64_t *seeds, double g
                                     h->d_Eloss + (size_t)(k - 1) * (h->P + 1), h->st);
                     h->launches++;
                 }
+                if (want_R) {
+                    rc = rdf_point(h, false, h->d_rdf_loss + (k - 1));
+                    if (rc) return rc;
+                }
             }
         }
         if (h->ktime && (stp & 1023) == 0) {
@@ -722,9 +865,16 @@ int32_t revsim_gas_forward(revsim_gas_handle *h, const uint64_t *seeds, double g
         CK(cudaStreamSynchronize(h->st));
         for (int b = 0; b < h->fwd_blocks; b++) h->Eloss[b] = e[(size_t)b * (h->P + 1)];
     }
+    h->fwd_has_R = want_R;
+    h->Rloss.assign(h->fwd_blocks, 0.0);
+    if (want_R && h->fwd_blocks > 0) {
+        CK(cudaMemcpyAsync(h->Rloss.data(), h->d_rdf_loss, sizeof(double) * h->fwd_blocks,
+                           cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    }
     h->fwd_valid = true;
     if (centres) std::copy(h->centres.begin(), h->centres.end(), centres);
-    double D = 0.0, l_diff = 0.0, l_ev = 0.0;
+    double D = 0.0, l_diff = 0.0, l_ev = 0.0, l_rdf = 0.0;
     if (h->fwd_blocks >= 2 && h->ng > 0)
         D = diffusion_D(h->centres, h->fwd_blocks, h->ng, h->L, n_steps_loss * dt, nullptr) * 1e-6;
     if (calc_loss) {
@@ -737,12 +887,17 @@ int32_t revsim_gas_forward(revsim_gas_handle *h, const uint64_t *seeds, double g
             }
             l_ev = kLossWeightEv * s / n_blocks;
         }
+        if (want_R) {
+            double s = 0.0;
+            for (int b = 0; b < h->fwd_blocks; b++) s += h->Rloss[b];
+            l_rdf = kLossWeightRdf * s / n_blocks;
+        }
     }
-    if (loss) *loss = l_diff + l_ev;
+    if (loss) *loss = l_diff + l_rdf + l_ev;
     if (parts) {
         parts[0] = D;
         parts[1] = l_diff;
-        parts[2] = 0.0;
+        parts[2] = l_rdf;
         parts[3] = l_ev;
     }
     return REVSIM_OK;
@@ -757,13 +912,16 @@ int32_t revsim_gas_reverse(revsim_gas_handle *h, const uint64_t *seeds, double g
     if (n_steps != h->fwd_steps || n_steps_loss != h->fwd_nl || dt != h->fwd_dt || gamma != h->fwd_gamma)
         return fail(h, REVSIM_ERR_BADARG, "reverse arguments differ from the forward pass");
     if (n_steps < 1 || n_steps_trunc < 1 || !seeds) return fail(h, REVSIM_ERR_BADARG, "bad step arguments");
-    if (loss_type & ~(REVSIM_GAS_DIFF | REVSIM_GAS_EV)) return fail(h, REVSIM_ERR_BADARG, "unknown loss_type bits");
+    if (loss_type & ~(REVSIM_GAS_DIFF | REVSIM_GAS_RDF | REVSIM_GAS_EV))
+        return fail(h, REVSIM_ERR_BADARG, "unknown loss_type bits");
     const int n_blocks = n_steps / n_steps_loss;
     if (n_blocks < 1) return fail(h, REVSIM_ERR_BADARG, "no loss point to reverse from");
     if ((loss_type & REVSIM_GAS_DIFF) && (n_blocks < 2 || h->ng < 1))
         return fail(h, REVSIM_ERR_BADARG, "the diffusion loss needs two loss points and gas molecules");
     if ((loss_type & REVSIM_GAS_EV) && !h->fwd_has_E)
         return fail(h, REVSIM_ERR_STATE, "the forward pass did not record the enthalpy term");
+    if ((loss_type & REVSIM_GAS_RDF) && (!h->fwd_has_R || h->rdf.empty()))
+        return fail(h, REVSIM_ERR_STATE, "the forward pass did not record the RDF term");
     CK(cudaSetDevice(h->dev));
     const size_t n3 = 3 * (size_t)h->N, fsz = 3 * (size_t)h->ng;
     const double c = std::exp(-gamma * dt), sn = std::sqrt(1 - c * c);
@@ -789,12 +947,14 @@ int32_t revsim_gas_reverse(revsim_gas_handle *h, const uint64_t *seeds, double g
     int rc = pack(h);
     if (!rc) rc = rebuild(h);
     if (rc) return rc;
-    double l_ev = 0.0, lp = 0.0;
+    double l_ev = 0.0, lp = 0.0, l_rdf = 0.0, lr = 0.0;
     rc = point_grad(h, loss_type, n_blocks, h->Eloss.empty() ? 0.0 : h->Eloss[n_blocks - 1],
-                    dgc.empty() ? nullptr : dgc.data() + fsz * (n_blocks - 1), &lp);
+                    h->Rloss.empty() ? 0.0 : h->Rloss[n_blocks - 1],
+                    dgc.empty() ? nullptr : dgc.data() + fsz * (n_blocks - 1), &lp, &lr);
     if (!rc) rc = reset_accums(h, c);
     if (rc) return rc;
     l_ev += lp;
+    l_rdf += lr;
     for (int lc = 1; lc <= n_blocks; lc++) {
         const int s_start = n_steps - (lc - 1) * n_steps_loss;
         const int s_end = std::max(s_start - n_steps_trunc + 1, 1);
@@ -837,10 +997,12 @@ int32_t revsim_gas_reverse(revsim_gas_handle *h, const uint64_t *seeds, double g
             if (!rc) rc = rebuild(h);
             if (!rc)
                 rc = point_grad(h, loss_type, n_blocks, h->Eloss.empty() ? 0.0 : h->Eloss[k - 1],
-                                dgc.empty() ? nullptr : dgc.data() + fsz * (k - 1), &lp);
+                                h->Rloss.empty() ? 0.0 : h->Rloss[k - 1],
+                                dgc.empty() ? nullptr : dgc.data() + fsz * (k - 1), &lp, &lr);
             if (!rc) rc = reset_accums(h, c);
             if (rc) return rc;
             l_ev += lp;
+            l_rdf += lr;
         }
         if (h->ktime) {
             rc = check_status(h);
@@ -856,11 +1018,11 @@ int32_t revsim_gas_reverse(revsim_gas_handle *h, const uint64_t *seeds, double g
     for (int i = 0; i < h->N; i++)
         for (int p = 0; p < h->P; p++) dl_dp[p] += part[(size_t)i * h->P + p];
     h->fwd_valid = false;
-    if (loss) *loss = l_diff + l_ev;
+    if (loss) *loss = l_diff + l_rdf + l_ev;
     if (parts) {
         parts[0] = D;
         parts[1] = l_diff;
-        parts[2] = 0.0;
+        parts[2] = l_rdf;
         parts[3] = l_ev;
     }
     return REVSIM_OK;

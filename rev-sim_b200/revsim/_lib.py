@@ -55,7 +55,7 @@ GAS_EXPORTS = [
     "revsim_gas_set_params", "revsim_gas_set_state", "revsim_gas_get_state", "revsim_gas_forces",
     "revsim_gas_force_vjp", "revsim_gas_energy", "revsim_gas_forward", "revsim_gas_reverse",
     "revsim_gas_stream", "revsim_gas_launch_count", "revsim_gas_set_kernel_timing",
-    "revsim_gas_kernel_time",
+    "revsim_gas_kernel_time", "revsim_gas_set_rdf",
 ]
 
 
@@ -227,6 +227,7 @@ def load(path=LIB_PATH):
         "revsim_gas_launch_count": (i64, [vp]),
         "revsim_gas_set_kernel_timing": (i32, [vp, i32]),
         "revsim_gas_kernel_time": (i32, [vp, i32, pd, pi64]),
+        "revsim_gas_set_rdf": (i32, [vp, i32, P(RdfTermC), P(pd)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -8,9 +8,10 @@ return tuples.  Differences, each deliberate:
 * coordinates / velocities are numpy arrays [N, 3] (nm, nm/ps), N = 3 n_water + 2 n_gas with
   the waters first (setup_system's order, diffusion.jl:1068-1118); ``coords_in=None`` (the
   reference's PDB start and steepest-descent minimisation) is not part of the engine;
-* ``loss_type`` is ``"diff"``, ``"ev"`` or ``"diff_ev"`` (a leading ``:`` is accepted); the
-  RDF term of diffusion.jl:759-774 (O-O / O-H against the Soper data) is not built for this
-  system, so the ``rdf`` combinations raise ``NotImplementedError``;
+* ``loss_type`` is any of diffusion.jl's :diff, :rdf, :ev, :diff_rdf, :diff_ev, :diff_rdf_ev
+  (a leading ``:`` is accepted); the RDF term's targets are explicit (``loss_terms``, the
+  engine's ``RdfTerm``s; ``loss.reference_rdf_terms`` builds the O-O / O-H L1 terms of
+  diffusion.jl:759-774 from the Soper data the reference reads at load time, 673-686);
 * ``run_grads=True`` (the Zygote unrolled-RAD check) is not part of the engine;
 * the forward's snapshots and gas centres stay on the engine: ``sys.loggers`` is the engine
   and ``loss_accum`` carries the centres and the loss parts for inspection;
@@ -23,9 +24,10 @@ import ctypes
 import numpy as np
 
 from . import constants as C
-from ._lib import GasDesc, RevsimError, f64p, load, u64p
+from ._lib import GasDesc, RdfTermC, RevsimError, f64p, load, u64p
 
-LOSS_BITS = {"diff": 1, "ev": 4, "diff_ev": 5}
+LOSS_BITS = {"diff": 1, "rdf": 2, "ev": 4, "diff_rdf": 3, "diff_ev": 5, "rdf_ev": 6,
+             "diff_rdf_ev": 7}
 INTER = {"lj": 0, "dexp": 1, "buck": 2, "ljsc": 3, "buff": 4}
 
 
@@ -33,8 +35,6 @@ def loss_bits(loss_type):
     lt = str(loss_type).lstrip(":")
     if lt in LOSS_BITS:
         return LOSS_BITS[lt]
-    if lt in ("rdf", "diff_rdf", "diff_rdf_ev", "rdf_ev"):
-        raise NotImplementedError("the RDF term of the gas-in-water loss is not built")
     raise ValueError("loss_type not recognised")
 
 
@@ -89,6 +89,21 @@ class GasEngine:
         x, v = np.zeros((self.n_atoms, 3)), np.zeros((self.n_atoms, 3))
         self._check(self._L.revsim_gas_get_state(self._h, f64p(x), f64p(v)))
         return x, v
+
+    def set_rdf(self, terms):
+        """The RDF term's smoothed-RDF terms over the water atoms (engine.RdfTerm, one target
+        [n_target] each); weighted 0.05 / n_blocks at every loss point."""
+        terms = list(terms)
+        arr = (RdfTermC * max(1, len(terms)))()
+        tg = []
+        for i, t in enumerate(terms):
+            target = np.ascontiguousarray(t.target, dtype=np.float64).reshape(-1)
+            tg.append(target)
+            arr[i] = RdfTermC(t.sel1, t.sel2, t.x_min, t.step, t.width, t.exp_cutoff, t.n_grid,
+                              t.slice_start, t.slice_stride, len(target), t.norm, t.weight)
+        ptrs = (ctypes.POINTER(ctypes.c_double) * max(1, len(tg)))(*[f64p(a) for a in tg])
+        self._check(self._L.revsim_gas_set_rdf(self._h, len(terms), arr, ptrs))
+        self.rdf_terms = terms
 
     def forces(self):
         F = np.zeros((self.n_atoms, 3))
@@ -186,7 +201,7 @@ def _engine_for(coords, inter_type, engine, n_gas, box):
 
 def forward_sim(coords_in, velocities_in, noise_seeds, gamma, n_steps, n_steps_loss, params, dt,
                 n_threads, inter_type, loss_type, run_grads=False, calc_loss=True, *, engine=None,
-                n_gas=C.GAS_N_GAS, box=C.GAS_BOX):
+                n_gas=C.GAS_N_GAS, box=C.GAS_BOX, loss_terms=None):
     """diffusion.jl:1181.  Returns (sys, loss, loss_accum, grads); grads is [None] * P as in
     the reference's run_grads=false branch (diffusion.jl:1301-1303)."""
     if run_grads:
@@ -194,6 +209,8 @@ def forward_sim(coords_in, velocities_in, noise_seeds, gamma, n_steps, n_steps_l
     if coords_in is None or velocities_in is None:
         raise ValueError("the engine starts from given coordinates and velocities")
     eng = _engine_for(coords_in, inter_type, engine, n_gas, box)
+    if loss_terms is not None:
+        eng.set_rdf(loss_terms)
     eng.set_params(params)
     eng.set_state(coords_in, velocities_in)
     loss, parts, centres = eng.forward(noise_seeds, gamma, n_steps, n_steps_loss, dt, loss_type,

@@ -156,6 +156,42 @@ def test_argument_checks(gas120):
         e.reverse(seeds, 1.0, 20, 5, 5, 0.001)       # differs from the forward pass
     with pytest.raises(RevsimError):
         e.reverse(seeds, 1.0, 20, 10, 10, 0.001, "ev")   # forward recorded no enthalpy term
-    with pytest.raises(NotImplementedError):
-        e.forward(seeds, 1.0, 20, 10, 0.001, "diff_rdf_ev")
+    with pytest.raises(RevsimError):
+        e.forward(seeds, 1.0, 20, 10, 0.001, "diff_rdf_ev")   # no RDF terms set
+    with pytest.raises(ValueError):
+        e.forward(seeds, 1.0, 20, 10, 0.001, "rdf_diff")
+    e.close()
+
+
+def _rdf_terms(seed):
+    """Two squared-error RDF terms (O-O, O-H) with seeded random targets, for the engine and
+    for the oracle."""
+    from revsim import RdfTerm
+    rng = np.random.default_rng(seed)
+    spec = [(0, 0, rng.uniform(0, 2, 200)), (0, 1, rng.uniform(0, 2, 200))]
+    eng = [RdfTerm(a, b, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, t, 2, 1.0) for a, b, t in spec]
+    orl = orc.Loss([orc.RdfTerm(a, b, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, t, 2, 1.0) for a, b, t in spec])
+    return eng, orl
+
+
+@pytest.mark.parametrize("loss_type", ["diff_rdf_ev", "rdf"])
+def test_rdf_term_matches_oracle(loss_type):
+    """The RDF term of the water atoms (diffusion.jl:759-774, weighted 0.05 / n_blocks) in the
+    forward loss and in the reverse gradient, against the oracle."""
+    s, p, x0, v0 = relaxed_gas(80, 5, 2.5, "lj", seed=6, steps=30)
+    terms, orl = _rdf_terms(7)
+    n, nl = 40, 10
+    seeds = systems.noise_seeds(n, seed=25)
+    xf, vf, lfo, sx, sv, gc, outf = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, loss_type,
+                                                        rdf=orl)
+    _, _, lro, dpo, outo = orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, n, nl, nl, 0.001, sx, sv, gc,
+                                               loss_type, rdf=orl)
+    e = _engine(s, p, x0, v0, "lj")
+    e.set_rdf(terms)
+    lf, partsf, _ = e.forward(seeds, 1.0, n, nl, 0.001, loss_type)
+    assert abs(lf - lfo) <= 1e-9 * abs(lfo) and np.allclose(partsf, outf, rtol=1e-9, atol=0)
+    lr, g, parts = e.reverse(seeds, 1.0, n, nl, nl, 0.001, loss_type)
+    assert abs(lr - lf) < 1e-7 and np.allclose(parts, outo, rtol=1e-9, atol=0)
+    scale = np.abs(dpo * p).max()
+    assert np.all(np.abs((g - dpo) * p) <= 1e-7 * scale), (g, dpo)
     e.close()
