@@ -922,26 +922,33 @@ def gas_oracle_rdf(a):
 
 
 def gas_cpu_sample(a, x0, v0, p):
-    """The FP64 oracle on a bounded sample: 10 forward steps (two loss points) and the 4
-    reverse steps of a truncation of 2, per-step costs scaled to the workload."""
+    """The FP64 oracle on a bounded sample, scaled to the workload: 10 forward steps, the 4
+    reverse steps of two truncated blocks (diffusion loss only), and one loss point of the RDF
+    and enthalpy terms (value and gradient), counted twice per loss point (forward value,
+    reverse gradient)."""
     from oracle import orc
     from revsim import systems
     s = orc.make_gas_system(a.gas_water, a.gas_n, a.gas_box, a.form)
     rdf = gas_oracle_rdf(a)
     seeds = systems.noise_seeds(10, seed=98)
     t0 = time.perf_counter()
-    xf, vf, _, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, 10, 5, 0.001, a.gas_loss,
-                                                   rdf=rdf)
+    xf, vf, _, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, 10, 5, 0.001, "diff")
     t1 = time.perf_counter()
-    orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, 10, 5, 2, 0.001, sx, sv, gc, a.gas_loss, rdf=rdf)
+    orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, 10, 5, 2, 0.001, sx, sv, gc, "diff")
     t2 = time.perf_counter()
+    if rdf is not None:
+        orc.loss_grad(orc.make_system(a.gas_water, a.gas_box), rdf, xf[:3 * a.gas_water])
+    if "ev" in a.gas_loss:
+        orc.gas_ev_point(s, p, xf, 1)
+    t3 = time.perf_counter()
     nb = a.gas_steps // a.gas_steps_loss
     n_rev = nb * min(a.gas_trunc, a.gas_steps_loss)
-    per_grad = (t1 - t0) / 10 * a.gas_steps + (t2 - t1) / 4 * n_rev
+    per_grad = (t1 - t0) / 10 * a.gas_steps + (t2 - t1) / 4 * n_rev + 2 * nb * (t3 - t2)
     n_atoms = 3 * a.gas_water + 2 * a.gas_n
     return n_atoms * a.gas_steps / per_grad, orc.num_threads(), (
-        f"10 forward steps (2 loss points) and 4 reverse steps of the {n_atoms}-atom box, FP64 "
-        f"oracle; per-step costs scaled to {a.gas_steps} forward + {n_rev} reverse steps")
+        f"10 forward and 4 reverse steps of the {n_atoms}-atom box and one loss point of the "
+        f"RDF / enthalpy terms, FP64 oracle; scaled to {a.gas_steps} forward + {n_rev} reverse "
+        f"steps and {nb} loss points (each counted twice)")
 
 
 def run_reference_diffusion(a):
