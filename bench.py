@@ -88,6 +88,7 @@ def parse():
     ap.add_argument("--gas-steps-loss", type=int, default=500)
     ap.add_argument("--gas-trunc", type=int, default=200)
     ap.add_argument("--gas-loss", default="diff_rdf_ev", choices=["diff", "diff_ev", "diff_rdf_ev"])
+    ap.add_argument("--gas-precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
@@ -841,13 +842,13 @@ DIFF_METRIC = "gas-in-water gradient atom-steps/s (forward steps of forward + tr
 
 
 def diffusion_config(a, extra=None):
-    c = {"workload": (f"gas_{a.gas_water}w+{a.gas_n}O2_{a.gas_box:g}nm_{a.form}_fp64_"
+    c = {"workload": (f"gas_{a.gas_water}w+{a.gas_n}O2_{a.gas_box:g}nm_{a.form}_{a.gas_precision}_"
                       f"{a.gas_steps}fwd_loss{a.gas_steps_loss}_trunc{a.gas_trunc}_{a.gas_loss}"),
          "n_atoms": 3 * a.gas_water + 2 * a.gas_n, "n_water": a.gas_water, "n_gas": a.gas_n,
          "box_nm": a.gas_box, "n_steps": a.gas_steps, "n_steps_loss": a.gas_steps_loss,
          "n_steps_trunc": a.gas_trunc,
          "reverse_steps": (a.gas_steps // a.gas_steps_loss) * min(a.gas_trunc, a.gas_steps_loss),
-         "dt_ps": 0.001, "gamma_per_ps": 1.0, "pair_form": a.form, "precision": "fp64",
+         "dt_ps": 0.001, "gamma_per_ps": 1.0, "pair_form": a.form, "precision": a.gas_precision,
          "loss": {"diff": "diffusion coefficient of the O2 centres (calculate_D, diffusion.jl:861-911)",
                   "diff_ev": "diffusion coefficient plus the enthalpy-of-vaporisation term "
                              "(diffusion.jl:799-815, 861-911)",
@@ -998,7 +999,7 @@ def run_ours_diffusion(a):
     from revsim import _lib, systems
     from revsim.gas import GasEngine, forward_sim, reverse_sim
     x0, v0, p = gas_prepare(a, local)
-    eng = GasEngine(a.gas_water, a.gas_n, a.gas_box, a.form, device=local)
+    eng = GasEngine(a.gas_water, a.gas_n, a.gas_box, a.form, device=local, precision=a.gas_precision)
     if "rdf" in a.gas_loss:
         eng.set_rdf(gas_rdf_terms(a))
     seeds = systems.noise_seeds(a.gas_steps, seed=700 + rank)
@@ -1047,7 +1048,9 @@ def run_ours_diffusion(a):
     eng.set_kernel_timing(False)
     ipairs, form_pairs = gas_count_ipairs(x0, a)
     peak = ctypes.c_double()
-    _lib.load().revsim_probe_fp64_tflops(local, ctypes.byref(peak))
+    mixed = a.gas_precision == "mixed"
+    (_lib.load().revsim_probe_fp32_tflops if mixed else _lib.load().revsim_probe_fp64_tflops)(
+        local, ctypes.byref(peak))
     fl_fwd = FLOPS_FWD_IPAIR * ipairs + FLOPS_FWD_OO_EXTRA * form_pairs
     fl_rev = FLOPS_REV_IPAIR * ipairs
     k_rev, k_fwd = rev_ms / max(rev_n, 1), fwd_ms / max(fwd_n, 1)
@@ -1055,14 +1058,15 @@ def run_ours_diffusion(a):
     launch_ms = k_rev if rev_dominant else k_fwd
     flops_launch = fl_rev if rev_dominant else fl_fwd
     achieved = flops_launch / (launch_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value if peak.value else None,
+    roofline = {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak.value,
+                "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
                 "traffic": GAS_REV_STEP_DRAM_BYTES if rev_dominant else GAS_FWD_STEP_DRAM_BYTES,
                 "traffic_note": "ncu, cold caches (rows and positions are L2-resident live)",
                 "kernel": ("k_gas_step<LJ, reverse>" if rev_dominant else "k_gas_step<LJ, forward>"),
                 "launch_ms": launch_ms, "ipairs": ipairs, "pair_form_ipairs": form_pairs,
                 "flops_per_launch": flops_launch,
-                "peak_source": "measured FP64 FMA throughput of this GPU (revsim_probe_fp64_tflops)",
+                "peak_source": ("measured FP32 FMA throughput of this GPU (revsim_probe_fp32_tflops)" if mixed
+                                else "measured FP64 FMA throughput of this GPU (revsim_probe_fp64_tflops)"),
                 "reverse_step_ms": k_rev, "forward_step_ms": k_fwd,
                 "reverse_share": rev_ms / ms, "forward_share": fwd_ms / ms}
     cpu = None
@@ -1074,7 +1078,8 @@ def run_ours_diffusion(a):
         nb = a.gas_steps // a.gas_steps_loss
         res = {"metric": DIFF_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "vs_baseline": None, "dtype": "f64" if a.gas_precision == "fp64" else "f32+f64",
+               "data": "synthetic",
                "config": diffusion_config(a, {"parallelism": f"replicas{world}" if world > 1 else "single"}),
                "e2e": {"value": value, "unit": UNIT,
                        "h2d_bytes_per_step": 2 * 3 * n_atoms * 8 + nb * 6 * a.gas_n * 8,

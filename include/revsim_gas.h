@@ -21,7 +21,7 @@
  *
  * Conventions as in revsim.h: FP64 AoS xyz host arrays copied in and out, int32 status
  * (REVSIM_OK or a negative REVSIM_ERR_*), one CUDA stream per handle, one host thread per
- * handle at a time.  All arithmetic is FP64.
+ * handle at a time.  All arithmetic is FP64 unless the descriptor asks for REVSIM_MIXED.
  */
 #ifndef REVSIM_GAS_H
 #define REVSIM_GAS_H
@@ -60,6 +60,8 @@ typedef struct {
     double kb_g, r0_g;        /* O2 bond (1640.4 * 4.184 * 100, 0.12074) */
     int32_t n_mol_ev;         /* molecules dividing U in the enthalpy term (n_water + n_gas) */
     int32_t device;           /* CUDA device ordinal */
+    int32_t precision;        /* REVSIM_FP64 (0) or REVSIM_MIXED: FP32 pair arithmetic; state,
+                                 bonded terms, integrator, adjoints and sums stay FP64 */
 } revsim_gas_desc;
 
 /* System(...) of setup_system. */

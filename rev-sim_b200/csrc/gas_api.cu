@@ -37,6 +37,8 @@ struct revsim_gas_handle {
     std::vector<double> theta;
     bool have_params = false, have_state = false;
     GasConsts kc{};
+    GasConstsT<float> kcf{};
+    bool mixed = false;   // FP32 pair arithmetic (REVSIM_MIXED)
     int cap = 0, cur = 0;
     int *d_rows = nullptr, *d_cnt = nullptr, *d_status = nullptr;
     double *d_x = nullptr, *d_v = nullptr, *d_A = nullptr, *d_B = nullptr, *d_C = nullptr,
@@ -44,7 +46,11 @@ struct revsim_gas_handle {
            *d_ac = nullptr, *d_part = nullptr, *d_epart = nullptr, *d_direct = nullptr,
            *d_gtail = nullptr, *d_Eloss = nullptr;
     size_t eloss_cap = 0;
-    double4 *d_pos[2] = {nullptr, nullptr}, *d_wgt[2] = {nullptr, nullptr};
+    // gather buffers (32 B per atom: double4 in FP64, float4 in mixed precision) and the FP64
+    // copy pos64 of the positions (aliases d_pos in FP64)
+    void *d_pos[2] = {nullptr, nullptr}, *d_wgt[2] = {nullptr, nullptr};
+    double4 *d_pos64[2] = {nullptr, nullptr};
+    double4 *d_p64own[2] = {nullptr, nullptr};   // allocations of pos64 in mixed precision
     // forward record
     double *d_snap_x = nullptr, *d_snap_v = nullptr;
     size_t snap_cap = 0;   // snapshots
@@ -187,6 +193,30 @@ void set_consts(revsim_gas_handle *h) {
         k.fc[c] = rs::form_consts<double>(h->form, pc[c], nfp);
         k.fc[c].on = k.on[c];
     }
+    // the same constants in FP32 for the mixed-precision pair arithmetic
+    GasConstsT<float> &kf = h->kcf;
+    std::memset(&kf, 0, sizeof(kf));
+    for (int q = 0; q < 3; q++) kf.qq[q] = (float)k.qq[q];
+    kf.krf = (float)k.krf;
+    kf.krf2 = (float)k.krf2;
+    kf.rc2 = (float)k.rc2;
+    kf.twoinvq = (float)k.twoinvq;
+    kf.crf_shift = k.crf_shift;
+    for (int c = 0; c < 3; c++) {
+        kf.fc[c] = rs::form_consts<float>(h->form, pc[c], nfp);
+        kf.fc[c].on = k.on[c];
+        kf.on[c] = k.on[c];
+        for (int q = 0; q < 4; q++) {
+            kf.fw[c][q] = k.fw[c][q];
+            kf.fg[c][q] = k.fg[c][q];
+        }
+    }
+    for (int q = 0; q < 4; q++) {
+        kf.iw[q] = k.iw[q];
+        kf.ig[q] = k.ig[q];
+    }
+    kf.P = k.P;
+    kf.iq = k.iq;
 }
 
 GasArgs args(revsim_gas_handle *h) {
@@ -203,6 +233,8 @@ GasArgs args(revsim_gas_handle *h) {
     a.pos_out = h->d_pos[h->cur ^ 1];
     a.wgt_in = h->d_wgt[h->cur];
     a.wgt_out = h->d_wgt[h->cur ^ 1];
+    a.pos64_in = h->d_pos64[h->cur];
+    a.pos64_out = h->d_pos64[h->cur ^ 1];
     a.x = h->d_x;
     a.v = h->d_v;
     a.A = h->d_A;
@@ -230,7 +262,7 @@ int rebuild(revsim_gas_handle *h) {
     r.nw3 = h->nw3;
     r.L = h->L;
     r.rc_nl2 = h->rc_nl * h->rc_nl;
-    r.pos = h->d_pos[h->cur];
+    r.x = h->d_x;
     r.rows = h->d_rows;
     r.cnt = h->d_cnt;
     r.cap = h->cap;
@@ -242,7 +274,7 @@ int rebuild(revsim_gas_handle *h) {
 }
 
 int pack(revsim_gas_handle *h) {
-    launch_gas_pack(h->N, h->d_x, h->d_pos[h->cur], h->st);
+    launch_gas_pack(h->mixed, h->N, h->d_x, h->d_pos[h->cur], h->d_pos64[h->cur], h->st);
     h->launches++;
     CK(cudaGetLastError());
     return REVSIM_OK;
@@ -266,7 +298,7 @@ int step(revsim_gas_handle *h, bool rev, const GasArgs &a, bool timed = true) {
         e1 = h->ev[w][h->ev_used[w]++];
         CK(cudaEventRecord(e0, h->st));
     }
-    launch_gas_step(h->form, rev, h->kc, a, h->st);
+    launch_gas_step(h->mixed, h->form, rev, h->kcf, h->kc, a, h->st);
     h->launches++;
     CK(cudaGetLastError());
     if (timed) CK(cudaEventRecord(e1, h->st));
@@ -531,7 +563,7 @@ int32_t revsim_gas_destroy(revsim_gas_handle *h) {
     void *bufs[] = {h->d_rows, h->d_cnt, h->d_status, h->d_x, h->d_v, h->d_A, h->d_B, h->d_C,
                     h->d_D, h->d_G, h->d_F, h->d_g, h->d_w, h->d_ac, h->d_part, h->d_epart,
                     h->d_direct, h->d_gtail, h->d_Eloss, h->d_pos[0], h->d_pos[1], h->d_wgt[0],
-                    h->d_wgt[1], h->d_snap_x, h->d_snap_v};
+                    h->d_wgt[1], h->d_snap_x, h->d_snap_v, h->d_p64own[0], h->d_p64own[1]};
     for (void *p : bufs)
         if (p) cudaFree(p);
     free_rdf(h);
@@ -571,8 +603,11 @@ int32_t revsim_gas_create(const revsim_gas_desc *d, revsim_gas_handle **out) {
     h->r0g = def(d->r0_g, 0.12074);
     h->n_mol_ev = d->n_mol_ev > 0 ? d->n_mol_ev : d->n_water + d->n_gas;
     h->dev = d->device;
+    h->mixed = d->precision == REVSIM_MIXED;
     int rc0 = REVSIM_OK;
-    if (h->nw < 0 || h->ng < 0 || h->nw + h->ng < 1)
+    if (d->precision != REVSIM_FP64 && d->precision != REVSIM_MIXED)
+        rc0 = fail(h, REVSIM_ERR_BADARG, "precision must be REVSIM_FP64 or REVSIM_MIXED");
+    else if (h->nw < 0 || h->ng < 0 || h->nw + h->ng < 1)
         rc0 = fail(h, REVSIM_ERR_BADARG, "need n_water, n_gas >= 0 and at least one molecule");
     else if (form_nparams(h->form) < 0)
         rc0 = fail(h, REVSIM_ERR_BADARG, "unknown inter_type");
@@ -600,8 +635,10 @@ int32_t revsim_gas_create(const revsim_gas_desc *d, revsim_gas_handle **out) {
         bad(dalloc(&h->d_g, n3)) || bad(dalloc(&h->d_w, n3)) || bad(dalloc(&h->d_ac, n3)) ||
         bad(dalloc(&h->d_part, N * kMaxP)) || bad(dalloc(&h->d_epart, N * (kMaxP + 1))) ||
         bad(dalloc(&h->d_direct, kMaxP + 1)) || bad(dalloc(&h->d_gtail, 6 * (size_t)h->ng)) ||
-        bad(dalloc(&h->d_pos[0], N)) || bad(dalloc(&h->d_pos[1], N)) || bad(dalloc(&h->d_wgt[0], N)) ||
-        bad(dalloc(&h->d_wgt[1], N)) || bad(dalloc(&h->d_rdf_int, 2)) ||
+        bad(dalloc((double4 **)&h->d_pos[0], N)) || bad(dalloc((double4 **)&h->d_pos[1], N)) ||
+        bad(dalloc((double4 **)&h->d_wgt[0], N)) || bad(dalloc((double4 **)&h->d_wgt[1], N)) ||
+        (h->mixed && (bad(dalloc(&h->d_p64own[0], N)) || bad(dalloc(&h->d_p64own[1], N)))) ||
+        bad(dalloc(&h->d_rdf_int, 2)) ||
         bad(dalloc(&h->d_rdf_box, 1)) || bad(dalloc(&h->d_rdf_dx, 9 * (size_t)h->nw)) ||
         bad(dalloc(&h->d_rdf_tmp, 1)) || bad(cudaMemset(h->d_status, 0, sizeof(int))) ||
         bad(cudaMemset(h->d_wgt[0], 0, N * sizeof(double4))) ||
@@ -610,6 +647,8 @@ int32_t revsim_gas_create(const revsim_gas_desc *d, revsim_gas_handle **out) {
         revsim_gas_destroy(h);
         return REVSIM_ERR_NOMEM;
     }
+    for (int b = 0; b < 2; b++)
+        h->d_pos64[b] = h->mixed ? h->d_p64own[b] : static_cast<double4 *>(h->d_pos[b]);
     const int tab[2] = {0, h->nw};
     if (bad(cudaMemcpy(h->d_rdf_int, tab, sizeof(tab), cudaMemcpyHostToDevice)) ||
         bad(cudaMemcpy(h->d_rdf_box, &h->L, sizeof(double), cudaMemcpyHostToDevice))) {
@@ -730,7 +769,7 @@ int32_t revsim_gas_force_vjp(revsim_gas_handle *h, const double *w, const double
     int rc = pack(h);
     if (!rc) rc = rebuild(h);
     if (rc) return rc;
-    launch_gas_pack_w(h->N, h->nw3, h->d_w, h->mO, h->mH, h->d_wgt[h->cur], h->st);
+    launch_gas_pack_w(h->mixed, h->N, h->nw3, h->d_w, h->mO, h->mH, h->d_wgt[h->cur], h->st);
     h->launches++;
     GasArgs a = args(h);
     a.mode = rs::MODE_FORCES_ONLY;
@@ -966,8 +1005,9 @@ int32_t revsim_gas_reverse(revsim_gas_handle *h, const uint64_t *seeds, double g
             a.s = sn;
             a.seed_next = seeds[s_start - 1];
             a.pos_out = h->d_pos[h->cur];
+            a.pos64_out = h->d_pos64[h->cur];
             a.wgt_out = h->d_wgt[h->cur];
-            launch_gas_part1(a, h->st);
+            launch_gas_part1(h->mixed, a, h->st);
             h->launches++;
             CK(cudaGetLastError());
         }

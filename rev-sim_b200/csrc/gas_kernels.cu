@@ -23,6 +23,21 @@ namespace {
 
 __device__ __forceinline__ double kind_mass(int k, double mO, double mH) { return k == 1 ? mH : mO; }
 
+__device__ __forceinline__ double4 ld3(const double *x, int i) {
+    const size_t b = 3 * (size_t)i;
+    return make_double4(x[b], x[b + 1], x[b + 2], 0.0);
+}
+
+template <typename V4>
+__device__ __forceinline__ V4 mk4(double a, double b, double c) {
+    V4 r;
+    r.x = a;
+    r.y = b;
+    r.z = c;
+    r.w = 0;
+    return r;
+}
+
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -73,7 +88,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
     if (i >= a.N) return;
-    const double4 pa = a.pos[i];
+    const double4 pa = ld3(a.x, i);
     const int ka = site_kind(i, a.nw3);
     const int mi = i < a.nw3 ? i / 3 : (a.nw3 / 3) + (i - a.nw3) / 2;
     int n = 0;
@@ -86,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
             const int kb = site_kind(j, a.nw3);
             const int mj = j < a.nw3 ? j / 3 : (a.nw3 / 3) + (j - a.nw3) / 2;
             if (mj != mi && !((ka == 1 && kb == 2) || (ka == 2 && kb == 1))) {
-                const double4 pb = a.pos[j];
+                const double4 pb = ld3(a.x, j);
                 const double d0 = vec1d(pa.x, pb.x, a.L), d1 = vec1d(pa.y, pb.y, a.L),
                              d2 = vec1d(pa.z, pb.z, a.L);
                 const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
@@ -114,88 +129,94 @@ __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
 template <int FORM, bool REV>
 constexpr int gas_min_blocks() { return (REV && FORM == F_LJ) ? 4 : 1; }
 
-template <int FORM, bool REV>
-__global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_step(const GasConsts k, const GasArgs a) {
+// R: pair arithmetic (float in mixed precision, double in FP64).  The pair loop gathers
+// V4T<R> positions and weights; the per-lane sums are R and are combined in FP64; the
+// bonded terms and the integrator run in FP64 on the FP64 gather copy pos64.
+template <typename R, int FORM, bool REV>
+__global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_step(const GasConstsT<R> k, const GasArgs a) {
+    using V4 = typename V4T<R>::T;
     constexpr int NP = FormInfo<FORM>::NP;
+    const V4 *pos_in = static_cast<const V4 *>(a.pos_in);
+    const V4 *wgt_in = static_cast<const V4 *>(a.wgt_in);
+    const R L = (R)a.L, invL = (R)a.invL;
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
     if (i >= a.N) return;   // whole warps only
     const int ka = site_kind(i, a.nw3);
     const double ma = kind_mass(ka, a.mO, a.mH);
-    const double4 pa = a.pos_in[i];
-    double4 wa = make_double4(0.0, 0.0, 0.0, 0.0);
-    double ca[3] = {0.0, 0.0, 0.0};
+    const V4 pa = pos_in[i];
+    V4 wa = mk4<V4>(0.0, 0.0, 0.0);
+    R ca[3] = {R(0), R(0), R(0)};
     if (REV) {
-        wa = a.wgt_in[i];
+        wa = wgt_in[i];
         const double cf = __ddiv_rn(__dmul_rn(a.dt, a.dt), __dmul_rn(2.0, ma));
 #pragma unroll
         for (int u = 0; u < 3; u++)
-            ca[u] = a.acoef_in ? a.acoef_in[3 * (size_t)i + u] : __dmul_rn(a.A[3 * (size_t)i + u], cf);
+            ca[u] = (R)(a.acoef_in ? a.acoef_in[3 * (size_t)i + u] : __dmul_rn(a.A[3 * (size_t)i + u], cf));
     }
-    double f[3] = {0.0, 0.0, 0.0}, g[3] = {0.0, 0.0, 0.0};
-    double acc[3][NP];
+    R fr[3] = {R(0), R(0), R(0)}, gr[3] = {R(0), R(0), R(0)};
+    R accr[3][NP];
 #pragma unroll
     for (int c = 0; c < 3; c++)
 #pragma unroll
-        for (int q = 0; q < NP; q++) acc[c][q] = 0.0;
-    double thq = 0.0;
+        for (int q = 0; q < NP; q++) accr[c][q] = R(0);
+    R thqr = R(0);
     const int n = a.cnt[i];
     const int *row = a.rows + (size_t)i * a.cap;
     // Pair terms of one row entry within the cutoff (displacement d, own atom to j).
-    auto pair = [&](const int j, const double dx, const double dy, const double dz,
-                    const double r2) {
+    auto pair = [&](const int j, const R dx, const R dy, const R dz, const R r2) {
         const int kb = site_kind(j, a.nw3);
-        const double rinv = xrsqrt(r2);
-        const double r = __dmul_rn(r2, rinv);
-        const double invr2 = __dmul_rn(rinv, rinv);
-        double F = 0.0, dF = 0.0, Fc = 0.0;
+        const R rinv = xrsqrt(r2);
+        const R r = xmul(r2, rinv);
+        const R invr2 = xmul(rinv, rinv);
+        R F = R(0), dF = R(0), Fc = R(0);
         const bool coul = ka != 2 && kb != 2;
         if (coul) {
             const int qi = (ka == 1) + (kb == 1);
-            const double qq = qi == 0 ? k.qq[0] : qi == 1 ? k.qq[1] : k.qq[2];
-            Fc = __dmul_rn(qq, __dsub_rn(invr2, __dmul_rn(k.krf2, r)));
+            const R qq = qi == 0 ? k.qq[0] : qi == 1 ? k.qq[1] : k.qq[2];
+            Fc = xmul(qq, xsub(invr2, xmul(k.krf2, r)));
             F = Fc;
-            if (REV) dF = -__dmul_rn(__dadd_rn(qq, qq), __dadd_rn(__dmul_rn(invr2, rinv), k.krf));
+            if (REV) dF = -xmul(xadd(qq, qq), xadd(xmul(invr2, rinv), k.krf));
         }
-        double gf[4] = {0.0, 0.0, 0.0, 0.0};
+        R gf[4] = {R(0), R(0), R(0), R(0)};
         int cls = -1;
         if (ka != 1 && kb != 1) {
             cls = (ka == 2) + (kb == 2);
             if (cls == 0 ? k.on[0] : cls == 1 ? k.on[1] : k.on[2]) {
                 // constant class indices keep the constants in the parameter bank
-                double Ff = 0.0, dFf = 0.0;
+                R Ff = R(0), dFf = R(0);
                 if (cls == 0)
-                    pair_form<double, FORM, REV>(k.fc[0], r, rinv, invr2, Ff, dFf, gf);
+                    pair_form<R, FORM, REV>(k.fc[0], r, rinv, invr2, Ff, dFf, gf);
                 else if (cls == 1)
-                    pair_form<double, FORM, REV>(k.fc[1], r, rinv, invr2, Ff, dFf, gf);
+                    pair_form<R, FORM, REV>(k.fc[1], r, rinv, invr2, Ff, dFf, gf);
                 else
-                    pair_form<double, FORM, REV>(k.fc[2], r, rinv, invr2, Ff, dFf, gf);
-                F = __dadd_rn(F, Ff);
-                if (REV) dF = __dadd_rn(dF, dFf);
+                    pair_form<R, FORM, REV>(k.fc[2], r, rinv, invr2, Ff, dFf, gf);
+                F = xadd(F, Ff);
+                if (REV) dF = xadd(dF, dFf);
             } else {
                 cls = -1;
             }
         }
-        const double Fr = __dmul_rn(F, rinv);
-        f[0] = __fma_rn(-Fr, dx, f[0]);
-        f[1] = __fma_rn(-Fr, dy, f[1]);
-        f[2] = __fma_rn(-Fr, dz, f[2]);
+        const R Fr = xmul(F, rinv);
+        fr[0] = xfma(-Fr, dx, fr[0]);
+        fr[1] = xfma(-Fr, dy, fr[1]);
+        fr[2] = xfma(-Fr, dz, fr[2]);
         if (REV) {
-            const double4 wb = a.wgt_in[j];
-            const double ex = __dsub_rn(wb.x, wa.x), ey = __dsub_rn(wb.y, wa.y),
-                         ez = __dsub_rn(wb.z, wa.z);
-            const double s = __dmul_rn(rinv, __fma_rn(dz, ez, __fma_rn(dy, ey, __dmul_rn(dx, ex))));
-            const double k1 = __dmul_rn(__dmul_rn(__dsub_rn(dF, Fr), s), rinv);
-            g[0] = __dsub_rn(g[0], __fma_rn(k1, dx, __dmul_rn(Fr, ex)));
-            g[1] = __dsub_rn(g[1], __fma_rn(k1, dy, __dmul_rn(Fr, ey)));
-            g[2] = __dsub_rn(g[2], __fma_rn(k1, dz, __dmul_rn(Fr, ez)));
-            const double na = __dmul_rn(rinv, __fma_rn(dz, ca[2], __fma_rn(dy, ca[1], __dmul_rn(dx, ca[0]))));
-            if (coul) thq = __fma_rn(-__dmul_rn(Fc, k.twoinvq), na, thq);
+            const V4 wb = wgt_in[j];
+            const R ex = xsub(wb.x, wa.x), ey = xsub(wb.y, wa.y),
+                         ez = xsub(wb.z, wa.z);
+            const R s = xmul(rinv, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
+            const R k1 = xmul(xmul(xsub(dF, Fr), s), rinv);
+            gr[0] = xsub(gr[0], xfma(k1, dx, xmul(Fr, ex)));
+            gr[1] = xsub(gr[1], xfma(k1, dy, xmul(Fr, ey)));
+            gr[2] = xsub(gr[2], xfma(k1, dz, xmul(Fr, ez)));
+            const R na = xmul(rinv, xfma(dz, ca[2], xfma(dy, ca[1], xmul(dx, ca[0]))));
+            if (coul) thqr = xfma(-xmul(Fc, k.twoinvq), na, thqr);
 #pragma unroll
             for (int c = 0; c < 3; c++)
                 if (c == cls)
 #pragma unroll
-                    for (int q = 0; q < NP; q++) acc[c][q] = __fma_rn(-gf[q], na, acc[c][q]);
+                    for (int q = 0; q < NP; q++) accr[c][q] = xfma(-gf[q], na, accr[c][q]);
         }
         };
     // Two phases per warp.  Phase 1: each lane loads GAS_U row entries (all loads issued
@@ -205,14 +226,14 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
     // lanes evaluate one each, so the pair arithmetic runs with full warps.  The queue is
     // processed last-in first-out in a fixed order (deterministic sums).
     constexpr int GAS_U = 4, QCAP = 32 * GAS_U + 32;
-    __shared__ double s_d[kWarpsPerCta][4][QCAP];
+    __shared__ R s_d[kWarpsPerCta][4][QCAP];
     __shared__ int s_j[kWarpsPerCta][QCAP];
     const int w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     int qn = 0;
     for (int base = 0; base < n; base += 32 * GAS_U) {
         int jj[GAS_U];
-        double4 pb[GAS_U];
+        V4 pb[GAS_U];
 #pragma unroll
         for (int u = 0; u < GAS_U; u++) {
             const int e = base + 32 * u + lane;
@@ -220,16 +241,16 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
         }
 #pragma unroll
         for (int u = 0; u < GAS_U; u++)
-            if (jj[u] >= 0) pb[u] = a.pos_in[jj[u]];
+            if (jj[u] >= 0) pb[u] = pos_in[jj[u]];
 #pragma unroll
         for (int u = 0; u < GAS_U; u++) {
             bool ok = false;
-            double dx = 0.0, dy = 0.0, dz = 0.0, r2 = 0.0;
+            R dx = R(0), dy = R(0), dz = R(0), r2 = R(0);
             if (jj[u] >= 0) {
-                dx = vec_mi(pa.x, pb[u].x, a.L, a.invL);
-                dy = vec_mi(pa.y, pb[u].y, a.L, a.invL);
-                dz = vec_mi(pa.z, pb[u].z, a.L, a.invL);
-                r2 = __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+                dx = vec_mi<R>(pa.x, pb[u].x, L, invL);
+                dy = vec_mi<R>(pa.y, pb[u].y, L, invL);
+                dz = vec_mi<R>(pa.z, pb[u].z, L, invL);
+                r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
                 ok = r2 <= k.rc2;
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -252,17 +273,22 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
         __syncwarp();
     }
     if (lane < qn) pair(s_j[w][lane], s_d[w][0][lane], s_d[w][1][lane], s_d[w][2][lane], s_d[w][3][lane]);
+    double f[3], g[3] = {0.0, 0.0, 0.0}, acc[3][NP], thq = 0.0;
 #pragma unroll
     for (int u = 0; u < 3; u++) {
-        f[u] = wsum(f[u]);
-        if (REV) g[u] = wsum(g[u]);
+        f[u] = wsum((double)fr[u]);
+        if (REV) g[u] = wsum((double)gr[u]);
     }
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int q = 0; q < NP; q++) acc[c][q] = 0.0;
     if (REV) {
-        thq = wsum(thq);
+        thq = wsum((double)thqr);
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
-            for (int q = 0; q < NP; q++) acc[c][q] = wsum(acc[c][q]);
+            for (int q = 0; q < NP; q++) acc[c][q] = wsum((double)accr[c][q]);
     }
     if (lane != 0) return;
 
@@ -272,12 +298,12 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
         double xm[9], w9[9], ac9[9], Fb[9], Gb[9], tb[4];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            const double4 p = a.pos_in[m0 + q];
+            const double4 p = a.pos64_in[m0 + q];
             xm[3 * q] = p.x;
             xm[3 * q + 1] = p.y;
             xm[3 * q + 2] = p.z;
-            double4 w = make_double4(0.0, 0.0, 0.0, 0.0);
-            if (REV) w = a.wgt_in[m0 + q];
+            V4 w = mk4<V4>(0.0, 0.0, 0.0);
+            if (REV) w = wgt_in[m0 + q];
             w9[3 * q] = w.x;
             w9[3 * q + 1] = w.y;
             w9[3 * q + 2] = w.z;
@@ -291,11 +317,11 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
         }
     } else {
         const int p = ((i - a.nw3) ^ 1) + a.nw3;
-        const double4 pp = a.pos_in[p];
-        const double d[3] = {vec1d(pa.x, pp.x, a.L), vec1d(pa.y, pp.y, a.L), vec1d(pa.z, pp.z, a.L)};
+        const double4 pp = a.pos64_in[p], po = a.pos64_in[i];
+        const double d[3] = {vec1d(po.x, pp.x, a.L), vec1d(po.y, pp.y, a.L), vec1d(po.z, pp.z, a.L)};
         double wo[3] = {0.0, 0.0, 0.0}, wp[3] = {0.0, 0.0, 0.0};
         if (REV) {
-            const double4 w = a.wgt_in[p];
+            const V4 w = wgt_in[p];
             wo[0] = wa.x; wo[1] = wa.y; wo[2] = wa.z;
             wp[0] = w.x; wp[1] = w.y; wp[2] = w.z;
         }
@@ -345,7 +371,8 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
             a.x[b + u] = x;
             xn[u] = x;
         }
-        a.pos_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
+        static_cast<V4 *>(a.pos_out)[i] = mk4<V4>(xn[0], xn[1], xn[2]);
+        a.pos64_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
         return;
     }
     // reverse part 2 (diffusion.jl:1580-1586) and, fused, part 1 of the next step (1566-1572)
@@ -380,11 +407,13 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
         a.v[e] = v;
     }
     if (fuse) {
-        a.pos_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
-        a.wgt_out[i] = make_double4(Cm[0], Cm[1], Cm[2], 0.0);
+        static_cast<V4 *>(a.pos_out)[i] = mk4<V4>(xn[0], xn[1], xn[2]);
+        a.pos64_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
+        static_cast<V4 *>(a.wgt_out)[i] = mk4<V4>(Cm[0], Cm[1], Cm[2]);
     }
 }
 
+template <typename V4>
 __global__ void k_gas_part1(const GasArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.N) return;
@@ -413,22 +442,27 @@ __global__ void k_gas_part1(const GasArgs a) {
         xn[u] = x;
         Cm[u] = __ddiv_rn(C, ma);
     }
-    a.pos_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
-    a.wgt_out[i] = make_double4(Cm[0], Cm[1], Cm[2], 0.0);
+    static_cast<V4 *>(a.pos_out)[i] = mk4<V4>(xn[0], xn[1], xn[2]);
+    a.pos64_out[i] = make_double4(xn[0], xn[1], xn[2], 0.0);
+    static_cast<V4 *>(a.wgt_out)[i] = mk4<V4>(Cm[0], Cm[1], Cm[2]);
 }
 
-__global__ void k_gas_pack(int N, const double *x, double4 *pos) {
+template <typename V4>
+__global__ void k_gas_pack(int N, const double *x, V4 *pos, double4 *pos64) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    pos[i] = make_double4(x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2], 0.0);
+    const double4 p = ld3(x, i);
+    pos[i] = mk4<V4>(p.x, p.y, p.z);
+    pos64[i] = p;
 }
 
-__global__ void k_gas_pack_w(int N, int nw3, const double *w, double mO, double mH, double4 *wgt) {
+template <typename V4>
+__global__ void k_gas_pack_w(int N, int nw3, const double *w, double mO, double mH, V4 *wgt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const double m = site_kind(i, nw3) == 1 ? mH : mO;
     const size_t b = 3 * (size_t)i;
-    wgt[i] = make_double4(__ddiv_rn(w[b], m), __ddiv_rn(w[b + 1], m), __ddiv_rn(w[b + 2], m), 0.0);
+    wgt[i] = mk4<V4>(__ddiv_rn(w[b], m), __ddiv_rn(w[b + 1], m), __ddiv_rn(w[b + 2], m));
 }
 
 __global__ void k_gas_reset(int n3, const double *g, double f1, double f2, double f3, double *A,
@@ -458,7 +492,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_energy(const GasConsts k, cons
     const int i = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
     if (i >= a.N) return;
     const int ka = site_kind(i, a.nw3);
-    const double4 pa = a.pos_in[i];
+    const double4 pa = ld3(a.x, i);
     double E = 0.0, eq = 0.0;
     double acc[3][NP];
 #pragma unroll
@@ -470,7 +504,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_energy(const GasConsts k, cons
     for (int e = lane; e < n; e += 32) {
         const int j = row[e];
         if (j <= i) continue;
-        const double4 pb = a.pos_in[j];
+        const double4 pb = ld3(a.x, j);
         const double d0 = vec1d(pa.x, pb.x, a.L), d1 = vec1d(pa.y, pb.y, a.L), d2 = vec1d(pa.z, pb.z, a.L);
         const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
         if (!(r2 <= k.rc2)) continue;
@@ -507,7 +541,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_energy(const GasConsts k, cons
         double x[9];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            const double4 p = a.pos_in[i + q];
+            const double4 p = ld3(a.x, i + q);
             x[3 * q] = p.x;
             x[3 * q + 1] = p.y;
             x[3 * q + 2] = p.z;
@@ -526,7 +560,7 @@ __global__ void __launch_bounds__(kThreads) k_gas_energy(const GasConsts k, cons
         const double th = acos(cth) - a.bw.th0;
         E += 0.5 * a.bw.ka * th * th;
     } else if (ka == 2 && ((i - a.nw3) & 1) == 0) {
-        const double4 pp = a.pos_in[i + 1];
+        const double4 pp = ld3(a.x, i + 1);
         const double d0 = vec1d(pa.x, pp.x, a.L), d1 = vec1d(pa.y, pp.y, a.L), d2 = vec1d(pa.z, pp.z, a.L);
         const double bl = sqrt(d0 * d0 + d1 * d1 + d2 * d2) - a.r0_g;
         E += 0.5 * a.kb_g * bl * bl;
@@ -568,14 +602,14 @@ __global__ void __launch_bounds__(256) k_gas_esum(int N, int P, const double *ep
     }
 }
 
-template <bool REV>
-void step_form(int form, const GasConsts &k, const GasArgs &a, dim3 grid, cudaStream_t st) {
+template <typename R, bool REV>
+void step_form(int form, const GasConstsT<R> &k, const GasArgs &a, dim3 grid, cudaStream_t st) {
     switch (form) {
-        case F_LJ: k_gas_step<F_LJ, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_DEXP: k_gas_step<F_DEXP, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_BUCK: k_gas_step<F_BUCK, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_LJSC: k_gas_step<F_LJSC, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_BUFF: k_gas_step<F_BUFF, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_LJ: k_gas_step<R, F_LJ, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_DEXP: k_gas_step<R, F_DEXP, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_BUCK: k_gas_step<R, F_BUCK, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_LJSC: k_gas_step<R, F_LJSC, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_BUFF: k_gas_step<R, F_BUFF, REV><<<grid, kThreads, 0, st>>>(k, a); break;
     }
 }
 
@@ -586,25 +620,42 @@ void launch_gas_rows(const GasRowArgs &a, cudaStream_t st) {
     k_gas_rows<<<grid, kThreads, 0, st>>>(a);
 }
 
-void launch_gas_step(int form, bool rev, const GasConsts &k, const GasArgs &a, cudaStream_t st) {
+void launch_gas_step(bool mixed, int form, bool rev, const GasConstsT<float> &kf,
+                     const GasConstsT<double> &kd, const GasArgs &a, cudaStream_t st) {
     const dim3 grid((a.N + kWarpsPerCta - 1) / kWarpsPerCta);
-    if (rev)
-        step_form<true>(form, k, a, grid, st);
+    if (mixed) {
+        if (rev)
+            step_form<float, true>(form, kf, a, grid, st);
+        else
+            step_form<float, false>(form, kf, a, grid, st);
+    } else {
+        if (rev)
+            step_form<double, true>(form, kd, a, grid, st);
+        else
+            step_form<double, false>(form, kd, a, grid, st);
+    }
+}
+
+void launch_gas_part1(bool mixed, const GasArgs &a, cudaStream_t st) {
+    if (mixed)
+        k_gas_part1<float4><<<(a.N + 127) / 128, 128, 0, st>>>(a);
     else
-        step_form<false>(form, k, a, grid, st);
+        k_gas_part1<double4><<<(a.N + 127) / 128, 128, 0, st>>>(a);
 }
 
-void launch_gas_part1(const GasArgs &a, cudaStream_t st) {
-    k_gas_part1<<<(a.N + 127) / 128, 128, 0, st>>>(a);
+void launch_gas_pack(bool mixed, int N, const double *x, void *pos, double4 *pos64, cudaStream_t st) {
+    if (mixed)
+        k_gas_pack<float4><<<(N + 127) / 128, 128, 0, st>>>(N, x, static_cast<float4 *>(pos), pos64);
+    else
+        k_gas_pack<double4><<<(N + 127) / 128, 128, 0, st>>>(N, x, static_cast<double4 *>(pos), pos64);
 }
 
-void launch_gas_pack(int N, const double *x, double4 *pos, cudaStream_t st) {
-    k_gas_pack<<<(N + 127) / 128, 128, 0, st>>>(N, x, pos);
-}
-
-void launch_gas_pack_w(int N, int nw3, const double *w, double mO, double mH, double4 *wgt,
+void launch_gas_pack_w(bool mixed, int N, int nw3, const double *w, double mO, double mH, void *wgt,
                        cudaStream_t st) {
-    k_gas_pack_w<<<(N + 127) / 128, 128, 0, st>>>(N, nw3, w, mO, mH, wgt);
+    if (mixed)
+        k_gas_pack_w<float4><<<(N + 127) / 128, 128, 0, st>>>(N, nw3, w, mO, mH, static_cast<float4 *>(wgt));
+    else
+        k_gas_pack_w<double4><<<(N + 127) / 128, 128, 0, st>>>(N, nw3, w, mO, mH, static_cast<double4 *>(wgt));
 }
 
 void launch_gas_reset(int n3, const double *g, double f1, double f2, double f3, double *A,

@@ -123,7 +123,7 @@ class GasDesc(ctypes.Structure):
         ("nl_cutoff", ctypes.c_double), ("n_steps_nf", ctypes.c_int32), ("kB", ctypes.c_double),
         ("kb_w", ctypes.c_double), ("r0_w", ctypes.c_double), ("ka_w", ctypes.c_double),
         ("th0_w", ctypes.c_double), ("kb_g", ctypes.c_double), ("r0_g", ctypes.c_double),
-        ("n_mol_ev", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("n_mol_ev", ctypes.c_int32), ("device", ctypes.c_int32), ("precision", ctypes.c_int32),
     ]
 
 

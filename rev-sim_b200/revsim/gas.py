@@ -41,11 +41,15 @@ def loss_bits(loss_type):
 class GasEngine:
     """One gas-in-water system on one GPU."""
 
-    def __init__(self, n_water, n_gas, box, inter_type="lj", temp=C.TEMP, device=0, **consts):
+    def __init__(self, n_water, n_gas, box, inter_type="lj", temp=C.TEMP, device=0,
+                 precision="fp64", **consts):
+        """precision: "fp64", or "mixed" for FP32 pair arithmetic (state, bonded terms,
+        integrator, adjoints and sums stay FP64)."""
         self._h = None
         self._L = load()
         d = GasDesc()
         d.n_water, d.n_gas, d.box = int(n_water), int(n_gas), float(box)
+        d.precision = {"fp64": 0, "mixed": 1}[precision]
         d.inter_type = INTER[inter_type] if isinstance(inter_type, str) else int(inter_type)
         d.temp = float(temp)
         d.device = int(device)

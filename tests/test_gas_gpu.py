@@ -195,3 +195,29 @@ def test_rdf_term_matches_oracle(loss_type):
     scale = np.abs(dpo * p).max()
     assert np.all(np.abs((g - dpo) * p) <= 1e-7 * scale), (g, dpo)
     e.close()
+
+
+@pytest.mark.parametrize("form", ["lj", "buck"])
+def test_mixed_precision_forces_and_gradient(form):
+    """Mixed precision (FP32 pair arithmetic; FP64 state, bonded terms, integrator, adjoints
+    and sums) against the FP64 oracle: forces to FP32 rounding, the reconstruction to FP64
+    state rounding, the reverse gradient to 1e-3 of its largest component."""
+    s, p, x0, v0 = relaxed_gas(80, 5, 2.5, form, seed=4, steps=30)
+    e = GasEngine(s.n_water, s.n_gas, s.box, form, precision="mixed")
+    e.set_params(p)
+    e.set_state(x0, v0)
+    assert _rel(e.forces(), orc.gas_forces(s, p, x0)) < 2e-5
+    n, nl = 40, 10
+    seeds = systems.noise_seeds(n, seed=26)
+    xf, vf, lfo, sx, sv, gc, _ = orc.gas_forward_sim(s, p, x0, v0, seeds, 1.0, n, nl, 0.001, "diff_ev")
+    _, _, lro, dpo, _ = orc.gas_reverse_sim(s, p, xf, vf, seeds, 1.0, n, nl, nl, 0.001, sx, sv, gc, "diff_ev")
+    lf, _, _ = e.forward(seeds, 1.0, n, nl, 0.001, "diff_ev")
+    lr, g, _ = e.reverse(seeds, 1.0, n, nl, nl, 0.001, "diff_ev")
+    xr, _ = e.get_state()
+    d = xr - x0
+    d -= s.box * np.round(d / s.box)
+    assert np.abs(d).max() < 1e-6 and abs(lr - lf) < 1e-7
+    assert abs(lf - lfo) <= 1e-3 * abs(lfo)
+    scale = np.abs(dpo * p).max()
+    assert np.all(np.abs((g - dpo) * p) <= 1e-3 * scale), (g, dpo)
+    e.close()
