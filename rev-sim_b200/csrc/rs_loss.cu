@@ -8,8 +8,8 @@
 // The loss (loss_rdf_part, water.jl:693-697) compares a strided slice of h with a
 // target; the gradient is the analytic derivative of the same windowed sums (the
 // quantity Enzyme differentiates in the reference's pullback, water.jl:715-736).
-// Runs once per loss block, so it is written for clarity: one thread per ordered
-// atom pair, shared-memory histogram, FP64 throughout.
+// One thread per ordered atom pair, shared-memory histogram, FP64 throughout; the window's
+// Gaussians by a two-multiplication recurrence re-anchored on exp every 16 points.
 #include <cmath>
 #include <mutex>
 
@@ -51,15 +51,41 @@ __device__ __forceinline__ void hist_window(const RdfArgs &a, double d, int &lo,
     hi = h;
 }
 
-__device__ __forceinline__ void den_sums(const RdfArgs &a, double d, double &den, double &dden) {
+// The Gaussians g_k = exp(-(x_k - d)^2 / width) of consecutive grid points by the recurrence
+// g_{k+1} = g_k r_k, r_{k+1} = r_k q with r_k = exp(-(2 e_k step + step^2) / width) and
+// q = exp(-2 step^2 / width): two multiplications per point instead of an exp.  The
+// recurrence restarts from exp every kGaussAnchor points, which bounds the accumulated
+// rounding at about kGaussAnchor^2 / 2 ulp (~1e-14 relative).
+constexpr int kGaussAnchor = 16;
+
+struct Gauss {
+    double g, r;
+};
+
+__device__ __forceinline__ void gauss_anchor(const RdfArgs &a, double d, int k, double inv_w,
+                                             Gauss &G) {
+    const double e = __dsub_rn(grid_x(a, k), d);
+    G.g = exp(-__dmul_rn(__dmul_rn(e, e), inv_w));
+    G.r = exp(-__dmul_rn(__fma_rn(__dmul_rn(2.0, e), a.step, __dmul_rn(a.step, a.step)), inv_w));
+}
+
+__device__ __forceinline__ void gauss_next(Gauss &G, double q) {
+    G.g = __dmul_rn(G.g, G.r);
+    G.r = __dmul_rn(G.r, q);
+}
+
+__device__ __forceinline__ void den_sums(const RdfArgs &a, double d, double inv_w, double q,
+                                         double &den, double &dden) {
     int lo, hi;
     den_window(a, d, lo, hi);
     double s = 0.0, ds = 0.0;
+    Gauss G{0.0, 0.0};
     for (int k = lo; k <= hi; k++) {
+        if (((k - lo) % kGaussAnchor) == 0) gauss_anchor(a, d, k, inv_w, G);
         const double e = __dsub_rn(grid_x(a, k), d);
-        const double g = exp(__ddiv_rn(-__dmul_rn(e, e), a.width));
-        s = __dadd_rn(s, g);
-        ds = __dadd_rn(ds, __ddiv_rn(__dmul_rn(__dmul_rn(g, 2.0), e), a.width));
+        s = __dadd_rn(s, G.g);
+        ds = __fma_rn(__dmul_rn(__dmul_rn(G.g, 2.0), e), inv_w, ds);
+        gauss_next(G, q);
     }
     den = s;
     dden = ds;
@@ -80,6 +106,8 @@ __global__ void k_rdf(RdfArgs a, const double *pre) {
         for (int k = threadIdx.x; k < a.n_grid; k += blockDim.x) s_hist[k] = 0.0;
         __syncthreads();
     }
+    const double inv_w = __drcp_rn(a.width);
+    const double q = exp(-__dmul_rn(__dmul_rn(2.0, __dmul_rn(a.step, a.step)), inv_w));
     const double dmin = __dsub_rn(__dsub_rn(a.x_min, a.cutoff), a.step);
     const double dmax = __dadd_rn(__dadd_rn(grid_x(a, a.n_grid - 1), a.cutoff), a.step);
     const long long total = n1 * n2;
@@ -98,27 +126,34 @@ __global__ void k_rdf(RdfArgs a, const double *pre) {
         hist_window(a, d, lo, hi);
         if (lo > hi) continue;
         double den, dden;
-        den_sums(a, d, den, dden);
+        den_sums(a, d, inv_w, q, den, dden);
+        const double inv_den = __drcp_rn(den);
+        Gauss G{0.0, 0.0};
         if (!GRAD) {
             for (int k = lo; k <= hi; k++) {
-                const double e = __dsub_rn(grid_x(a, k), d);
-                const double g = __ddiv_rn(exp(__ddiv_rn(-__dmul_rn(e, e), a.width)), den);
+                if (((k - lo) % kGaussAnchor) == 0) gauss_anchor(a, d, k, inv_w, G);
+                const double g = __dmul_rn(G.g, inv_den);
                 if (use_smem)
                     atomicAdd(s_hist + k, g);
                 else
                     atomicAdd(hist + k, g);
+                gauss_next(G, q);
             }
         } else {
             const double *dLdh = a.dLdh + (size_t)r * a.n_grid;
+            const double dd2 = __dmul_rn(dden, __dmul_rn(inv_den, inv_den));
             double dLdd = 0.0;
             for (int k = lo; k <= hi; k++) {
+                if (((k - lo) % kGaussAnchor) == 0) gauss_anchor(a, d, k, inv_w, G);
                 const double w = dLdh[k];
-                if (w == 0.0) continue;
-                const double xk = grid_x(a, k), e = __dsub_rn(xk, d);
-                const double g = exp(__ddiv_rn(-__dmul_rn(e, e), a.width));
-                const double gp = __ddiv_rn(__dmul_rn(__dmul_rn(g, 2.0), e), a.width);
-                const double t = __dsub_rn(__ddiv_rn(gp, den), __ddiv_rn(__dmul_rn(g, dden), __dmul_rn(den, den)));
-                dLdd = __dadd_rn(dLdd, __dmul_rn(__ddiv_rn(__dmul_rn(w, pre[r]), __dmul_rn(xk, xk)), t));
+                if (w != 0.0) {
+                    const double xk = grid_x(a, k), e = __dsub_rn(xk, d);
+                    const double g = G.g;
+                    const double gp = __dmul_rn(__dmul_rn(__dmul_rn(g, 2.0), e), inv_w);
+                    const double t = __dsub_rn(__dmul_rn(gp, inv_den), __dmul_rn(g, dd2));
+                    dLdd = __dadd_rn(dLdd, __dmul_rn(__ddiv_rn(__dmul_rn(w, pre[r]), __dmul_rn(xk, xk)), t));
+                }
+                gauss_next(G, q);
             }
             if (dLdd != 0.0) {
 #pragma unroll
