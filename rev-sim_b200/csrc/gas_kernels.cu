@@ -136,6 +136,7 @@ template <typename R, int FORM, bool REV>
 __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_step(const GasConstsT<R> k, const GasArgs a) {
     using V4 = typename V4T<R>::T;
     constexpr int NP = FormInfo<FORM>::NP;
+    chain_enter();
     const V4 *pos_in = static_cast<const V4 *>(a.pos_in);
     const V4 *wgt_in = static_cast<const V4 *>(a.wgt_in);
     const R L = (R)a.L, invL = (R)a.invL;
@@ -605,11 +606,11 @@ __global__ void __launch_bounds__(256) k_gas_esum(int N, int P, const double *ep
 template <typename R, bool REV>
 void step_form(int form, const GasConstsT<R> &k, const GasArgs &a, dim3 grid, cudaStream_t st) {
     switch (form) {
-        case F_LJ: k_gas_step<R, F_LJ, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_DEXP: k_gas_step<R, F_DEXP, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_BUCK: k_gas_step<R, F_BUCK, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_LJSC: k_gas_step<R, F_LJSC, REV><<<grid, kThreads, 0, st>>>(k, a); break;
-        case F_BUFF: k_gas_step<R, F_BUFF, REV><<<grid, kThreads, 0, st>>>(k, a); break;
+        case F_LJ: launch_chained(k_gas_step<R, F_LJ, REV>, grid, dim3(kThreads), 0, st, k, a); break;
+        case F_DEXP: launch_chained(k_gas_step<R, F_DEXP, REV>, grid, dim3(kThreads), 0, st, k, a); break;
+        case F_BUCK: launch_chained(k_gas_step<R, F_BUCK, REV>, grid, dim3(kThreads), 0, st, k, a); break;
+        case F_LJSC: launch_chained(k_gas_step<R, F_LJSC, REV>, grid, dim3(kThreads), 0, st, k, a); break;
+        case F_BUFF: launch_chained(k_gas_step<R, F_BUFF, REV>, grid, dim3(kThreads), 0, st, k, a); break;
     }
 }
 

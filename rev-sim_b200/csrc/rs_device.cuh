@@ -18,6 +18,18 @@ constexpr int ST_NAN = 2;
 constexpr int ST_GEOMETRY = 4;
 constexpr int ST_CELL_OVERFLOW = 8;
 
+// ---------------------------------------------------------------- launch chaining
+// Programmatic dependent launch of consecutive step kernels: a kernel launched with
+// programmatic stream serialisation (launch_chained) waits here until the previous kernel in
+// the stream has completed and its writes are visible, and then lets the next step kernel
+// be scheduled, so that its CTAs become resident while this one runs and wait at the same
+// point.  Called first, by every thread, before any read of device state or any write.
+// Without the launch attribute both instructions return at once.
+__device__ __forceinline__ void chain_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- arithmetic
 __device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }

@@ -3,11 +3,42 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdlib>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "rs_device.cuh"
 
 namespace rs {
+
+// Step kernels are launched chained (programmatic dependent launch; the kernel side is
+// chain_enter) unless REVSIM_CHAIN=0 is set in the environment when the library first
+// launches one.
+inline bool chain_on() {
+    static const bool on = [] {
+        const char *e = std::getenv("REVSIM_CHAIN");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// Launch of a kernel whose first statement is chain_enter(): with programmatic stream
+// serialisation, so that it may be scheduled while the previous kernel in the stream runs.
+template <typename... P, typename... A>
+cudaError_t launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t st, A &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = chain_on() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 // Learned pair correction (rs_mlp.cu): 16 radial basis functions -> 64 -> 64 SiLU -> 1
 // per element pair (O-O, O-H, H-H), tabulated on MLP_NG intervals of [0, cutoff].

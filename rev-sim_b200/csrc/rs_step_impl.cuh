@@ -450,6 +450,7 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     // dynamic shared memory: [groups][P] dtheta (double), [groups] |dl_dfi|^2 (double),
     // then [groups][22] bonded results (R): forces (9), VJP (9), dtheta (4)
     extern __shared__ double s_th[];
+    chain_enter();
 
     const int grp = threadIdx.x / G;
     const int lane = threadIdx.x % G;
@@ -666,10 +667,10 @@ cudaError_t launch_one(bool rev, int n_blk, int threads, const StepArgs &a, cons
     const int ngrp = threads / G;
     const size_t smem = sizeof(double) * (size_t)ngrp * (a.P + 1) + sizeof(R) * 22 * (size_t)ngrp;
     if (rev)
-        k_water_step<R, FORM, G, true, SHIFT, U><<<n_blk, threads, smem, st>>>(a, nb, bc);
-    else
-        k_water_step<R, FORM, G, false, SHIFT, U><<<n_blk, threads, smem, st>>>(a, nb, bc);
-    return cudaGetLastError();
+        return launch_chained(k_water_step<R, FORM, G, true, SHIFT, U>, dim3(n_blk), dim3(threads), smem,
+                              st, a, nb, bc);
+    return launch_chained(k_water_step<R, FORM, G, false, SHIFT, U>, dim3(n_blk), dim3(threads), smem, st,
+                          a, nb, bc);
 }
 
 template <typename R, int FORM, int G, bool SHIFT>
