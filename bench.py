@@ -420,7 +420,10 @@ def run_ours(a):
                 "shape": {"reverse": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[0])),
                           "forward": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[1]))},
                 "forward_step_launch_ms": ft_ms / max(ft_n, 1),
-                "step_kernels_share_of_gradient": (kt_ms + ft_ms) / ms_step}
+                "step_kernels_share_of_gradient": (kt_ms + ft_ms) / ms_step,
+                "launch_ms_note": "per-launch times come from a pass with events between the "
+                                  "launches, which breaks the launch chaining of the timed "
+                                  "gradient, so they include the launch gap the chain hides"}
 
     extra = {}
     if not a.no_compare and rank == 0:
