@@ -293,6 +293,20 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
     }
     if (lane != 0) return;
 
+    // Every load of the atom's state is issued before its first store: the state arrays
+    // are distinct, but the compiler cannot know that and would otherwise serialise the
+    // three components behind the stores.  Forward: x and v, before the bonded terms.
+    const size_t b = 3 * (size_t)i;
+    const bool upd = !(a.mode & MODE_FORCES_ONLY);
+    double xk[3] = {0.0, 0.0, 0.0}, vk[3] = {0.0, 0.0, 0.0};
+    if (!REV && upd) {
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            vk[u] = a.v[b + u];
+            xk[u] = a.x[b + u];
+        }
+    }
+
     // bonded terms of the atom's molecule (diffusion.jl:997-1050, 1367-1498)
     if (ka != 2) {
         const int m0 = i - i % 3, kk = i % 3;
@@ -331,22 +345,28 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
     if (!isfinite(f[0]) || !isfinite(f[1]) || !isfinite(f[2])) atomicOr(a.status, ST_NAN);
 
     if (REV) {
-        double th[kMaxP];
-#pragma unroll
-        for (int p = 0; p < kMaxP; p++) th[p] = 0.0;
-#pragma unroll
-        for (int q = 0; q < NP; q++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                th[k.iw[q]] = __fma_rn(k.fw[c][q], acc[c][q], th[k.iw[q]]);
-                if (k.ig[q] >= 0) th[k.ig[q]] = __fma_rn(k.fg[c][q], acc[c][q], th[k.ig[q]]);
-            }
-        th[k.iq] = __dadd_rn(th[k.iq], thq);
+        // dtheta of the atom: each parameter's contributions in (q, class) order, then the
+        // charge term, with compile-time parameter indices so that the sums stay in
+        // registers; the partials' loads all issued before their stores
         double *pt = a.part + (size_t)i * k.P;
-        for (int p = 0; p < k.P; p++) pt[p] = __dadd_rn(pt[p], th[p]);
+        double old[kMaxP];
+#pragma unroll
+        for (int p = 0; p < kMaxP; p++) old[p] = p < k.P ? pt[p] : 0.0;
+#pragma unroll
+        for (int p = 0; p < kMaxP; p++) {
+            double t = 0.0;
+#pragma unroll
+            for (int q = 0; q < NP; q++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    if (k.iw[q] == p) t = __fma_rn(k.fw[c][q], acc[c][q], t);
+                    if (k.ig[q] == p) t = __fma_rn(k.fg[c][q], acc[c][q], t);
+                }
+            if (k.iq == p) t = __dadd_rn(t, thq);
+            if (p < k.P) pt[p] = __dadd_rn(old[p], t);
+        }
     }
-    const size_t b = 3 * (size_t)i;
-    if (a.mode & MODE_FORCES_ONLY) {
+    if (!upd) {
 #pragma unroll
         for (int u = 0; u < 3; u++) {
             a.F_out[b + u] = f[u];
@@ -362,7 +382,7 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
         double xn[3];
 #pragma unroll
         for (int u = 0; u < 3; u++) {
-            double v = a.v[b + u], x = a.x[b + u];
+            double v = vk[u], x = xk[u];
             v = __dadd_rn(v, __ddiv_rn(__dmul_rn(f[u], a.dt), ma));
             x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
             v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
@@ -379,6 +399,18 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
     // reverse part 2 (diffusion.jl:1580-1586) and, fused, part 1 of the next step (1566-1572)
     const double dt2 = __dmul_rn(a.dt, a.dt);
     const bool fuse = (a.mode & MODE_FUSE_NEXT) != 0;
+    double Bk[3], Ak[3], Dk[3] = {0.0, 0.0, 0.0}, Ck[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        vk[u] = a.v[b + u];
+        Bk[u] = a.B[b + u];
+        Ak[u] = a.A[b + u];
+        if (fuse) {
+            xk[u] = a.x[b + u];
+            Dk[u] = a.D[b + u];
+            Ck[u] = a.C[b + u];
+        }
+    }
     double xi[3] = {0.0, 0.0, 0.0};
     if (fuse && a.s != 0.0) atom_noise(a.seed_next, (uint32_t)i, sd, xi);
     double xn[3], Cm[3];
@@ -386,19 +418,19 @@ __global__ void __launch_bounds__(kThreads, gas_min_blocks<FORM, REV>()) k_gas_s
     for (int u = 0; u < 3; u++) {
         const size_t e = b + u;
         a.G[e] = g[u];
-        double v = __dsub_rn(a.v[e], __ddiv_rn(__dmul_rn(f[u], a.dt), ma));
-        const double B = __dadd_rn(__dmul_rn(a.c, a.B[e]), __dmul_rn(dt2, g[u]));
+        double v = __dsub_rn(vk[u], __ddiv_rn(__dmul_rn(f[u], a.dt), ma));
+        const double B = __dadd_rn(__dmul_rn(a.c, Bk[u]), __dmul_rn(dt2, g[u]));
         a.B[e] = B;
-        a.A[e] = __dadd_rn(a.A[e], B);
+        a.A[e] = __dadd_rn(Ak[u], B);
         if (fuse) {
-            double x = a.x[e];
+            double x = xk[u];
             x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
             v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
             x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
             x = wrap1d(x, a.L);
-            const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
+            const double D = __dadd_rn(__dmul_rn(a.c, Dk[u]),
                                        __ddiv_rn(__dmul_rn(__dmul_rn(dt2, g[u]), __dadd_rn(1.0, a.c)), 2.0));
-            const double C = __dadd_rn(a.C[e], D);
+            const double C = __dadd_rn(Ck[u], D);
             a.D[e] = D;
             a.C[e] = C;
             a.x[e] = x;

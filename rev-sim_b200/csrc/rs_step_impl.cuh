@@ -355,11 +355,14 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
     } else if (!REV) {
         // B-A-O-A (water.jl:1032-1037)
         const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
+        // every load before the first store: the state arrays are distinct, but the compiler
+        // cannot know that, and would otherwise serialise the three components
+        const double vk[3] = {a.v[3 * ia], a.v[3 * ia + 1], a.v[3 * ia + 2]};
         double xi[3] = {0.0, 0.0, 0.0};
         if (a.s != 0.0) atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
 #pragma unroll
         for (int u = 0; u < 3; u++) {
-            double v = a.v[3 * ia + u], x = xk[u];
+            double v = vk[u], x = xk[u];
             v = __dadd_rn(v, __ddiv_rn(__dmul_rn(F[u], a.dt), m));
             x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
             v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
@@ -374,6 +377,21 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
         const double dt2 = __dmul_rn(a.dt, a.dt);
         const bool fuse = (a.mode & MODE_FUSE_NEXT) != 0;
         const bool defer = (a.mode & MODE_DEFER_BA) != 0;
+        // every load before the first store (as in the forward branch)
+        double vk[3], Bk[3], Ak[3], Dk[3], Ck[3];
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const size_t e = 3 * ia + u;
+            vk[u] = a.v[e];
+            if (!defer) {
+                Bk[u] = a.B[e];
+                Ak[u] = a.A[e];
+            }
+            if (fuse) {
+                Dk[u] = a.D[e];
+                Ck[u] = a.C[e];
+            }
+        }
         double xi[3] = {0.0, 0.0, 0.0};
         if (fuse && a.s != 0.0) {
             const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
@@ -386,12 +404,12 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
             a.G[e] = Gv[u];
             n2 = __dadd_rn(n2, __dmul_rn(Gv[u], Gv[u]));
             // v_{n-1} = v' - F dt / m (water.jl:1516)
-            double v = __dsub_rn(a.v[e], __ddiv_rn(__dmul_rn(F[u], a.dt), m));
+            double v = __dsub_rn(vk[u], __ddiv_rn(__dmul_rn(F[u], a.dt), m));
             if (!defer) {
                 // water.jl:1520-1521
-                const double B = __dadd_rn(__dmul_rn(a.c, a.B[e]), __dmul_rn(dt2, Gv[u]));
+                const double B = __dadd_rn(__dmul_rn(a.c, Bk[u]), __dmul_rn(dt2, Gv[u]));
                 a.B[e] = B;
-                a.A[e] = __dadd_rn(a.A[e], B);
+                a.A[e] = __dadd_rn(Ak[u], B);
             }
             if (fuse) {
                 // part 1 of the next reverse step (water.jl:1496-1502)
@@ -400,11 +418,11 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
                 v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
                 x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
                 x = wrap1d(x, Ld);
-                const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
+                const double D = __dadd_rn(__dmul_rn(a.c, Dk[u]),
                                            __ddiv_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]),
                                                                __dadd_rn(1.0, a.c)),
                                                      2.0));
-                const double C = __dadd_rn(a.C[e], D);
+                const double C = __dadd_rn(Ck[u], D);
                 a.D[e] = D;
                 a.C[e] = C;
                 a.x[e] = x;
