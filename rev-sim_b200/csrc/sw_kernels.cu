@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(TERM_THREADS) k_terms(SwTermArgs t, SwConsts<R
     using V4 = typename V4T<R>::T;
     __shared__ V4 s_uh[GPB][G];
     __shared__ V4 s_ut[GPB][K > 0 ? G : 1];
+    chain_enter();
     __shared__ V4 s_ht[GPB][K > 0 ? G : 1];
     __shared__ double s_red[TERM_THREADS / 32][9];
 
@@ -616,6 +617,7 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
     // with the same bits: each level adds two equal-order pairs) gives f = dE/dx_e and
     // tg, its derivative along the tangent (H w or H u).  Lane 0 writes F = -f and
     // G = -tg; k_finish integrates.
+    chain_enter();
     const int lane = threadIdx.x % G;
     const int e = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G);
     const int gshift = (threadIdx.x % 32) / G * G;
@@ -682,6 +684,7 @@ __global__ void __launch_bounds__(256) k_gather(SwGatherArgs g) {
 // One thread per atom: the step (or loss) arithmetic after the gather.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_finish(SwGatherArgs g) {
+    chain_enter();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= g.N) return;
     double f[3], tg[3];
@@ -910,7 +913,7 @@ cudaError_t launch_sw_nlist(const SwNlArgs &a, cudaStream_t st) {
 template <typename R>
 cudaError_t launch_sw_terms(int mode, int G, int n_blk, const SwTermArgs &a, const SwConsts<R> &p,
                             cudaStream_t st) {
-#define RS_TERMS(GG, MM) k_terms<R, GG, MM><<<n_blk, TERM_THREADS, 0, st>>>(a, p)
+#define RS_TERMS(GG, MM) launch_chained(k_terms<R, GG, MM>, dim3(n_blk), dim3(TERM_THREADS), 0, st, a, p)
     if (G == 16) {
         if (mode == TM_VALUE) RS_TERMS(16, TM_VALUE);
         else if (mode == TM_REV) RS_TERMS(16, TM_REV);
@@ -931,18 +934,18 @@ cudaError_t launch_sw_gather(int mode, int G, bool tangent, const SwGatherArgs &
     const int nb = (int)(((size_t)a.N * G + 255) / 256);
     const bool tan = tangent || mode == GM_REV || mode == GM_LOSS;
     if (G == 16) {
-        if (tan) k_gather<R, 16, true><<<nb, 256, 0, st>>>(a);
-        else k_gather<R, 16, false><<<nb, 256, 0, st>>>(a);
+        if (tan) launch_chained(k_gather<R, 16, true>, dim3(nb), dim3(256), 0, st, a);
+        else launch_chained(k_gather<R, 16, false>, dim3(nb), dim3(256), 0, st, a);
     } else if (G == 32) {
-        if (tan) k_gather<R, 32, true><<<nb, 256, 0, st>>>(a);
-        else k_gather<R, 32, false><<<nb, 256, 0, st>>>(a);
+        if (tan) launch_chained(k_gather<R, 32, true>, dim3(nb), dim3(256), 0, st, a);
+        else launch_chained(k_gather<R, 32, false>, dim3(nb), dim3(256), 0, st, a);
     } else {
         return cudaErrorInvalidValue;
     }
     const int na = nblk(a.N, 256);
-    if (mode == GM_FWD) k_finish<GM_FWD><<<na, 256, 0, st>>>(a);
-    else if (mode == GM_REV) k_finish<GM_REV><<<na, 256, 0, st>>>(a);
-    else if (mode == GM_LOSS) k_finish<GM_LOSS><<<na, 256, 0, st>>>(a);
+    if (mode == GM_FWD) launch_chained(k_finish<GM_FWD>, dim3(na), dim3(256), 0, st, a);
+    else if (mode == GM_REV) launch_chained(k_finish<GM_REV>, dim3(na), dim3(256), 0, st, a);
+    else if (mode == GM_LOSS) launch_chained(k_finish<GM_LOSS>, dim3(na), dim3(256), 0, st, a);
     return cudaGetLastError();
 }
 
