@@ -123,11 +123,13 @@ __global__ void __launch_bounds__(kThreads) k_gas_rows(GasRowArgs a) {
 }
 
 // ------------------------------------------------------------------ step kernels
-// Register budget: the LJ reverse kernel at <= 128 registers (4 CTAs, 16 warps per SM; it
-// spills only in its lane-0 epilogue there); the other reverse forms (dual numbers, more
-// live values) and the forward kernels (76 registers) unconstrained.
+// Register budget: the LJ reverse kernel at 5 CTAs per SM (96 registers, some spills), so
+// that one warp per atom of the 2,675-atom diffusion box fits in one wave (at 128 registers
+// 4 CTAs per SM held 2,368 of its warps and the rest ran as a second wave: 50.7 against
+// 39.5 us per step); the other reverse forms (dual numbers, more live values) and the
+// forward kernels (90 registers, 5 CTAs per SM) unconstrained.
 template <int FORM, bool REV>
-constexpr int gas_min_blocks() { return (REV && FORM == F_LJ) ? 4 : 1; }
+constexpr int gas_min_blocks() { return (REV && FORM == F_LJ) ? 5 : 1; }
 
 // R: pair arithmetic (float in mixed precision, double in FP64).  The pair loop gathers
 // V4T<R> positions and weights; the per-lane sums are R and are combined in FP64; the
