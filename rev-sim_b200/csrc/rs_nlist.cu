@@ -11,6 +11,8 @@
 // gathers a whole molecule (3 positions) per entry and accumulates the forces of its
 // own molecule with no atomics.  Membership distances are FP64, each product and sum
 // rounded separately, exactly as the CPU restatement computes them.
+#include <algorithm>
+
 #include "rs_internal.h"
 
 namespace rs {
@@ -92,7 +94,7 @@ __global__ void k_cell_sort(NlistArgs a) {
     a.cell_sorted[s + rank] = I;
 }
 
-// Rows of every molecule of one home cell (one CTA per cell).  The CTA stages the
+// Rows of the molecules of one home cell (one to four CTAs per cell).  The CTA stages the
 // neighbourhood -- the members of the surrounding cells, in the canonical cell order
 // and index order within a cell -- with all three atoms in FP32 in shared memory, in
 // chunks of up to kRowChunk molecules.  Each warp takes one home molecule at a time:
@@ -101,7 +103,7 @@ __global__ void k_cell_sort(NlistArgs a) {
 // clearly inside / clearly outside the list cutoff, and the few pairs within `band` of
 // the cutoff are decided by the exact FP64 Molly arithmetic (dist2_fp64), so the set
 // is bit-identical to the all-FP64 test.  Entries are appended in candidate order.
-constexpr int kRowChunk = 2048;
+constexpr int kRowChunk = 1024;
 constexpr int kCandBatch = 256;
 
 __device__ __forceinline__ float mi_f(float d, float L, float hL) {
@@ -120,7 +122,9 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     const double Ld = a.rep_box[r];
     const float L = (float)Ld, hL = 0.5f * (float)Ld;
     const int hs = a.cell_start[c_home], hn = a.cell_cnt[c_home];
-    if (hn == 0) return;
+    // gridDim.y CTAs share a home cell: CTA y takes every gridDim.y-th group of nwarp home
+    // molecules (each stages the whole neighbourhood)
+    if ((int)blockIdx.y * (int)(blockDim.x >> 5) >= hn) return;
     const int cl = c_home - off0;
     const int cx = cl % nc, cy = (cl / nc) % nc, cz = cl / (nc * nc);
     const int span = nc >= 5 ? 5 : nc;
@@ -144,7 +148,9 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     }
     __syncthreads();
     const int total = s_off[ncell];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int nwarp = (int)gridDim.y * (int)(blockDim.x >> 5);               // warps per home cell
+    const int warp = (int)blockIdx.y * (int)(blockDim.x >> 5) + (threadIdx.x >> 5);
     const float rcand2 = (float)a.rcand2 + 1e-3f;
     const float rc2f = (float)a.rc_nl2;
     const float band = a.band;
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                 // in batches of kCandBatch candidates: the O-O test first, compacting the
                 // passing candidates (in order) for the nine-pair test, so the lanes of the
                 // second pass are all busy
-                int *s_k = s_kbuf + warp * kCandBatch;
+                int *s_k = s_kbuf + (threadIdx.x >> 5) * kCandBatch;
                 for (int b0 = 0; b0 < cn; b0 += kCandBatch) {
                     const int b1 = min(b0 + kCandBatch, cn);
                     int nk = 0;
@@ -282,7 +288,11 @@ cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
     k_cell_sort<<<b, t, 0, st>>>(a);
     const size_t smem = (9 * sizeof(float) + sizeof(int)) * kRowChunk;
     cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_rows<<<a.n_cells, 256, smem, st>>>(a);
+    // home molecules per cell over the 8 warps of a CTA: split a cell over up to 4 CTAs so
+    // that a warp has about one home molecule
+    const int per_cell = (a.M + a.n_cells - 1) / a.n_cells;
+    const int split = std::min(4, std::max(1, (per_cell + 7) / 8));
+    k_rows<<<dim3(a.n_cells, split), 256, smem, st>>>(a);
     return cudaGetLastError();
 }
 
