@@ -1,8 +1,9 @@
 """Chained step launches change no result: the same forward + reverse run, in a process
 with REVSIM_CHAIN=0 (plain stream serialisation) and in one with chaining on, gives
 bit-identical trajectories — water (mixed and FP64, Langevin noise, neighbour rebuilds, two
-loss blocks) and gas in water (FP64, diffusion + enthalpy loss, where losses and gradients
-are bit-identical too).  The water RDF loss and its dL/dx are FP64 atomic sums whose order
+loss blocks), Stillinger-Weber diamond (mixed and FP64, stress loss, four blocks) and gas in
+water (FP64, diffusion + enthalpy loss, where losses and gradients are bit-identical too).
+The water and diamond losses and gradients are compared with tolerances.  The water RDF loss and its dL/dx are FP64 atomic sums whose order
 varies from run to run, so the water losses are compared to 1e-12 relative and the
 gradients to 1e-10 (FP64) and 1e-5 (mixed: an FP64 adjoint that differs in its last bit may
 round to a different FP32 operand).
@@ -48,6 +49,22 @@ for prec in ("mixed", "fp64"):
     out[prec + "_g"] = np.asarray(g, dtype=np.float64)
     out[prec + "_x"] = x
     out[prec + "_v"] = v
+from revsim import SwEngine, diamond as D
+sx, sbox = D.diamond_coords(3, noise=0.003, seed=4)
+sv = D.mb_velocities(len(sx), seed=5)
+sseeds = np.arange(1, 41, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+for prec in ("mixed", "fp64"):
+    with SwEngine(len(sx), sbox, precision=prec) as se:
+        se.set_params(D.default_params())
+        se.set_state(sx, sv)
+        se.set_loss()
+        lf, _ = se.forward(sseeds, 4.0, 40, 10, 0.0005)
+        out["sw" + prec + "_xf"], out["sw" + prec + "_vf"] = se.get_state()
+        lr, g = se.reverse(sseeds, 4.0, 40, 10, 10, 0.0005)
+        out["sw" + prec + "_x"], out["sw" + prec + "_v"] = se.get_state()
+        out["sw" + prec + "_lf"] = np.asarray(lf, dtype=np.float64)
+        out["sw" + prec + "_lr"] = np.asarray(lr, dtype=np.float64)
+        out["sw" + prec + "_g"] = np.asarray(g, dtype=np.float64)
 ge = GasEngine(int(d["n_water"]), int(d["n_gas"]), float(d["gbox"]))
 ge.set_params(d["gp"])
 ge.set_state(d["gx"], d["gv"])
@@ -88,7 +105,7 @@ def test_chained_launches_bit_identical(tmp_path):
         assert np.all(np.isfinite(plain[k])), k
         prec, what = k.split("_")
         if prec != "gas" and what in ("lf", "lr", "g"):
-            tol = 1e-12 if what != "g" else (1e-10 if prec == "fp64" else 1e-5)
+            tol = 1e-12 if what != "g" else (1e-10 if prec.endswith("fp64") else 1e-5)
             scale = np.abs(plain[k]).max()
             assert np.abs(chained[k] - plain[k]).max() <= tol * scale, k
         else:
