@@ -248,9 +248,12 @@ cudaError_t launch_rdf_finalize(const RdfArgs &a, int R, const double *pre, cons
 // process exits.  Host code cannot use the array's name as a device address: the
 // address is looked up once per device with cudaGetSymbolAddress, with that device
 // current, on the first call that device sees (make that first call before any
-// stream capture).  All calls share the one array and leave the last call's values
-// in it; each call clears what must start at zero, and calls that overlap on the GPU
-// (concurrent streams, or several host threads on one device) race on it.
+// stream capture).  The looked-up address belongs to the device's current context: a
+// cudaDeviceReset of that device invalidates it, so the entry point must not be called
+// again in a process after it has reset the device.  All calls share the one array and
+// leave the last call's values in it; each call clears what must start at zero, and calls
+// that overlap on the GPU (concurrent streams, or several host threads on one device) race
+// on it.  On an error return the outputs may be partly written.
 namespace {
 
 constexpr int kNoallocMaxGrid = 8192;
@@ -290,6 +293,7 @@ extern "C" int32_t revsim_rdf_loss_grad_noalloc(const double *d_x, int32_t n_mol
         return REVSIM_ERR_BADARG;
     const double q = t->x_min / t->step;
     if (std::fabs(q - std::llround(q)) > 1e-6) return REVSIM_ERR_BADARG;
+    if (!rdf_term_recurrence_ok(t->step, t->width, t->exp_cutoff)) return REVSIM_ERR_BADARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return REVSIM_ERR_CUDA;
     double *s = nullptr;
@@ -307,6 +311,7 @@ extern "C" int32_t revsim_rdf_loss_grad_noalloc(const double *d_x, int32_t n_mol
     const double n2 = t->sel2 == 0 ? n_mol : 2.0 * n_mol;
     const double pre = box * box * box / (4 * 3.14159265358979323846 * n1 * n2 * t->step);
     k_noalloc_tables<<<1, 1, 0, st>>>(s, t->n_grid, pre, box, n_mol);
+    if (cudaGetLastError() != cudaSuccess) return REVSIM_ERR_CUDA;
     if (cudaMemsetAsync(s, 0, sizeof(double) * t->n_grid, st) != cudaSuccess ||
         cudaMemsetAsync(d_loss, 0, sizeof(double), st) != cudaSuccess ||
         cudaMemsetAsync(d_dLdx, 0, sizeof(double) * 9 * (size_t)n_mol, st) != cudaSuccess)

@@ -37,6 +37,10 @@ def setup():
     v = np.zeros_like(x)
     terms = [RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, rng.uniform(0, 2, 200), 2, 1.0)]
     terms += reference_rdf_terms(rng.uniform(0, 2, 248), rng.uniform(0, 2, 281))
+    # the largest grid the scratch holds (8,192 points, 0.0005 nm apart): above 6,144 points
+    # the histogram kernel sums in global memory instead of shared memory, and the
+    # normaliser sits right after the last histogram entry, next to dL/dh
+    terms.append(RdfTerm(0, 0, 0.0005, 0.0005, 0.0005, 0.04, 8192, 0, 1, rng.uniform(0, 2, 8192), 2, 1.0))
     refs = []
     for t in terms:
         e = Engine(n_mol, box)
@@ -60,7 +64,7 @@ def _call(L, torch, n_mol, box, dx, t, dtarget, dloss, dgrad):
     return rc
 
 
-@pytest.mark.parametrize("which", [0, 1, 2])
+@pytest.mark.parametrize("which", [0, 1, 2, 3])
 def test_noalloc_matches_handle_loss_twice(setup, which):
     L, torch, n_mol, box, x, terms, refs = setup
     t = terms[which]
@@ -86,3 +90,6 @@ def test_noalloc_rejects_grid_beyond_scratch(setup):
     dloss = torch.zeros(1, dtype=torch.float64, device="cuda")
     dgrad = torch.zeros_like(dx)
     assert _call(L, torch, n_mol, box, dx, big, dtarget, dloss, dgrad) == -1
+    # a width so small against the grid step that the Gaussian recurrence would overflow
+    thin = RdfTerm(0, 0, 0.005, 0.005, 1e-7, 0.04, 200, 0, 1, np.zeros(10), 2, 1.0)
+    assert _call(L, torch, n_mol, box, dx, thin, dtarget, dloss, dgrad) == -1
