@@ -226,6 +226,24 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
                        int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
                        double clip_norm_threshold, double *loss_out, double *dl_dp_out);
 
+/* forward_sim / reverse_sim with the caller's own noise in place of the engine's seeded
+ * Philox draws: host_noise [n_steps][3 n_atoms] (step-major; within a step the replicas'
+ * atoms concatenated, xyz), entry step-1 = the velocity noise xi that generate_noise!
+ * (water.jl:867-873) returns for the seed of step `step` (Molly random_velocity_3D, nm/ps,
+ * sd sqrt(kB T / m)), used as v = v c + xi s in the forward step (water.jl:1033-1036) and
+ * v = (v - xi s) / c in the reverse un-integration (water.jl:1497-1498).  A Julia host passes
+ * the noise it draws with Xoshiro(seed), so that the engine runs the reference's own
+ * trajectory for gamma > 0.  The reverse pass must get the same array as the forward pass.
+ * The array is copied to the device (8 * 3 n_atoms * n_steps bytes) and not retained.
+ * Otherwise as revsim_forward / revsim_reverse. */
+int32_t revsim_forward_noise(revsim_handle *h, const double *host_noise, double gamma,
+                             int32_t n_steps, int32_t n_steps_loss, double dt, int32_t calc_loss,
+                             double *loss_out);
+int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double gamma,
+                             int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_trunc,
+                             double dt, double clip_norm_threshold, double *loss_out,
+                             double *dl_dp_out);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time with events. */
 void *revsim_stream(revsim_handle *h);
 
@@ -261,7 +279,10 @@ int32_t revsim_autotune(revsim_handle *h, double dt);
  * a fixed array inside the library (grids of at most 8192 points; a larger n_grid
  * returns REVSIM_ERR_BADARG); it calls no cudaMalloc or cudaFree.  The first call on
  * a device looks up that array's device address, so make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * capture; a cudaDeviceReset of that device invalidates the address, so do not call
+ * this entry point again in a process that has reset the device.  All calls share the
+ * array: calls that overlap on the GPU race.  On an error return the outputs are
+ * undefined (they may be partly written). */
 int32_t revsim_rdf_loss_grad_noalloc(const double *d_x, int32_t n_mol, double box,
                                      const revsim_rdf_term *term, const double *d_target,
                                      double *d_loss, double *d_dLdx, void *stream);

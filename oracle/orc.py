@@ -100,6 +100,13 @@ def lib():
         L.orc_reverse_sim.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PU64, _D, _I32,
                                       _I32, _I32, _D, _I32, _PD, _PD, _D,
                                       ctypes.POINTER(OrcLoss), _PD, _PD]
+        L.orc_forward_sim_hn.restype = _D
+        L.orc_forward_sim_hn.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PD, _D, _I32,
+                                         _I32, _D, _I32, ctypes.POINTER(OrcLoss), _I32, _PD, _PD, _PD]
+        L.orc_reverse_sim_hn.restype = _D
+        L.orc_reverse_sim_hn.argtypes = [ctypes.POINTER(OrcSystem), _PD, _PD, _PD, _PD, _D, _I32,
+                                         _I32, _I32, _D, _I32, _PD, _PD, _D, ctypes.POINTER(OrcLoss),
+                                         _PD, _PD]
         L.orc_loss_and_grads.restype = _D
         L.orc_loss_and_grads.argtypes = [ctypes.POINTER(OrcSystem), _PD, ctypes.POINTER(OrcLoss),
                                          _PD, _PD, _PD, _PD]
@@ -319,35 +326,58 @@ def loss_and_grads(s, params, loss, x):
     return val, (parts[0], parts[1]), g.reshape(-1, 3), dp
 
 
+def _host_noise(noise, n_steps, n3):
+    xi = np.ascontiguousarray(noise, dtype=np.float64)
+    if xi.size != n_steps * n3:
+        raise ValueError("host noise must hold [n_steps, N, 3] values")
+    return xi
+
+
 def forward_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, dt, loss=None,
-                calc_loss=True, n_steps_log=1000, parts=False):
-    """(x, v, loss, snaps_x, snaps_v), plus (l_rdf, l_ev) when ``parts``."""
+                calc_loss=True, n_steps_log=1000, parts=False, noise=None):
+    """(x, v, loss, snaps_x, snaps_v), plus (l_rdf, l_ev) when ``parts``.  ``noise``
+    [n_steps, N, 3] replaces the seeds' draws (orc_forward_sim_hn)."""
     x, v, p = _f64(x).copy(), _f64(v).copy(), _f64(params)
-    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
     n_snap = n_steps // n_steps_log + 1
     sx = np.zeros((n_snap, x.size))
     sv = np.zeros((n_snap, x.size))
     lp = np.zeros(2)
-    val = lib().orc_forward_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v), seeds.ctypes.data_as(_PU64),
-                                gamma, n_steps, n_steps_loss, dt, n_steps_log,
-                                ctypes.byref(loss.c) if loss is not None else None,
-                                1 if (calc_loss and loss is not None) else 0, _pd(sx), _pd(sv),
-                                _pd(lp))
+    lc = ctypes.byref(loss.c) if loss is not None else None
+    cl = 1 if (calc_loss and loss is not None) else 0
+    if noise is not None:
+        xi = _host_noise(noise, n_steps, x.size)
+        val = lib().orc_forward_sim_hn(ctypes.byref(s), _pd(p), _pd(x), _pd(v), _pd(xi), gamma,
+                                       n_steps, n_steps_loss, dt, n_steps_log, lc, cl, _pd(sx),
+                                       _pd(sv), _pd(lp))
+    else:
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        val = lib().orc_forward_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v),
+                                    seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss, dt,
+                                    n_steps_log, lc, cl, _pd(sx), _pd(sv), _pd(lp))
     out = (x.reshape(-1, 3), v.reshape(-1, 3), val, sx, sv)
     return out + ((lp[0], lp[1]),) if parts else out
 
 
 def reverse_sim(s, params, x, v, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
-                snaps_x, snaps_v, loss, clip=float("inf"), n_steps_log=1000, parts=False):
-    """(x0, v0, loss, dl/dtheta), plus (l_rdf, l_ev) when ``parts``."""
+                snaps_x, snaps_v, loss, clip=float("inf"), n_steps_log=1000, parts=False,
+                noise=None):
+    """(x0, v0, loss, dl/dtheta), plus (l_rdf, l_ev) when ``parts``; ``noise`` as for
+    forward_sim (the same array)."""
     x, v, p = _f64(x).copy(), _f64(v).copy(), _f64(params)
-    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
     sx, sv = _f64(snaps_x), _f64(snaps_v)
     g = np.zeros(n_params(s))
     lp = np.zeros(2)
-    val = lib().orc_reverse_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v), seeds.ctypes.data_as(_PU64),
-                                gamma, n_steps, n_steps_loss, n_steps_trunc, dt, n_steps_log,
-                                _pd(sx), _pd(sv), clip, ctypes.byref(loss.c), _pd(g), _pd(lp))
+    if noise is not None:
+        xi = _host_noise(noise, n_steps, x.size)
+        val = lib().orc_reverse_sim_hn(ctypes.byref(s), _pd(p), _pd(x), _pd(v), _pd(xi), gamma,
+                                       n_steps, n_steps_loss, n_steps_trunc, dt, n_steps_log,
+                                       _pd(sx), _pd(sv), clip, ctypes.byref(loss.c), _pd(g), _pd(lp))
+    else:
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        val = lib().orc_reverse_sim(ctypes.byref(s), _pd(p), _pd(x), _pd(v),
+                                    seeds.ctypes.data_as(_PU64), gamma, n_steps, n_steps_loss,
+                                    n_steps_trunc, dt, n_steps_log, _pd(sx), _pd(sv), clip,
+                                    ctypes.byref(loss.c), _pd(g), _pd(lp))
     out = (x.reshape(-1, 3), v.reshape(-1, 3), val, g)
     return out + ((lp[0], lp[1]),) if parts else out
 

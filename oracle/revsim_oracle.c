@@ -1118,11 +1118,21 @@ static int64_t rebuild_pairs(const orc_system *s, const double *x, int32_t **pai
     return cnt;
 }
 
-double orc_forward_sim(const orc_system *s, const double *params, double *x, double *v,
-                       const uint64_t *noise_seeds, double gamma, int32_t n_steps,
-                       int32_t n_steps_loss, double dt, int32_t n_steps_log,
-                       const orc_loss *loss, int32_t calc_loss,
-                       double *snap_x, double *snap_v, double *l_parts) {
+/* The noise of one step: the caller's array (host_noise [n_steps][3N], entry step - 1) when
+ * given, else the Philox draw of the step's seed. */
+static void step_noise(const orc_system *s, const uint64_t *noise_seeds, const double *host_noise,
+                       int32_t step, int64_t n3, double *xi) {
+    if (host_noise)
+        memcpy(xi, host_noise + (size_t)(step - 1) * (size_t)n3, sizeof(double) * (size_t)n3);
+    else
+        orc_noise(s, noise_seeds[step - 1], s->temp, xi);
+}
+
+static double forward_sim_any(const orc_system *s, const double *params, double *x, double *v,
+                              const uint64_t *noise_seeds, const double *host_noise, double gamma,
+                              int32_t n_steps, int32_t n_steps_loss, double dt, int32_t n_steps_log,
+                              const orc_loss *loss, int32_t calc_loss, double *snap_x,
+                              double *snap_v, double *l_parts) {
     const int64_t n = 3 * (int64_t)s->n_mol, n3 = 3 * n;
     const double L = s->box;
     const double c = exp(-gamma * dt), sn = sqrt(1 - c * c);   /* water.jl:1019-1020 */
@@ -1146,7 +1156,7 @@ double orc_forward_sim(const orc_system *s, const double *params, double *x, dou
             for (int u = 0; u < 3; u++) v[3 * a + u] = v[3 * a + u] + F[3 * a + u] * dt / m;
         }
         for (int64_t e = 0; e < n3; e++) x[e] = x[e] + v[e] * dt / 2;
-        orc_noise(s, noise_seeds[step - 1], s->temp, xi);
+        step_noise(s, noise_seeds, host_noise, step, n3, xi);
         for (int64_t e = 0; e < n3; e++) v[e] = v[e] * c + xi[e] * sn;
         for (int64_t e = 0; e < n3; e++) x[e] = x[e] + v[e] * dt / 2;
         for (int64_t e = 0; e < n3; e++) x[e] = orc_wrap1d(x[e], L);
@@ -1186,12 +1196,30 @@ static void reset_accums(int64_t n3, double c, const double *g, double *A, doubl
     }
 }
 
-double orc_reverse_sim(const orc_system *s, const double *params, double *x, double *v,
+double orc_forward_sim(const orc_system *s, const double *params, double *x, double *v,
                        const uint64_t *noise_seeds, double gamma, int32_t n_steps,
-                       int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
-                       int32_t n_steps_log, const double *snap_x, const double *snap_v,
-                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
-                       double *l_parts) {
+                       int32_t n_steps_loss, double dt, int32_t n_steps_log,
+                       const orc_loss *loss, int32_t calc_loss,
+                       double *snap_x, double *snap_v, double *l_parts) {
+    return forward_sim_any(s, params, x, v, noise_seeds, NULL, gamma, n_steps, n_steps_loss, dt,
+                           n_steps_log, loss, calc_loss, snap_x, snap_v, l_parts);
+}
+
+double orc_forward_sim_hn(const orc_system *s, const double *params, double *x, double *v,
+                          const double *host_noise, double gamma, int32_t n_steps,
+                          int32_t n_steps_loss, double dt, int32_t n_steps_log,
+                          const orc_loss *loss, int32_t calc_loss,
+                          double *snap_x, double *snap_v, double *l_parts) {
+    return forward_sim_any(s, params, x, v, NULL, host_noise, gamma, n_steps, n_steps_loss, dt,
+                           n_steps_log, loss, calc_loss, snap_x, snap_v, l_parts);
+}
+
+static double reverse_sim_any(const orc_system *s, const double *params, double *x, double *v,
+                              const uint64_t *noise_seeds, const double *host_noise, double gamma,
+                              int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_trunc,
+                              double dt, int32_t n_steps_log, const double *snap_x,
+                              const double *snap_v, double clip_norm_threshold,
+                              const orc_loss *loss, double *dl_dp, double *l_parts) {
     if (n_steps_trunc > n_steps_loss || n_steps_loss <= 0) return NAN;  /* water.jl:1437-1439 */
     const int64_t n = 3 * (int64_t)s->n_mol, n3 = 3 * n;
     const double L = s->box;
@@ -1225,7 +1253,7 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
         if (trunc_count <= n_steps_trunc) {
             /* part 1, water.jl:1496-1502 */
             for (int64_t e = 0; e < n3; e++) x[e] = x[e] - v[e] * dt / 2;
-            orc_noise(s, noise_seeds[step_n - 1], s->temp, xi);
+            step_noise(s, noise_seeds, host_noise, step_n, n3, xi);
             for (int64_t e = 0; e < n3; e++) v[e] = (v[e] - xi[e] * sn) / c;
             for (int64_t e = 0; e < n3; e++) x[e] = x[e] - v[e] * dt / 2;
             for (int64_t e = 0; e < n3; e++) x[e] = orc_wrap1d(x[e], L);
@@ -1281,6 +1309,28 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
     free(buf);
     free(pairs);
     return loss_accum / n_blocks;
+}
+
+double orc_reverse_sim(const orc_system *s, const double *params, double *x, double *v,
+                       const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                       int32_t n_steps_log, const double *snap_x, const double *snap_v,
+                       double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
+                       double *l_parts) {
+    return reverse_sim_any(s, params, x, v, noise_seeds, NULL, gamma, n_steps, n_steps_loss,
+                           n_steps_trunc, dt, n_steps_log, snap_x, snap_v, clip_norm_threshold,
+                           loss, dl_dp, l_parts);
+}
+
+double orc_reverse_sim_hn(const orc_system *s, const double *params, double *x, double *v,
+                          const double *host_noise, double gamma, int32_t n_steps,
+                          int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                          int32_t n_steps_log, const double *snap_x, const double *snap_v,
+                          double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
+                          double *l_parts) {
+    return reverse_sim_any(s, params, x, v, NULL, host_noise, gamma, n_steps, n_steps_loss,
+                           n_steps_trunc, dt, n_steps_log, snap_x, snap_v, clip_norm_threshold,
+                           loss, dl_dp, l_parts);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -177,6 +177,21 @@ double orc_reverse_sim(const orc_system *s, const double *params, double *x, dou
                        double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
                        double *l_parts);
 
+/* orc_forward_sim / orc_reverse_sim with the caller's noise host_noise [n_steps][3N] (entry
+ * step - 1 = generate_noise!'s xi of step `step`, water.jl:867-873) in place of the seeds'
+ * Philox draws (water.jl:1033-1036, 1497-1498). */
+double orc_forward_sim_hn(const orc_system *s, const double *params, double *x, double *v,
+                          const double *host_noise, double gamma, int32_t n_steps,
+                          int32_t n_steps_loss, double dt, int32_t n_steps_log,
+                          const orc_loss *loss, int32_t calc_loss,
+                          double *snap_x, double *snap_v, double *l_parts);
+double orc_reverse_sim_hn(const orc_system *s, const double *params, double *x, double *v,
+                          const double *host_noise, double gamma, int32_t n_steps,
+                          int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                          int32_t n_steps_log, const double *snap_x, const double *snap_v,
+                          double clip_norm_threshold, const orc_loss *loss, double *dl_dp,
+                          double *l_parts);
+
 /* Monte-Carlo barostat: MonteCarloBarostatNoUnits and its apply_coupling!
  * (water.jl:789-865) as forward_sim runs it with use_barostat (water.jl:1009-1014,
  * 1043-1044): every n_steps steps, after the step's neighbour refresh, one volume move

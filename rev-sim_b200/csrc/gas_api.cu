@@ -675,6 +675,8 @@ int32_t revsim_gas_set_rdf(revsim_gas_handle *h, int32_t n_terms, const revsim_r
         const double q = t.x_min / t.step;
         if (std::fabs(q - std::llround(q)) > 1e-6)
             return fail(h, REVSIM_ERR_BADARG, "x_min must be a multiple of step (diffusion.jl:709)");
+        if (!rs::rdf_term_recurrence_ok(t.step, t.width, t.exp_cutoff))
+            return fail(h, REVSIM_ERR_BADARG, "width too small for the grid step and window");
     }
     if (n_terms > 0 && h->nw < 1) return fail(h, REVSIM_ERR_BADARG, "the RDF term needs water molecules");
     CK(cudaSetDevice(h->dev));

@@ -111,6 +111,11 @@ struct revsim_handle {
     int fwd_steps = 0;
     uint64_t *d_seeds = nullptr;
     size_t seeds_cap = 0;
+    // caller-supplied noise [n_steps][3N] of the host-noise entry points (use_noise: the
+    // running pass reads it instead of drawing Philox noise from the seeds)
+    double *d_noise = nullptr;
+    size_t noise_cap = 0;
+    bool use_noise = false;
     // loss
     std::vector<Term> terms;
     double *d_loss = nullptr, *d_loss_acc = nullptr, *d_dLdx = nullptr;
@@ -796,6 +801,7 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
         a.pos_in = h->d_pos[cur];
         a.pos_out = h->d_pos[cur ^ 1];
         a.seed_cur = h->d_seeds + (size_t)(step - 1) * R;
+        a.noise_cur = h->use_noise ? h->d_noise + (size_t)(step - 1) * n3 : nullptr;
         if ((rc = launch_step_k(h, false, a))) return rc;
         cur ^= 1;
         if (step % h->nf == 0 && step < n_steps) {
@@ -871,6 +877,7 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
             if (pending) {
                 StepArgs u = a;
                 u.seed_cur = h->d_seeds + (size_t)(step_n - 1) * R;
+                u.noise_cur = h->use_noise ? h->d_noise + (size_t)(step_n - 1) * n3 : nullptr;
                 u.pos_out = h->d_pos[cur];
                 u.wgt_out = h->d_wgt[cur];
                 CK(launch_unintegrate(h->M, h->prec, u, h->d_mol_rep, h->st));
@@ -904,6 +911,7 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
             a.pos_out = h->d_pos[cur ^ 1];
             a.wgt_out = h->d_wgt[cur ^ 1];
             a.seed_next = fuse ? h->d_seeds + (size_t)(step_n - 2) * R : nullptr;
+            a.noise_next = fuse && h->use_noise ? h->d_noise + (size_t)(step_n - 2) * n3 : nullptr;
             a.mode = (fuse ? MODE_FUSE_NEXT : 0) | (clipping ? MODE_DEFER_BA : 0);
             if ((rc = launch_step_k(h, true, a))) return rc;
             if (clipping) {
@@ -990,7 +998,7 @@ void free_all(revsim_handle *h) {
                     h->d_v, h->d_A, h->d_B, h->d_C, h->d_D, h->d_G, h->d_F, h->d_x0, h->d_v0,
                     h->d_pos[0], h->d_pos[1], h->d_wgt[0], h->d_wgt[1], h->d_part, h->d_norm2,
                     h->d_scale, h->d_status, h->d_maxcnt, h->d_count, h->d_snap_x, h->d_snap_v,
-                    h->d_ckpt, h->d_seeds, h->d_loss, h->d_loss_acc, h->d_dLdx,
+                    h->d_ckpt, h->d_seeds, h->d_noise, h->d_loss, h->d_loss_acc, h->d_dLdx,
                     h->d_cell_rep, h->d_nbr_store, h->d_cnt_store, h->d_ev_acc, h->d_ev_k,
                     h->d_ev_grad, h->d_nbr_ev, h->d_cnt_ev, h->d_bx, h->d_lsc, h->d_bacc, h->d_repE};
     for (void *p : ptrs) dfree(p);
@@ -1280,6 +1288,8 @@ int32_t revsim_set_loss(revsim_handle *h, int32_t n_terms, const revsim_rdf_term
         const double q = t.x_min / t.step;
         if (std::fabs(q - std::llround(q)) > 1e-6)
             return fail(h, REVSIM_ERR_BADARG, "x_min must be a multiple of step (water.jl:660)");
+        if (!rdf_term_recurrence_ok(t.step, t.width, t.exp_cutoff))
+            return fail(h, REVSIM_ERR_BADARG, "width too small for the grid step and window");
         Term T;
         T.t = t;
         T.off = (int)std::llround(q) - 1;
@@ -1586,15 +1596,44 @@ int32_t revsim_rdf(revsim_handle *h, int32_t term, int32_t replica, double *hist
     return REVSIM_OK;
 }
 
-int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gamma, int32_t n_steps,
-                       int32_t n_steps_loss, double dt, int32_t calc_loss, double *loss_out) {
+}  // extern "C"
+
+namespace {
+
+// Noise of a pass: the per-step seeds (Philox draws on the device) or, from the host-noise
+// entry points, the caller's noise [n_steps][3N] copied to the device.  The guard clears the
+// host-noise switch when the pass returns, on every path.
+struct NoiseGuard {
+    revsim_handle *h;
+    ~NoiseGuard() { h->use_noise = false; }
+};
+
+int upload_noise(revsim_handle *h, const uint64_t *seeds, const double *noise, int n_steps) {
+    h->use_noise = false;
+    if (!noise) return upload_seeds(h, seeds, (size_t)n_steps * h->R);
+    const size_t n = (size_t)n_steps * 3 * (size_t)h->N;
+    if (n > h->noise_cap) {
+        dfree(h->d_noise);
+        h->d_noise = nullptr;
+        h->noise_cap = 0;
+        CK(dalloc(&h->d_noise, n));
+        h->noise_cap = n;
+    }
+    if (n) CK(cudaMemcpyAsync(h->d_noise, noise, sizeof(double) * n, cudaMemcpyHostToDevice, h->st));
+    h->use_noise = true;
+    return REVSIM_OK;
+}
+
+int32_t forward_entry(revsim_handle *h, const uint64_t *noise_seeds, const double *noise, double gamma,
+                      int32_t n_steps, int32_t n_steps_loss, double dt, int32_t calc_loss, double *loss_out) {
     int rc = check_ready(h);
     if (rc) return rc;
-    if (n_steps < 0 || (n_steps > 0 && !noise_seeds) || !(dt > 0) || !(gamma >= 0))
+    if (n_steps < 0 || (n_steps > 0 && !noise_seeds && !noise) || !(dt > 0) || !(gamma >= 0))
         return fail(h, REVSIM_ERR_BADARG, "bad forward arguments");
     if (calc_loss && n_steps > 0 && n_steps_loss < 1) return fail(h, REVSIM_ERR_BADARG, "n_steps_loss < 1");
     const size_t n3 = 3 * (size_t)h->N;
-    if ((rc = upload_seeds(h, noise_seeds, (size_t)n_steps * h->R))) return rc;
+    NoiseGuard guard{h};
+    if ((rc = upload_noise(h, noise_seeds, noise, n_steps))) return rc;
     const size_t n_snap = (h->nlog > 0 ? (size_t)n_steps / h->nlog : 0) + 1;
     const size_t n_ckpt = n_steps > 0 ? (size_t)(n_steps - 1) / h->nf + 1 : 1;
     if ((rc = ensure_store(h, &h->d_snap_x, &h->snap_cap, n_snap * n3))) return rc;
@@ -1647,14 +1686,15 @@ int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gam
     return REVSIM_OK;
 }
 
-int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gamma, int32_t n_steps,
-                       int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
-                       double clip_norm_threshold, double *loss_out, double *dl_dp_out) {
+int32_t reverse_entry(revsim_handle *h, const uint64_t *noise_seeds, const double *noise, double gamma,
+                      int32_t n_steps, int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                      double clip_norm_threshold, double *loss_out, double *dl_dp_out) {
     int rc = check_ready(h);
     if (rc) return rc;
     if (n_steps_trunc > n_steps_loss)
         return fail(h, REVSIM_ERR_BADARG, "n_steps_trunc must not be greater than n_steps_loss");
-    if (n_steps < 1 || n_steps_loss < 1 || !noise_seeds || !(dt > 0) || !(gamma >= 0) || !(clip_norm_threshold > 0))
+    if (n_steps < 1 || n_steps_loss < 1 || (!noise_seeds && !noise) || !(dt > 0) || !(gamma >= 0) ||
+        !(clip_norm_threshold > 0))
         return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
     if (!has_loss(h)) return fail(h, REVSIM_ERR_STATE, "no loss set");
     if (h->fwd_baro)
@@ -1663,7 +1703,8 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
     const bool need_store = h->nl_mode == REVSIM_NL_CHECKPOINT || (h->nlog > 0 && n_steps > h->nlog);
     if (need_store && !(h->fwd_valid && h->fwd_steps == n_steps))
         return fail(h, REVSIM_ERR_STATE, "reverse needs the forward pass of the same n_steps");
-    if ((rc = upload_seeds(h, noise_seeds, (size_t)n_steps * h->R))) return rc;
+    NoiseGuard guard{h};
+    if ((rc = upload_noise(h, noise_seeds, noise, n_steps))) return rc;
     if ((rc = reverse_impl(h, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip_norm_threshold))) return rc;
     int s;
     if ((rc = read_status(h, &s))) return rc;
@@ -1687,6 +1728,38 @@ int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gam
     }
     if (h->ktime && (rc = collect_kernel_times(h))) return rc;
     return REVSIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t revsim_forward(revsim_handle *h, const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, double dt, int32_t calc_loss, double *loss_out) {
+    if (h && n_steps > 0 && !noise_seeds) return fail(h, REVSIM_ERR_BADARG, "bad forward arguments");
+    return forward_entry(h, noise_seeds, nullptr, gamma, n_steps, n_steps_loss, dt, calc_loss, loss_out);
+}
+
+int32_t revsim_forward_noise(revsim_handle *h, const double *host_noise, double gamma, int32_t n_steps,
+                             int32_t n_steps_loss, double dt, int32_t calc_loss, double *loss_out) {
+    if (h && n_steps > 0 && !host_noise) return fail(h, REVSIM_ERR_BADARG, "bad forward arguments");
+    return forward_entry(h, nullptr, host_noise, gamma, n_steps, n_steps_loss, dt, calc_loss, loss_out);
+}
+
+int32_t revsim_reverse(revsim_handle *h, const uint64_t *noise_seeds, double gamma, int32_t n_steps,
+                       int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                       double clip_norm_threshold, double *loss_out, double *dl_dp_out) {
+    if (h && !noise_seeds) return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
+    return reverse_entry(h, noise_seeds, nullptr, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
+                         clip_norm_threshold, loss_out, dl_dp_out);
+}
+
+int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double gamma, int32_t n_steps,
+                             int32_t n_steps_loss, int32_t n_steps_trunc, double dt,
+                             double clip_norm_threshold, double *loss_out, double *dl_dp_out) {
+    if (h && !host_noise) return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
+    return reverse_entry(h, nullptr, host_noise, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
+                         clip_norm_threshold, loss_out, dl_dp_out);
 }
 
 void *revsim_stream(revsim_handle *h) { return h ? (void *)h->st : nullptr; }

@@ -93,6 +93,9 @@ struct StepArgs {
     double *F_out;     // forces-only mode
     double dt, c, s, mO, mH, acoefO, acoefH;
     const uint64_t *seed_cur, *seed_next;   // [n_replicas]
+    // Caller-supplied noise of the current / next step, [3N] each (host_noise entry points);
+    // when set it replaces the Philox draw of seed_cur / seed_next.
+    const double *noise_cur, *noise_next;
     int mode;
 };
 
@@ -130,6 +133,15 @@ struct RdfArgs {
     const double *dLdh; // [R * n_grid]
     double *dLdx;      // [3N]
 };
+
+// The RDF kernels form consecutive Gaussians by a recurrence whose ratio at a window's
+// anchor is exp(-(2 e step + step^2) / width) with |e| <= exp_cutoff + 2 step; it must stay
+// finite (exp overflows above ~709), so terms whose ratio exponent could exceed 700 are
+// rejected when they are set.
+inline bool rdf_term_recurrence_ok(double step, double width, double exp_cutoff) {
+    const double worst = (2.0 * (exp_cutoff + 2.0 * step) * step + step * step) / width;
+    return worst <= 700.0;
+}
 
 // Launchers (return cudaError_t of the launch).
 cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st);

@@ -55,9 +55,15 @@ __global__ void k_unintegrate(int M, StepArgs a, const int *mol_rep) {
         const bool isO = k == 0;
         const double m = isO ? a.mO : a.mH;
         double xi[3] = {0.0, 0.0, 0.0};
-        if (a.s != 0.0)
-            atom_noise(a.seed_cur[rep], (uint32_t)(i - a.rep_atom0[rep]), isO ? a.rep_sdO[rep] : a.rep_sdH[rep],
-                       xi);
+        if (a.s != 0.0) {
+            if (a.noise_cur) {
+#pragma unroll
+                for (int u = 0; u < 3; u++) xi[u] = a.noise_cur[3 * (size_t)i + u];
+            } else {
+                atom_noise(a.seed_cur[rep], (uint32_t)(i - a.rep_atom0[rep]),
+                           isO ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+            }
+        }
         double Cm[3];
 #pragma unroll
         for (int u = 0; u < 3; u++) {

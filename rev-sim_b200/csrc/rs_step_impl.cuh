@@ -359,7 +359,14 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
         // cannot know that, and would otherwise serialise the three components
         const double vk[3] = {a.v[3 * ia], a.v[3 * ia + 1], a.v[3 * ia + 2]};
         double xi[3] = {0.0, 0.0, 0.0};
-        if (a.s != 0.0) atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+        if (a.s != 0.0) {
+            if (a.noise_cur) {
+#pragma unroll
+                for (int u = 0; u < 3; u++) xi[u] = a.noise_cur[3 * ia + u];
+            } else {
+                atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+            }
+        }
 #pragma unroll
         for (int u = 0; u < 3; u++) {
             double v = vk[u], x = xk[u];
@@ -394,8 +401,13 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
         }
         double xi[3] = {0.0, 0.0, 0.0};
         if (fuse && a.s != 0.0) {
-            const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
-            atom_noise(a.seed_next[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+            if (a.noise_next) {
+#pragma unroll
+                for (int u = 0; u < 3; u++) xi[u] = a.noise_next[3 * ia + u];
+            } else {
+                const uint32_t la = (uint32_t)(ia - a.rep_atom0[rep]);
+                atom_noise(a.seed_next[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
+            }
         }
         double Cm[3];
 #pragma unroll

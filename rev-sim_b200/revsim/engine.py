@@ -250,17 +250,39 @@ class Engine:
             raise ValueError(f"noise seeds must be [n_steps] or [n_steps, n_replicas], got {s.shape}")
         return np.ascontiguousarray(s)
 
-    def forward(self, seeds, gamma, n_steps, n_steps_loss, dt, calc_loss=True):
-        s = self._seeds(seeds, n_steps)
+    def _noise(self, noise, n_steps):
+        xi = np.ascontiguousarray(noise, dtype=np.float64)
+        if xi.size != n_steps * self.n_atoms * 3:
+            raise ValueError(f"host noise must hold [n_steps, n_atoms, 3] = "
+                             f"[{n_steps}, {self.n_atoms}, 3] values, got {xi.shape}")
+        return xi
+
+    def forward(self, seeds, gamma, n_steps, n_steps_loss, dt, calc_loss=True, noise=None):
+        """forward_sim from the current state.  ``seeds`` [n_steps] or [n_steps, R] draw the
+        Langevin noise on the device; ``noise`` [n_steps, n_atoms, 3] (generate_noise!'s
+        output for every step) is used instead when given (seeds may then be None)."""
         loss = np.zeros(self.R)
+        if noise is not None:
+            xi = self._noise(noise, n_steps)
+            self._check(self._L.revsim_forward_noise(self._h, f64p(xi), gamma, n_steps, n_steps_loss,
+                                                     dt, 1 if calc_loss else 0, f64p(loss)))
+            return loss
+        s = self._seeds(seeds, n_steps)
         self._check(self._L.revsim_forward(self._h, u64p(s), gamma, n_steps, n_steps_loss, dt,
                                            1 if calc_loss else 0, f64p(loss)))
         return loss
 
-    def reverse(self, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip=np.inf):
-        s = self._seeds(seeds, n_steps)
+    def reverse(self, seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip=np.inf,
+                noise=None):
+        """reverse_sim from the forward end state; ``noise`` as for forward (the same array)."""
         loss = np.zeros(self.R)
         g = np.zeros((self.R, self.n_params))
+        if noise is not None:
+            xi = self._noise(noise, n_steps)
+            self._check(self._L.revsim_reverse_noise(self._h, f64p(xi), gamma, n_steps, n_steps_loss,
+                                                     n_steps_trunc, dt, clip, f64p(loss), f64p(g)))
+            return loss, g
+        s = self._seeds(seeds, n_steps)
         self._check(self._L.revsim_reverse(self._h, u64p(s), gamma, n_steps, n_steps_loss,
                                            n_steps_trunc, dt, clip, f64p(loss), f64p(g)))
         return loss, g

@@ -20,7 +20,10 @@ Differences, each deliberate:
   ``NotImplementedError``;
 * ``n_threads`` is accepted and ignored;
 * noise: per-step seeds drive a counter-based Philox generator, regenerated
-  identically in the reverse pass (the reference uses Xoshiro(seed) + randn).
+  identically in the reverse pass (the reference uses Xoshiro(seed) + randn); a caller
+  that holds the reference's own noise (generate_noise!, water.jl:867-873, one [N, 3] array
+  per step) passes it as ``host_noise`` [n_steps, N, 3] to both calls instead, and the
+  engine then integrates exactly the reference's trajectory.
 """
 
 import numpy as np
@@ -76,9 +79,11 @@ def _set_loss(eng, loss_type, loss_terms):
 
 def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss, params,
                 dt, n_threads, inter_type, loss_type, run_grads=False, calc_loss=True,
-                use_barostat=False, *, loss_terms=None, engine=None, precision="fp64"):
+                use_barostat=False, *, loss_terms=None, engine=None, precision="fp64",
+                host_noise=None):
     """water.jl:977.  Returns (sys, loss, grads); grads is [None] * P as in the
-    reference's run_grads=false branch (water.jl:1100-1102)."""
+    reference's run_grads=false branch (water.jl:1100-1102).  ``host_noise``
+    [n_steps, N, 3]: the noise of every step, used in place of the seeds' draws."""
     if run_grads:
         raise NotImplementedError("run_grads (Zygote unrolled RAD) is not part of the engine")
     eng = _engine_for(coords, boundary, inter_type, engine, precision)
@@ -93,7 +98,7 @@ def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
         eng.set_barostat(True, seed=int(seeds.reshape(-1)[0]) if seeds.size else 0)
     try:
         loss = eng.forward(seeds, gamma, n_steps, n_steps_loss if n_steps_loss else max(n_steps, 1),
-                           dt, calc_loss)
+                           dt, calc_loss, noise=host_noise)
     finally:
         if use_barostat:
             eng.set_barostat(False)
@@ -105,8 +110,9 @@ def forward_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
 
 def reverse_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_steps_loss,
                 n_steps_trunc, params, dt, n_threads, fwd_loggers, clip_norm_threshold, inter_type,
-                loss_type, *, loss_terms=None):
-    """water.jl:1435.  ``fwd_loggers`` is ``sys.loggers`` of the forward_sim result.
+                loss_type, *, loss_terms=None, host_noise=None):
+    """water.jl:1435.  ``fwd_loggers`` is ``sys.loggers`` of the forward_sim result;
+    ``host_noise`` the array the forward_sim call was given, if any.
     Returns (sys, l, dl_dp, l_rdf, l_ev)."""
     if n_steps_trunc > n_steps_loss:
         raise ValueError("n_steps_trunc must not be greater than n_steps_loss")
@@ -117,7 +123,8 @@ def reverse_sim(coords, velocities, boundary, noise_seeds, gamma, n_steps, n_ste
     eng.set_params(params)
     eng.set_state(coords, velocities)
     clip = np.inf if clip_norm_threshold is None else float(clip_norm_threshold)
-    loss, g = eng.reverse(noise_seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip)
+    loss, g = eng.reverse(noise_seeds, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip,
+                          noise=host_noise)
     x, v = eng.get_state()
     sys = SimSystem(eng, x, v, float(eng.box[0]) if boundary is None else boundary)
     l_rdf, l_ev = eng.loss_parts()

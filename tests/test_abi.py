@@ -79,6 +79,8 @@ def test_new_entry_points_reject_a_null_handle(lib):
     assert L.revsim_set_barostat(None, ctypes.byref(d)) == -1
     assert L.revsim_barostat_state(None, None, None, None, None) == -1
     assert L.revsim_set_box(None, None) == -1
+    assert L.revsim_forward_noise(None, None, 0.0, 0, 0, 0.0, 0, None) == -1
+    assert L.revsim_reverse_noise(None, None, 0.0, 1, 1, 1, 0.001, 1.0, None, None) == -1
 
 
 def test_descriptor_validation_before_any_device_call(lib):
