@@ -42,11 +42,12 @@ UNIT = "atom-steps/s"
 # reference expressions (add/mul = 1, FMA = 2, sqrt/div/exp = 1): forward 40 (+15 for
 # an O-O LJ pair), reverse 170 (force + 3x3 VJP with mass scaling + dF/dtheta).
 FLOPS_FWD_IPAIR, FLOPS_FWD_OO_EXTRA, FLOPS_REV_IPAIR = 40, 15, 170
-# DRAM traffic per reverse-step launch of the default workload, from ncu
-# (profiles/rev_step_ncu_water3000.md: dram__bytes_read.sum 5.395 MB, write 0).
+# DRAM traffic per reverse-step launch of the default workload: dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture of that kernel on the same 9,000-atom system
+# (5.395 MB read, 0 written).
 REV_STEP_DRAM_BYTES = 5.395e6
-# DRAM traffic per forward-step launch of the gas-in-water engine (2,675 atoms), from ncu
-# with cold caches (profiles/gas_step_ncu_gas2675.md: 8.11 MB read, 0.11 MB written).
+# DRAM traffic per forward-step launch of the gas-in-water engine (2,675 atoms), from one ncu
+# capture with cold caches (8.11 MB read, 0.11 MB written).
 GAS_FWD_STEP_DRAM_BYTES = 8.22e6
 GAS_REV_STEP_DRAM_BYTES = 8.97e6
 
@@ -72,8 +73,12 @@ def parse():
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
     ap.add_argument("--n-replicas", type=int, default=64, help="replicas workload: boxes")
     ap.add_argument("--rep-steps", type=int, default=2000, help="replicas workload: steps")
+    ap.add_argument("--cfg1-replicas", type=int, default=16,
+                    help="895-water target configuration: replicas batched in one handle")
+    ap.add_argument("--no-target", action="store_true",
+                    help="water: skip the 895-water target configuration in the headline line")
     ap.add_argument("--workload", default="water", choices=["water", "diamond", "mlp", "replicas", "equil", "reweight",
-                             "diffusion"],
+                             "diffusion", "cfg1"],
                     help="water: 3,000-molecule box (the headline); diamond: Stillinger-Weber "
                          "carbon, 16 replicas of 8,000 atoms; mlp: 895 waters with the learned "
                          "pair correction, gradient throughput and a training comparison; "
@@ -402,6 +407,9 @@ def run_ours(a):
     eng.set_kernel_timing(False)
     launch_ms = kt_ms / max(kt_n, 1)
     xs, _ = eng.get_state()
+    # the reverse pass ends at the start state, rebuilt over the first snapshot block
+    recon = {"mixed" if a.precision == "mixed" else "fp64": recon_error(xs, x0, a.box),
+             "steps_reconstructed": 1000}
     pairs = eng.neighbor_pairs(0)
     ipairs, oo = count_ipairs(xs, a.box, pairs)
     flops_launch = FLOPS_REV_IPAIR * ipairs
@@ -412,6 +420,8 @@ def run_ours(a):
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value if peak.value else None,
                 "traffic": REV_STEP_DRAM_BYTES,
+                "traffic_source": "ncu constant: dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "capture of this kernel on this system, not measured in this run",
                 "kernel": "k_water_step<float, LJ, reverse> (fused reverse step)",
                 "launch_ms": launch_ms, "launches_timed": kt_n, "ipairs": ipairs,
                 "flops_per_launch": flops_launch,
@@ -446,6 +456,7 @@ def run_ours(a):
         e1.record(s64)
         torch.cuda.synchronize()
         ms64 = e0.elapsed_time(e1)
+        recon["fp64"] = recon_error(e64.get_state()[0], x0, a.box)
         eng.set_state(x0, v0)
         eng.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
         _, gm = eng.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
@@ -456,31 +467,30 @@ def run_ours(a):
             eng_.set_state(x0, v0)
             eng_.forward(seeds[:100], a.gamma, 100, 100, 0.001)
             short[key] = eng_.reverse(seeds[:100], a.gamma, 100, 100, 100, 0.001)[1][0]
-        gs = np.abs(g64[0] * p)
+        e64.close()
 
-        def rel(gx, gref):
-            # SW parameters in units of dL/dlog(theta); the MLP's (when present) relative to
-            # the largest MLP entry
-            q = p[:7]
-            sc = np.abs(gref[:7] * q)
-            e = float(np.max(np.abs((gx[:7] - gref[:7]) * q) / np.maximum(sc, 0.01 * sc.max())))
-            if len(p) > 7:
-                e = max(e, float(np.abs(gx[7:] - gref[7:]).max() / np.abs(gref[7:]).max()))
+        def make(prec):
+            e = Engine(a.n_mol, a.box, inter_type=a.form, precision=prec, device=local)
+            e.set_params(p)
+            apply_loss(e, a, target)
             return e
         extra = {"fp64_gpu": {"value": n_atoms * a.n_steps / (ms64 * 1e-3), "ms_per_step": ms64,
                               "speedup_mixed_over_fp64": (ms64 / ms_step)},
                  "grad_rel_err_vs_fp64": {
-                     "full_workload": rel(gm[0], g64[0]),
-                     "first_100_steps": rel(short["mixed"], short["fp64"]),
-                     "definition": "max over parameters of |g - g_fp64| * |theta| / max(|g_fp64 * theta|, "
-                                   "0.01 max_k |g_fp64,k * theta_k|)"}}
-        e64.close()
-        del gs
+                     "full_workload": grad_rel_err(gm[0], g64[0], p),
+                     "full_workload_note": "one mixed / FP64 pair over 1,000-step untruncated blocks "
+                                           "at gamma = 0: the trajectories part ways within a block "
+                                           "(chaos), so this is not a precision bound",
+                     "first_100_steps": grad_rel_err(short["mixed"], short["fp64"], p),
+                     "train_schedule_windows": train_window_errors(make, x0, v0, p),
+                     "definition": GRAD_ERR_DEFINITION}}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         val, cores, desc = cpu_sample(a, x0, v0, p, target, a.cpu_sample_steps)
         cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0 and world == 1 and not a.no_target and a.form == "lj" and a.loss == "rdf":
+        extra["target_config"] = run_target_cfg1(a, local, with_cpu=not a.no_cpu_baseline)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -491,13 +501,288 @@ def run_ours(a):
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-               "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])}}
+               "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])},
+               "recon": recon}
         out.update(extra)
         print(json.dumps(out), flush=True)
     eng.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ accuracy of a result
+GRAD_ERR_DEFINITION = ("max over parameters of |g - g_fp64| * |theta| / max(|g_fp64 * theta|, "
+                       "0.01 max_k |g_fp64,k * theta_k|)")
+
+
+def grad_rel_err(gx, gref, p):
+    """Classical parameters in units of dL/dlog(theta), floored at 1 % of the largest; the
+    MLP's (when present) relative to the largest MLP entry."""
+    p = np.asarray(p)
+    nc = min(len(p), 9)
+    q = p[:nc]
+    sc = np.abs(gref[:nc] * q)
+    e = float(np.max(np.abs((gx[:nc] - gref[:nc]) * q) / np.maximum(sc, 0.01 * sc.max())))
+    if len(p) > nc:
+        e = max(e, float(np.abs(gx[nc:] - gref[nc:]).max() / np.abs(gref[nc:]).max()))
+    return e
+
+
+def recon_error(x_rec, x0, box):
+    """How well a reverse pass rebuilt the start state: minimum-image RMSD and largest
+    component error over the atoms, nm.  ``box``: a side or one side per atom."""
+    b = np.asarray(box, dtype=np.float64)
+    b = b if b.ndim == 0 else b[:, None]
+    d = np.asarray(x_rec) - np.asarray(x0)
+    d -= b * np.round(d / b)
+    return {"rmsd_nm": float(np.sqrt((d * d).sum(1).mean())), "max_nm": float(np.abs(d).max())}
+
+
+def train_window_errors(make, x0, v0, p, gamma=1.0, n_windows=5, n_loss=2000, n_trunc=200, seed=500):
+    """Mixed-precision gradient error under train()'s schedule (water.jl:1624-1631, 1666-1669:
+    gamma = 1/ps, a loss point every 2,000 steps, each reverse window truncated at 200 steps).
+    That gradient is a sum over loss points of 200-step window gradients; the forward run only
+    samples the windows' start states, and any two runs of it (FP32 or FP64 rounding alike)
+    part ways within a few ps.  So a mixed-precision sampler runs the schedule, and at each of
+    n_windows loss points the window gradient is computed from the same start state in mixed
+    precision and in FP64; returns the per-window errors and the windows' reconstruction."""
+    from revsim import systems
+    sampler, em, e64 = make("mixed"), make("mixed"), make("fp64")
+    sampler.set_state(x0, v0)
+    seeds = systems.noise_seeds(n_windows * n_loss, seed=seed)
+    errs, recon = [], {"mixed": 0.0, "fp64": 0.0}
+    for w in range(n_windows):
+        s0 = w * n_loss
+        sampler.forward(seeds[s0:s0 + n_loss - n_trunc], gamma, n_loss - n_trunc, n_loss, 0.001,
+                        calc_loss=False)
+        xs, vs = sampler.get_state()
+        sw = seeds[s0 + n_loss - n_trunc:s0 + n_loss]
+        gw = {}
+        for key, e in (("mixed", em), ("fp64", e64)):
+            e.set_state(xs, vs)
+            e.forward(sw, gamma, n_trunc, n_trunc, 0.001, calc_loss=False)
+            gw[key] = e.reverse(sw, gamma, n_trunc, n_trunc, n_trunc, 0.001)[1][0]
+            xr, _ = e.get_state()
+            recon[key] = max(recon[key], recon_error(xr, xs, e.box[0] if e.R == 1 else
+                                                     np.repeat(e.box, 3 * e.n_mol))["max_nm"])
+        errs.append(grad_rel_err(gw["mixed"], gw["fp64"], p))
+        sampler.forward(sw, gamma, n_trunc, n_trunc, 0.001, calc_loss=False)
+    for e in (sampler, em, e64):
+        e.close()
+    return {"schedule": f"gamma {gamma:g}/ps, loss every {n_loss} steps, reverse truncated at "
+                        f"{n_trunc} steps (train(), water.jl:1624-1631)",
+            "windows": n_windows, "max": float(max(errs)), "mean": float(np.mean(errs)),
+            "per_window": [float(t) for t in errs],
+            "window_recon_max_nm": {k: float(v) for k, v in recon.items()},
+            "method": "each window's gradient from the same start state (a mixed-precision run's "
+                      "state 200 steps before the loss point) in mixed precision and in FP64"}
+
+
+def seed_ensemble(make, x0, n_mol, p, n_seeds=8, n_steps=1000, gamma=0.0):
+    """Untruncated n_steps-step gradients from n_seeds start states (the same positions,
+    Maxwell-Boltzmann velocities from n_seeds seeds) in both precisions.  One mixed / FP64
+    pair from one state is a chaotic pair (the trajectories part ways within the block); the
+    ensemble means are compared against their standard error instead."""
+    from revsim import systems
+    em, e64 = make("mixed"), make("fp64")
+    G = {"mixed": [], "fp64": []}
+    for k in range(n_seeds):
+        v = systems.mb_velocities(n_mol, seed=1000 + k)
+        seeds = systems.noise_seeds(n_steps, seed=2000 + k)
+        for key, e in (("mixed", em), ("fp64", e64)):
+            e.set_state(x0, v)
+            e.forward(seeds, gamma, n_steps, n_steps, 0.001)
+            G[key].append(e.reverse(seeds, gamma, n_steps, n_steps, n_steps, 0.001)[1][0])
+    em.close()
+    e64.close()
+    gm, g64 = np.array(G["mixed"]), np.array(G["fp64"])
+    diff = gm.mean(0) - g64.mean(0)
+    se = np.sqrt(gm.var(0, ddof=1) / n_seeds + g64.var(0, ddof=1) / n_seeds)
+    z = diff / np.where(se > 0, se, np.inf)
+    paired = [grad_rel_err(gm[k], g64[k], p) for k in range(n_seeds)]
+    return {"n_seeds": n_seeds, "n_steps": n_steps, "gamma_per_ps": gamma,
+            "max_abs_z_of_mean_difference": float(np.max(np.abs(z))),
+            "z_per_parameter": [float(t) for t in z],
+            "rel_err_of_means": grad_rel_err(gm.mean(0), g64.mean(0), p),
+            "rel_err_of_one_seed_pairs": {"median": float(np.median(paired)), "max": float(max(paired))},
+            "reading": "|z| below ~3 for every parameter: the mixed and FP64 ensemble means agree "
+                       "within their standard error"}
+
+
+def time_gradients(eng, x0, v0, seeds, gamma, n_steps, n_steps_loss, reps, flush=None):
+    """Device time (ms) of `reps` gradients (forward + reverse from x0, v0), each bracketed by
+    CUDA events on the engine's stream, the L2 flushed in between; returns (mean ms, last
+    gradient, launches per gradient)."""
+    import torch
+    st = torch.cuda.ExternalStream(eng.stream())
+    ms, g, n0 = [], None, eng.launch_count()
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        eng.set_state(x0, v0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.forward(seeds, gamma, n_steps, n_steps_loss, 0.001)
+        _, g = eng.reverse(seeds, gamma, n_steps, n_steps_loss, n_steps_loss, 0.001)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms)), g, (eng.launch_count() - n0) // max(reps, 1)
+
+
+# ------------------------------------------------------- the 895-water target configuration
+TIP3P_FIXTURE = os.path.join(ROOT, "tests", "golden", "reference_inputs.npz")
+
+
+def cfg1_start(R, device):
+    """R replicas of the reference's own input box (water/tip3p.pdb: 895 waters, 3.0 nm, read
+    from the committed fixture), Maxwell-Boltzmann velocities at 295.15 K from seeds 0..R-1,
+    1 ps of Langevin equilibration (gamma = 5/ps) on the GPU; the target is the replica-mean
+    O-O RDF of a 0.5 ps run of the same code with sigma x 1.02, eps x 0.95.  Returns
+    (x [R * 2685, 3], v, params, target)."""
+    from revsim import Engine, constants as C, oo_l2_term, systems
+    d = np.load(TIP3P_FIXTURE)
+    x1, box = d["x_tip3p"], float(d["box_tip3p"])
+    x = np.concatenate([x1] * R)
+    v = np.concatenate([systems.mb_velocities(895, seed=r) for r in range(R)])
+    p = np.array(C.default_params("lj"))
+    eq = Engine([895] * R, [box] * R, precision="mixed", device=device)
+    eq.set_params(p)
+    eq.set_state(x, v)
+    eq.forward(systems.noise_seeds(1000 * R, seed=40).reshape(1000, R), 5.0, 1000, 1000, 0.001,
+               calc_loss=False)
+    x0, v0 = eq.get_state()
+    pt = p.copy()
+    pt[0] *= 1.02
+    pt[1] *= 0.95
+    eq.set_params(pt)
+    eq.forward(systems.noise_seeds(500 * R, seed=41).reshape(500, R), 5.0, 500, 500, 0.001,
+               calc_loss=False)
+    eq.set_loss([oo_l2_term(np.zeros(200))])
+    target = np.mean([eq.rdf(0, r) for r in range(R)], axis=0)
+    eq.close()
+    return x0, v0, p, target, box
+
+
+def cfg1_cpu_sample(x0, v0, p, target, box, n_s=10):
+    """The FP64 oracle on n_s forward + n_s reverse steps of one 895-water box (all host
+    threads), the loss amortised at one evaluation per 1,000 steps."""
+    from oracle import orc
+    from revsim import systems
+    s = orc.make_system(895, box)
+    t = orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, target, 2, 1.0)
+    loss = orc.Loss([t])
+    seeds = systems.noise_seeds(n_s, seed=99)
+    t0 = time.perf_counter()
+    xf, vf, _, sx, sv = orc.forward_sim(s, p, x0, v0, seeds, 0.0, n_s, n_s, 0.001, loss, False)
+    t1 = time.perf_counter()
+    orc.reverse_sim(s, p, xf, vf, seeds, 0.0, n_s, n_s, n_s, 0.001, sx, sv, loss)
+    t2 = time.perf_counter()
+    orc.loss_and_grads(s, p, loss, xf)
+    t3 = time.perf_counter()
+    t_loss = t3 - t2
+    t_steps = (t1 - t0) + (t2 - t1 - t_loss) + 2 * t_loss * n_s / 1000
+    return 2685 * n_s / t_steps, orc.num_threads(), (
+        f"{n_s} forward + {n_s} reverse steps of one 895-water box, FP64 oracle, loss amortised "
+        f"at one evaluation per 1,000 steps")
+
+
+def run_target_cfg1(a, device, reps=3, with_cpu=True):
+    """BASELINE configs[0] as the target of the engine: the 895-water box, 1,000 steps forward
+    + 1,000 reverse (velocity Verlet, gamma = 0), loss = O-O RDF L2 (200 bins, 0-1 nm) against
+    the sigma x 1.02 / eps x 0.95 target; R replicas of it batched in one handle (one launch
+    per step), mixed precision against the same engine in FP64 and against the FP64 oracle on
+    the host cores, with the gradient's accuracy (train()'s window schedule, a seed ensemble)
+    and the reconstruction of the start state in both precisions."""
+    import torch
+    from revsim import Engine, oo_l2_term, systems
+    R = a.cfg1_replicas
+    n, nl = 1000, 1000
+    x0, v0, p, target, box = cfg1_start(R, device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+    seeds = systems.noise_seeds(n * R, seed=42).reshape(n, R)
+    n_atoms = 2685 * R
+    out = {"workload": f"water_895mol_3nm_tip3p_x{R}replicas_lj_1000fwd+1000rev",
+           "start": "water/tip3p.pdb positions (committed fixture), MB velocities at 295.15 K, 1 ps "
+                    "Langevin equilibration on the GPU", "replicas": R, "n_atoms": n_atoms,
+           "n_steps": n, "gamma_per_ps": 0.0, "dt_ps": 0.001}
+    res = {}
+    for prec in ("mixed", "fp64"):
+        e = Engine([895] * R, [box] * R, precision=prec, device=device)
+        e.set_params(p)
+        e.set_loss([oo_l2_term(target)])
+        e.set_state(x0, v0)
+        shape = e.autotune()
+        time_gradients(e, x0, v0, seeds, 0.0, n, nl, 2, flush)          # warm-up
+        ms, g, launches = time_gradients(e, x0, v0, seeds, 0.0, n, nl, reps, flush)
+        xr, _ = e.get_state()
+        res[prec] = {"value": n_atoms * n / (ms * 1e-3), "ms_per_gradient": ms, "gpu_launches": launches,
+                     "shape": {"reverse": list(shape[0]), "forward": list(shape[1])},
+                     "recon_1000_steps": recon_error(xr, x0, box), "grad": g}
+        # one replica alone (the unbatched form) for the same comparison
+        e.close()
+        e1 = Engine(895, box, precision=prec, device=device)
+        e1.set_params(p)
+        e1.set_loss([oo_l2_term(target)])
+        e1.set_state(x0[:2685], v0[:2685])
+        e1.autotune()
+        time_gradients(e1, x0[:2685], v0[:2685], seeds[:, 0], 0.0, n, nl, 2, flush)
+        ms1, _, _ = time_gradients(e1, x0[:2685], v0[:2685], seeds[:, 0], 0.0, n, nl, reps, flush)
+        res[prec]["single_replica"] = {"value": 2685 * n / (ms1 * 1e-3), "ms_per_gradient": ms1}
+        e1.close()
+    gm, g64 = res["mixed"].pop("grad"), res["fp64"].pop("grad")
+    out["mixed"], out["fp64"] = res["mixed"], res["fp64"]
+    out["speedup_mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    out["speedup_mixed_over_fp64_single_replica"] = (res["mixed"]["single_replica"]["value"] /
+                                                     res["fp64"]["single_replica"]["value"])
+
+    def make(prec):
+        e = Engine(895, box, precision=prec, device=device)
+        e.set_params(p)
+        e.set_loss([oo_l2_term(target)])
+        return e
+    out["grad_rel_err_vs_fp64"] = {
+        "same_start_1000_steps": float(np.median([grad_rel_err(gm[r], g64[r], p) for r in range(R)])),
+        "same_start_note": "median over the replicas of one mixed / FP64 pair each: a chaotic pair "
+                           "over 1,000 untruncated steps, not a precision bound",
+        "train_schedule_windows": train_window_errors(make, x0[:2685], v0[:2685], p),
+        "seed_ensemble": seed_ensemble(make, x0[:2685], 895, p),
+        "definition": GRAD_ERR_DEFINITION}
+    if with_cpu:
+        val, cores, desc = cfg1_cpu_sample(x0[:2685], v0[:2685], p, target, box)
+        out["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+        out["speedup_mixed_over_cpu"] = res["mixed"]["value"] / val
+    return out
+
+
+def run_ours_cfg1(a):
+    """--workload cfg1: the target configuration as its own bench line."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    import build as _build
+    _build.build()
+    with Clocks(local) as clk:
+        t = run_target_cfg1(a, local, reps=max(a.steps, 1))
+    if rank != 0:
+        return
+    m = t["mixed"]
+    out = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": 1, "steps": a.steps,
+           "warmup": 2, "ms_per_step": m["ms_per_gradient"], "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+           "config": {"workload": t["workload"], "replicas": t["replicas"], "n_atoms": t["n_atoms"],
+                      "l2": "flushed (256 MiB write) between timed gradients",
+                      "start": t["start"]},
+           "e2e": {"value": m["value"], "unit": UNIT,
+                   "h2d_bytes_per_step": 2 * 3 * t["n_atoms"] * 8 + 2 * 1000 * t["replicas"] * 8,
+                   "d2h_bytes_per_step": 2 * t["replicas"] * 8 + t["replicas"] * 7 * 8},
+           "gpu_launches": m["gpu_launches"], "cpu_baseline": t.get("cpu_baseline"),
+           "clocks": clk.summary(), "target": t,
+           "e2e_note": "every timed gradient starts from host arrays (set_state), so value is end to end"}
+    print(json.dumps(out), flush=True)
 
 
 # --------------------------------------------------------- equilibration workload
@@ -1064,6 +1349,7 @@ def run_ours_diffusion(a):
     roofline = {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak.value,
                 "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
                 "traffic": GAS_REV_STEP_DRAM_BYTES if rev_dominant else GAS_FWD_STEP_DRAM_BYTES,
+                "traffic_source": "ncu constant from one capture of this kernel on this system",
                 "traffic_note": "ncu, cold caches (rows and positions are L2-resident live)",
                 "kernel": ("k_gas_step<LJ, reverse>" if rev_dominant else "k_gas_step<LJ, forward>"),
                 "launch_ms": launch_ms, "ipairs": ipairs, "pair_form_ipairs": form_pairs,
@@ -1373,6 +1659,7 @@ def run_ours_diamond(a):
         e1.record(s64)
         torch.cuda.synchronize()
         ms64 = e0.elapsed_time(e1)
+        recon["fp64"] = recon_error(e64.get_state()[0], x0, a.box)
         eng.set_state(x0, v0)
         _, _, gm = gradient()
         short = {}
@@ -1647,34 +1934,40 @@ def run_ours_replicas(a):
     import build as _build
     _build.build()
     from revsim import Engine, _lib, constants as C, oo_l2_term, systems
-    from revsim.distributed import allreduce_mean
-    n_mol, boxes, temps = replica_systems(a.n_replicas)
-    R, K = a.n_replicas, a.rep_steps
+    from revsim.distributed import allreduce_mean, allreduce_sum, rank_share
+    n_all, boxes_all, temps_all = replica_systems(a.n_replicas)
+    R_all, K = a.n_replicas, a.rep_steps
+    # this rank's share of the replicas (greedy atom-count balance); every per-replica input
+    # is selected by replica index, so the job is the same at every rank count
+    mine = rank_share(3 * n_all, world, rank)
+    n_mol, boxes, temps = n_all[mine], boxes_all[mine], temps_all[mine]
+    R = len(mine)
     p = np.array(C.default_params("lj"))
-    x = np.concatenate([systems.water_coords(n, b, seed=10 + r) for r, (n, b) in enumerate(zip(n_mol, boxes))])
-    v = np.concatenate([systems.mb_velocities(n, t, seed=100 + r) for r, (n, t) in enumerate(zip(n_mol, temps))])
+    x = np.concatenate([systems.water_coords(n_all[r], boxes_all[r], seed=10 + r) for r in mine])
+    v = np.concatenate([systems.mb_velocities(n_all[r], temps_all[r], seed=100 + r) for r in mine])
     eq = Engine(n_mol, boxes, temp=temps, precision="mixed", device=local)
     eq.set_params(p)
     eq.set_state(x, v)
     for blk in range(2):
-        eq.forward(systems.noise_seeds(1000 * R, seed=20 + blk).reshape(1000, R), 5.0, 1000, 1000,
-                   0.001, calc_loss=False)
+        eq.forward(systems.noise_seeds(1000 * R_all, seed=20 + blk).reshape(1000, R_all)[:, mine], 5.0,
+                   1000, 1000, 0.001, calc_loss=False)
     x0, v0 = eq.get_state()
     pt = p.copy()
     pt[0] *= 1.02
     pt[1] *= 0.95
     eq.set_params(pt)
-    eq.forward(systems.noise_seeds(1000 * R, seed=30).reshape(1000, R), 5.0, 1000, 1000, 0.001,
-               calc_loss=False)
+    eq.forward(systems.noise_seeds(1000 * R_all, seed=30).reshape(1000, R_all)[:, mine], 5.0, 1000, 1000,
+               0.001, calc_loss=False)
     eq.set_loss([oo_l2_term(np.zeros(200))])
-    target = np.mean([eq.rdf(0, r) for r in range(R)], axis=0)
+    # the target: the mean RDF over all replicas of all ranks (set-up, untimed)
+    target = allreduce_sum(np.sum([eq.rdf(0, r) for r in range(R)], axis=0)) / R_all
     eq.close()
     eng = Engine(n_mol, boxes, temp=temps, precision=a.precision, device=local)
     eng.set_params(p)
     eng.set_loss([oo_l2_term(target)])
     eng.set_state(x0, v0)
     shape = eng.autotune()
-    seeds = systems.noise_seeds(K * R, seed=400 + rank).reshape(K, R)
+    seeds = systems.noise_seeds(K * R_all, seed=400).reshape(K, R_all)[:, mine]
     stream = torch.cuda.ExternalStream(eng.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
@@ -1721,8 +2014,8 @@ def run_ours_replicas(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_step = total_ms / a.steps
-    n_atoms = int(3 * n_mol.sum())
-    value = world * n_atoms * K / (ms_step * 1e-3)
+    n_atoms = int(3 * n_all.sum())            # the whole job: every rank's replicas
+    value = n_atoms * K / (ms_step * 1e-3)
     eng.set_kernel_timing(True)
     gradient()
     kt_ms, kt_n = eng.kernel_time(0)
@@ -1740,22 +2033,24 @@ def run_ours_replicas(a):
     achieved = flops_launch / (launch_ms * 1e-3) / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value if peak.value else None, "traffic": None,
-                "kernel": "k_water_step<float, LJ, reverse> over all 64 replicas",
+                "kernel": "k_water_step<float, LJ, reverse> over this rank's replicas",
                 "launch_ms": launch_ms, "ipairs": ipairs, "flops_per_launch": flops_launch,
                 "forward_step_launch_ms": ft_ms / max(ft_n, 1),
                 "shape": {"reverse": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[0])),
                           "forward": dict(zip(("lanes_per_mol", "mols_per_cta", "unroll"), shape[1]))},
                 "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)"}
-    h2d = 2 * 3 * n_atoms * 8 + 2 * K * R * 8
-    d2h = 2 * R * 8 + R * len(p) * 8
+    h2d = 2 * 3 * n_atoms * 8 + 2 * K * R_all * 8
+    d2h = 2 * R_all * 8 + R_all * len(p) * 8
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-           "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
            "data": "synthetic",
-           "config": replicas_config(a, n_mol, {
+           "config": replicas_config(a, n_all, {
                "parallelism": f"replicas{world}" if world > 1 else "single",
                "gradient_exchange": "per-replica gradients averaged over all ranks by one "
-                                    "all-reduce of P + 1 doubles per update (timed)"}),
+                                    "all-reduce of P + 1 doubles per update (timed)",
+               "sharding": "rank k runs partition_replicas(atoms, N)[k] of the 64 replicas "
+                           "(greedy atom-count balance); the job is the same at every N"}),
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None, "clocks": clocks,
            "loss": {"forward_mean": float(lf.mean()), "reverse_mean": float(lr.mean())},
@@ -1773,6 +2068,8 @@ if __name__ == "__main__":
     args = parse()
     if args.workload == "replicas":
         run_ours_replicas(args)
+    elif args.workload == "cfg1":
+        run_ours_cfg1(args)
     elif args.workload == "mlp":
         run_ours_mlp(args)
     elif args.workload == "diamond":

@@ -260,8 +260,13 @@ int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, in
 /* Block shape of the step kernels (which = 0: reverse step, 1: forward step, -1: both):
  * lanes per molecule (8, 16 or 32), molecules per CTA, and the neighbour loop form
  * (1: one entry per lane per iteration, 2: two, 3: one with the next entry prefetched;
- * 3 allows at most 256 threads per CTA); 0 keeps the current value.  revsim_autotune times the
- * allowed shapes of each kernel on the current state and keeps the fastest. */
+ * 3 allows at most 256 threads per CTA); 0 keeps the current value.  Lanes per molecule are
+ * one setting for both kernels whatever `which` says (the order in which a molecule's
+ * forces are summed depends on it, and the reverse pass rebuilds the trajectory only when
+ * its forces are the forward pass's bits); a count the other kernel's shape does not allow
+ * returns REVSIM_ERR_BADARG.  revsim_autotune times the allowed shapes on the current state
+ * and keeps the lane count with the smallest forward + reverse time and, for it, each
+ * kernel's fastest shape. */
 int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes_per_mol,
                                 int32_t mols_per_cta, int32_t unroll);
 int32_t revsim_get_launch_shape(revsim_handle *h, int32_t which, int32_t *lanes_per_mol,

@@ -1784,27 +1784,56 @@ int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, in
     return REVSIM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+bool shape_ok(int G, int m, int U) {
+    const int thr = G * m;
+    return (G == 8 || G == 16 || G == 32) && m >= 1 && thr <= 512 && thr % 32 == 0 && U >= 1 && U <= 3 &&
+           !(U == 3 && thr > 256);
+}
+
+// Shape of one step kernel (dir 0 reverse, 1 forward), after shape_ok.
+int set_shape_dir(revsim_handle *h, int dir, int G, int m, int U) {
+    revsim_handle::Shape &sh = h->shp[dir];
+    sh.G = G;
+    sh.U = U;
+    if (m != sh.mpc || !sh.d_blk_rep) {
+        sh.mpc = m;
+        int rc = build_block_table(h, dir);
+        if (rc) return rc;
+    }
+    return REVSIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Lanes per molecule are one setting for both step kernels: a lane's share of a neighbour
+// row and the butterfly that sums the lanes depend on it, so forward and reverse forces are
+// the same bits only when both kernels use the same count.
 int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes, int32_t mpc,
                                 int32_t unroll) {
     if (!h || which < -1 || which > 1) return REVSIM_ERR_BADARG;
     CK(cudaSetDevice(h->dev));
     CK(cudaStreamSynchronize(h->st));
+    int G[2], m[2], U[2];
     for (int dir = 0; dir < 2; dir++) {
-        if (which >= 0 && which != dir) continue;
-        revsim_handle::Shape &sh = h->shp[dir];
-        const int G = lanes ? lanes : sh.G, m = mpc ? mpc : sh.mpc, U = unroll ? unroll : sh.U;
-        const int thr = G * m;
-        if ((G != 8 && G != 16 && G != 32) || m < 1 || thr > 512 || thr % 32 != 0 || U < 1 || U > 3 ||
-            (U == 3 && thr > 256))
-            return fail(h, REVSIM_ERR_BADARG, "unsupported launch shape");
-        sh.G = G;
-        sh.U = U;
-        if (m != sh.mpc || !sh.d_blk_rep) {
-            sh.mpc = m;
-            int rc = build_block_table(h, dir);
-            if (rc) return rc;
-        }
+        const revsim_handle::Shape &sh = h->shp[dir];
+        const bool sel = which < 0 || which == dir;
+        G[dir] = lanes ? lanes : sh.G;
+        m[dir] = sel && mpc ? mpc : sh.mpc;
+        U[dir] = sel && unroll ? unroll : sh.U;
+        if (!shape_ok(G[dir], m[dir], U[dir]))
+            return fail(h, REVSIM_ERR_BADARG,
+                        sel ? "unsupported launch shape"
+                            : "lanes per molecule apply to both step kernels; the other kernel's "
+                              "shape does not allow this count");
     }
+    for (int dir = 0; dir < 2; dir++)
+        if (int rc = set_shape_dir(h, dir, G[dir], m[dir], U[dir])) return rc;
     return REVSIM_OK;
 }
 
@@ -1817,9 +1846,11 @@ int32_t revsim_get_launch_shape(revsim_handle *h, int32_t which, int32_t *lanes,
     return REVSIM_OK;
 }
 
-// Project autotuner: times the reverse and the forward step kernel separately
-// (forces-only mode, on the current state) for every allowed (lanes per molecule,
-// molecules per CTA, entries per iteration) and keeps the fastest shape of each.
+// Project autotuner: for every lanes-per-molecule count G (one setting for both kernels, so
+// that forward and reverse forces agree bit for bit) it times the reverse and the forward
+// step kernel (forces-only mode, on the current state) at every allowed (molecules per CTA,
+// entries per iteration), and keeps the G with the smallest reverse + forward time and, for
+// it, each kernel's fastest shape.
 int32_t revsim_autotune(revsim_handle *h, double dt) {
     int rc = check_ready(h);
     if (rc) return rc;
@@ -1828,17 +1859,20 @@ int32_t revsim_autotune(revsim_handle *h, double dt) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    for (int dir = 0; dir < 2 && !rc; dir++) {
-        const bool rev = dir == 0;
-        double best = std::numeric_limits<double>::infinity();
-        int bg = h->shp[dir].G, bm = h->shp[dir].mpc, bu = h->shp[dir].U;
-        for (int G : {8, 16, 32}) {
+    double best_total = std::numeric_limits<double>::infinity();
+    int bm[2] = {h->shp[0].mpc, h->shp[1].mpc}, bu[2] = {h->shp[0].U, h->shp[1].U}, bg = h->shp[0].G;
+    for (int G : {8, 16, 32}) {
+        double tot = 0.0;
+        int gm[2] = {0, 0}, gu[2] = {1, 1};
+        for (int dir = 0; dir < 2 && !rc; dir++) {
+            const bool rev = dir == 0;
+            double best = std::numeric_limits<double>::infinity();
             for (int threads : {64, 128, 192, 256, 384, 512}) {
                 if (threads < G || threads % G) continue;
                 for (int U : {1, 2, 3}) {
                     const int mpc = threads / G;
-                    if (U == 3 && threads > 256) continue;
-                    if ((rc = revsim_set_launch_shape(h, dir, G, mpc, U))) break;
+                    if (!shape_ok(G, mpc, U)) continue;
+                    if ((rc = set_shape_dir(h, dir, G, mpc, U))) break;
                     StepArgs a = base_args(h, rev);
                     a.pos_in = h->d_pos[0];
                     a.wgt_in = h->d_wgt[0];
@@ -1857,17 +1891,25 @@ int32_t revsim_autotune(revsim_handle *h, double dt) {
                     CK(cudaEventElapsedTime(&ms, e0, e1));
                     if (ms < best) {
                         best = ms;
-                        bg = G;
-                        bm = mpc;
-                        bu = U;
+                        gm[dir] = mpc;
+                        gu[dir] = U;
                     }
                 }
                 if (rc) break;
             }
-            if (rc) break;
+            tot += best;
         }
-        if (!rc) rc = revsim_set_launch_shape(h, dir, bg, bm, bu);
+        if (rc) break;
+        if (tot < best_total) {
+            best_total = tot;
+            bg = G;
+            for (int d = 0; d < 2; d++) {
+                bm[d] = gm[d];
+                bu[d] = gu[d];
+            }
+        }
     }
+    for (int dir = 0; dir < 2 && !rc; dir++) rc = set_shape_dir(h, dir, bg, bm[dir], bu[dir]);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return rc;

@@ -28,6 +28,30 @@ def partition_replicas(n_atoms, world):
     return [sorted(p) for p in parts]
 
 
+def rank_share(n_atoms, world, rank):
+    """The replicas rank `rank` of `world` runs: its part of partition_replicas (ascending
+    replica indices).  Per-replica inputs (start states, temperatures, noise seed columns)
+    are selected with it, so each replica gets the same inputs at every world size."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    return partition_replicas(n_atoms, world)[rank]
+
+
+def allreduce_sum(values, group=None):
+    """Element-wise sum over the ranks of a float64 array (the local array when no process
+    group is initialised); used for set-up sums such as a replica-mean target."""
+    import torch
+    import torch.distributed as dist
+    v = np.asarray(values, dtype=np.float64)
+    if not (dist.is_available() and dist.is_initialized()):
+        return v.copy()
+    device = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    t = torch.from_numpy(v.copy()).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()
+
+
 def allreduce_mean(grads, group=None):
     """Mean over every replica of every rank of the per-replica gradients.
 

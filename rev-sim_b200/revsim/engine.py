@@ -299,7 +299,8 @@ class Engine:
         return ms.value, n.value
 
     def set_launch_shape(self, lanes=0, mols_per_cta=0, unroll=0, which=-1):
-        """which: 0 reverse step, 1 forward step, -1 both."""
+        """which: 0 reverse step, 1 forward step, -1 both.  ``lanes`` applies to both
+        kernels (forward and reverse forces must be summed in the same order)."""
         self._check(self._L.revsim_set_launch_shape(self._h, which, lanes, mols_per_cta, unroll))
 
     def launch_shape(self, which=0):
