@@ -244,6 +244,19 @@ int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double 
                              double dt, double clip_norm_threshold, double *loss_out,
                              double *dl_dp_out);
 
+/* CUDA-graph mode (no counterpart in the reference, whose step loop is water.jl:1029-1045 /
+ * 1492-1521): with enable = 1 each revsim_forward* / revsim_reverse* pass is captured from the
+ * handle's stream into a CUDA graph the first time it runs with a given set of arguments and
+ * handle configuration, and replayed with one graph launch on later calls (the per-step seeds
+ * or noise are copied to the device before the replay, so new seeds reuse the graph).  A
+ * change of parameters, loss terms, box, launch shape or any device buffer recaptures it (an
+ * update in place when the graph keeps its shape).  Passes with a host decision inside
+ * (barostat attempts, gradient clipping), with the enthalpy term or with kernel timing on run
+ * as plain launches.  Results are the same bits either way.  enable = 0 (the default) turns
+ * it off.  revsim_graph_stats: captures and replays so far. */
+int32_t revsim_set_graph_mode(revsim_handle *h, int32_t enable);
+int32_t revsim_graph_stats(const revsim_handle *h, int64_t *captures, int64_t *replays);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time with events. */
 void *revsim_stream(revsim_handle *h);
 

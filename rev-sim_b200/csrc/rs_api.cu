@@ -11,6 +11,7 @@
 //                next step's un-integration); snapshot restores, loss blocks and
 //                truncation exactly as the reference orders them.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -139,6 +140,18 @@ struct revsim_handle {
     double *d_bx = nullptr, *d_lsc = nullptr, *d_repE = nullptr;
     int *d_bacc = nullptr;
     int cell_cap = 0;   // allocated cells (the cell grid follows the boxes)
+    // CUDA-graph mode: each forward / reverse pass is captured once and replayed while its
+    // key (pass arguments, the handle's configuration generation `gen` and the allocation
+    // counter) is unchanged
+    bool graph_on = false;
+    unsigned long long gen = 0;
+    struct GraphCache {
+        std::vector<double> key;
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        long long launches = 0;
+    } gc[2];
+    long long graph_captures = 0, graph_replays = 0;
     // instrumentation
     long long launches = 0;
     bool ktime = false;
@@ -162,15 +175,23 @@ int fail(revsim_handle *h, int code, const std::string &msg) {
             return fail(h, REVSIM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// Every device allocation or free moves this counter; a captured pass graph holds device
+// addresses, so it is replayed only while the counter it was captured at still holds.
+std::atomic<unsigned long long> g_alloc_gen{0};
+
 template <typename T>
 cudaError_t dalloc(T **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
+    g_alloc_gen++;
     return cudaMalloc((void **)p, sizeof(T) * n);
 }
 
 void dfree(void *p) {
-    if (p) cudaFree(p);
+    if (p) {
+        g_alloc_gen++;
+        cudaFree(p);
+    }
 }
 
 }  // namespace
@@ -668,6 +689,7 @@ int set_cells(revsim_handle *h) {
     }
     h->band = (float)(2e-5 * std::max(1.0, lmax / 4.0));
     if (nc == h->nc) return REVSIM_OK;
+    h->gen++;
     if (ncell > h->cell_cap) {
         int **arrs[] = {&h->d_cell_cnt, &h->d_cell_start, &h->d_cell_fill, &h->d_cell_rep};
         for (int **a : arrs) {
@@ -1009,6 +1031,10 @@ void free_all(revsim_handle *h) {
     }
     for (int w = 0; w < 2; w++)
         for (cudaEvent_t e : h->ev[w]) cudaEventDestroy(e);
+    for (auto &c : h->gc) {
+        if (c.ex) cudaGraphExecDestroy(c.ex);
+        if (c.g) cudaGraphDestroy(c.g);
+    }
     if (h->st) cudaStreamDestroy(h->st);
 }
 
@@ -1241,6 +1267,8 @@ int32_t revsim_set_params(revsim_handle *h, const double *theta, int32_t n) {
         int rc = set_mlp(h, theta + h->P);
         if (rc) return rc;
     }
+    // the classical parameters are kernel arguments: a captured graph holds them
+    if (!h->have_params || !std::equal(h->theta.begin(), h->theta.end(), theta)) h->gen++;
     h->theta.assign(theta, theta + h->P);
     h->have_params = true;
     return REVSIM_OK;
@@ -1469,6 +1497,7 @@ int32_t revsim_set_barostat(revsim_handle *h, const revsim_barostat_desc *d) {
     h->baro_acc_tot.assign(h->R, 0);
     h->baro_step = 0;
     h->baro_on = true;
+    h->gen++;
     return REVSIM_OK;
 }
 
@@ -1501,6 +1530,7 @@ int32_t revsim_set_box(revsim_handle *h, const double *box) {
     CK(cudaMemcpyAsync(h->d_rep_box, h->box.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->fwd_valid = false;
+    h->gen++;
     return REVSIM_OK;
 }
 
@@ -1516,6 +1546,7 @@ int32_t revsim_set_enth_vap(revsim_handle *h, int32_t enable, double u_gas, doub
         CK(cudaMemset(h->d_ev_acc, 0, sizeof(double) * 2 * h->R));
     }
     h->ev_on = enable != 0;
+    h->gen++;
     h->ev_ugas = u_gas;
     h->ev_rt = rt;
     h->ev_target = target;
@@ -1624,6 +1655,61 @@ int upload_noise(revsim_handle *h, const uint64_t *seeds, const double *noise, i
     return REVSIM_OK;
 }
 
+// A pass (dir 0 reverse, 1 forward) through the handle's CUDA graph: captured from the
+// stream on the first call with a given key, replayed on later calls.  Passes with a host
+// decision inside (barostat attempts, gradient clipping), with the enthalpy term (its energy
+// rows are allocated on first use) or with per-launch timing run as plain launches.
+template <typename F>
+int run_graphed(revsim_handle *h, int dir, std::vector<double> key, F &&pass) {
+    if (!h->graph_on || h->ktime || h->baro_on || h->ev_on) return pass();
+    key.push_back((double)h->gen);
+    key.push_back((double)g_alloc_gen.load());
+    revsim_handle::GraphCache &c = h->gc[dir];
+    if (c.ex == nullptr || c.key != key) {
+        const long long l0 = h->launches;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        const int rc = pass();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->st, &g);
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            h->launches = l0;
+            if (rc) return rc;
+            return fail(h, REVSIM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        }
+        // a graph of the same shape updates the executable in place; otherwise a new one
+        bool updated = false;
+        if (c.ex) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(c.ex, g, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(c.ex);
+                c.ex = nullptr;
+            }
+        }
+        if (!updated) {
+            const cudaError_t ie = cudaGraphInstantiate(&c.ex, g, 0);
+            if (ie != cudaSuccess) {
+                cudaGraphDestroy(g);
+                c.ex = nullptr;
+                return fail(h, REVSIM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+            }
+        }
+        if (c.g) cudaGraphDestroy(c.g);
+        c.g = g;
+        c.key = key;
+        c.launches = h->launches - l0;
+        h->launches = l0;
+        h->graph_captures++;
+    }
+    CK(cudaGraphLaunch(c.ex, h->st));
+    h->launches += c.launches;
+    h->graph_replays++;
+    return REVSIM_OK;
+}
+
 int32_t forward_entry(revsim_handle *h, const uint64_t *noise_seeds, const double *noise, double gamma,
                       int32_t n_steps, int32_t n_steps_loss, double dt, int32_t calc_loss, double *loss_out) {
     int rc = check_ready(h);
@@ -1649,7 +1735,10 @@ int32_t forward_entry(revsim_handle *h, const uint64_t *noise_seeds, const doubl
     const long long bstep0 = h->baro_step;
     for (int attempt = 0; attempt < 3; attempt++) {
         if (h->nl_mode == REVSIM_NL_CHECKPOINT) ensure_list_store(h, n_ckpt);
-        if ((rc = forward_impl(h, gamma, n_steps, n_steps_loss, dt, calc_loss))) return rc;
+        const std::vector<double> key = {gamma, (double)n_steps, (double)n_steps_loss, dt, (double)calc_loss,
+                                         (double)h->use_noise};
+        if ((rc = run_graphed(h, 1, key, [&] { return forward_impl(h, gamma, n_steps, n_steps_loss, dt, calc_loss); })))
+            return rc;
         int s;
         if ((rc = read_status(h, &s))) return rc;
         if (!(s & ST_NLIST_OVERFLOW)) {
@@ -1705,7 +1794,10 @@ int32_t reverse_entry(revsim_handle *h, const uint64_t *noise_seeds, const doubl
         return fail(h, REVSIM_ERR_STATE, "reverse needs the forward pass of the same n_steps");
     NoiseGuard guard{h};
     if ((rc = upload_noise(h, noise_seeds, noise, n_steps))) return rc;
-    if ((rc = reverse_impl(h, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip_norm_threshold))) return rc;
+    const std::vector<double> key = {gamma, (double)n_steps, (double)n_steps_loss, (double)n_steps_trunc, dt,
+                                     clip_norm_threshold, (double)h->use_noise};
+    auto pass = [&] { return reverse_impl(h, gamma, n_steps, n_steps_loss, n_steps_trunc, dt, clip_norm_threshold); };
+    if ((rc = std::isfinite(clip_norm_threshold) ? pass() : run_graphed(h, 0, key, pass))) return rc;
     int s;
     if ((rc = read_status(h, &s))) return rc;
     if ((rc = status_code(h, s))) return rc;
@@ -1762,6 +1854,19 @@ int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double 
                          clip_norm_threshold, loss_out, dl_dp_out);
 }
 
+int32_t revsim_set_graph_mode(revsim_handle *h, int32_t enable) {
+    if (!h) return REVSIM_ERR_BADARG;
+    h->graph_on = enable != 0;
+    return REVSIM_OK;
+}
+
+int32_t revsim_graph_stats(const revsim_handle *h, int64_t *captures, int64_t *replays) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (captures) *captures = h->graph_captures;
+    if (replays) *replays = h->graph_replays;
+    return REVSIM_OK;
+}
+
 void *revsim_stream(revsim_handle *h) { return h ? (void *)h->st : nullptr; }
 
 int64_t revsim_launch_count(const revsim_handle *h) { return h ? h->launches : 0; }
@@ -1769,6 +1874,7 @@ int64_t revsim_launch_count(const revsim_handle *h) { return h ? h->launches : 0
 int32_t revsim_set_kernel_timing(revsim_handle *h, int32_t enable) {
     if (!h) return REVSIM_ERR_BADARG;
     h->ktime = enable != 0;
+    h->gen++;
     for (int w = 0; w < 2; w++) {
         h->kt_ms[w] = 0.0;
         h->kt_n[w] = 0;
@@ -1788,15 +1894,20 @@ int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, in
 
 namespace {
 
-bool shape_ok(int G, int m, int U) {
+// An allowed shape of step kernel dir (0 reverse, 1 forward): lanes 8, 16 or 32, whole warps,
+// at most 512 threads and no more than the kernel's register budget lets one CTA have.
+bool shape_ok(const revsim_handle *h, int dir, int G, int m, int U) {
     const int thr = G * m;
-    return (G == 8 || G == 16 || G == 32) && m >= 1 && thr <= 512 && thr % 32 == 0 && U >= 1 && U <= 3 &&
-           !(U == 3 && thr > 256);
+    if (!((G == 8 || G == 16 || G == 32) && m >= 1 && thr <= 512 && thr % 32 == 0 && U >= 1 && U <= 3 &&
+          !(U == 3 && thr > 256)))
+        return false;
+    return thr <= step_max_threads(h->prec == REVSIM_MIXED, dir == 0, U);
 }
 
 // Shape of one step kernel (dir 0 reverse, 1 forward), after shape_ok.
 int set_shape_dir(revsim_handle *h, int dir, int G, int m, int U) {
     revsim_handle::Shape &sh = h->shp[dir];
+    h->gen++;
     sh.G = G;
     sh.U = U;
     if (m != sh.mpc || !sh.d_blk_rep) {
@@ -1826,7 +1937,7 @@ int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes, 
         G[dir] = lanes ? lanes : sh.G;
         m[dir] = sel && mpc ? mpc : sh.mpc;
         U[dir] = sel && unroll ? unroll : sh.U;
-        if (!shape_ok(G[dir], m[dir], U[dir]))
+        if (!shape_ok(h, dir, G[dir], m[dir], U[dir]))
             return fail(h, REVSIM_ERR_BADARG,
                         sel ? "unsupported launch shape"
                             : "lanes per molecule apply to both step kernels; the other kernel's "
@@ -1871,7 +1982,7 @@ int32_t revsim_autotune(revsim_handle *h, double dt) {
                 if (threads < G || threads % G) continue;
                 for (int U : {1, 2, 3}) {
                     const int mpc = threads / G;
-                    if (!shape_ok(G, mpc, U)) continue;
+                    if (!shape_ok(h, dir, G, mpc, U)) continue;
                     if ((rc = set_shape_dir(h, dir, G, mpc, U))) break;
                     StepArgs a = base_args(h, rev);
                     a.pos_in = h->d_pos[0];

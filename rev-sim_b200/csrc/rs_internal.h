@@ -75,6 +75,31 @@ struct BondConsts {
     double kb, r0, ka, th0;
 };
 
+// Register budget per thread of the step kernels (__maxnreg__), by precision, direction and
+// loop form U.  FP32 (two entries per lane step in packed arithmetic): forward 128, reverse
+// 168 (U = 1) and 200 (U = 2, 3); FP64 (one entry per step): 128, and 255 for U = 3.
+#ifndef RS_NREG_F_FWD
+#define RS_NREG_F_FWD 128
+#endif
+#ifndef RS_NREG_F_REV1
+#define RS_NREG_F_REV1 168
+#endif
+#ifndef RS_NREG_F_REV2
+#define RS_NREG_F_REV2 200
+#endif
+#ifndef RS_NREG_F_REV3
+#define RS_NREG_F_REV3 200
+#endif
+constexpr int step_nreg(bool fp32, bool rev, int U) {
+    return !fp32 ? (U == 3 ? 255 : 128)
+                 : (!rev ? RS_NREG_F_FWD : (U == 3 ? RS_NREG_F_REV3 : (U == 1 ? RS_NREG_F_REV1 : RS_NREG_F_REV2)));
+}
+// The largest CTA such a kernel can be launched with: whole warps of the 65,536 registers of
+// an SM, a thread's registers allocated in units of 8.
+constexpr int step_max_threads(bool fp32, bool rev, int U) {
+    return 32 * (65536 / (32 * ((step_nreg(fp32, rev, U) + 7) / 8 * 8)));
+}
+
 // Everything the step kernels read or write.
 struct StepArgs {
     const int *blk_rep, *blk_mol0, *blk_nmol;

@@ -18,6 +18,7 @@
 #pragma once
 
 #include "rs_internal.h"
+#include "rs_pack.cuh"
 
 namespace rs {
 
@@ -213,12 +214,180 @@ __device__ __forceinline__ R vec_mi(R c1, R c2, R L, R invL) {
     return xfma(-r_rint(xmul(d, invL)), L, d);
 }
 
+// The learned pair correction's cubic segment at distance r of type QI (O-O, O-H, H-H):
+// interval gi, offset sm in it, F contribution -d1 = -u'(r) = -(c1 + 2 c2 s + 3 c3 s^2) / h and
+// dF/dr contribution -d2 = -(2 c2 + 6 c3 s) / h^2.
+template <typename R, bool REV>
+__device__ __forceinline__ void mlp_segment(const NbConsts<R> &nb, int QI, R r, int &gi, R &sm, R &d1,
+                                            R &d2) {
+    using V4m = typename V4T<R>::T;
+    const R q = xmul(r, nb.mlp_hinv);
+    gi = min((int)q, MLP_NG - 1);
+    sm = xsub(q, (R)gi);
+    const V4m cf = reinterpret_cast<const V4m *>(nb.mlp_tab)[QI * MLP_NG + gi];
+    d1 = xmul(xfma(sm, xfma(xmul(R(3), sm), cf.w, xmul(R(2), cf.z)), cf.y), nb.mlp_hinv);
+    d2 = R(0);
+    if (REV) d2 = xmul(xmul(xfma(xmul(R(6), sm), cf.w, xmul(R(2), cf.z)), nb.mlp_hinv), nb.mlp_hinv);
+}
+
+// -(dF/dc_k) (n . acoef_a) for the interval's coefficients c1, c2, c3 (one in-cutoff pair).
+template <typename R>
+__device__ __forceinline__ void mlp_adjoint(double *madj, int QI, int gi, R na, R sm, R hinv) {
+    const double v = (double)na * (double)hinv, s1 = (double)sm;
+    double *adj = madj + ((size_t)QI * MLP_NG + gi) * 4;
+    atomicAdd(adj + 1, v);
+    atomicAdd(adj + 2, 2.0 * s1 * v);
+    atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
+}
+
+// Two-entry form (FP32 kernels).  One (own atom KA, neighbour atom KB) slot of two neighbour
+// entries at once: the .x halves of the displacement (dx, dy, dz), of the VJP differences
+// (ex, ey, ez) = w_b - w_a, of the accumulators and of every intermediate belong to entry
+// "x", the .y halves to entry "y" (rs_pack.cuh).  Evaluated unconditionally: pairs outside the
+// neighbour mask or the cutoff contribute exact zeros, so the nine slots of an entry pair run
+// as straight-line code with no divergence between the lanes of a warp.
+template <typename R, int FORM, bool REV, int KA, int KB>
+__device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>::T dx,
+                                          typename PkT<R>::T dy, typename PkT<R>::T dz,
+                                          typename PkT<R>::T ex, typename PkT<R>::T ey,
+                                          typename PkT<R>::T ez, const R ca[3],
+                                          const NbConsts<R> &nb, typename PkT<R>::T f[3],
+                                          typename PkT<R>::T g[3], typename PkT<R>::T *th,
+                                          double *madj) {
+    using P = typename PkT<R>::T;
+    constexpr int NF = FormInfo<FORM>::NP;
+    constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
+    const P r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
+    const bool onx = bitx && r2.x <= nb.rc2;
+    const bool ony = bity && r2.y <= nb.rc2;
+    const P z = pk(onx ? R(1) : R(0), ony ? R(1) : R(0));
+    const P r2s = pk(onx ? r2.x : R(1), ony ? r2.y : R(1));
+    const P rinv = xrsqrt(r2s);
+    const P r = xmul(r2s, rinv);
+    const P invr2 = xmul(rinv, rinv);
+    constexpr int QI = (KA > 0) + (KB > 0);
+    const R qq = nb.qq[QI];
+    const P Fc = xmul(pk1(qq), xsub(invr2, xmul(pk1(nb.krf2), r)));
+    P F = Fc;
+    P dF = pk1(R(0));
+    P gf[4];
+    if (REV) dF = xneg(xmul(pk1(xadd(qq, qq)), xadd(xmul(invr2, rinv), pk1(nb.krf))));
+    if (KA == 0 && KB == 0) {
+        if (nb.fc.on) {
+            // one O-O slot in nine: the pair form runs per half with the scalar code
+            R Fx, Fy, dFx = R(0), dFy = R(0), gx[4], gy[4];
+            pair_form<R, PF, REV>(nb.fc, r.x, rinv.x, invr2.x, Fx, dFx, gx);
+            pair_form<R, PF, REV>(nb.fc, r.y, rinv.y, invr2.y, Fy, dFy, gy);
+            F = xadd(F, pk(Fx, Fy));
+            if (REV) {
+                dF = xadd(dF, pk(dFx, dFy));
+#pragma unroll
+                for (int p = 0; p < NF; p++) gf[p] = pk(gx[p], gy[p]);
+            }
+        }
+    }
+    int gix = 0, giy = 0;
+    R smx = R(0), smy = R(0);
+    if constexpr (FORM == F_LJ_MLP) {
+        R d1x, d1y, d2x, d2y;
+        mlp_segment<R, REV>(nb, QI, r.x, gix, smx, d1x, d2x);
+        mlp_segment<R, REV>(nb, QI, r.y, giy, smy, d1y, d2y);
+        F = xsub(F, pk(d1x, d1y));
+        if (REV) dF = xsub(dF, pk(d2x, d2y));
+    }
+    const P Fr = xmul(xmul(F, rinv), z);
+    // force on the own atom: -F n = -(F/r) dr
+    const P mFr = xneg(Fr);
+    f[0] = xfma(mFr, dx, f[0]);
+    f[1] = xfma(mFr, dy, f[1]);
+    f[2] = xfma(mFr, dz, f[2]);
+    if (REV) {
+        // VJP: M delta, delta = (ex, ey, ez), M = -[F' n n + (F/r)(I - n n)]
+        const P s = xmul(rinv, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
+        const P k1 = xmul(xmul(xsub(xmul(dF, z), Fr), s), rinv);
+        g[0] = xsub(g[0], xfma(k1, dx, xmul(Fr, ex)));
+        g[1] = xsub(g[1], xfma(k1, dy, xmul(Fr, ey)));
+        g[2] = xsub(g[2], xfma(k1, dz, xmul(Fr, ez)));
+        // dtheta: acoef_a . dF_a/dtheta_p = -(dF/dtheta_p) (n . acoef_a)
+        const P na = xmul(xmul(rinv, xfma(dz, pk1(ca[2]), xfma(dy, pk1(ca[1]), xmul(dx, pk1(ca[0]))))), z);
+        th[NF] = xfma(xneg(xmul(Fc, pk1(nb.twoinvq))), na, th[NF]);
+        if (KA == 0 && KB == 0) {
+            if (nb.fc.on) {
+#pragma unroll
+                for (int p = 0; p < NF; p++) th[p] = xfma(xneg(gf[p]), na, th[p]);
+            }
+        }
+        if constexpr (FORM == F_LJ_MLP) {
+            if (onx) mlp_adjoint<R>(madj, QI, gix, na.x, smx, nb.mlp_hinv);
+            if (ony) mlp_adjoint<R>(madj, QI, giy, na.y, smy, nb.mlp_hinv);
+        }
+    }
+}
+
+// Displacement of one slot for both entries: cx / cy = the neighbour atom's coordinate in
+// entry x / y, c = the own atom's; formed per half (the two results land in one register
+// pair) and packed from there on.  SHIFT: one periodic image per molecule pair (chosen from
+// the O-O vector) is applied to all nine atom pairs; d + s rounds exactly as Molly's
+// (c2 - c1) -/+ L, and the image is the minimum one for every pair within the cutoff whenever
+// L > 2 (cutoff + 2 * max O-H distance).  Otherwise per slot d - L rint(d / L), which for every
+// pair within the cutoff gives the same bits as Molly's rule (vec1d); it differs only for
+// pairs near L/2, far outside the cutoff.
+template <typename R, bool SHIFT>
+__device__ __forceinline__ typename PkT<R>::T slot_d(R c, R cx, R cy, typename PkT<R>::T s, R L, R invL) {
+    using P = typename PkT<R>::T;
+    const P d = pk(xsub(cx, c), xsub(cy, c));
+    if (SHIFT) return xadd(d, s);
+    const P q = xmul(d, pk1(invL));
+    return xfma(pk(-r_rint(q.x), -r_rint(q.y)), pk1(L), d);
+}
+
+template <typename R>
+__device__ __forceinline__ R image_shift(R d, R L, R hL) {
+    return d > hL ? -L : (d < -hL ? L : R(0));
+}
+
+// The three slots of own atom KA against the three atoms of the two neighbour molecules
+// (entry x: pbx, wbx; entry y: pby, wby).
+template <typename R, int FORM, bool REV, bool SHIFT, int KA>
+__device__ __forceinline__ void pair_row(uint32_t maskx, uint32_t masky, const typename V4T<R>::T &pa,
+                                         const typename V4T<R>::T pbx[3],
+                                         const typename V4T<R>::T pby[3],
+                                         const typename V4T<R>::T &wa,
+                                         const typename V4T<R>::T wbx[3],
+                                         const typename V4T<R>::T wby[3], const R ca[3],
+                                         const typename PkT<R>::T sh[3], R L, R invL,
+                                         const NbConsts<R> &nb, typename PkT<R>::T f[3],
+                                         typename PkT<R>::T g[3], typename PkT<R>::T *th,
+                                         double *madj) {
+    using P = typename PkT<R>::T;
+#define RS_SLOT(KB)                                                                               \
+    {                                                                                             \
+        P ex = pk1(R(0)), ey = pk1(R(0)), ez = pk1(R(0));                                         \
+        if (REV) {                                                                                \
+            ex = pk(xsub(wbx[KB].x, wa.x), xsub(wby[KB].x, wa.x));                                \
+            ey = pk(xsub(wbx[KB].y, wa.y), xsub(wby[KB].y, wa.y));                                \
+            ez = pk(xsub(wbx[KB].z, wa.z), xsub(wby[KB].z, wa.z));                                \
+        }                                                                                         \
+        pair_term<R, FORM, REV, KA, KB>((maskx >> (3 * KA + KB)) & 1u, (masky >> (3 * KA + KB)) & 1u, \
+                                        slot_d<R, SHIFT>(pa.x, pbx[KB].x, pby[KB].x, sh[0], L, invL), \
+                                        slot_d<R, SHIFT>(pa.y, pbx[KB].y, pby[KB].y, sh[1], L, invL), \
+                                        slot_d<R, SHIFT>(pa.z, pbx[KB].z, pby[KB].z, sh[2], L, invL), \
+                                        ex, ey, ez, ca, nb, f, g, th, madj);                      \
+    }
+    RS_SLOT(0);
+    RS_SLOT(1);
+    RS_SLOT(2);
+#undef RS_SLOT
+}
+
+// Single-entry form of the slots, used by the FP64 kernels (no packed FP64 arithmetic, and
+// two entries per lane would exceed their registers).
 // One (own atom KA, neighbour atom KB) interaction with displacement (dx, dy, dz),
 // evaluated unconditionally: pairs outside the neighbour mask or the cutoff
 // contribute exact zeros, so the nine slots of an entry run as straight-line code with
 // no divergence between the lanes of a warp (each lane holds a different neighbour).
 template <typename R, int FORM, bool REV, int KA, int KB>
-__device__ __forceinline__ void pair_term(bool bit, R dx, R dy, R dz,
+__device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
                                           const typename V4T<R>::T &wa,
                                           const typename V4T<R>::T &wb, const R ca[3],
                                           const NbConsts<R> &nb, R f[3], R g[3], R *th,
@@ -304,28 +473,28 @@ __device__ __forceinline__ void pair_term(bool bit, R dx, R dy, R dz,
 // (c2 - c1) -/+ L, and the image is the minimum one for every pair within the cutoff
 // whenever L > 2 (cutoff + 2 * max O-H distance).  Otherwise per-slot vec_mi.
 template <typename R, bool SHIFT>
-__device__ __forceinline__ R slot_d(R ca_, R cb_, R s, R L, R invL) {
+__device__ __forceinline__ R slot_d1(R ca_, R cb_, R s, R L, R invL) {
     if (SHIFT) return xadd(xsub(cb_, ca_), s);
     return vec_mi(ca_, cb_, L, invL);
 }
 
 template <typename R, bool SHIFT>
-__device__ __forceinline__ R image_shift(R d, R L, R hL) {
+__device__ __forceinline__ R image_shift1(R d, R L, R hL) {
     return d > hL ? -L : (d < -hL ? L : R(0));
 }
 
 template <typename R, int FORM, bool REV, bool SHIFT, int KA>
-__device__ __forceinline__ void pair_row(uint32_t mask, const typename V4T<R>::T &pa,
+__device__ __forceinline__ void pair_row1(uint32_t mask, const typename V4T<R>::T &pa,
                                          const typename V4T<R>::T pb[3],
                                          const typename V4T<R>::T &wa,
                                          const typename V4T<R>::T wb[3], const R ca[3],
                                          const R sh[3], R L, R invL, const NbConsts<R> &nb,
                                          R f[3], R g[3], R *th, double *madj) {
 #define RS_SLOT(KB)                                                                             \
-    pair_term<R, FORM, REV, KA, KB>((mask >> (3 * KA + KB)) & 1u,                               \
-                                    slot_d<R, SHIFT>(pa.x, pb[KB].x, sh[0], L, invL),           \
-                                    slot_d<R, SHIFT>(pa.y, pb[KB].y, sh[1], L, invL),           \
-                                    slot_d<R, SHIFT>(pa.z, pb[KB].z, sh[2], L, invL), wa, wb[KB], \
+    pair_term1<R, FORM, REV, KA, KB>((mask >> (3 * KA + KB)) & 1u,                               \
+                                    slot_d1<R, SHIFT>(pa.x, pb[KB].x, sh[0], L, invL),           \
+                                    slot_d1<R, SHIFT>(pa.y, pb[KB].y, sh[1], L, invL),           \
+                                    slot_d1<R, SHIFT>(pa.z, pb[KB].z, sh[2], L, invL), wa, wb[KB], \
                                     ca, nb, f, g, th, madj)
     RS_SLOT(0);
     RS_SLOT(1);
@@ -455,22 +624,16 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
     }
 }
 
-// Register budget per thread.  FP32: the forward kernels at 80 (no spills), the reverse
-// kernel at 104 (U = 1, no spills), 128 (U = 2) and 168 (U = 3, launched with at most 256
-// threads; software pipelining wants the registers); on the 9,000-atom box these budgets
-// took the autotuned gradient from 134.5 to 139.8 M atom-steps/s.  FP64: 128, and 255
-// for U = 3.
+// Register budget per thread: step_nreg (rs_internal.h).
 template <typename R, bool REV, int U>
 constexpr int step_maxnreg() {
-    if (sizeof(R) == 8) return U == 3 ? 255 : 128;
-    if (!REV) return 80;
-    return U == 3 ? 168 : (U == 1 ? 104 : 128);
+    return step_nreg(sizeof(R) == 4, REV, U);
 }
 
-// U = 1: one neighbour entry per lane per iteration; 2: two entries, all loads issued
-// first; 3: one entry, with the next entry's index and coordinates loaded while the
-// current one is computed (software pipelining; launched with at most 256 threads so
-// the compiler may use more registers).
+// U = 1: one neighbour entry (FP32: entry pair) per lane per iteration; 2: two, all loads
+// issued first; 3: one, with the next one's indices and coordinates loaded while the
+// current one is computed (software pipelining; launched with at most 256 threads).  Every
+// form sums a lane's entries in the same order, so at one lane count they give the same bits.
 template <typename R, int FORM, int G, bool REV, bool SHIFT, int U>
 __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a, NbConsts<R> nb,
                                                                       BondConsts bc) {
@@ -499,16 +662,27 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                        ? nb.mlp_adj + ((size_t)rep * MLP_NCOPY + (blk % MLP_NCOPY)) * MLP_NT * MLP_NG * 4
                        : nullptr;
 
+    // FP32: two entries per lane step in packed arithmetic (rs_pack.cuh), accumulated in
+    // the halves of f2, g2, th2 and combined after the row loop; FP64: one entry per step
+    // into f, g, th.
+    constexpr bool PACKED = sizeof(R) == 4;
+    using P = typename PkT<R>::T;
+    P f2[3][3], g2[3][3], th2[NTH];
     R f[3][3], g[3][3], th[NTH];
 #pragma unroll
     for (int k = 0; k < 3; k++)
 #pragma unroll
         for (int u = 0; u < 3; u++) {
+            f2[k][u] = pk1(R(0));
+            g2[k][u] = pk1(R(0));
             f[k][u] = R(0);
             g[k][u] = R(0);
         }
 #pragma unroll
-    for (int p = 0; p < NTH; p++) th[p] = R(0);
+    for (int p = 0; p < NTH; p++) {
+        th2[p] = pk1(R(0));
+        th[p] = R(0);
+    }
 
     V4 pa[3], wa[3];
     R ca[3][3];
@@ -552,22 +726,6 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
         const uint32_t *__restrict__ row = a.nbr + (size_t)I * a.cap;
         const int cnt = min(a.nbr_cnt[I], a.cap);
         const R hL = xmul(L, R(0.5));
-        // one neighbour entry: displacement image and the nine slots
-        auto entry = [&](uint32_t ent, const V4 pbq[3], const V4 wbq[3]) {
-            const uint32_t mask = ent >> 23;
-            R sh[3] = {R(0), R(0), R(0)};
-            if (SHIFT) {
-                sh[0] = image_shift<R, SHIFT>(xsub(pbq[0].x, pa[0].x), L, hL);
-                sh[1] = image_shift<R, SHIFT>(xsub(pbq[0].y, pa[0].y), L, hL);
-                sh[2] = image_shift<R, SHIFT>(xsub(pbq[0].z, pa[0].z), L, hL);
-            }
-            pair_row<R, FORM, REV, SHIFT, 0>(mask, pa[0], pbq, wa[0], wbq, ca[0], sh, L, invL, nb, f[0],
-                                             g[0], th, madj);
-            pair_row<R, FORM, REV, SHIFT, 1>(mask, pa[1], pbq, wa[1], wbq, ca[1], sh, L, invL, nb, f[1],
-                                             g[1], th, madj);
-            pair_row<R, FORM, REV, SHIFT, 2>(mask, pa[2], pbq, wa[2], wbq, ca[2], sh, L, invL, nb, f[2],
-                                             g[2], th, madj);
-        };
         auto fetch = [&](uint32_t ent, V4 pbq[3], V4 wbq[3]) {
             const int J = (int)(ent & 0x7FFFFFu);
 #pragma unroll
@@ -576,42 +734,137 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 if (REV) wbq[k] = wgt[3 * J + k];
             }
         };
-        if (U == 3) {
-            // padding entries (past the row end) read molecule 0 with an empty mask
-            uint32_t ent_n = lane < cnt ? __ldg(row + lane) : 0u;
-            V4 pbn[3], wbn[3];
-            fetch(ent_n, pbn, wbn);
-            for (int e = lane; e < cnt; e += G) {
-                const uint32_t ent = ent_n;
-                V4 pbq[3], wbq[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    pbq[k] = pbn[k];
-                    if (REV) wbq[k] = wbn[k];
+        // padding entries (past the row end) read molecule 0 with an empty mask
+        auto ent_at = [&](int e) { return e < cnt ? __ldg(row + e) : 0u; };
+        if constexpr (PACKED) {
+            // Entries e and e + G of the row as one pair (halves x and y); a lane takes the
+            // pairs starting at lane, lane + 2G, lane + 4G, ...
+            auto entry2 = [&](uint32_t ex, uint32_t ey, const V4 pbx[3], const V4 wbx[3], const V4 pby[3],
+                              const V4 wby[3]) {
+                P sh[3] = {pk1(R(0)), pk1(R(0)), pk1(R(0))};
+                if (SHIFT) {
+                    sh[0] = pk(image_shift(xsub(pbx[0].x, pa[0].x), L, hL), image_shift(xsub(pby[0].x, pa[0].x), L, hL));
+                    sh[1] = pk(image_shift(xsub(pbx[0].y, pa[0].y), L, hL), image_shift(xsub(pby[0].y, pa[0].y), L, hL));
+                    sh[2] = pk(image_shift(xsub(pbx[0].z, pa[0].z), L, hL), image_shift(xsub(pby[0].z, pa[0].z), L, hL));
                 }
-                ent_n = e + G < cnt ? __ldg(row + e + G) : 0u;
-                if (e + G < cnt) fetch(ent_n, pbn, wbn);
-                entry(ent, pbq, wbq);
+                const uint32_t mx = ex >> 23, my = ey >> 23;
+                pair_row<R, FORM, REV, SHIFT, 0>(mx, my, pa[0], pbx, pby, wa[0], wbx, wby, ca[0], sh, L, invL, nb,
+                                                 f2[0], g2[0], th2, madj);
+                pair_row<R, FORM, REV, SHIFT, 1>(mx, my, pa[1], pbx, pby, wa[1], wbx, wby, ca[1], sh, L, invL, nb,
+                                                 f2[1], g2[1], th2, madj);
+                pair_row<R, FORM, REV, SHIFT, 2>(mx, my, pa[2], pbx, pby, wa[2], wbx, wby, ca[2], sh, L, invL, nb,
+                                                 f2[2], g2[2], th2, madj);
+            };
+            if (U == 3) {
+                // one entry pair per iteration, the next pair's indices and coordinates
+                // loaded while the current pair is computed
+                uint32_t nx = ent_at(lane), ny = ent_at(lane + G);
+                V4 pnx[3], wnx[3], pny[3], wny[3];
+                fetch(nx, pnx, wnx);
+                fetch(ny, pny, wny);
+                for (int e = lane; e < cnt; e += 2 * G) {
+                    const uint32_t ex = nx, ey = ny;
+                    V4 pbx[3], wbx[3], pby[3], wby[3];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        pbx[k] = pnx[k];
+                        pby[k] = pny[k];
+                        if (REV) {
+                            wbx[k] = wnx[k];
+                            wby[k] = wny[k];
+                        }
+                    }
+                    if (e + 2 * G < cnt) {
+                        nx = ent_at(e + 2 * G);
+                        ny = ent_at(e + 3 * G);
+                        fetch(nx, pnx, wnx);
+                        fetch(ny, pny, wny);
+                    }
+                    entry2(ex, ey, pbx, wbx, pby, wby);
+                }
+            } else {
+                for (int e0 = lane; e0 < cnt; e0 += 2 * U * G) {
+                    // U entry pairs per lane per iteration: all their loads are issued first
+                    constexpr int UP = U == 3 ? 1 : U;
+                    uint32_t ex[UP], ey[UP];
+#pragma unroll
+                    for (int q = 0; q < UP; q++) {
+                        ex[q] = ent_at(e0 + 2 * q * G);
+                        ey[q] = ent_at(e0 + (2 * q + 1) * G);
+                    }
+                    V4 pbx[UP][3], wbx[UP][3], pby[UP][3], wby[UP][3];
+#pragma unroll
+                    for (int q = 0; q < UP; q++) {
+                        fetch(ex[q], pbx[q], wbx[q]);
+                        fetch(ey[q], pby[q], wby[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < UP; q++) entry2(ex[q], ey[q], pbx[q], wbx[q], pby[q], wby[q]);
+                }
             }
         } else {
-            for (int e0 = lane; e0 < cnt; e0 += U * G) {
-                // U entries per lane per iteration: all their loads are issued first.
-                uint32_t ent[U == 3 ? 1 : U];
-#pragma unroll
-                for (int q = 0; q < U; q++) {
-                    const int e = e0 + q * G;
-                    ent[q] = e < cnt ? __ldg(row + e) : 0u;   // padding: molecule 0, empty mask
+            // one neighbour entry: displacement image and the nine slots
+            auto entry = [&](uint32_t ent, const V4 pbq[3], const V4 wbq[3]) {
+                const uint32_t mask = ent >> 23;
+                R sh[3] = {R(0), R(0), R(0)};
+                if (SHIFT) {
+                    sh[0] = image_shift1<R, SHIFT>(xsub(pbq[0].x, pa[0].x), L, hL);
+                    sh[1] = image_shift1<R, SHIFT>(xsub(pbq[0].y, pa[0].y), L, hL);
+                    sh[2] = image_shift1<R, SHIFT>(xsub(pbq[0].z, pa[0].z), L, hL);
                 }
-                V4 pb[U == 3 ? 1 : U][3], wb[U == 3 ? 1 : U][3];
+                pair_row1<R, FORM, REV, SHIFT, 0>(mask, pa[0], pbq, wa[0], wbq, ca[0], sh, L, invL, nb, f[0],
+                                                  g[0], th, madj);
+                pair_row1<R, FORM, REV, SHIFT, 1>(mask, pa[1], pbq, wa[1], wbq, ca[1], sh, L, invL, nb, f[1],
+                                                  g[1], th, madj);
+                pair_row1<R, FORM, REV, SHIFT, 2>(mask, pa[2], pbq, wa[2], wbq, ca[2], sh, L, invL, nb, f[2],
+                                                  g[2], th, madj);
+            };
+            if (U == 3) {
+                uint32_t ent_n = ent_at(lane);
+                V4 pbn[3], wbn[3];
+                fetch(ent_n, pbn, wbn);
+                for (int e = lane; e < cnt; e += G) {
+                    const uint32_t ent = ent_n;
+                    V4 pbq[3], wbq[3];
 #pragma unroll
-                for (int q = 0; q < U; q++) fetch(ent[q], pb[q], wb[q]);
+                    for (int k = 0; k < 3; k++) {
+                        pbq[k] = pbn[k];
+                        if (REV) wbq[k] = wbn[k];
+                    }
+                    ent_n = ent_at(e + G);
+                    if (e + G < cnt) fetch(ent_n, pbn, wbn);
+                    entry(ent, pbq, wbq);
+                }
+            } else {
+                for (int e0 = lane; e0 < cnt; e0 += U * G) {
+                    // U entries per lane per iteration: all their loads are issued first
+                    constexpr int UE = U == 3 ? 1 : U;
+                    uint32_t ent[UE];
 #pragma unroll
-                for (int q = 0; q < U; q++) entry(ent[q], pb[q], wb[q]);
+                    for (int q = 0; q < UE; q++) ent[q] = ent_at(e0 + q * G);
+                    V4 pb[UE][3], wb[UE][3];
+#pragma unroll
+                    for (int q = 0; q < UE; q++) fetch(ent[q], pb[q], wb[q]);
+#pragma unroll
+                    for (int q = 0; q < UE; q++) entry(ent[q], pb[q], wb[q]);
+                }
             }
         }
     }
 
-    // Fixed butterfly over the group: every lane ends with the same totals.
+    // FP32: the lane's two halves.  Then a fixed butterfly over the group: every lane ends
+    // with the same totals.
+    if constexpr (PACKED) {
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                f[k][u] = xadd(f2[k][u].x, f2[k][u].y);
+                g[k][u] = xadd(g2[k][u].x, g2[k][u].y);
+            }
+#pragma unroll
+        for (int p = 0; p < NTH; p++) th[p] = xadd(th2[p].x, th2[p].y);
+    }
 #pragma unroll
     for (int k = 0; k < 3; k++)
 #pragma unroll

@@ -36,7 +36,7 @@ EXPORTS = [
     "revsim_probe_fp32_tflops", "revsim_rdf_loss_grad_noalloc", "revsim_energy_grad",
     "revsim_set_enth_vap", "revsim_loss_parts", "revsim_loss_and_grads", "revsim_set_barostat",
     "revsim_barostat_state", "revsim_set_box", "revsim_probe_fp64_tflops",
-    "revsim_forward_noise", "revsim_reverse_noise",
+    "revsim_forward_noise", "revsim_reverse_noise", "revsim_set_graph_mode", "revsim_graph_stats",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -183,6 +183,8 @@ def load(path=LIB_PATH):
         "revsim_forward": (i32, [vp, pu64, d, i32, i32, d, i32, pd]),
         "revsim_reverse": (i32, [vp, pu64, d, i32, i32, i32, d, d, pd, pd]),
         "revsim_forward_noise": (i32, [vp, pd, d, i32, i32, d, i32, pd]),
+        "revsim_set_graph_mode": (i32, [vp, i32]),
+        "revsim_graph_stats": (i32, [vp, pi64, pi64]),
         "revsim_reverse_noise": (i32, [vp, pd, d, i32, i32, i32, d, d, pd, pd]),
         "revsim_stream": (vp, [vp]),
         "revsim_launch_count": (i64, [vp]),

@@ -288,6 +288,17 @@ class Engine:
         return loss, g
 
     # --------------------------------------------------------- instrumentation
+    def set_graph_mode(self, on=True):
+        """Capture each forward / reverse pass into a CUDA graph and replay it on later calls
+        with the same arguments (revsim_set_graph_mode); the results are the same bits."""
+        self._check(self._L.revsim_set_graph_mode(self._h, 1 if on else 0))
+
+    def graph_stats(self):
+        """(captures, replays) of the handle's CUDA graphs so far."""
+        c, r = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self._L.revsim_graph_stats(self._h, ctypes.byref(c), ctypes.byref(r)))
+        return c.value, r.value
+
     def set_kernel_timing(self, on):
         self._check(self._L.revsim_set_kernel_timing(self._h, 1 if on else 0))
 
