@@ -718,7 +718,12 @@ def run_target_cfg1(a, device, reps=3, with_cpu=True):
         time_gradients(e, x0, v0, seeds, 0.0, n, nl, 2, flush)          # warm-up
         ms, g, launches = time_gradients(e, x0, v0, seeds, 0.0, n, nl, reps, flush)
         xr, _ = e.get_state()
+        e.set_graph_mode(True)
+        time_gradients(e, x0, v0, seeds, 0.0, n, nl, 2, flush)
+        msg, _, _ = time_gradients(e, x0, v0, seeds, 0.0, n, nl, reps, flush)
+        e.set_graph_mode(False)
         res[prec] = {"value": n_atoms * n / (ms * 1e-3), "ms_per_gradient": ms, "gpu_launches": launches,
+                     "cuda_graph": {"value": n_atoms * n / (msg * 1e-3), "ms_per_gradient": msg},
                      "shape": {"reverse": list(shape[0]), "forward": list(shape[1])},
                      "recon_1000_steps": recon_error(xr, x0, box), "grad": g}
         # one replica alone (the unbatched form) for the same comparison
@@ -731,6 +736,12 @@ def run_target_cfg1(a, device, reps=3, with_cpu=True):
         time_gradients(e1, x0[:2685], v0[:2685], seeds[:, 0], 0.0, n, nl, 2, flush)
         ms1, _, _ = time_gradients(e1, x0[:2685], v0[:2685], seeds[:, 0], 0.0, n, nl, reps, flush)
         res[prec]["single_replica"] = {"value": 2685 * n / (ms1 * 1e-3), "ms_per_gradient": ms1}
+        # the same passes captured in CUDA graphs (revsim_set_graph_mode), against chained launches
+        e1.set_graph_mode(True)
+        time_gradients(e1, x0[:2685], v0[:2685], seeds[:, 0], 0.0, n, nl, 2, flush)
+        msg, _, _ = time_gradients(e1, x0[:2685], v0[:2685], seeds[:, 0], 0.0, n, nl, reps, flush)
+        res[prec]["single_replica"]["cuda_graph"] = {"value": 2685 * n / (msg * 1e-3), "ms_per_gradient": msg,
+                                                     "captures_replays": list(e1.graph_stats())}
         e1.close()
     gm, g64 = res["mixed"].pop("grad"), res["fp64"].pop("grad")
     out["mixed"], out["fp64"] = res["mixed"], res["fp64"]
