@@ -3,12 +3,13 @@
 
 Tolerances: neighbour pair set bit-exact; forces 1e-10 (FP64) / 1e-5 (mixed) relative,
 norm-wise; a 30-step forward + reverse gradient, in units of dL/dlog(theta), for velocity
-Verlet (gamma = 0, the benchmark's) and Langevin (gamma = 1/ps) dynamics: norm-wise 1e-6
+Verlet (gamma = 0, the benchmark's) and Langevin (gamma = 1/ps) dynamics: norm-wise 1e-5
 (FP64) / 1e-4 (mixed), and per parameter 1e-4 (FP64) / 1e-3 (mixed) floored at 1 % of the
 largest component.  The per-parameter bar is wider than on the small boxes (1e-6 / 1e-4)
 because at 9,000 atoms the bonded-parameter gradients are sums of ~10^4 terms of both signs
 that cancel to a small remainder, whose relative rounding the different summation orders of
-engine and oracle expose (measured 5e-6 to 2.2e-5 in FP64 for k_b, r0, k_a, theta0).
+engine and oracle expose (measured 5e-6 to 2.2e-5 in FP64 for k_b, r0, k_a, theta0, and
+4.6e-6 norm-wise, all of it from r0).
 Reconstruction of the start state < 1e-9 nm (FP64) / 1e-7 nm (mixed) and |L_rev - L_fwd| <
 1e-7 (water.jl:1613-1614).
 """
@@ -69,7 +70,7 @@ def test_box45_forces(box45, prec, tol):
 
 
 @pytest.mark.parametrize("gamma", [0.0, 1.0])
-@pytest.mark.parametrize("prec,tol_norm,tol", [("fp64", 1e-6, 1e-4), ("mixed", 1e-4, 1e-3)])
+@pytest.mark.parametrize("prec,tol_norm,tol", [("fp64", 1e-5, 1e-4), ("mixed", 1e-4, 1e-3)])
 def test_box45_gradient(box45, gamma, prec, tol_norm, tol):
     x, v, s, target = box45
     p = np.array(C.default_params())

@@ -1,7 +1,9 @@
 """CUDA-graph mode (revsim_set_graph_mode): forward and reverse passes captured once and
-replayed give the same bits as plain launches, across new seeds, host noise, a parameter
-change (recapture) and batched replicas; passes with a host decision inside (gradient
-clipping) still run, as plain launches."""
+replayed give the same trajectories (bit for bit) as plain launches, across new seeds, host
+noise, a parameter change (recapture) and batched replicas; passes with a host decision
+inside (gradient clipping) still run, as plain launches.  The losses and gradients agree to
+1e-12 relative: the smoothed-RDF histogram sums with FP64 atomics, whose order varies from
+run to run in the last bits, in either mode."""
 
 import numpy as np
 import pytest
@@ -23,6 +25,16 @@ def _target(x, n_mol, box):
     s = orc.make_system(n_mol, box)
     t0 = orc.RdfTerm(0, 0, 0.005, 0.005, 0.0005, 0.04, 200, 0, 1, np.zeros(200), 2, 1.0)
     return 0.9 * orc.rdf(s, t0, x) + 0.05
+
+
+def _same(a, b):
+    """Trajectories bit for bit; losses and gradients to the RDF atomics' rounding."""
+    lf, xf, vf, lr, g, x0, v0 = a
+    lf2, xf2, vf2, lr2, g2, x02, v02 = b
+    for u, w in ((xf, xf2), (vf, vf2), (x0, x02), (v0, v02)):
+        np.testing.assert_array_equal(u, w)
+    for u, w in ((lf, lf2), (lr, lr2), (g, g2)):
+        np.testing.assert_allclose(u, w, rtol=1e-12, atol=1e-12 * np.abs(w).max())
 
 
 def _run(e, x, v, seeds, p, n=60, nl=30, tr=20, noise=None, clip=np.inf):
@@ -50,24 +62,15 @@ def test_graph_replays_match_plain_launches(small_water, prec):
     graph.set_graph_mode(True)
     cases = [(systems.noise_seeds(60, seed=s), p) for s, p in ((1, p0), (2, p0), (3, p1), (4, p1))]
     for seeds, p in cases:
-        a = _run(plain, x, v, seeds, p)
-        b = _run(graph, x, v, seeds, p)
-        for u, w in zip(a, b):
-            np.testing.assert_array_equal(u, w)
+        _same(_run(plain, x, v, seeds, p), _run(graph, x, v, seeds, p))
     captures, replays = graph.graph_stats()
     # forward + reverse captured for p0 and again for p1; every pass launched as a graph
     assert captures == 4 and replays == 8, (captures, replays)
     assert plain.graph_stats() == (0, 0)
     # host noise through the graph, and a clipped reverse pass (plain launches)
     xi = np.stack([plain.noise([sd]) for sd in cases[0][0]])
-    a = _run(plain, x, v, None, p0, noise=xi)
-    b = _run(graph, x, v, None, p0, noise=xi)
-    for u, w in zip(a, b):
-        np.testing.assert_array_equal(u, w)
-    a = _run(plain, x, v, cases[0][0], p0, clip=1e-3)
-    b = _run(graph, x, v, cases[0][0], p0, clip=1e-3)
-    for u, w in zip(a, b):
-        np.testing.assert_array_equal(u, w)
+    _same(_run(plain, x, v, None, p0, noise=xi), _run(graph, x, v, None, p0, noise=xi))
+    _same(_run(plain, x, v, cases[0][0], p0, clip=1e-3), _run(graph, x, v, cases[0][0], p0, clip=1e-3))
 
 
 def test_graph_mode_with_replicas():
@@ -88,5 +91,4 @@ def test_graph_mode_with_replicas():
         out.append(res)
         e.close()
     for ra, rb in zip(*out):
-        for u, w in zip(ra, rb):
-            np.testing.assert_array_equal(u, w)
+        _same(ra, rb)
