@@ -84,6 +84,16 @@ typedef struct {
  * W2[64][64], b2[64], w3[64], b3. */
 #define REVSIM_MLP_NPARAMS 15939
 
+/* Arithmetic of the learned term's network (no reference counterpart).  The interval table
+ * is built from the network's value and r-derivative at its 1,025 nodes per type, and the
+ * reverse pass carries the table's adjoints back to the weights; both run either in FP64
+ * scalar kernels (REVSIM_MLP_FP64, the default) or on the tensor cores with BF16 operands
+ * and FP32 accumulation (REVSIM_MLP_BF16_TC: the forward and r-tangent GEMMs, the backward
+ * through both streams with the mixed second derivative d^2u/dr dtheta, and the weight-
+ * gradient GEMMs over the node batch; parameters stay FP64 and are rounded to BF16 per use). */
+#define REVSIM_MLP_FP64 0
+#define REVSIM_MLP_BF16_TC 1
+
 /* One smoothed-RDF loss term (rdf_differentiable + loss_rdf_part, water.jl:631-697):
  * grid x_k = x_min + step*k, k < n_grid; Gaussian exp(-(x-d)^2/width) truncated at
  * |x-d| <= exp_cutoff and normalised per distance; loss =
@@ -256,6 +266,15 @@ int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double 
  * it off.  revsim_graph_stats: captures and replays so far. */
 int32_t revsim_set_graph_mode(revsim_handle *h, int32_t enable);
 int32_t revsim_graph_stats(const revsim_handle *h, int64_t *captures, int64_t *replays);
+
+/* The learned term's network arithmetic (REVSIM_MLP_FP64 or REVSIM_MLP_BF16_TC); rebuilds the
+ * interval table from the current parameters.  REVSIM_ERR_STATE on a handle without the term. */
+int32_t revsim_set_mlp_precision(revsim_handle *h, int32_t mode);
+/* The network itself on the tensor cores (BF16 operands, FP32 accumulation) at n distances
+ * per type: r [3][n] nm (O-O, O-H, H-H rows; NULL = the table's nodes k rc / 1024, n = 1025),
+ * u [3][n] = MLP(phi(r)) fc(r) and du [3][n] = du/dr.  For tests and for timing a per-pair
+ * evaluation against the table. */
+int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that time with events. */
 void *revsim_stream(revsim_handle *h);

@@ -69,6 +69,10 @@ struct revsim_handle {
     double *d_mlp_theta = nullptr, *d_mlp_adj = nullptr, *d_mlp_scratch = nullptr,
            *d_mlp_grad = nullptr;
     void *d_mlp_tab = nullptr;
+    int mlp_mode = 0;           // 0: FP64 network evaluation, 1: BF16 tensor cores (rs_mlp_tc.cu)
+    void *d_mlp_tc = nullptr;   // scratch of the tensor-core backward pass
+    double *d_mlp_r = nullptr, *d_mlp_u = nullptr;   // revsim_mlp_eval buffers
+    size_t mlp_eval_cap = 0;
     double *d_epart = nullptr;   // [M][P + 1] energy-gradient partials
     bool have_params = false, have_state = false;
 
@@ -1011,7 +1015,7 @@ void free_all(revsim_handle *h) {
         dfree(sh.d_blk_nmol);
     }
     void *mptrs[] = {h->d_mlp_theta, h->d_mlp_adj, h->d_mlp_scratch, h->d_mlp_grad, h->d_mlp_tab,
-                     h->d_epart};
+                     h->d_epart, h->d_mlp_tc, h->d_mlp_r, h->d_mlp_u};
     for (void *p : mptrs) dfree(p);
     void *ptrs[] = {h->d_mol_rep, h->d_atom_rep,
                     h->d_rep_atom0, h->d_rep_nmol, h->d_rep_box, h->d_rep_sdO, h->d_rep_sdH,
@@ -1211,6 +1215,23 @@ int32_t revsim_sizes(const revsim_handle *h, int64_t *n_atoms, int32_t *n_params
 
 namespace {
 // Upload the MLP parameters and rebuild the interval table.
+// The interval table from the device copy of the MLP parameters, in the handle's network
+// precision (FP64 scalar kernels, or BF16 tensor cores with FP32 accumulation).
+int build_mlp_table(revsim_handle *h) {
+    cudaError_t e;
+    if (h->mlp_mode == 1) {
+        e = launch_mlp_tc_eval(h->d_mlp_theta, MLP_NT, h->rc, MLP_WIDTH, MLP_NG + 1, nullptr,
+                               mlp_scratch_nodes(h->d_mlp_scratch, 0), mlp_scratch_nodes(h->d_mlp_scratch, 1), h->st);
+        if (e == cudaSuccess) e = launch_mlp_table_from_nodes(h->prec, h->d_mlp_scratch, h->rc, h->d_mlp_tab, h->st);
+    } else {
+        e = launch_mlp_table(h->prec, h->d_mlp_theta, h->rc, h->d_mlp_scratch, h->d_mlp_tab, h->st);
+    }
+    h->launches += 2;
+    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP table: ") + cudaGetErrorString(e));
+    CK(cudaStreamSynchronize(h->st));
+    return REVSIM_OK;
+}
+
 int set_mlp(revsim_handle *h, const double *theta_mlp) {
     const size_t adj = (size_t)h->R * MLP_NCOPY * MLP_NT * MLP_NG * 4;
     if (!h->d_mlp_theta) {
@@ -1222,20 +1243,26 @@ int set_mlp(revsim_handle *h, const double *theta_mlp) {
         CK(cudaMemset(h->d_mlp_adj, 0, sizeof(double) * adj));
     }
     CK(cudaMemcpyAsync(h->d_mlp_theta, theta_mlp, sizeof(double) * MLP_NPARAMS, cudaMemcpyHostToDevice, h->st));
-    cudaError_t e = launch_mlp_table(h->prec, h->d_mlp_theta, h->rc, h->d_mlp_scratch, h->d_mlp_tab, h->st);
-    h->launches += 2;
-    if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP table: ") + cudaGetErrorString(e));
-    CK(cudaStreamSynchronize(h->st));
-    return REVSIM_OK;
+    return build_mlp_table(h);
 }
 
 // The accumulated interval-coefficient adjoints of every replica -> dtheta_mlp [R][MLP_NPARAMS].
 int mlp_grads(revsim_handle *h, std::vector<double> &out) {
     for (int r = 0; r < h->R; r++) {
-        cudaError_t e = launch_mlp_backprop(h->d_mlp_theta, h->rc,
-                                            h->d_mlp_adj + (size_t)r * MLP_NCOPY * MLP_NT * MLP_NG * 4, MLP_NCOPY,
-                                            h->d_mlp_scratch, h->d_mlp_grad + (size_t)r * MLP_NPARAMS, h->st);
-        h->launches += 3;
+        const double *cadj = h->d_mlp_adj + (size_t)r * MLP_NCOPY * MLP_NT * MLP_NG * 4;
+        double *grad = h->d_mlp_grad + (size_t)r * MLP_NPARAMS;
+        cudaError_t e;
+        if (h->mlp_mode == 1) {
+            e = launch_mlp_node_adjoints(cadj, MLP_NCOPY, h->rc, h->d_mlp_scratch, h->st);
+            if (e == cudaSuccess)
+                e = launch_mlp_tc_backprop(h->d_mlp_theta, MLP_NT, h->rc, MLP_WIDTH,
+                                           mlp_scratch_nodes(h->d_mlp_scratch, 2),
+                                           mlp_scratch_nodes(h->d_mlp_scratch, 3), h->d_mlp_tc, grad, h->st);
+            h->launches += 4;
+        } else {
+            e = launch_mlp_backprop(h->d_mlp_theta, h->rc, cadj, MLP_NCOPY, h->d_mlp_scratch, grad, h->st);
+            h->launches += 3;
+        }
         if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("MLP backprop: ") + cudaGetErrorString(e));
     }
     out.resize((size_t)h->R * MLP_NPARAMS);
@@ -1864,6 +1891,46 @@ int32_t revsim_graph_stats(const revsim_handle *h, int64_t *captures, int64_t *r
     if (!h) return REVSIM_ERR_BADARG;
     if (captures) *captures = h->graph_captures;
     if (replays) *replays = h->graph_replays;
+    return REVSIM_OK;
+}
+
+int32_t revsim_set_mlp_precision(revsim_handle *h, int32_t mode) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (!h->mlp) return fail(h, REVSIM_ERR_STATE, "the handle has no learned pair term");
+    if (mode != REVSIM_MLP_FP64 && mode != REVSIM_MLP_BF16_TC) return fail(h, REVSIM_ERR_BADARG, "bad MLP precision");
+    CK(cudaSetDevice(h->dev));
+    if (mode == REVSIM_MLP_BF16_TC && !h->d_mlp_tc) {
+        void *p = nullptr;
+        g_alloc_gen++;
+        CK(cudaMalloc(&p, mlp_tc_scratch_bytes()));
+        h->d_mlp_tc = p;
+    }
+    h->mlp_mode = mode;
+    if (h->have_params && h->d_mlp_theta) return build_mlp_table(h);
+    return REVSIM_OK;
+}
+
+int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du) {
+    if (!h || n < 1 || !u || !du) return REVSIM_ERR_BADARG;
+    if (!h->mlp || !h->have_params || !h->d_mlp_theta) return fail(h, REVSIM_ERR_STATE, "no learned pair term set");
+    CK(cudaSetDevice(h->dev));
+    const size_t need = (size_t)MLP_NT * n;
+    if (need > h->mlp_eval_cap) {
+        dfree(h->d_mlp_r);
+        dfree(h->d_mlp_u);
+        h->d_mlp_r = h->d_mlp_u = nullptr;
+        h->mlp_eval_cap = 0;
+        CK(dalloc(&h->d_mlp_r, need));
+        CK(dalloc(&h->d_mlp_u, 2 * need));
+        h->mlp_eval_cap = need;
+    }
+    if (r) CK(cudaMemcpyAsync(h->d_mlp_r, r, sizeof(double) * need, cudaMemcpyHostToDevice, h->st));
+    CK(launch_mlp_tc_eval(h->d_mlp_theta, MLP_NT, h->rc, MLP_WIDTH, n, r ? h->d_mlp_r : nullptr, h->d_mlp_u,
+                          h->d_mlp_u + need, h->st));
+    h->launches++;
+    CK(cudaMemcpyAsync(u, h->d_mlp_u, sizeof(double) * need, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(du, h->d_mlp_u + need, sizeof(double) * need, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
     return REVSIM_OK;
 }
 

@@ -246,6 +246,22 @@ cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *ca
                                 double *scratch, double *dtheta, cudaStream_t st, int nt = MLP_NT,
                                 double w = MLP_WIDTH);
 
+// Node values -> interval table, the scratch's node arrays (0 u, 1 du, 2 au, 3 ad), and the
+// coefficient adjoints -> node adjoints alone (rs_mlp.cu).
+cudaError_t launch_mlp_table_from_nodes(int prec, double *scratch, double rc, void *tab, cudaStream_t st,
+                                        int nt = MLP_NT);
+double *mlp_scratch_nodes(double *scratch, int which);
+cudaError_t launch_mlp_node_adjoints(const double *cadj, int ncopy, double rc, double *scratch, cudaStream_t st,
+                                     int nt = MLP_NT);
+// The network on the tensor cores (rs_mlp_tc.cu, BF16 operands, FP32 accumulation): u and
+// du/dr at n distances per type (r null: the NG + 1 nodes of [0, rc]); the backward pass from
+// node adjoints au, ad [nt][NG + 1] to dtheta [nt * MLP_PER_TYPE] (FP64), with its scratch.
+size_t mlp_tc_scratch_bytes();
+cudaError_t launch_mlp_tc_eval(const double *theta, int nt, double rc, double w, int n, const double *r,
+                               double *u, double *du, cudaStream_t st);
+cudaError_t launch_mlp_tc_backprop(const double *theta, int nt, double rc, double w, const double *au,
+                                   const double *ad, void *scratch, double *dtheta, cudaStream_t st);
+
 cudaError_t launch_pack(int N, int prec, const double *x, const double *C, double mO, double mH,
                         const int *atom_rep, const double *rep_box, void *pos, void *wgt,
                         cudaStream_t st);

@@ -248,6 +248,35 @@ cudaError_t launch_mlp_table(int prec, const double *theta, double rc, double *s
     return cudaGetLastError();
 }
 
+// The tensor-core path (rs_mlp_tc.cu) shares the node arrays of this scratch: the interval
+// table from node values computed elsewhere, and the node adjoints alone.
+cudaError_t launch_mlp_table_from_nodes(int prec, double *scratch, double rc, void *tab, cudaStream_t st,
+                                        int nt) {
+    if (nt < 1 || nt > MLP_NT) return cudaErrorInvalidValue;
+    const size_t S = (size_t)MLP_NT * (NG + 1) * NA, NN = (size_t)MLP_NT * (NG + 1);
+    double *u = scratch + 2 * S, *du = u + NN;
+    const int n = nt * NG;
+    if (prec == 1)
+        k_mlp_coef<float4><<<(n + 255) / 256, 256, 0, st>>>(u, du, rc, nt, (float4 *)tab);
+    else
+        k_mlp_coef<double4><<<(n + 255) / 256, 256, 0, st>>>(u, du, rc, nt, (double4 *)tab);
+    return cudaGetLastError();
+}
+
+double *mlp_scratch_nodes(double *scratch, int which) {
+    const size_t S = (size_t)MLP_NT * (NG + 1) * NA, NN = (size_t)MLP_NT * (NG + 1);
+    return scratch + 2 * S + (size_t)which * NN;   // 0: u, 1: du, 2: au, 3: ad
+}
+
+cudaError_t launch_mlp_node_adjoints(const double *cadj, int ncopy, double rc, double *scratch, cudaStream_t st,
+                                     int nt) {
+    if (nt < 1 || nt > MLP_NT) return cudaErrorInvalidValue;
+    const int nn = nt * (NG + 1);
+    k_mlp_adj_nodes<<<(nn + 255) / 256, 256, 0, st>>>(cadj, ncopy, nt, rc, mlp_scratch_nodes(scratch, 2),
+                                                        mlp_scratch_nodes(scratch, 3));
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mlp_backprop(const double *theta, double rc, const double *cadj, int ncopy,
                                 double *scratch, double *dtheta, cudaStream_t st, int nt, double w) {
     if (nt < 1 || nt > MLP_NT) return cudaErrorInvalidValue;

@@ -288,6 +288,23 @@ class Engine:
         return loss, g
 
     # --------------------------------------------------------- instrumentation
+    def set_mlp_precision(self, mode="fp64"):
+        """The learned term's network arithmetic: "fp64" (scalar kernels) or "bf16_tc" (tensor
+        cores, BF16 operands, FP32 accumulation)."""
+        self._check(self._L.revsim_set_mlp_precision(self._h, {"fp64": 0, "bf16_tc": 1}[mode]))
+
+    def mlp_eval(self, r=None):
+        """The network on the tensor cores at distances r [3, n] (None: the 1,025 table nodes):
+        (u [3, n], du/dr [3, n])."""
+        if r is None:
+            n, rp = 1025, None
+        else:
+            r = np.ascontiguousarray(r, dtype=np.float64).reshape(3, -1)
+            n, rp = r.shape[1], f64p(r)
+        u, du = np.zeros((3, n)), np.zeros((3, n))
+        self._check(self._L.revsim_mlp_eval(self._h, n, rp, f64p(u), f64p(du)))
+        return u, du
+
     def set_graph_mode(self, on=True):
         """Capture each forward / reverse pass into a CUDA graph and replay it on later calls
         with the same arguments (revsim_set_graph_mode); the results are the same bits."""
