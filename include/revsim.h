@@ -254,6 +254,21 @@ int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double 
                              double dt, double clip_norm_threshold, double *loss_out,
                              double *dl_dp_out);
 
+/* Integrator arithmetic (no counterpart in the reference, whose FP64 step water.jl:1032-1037
+ * and inverse 1496-1502 rebuild the start state only to rounding, which the dynamics' chaos
+ * amplifies: in FP64 to ~1e-8 nm over 1,000 steps, and in mixed precision until a position
+ * crosses an FP32 rounding boundary, after which the two passes' forces differ).
+ * REVSIM_INTEGRATOR_REFERENCE (default): the reference's arithmetic.  REVSIM_INTEGRATOR_EXACT:
+ * positions, velocities and box sides on the grid of multiples of 2^-44 nm (nm/ps), every
+ * increment of the step (kick F dt / m, half drifts v dt / 2, the O step's result) rounded to
+ * it, so the reverse pass subtracts exactly what the forward pass added: with gamma = 0 the
+ * trajectory is rebuilt bit for bit in both precisions, however long the run; with friction
+ * the O step's inverse stays approximate.  The state and boxes are rounded to the grid at the
+ * start of each forward pass (<= 2^-45 nm, ~3e-14 nm).  Invalidates the forward record. */
+#define REVSIM_INTEGRATOR_REFERENCE 0
+#define REVSIM_INTEGRATOR_EXACT 1
+int32_t revsim_set_integrator(revsim_handle *h, int32_t mode);
+
 /* CUDA-graph mode (no counterpart in the reference, whose step loop is water.jl:1029-1045 /
  * 1492-1521): with enable = 1 each revsim_forward* / revsim_reverse* pass is captured from the
  * handle's stream into a CUDA graph the first time it runs with a given set of arguments and

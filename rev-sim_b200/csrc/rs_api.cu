@@ -148,6 +148,7 @@ struct revsim_handle {
     // key (pass arguments, the handle's configuration generation `gen` and the allocation
     // counter) is unchanged
     bool graph_on = false;
+    bool exact = false;   // the exactly reversible integrator (REVSIM_INTEGRATOR_EXACT)
     unsigned long long gen = 0;
     struct GraphCache {
         std::vector<double> key;
@@ -322,7 +323,29 @@ StepArgs base_args(revsim_handle *h, bool rev) {
     a.status = h->d_status;
     a.mO = h->mO;
     a.mH = h->mH;
+    a.exact = h->exact ? 1 : 0;
     return a;
+}
+
+int set_cells(revsim_handle *h);
+
+// The exact integrator's grid: box sides and then the state rounded to it (a no-op for a state
+// already on it, e.g. the end state of a previous exact pass).
+int quantize_for_exact(revsim_handle *h) {
+    bool moved = false;
+    for (int r = 0; r < h->R; r++) {
+        const double q = qgrid(h->box[r]);
+        moved = moved || q != h->box[r];
+        h->box[r] = q;
+    }
+    if (moved) {
+        CK(cudaMemcpyAsync(h->d_rep_box, h->box.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice, h->st));
+        if (int rc = set_cells(h)) return rc;
+        h->gen++;
+    }
+    CK(launch_quantize_state(h->N, h->d_x, h->d_v, h->d_atom_rep, h->d_rep_box, h->st));
+    h->launches++;
+    return REVSIM_OK;
 }
 
 int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a_in) {
@@ -1747,6 +1770,7 @@ int32_t forward_entry(revsim_handle *h, const uint64_t *noise_seeds, const doubl
     const size_t n3 = 3 * (size_t)h->N;
     NoiseGuard guard{h};
     if ((rc = upload_noise(h, noise_seeds, noise, n_steps))) return rc;
+    if (h->exact && (rc = quantize_for_exact(h))) return rc;
     const size_t n_snap = (h->nlog > 0 ? (size_t)n_steps / h->nlog : 0) + 1;
     const size_t n_ckpt = n_steps > 0 ? (size_t)(n_steps - 1) / h->nf + 1 : 1;
     if ((rc = ensure_store(h, &h->d_snap_x, &h->snap_cap, n_snap * n3))) return rc;
@@ -1879,6 +1903,16 @@ int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double 
     if (h && !host_noise) return fail(h, REVSIM_ERR_BADARG, "bad reverse arguments");
     return reverse_entry(h, nullptr, host_noise, gamma, n_steps, n_steps_loss, n_steps_trunc, dt,
                          clip_norm_threshold, loss_out, dl_dp_out);
+}
+
+int32_t revsim_set_integrator(revsim_handle *h, int32_t mode) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (mode != REVSIM_INTEGRATOR_REFERENCE && mode != REVSIM_INTEGRATOR_EXACT)
+        return fail(h, REVSIM_ERR_BADARG, "bad integrator");
+    if (h->exact != (mode == REVSIM_INTEGRATOR_EXACT)) h->gen++;
+    h->exact = mode == REVSIM_INTEGRATOR_EXACT;
+    h->fwd_valid = false;
+    return REVSIM_OK;
 }
 
 int32_t revsim_set_graph_mode(revsim_handle *h, int32_t enable) {

@@ -7,6 +7,7 @@
 // nor reassociate, so the two kernels round identically whatever else they do.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -66,6 +67,34 @@ __device__ __forceinline__ R vec1d(R c1, R c2, R L) {
 // Molly wrap_coords: c - floor(c / L) * L, each operation rounded separately.
 __device__ __forceinline__ double wrap1d(double c, double L) {
     return __dsub_rn(c, __dmul_rn(floor(__ddiv_rn(c, L)), L));
+}
+
+// Exactly reversible integration (revsim_set_integrator, REVSIM_INTEGRATOR_EXACT): positions,
+// velocities and box sides are kept on the grid of multiples of 2^-44 (nm, nm/ps), and every
+// increment of the velocity Verlet step (the kick F dt / m, each half drift v dt / 2) is
+// rounded to that grid before it is added.  Sums of grid values below 2^9 in magnitude are
+// exact in FP64, so the reverse pass, which subtracts the same increments computed from the
+// same bits, restores the previous state exactly: with gamma = 0 the start state is rebuilt
+// bit for bit however long the run (the reference's FP64 arithmetic rebuilds it to rounding
+// that the dynamics' chaos amplifies).  With friction the O step v c + xi s is rounded to the
+// grid too and its inverse is approximate, as in the reference.
+constexpr double kGrid = 5.684341886080801486968994140625e-14;   // 2^-44
+constexpr double kGridInv = 17592186044416.0;                    // 2^44
+__host__ __device__ __forceinline__ double qgrid(double y) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(rint(__dmul_rn(y, kGridInv)), kGrid);
+#else
+    return std::rint(y * kGridInv) * kGrid;
+#endif
+}
+
+// Wrap into [0, L) exactly for grid values (c - k L, then one correction into the interval),
+// so that the wrap of a reversed step undoes the forward wrap.
+__device__ __forceinline__ double wrap_exact(double c, double L) {
+    double w = __dsub_rn(c, __dmul_rn(floor(__ddiv_rn(c, L)), L));
+    if (w < 0.0) w = __dadd_rn(w, L);
+    else if (w >= L) w = __dsub_rn(w, L);
+    return w;
 }
 
 // Coordinate written to the gather buffers read by the step kernels: an O as stored

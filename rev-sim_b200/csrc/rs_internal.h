@@ -122,6 +122,7 @@ struct StepArgs {
     // when set it replaces the Philox draw of seed_cur / seed_next.
     const double *noise_cur, *noise_next;
     int mode;
+    int exact;         // 1: the exactly reversible integrator (grid increments, rs_device.cuh)
 };
 
 enum StepMode {
@@ -267,6 +268,10 @@ cudaError_t launch_pack(int N, int prec, const double *x, const double *C, doubl
                         cudaStream_t st);
 cudaError_t launch_unintegrate(int M, int prec, const StepArgs &a, const int *mol_rep,
                                cudaStream_t st);
+// Positions (wrapped into the replica's box) and velocities rounded to the exact
+// integrator's grid, in place.
+cudaError_t launch_quantize_state(int N, double *x, double *v, const int *atom_rep, const double *rep_box,
+                                  cudaStream_t st);
 cudaError_t launch_clip_post(int N, const StepArgs &a, const int *atom_rep, const double *scale,
                              cudaStream_t st);
 cudaError_t launch_init_adjoint(int N, const double *g, double c, double *A, double *B, double *C,

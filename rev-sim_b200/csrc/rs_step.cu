@@ -69,10 +69,13 @@ __global__ void k_unintegrate(int M, StepArgs a, const int *mol_rep) {
         for (int u = 0; u < 3; u++) {
             const size_t e = 3 * (size_t)i + u;
             double x = a.x[e], v = a.v[e];
-            x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            const double h2 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
+            x = __dsub_rn(x, a.exact ? qgrid(h2) : h2);
             v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
-            x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-            x = wrap1d(x, Ld);
+            if (a.exact) v = qgrid(v);
+            const double h1 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
+            x = __dsub_rn(x, a.exact ? qgrid(h1) : h1);
+            x = a.exact ? wrap_exact(x, Ld) : wrap1d(x, Ld);
             const double D = __dadd_rn(__dmul_rn(a.c, a.D[e]),
                                        __ddiv_rn(__dmul_rn(__dmul_rn(dt2, a.G[e]), __dadd_rn(1.0, a.c)), 2.0));
             const double C = __dadd_rn(a.C[e], D);
@@ -100,6 +103,18 @@ __global__ void k_unintegrate(int M, StepArgs a, const int *mol_rep) {
         po.z = (R)gather_coord(xn[2], xn[3 * k + 2], k != 0, Ld);
         po.w = R(0);
         ((V4 *)a.pos_out)[3 * I + k] = po;
+    }
+}
+
+__global__ void k_quantize_state(int N, double *x, double *v, const int *atom_rep, const double *rep_box) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double L = rep_box[atom_rep[i]];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const size_t e = 3 * (size_t)i + u;
+        x[e] = wrap_exact(qgrid(x[e]), L);
+        v[e] = qgrid(v[e]);
     }
 }
 
@@ -186,6 +201,13 @@ cudaError_t launch_unintegrate(int M, int prec, const StepArgs &a, const int *mo
         k_unintegrate<float4><<<b, t, 0, st>>>(M, a, mol_rep);
     else
         k_unintegrate<double4><<<b, t, 0, st>>>(M, a, mol_rep);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quantize_state(int N, double *x, double *v, const int *atom_rep, const double *rep_box,
+                                  cudaStream_t st) {
+    const int t = 256, b = (N + t - 1) / t;
+    k_quantize_state<<<b, t, 0, st>>>(N, x, v, atom_rep, rep_box);
     return cudaGetLastError();
 }
 

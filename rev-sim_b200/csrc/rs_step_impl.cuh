@@ -536,14 +536,19 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
                 atom_noise(a.seed_cur[rep], la, k == 0 ? a.rep_sdO[rep] : a.rep_sdH[rep], xi);
             }
         }
+        const bool ex = a.exact != 0;
 #pragma unroll
         for (int u = 0; u < 3; u++) {
             double v = vk[u], x = xk[u];
-            v = __dadd_rn(v, __ddiv_rn(__dmul_rn(F[u], a.dt), m));
-            x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+            const double kick = __ddiv_rn(__dmul_rn(F[u], a.dt), m);
+            v = __dadd_rn(v, ex ? qgrid(kick) : kick);
+            const double h1 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
+            x = __dadd_rn(x, ex ? qgrid(h1) : h1);
             v = __dadd_rn(__dmul_rn(v, a.c), __dmul_rn(xi[u], a.s));
-            x = __dadd_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-            x = wrap1d(x, Ld);
+            if (ex) v = qgrid(v);
+            const double h2 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
+            x = __dadd_rn(x, ex ? qgrid(h2) : h2);
+            x = ex ? wrap_exact(x, Ld) : wrap1d(x, Ld);
             a.v[3 * ia + u] = v;
             a.x[3 * ia + u] = x;
             xn[u] = x;
@@ -585,7 +590,8 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
             a.G[e] = Gv[u];
             n2 = __dadd_rn(n2, __dmul_rn(Gv[u], Gv[u]));
             // v_{n-1} = v' - F dt / m (water.jl:1516)
-            double v = __dsub_rn(vk[u], __ddiv_rn(__dmul_rn(F[u], a.dt), m));
+            const double kick = __ddiv_rn(__dmul_rn(F[u], a.dt), m);
+            double v = __dsub_rn(vk[u], a.exact ? qgrid(kick) : kick);
             if (!defer) {
                 // water.jl:1520-1521
                 const double B = __dadd_rn(__dmul_rn(a.c, Bk[u]), __dmul_rn(dt2, Gv[u]));
@@ -595,10 +601,13 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
             if (fuse) {
                 // part 1 of the next reverse step (water.jl:1496-1502)
                 double x = xk[u];
-                x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
+                const double h2 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
+                x = __dsub_rn(x, a.exact ? qgrid(h2) : h2);
                 v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
-                x = __dsub_rn(x, __dmul_rn(__dmul_rn(v, a.dt), 0.5));
-                x = wrap1d(x, Ld);
+                if (a.exact) v = qgrid(v);
+                const double h1 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
+                x = __dsub_rn(x, a.exact ? qgrid(h1) : h1);
+                x = a.exact ? wrap_exact(x, Ld) : wrap1d(x, Ld);
                 const double D = __dadd_rn(__dmul_rn(a.c, Dk[u]),
                                            __ddiv_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]),
                                                                __dadd_rn(1.0, a.c)),

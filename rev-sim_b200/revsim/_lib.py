@@ -37,7 +37,7 @@ EXPORTS = [
     "revsim_set_enth_vap", "revsim_loss_parts", "revsim_loss_and_grads", "revsim_set_barostat",
     "revsim_barostat_state", "revsim_set_box", "revsim_probe_fp64_tflops",
     "revsim_forward_noise", "revsim_reverse_noise", "revsim_set_graph_mode", "revsim_graph_stats",
-    "revsim_set_mlp_precision", "revsim_mlp_eval",
+    "revsim_set_mlp_precision", "revsim_mlp_eval", "revsim_set_integrator",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -185,6 +185,7 @@ def load(path=LIB_PATH):
         "revsim_reverse": (i32, [vp, pu64, d, i32, i32, i32, d, d, pd, pd]),
         "revsim_forward_noise": (i32, [vp, pd, d, i32, i32, d, i32, pd]),
         "revsim_set_graph_mode": (i32, [vp, i32]),
+        "revsim_set_integrator": (i32, [vp, i32]),
         "revsim_set_mlp_precision": (i32, [vp, i32]),
         "revsim_mlp_eval": (i32, [vp, i32, pd, pd, pd]),
         "revsim_graph_stats": (i32, [vp, pi64, pi64]),

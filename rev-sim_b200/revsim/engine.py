@@ -305,6 +305,11 @@ class Engine:
         self._check(self._L.revsim_mlp_eval(self._h, n, rp, f64p(u), f64p(du)))
         return u, du
 
+    def set_integrator(self, mode="reference"):
+        """"reference" (the reference's FP64 step arithmetic) or "exact" (grid increments: with
+        gamma = 0 the reverse pass rebuilds the trajectory bit for bit), revsim_set_integrator."""
+        self._check(self._L.revsim_set_integrator(self._h, {"reference": 0, "exact": 1}[mode]))
+
     def set_graph_mode(self, on=True):
         """Capture each forward / reverse pass into a CUDA graph and replay it on later calls
         with the same arguments (revsim_set_graph_mode); the results are the same bits."""
