@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--equil-ps", type=int, default=3, help="ps of Langevin equilibration")
     ap.add_argument("--n-replicas", type=int, default=64, help="replicas workload: boxes")
     ap.add_argument("--rep-steps", type=int, default=2000, help="replicas workload: steps")
+    ap.add_argument("--integrator", default="exact", choices=["exact", "reference"],
+                    help="water: the exactly reversible integrator (grid increments) or the "
+                         "reference's FP64 step arithmetic")
     ap.add_argument("--cfg1-replicas", type=int, default=16,
                     help="895-water target configuration: replicas batched in one handle")
     ap.add_argument("--no-target", action="store_true",
@@ -125,6 +128,12 @@ LOSS_TEXT = {
 }
 
 
+def integ(e, a):
+    """The integrator arithmetic of a timed water engine (revsim_set_integrator)."""
+    e.set_integrator(a.integrator)
+    return e
+
+
 def apply_loss(e, a, target):
     """loss_type: the RDF term, the enthalpy term or both on an engine."""
     from revsim import oo_l2_term
@@ -144,7 +153,7 @@ def config(a, extra=None):
          "n_steps_log": 1000, "dt_ps": 0.001, "gamma_per_ps": a.gamma, "pair_form": a.form,
          "precision": a.precision,
          "loss": LOSS_TEXT[a.loss],
-         "l2": "flushed (256 MiB write) between timed steps"}
+         "l2": "flushed (256 MiB write) between timed steps", "integrator": a.integrator}
     if extra:
         c.update(extra)
     return c
@@ -312,7 +321,7 @@ def run_ours(a):
     from revsim import Engine, _lib, oo_l2_term, systems
 
     x0, v0, p, target = prepare(a, local, a.equil_ps)
-    eng = Engine(a.n_mol, a.box, inter_type=a.form, precision=a.precision, device=local)
+    eng = integ(Engine(a.n_mol, a.box, inter_type=a.form, precision=a.precision, device=local), a)
     eng.set_params(p)
     apply_loss(eng, a, target)
     eng.set_state(x0, v0)
@@ -409,7 +418,19 @@ def run_ours(a):
     xs, _ = eng.get_state()
     # the reverse pass ends at the start state, rebuilt over the first snapshot block
     recon = {"mixed" if a.precision == "mixed" else "fp64": recon_error(xs, x0, a.box),
-             "steps_reconstructed": 1000}
+             "steps_reconstructed": 1000, "integrator": a.integrator}
+    if a.integrator == "exact" and rank == 0:
+        # the same gradient with the reference's step arithmetic, for its reconstruction
+        recon["reference_arithmetic"] = {}
+        for prec in ("mixed", "fp64"):
+            er = Engine(a.n_mol, a.box, inter_type=a.form, precision=prec, device=local)
+            er.set_params(p)
+            apply_loss(er, a, target)
+            er.set_state(x0, v0)
+            er.forward(seeds, a.gamma, a.n_steps, a.n_steps_loss, 0.001)
+            er.reverse(seeds, a.gamma, a.n_steps, a.n_steps_loss, a.n_steps_loss, 0.001)
+            recon["reference_arithmetic"][prec] = recon_error(er.get_state()[0], x0, a.box)
+            er.close()
     pairs = eng.neighbor_pairs(0)
     ipairs, oo = count_ipairs(xs, a.box, pairs)
     flops_launch = FLOPS_REV_IPAIR * ipairs
@@ -438,7 +459,7 @@ def run_ours(a):
     extra = {}
     if not a.no_compare and rank == 0:
         # the same gradient in plain FP64 on the GPU: throughput and gradient difference
-        e64 = Engine(a.n_mol, a.box, inter_type=a.form, precision="fp64", device=local)
+        e64 = integ(Engine(a.n_mol, a.box, inter_type=a.form, precision="fp64", device=local), a)
         e64.set_params(p)
         apply_loss(e64, a, target)
         e64.set_state(x0, v0)
@@ -470,7 +491,7 @@ def run_ours(a):
         e64.close()
 
         def make(prec):
-            e = Engine(a.n_mol, a.box, inter_type=a.form, precision=prec, device=local)
+            e = integ(Engine(a.n_mol, a.box, inter_type=a.form, precision=prec, device=local), a)
             e.set_params(p)
             apply_loss(e, a, target)
             return e
@@ -707,10 +728,10 @@ def run_target_cfg1(a, device, reps=3, with_cpu=True):
     out = {"workload": f"water_895mol_3nm_tip3p_x{R}replicas_lj_1000fwd+1000rev",
            "start": "water/tip3p.pdb positions (committed fixture), MB velocities at 295.15 K, 1 ps "
                     "Langevin equilibration on the GPU", "replicas": R, "n_atoms": n_atoms,
-           "n_steps": n, "gamma_per_ps": 0.0, "dt_ps": 0.001}
+           "n_steps": n, "gamma_per_ps": 0.0, "dt_ps": 0.001, "integrator": a.integrator}
     res = {}
     for prec in ("mixed", "fp64"):
-        e = Engine([895] * R, [box] * R, precision=prec, device=device)
+        e = integ(Engine([895] * R, [box] * R, precision=prec, device=device), a)
         e.set_params(p)
         e.set_loss([oo_l2_term(target)])
         e.set_state(x0, v0)
@@ -728,7 +749,7 @@ def run_target_cfg1(a, device, reps=3, with_cpu=True):
                      "recon_1000_steps": recon_error(xr, x0, box), "grad": g}
         # one replica alone (the unbatched form) for the same comparison
         e.close()
-        e1 = Engine(895, box, precision=prec, device=device)
+        e1 = integ(Engine(895, box, precision=prec, device=device), a)
         e1.set_params(p)
         e1.set_loss([oo_l2_term(target)])
         e1.set_state(x0[:2685], v0[:2685])
@@ -750,7 +771,7 @@ def run_target_cfg1(a, device, reps=3, with_cpu=True):
                                                      res["fp64"]["single_replica"]["value"])
 
     def make(prec):
-        e = Engine(895, box, precision=prec, device=device)
+        e = integ(Engine(895, box, precision=prec, device=device), a)
         e.set_params(p)
         e.set_loss([oo_l2_term(target)])
         return e
@@ -1973,7 +1994,7 @@ def run_ours_replicas(a):
     # the target: the mean RDF over all replicas of all ranks (set-up, untimed)
     target = allreduce_sum(np.sum([eq.rdf(0, r) for r in range(R)], axis=0)) / R_all
     eq.close()
-    eng = Engine(n_mol, boxes, temp=temps, precision=a.precision, device=local)
+    eng = integ(Engine(n_mol, boxes, temp=temps, precision=a.precision, device=local), a)
     eng.set_params(p)
     eng.set_loss([oo_l2_term(target)])
     eng.set_state(x0, v0)
