@@ -90,7 +90,8 @@ typedef struct {
  * scalar kernels (REVSIM_MLP_FP64, the default) or on the tensor cores with BF16 operands
  * and FP32 accumulation (REVSIM_MLP_BF16_TC: the forward and r-tangent GEMMs, the backward
  * through both streams with the mixed second derivative d^2u/dr dtheta, and the weight-
- * gradient GEMMs over the node batch; parameters stay FP64 and are rounded to BF16 per use). */
+ * gradient GEMMs over the node batch; parameters stay FP64; each operand is split into a
+ * BF16 high part and a BF16 remainder, three MMAs per product, ~16 significant bits). */
 #define REVSIM_MLP_FP64 0
 #define REVSIM_MLP_BF16_TC 1
 
@@ -259,12 +260,13 @@ int32_t revsim_reverse_noise(revsim_handle *h, const double *host_noise, double 
  * amplifies: in FP64 to ~1e-8 nm over 1,000 steps, and in mixed precision until a position
  * crosses an FP32 rounding boundary, after which the two passes' forces differ).
  * REVSIM_INTEGRATOR_REFERENCE (default): the reference's arithmetic.  REVSIM_INTEGRATOR_EXACT:
- * positions, velocities and box sides on the grid of multiples of 2^-44 nm (nm/ps), every
+ * positions, velocities and box sides on the grid of multiples of 2^-48 nm (nm/ps), every
  * increment of the step (kick F dt / m, half drifts v dt / 2, the O step's result) rounded to
  * it, so the reverse pass subtracts exactly what the forward pass added: with gamma = 0 the
  * trajectory is rebuilt bit for bit in both precisions, however long the run; with friction
  * the O step's inverse stays approximate.  The state and boxes are rounded to the grid at the
- * start of each forward pass (<= 2^-45 nm, ~3e-14 nm).  Invalidates the forward record. */
+ * start of each forward pass (<= 2^-49 nm, ~2e-15 nm); boxes must be under 32 nm
+ * (REVSIM_ERR_BADARG otherwise).  Invalidates the forward record. */
 #define REVSIM_INTEGRATOR_REFERENCE 0
 #define REVSIM_INTEGRATOR_EXACT 1
 int32_t revsim_set_integrator(revsim_handle *h, int32_t mode);

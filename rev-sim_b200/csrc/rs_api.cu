@@ -1566,9 +1566,12 @@ int32_t revsim_barostat_state(revsim_handle *h, double *box, double *volume_scal
 
 int32_t revsim_set_box(revsim_handle *h, const double *box) {
     if (!h || !box) return REVSIM_ERR_BADARG;
-    for (int r = 0; r < h->R; r++)
+    for (int r = 0; r < h->R; r++) {
         if (!(box[r] > 2 * h->rc_nl) || !std::isfinite(box[r]))
             return fail(h, REVSIM_ERR_BADARG, "box side must exceed twice the neighbour cutoff");
+        if (h->exact && !(box[r] < kGridMaxBox))
+            return fail(h, REVSIM_ERR_BADARG, "the exact integrator needs boxes under 32 nm");
+    }
     CK(cudaSetDevice(h->dev));
     const std::vector<double> old = h->box;
     h->box.assign(box, box + h->R);
@@ -1909,6 +1912,10 @@ int32_t revsim_set_integrator(revsim_handle *h, int32_t mode) {
     if (!h) return REVSIM_ERR_BADARG;
     if (mode != REVSIM_INTEGRATOR_REFERENCE && mode != REVSIM_INTEGRATOR_EXACT)
         return fail(h, REVSIM_ERR_BADARG, "bad integrator");
+    if (mode == REVSIM_INTEGRATOR_EXACT)
+        for (int r = 0; r < h->R; r++)
+            if (!(h->box[r] < kGridMaxBox))
+                return fail(h, REVSIM_ERR_BADARG, "the exact integrator needs boxes under 32 nm");
     if (h->exact != (mode == REVSIM_INTEGRATOR_EXACT)) h->gen++;
     h->exact = mode == REVSIM_INTEGRATOR_EXACT;
     h->fwd_valid = false;

@@ -70,16 +70,17 @@ __device__ __forceinline__ double wrap1d(double c, double L) {
 }
 
 // Exactly reversible integration (revsim_set_integrator, REVSIM_INTEGRATOR_EXACT): positions,
-// velocities and box sides are kept on the grid of multiples of 2^-44 (nm, nm/ps), and every
+// velocities and box sides are kept on the grid of multiples of 2^-48 (nm, nm/ps), and every
 // increment of the velocity Verlet step (the kick F dt / m, each half drift v dt / 2) is
-// rounded to that grid before it is added.  Sums of grid values below 2^9 in magnitude are
-// exact in FP64, so the reverse pass, which subtracts the same increments computed from the
+// rounded to that grid before it is added.  Sums of grid values below 2^5 in magnitude (box
+// sides under 32 nm, speeds under 32 nm/ps) are exact in FP64, so the reverse pass, which subtracts the same increments computed from the
 // same bits, restores the previous state exactly: with gamma = 0 the start state is rebuilt
 // bit for bit however long the run (the reference's FP64 arithmetic rebuilds it to rounding
 // that the dynamics' chaos amplifies).  With friction the O step v c + xi s is rounded to the
 // grid too and its inverse is approximate, as in the reference.
-constexpr double kGrid = 5.684341886080801486968994140625e-14;   // 2^-44
-constexpr double kGridInv = 17592186044416.0;                    // 2^44
+constexpr double kGrid = 3.5527136788005009293556213378906e-15;   // 2^-48
+constexpr double kGridInv = 281474976710656.0;                      // 2^48
+constexpr double kGridMaxBox = 32.0;                                // 2^5 nm
 __host__ __device__ __forceinline__ double qgrid(double y) {
 #ifdef __CUDA_ARCH__
     return __dmul_rn(rint(__dmul_rn(y, kGridInv)), kGrid);

@@ -2,6 +2,12 @@
 // FP32 accumulation (mma.sync.m16n8k16 with bf16 inputs), for the node evaluation that builds
 // the interval table and for its backward pass to the weights.
 //
+// Each FP32 operand x is split into two BF16 values, hi = bf16(x) and lo = bf16(x - hi), and
+// each product is formed as A_lo B_hi + A_hi B_lo + A_hi B_hi (three MMAs, the small terms
+// first): about 16 significant bits per operand instead of 8.  With plain BF16 operands the
+// weight gradients, sums over the 1,025 nodes whose terms largely cancel, came out ~40 % off
+// the FP64 result; split they agree to ~1e-4.
+//
 // Per element pair type t the network is u(r) = fc(r) (b3 + w3 . silu(W2 silu(W1 phi(r) + b1)
 // + b2)) with 16 Gaussian radial basis functions phi (rs_mlp.cu).  Evaluated at many distances
 // at once it is a chain of small GEMMs over a batch of rows (distances):
@@ -34,10 +40,10 @@ constexpr int CHUNK = 80, NCHUNK = NPAD / CHUNK;
 constexpr int W1S = 12;   // shared-memory row stride of W1 in 32-bit words (8 used)
 constexpr int W2S = 36;   // ... of W2 and W2^T (32 used)
 
-struct TcWeights {        // one type's weights in shared memory
-    uint32_t w1[H * W1S];     // W1 [i][k] as bf16 pairs along k
-    uint32_t w2[H * W2S];     // W2 [i][j] as bf16 pairs along j
-    uint32_t w2t[H * W2S];    // W2^T [j][i] as bf16 pairs along i
+struct TcWeights {        // one type's weights in shared memory, split hi / lo
+    uint32_t w1[H * W1S], w1l[H * W1S];     // W1 [i][k] as bf16 pairs along k
+    uint32_t w2[H * W2S], w2l[H * W2S];     // W2 [i][j] as bf16 pairs along j
+    uint32_t w2t[H * W2S], w2tl[H * W2S];   // W2^T [j][i] as bf16 pairs along i
     float b1[H], b2[H], w3[H];
     float b3;
 };
@@ -47,6 +53,19 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<uint32_t *>(&v);
 }
 
+// x = hi + lo with hi = bf16(x): the remainder x - hi is exact in FP32.
+__device__ __forceinline__ float bf16_rest(float x) {
+    return x - __bfloat162float(__float2bfloat16_rn(x));
+}
+
+// Two consecutive elements (a, b) as split bf16 pairs.
+struct Pair2 {
+    uint32_t hi, lo;
+};
+__device__ __forceinline__ Pair2 split2(float a, float b) {
+    return Pair2{pack_bf16(a, b), pack_bf16(bf16_rest(a), bf16_rest(b))};
+}
+
 // D = A B + D, m16n8k16, A 16x16 row-major bf16, B 16x8 column-major bf16, D FP32.
 __device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
     asm volatile(
@@ -54,6 +73,23 @@ __device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], uint32
         "{%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// D += A B with split operands: A_lo B_hi + A_hi B_lo + A_hi B_hi.
+__device__ __forceinline__ void mma3(float d[4], const uint32_t ah[4], const uint32_t al[4], uint32_t bh0,
+                                     uint32_t bh1, uint32_t bl0, uint32_t bl1) {
+    mma_bf16(d, al, bh0, bh1);
+    mma_bf16(d, ah, bl0, bl1);
+    mma_bf16(d, ah, bh0, bh1);
+}
+
+// An A fragment (four split pairs) from rows/columns already placed per the m16n8k16 layout.
+__device__ __forceinline__ void frag_split(const Pair2 p[4], uint32_t ah[4], uint32_t al[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        ah[q] = p[q].hi;
+        al[q] = p[q].lo;
+    }
 }
 
 __device__ __forceinline__ float sigm(float z) { return 1.f / (1.f + expf(-z)); }
@@ -80,12 +116,18 @@ __device__ void load_weights(const double *theta, int t, TcWeights &s) {
     const double *b1 = W1 + H * NR, *W2 = b1 + H, *b2 = W2 + H * H, *w3 = b2 + H, *b3 = w3 + H;
     for (int q = threadIdx.x; q < H * NR / 2; q += blockDim.x) {
         const int i = q / (NR / 2), k2 = q % (NR / 2);
-        s.w1[i * W1S + k2] = pack_bf16((float)W1[i * NR + 2 * k2], (float)W1[i * NR + 2 * k2 + 1]);
+        const Pair2 w = split2((float)W1[i * NR + 2 * k2], (float)W1[i * NR + 2 * k2 + 1]);
+        s.w1[i * W1S + k2] = w.hi;
+        s.w1l[i * W1S + k2] = w.lo;
     }
     for (int q = threadIdx.x; q < H * H / 2; q += blockDim.x) {
         const int i = q / (H / 2), j2 = q % (H / 2);
-        s.w2[i * W2S + j2] = pack_bf16((float)W2[i * H + 2 * j2], (float)W2[i * H + 2 * j2 + 1]);
-        s.w2t[i * W2S + j2] = pack_bf16((float)W2[(2 * j2) * H + i], (float)W2[(2 * j2 + 1) * H + i]);
+        const Pair2 w = split2((float)W2[i * H + 2 * j2], (float)W2[i * H + 2 * j2 + 1]);
+        const Pair2 t = split2((float)W2[(2 * j2) * H + i], (float)W2[(2 * j2 + 1) * H + i]);
+        s.w2[i * W2S + j2] = w.hi;
+        s.w2l[i * W2S + j2] = w.lo;
+        s.w2t[i * W2S + j2] = t.hi;
+        s.w2tl[i * W2S + j2] = t.lo;
     }
     for (int i = threadIdx.x; i < H; i += blockDim.x) {
         s.b1[i] = (float)b1[i];
@@ -115,17 +157,23 @@ __device__ __forceinline__ void tile_forward(const TcWeights &s, float r0, float
         rbf_f(r0, rc, w, ks[q], p[0][q], dp[0][q]);
         rbf_f(r1, rc, w, ks[q], p[1][q], dp[1][q]);
     }
-    const uint32_t a1[4] = {pack_bf16(p[0][0], p[0][1]), pack_bf16(p[1][0], p[1][1]),
-                            pack_bf16(p[0][2], p[0][3]), pack_bf16(p[1][2], p[1][3])};
-    const uint32_t da1[4] = {pack_bf16(dp[0][0], dp[0][1]), pack_bf16(dp[1][0], dp[1][1]),
-                             pack_bf16(dp[0][2], dp[0][3]), pack_bf16(dp[1][2], dp[1][3])};
+    uint32_t a1h[4], a1l[4], da1h[4], da1l[4];
+    {
+        const Pair2 pa[4] = {split2(p[0][0], p[0][1]), split2(p[1][0], p[1][1]), split2(p[0][2], p[0][3]),
+                             split2(p[1][2], p[1][3])};
+        const Pair2 pd[4] = {split2(dp[0][0], dp[0][1]), split2(dp[1][0], dp[1][1]), split2(dp[0][2], dp[0][3]),
+                             split2(dp[1][2], dp[1][3])};
+        frag_split(pa, a1h, a1l);
+        frag_split(pd, da1h, da1l);
+    }
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-        const uint32_t b0 = s.w1[(8 * j + g) * W1S + tq], b1 = s.w1[(8 * j + g) * W1S + 4 + tq];
+        const int o = (8 * j + g) * W1S + tq;
+        const uint32_t b0 = s.w1[o], b1 = s.w1[o + 4], bl0 = s.w1l[o], bl1 = s.w1l[o + 4];
         const float bb0 = s.b1[8 * j + 2 * tq], bb1 = s.b1[8 * j + 2 * tq + 1];
         float c[4] = {bb0, bb1, bb0, bb1}, dc[4] = {0.f, 0.f, 0.f, 0.f};
-        mma_bf16(c, a1, b0, b1);
-        mma_bf16(dc, da1, b0, b1);
+        mma3(c, a1h, a1l, b0, b1, bl0, bl1);
+        mma3(dc, da1h, da1l, b0, b1, bl0, bl1);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             f.z1[j][q] = c[q];
@@ -154,16 +202,21 @@ __device__ __forceinline__ void tile_forward(const TcWeights &s, float r0, float
                 h[u][q] = silu0(z);
                 dh[u][q] = silu1(z) * f.dz1[2 * kt + u][q];
             }
-        const uint32_t a[4] = {pack_bf16(h[0][0], h[0][1]), pack_bf16(h[0][2], h[0][3]),
-                               pack_bf16(h[1][0], h[1][1]), pack_bf16(h[1][2], h[1][3])};
-        const uint32_t da[4] = {pack_bf16(dh[0][0], dh[0][1]), pack_bf16(dh[0][2], dh[0][3]),
-                                pack_bf16(dh[1][0], dh[1][1]), pack_bf16(dh[1][2], dh[1][3])};
+        uint32_t ah[4], al[4], dah[4], dal[4];
+        {
+            const Pair2 ph[4] = {split2(h[0][0], h[0][1]), split2(h[0][2], h[0][3]), split2(h[1][0], h[1][1]),
+                                 split2(h[1][2], h[1][3])};
+            const Pair2 pd[4] = {split2(dh[0][0], dh[0][1]), split2(dh[0][2], dh[0][3]), split2(dh[1][0], dh[1][1]),
+                                 split2(dh[1][2], dh[1][3])};
+            frag_split(ph, ah, al);
+            frag_split(pd, dah, dal);
+        }
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            const uint32_t b0 = s.w2[(8 * j + g) * W2S + 8 * kt + tq];
-            const uint32_t b1 = s.w2[(8 * j + g) * W2S + 8 * kt + 4 + tq];
-            mma_bf16(f.z2[j], a, b0, b1);
-            mma_bf16(f.dz2[j], da, b0, b1);
+            const int o = (8 * j + g) * W2S + 8 * kt + tq;
+            const uint32_t b0 = s.w2[o], b1 = s.w2[o + 4], bl0 = s.w2l[o], bl1 = s.w2l[o + 4];
+            mma3(f.z2[j], ah, al, b0, b1, bl0, bl1);
+            mma3(f.dz2[j], dah, dal, b0, b1, bl0, bl1);
         }
     }
     // outputs: y = b3 + w3 . silu(z2), dy = w3 . (silu'(z2) dz2), rows g and g + 8
@@ -232,12 +285,13 @@ __global__ void __launch_bounds__(128) k_mlp_tc_fwd(const double *theta, double 
 // per-tile FP32 partials [NTILE][64] of b1, b2, w3 and [NTILE] of b3, per-chunk FP32 partials
 // [NCHUNK][64][64] of W2 and [NCHUNK][64][16] of W1.
 struct TcScratch {
-    __nv_bfloat16 *z2b, *dz2b, *h1, *dh1, *z1b, *dz1b, *phi, *dphi;
+    // [0]: hi parts, [1]: lo parts
+    __nv_bfloat16 *z2b[2], *dz2b[2], *h1[2], *dh1[2], *z1b[2], *dz1b[2], *phi[2], *dphi[2];
     float *pb1, *pb2, *pw3, *pb3, *pW2, *pW1;
 };
 
 __host__ __device__ inline size_t tc_scratch_bytes_per_type() {
-    const size_t b = sizeof(__nv_bfloat16) * ((size_t)6 * H * NPAD + 2 * (size_t)NR * NPAD) +
+    const size_t b = 2 * sizeof(__nv_bfloat16) * ((size_t)6 * H * NPAD + 2 * (size_t)NR * NPAD) +
                      sizeof(float) * ((size_t)3 * NTILE * H + NTILE + (size_t)NCHUNK * H * H +
                                       (size_t)NCHUNK * H * NR);
     return (b + 255) / 256 * 256;
@@ -256,14 +310,16 @@ __host__ __device__ inline TcScratch tc_view(void *base, int t) {
         p += sizeof(float) * n;
         return q;
     };
-    s.z2b = take_b((size_t)H * NPAD);
-    s.dz2b = take_b((size_t)H * NPAD);
-    s.h1 = take_b((size_t)H * NPAD);
-    s.dh1 = take_b((size_t)H * NPAD);
-    s.z1b = take_b((size_t)H * NPAD);
-    s.dz1b = take_b((size_t)H * NPAD);
-    s.phi = take_b((size_t)NR * NPAD);
-    s.dphi = take_b((size_t)NR * NPAD);
+    for (int h = 0; h < 2; h++) {
+        s.z2b[h] = take_b((size_t)H * NPAD);
+        s.dz2b[h] = take_b((size_t)H * NPAD);
+        s.h1[h] = take_b((size_t)H * NPAD);
+        s.dh1[h] = take_b((size_t)H * NPAD);
+        s.z1b[h] = take_b((size_t)H * NPAD);
+        s.dz1b[h] = take_b((size_t)H * NPAD);
+        s.phi[h] = take_b((size_t)NR * NPAD);
+        s.dphi[h] = take_b((size_t)NR * NPAD);
+    }
     s.pb1 = take_f((size_t)NTILE * H);
     s.pb2 = take_f((size_t)NTILE * H);
     s.pw3 = take_f((size_t)NTILE * H);
@@ -342,19 +398,24 @@ __global__ void __launch_bounds__(128) k_mlp_tc_bwd_nodes(const double *theta, d
             }
 #pragma unroll
         for (int kt = 0; kt < 4; kt++) {
-            const uint32_t a[4] = {pack_bf16(z2b[2 * kt][0], z2b[2 * kt][1]), pack_bf16(z2b[2 * kt][2], z2b[2 * kt][3]),
-                                   pack_bf16(z2b[2 * kt + 1][0], z2b[2 * kt + 1][1]),
-                                   pack_bf16(z2b[2 * kt + 1][2], z2b[2 * kt + 1][3])};
-            const uint32_t da[4] = {pack_bf16(dz2b[2 * kt][0], dz2b[2 * kt][1]),
-                                    pack_bf16(dz2b[2 * kt][2], dz2b[2 * kt][3]),
-                                    pack_bf16(dz2b[2 * kt + 1][0], dz2b[2 * kt + 1][1]),
-                                    pack_bf16(dz2b[2 * kt + 1][2], dz2b[2 * kt + 1][3])};
+            uint32_t ah[4], al[4], dah[4], dal[4];
+            {
+                const Pair2 pz[4] = {split2(z2b[2 * kt][0], z2b[2 * kt][1]), split2(z2b[2 * kt][2], z2b[2 * kt][3]),
+                                     split2(z2b[2 * kt + 1][0], z2b[2 * kt + 1][1]),
+                                     split2(z2b[2 * kt + 1][2], z2b[2 * kt + 1][3])};
+                const Pair2 pd[4] = {split2(dz2b[2 * kt][0], dz2b[2 * kt][1]),
+                                     split2(dz2b[2 * kt][2], dz2b[2 * kt][3]),
+                                     split2(dz2b[2 * kt + 1][0], dz2b[2 * kt + 1][1]),
+                                     split2(dz2b[2 * kt + 1][2], dz2b[2 * kt + 1][3])};
+                frag_split(pz, ah, al);
+                frag_split(pd, dah, dal);
+            }
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const uint32_t b0 = s.w2t[(8 * j + g) * W2S + 8 * kt + tq];
-                const uint32_t b1 = s.w2t[(8 * j + g) * W2S + 8 * kt + 4 + tq];
-                mma_bf16(h1b[j], a, b0, b1);
-                mma_bf16(dh1b[j], da, b0, b1);
+                const int o = (8 * j + g) * W2S + 8 * kt + tq;
+                const uint32_t b0 = s.w2t[o], b1 = s.w2t[o + 4], bl0 = s.w2tl[o], bl1 = s.w2tl[o + 4];
+                mma3(h1b[j], ah, al, b0, b1, bl0, bl1);
+                mma3(dh1b[j], dah, dal, b0, b1, bl0, bl1);
             }
         }
         // hidden layer: Z1b (with the mixed second derivative through silu'') and dZ1b;
@@ -370,12 +431,17 @@ __global__ void __launch_bounds__(128) k_mlp_tc_bwd_nodes(const double *theta, d
                 dz1b[j][q] = dh1b[j][q] * s1;
                 const int rw = row[q >> 1], col = 8 * j + 2 * tq + (q & 1);
                 const size_t o = (size_t)col * NPAD + rw;
-                sc.z2b[o] = __float2bfloat16_rn(z2b[j][q]);
-                sc.dz2b[o] = __float2bfloat16_rn(dz2b[j][q]);
-                sc.h1[o] = __float2bfloat16_rn(silu0(z));
-                sc.dh1[o] = __float2bfloat16_rn(s1 * dz);
-                sc.z1b[o] = __float2bfloat16_rn(z1b[j][q]);
-                sc.dz1b[o] = __float2bfloat16_rn(dz1b[j][q]);
+                auto put = [&](__nv_bfloat16 *const dst[2], float x) {
+                    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+                    dst[0][o] = hi;
+                    dst[1][o] = __float2bfloat16_rn(x - __bfloat162float(hi));
+                };
+                put(sc.z2b, z2b[j][q]);
+                put(sc.dz2b, dz2b[j][q]);
+                put(sc.h1, silu0(z));
+                put(sc.dh1, s1 * dz);
+                put(sc.z1b, z1b[j][q]);
+                put(sc.dz1b, dz1b[j][q]);
             }
         // basis functions of the tile's rows, transposed [k][node]
         if (lane < 16) {
@@ -385,8 +451,12 @@ __global__ void __launch_bounds__(128) k_mlp_tc_bwd_nodes(const double *theta, d
             for (int k = 0; k < NR; k++) {
                 float ph, dph;
                 rbf_f(rf, (float)rc, (float)w, k, ph, dph);
-                sc.phi[(size_t)k * NPAD + rw] = __float2bfloat16_rn(ph);
-                sc.dphi[(size_t)k * NPAD + rw] = __float2bfloat16_rn(dph);
+                const size_t o = (size_t)k * NPAD + rw;
+                const __nv_bfloat16 hp = __float2bfloat16_rn(ph), hd = __float2bfloat16_rn(dph);
+                sc.phi[0][o] = hp;
+                sc.phi[1][o] = __float2bfloat16_rn(ph - __bfloat162float(hp));
+                sc.dphi[0][o] = hd;
+                sc.dphi[1][o] = __float2bfloat16_rn(dph - __bfloat162float(hd));
             }
         }
         // per-tile sums of the bias and output-layer gradients
@@ -436,29 +506,44 @@ __global__ void __launch_bounds__(256) k_mlp_tc_wgrad(void *scratch) {
     const int m1 = warp >> 1, n1 = warp & 1;
     for (int ks = 0; ks < CHUNK / 16; ks++) {
         const int k0 = ch * CHUNK + ks * 16;
-        // B fragments: H1 / dH1 for columns 8 warp + g; Phi / dPhi for columns 8 n1 + g
+        // B fragments (hi, lo): H1 / dH1 for columns 8 warp + g; Phi / dPhi for columns 8 n1 + g
         const size_t bo = (size_t)(8 * warp + g) * NPAD + k0 + 2 * tq;
-        const uint32_t bh0 = ld2(sc.h1 + bo), bh1 = ld2(sc.h1 + bo + 8);
-        const uint32_t bd0 = ld2(sc.dh1 + bo), bd1 = ld2(sc.dh1 + bo + 8);
         const size_t po = (size_t)(8 * n1 + g) * NPAD + k0 + 2 * tq;
-        const uint32_t bp0 = ld2(sc.phi + po), bp1 = ld2(sc.phi + po + 8);
-        const uint32_t bq0 = ld2(sc.dphi + po), bq1 = ld2(sc.dphi + po + 8);
+        uint32_t bh[2][2], bd[2][2], bp[2][2], bq[2][2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            bh[h][0] = ld2(sc.h1[h] + bo);
+            bh[h][1] = ld2(sc.h1[h] + bo + 8);
+            bd[h][0] = ld2(sc.dh1[h] + bo);
+            bd[h][1] = ld2(sc.dh1[h] + bo + 8);
+            bp[h][0] = ld2(sc.phi[h] + po);
+            bp[h][1] = ld2(sc.phi[h] + po + 8);
+            bq[h][0] = ld2(sc.dphi[h] + po);
+            bq[h][1] = ld2(sc.dphi[h] + po + 8);
+        }
+        auto afrag = [&](__nv_bfloat16 *const src[2], int m, uint32_t ah[4], uint32_t al[4]) {
+            const size_t r0 = (size_t)(16 * m + g) * NPAD + k0 + 2 * tq, r1 = r0 + 8 * (size_t)NPAD;
+            const size_t off[4] = {r0, r1, r0 + 8, r1 + 8};
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                ah[q] = ld2(src[0] + off[q]);
+                al[q] = ld2(src[1] + off[q]);
+            }
+        };
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            const size_t r0 = (size_t)(16 * m + g) * NPAD + k0 + 2 * tq, r1 = r0 + 8 * (size_t)NPAD;
-            const uint32_t a[4] = {ld2(sc.z2b + r0), ld2(sc.z2b + r1), ld2(sc.z2b + r0 + 8), ld2(sc.z2b + r1 + 8)};
-            const uint32_t da[4] = {ld2(sc.dz2b + r0), ld2(sc.dz2b + r1), ld2(sc.dz2b + r0 + 8),
-                                    ld2(sc.dz2b + r1 + 8)};
-            mma_bf16(acc2[m], a, bh0, bh1);
-            mma_bf16(acc2[m], da, bd0, bd1);
+            uint32_t ah[4], al[4];
+            afrag(sc.z2b, m, ah, al);
+            mma3(acc2[m], ah, al, bh[0][0], bh[0][1], bh[1][0], bh[1][1]);
+            afrag(sc.dz2b, m, ah, al);
+            mma3(acc2[m], ah, al, bd[0][0], bd[0][1], bd[1][0], bd[1][1]);
         }
         {
-            const size_t r0 = (size_t)(16 * m1 + g) * NPAD + k0 + 2 * tq, r1 = r0 + 8 * (size_t)NPAD;
-            const uint32_t a[4] = {ld2(sc.z1b + r0), ld2(sc.z1b + r1), ld2(sc.z1b + r0 + 8), ld2(sc.z1b + r1 + 8)};
-            const uint32_t da[4] = {ld2(sc.dz1b + r0), ld2(sc.dz1b + r1), ld2(sc.dz1b + r0 + 8),
-                                    ld2(sc.dz1b + r1 + 8)};
-            mma_bf16(acc1, a, bp0, bp1);
-            mma_bf16(acc1, da, bq0, bq1);
+            uint32_t ah[4], al[4];
+            afrag(sc.z1b, m1, ah, al);
+            mma3(acc1, ah, al, bp[0][0], bp[0][1], bp[1][0], bp[1][1]);
+            afrag(sc.dz1b, m1, ah, al);
+            mma3(acc1, ah, al, bq[0][0], bq[0][1], bq[1][0], bq[1][1]);
         }
     }
     // C fragment (row 16 m + g (+8), column 8 warp + 2 tq (+1)) -> per-chunk partials

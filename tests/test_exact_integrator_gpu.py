@@ -6,7 +6,7 @@
   to ~0.1 nm);
 * it stays the reference's dynamics: over 30 steps the trajectory within 1e-9 nm and the
   reverse-pass gradient within 1e-6 (FP64, dL/dlog(theta) units floored at 1 %) of the FP64
-  oracle, the state and box differing from the reference's by the grid rounding (<= 2^-45 nm);
+  oracle, the state and box differing from the reference's by the grid rounding (<= 2^-49 nm);
 * gamma = 1/ps: the reverse pass rebuilds 100 steps to < 1e-9 nm (FP64), the O step's inverse
   being approximate as in the reference.
 """
@@ -27,7 +27,7 @@ def _built():
 
 
 def _grid(y):
-    return np.rint(y * 2.0 ** 44) * 2.0 ** -44
+    return np.rint(y * 2.0 ** 48) * 2.0 ** -48
 
 
 def _terms(x, n_mol, box):
@@ -45,6 +45,7 @@ def test_exact_reversal_over_1000_steps(dense_water, prec):
     e.set_params(C.default_params())
     e.set_loss(terms)
     e.set_integrator("exact")
+    e.set_state(x, v)
     e.autotune()
     e.set_state(x, v)
     n = 1000

@@ -1,17 +1,17 @@
 """The learned term's network on the tensor cores (revsim_set_mlp_precision REVSIM_MLP_BF16_TC:
-BF16 operands, FP32 accumulation) against the FP64 oracle and the FP64 kernels.
-
-BF16 keeps 8 significant bits (unit roundoff 2^-9 ~ 2e-3), so every bar here is stated against
-the size of what is compared:
-* node values u and du/dr of all three types: max error <= 2e-2 of the largest |u|, |du/dr|;
+BF16 operands, each FP32 value split into a BF16 high part and a BF16 remainder and every
+product formed by three MMAs with FP32 accumulation) against the FP64 oracle and the FP64
+kernels.  Split operands carry ~16 significant bits, so the bars are:
+* node values u and du/dr of all three types: max error <= 1e-3 of the largest |u|, |du/dr|;
 * at arbitrary distances (a per-pair evaluation): the same bar against the oracle's table
   interpolant, which is < 1e-8 from the exact network;
 * the weight gradient from the same interval-coefficient adjoints (a force VJP at the same
   positions: the adjoints do not depend on the table values): per layer group (W1 + b1,
-  W2 + b2, w3 + b3 of each type) the relative L2 error against the FP64 backward <= 5e-2 and
-  the cosine >= 0.998;
-* the reverse-pass gradient of a 20-step run: classical parameters within 5e-3 of the
-  FP64-network run (parameter-scaled as the classical tests), MLP groups as above.
+  W2 + b2, w3 + b3 of each type) the relative L2 error against the FP64 backward <= 1e-2 and
+  the cosine >= 0.9999 (the gradients are node sums whose terms largely cancel);
+* the reverse-pass gradient of a 20-step run, which also sees the two tables' different
+  dynamics: classical parameters within 5e-3 of the FP64-network run (parameter-scaled as the
+  classical tests), MLP groups within 1e-2 / 0.9999.
 """
 
 import numpy as np
@@ -48,8 +48,8 @@ def _engine(n_mol, box, theta, mode, prec="fp64"):
 def _groups_close(a_all, b_all):
     for ix in groups(len(b_all))[1:]:
         a, b = a_all[ix], b_all[ix]
-        assert np.linalg.norm(a - b) <= 5e-2 * np.linalg.norm(b), (ix[0], np.linalg.norm(a - b) / np.linalg.norm(b))
-        assert a @ b >= 0.998 * np.linalg.norm(a) * np.linalg.norm(b)
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b), (ix[0], np.linalg.norm(a - b) / np.linalg.norm(b))
+        assert a @ b >= 0.9999 * np.linalg.norm(a) * np.linalg.norm(b)
 
 
 def test_tc_nodes_match_oracle(small_water, theta):
@@ -57,8 +57,8 @@ def test_tc_nodes_match_oracle(small_water, theta):
     e = _engine(n_mol, box, theta, "bf16_tc")
     u, du = e.mlp_eval()
     uo, duo = orc.mlp_nodes(theta[7:])
-    assert np.abs(u - uo).max() <= 2e-2 * np.abs(uo).max(), np.abs(u - uo).max() / np.abs(uo).max()
-    assert np.abs(du - duo).max() <= 2e-2 * np.abs(duo).max()
+    assert np.abs(u - uo).max() <= 1e-3 * np.abs(uo).max(), np.abs(u - uo).max() / np.abs(uo).max()
+    assert np.abs(du - duo).max() <= 1e-3 * np.abs(duo).max()
 
 
 def test_tc_per_pair_evaluation(small_water, theta):
@@ -69,8 +69,8 @@ def test_tc_per_pair_evaluation(small_water, theta):
     coef = orc.mlp_table(theta[7:])
     uo = np.array([[orc.mlp_pair(coef, t, rr)[0] for rr in r[t]] for t in range(3)])
     Fo = np.array([[orc.mlp_pair(coef, t, rr)[1] for rr in r[t]] for t in range(3)])
-    assert np.abs(u - uo).max() <= 2e-2 * np.abs(uo).max()
-    assert np.abs(-du - Fo).max() <= 2e-2 * np.abs(Fo).max()
+    assert np.abs(u - uo).max() <= 1e-3 * np.abs(uo).max()
+    assert np.abs(-du - Fo).max() <= 1e-3 * np.abs(Fo).max()
 
 
 def test_tc_backward_matches_fp64(small_water, theta):
