@@ -97,7 +97,10 @@ def parse():
     ap.add_argument("--gas-trunc", type=int, default=200)
     ap.add_argument("--gas-loss", default="diff_rdf_ev", choices=["diff", "diff_ev", "diff_rdf_ev"])
     ap.add_argument("--gas-precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--updates", type=int, default=200, help="mlp: training updates per arm")
+    ap.add_argument("--updates", type=int, default=200, help="mlp: classical training updates "
+                    "(the MLP arm trains for the same wall-clock time)")
+    ap.add_argument("--mlp-precision", default="bf16_tc", choices=["bf16_tc", "fp64"],
+                    help="mlp: the network arithmetic (split-BF16 tensor cores or FP64 CUDA cores)")
     ap.add_argument("--train-steps", type=int, default=2000, help="mlp: steps per update")
     ap.add_argument("--train-steps-loss", type=int, default=500)
     ap.add_argument("--train-trunc", type=int, default=200)
@@ -109,7 +112,7 @@ def parse():
                     help="diamond without the learned radial term (SW alone)")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed gradient and exit (the command profiled under ncu)")
-    ap.add_argument("--profile-shape", default="16,8,3/32,4,1",
+    ap.add_argument("--profile-shape", default="16,24,1/16,24,2",
                     help="water --profile: reverse/forward launch shapes (lanes,mols_per_cta,unroll)")
     return ap.parse_args()
 
@@ -1759,9 +1762,13 @@ def mlp_config(a, extra=None):
                          "-> 64 -> 64 SiLU -> 1, cosine cutoff, 15,939 parameters, seeded "
                          "Xavier init; tabulated on 1,024 intervals, cubic Hermite per pair",
          "loss": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs sigma x1.02 / eps x0.95 target",
-         "training": f"{a.updates} Adam updates per arm, {a.train_steps} steps per update, loss "
-                     f"every {a.train_steps_loss}, truncation {a.train_trunc}, gamma 1/ps; "
-                     "classical lr 2e-3 x |theta_0| (the reference's scaled Adam), MLP lr 1e-3",
+         "training": f"classical: {a.updates} Adam updates; classical + MLP: the same wall-clock "
+                     f"time; {a.train_steps} steps per update, loss every {a.train_steps_loss}, "
+                     f"truncation {a.train_trunc}, gamma 1/ps; classical lr 2e-3 x |theta_0| (the "
+                     "reference's scaled Adam), MLP lr 1e-3; target: the O-O RDF of a teacher "
+                     "(default LJ + a fixed MLP correction, seeded init + N(0, 0.05)), outside "
+                     "the classical family",
+         "mlp_precision": a.mlp_precision,
          "precision": a.precision, "l2": "flushed (256 MiB write) between timed steps"}
     if extra:
         c.update(extra)
@@ -1786,6 +1793,7 @@ def run_ours_mlp(a):
     x0, v0, p, target = prepare(a, local, a.equil_ps)
     theta0 = np.concatenate([p, mlp.init_params(3)])
     eng = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=True)
+    eng.set_mlp_precision(a.mlp_precision)
     eng.set_params(theta0)
     eng.set_loss([oo_l2_term(target)])
     eng.set_state(x0, v0)
@@ -1852,6 +1860,31 @@ def run_ours_mlp(a):
                 "ipairs": ipairs, "flops_per_launch": flops_launch,
                 "peak_source": "measured FP32 FFMA throughput of this GPU (revsim_probe_fp32_tflops)"}
 
+    # the network per pair against the table: one evaluation at every atom pair within the
+    # cutoff (what a per-pair network would run in each forward step), and at the table nodes
+    d = xs[pairs[:, 1]] - xs[pairs[:, 0]]
+    d -= 3.0 * np.round(d / 3.0)
+    rr = np.sqrt((d * d).sum(1))
+    rr = rr[rr <= 1.0]
+    n_row = (len(rr) + 2) // 3
+    r_rows = np.resize(rr, 3 * n_row).reshape(3, n_row)
+    eng.mlp_eval_time(r_rows)
+    per_pair_ms = min(eng.mlp_eval_time(r_rows) for _ in range(5))
+    nodes_ms = min(eng.mlp_eval_time() for _ in range(5))
+    eng.set_kernel_timing(True)
+    eng.set_state(x0, v0)
+    eng.forward(seeds[:100], 0.0, 100, 100, 0.001)
+    fk_ms, fk_n = eng.kernel_time(1)
+    eng.set_kernel_timing(False)
+    fwd_launch_ms = fk_ms / max(fk_n, 1)
+    network = {"pairs_within_cutoff": int(len(rr)), "per_pair_eval_ms": per_pair_ms,
+               "table_nodes_eval_ms": nodes_ms, "forward_step_kernel_ms": fwd_launch_ms,
+               "note": "per_pair_eval_ms: the tensor-core network evaluated once at every atom "
+                       "pair within the cutoff (value and derivative), the cost a per-pair "
+                       "network would add to each forward step; the engine instead evaluates "
+                       "3 x 1,025 table nodes once per parameter update (table_nodes_eval_ms) "
+                       "and reads cubic Hermite intervals inside the step kernel"}
+
     # accuracy: mixed vs FP64 GPU gradient over the first 100 steps
     e64 = Engine(895, 3.0, inter_type="lj", precision="fp64", device=local, mlp=True)
     e64.set_params(theta0)
@@ -1868,12 +1901,29 @@ def run_ours_mlp(a):
     err_mlp = float(np.abs(gm[nc:] - g64[nc:]).max() / np.abs(g64[nc:]).max())
     e64.close()
 
-    # training comparison (same start, same seeds per update)
+    # training comparison (same start, same seeds per update) against a target the classical
+    # model cannot represent: the RDF of LJ plus a fixed MLP correction
+    teach = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=True)
+    teach.set_mlp_precision(a.mlp_precision)
+    teach.set_params(np.concatenate([p, mlp.init_params(11) + np.random.default_rng(12).normal(
+        scale=0.05, size=mlp.N_PARAMS)]))
+    teach.set_state(x0, v0)
+    teach.forward(systems.noise_seeds(1000, seed=13), 5.0, 1000, 1000, 0.001, calc_loss=False)
+    teach.set_loss([oo_l2_term(np.zeros(200))])
+    rdfs = []
+    for k in range(8):
+        teach.forward(systems.noise_seeds(500, seed=14 + k), 1.0, 500, 500, 0.001, calc_loss=False)
+        rdfs.append(teach.rdf(0, 0))
+    teach.close()
+    teacher = np.mean(rdfs, axis=0)
     train = {}
+    wall_budget = None
     for arm, use_mlp in (("classical", False), ("classical+mlp", True)):
         e_ = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=use_mlp)
+        if use_mlp:
+            e_.set_mlp_precision(a.mlp_precision)
         th = np.array(theta0 if use_mlp else p)
-        e_.set_loss([oo_l2_term(target)])
+        e_.set_loss([oo_l2_term(teacher)])
         e_.set_params(th)
         e_.set_state(x0, v0)
         e_.autotune()
@@ -1885,7 +1935,8 @@ def run_ours_mlp(a):
         opt = mlp.Adam(len(th), lr=scale)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for u in range(a.updates):
+        u = 0
+        while (u < a.updates) if wall_budget is None else (time.perf_counter() - t0 < wall_budget):
             e_.set_params(th)
             e_.set_state(state["x"], state["v"])
             sd = systems.noise_seeds(a.train_steps, seed=5000 + u)
@@ -1894,12 +1945,14 @@ def run_ours_mlp(a):
             _, gr = e_.reverse(sd, 1.0, a.train_steps, a.train_steps_loss, a.train_trunc, 0.001)
             losses.append(float(l_u[0]))
             th = opt.step(th, gr[0])
+            u += 1
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        wall_budget = wall if wall_budget is None else wall_budget
         e_.close()
-        k = max(1, a.updates // 10)
+        k = max(1, u // 10)
         train[arm] = {"wall_s": wall, "loss_first": float(np.mean(losses[:k])),
-                      "loss_last": float(np.mean(losses[-k:])), "updates": a.updates,
+                      "loss_last": float(np.mean(losses[-k:])), "updates": u,
                       "loss_curve_every_10": [float(np.mean(losses[i:i + 10]))
                                               for i in range(0, len(losses), 10)]}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -1910,7 +1963,7 @@ def run_ours_mlp(a):
            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None,
            "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])},
            "grad_rel_err_vs_fp64_first_100_steps": {"classical": err_cl, "mlp": err_mlp},
-           "training": train,
+           "training": train, "network_per_pair_vs_table": network,
            "e2e_note": "every timed gradient starts from host arrays (set_state), so value is "
                        "end to end"}
     if rank == 0:

@@ -287,11 +287,12 @@ int32_t revsim_graph_stats(const revsim_handle *h, int64_t *captures, int64_t *r
 /* The learned term's network arithmetic (REVSIM_MLP_FP64 or REVSIM_MLP_BF16_TC); rebuilds the
  * interval table from the current parameters.  REVSIM_ERR_STATE on a handle without the term. */
 int32_t revsim_set_mlp_precision(revsim_handle *h, int32_t mode);
-/* The network itself on the tensor cores (BF16 operands, FP32 accumulation) at n distances
- * per type: r [3][n] nm (O-O, O-H, H-H rows; NULL = the table's nodes k rc / 1024, n = 1025),
- * u [3][n] = MLP(phi(r)) fc(r) and du [3][n] = du/dr.  For tests and for timing a per-pair
- * evaluation against the table. */
-int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du);
+/* The network itself on the tensor cores (split BF16 operands, FP32 accumulation) at n
+ * distances per type: r [3][n] nm (O-O, O-H, H-H rows; NULL = the table's nodes k rc / 1024,
+ * n = 1025), u [3][n] = MLP(phi(r)) fc(r) and du [3][n] = du/dr (both NULL: not copied back),
+ * ms (may be NULL) = the device time of the evaluation kernel.  For tests and for timing a
+ * per-pair evaluation against the table. */
+int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du, double *ms);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that time with events. */
 void *revsim_stream(revsim_handle *h);

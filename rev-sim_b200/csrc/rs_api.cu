@@ -1951,8 +1951,8 @@ int32_t revsim_set_mlp_precision(revsim_handle *h, int32_t mode) {
     return REVSIM_OK;
 }
 
-int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du) {
-    if (!h || n < 1 || !u || !du) return REVSIM_ERR_BADARG;
+int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du, double *ms) {
+    if (!h || n < 1 || (!u != !du)) return REVSIM_ERR_BADARG;
     if (!h->mlp || !h->have_params || !h->d_mlp_theta) return fail(h, REVSIM_ERR_STATE, "no learned pair term set");
     CK(cudaSetDevice(h->dev));
     const size_t need = (size_t)MLP_NT * n;
@@ -1966,12 +1966,28 @@ int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u,
         h->mlp_eval_cap = need;
     }
     if (r) CK(cudaMemcpyAsync(h->d_mlp_r, r, sizeof(double) * need, cudaMemcpyHostToDevice, h->st));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, h->st));
+    }
     CK(launch_mlp_tc_eval(h->d_mlp_theta, MLP_NT, h->rc, MLP_WIDTH, n, r ? h->d_mlp_r : nullptr, h->d_mlp_u,
                           h->d_mlp_u + need, h->st));
     h->launches++;
-    CK(cudaMemcpyAsync(u, h->d_mlp_u, sizeof(double) * need, cudaMemcpyDeviceToHost, h->st));
-    CK(cudaMemcpyAsync(du, h->d_mlp_u + need, sizeof(double) * need, cudaMemcpyDeviceToHost, h->st));
+    if (ms) CK(cudaEventRecord(e1, h->st));
+    if (u) {
+        CK(cudaMemcpyAsync(u, h->d_mlp_u, sizeof(double) * need, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(du, h->d_mlp_u + need, sizeof(double) * need, cudaMemcpyDeviceToHost, h->st));
+    }
     CK(cudaStreamSynchronize(h->st));
+    if (ms) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        *ms = t;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
     return REVSIM_OK;
 }
 

@@ -187,7 +187,7 @@ def load(path=LIB_PATH):
         "revsim_set_graph_mode": (i32, [vp, i32]),
         "revsim_set_integrator": (i32, [vp, i32]),
         "revsim_set_mlp_precision": (i32, [vp, i32]),
-        "revsim_mlp_eval": (i32, [vp, i32, pd, pd, pd]),
+        "revsim_mlp_eval": (i32, [vp, i32, pd, pd, pd, pd]),
         "revsim_graph_stats": (i32, [vp, pi64, pi64]),
         "revsim_reverse_noise": (i32, [vp, pd, d, i32, i32, i32, d, d, pd, pd]),
         "revsim_stream": (vp, [vp]),

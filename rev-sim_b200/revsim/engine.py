@@ -302,8 +302,19 @@ class Engine:
             r = np.ascontiguousarray(r, dtype=np.float64).reshape(3, -1)
             n, rp = r.shape[1], f64p(r)
         u, du = np.zeros((3, n)), np.zeros((3, n))
-        self._check(self._L.revsim_mlp_eval(self._h, n, rp, f64p(u), f64p(du)))
+        self._check(self._L.revsim_mlp_eval(self._h, n, rp, f64p(u), f64p(du), None))
         return u, du
+
+    def mlp_eval_time(self, r=None):
+        """Device milliseconds of one tensor-core evaluation of the network at r [3, n]
+        (None: the 1,025 table nodes per type)."""
+        ms = ctypes.c_double()
+        if r is None:
+            self._check(self._L.revsim_mlp_eval(self._h, 1025, None, None, None, ctypes.byref(ms)))
+        else:
+            r = np.ascontiguousarray(r, dtype=np.float64).reshape(3, -1)
+            self._check(self._L.revsim_mlp_eval(self._h, r.shape[1], f64p(r), None, None, ctypes.byref(ms)))
+        return ms.value
 
     def set_integrator(self, mode="reference"):
         """"reference" (the reference's FP64 step arithmetic) or "exact" (grid increments: with
