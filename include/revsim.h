@@ -315,8 +315,9 @@ int32_t revsim_kernel_time(revsim_handle *h, int32_t which, double *total_ms, in
  * forces are summed depends on it, and the reverse pass rebuilds the trajectory only when
  * its forces are the forward pass's bits); a count the other kernel's shape does not allow
  * returns REVSIM_ERR_BADARG.  revsim_autotune times the allowed shapes on the current state
- * and keeps the lane count with the smallest forward + reverse time and, for it, each
- * kernel's fastest shape. */
+ * (CTAs of 64-512 threads, plus the molecule counts that spread the CTAs over every SM in
+ * one wave of one or two per SM) and keeps the lane count with the smallest forward +
+ * reverse time and, for it, each kernel's fastest shape. */
 int32_t revsim_set_launch_shape(revsim_handle *h, int32_t which, int32_t lanes_per_mol,
                                 int32_t mols_per_cta, int32_t unroll);
 int32_t revsim_get_launch_shape(revsim_handle *h, int32_t which, int32_t *lanes_per_mol,

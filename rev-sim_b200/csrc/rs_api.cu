@@ -28,6 +28,10 @@ using namespace rs;
 namespace {
 
 constexpr double kRext = 0.15;        // bound on intramolecular O-H distance, nm
+// Tighter O-H bound under which the row build takes one periodic image per molecule pair
+// (boxes above 2 (rc_nl + 2 kRnear) + 0.02 nm); a molecule beyond it sends the build back to
+// per-atom-pair images (same rows either way).
+constexpr double kRnear = 0.12;
 constexpr double kTwoPow1o6 = 1.122462048309373;
 
 int form_nparams(int f) {
@@ -477,6 +481,8 @@ int build_nlist(revsim_handle *h, const double *xsrc, uint32_t *nbr = nullptr, i
     const double rcand = h->rc_nl + 2 * kRext;
     a.rcand2 = rcand * rcand;
     a.rext2 = kRext * kRext;
+    a.rnear2 = kRnear * kRnear;
+    a.shift_box = 2 * (h->rc_nl + 2 * kRnear) + 0.02;
     a.status = h->d_status;
     a.max_cnt = h->d_maxcnt;
     cudaError_t e = launch_nlist(a, h->st);
@@ -1185,7 +1191,7 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
               cudaMalloc(&h->d_pos[0], v4 * h->N) == cudaSuccess && cudaMalloc(&h->d_pos[1], v4 * h->N) == cudaSuccess &&
               cudaMalloc(&h->d_wgt[0], v4 * h->N) == cudaSuccess && cudaMalloc(&h->d_wgt[1], v4 * h->N) == cudaSuccess &&
               dalloc(&h->d_scale, 2 * h->R) == cudaSuccess && dalloc(&h->d_status, 1) == cudaSuccess &&
-              dalloc(&h->d_maxcnt, 1) == cudaSuccess && dalloc(&h->d_count, 1) == cudaSuccess &&
+              dalloc(&h->d_maxcnt, 2) == cudaSuccess && dalloc(&h->d_count, 1) == cudaSuccess &&
               dalloc(&h->d_loss, h->R) == cudaSuccess && dalloc(&h->d_loss_acc, h->R) == cudaSuccess &&
               dalloc(&h->d_cell_rep, ncell) == cudaSuccess;
     if (!ok) return cfail("alloc");
@@ -1200,7 +1206,7 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
          cudaMemcpy(h->d_rep_nc, rep_nc.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(h->d_rep_cell_off, rep_coff.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(h->d_cell_rep, cell_rep.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemset(h->d_status, 0, sizeof(int)) == cudaSuccess && cudaMemset(h->d_maxcnt, 0, sizeof(int)) == cudaSuccess &&
+         cudaMemset(h->d_status, 0, sizeof(int)) == cudaSuccess && cudaMemset(h->d_maxcnt, 0, 2 * sizeof(int)) == cudaSuccess &&
          cudaMemset(h->d_C, 0, sizeof(double) * n3) == cudaSuccess &&
          cudaMemset(h->d_A, 0, sizeof(double) * n3) == cudaSuccess;
     if (!ok) return cfail("upload");
@@ -2096,16 +2102,33 @@ int32_t revsim_autotune(revsim_handle *h, double dt) {
     CK(cudaEventCreate(&e1));
     double best_total = std::numeric_limits<double>::infinity();
     int bm[2] = {h->shp[0].mpc, h->shp[1].mpc}, bu[2] = {h->shp[0].U, h->shp[1].U}, bg = h->shp[0].G;
+    int n_sm = 148;
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->dev));
+    auto blocks_for = [&](int m) {
+        long b = 0;
+        for (int r = 0; r < h->R; r++) b += (h->nmol[r] + m - 1) / m;
+        return b;
+    };
     for (int G : {8, 16, 32}) {
         double tot = 0.0;
         int gm[2] = {0, 0}, gu[2] = {1, 1};
+        // molecules per CTA: the fixed thread counts, plus the smallest counts (whole warps)
+        // whose CTAs fit in one wave of one or two CTAs per SM, which spread the molecules
+        // over every SM
+        std::vector<int> mpcs;
+        for (int threads : {64, 128, 192, 256, 384, 512})
+            if (threads >= G && threads % G == 0) mpcs.push_back(threads / G);
+        const int mstep = std::max(1, 32 / G);
+        for (int k : {1, 2}) {
+            int m = mstep;
+            while (m * G <= 512 && blocks_for(m) > (long)k * n_sm) m += mstep;
+            if (m * G <= 512 && std::find(mpcs.begin(), mpcs.end(), m) == mpcs.end()) mpcs.push_back(m);
+        }
         for (int dir = 0; dir < 2 && !rc; dir++) {
             const bool rev = dir == 0;
             double best = std::numeric_limits<double>::infinity();
-            for (int threads : {64, 128, 192, 256, 384, 512}) {
-                if (threads < G || threads % G) continue;
+            for (int mpc : mpcs) {
                 for (int U : {1, 2, 3}) {
-                    const int mpc = threads / G;
                     if (!shape_ok(h, dir, G, mpc, U)) continue;
                     if ((rc = set_shape_dir(h, dir, G, mpc, U))) break;
                     StepArgs a = base_args(h, rev);

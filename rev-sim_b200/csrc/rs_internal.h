@@ -143,9 +143,12 @@ struct NlistArgs {
     double rc_nl2;     // neighbour-list cutoff^2
     double rcand2;     // O-O candidate radius^2
     double rext2;      // max intramolecular O-H distance^2
+    double rnear2;     // O-H distance^2 bound under which one image shift per molecule pair holds
+    double shift_box;  // boxes above this side may use one image shift per molecule pair
     float band;        // |FP32 d^2 - rc_nl^2| at or below which FP64 decides membership
     int *status;
-    int *max_cnt;      // [1] running maximum of the row counts
+    int *max_cnt;      // [0] running maximum of the row counts; [1] this build's count of
+                       // molecules with an O-H distance above sqrt(rnear2)
 };
 
 struct RdfArgs {

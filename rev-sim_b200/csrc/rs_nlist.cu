@@ -44,8 +44,9 @@ __global__ void k_cell_count(NlistArgs a) {
     a.cell_of_mol[I] = cell;
     atomicAdd(a.cell_cnt + cell, 1);
     // Molecules are matched by O-O distance with a margin of two O-H lengths.
-    if (dist2_fp64(xo, xo + 3, L) > a.rext2 || dist2_fp64(xo, xo + 6, L) > a.rext2)
-        atomicOr(a.status, ST_GEOMETRY);
+    const double d1 = dist2_fp64(xo, xo + 3, L), d2 = dist2_fp64(xo, xo + 6, L);
+    if (d1 > a.rext2 || d2 > a.rext2) atomicOr(a.status, ST_GEOMETRY);
+    if (!(d1 <= a.rnear2 && d2 <= a.rnear2)) atomicAdd(a.max_cnt + 1, 1);
 }
 
 // Exclusive scan of the cell counts (one CTA; cells are few).
@@ -94,15 +95,25 @@ __global__ void k_cell_sort(NlistArgs a) {
     a.cell_sorted[s + rank] = I;
 }
 
-// Rows of the molecules of one home cell (one to four CTAs per cell).  The CTA stages the
-// neighbourhood -- the members of the surrounding cells, in the canonical cell order
-// and index order within a cell -- with all three atoms in FP32 in shared memory, in
-// chunks of up to kRowChunk molecules.  Each warp takes one home molecule at a time:
-// an FP32 O-O test against the candidate radius (with a margin far above FP32 error)
-// selects candidate molecules, an FP32 test classifies each of the nine atom pairs as
-// clearly inside / clearly outside the list cutoff, and the few pairs within `band` of
-// the cutoff are decided by the exact FP64 Molly arithmetic (dist2_fp64), so the set
-// is bit-identical to the all-FP64 test.  Entries are appended in candidate order.
+// Rows of the molecules of one home cell (up to eight CTAs of eight warps per cell, so that
+// a warp has at most one home molecule in all but the fullest cells: the build's time is
+// that of its slowest warp).  The CTA stages the neighbourhood -- the members of the
+// surrounding cells, in the canonical cell order and index order within a cell -- with all
+// three atoms in FP32 in shared memory, in chunks of up to kRowChunk molecules.  Each warp
+// takes one home molecule at a time: an FP32 O-O test against the candidate radius (with a
+// margin far above FP32 error) selects candidate molecules, an FP32 test classifies each of
+// the nine atom pairs as clearly inside / clearly outside the list cutoff, and the few pairs
+// within `band` of the cutoff are decided by the exact FP64 Molly arithmetic (dist2_fp64),
+// so the set is bit-identical to the all-FP64 test.  Entries are appended in candidate order.
+//
+// Periodic images.  The FP64 test takes each atom pair's own minimum image.  When every O-H
+// distance is at most r_near (counted by k_cell_count) and the box side L exceeds
+// 2 (rc_nl + 2 r_near) + 0.02 nm, the FP32 test shifts all three atoms of the candidate by
+// the image of the O-O vector instead: an atom pair whose own image differs has a component
+// beyond L/2 after that shift, so both distances exceed L/2 - 2 r_near > rc_nl + 0.01 nm and
+// the pair is outside either way; every other pair gets the same vector up to FP32 rounding
+// (|d^2 error| < 5e-6 L/4.5 nm, a quarter of `band`).  The rows are the same bits with
+// either form; the shifted form saves the 27 per-component image selections.
 constexpr int kRowChunk = 1024;
 constexpr int kCandBatch = 256;
 
@@ -121,6 +132,7 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     const int off0 = a.rep_cell_off[r];
     const double Ld = a.rep_box[r];
     const float L = (float)Ld, hL = 0.5f * (float)Ld;
+    const bool one_image = Ld > a.shift_box && a.max_cnt[1] == 0;
     const int hs = a.cell_start[c_home], hn = a.cell_cnt[c_home];
     // gridDim.y CTAs share a home cell: CTA y takes every gridDim.y-th group of nwarp home
     // molecules (each stages the whole neighbourhood)
@@ -148,6 +160,9 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     }
     __syncthreads();
     const int total = s_off[ncell];
+    // the home cell's place in the neighbourhood order (its members are staged in index
+    // order there, so home molecule hi is staged candidate s_off[tc] + hi)
+    const int tc = nc >= 5 ? (2 * span + 2) * span + 2 : (cz * span + cy) * span + cx;
     const int lane = threadIdx.x & 31;
     const int nwarp = (int)gridDim.y * (int)(blockDim.x >> 5);               // warps per home cell
     const int warp = (int)blockIdx.y * (int)(blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -156,7 +171,8 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     const float band = a.band;
     // per home molecule state kept across chunks (a warp owns the same molecules in
     // every chunk: home members warp, warp + nwarp, ...)
-    constexpr int kMaxHome = 8;   // home molecules per warp per pass
+    constexpr int kMaxHome = 1;   // home molecules per warp per staging pass (the split gives
+                                  // warps for twice the mean count; fuller cells restage)
     for (int h0 = 0; h0 < hn; h0 += nwarp * kMaxHome) {
         int cnt[kMaxHome];
 #pragma unroll
@@ -164,10 +180,15 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
         for (int c0 = 0; c0 < total; c0 += kRowChunk) {
             const int cn = min(kRowChunk, total - c0);
             __syncthreads();
-            int t = 0;   // cell of candidate g (g grows with k, so t only moves forward)
             for (int k = threadIdx.x; k < cn; k += blockDim.x) {
                 const int g = c0 + k;
-                while (s_off[t + 1] <= g) t++;
+                // the cell t with s_off[t] <= g < s_off[t + 1]
+                int t = 0, t1 = ncell;
+                while (t1 - t > 1) {
+                    const int mid = (t + t1) >> 1;
+                    if (s_off[mid] <= g) t = mid;
+                    else t1 = mid;
+                }
                 const int J = a.cell_sorted[s_start[t] + (g - s_off[t])];
                 s_idx[k] = J;
                 const double *xj = a.x + 9 * (size_t)J;
@@ -180,6 +201,7 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                 const int hi = h0 + q * nwarp + warp;
                 if (hi >= hn) break;
                 const int I = a.cell_sorted[hs + hi];
+                const int kself = s_off[tc] + hi - c0;   // the home molecule in this chunk
                 float xi[9];
 #pragma unroll
                 for (int u = 0; u < 9; u++) xi[u] = (float)a.x[9 * (size_t)I + u];
@@ -198,7 +220,7 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                             const float ox = mi_f(s_c[k] - xi[0], L, hL);
                             const float oy = mi_f(s_c[kRowChunk + k] - xi[1], L, hL);
                             const float oz = mi_f(s_c[2 * kRowChunk + k] - xi[2], L, hL);
-                            pass = s_idx[k] != I && ox * ox + oy * oy + oz * oz <= rcand2;
+                            pass = k != kself && ox * ox + oy * oy + oz * oz <= rcand2;
                         }
                         const unsigned bal = __ballot_sync(0xffffffffu, pass);
                         if (pass) s_k[nk + __popc(bal & ((1u << lane) - 1u))] = k;
@@ -212,13 +234,31 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                             const int k = s_k[idx];
                             const int J = s_idx[k];
                             uint32_t mask = 0;
+                            float cb[9];
+                            if (one_image) {
+#pragma unroll
+                                for (int u = 0; u < 3; u++) {
+                                    const float d = s_c[u * kRowChunk + k] - xi[u];
+                                    const float sft = d > hL ? -L : (d < -hL ? L : 0.f);
+#pragma unroll
+                                    for (int kb = 0; kb < 3; kb++)
+                                        cb[3 * kb + u] = s_c[(3 * kb + u) * kRowChunk + k] + sft;
+                                }
+                            }
 #pragma unroll
                             for (int ka = 0; ka < 3; ka++)
 #pragma unroll
                                 for (int kb = 0; kb < 3; kb++) {
-                                    const float dx = mi_f(s_c[(3 * kb) * kRowChunk + k] - xi[3 * ka], L, hL);
-                                    const float dy = mi_f(s_c[(3 * kb + 1) * kRowChunk + k] - xi[3 * ka + 1], L, hL);
-                                    const float dz = mi_f(s_c[(3 * kb + 2) * kRowChunk + k] - xi[3 * ka + 2], L, hL);
+                                    float dx, dy, dz;
+                                    if (one_image) {
+                                        dx = cb[3 * kb] - xi[3 * ka];
+                                        dy = cb[3 * kb + 1] - xi[3 * ka + 1];
+                                        dz = cb[3 * kb + 2] - xi[3 * ka + 2];
+                                    } else {
+                                        dx = mi_f(s_c[(3 * kb) * kRowChunk + k] - xi[3 * ka], L, hL);
+                                        dy = mi_f(s_c[(3 * kb + 1) * kRowChunk + k] - xi[3 * ka + 1], L, hL);
+                                        dz = mi_f(s_c[(3 * kb + 2) * kRowChunk + k] - xi[3 * ka + 2], L, hL);
+                                    }
                                     const float d2 = dx * dx + dy * dy + dz * dz;
                                     bool in = d2 < rc2f;
                                     if (fabsf(d2 - rc2f) <= band)
@@ -281,6 +321,7 @@ __global__ void k_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap,
 
 cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
     cudaMemsetAsync(a.cell_cnt, 0, sizeof(int) * a.n_cells, st);
+    cudaMemsetAsync(a.max_cnt + 1, 0, sizeof(int), st);
     const int t = 256, b = (a.M + t - 1) / t;
     k_cell_count<<<b, t, 0, st>>>(a);
     k_cell_scan<<<1, 1024, 0, st>>>(a);
@@ -288,10 +329,11 @@ cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
     k_cell_sort<<<b, t, 0, st>>>(a);
     const size_t smem = (9 * sizeof(float) + sizeof(int)) * kRowChunk;
     cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // home molecules per cell over the 8 warps of a CTA: split a cell over up to 4 CTAs so
-    // that a warp has about one home molecule
+    // home molecules per cell over the 8 warps of a CTA: split a cell over up to 8 CTAs,
+    // with warps for twice the mean count, so that the fullest cells of a Poisson-like
+    // occupancy still give a warp one home molecule (CTAs beyond a cell's count exit at once)
     const int per_cell = (a.M + a.n_cells - 1) / a.n_cells;
-    const int split = std::min(4, std::max(1, (per_cell + 7) / 8));
+    const int split = std::min(8, std::max(1, (2 * per_cell + 7) / 8));
     k_rows<<<dim3(a.n_cells, split), 256, smem, st>>>(a);
     return cudaGetLastError();
 }
