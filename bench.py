@@ -76,6 +76,9 @@ def parse():
     ap.add_argument("--integrator", default="exact", choices=["exact", "reference"],
                     help="water: the exactly reversible integrator (grid increments) or the "
                          "reference's FP64 step arithmetic")
+    ap.add_argument("--pair-mode", default="both_sides", choices=["both_sides", "half_shell"],
+                    help="water, mixed precision: each molecule pair evaluated from both sides in "
+                         "one fused kernel, or once by its owner with a gather kernel")
     ap.add_argument("--cfg1-replicas", type=int, default=16,
                     help="895-water target configuration: replicas batched in one handle")
     ap.add_argument("--no-target", action="store_true",
@@ -132,8 +135,11 @@ LOSS_TEXT = {
 
 
 def integ(e, a):
-    """The integrator arithmetic of a timed water engine (revsim_set_integrator)."""
+    """The integrator arithmetic of a timed water engine (revsim_set_integrator) and, for
+    mixed precision, its pair evaluation (revsim_set_pair_mode)."""
     e.set_integrator(a.integrator)
+    if e.precision == "mixed":
+        e.set_pair_mode(a.pair_mode)
     return e
 
 
@@ -156,7 +162,8 @@ def config(a, extra=None):
          "n_steps_log": 1000, "dt_ps": 0.001, "gamma_per_ps": a.gamma, "pair_form": a.form,
          "precision": a.precision,
          "loss": LOSS_TEXT[a.loss],
-         "l2": "flushed (256 MiB write) between timed steps", "integrator": a.integrator}
+         "l2": "flushed (256 MiB write) between timed steps", "integrator": a.integrator,
+         "pair_mode": a.pair_mode}
     if extra:
         c.update(extra)
     return c

@@ -294,6 +294,21 @@ int32_t revsim_set_mlp_precision(revsim_handle *h, int32_t mode);
  * per-pair evaluation against the table. */
 int32_t revsim_mlp_eval(revsim_handle *h, int32_t n, const double *r, double *u, double *du, double *ms);
 
+/* Pair evaluation of the mixed-precision step kernels.  REVSIM_PAIRS_BOTH_SIDES (default):
+ * each molecule's lanes evaluate its whole neighbour row, so every unordered pair is
+ * evaluated twice and each molecule's forces are summed by its own lanes in one fused
+ * kernel.  REVSIM_PAIRS_HALF_SHELL: each pair is evaluated once, by one of its molecules
+ * (I when I + J is odd and I < J, or even and I > J), which writes the partner's share to a
+ * slot; a second kernel per step sums each molecule's slots in row order (deterministic,
+ * forward and reverse forces the same bits).  In effect only with FP32 pair arithmetic,
+ * boxes above 2 (cutoff + 0.3 nm) + 0.02 nm and no barostat; otherwise the both-sides
+ * kernels run.  REVSIM_ERR_STATE for an FP64 handle.  Invalidates the forward record.
+ * revsim_get_pair_mode returns the requested mode and the one in effect. */
+#define REVSIM_PAIRS_BOTH_SIDES 0
+#define REVSIM_PAIRS_HALF_SHELL 1
+int32_t revsim_set_pair_mode(revsim_handle *h, int32_t mode);
+int32_t revsim_get_pair_mode(const revsim_handle *h, int32_t *requested, int32_t *active);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time with events. */
 void *revsim_stream(revsim_handle *h);
 

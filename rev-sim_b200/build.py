@@ -22,6 +22,7 @@ LIB = os.path.join(HERE, "librevsim.so")
 SOURCES = ["rs_api.cu", "rs_step.cu", "rs_nlist.cu", "rs_loss.cu", "rs_probe.cu", "sw_kernels.cu",
            "sw_api.cu"] + [
     f"rs_step_{p}_{f}.cu" for p in "fd" for f in ("lj", "dexp", "buck", "ljsc", "buff", "ljmlp")] + [
+    f"rs_half_{f}.cu" for f in ("lj", "dexp", "buck", "ljsc", "buff", "ljmlp")] + [
     "rs_mlp.cu", "rs_mlp_tc.cu", "rs_energy.cu", "rs_barostat.cu", "gas_kernels.cu", "gas_api.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

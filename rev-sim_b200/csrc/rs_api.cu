@@ -98,8 +98,17 @@ struct revsim_handle {
     int *d_rep_nc = nullptr, *d_rep_cell_off = nullptr;
     int *d_cell_of_mol = nullptr, *d_cell_cnt = nullptr, *d_cell_start = nullptr,
         *d_cell_fill = nullptr, *d_cell_tmp = nullptr, *d_cell_sorted = nullptr;
-    uint32_t *d_nbr = nullptr;       // working rows [M * cap]
-    int *d_nbr_cnt = nullptr;
+    uint32_t *d_nbr = nullptr;       // working rows [M * cap] (+ the split rows, mixed precision)
+    int *d_nbr_cnt = nullptr;        // [M] (+ owned and incoming counts, mixed precision)
+    // Half-shell pair evaluation (mixed precision; REVSIM_PAIRS_HALF_SHELL): requested, in
+    // effect at the last forward pass, and its scratch (compact owned positions of the split,
+    // per-entry partner slots, per-molecule own partials), sized for half_cap
+    bool half_req = false, fwd_half = false;
+    int *d_ownpos = nullptr;
+    float4 *d_slot_f = nullptr;
+    float2 *d_slot_g = nullptr;
+    float *d_own = nullptr;
+    int half_cap = 0;
     int *d_cell_rep = nullptr;
     float band = 2e-5f;
     // rows of every forward build, reused by the reverse pass (checkpoint mode)
@@ -352,6 +361,40 @@ int quantize_for_exact(revsim_handle *h) {
     return REVSIM_OK;
 }
 
+// A row set: the rows [M * cap], then (mixed precision) the split rows [M * cap] of the
+// half-shell kernels; counts [M], then (mixed precision) owned [M] and incoming [M] counts.
+bool split_rows(const revsim_handle *h) { return h->prec == REVSIM_MIXED; }
+size_t rows_set(const revsim_handle *h) { return (size_t)h->M * h->cap * (split_rows(h) ? 2 : 1); }
+size_t cnts_set(const revsim_handle *h) { return (size_t)h->M * (split_rows(h) ? 3 : 1); }
+
+// Half-shell pair evaluation in effect: requested, FP32 pair arithmetic, one periodic image
+// per molecule pair in every box, and no barostat (whose box moves could end that).
+bool half_eff(const revsim_handle *h) { return h->half_req && split_rows(h) && h->shift_ok && !h->baro_on; }
+
+void free_half(revsim_handle *h) {
+    dfree(h->d_ownpos);
+    dfree(h->d_slot_f);
+    dfree(h->d_slot_g);
+    dfree(h->d_own);
+    h->d_ownpos = nullptr;
+    h->d_slot_f = nullptr;
+    h->d_slot_g = nullptr;
+    h->d_own = nullptr;
+    h->half_cap = 0;
+}
+
+int ensure_half(revsim_handle *h) {
+    if (h->half_cap == h->cap && h->d_own) return REVSIM_OK;
+    free_half(h);
+    const size_t mc = (size_t)h->M * h->cap;
+    CK(dalloc(&h->d_ownpos, mc));
+    CK(dalloc(&h->d_slot_f, 3 * mc));
+    CK(dalloc(&h->d_slot_g, 3 * mc));
+    CK(dalloc(&h->d_own, (size_t)h->M * 36));
+    h->half_cap = h->cap;
+    return REVSIM_OK;
+}
+
 int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a_in) {
     const revsim_handle::Shape &sh = h->shp[rev ? 0 : 1];
     StepArgs a = a_in;
@@ -371,7 +414,18 @@ int launch_step_k(revsim_handle *h, bool rev, const StepArgs &a_in) {
         CK(cudaEventRecord(h->ev[which][h->ev_used[which]], h->st));
     }
     cudaError_t e;
-    if (h->prec == REVSIM_MIXED)
+    if (half_eff(h)) {
+        if (int rc = ensure_half(h)) return rc;
+        a.split = a.nbr + (size_t)h->M * h->cap;
+        a.cnt_own = a.nbr_cnt + h->M;
+        a.cnt_inc = a.nbr_cnt + 2 * (size_t)h->M;
+        a.slot_f = h->d_slot_f;
+        a.slot_g = h->d_slot_g;
+        a.own = h->d_own;
+        e = launch_half(rev, h->mlp ? (int)F_LJ_MLP : h->form, sh.G, sh.n_blk, threads, a, nb_consts<float>(h), bc,
+                        h->st);
+        h->launches++;
+    } else if (h->prec == REVSIM_MIXED)
         e = launch_step<float>(rev, h->mlp ? (int)F_LJ_MLP : h->form, sh.G, sh.U, h->shift_ok, sh.n_blk,
                                threads, a, nb_consts<float>(h), bc, h->st);
     else
@@ -426,8 +480,9 @@ int alloc_nbr(revsim_handle *h, int cap) {
     h->d_nbr_store = nullptr;
     h->d_cnt_store = nullptr;
     h->store_slots = 0;
+    free_half(h);
     h->cap = cap;
-    CK(dalloc(&h->d_nbr, (size_t)h->M * cap));
+    CK(dalloc(&h->d_nbr, rows_set(h)));
     return REVSIM_OK;
 }
 
@@ -442,8 +497,8 @@ void ensure_list_store(revsim_handle *h, size_t slots) {
     h->store_slots = 0;
     uint32_t *p = nullptr;
     int *c = nullptr;
-    if (cudaMalloc((void **)&p, sizeof(uint32_t) * (size_t)h->M * h->cap * slots) != cudaSuccess ||
-        cudaMalloc((void **)&c, sizeof(int) * (size_t)h->M * slots) != cudaSuccess) {
+    if (cudaMalloc((void **)&p, sizeof(uint32_t) * rows_set(h) * slots) != cudaSuccess ||
+        cudaMalloc((void **)&c, sizeof(int) * cnts_set(h) * slots) != cudaSuccess) {
         cudaGetLastError();   // clear the failed allocation; fall back to rebuilding
         dfree(p);
         dfree(c);
@@ -485,6 +540,16 @@ int build_nlist(revsim_handle *h, const double *xsrc, uint32_t *nbr = nullptr, i
     a.shift_box = 2 * (h->rc_nl + 2 * kRnear) + 0.02;
     a.status = h->d_status;
     a.max_cnt = h->d_maxcnt;
+    a.split = nullptr;
+    a.cnt_own = a.cnt_inc = a.ownpos = nullptr;
+    if (half_eff(h)) {
+        if (int rc = ensure_half(h)) return rc;
+        a.split = a.nbr + (size_t)h->M * h->cap;
+        a.cnt_own = a.nbr_cnt + h->M;
+        a.cnt_inc = a.nbr_cnt + 2 * (size_t)h->M;
+        a.ownpos = h->d_ownpos;
+        h->launches += 2;
+    }
     cudaError_t e = launch_nlist(a, h->st);
     h->launches += 6;
     if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("nlist: ") + cudaGetErrorString(e));
@@ -505,6 +570,7 @@ int status_code(revsim_handle *h, int s) {
     if (s & ST_GEOMETRY)
         return fail(h, REVSIM_ERR_GEOMETRY, "an O-H distance exceeds the 0.15 nm molecule bound");
     if (s & ST_NAN) return fail(h, REVSIM_ERR_NAN, "non-finite force");
+    if (s & ST_ROW_ASYM) return fail(h, REVSIM_ERR_STATE, "neighbour rows are not symmetric (half-shell split)");
     return REVSIM_OK;
 }
 
@@ -581,8 +647,8 @@ int enth_dev(revsim_handle *h, double *acc, double *ev_acc, bool grad_x, bool gr
         h->d_nbr_ev = nullptr;
         h->d_cnt_ev = nullptr;
         h->ev_cap = 0;
-        CK(dalloc(&h->d_nbr_ev, (size_t)h->M * h->cap));
-        CK(dalloc(&h->d_cnt_ev, (size_t)h->M));
+        CK(dalloc(&h->d_nbr_ev, rows_set(h)));
+        CK(dalloc(&h->d_cnt_ev, cnts_set(h)));
         h->ev_cap = h->cap;
     }
     if (!h->d_epart) CK(dalloc(&h->d_epart, (size_t)h->M * (h->P + 1)));
@@ -834,6 +900,7 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     const size_t n3 = 3 * (size_t)h->N;
     const int R = h->R;
     int rc;
+    h->fwd_half = half_eff(h);
     if ((rc = pack(h, 0, false))) return rc;
     int cur = 0;
     const bool store = h->d_nbr_store != nullptr;
@@ -864,8 +931,8 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
             CK(cudaMemcpyAsync(h->d_ckpt + k * n3, h->d_x, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
                                h->st));
             if (store) {
-                nbr = h->d_nbr_store + k * (size_t)h->M * h->cap;
-                ncnt = h->d_cnt_store + k * (size_t)h->M;
+                nbr = h->d_nbr_store + k * rows_set(h);
+                ncnt = h->d_cnt_store + k * cnts_set(h);
             }
             if ((rc = build_nlist(h, h->d_x, nbr, ncnt))) return rc;
         }
@@ -896,6 +963,9 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     const int R = h->R;
     const bool clipping = std::isfinite(clip);
     int rc;
+    // the reverse pass must evaluate pairs as the forward pass did (same force bits)
+    if (half_eff(h) != h->fwd_half)
+        return fail(h, REVSIM_ERR_STATE, "the pair evaluation mode changed since the forward pass");
     CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
     if (int rc_ = mlp_zero_adj(h)) return rc_;
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
@@ -942,8 +1012,8 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
                 const long g = m / h->nf;
                 if (g != group) {
                     if (h->d_nbr_store && (size_t)g < h->store_slots) {
-                        a.nbr = h->d_nbr_store + (size_t)g * h->M * h->cap;
-                        a.nbr_cnt = h->d_cnt_store + (size_t)g * h->M;
+                        a.nbr = h->d_nbr_store + (size_t)g * rows_set(h);
+                        a.nbr_cnt = h->d_cnt_store + (size_t)g * cnts_set(h);
                     } else {
                         if ((rc = build_nlist(h, h->d_ckpt + (size_t)g * n3))) return rc;
                         a.nbr = h->d_nbr;
@@ -1046,6 +1116,7 @@ void free_all(revsim_handle *h) {
     void *mptrs[] = {h->d_mlp_theta, h->d_mlp_adj, h->d_mlp_scratch, h->d_mlp_grad, h->d_mlp_tab,
                      h->d_epart, h->d_mlp_tc, h->d_mlp_r, h->d_mlp_u};
     for (void *p : mptrs) dfree(p);
+    free_half(h);
     void *ptrs[] = {h->d_mol_rep, h->d_atom_rep,
                     h->d_rep_atom0, h->d_rep_nmol, h->d_rep_box, h->d_rep_sdO, h->d_rep_sdH,
                     h->d_rep_nc, h->d_rep_cell_off, h->d_cell_of_mol, h->d_cell_cnt, h->d_cell_start,
@@ -1182,7 +1253,7 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
               dalloc(&h->d_cell_of_mol, h->M) == cudaSuccess && dalloc(&h->d_cell_cnt, ncell) == cudaSuccess &&
               dalloc(&h->d_cell_start, ncell) == cudaSuccess && dalloc(&h->d_cell_fill, ncell) == cudaSuccess &&
               dalloc(&h->d_cell_tmp, h->M) == cudaSuccess && dalloc(&h->d_cell_sorted, h->M) == cudaSuccess &&
-              dalloc(&h->d_nbr_cnt, h->M) == cudaSuccess && dalloc(&h->d_x, n3) == cudaSuccess &&
+              dalloc(&h->d_nbr_cnt, cnts_set(h)) == cudaSuccess && dalloc(&h->d_x, n3) == cudaSuccess &&
               dalloc(&h->d_v, n3) == cudaSuccess && dalloc(&h->d_A, n3) == cudaSuccess &&
               dalloc(&h->d_B, n3) == cudaSuccess && dalloc(&h->d_C, n3) == cudaSuccess &&
               dalloc(&h->d_D, n3) == cudaSuccess && dalloc(&h->d_G, n3) == cudaSuccess &&
@@ -2031,6 +2102,7 @@ bool shape_ok(const revsim_handle *h, int dir, int G, int m, int U) {
     if (!((G == 8 || G == 16 || G == 32) && m >= 1 && thr <= 512 && thr % 32 == 0 && U >= 1 && U <= 3 &&
           !(U == 3 && thr > 256)))
         return false;
+    if (half_eff(h) && thr > half_max_threads(dir == 0)) return false;
     return thr <= step_max_threads(h->prec == REVSIM_MIXED, dir == 0, U);
 }
 
@@ -2051,6 +2123,35 @@ int set_shape_dir(revsim_handle *h, int dir, int G, int m, int U) {
 }  // namespace
 
 extern "C" {
+
+int32_t revsim_set_pair_mode(revsim_handle *h, int32_t mode) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (mode != REVSIM_PAIRS_BOTH_SIDES && mode != REVSIM_PAIRS_HALF_SHELL)
+        return fail(h, REVSIM_ERR_BADARG, "bad pair evaluation mode");
+    if (mode == REVSIM_PAIRS_HALF_SHELL && !split_rows(h))
+        return fail(h, REVSIM_ERR_STATE, "half-shell pair evaluation needs mixed precision");
+    const bool want = mode == REVSIM_PAIRS_HALF_SHELL;
+    if (want == h->half_req) return REVSIM_OK;
+    h->half_req = want;
+    h->gen++;
+    h->fwd_valid = false;
+    // the half-shell reverse kernel allows fewer threads per CTA: shrink a shape beyond it
+    for (int dir = 0; dir < 2; dir++) {
+        revsim_handle::Shape &sh = h->shp[dir];
+        if (shape_ok(h, dir, sh.G, sh.mpc, sh.U)) continue;
+        int m = sh.mpc;
+        while (m > 1 && !shape_ok(h, dir, sh.G, m, 1)) m--;
+        if (int rc = set_shape_dir(h, dir, sh.G, m, 1)) return rc;
+    }
+    return REVSIM_OK;
+}
+
+int32_t revsim_get_pair_mode(const revsim_handle *h, int32_t *requested, int32_t *active) {
+    if (!h) return REVSIM_ERR_BADARG;
+    if (requested) *requested = h->half_req ? REVSIM_PAIRS_HALF_SHELL : REVSIM_PAIRS_BOTH_SIDES;
+    if (active) *active = half_eff(h) ? REVSIM_PAIRS_HALF_SHELL : REVSIM_PAIRS_BOTH_SIDES;
+    return REVSIM_OK;
+}
 
 // Lanes per molecule are one setting for both step kernels: a lane's share of a neighbour
 // row and the butterfly that sums the lanes depend on it, so forward and reverse forces are

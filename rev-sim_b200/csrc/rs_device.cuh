@@ -18,6 +18,7 @@ constexpr int ST_NLIST_OVERFLOW = 1;
 constexpr int ST_NAN = 2;
 constexpr int ST_GEOMETRY = 4;
 constexpr int ST_CELL_OVERFLOW = 8;
+constexpr int ST_ROW_ASYM = 64;   // half-shell split: a row member whose row lacks the owner
 
 // ---------------------------------------------------------------- launch chaining
 // Programmatic dependent launch of consecutive step kernels: a kernel launched with

@@ -99,6 +99,13 @@ constexpr int step_nreg(bool fp32, bool rev, int U) {
 constexpr int step_max_threads(bool fp32, bool rev, int U) {
     return 32 * (65536 / (32 * ((step_nreg(fp32, rev, U) + 7) / 8 * 8)));
 }
+// Half-shell pair kernels (k_water_half): forward 128, reverse 184 registers (at most 352
+// threads per CTA in reverse).
+#ifndef RS_NREG_HALF_REV
+#define RS_NREG_HALF_REV 184
+#endif
+constexpr int half_nreg(bool rev) { return rev ? RS_NREG_HALF_REV : RS_NREG_F_FWD; }
+constexpr int half_max_threads(bool rev) { return 32 * (65536 / (32 * ((half_nreg(rev) + 7) / 8 * 8))); }
 
 // Everything the step kernels read or write.
 struct StepArgs {
@@ -123,7 +130,21 @@ struct StepArgs {
     const double *noise_cur, *noise_next;
     int mode;
     int exact;         // 1: the exactly reversible integrator (grid increments, rs_device.cuh)
+    // Half-shell pair evaluation (FP32 kernels, rs_half.cu): each unordered molecule pair is
+    // evaluated once, by its owner, which writes the partner's share into a slot; a second
+    // kernel per step sums every molecule's own partial and its incoming slots in row order.
+    const uint32_t *split;   // [M * cap]: owned entries from the front, incoming slots from the back
+    const int *cnt_own, *cnt_inc;   // [M]
+    float4 *slot_f;    // [M * cap * 3]: per owned entry and partner atom (F_x, F_y, F_z, G_x)
+    float2 *slot_g;    // [M * cap * 3]: (G_y, G_z)
+    float *own;        // [M * 36]: own forces, own VJP, bonded forces, bonded VJP (9 each)
 };
+
+// Owner of an unordered molecule pair {I, J}: I when I + J is odd and I < J, or I + J is even
+// and I > J -- every molecule owns about half of its row whatever the index order.
+__host__ __device__ __forceinline__ bool half_owns(int I, int J) {
+    return ((I ^ J) & 1) ? I < J : I > J;
+}
 
 enum StepMode {
     MODE_FORCES_ONLY = 1,   // write F_out (and G / part in reverse), no integration
@@ -149,6 +170,10 @@ struct NlistArgs {
     int *status;
     int *max_cnt;      // [0] running maximum of the row counts; [1] this build's count of
                        // molecules with an O-H distance above sqrt(rnear2)
+    // Half-shell split of the rows (null: none): split, cnt_own, cnt_inc as in StepArgs;
+    // ownpos [M * cap] scratch (compact owned index of each owned row entry).
+    uint32_t *split;
+    int *cnt_own, *cnt_inc, *ownpos;
 };
 
 struct RdfArgs {
@@ -178,6 +203,12 @@ cudaError_t launch_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap
                                 int nmol, int32_t *pairs, unsigned long long *count,
                                 long long max_pairs, cudaStream_t st);
 
+// Half-shell step (two kernels, FP32, one image per molecule pair): rs_half.cu.
+cudaError_t launch_half(bool rev, int form, int G, int n_blk, int threads, const StepArgs &a,
+                        const NbConsts<float> &nb, const BondConsts &bc, cudaStream_t st);
+template <typename R, int FORM>
+cudaError_t launch_half_form(bool rev, int G, int n_blk, int threads, const StepArgs &a,
+                             const NbConsts<R> &nb, const BondConsts &bc, cudaStream_t st);
 // Fused step kernels: lanes per molecule G (8/16/32), entries per iteration unroll (1/2),
 // shift = one periodic image per molecule pair (valid when every box side exceeds
 // 2 (cutoff + 2 * max O-H distance)).

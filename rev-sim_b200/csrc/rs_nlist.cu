@@ -106,7 +106,9 @@ __global__ void k_cell_sort(NlistArgs a) {
 // within `band` of the cutoff are decided by the exact FP64 Molly arithmetic (dist2_fp64),
 // so the set is bit-identical to the all-FP64 test.  Entries are appended in candidate order.
 //
-// Periodic images.  The FP64 test takes each atom pair's own minimum image.  When every O-H
+// Periodic images.  The FP64 test takes each atom pair's own minimum image.  The FP32 test
+// sees whole molecules (each H placed at its O plus the O-H minimum image, as the step
+// kernels' gather buffer holds them; the state wraps every atom on its own).  When every O-H
 // distance is at most r_near (counted by k_cell_count) and the box side L exceeds
 // 2 (rc_nl + 2 r_near) + 0.02 nm, the FP32 test shifts all three atoms of the candidate by
 // the image of the O-O vector instead: an atom pair whose own image differs has a component
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                 s_idx[k] = J;
                 const double *xj = a.x + 9 * (size_t)J;
 #pragma unroll
-                for (int u = 0; u < 9; u++) s_c[u * kRowChunk + k] = (float)xj[u];
+                for (int u = 0; u < 9; u++) s_c[u * kRowChunk + k] = (float)gather_coord(xj[u % 3], xj[u], u >= 3, Ld);
             }
             __syncthreads();
 #pragma unroll 1
@@ -204,7 +206,8 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                 const int kself = s_off[tc] + hi - c0;   // the home molecule in this chunk
                 float xi[9];
 #pragma unroll
-                for (int u = 0; u < 9; u++) xi[u] = (float)a.x[9 * (size_t)I + u];
+                for (int u = 0; u < 9; u++)
+                    xi[u] = (float)gather_coord(a.x[9 * (size_t)I + u % 3], a.x[9 * (size_t)I + u], u >= 3, Ld);
                 uint32_t *row = a.nbr + (size_t)I * a.cap;
                 // in batches of kCandBatch candidates: the O-O test first, compacting the
                 // passing candidates (in order) for the nine-pair test, so the lanes of the
@@ -293,6 +296,102 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
     }
 }
 
+// Half-shell split of the rows.  Row order is the candidate order of k_rows: by the
+// neighbourhood position t of the neighbour's cell relative to the row owner's cell (the
+// canonical cell index when the grid has fewer than five cells a side), then by molecule
+// index.  The key (t << 23) | K is therefore increasing along every row.
+__device__ __forceinline__ uint32_t row_key(const NlistArgs &a, int nc, int off0, int cx, int cy, int cz,
+                                            int K) {
+    const int cl = a.cell_of_mol[K] - off0;
+    const int kx = cl % nc, ky = (cl / nc) % nc, kz = cl / (nc * nc);
+    int t;
+    if (nc >= 5) {
+        const int dx = (kx - cx + 2 + nc) % nc, dy = (ky - cy + 2 + nc) % nc, dz = (kz - cz + 2 + nc) % nc;
+        t = (dz * 5 + dy) * 5 + dx;
+    } else {
+        t = cl;
+    }
+    return ((uint32_t)t << 23) | (uint32_t)K;
+}
+
+// Owned entries of each row, compacted in row order to the front of its split row; the
+// compact index of each owned entry in ownpos.  One warp per row.
+__global__ void k_split_own(NlistArgs a) {
+    const int I = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (I >= a.M) return;
+    const int n = min(a.nbr_cnt[I], a.cap);
+    const uint32_t *row = a.nbr + (size_t)I * a.cap;
+    uint32_t *out = a.split + (size_t)I * a.cap;
+    int *op = a.ownpos + (size_t)I * a.cap;
+    int c = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int e = base + lane;
+        uint32_t ent = 0;
+        bool own = false;
+        if (e < n) {
+            ent = row[e];
+            own = half_owns(I, (int)(ent & 0x7FFFFFu));
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, own);
+        if (own) {
+            const int p = c + __popc(bal & ((1u << lane) - 1u));
+            out[p] = ent;
+            op[e] = p;
+        }
+        c += __popc(bal);
+    }
+    if (lane == 0) a.cnt_own[I] = c;
+}
+
+// Incoming slots of each row: for every entry I that owns the pair, the slot I * cap + p'
+// where I's owned entry of this molecule sits at compact index p' (found by binary search
+// on the row key in I's row).  Written from the back of the split row, in row order, so
+// that the owned entries (front) and the incoming slots (back) share the row's capacity.
+__global__ void k_split_inc(NlistArgs a) {
+    const int J = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (J >= a.M) return;
+    const int n = min(a.nbr_cnt[J], a.cap);
+    const uint32_t *row = a.nbr + (size_t)J * a.cap;
+    uint32_t *out = a.split + (size_t)J * a.cap + (a.cap - 1);
+    const int r = a.mol_rep[J];
+    const int nc = a.rep_nc[r], off0 = a.rep_cell_off[r];
+    int c = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int e = base + lane;
+        bool inc = false;
+        uint32_t slot = 0;
+        if (e < n) {
+            const int I = (int)(row[e] & 0x7FFFFFu);
+            if (!half_owns(J, I)) {
+                inc = true;
+                const int cl = a.cell_of_mol[I] - off0;
+                const int cx = cl % nc, cy = (cl / nc) % nc, cz = cl / (nc * nc);
+                const uint32_t target = row_key(a, nc, off0, cx, cy, cz, J);
+                const uint32_t *ri = a.nbr + (size_t)I * a.cap;
+                const int ni = min(a.nbr_cnt[I], a.cap);
+                int lo = 0, hi = ni;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (row_key(a, nc, off0, cx, cy, cz, (int)(ri[mid] & 0x7FFFFFu)) < target) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < ni && (int)(ri[lo] & 0x7FFFFFu) == J) {
+                    slot = (uint32_t)((size_t)I * a.cap + a.ownpos[(size_t)I * a.cap + lo]);
+                } else {
+                    atomicOr(a.status, ST_ROW_ASYM);
+                    slot = (uint32_t)((size_t)I * a.cap);   // a valid slot; the status fails the call
+                }
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, inc);
+        if (inc) out[-(c + __popc(bal & ((1u << lane) - 1u)))] = slot;
+        c += __popc(bal);
+    }
+    if (lane == 0) a.cnt_inc[J] = c;
+}
+
 // Atom pairs (i < j, replica-local indices) of one replica's rows.
 __global__ void k_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap, int mol0,
                                int nmol, int32_t *pairs, unsigned long long *count,
@@ -335,6 +434,11 @@ cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
     const int per_cell = (a.M + a.n_cells - 1) / a.n_cells;
     const int split = std::min(8, std::max(1, (2 * per_cell + 7) / 8));
     k_rows<<<dim3(a.n_cells, split), 256, smem, st>>>(a);
+    if (a.split) {
+        const int wb = (a.M + 7) / 8;   // one warp per row, eight per CTA
+        k_split_own<<<wb, 256, 0, st>>>(a);
+        k_split_inc<<<wb, 256, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 

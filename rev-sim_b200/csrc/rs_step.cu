@@ -178,6 +178,19 @@ cudaError_t launch_step(bool rev, int form, int G, int unroll, bool shift, int n
     return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_half(bool rev, int form, int G, int n_blk, int threads, const StepArgs &a,
+                        const NbConsts<float> &nb, const BondConsts &bc, cudaStream_t st) {
+    switch (form) {
+        case F_LJ: return launch_half_form<float, F_LJ>(rev, G, n_blk, threads, a, nb, bc, st);
+        case F_DEXP: return launch_half_form<float, F_DEXP>(rev, G, n_blk, threads, a, nb, bc, st);
+        case F_BUCK: return launch_half_form<float, F_BUCK>(rev, G, n_blk, threads, a, nb, bc, st);
+        case F_LJSC: return launch_half_form<float, F_LJSC>(rev, G, n_blk, threads, a, nb, bc, st);
+        case F_BUFF: return launch_half_form<float, F_BUFF>(rev, G, n_blk, threads, a, nb, bc, st);
+        case F_LJ_MLP: return launch_half_form<float, F_LJ_MLP>(rev, G, n_blk, threads, a, nb, bc, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
 template cudaError_t launch_step<float>(bool, int, int, int, bool, int, int, const StepArgs &,
                                         const NbConsts<float> &, const BondConsts &, cudaStream_t);
 template cudaError_t launch_step<double>(bool, int, int, int, bool, int, int, const StepArgs &,

@@ -38,6 +38,7 @@ EXPORTS = [
     "revsim_barostat_state", "revsim_set_box", "revsim_probe_fp64_tflops",
     "revsim_forward_noise", "revsim_reverse_noise", "revsim_set_graph_mode", "revsim_graph_stats",
     "revsim_set_mlp_precision", "revsim_mlp_eval", "revsim_set_integrator",
+    "revsim_set_pair_mode", "revsim_get_pair_mode",
 ]
 
 # Every symbol include/revsim_sw.h declares.
@@ -186,6 +187,8 @@ def load(path=LIB_PATH):
         "revsim_forward_noise": (i32, [vp, pd, d, i32, i32, d, i32, pd]),
         "revsim_set_graph_mode": (i32, [vp, i32]),
         "revsim_set_integrator": (i32, [vp, i32]),
+        "revsim_set_pair_mode": (i32, [vp, i32]),
+        "revsim_get_pair_mode": (i32, [vp, pi32, pi32]),
         "revsim_set_mlp_precision": (i32, [vp, i32]),
         "revsim_mlp_eval": (i32, [vp, i32, pd, pd, pd, pd]),
         "revsim_graph_stats": (i32, [vp, pi64, pi64]),

@@ -316,6 +316,20 @@ class Engine:
             self._check(self._L.revsim_mlp_eval(self._h, r.shape[1], f64p(r), None, None, ctypes.byref(ms)))
         return ms.value
 
+    def set_pair_mode(self, mode="both_sides"):
+        """"both_sides" (each molecule's lanes evaluate its whole row) or "half_shell" (each
+        molecule pair evaluated once, the partner's share gathered by a second kernel; mixed
+        precision only), revsim_set_pair_mode."""
+        code = {"both_sides": 0, "half_shell": 1}[mode]
+        self._check(self._L.revsim_set_pair_mode(self._h, code))
+
+    def pair_mode(self):
+        """(requested, in effect) pair evaluation modes, revsim_get_pair_mode."""
+        req, act = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._L.revsim_get_pair_mode(self._h, ctypes.byref(req), ctypes.byref(act)))
+        names = {0: "both_sides", 1: "half_shell"}
+        return names[req.value], names[act.value]
+
     def set_integrator(self, mode="reference"):
         """"reference" (the reference's FP64 step arithmetic) or "exact" (grid increments: with
         gamma = 0 the reverse pass rebuilds the trajectory bit for bit), revsim_set_integrator."""
