@@ -1792,6 +1792,9 @@ int upload_noise(revsim_handle *h, const uint64_t *seeds, const double *noise, i
 template <typename F>
 int run_graphed(revsim_handle *h, int dir, std::vector<double> key, F &&pass) {
     if (!h->graph_on || h->ktime || h->baro_on || h->ev_on) return pass();
+    // nothing may be allocated while the stream is capturing
+    if (half_eff(h))
+        if (int rc = ensure_half(h)) return rc;
     key.push_back((double)h->gen);
     key.push_back((double)g_alloc_gen.load());
     revsim_handle::GraphCache &c = h->gc[dir];

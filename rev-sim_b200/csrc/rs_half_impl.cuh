@@ -239,22 +239,21 @@ __global__ void __maxnreg__((half_nreg(REV))) k_water_half(StepArgs a, NbConsts<
             const uint32_t ex = __ldg(row + e);
             const uint32_t ey = e2 < cnt ? __ldg(row + e2) : 0u;
             const int Jx = (int)(ex & 0x7FFFFFu), Jy = (int)(ey & 0x7FFFFFu);
-            V4 pbx[3], pby[3], wbx[3], wby[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                pbx[k] = pos[3 * Jx + k];
-                pby[k] = pos[3 * Jy + k];
-                if (REV) {
-                    wbx[k] = wgt[3 * Jx + k];
-                    wby[k] = wgt[3 * Jy + k];
-                }
-            }
-            const P sh[3] = {pk(image_shift(xsub(pbx[0].x, pa[0].x), L, hL), image_shift(xsub(pby[0].x, pa[0].x), L, hL)),
-                             pk(image_shift(xsub(pbx[0].y, pa[0].y), L, hL), image_shift(xsub(pby[0].y, pa[0].y), L, hL)),
-                             pk(image_shift(xsub(pbx[0].z, pa[0].z), L, hL), image_shift(xsub(pby[0].z, pa[0].z), L, hL))};
+            // the partner atoms' coordinates, weights and coefficients are loaded per partner
+            // atom (RS_HCOL), the O coordinates first for the image shift
+            const V4 pox = pos[3 * Jx], poy = pos[3 * Jy];
+            const P sh[3] = {pk(image_shift(xsub(pox.x, pa[0].x), L, hL), image_shift(xsub(poy.x, pa[0].x), L, hL)),
+                             pk(image_shift(xsub(pox.y, pa[0].y), L, hL), image_shift(xsub(poy.y, pa[0].y), L, hL)),
+                             pk(image_shift(xsub(pox.z, pa[0].z), L, hL), image_shift(xsub(poy.z, pa[0].z), L, hL))};
             const uint32_t mx = ex >> 23, my = ey >> 23;
 #define RS_HCOL(KB)                                                                                    \
     {                                                                                                  \
+        const V4 pbx = KB == 0 ? pox : pos[3 * Jx + KB], pby = KB == 0 ? poy : pos[3 * Jy + KB];       \
+        V4 wbx = {}, wby = {};                                                                         \
+        if (REV) {                                                                                     \
+            wbx = wgt[3 * Jx + KB];                                                                    \
+            wby = wgt[3 * Jy + KB];                                                                    \
+        }                                                                                              \
         P pf[3] = {pk1(R(0)), pk1(R(0)), pk1(R(0))}, pg[3] = {pk1(R(0)), pk1(R(0)), pk1(R(0))};        \
         R cbx[3] = {R(0), R(0), R(0)}, cby[3] = {R(0), R(0), R(0)};                                    \
         if (REV) {                                                                                     \
@@ -264,7 +263,7 @@ __global__ void __maxnreg__((half_nreg(REV))) k_water_half(StepArgs a, NbConsts<
                 cby[u] = (R)__dmul_rn(a.A[9 * (size_t)Jy + 3 * KB + u], sc);                           \
             }                                                                                          \
         }                                                                                              \
-        half_col<FORM, REV, KB>(mx, my, pa, pbx[KB], pby[KB], wa, wbx[KB], wby[KB], ca, cbx, cby, sh, L, \
+        half_col<FORM, REV, KB>(mx, my, pa, pbx, pby, wa, wbx, wby, ca, cbx, cby, sh, L,                \
                                 invL, nb, f2, g2, th2, pf, pg, madj);                                  \
         sf[3 * e + KB] = make_float4(pf[0].x, pf[1].x, pf[2].x, REV ? pg[0].x : R(0));                 \
         if (REV) sg[3 * e + KB] = make_float2(pg[1].x, pg[2].x);                                       \

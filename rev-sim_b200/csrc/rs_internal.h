@@ -94,18 +94,18 @@ constexpr int step_nreg(bool fp32, bool rev, int U) {
     return !fp32 ? (U == 3 ? 255 : 128)
                  : (!rev ? RS_NREG_F_FWD : (U == 3 ? RS_NREG_F_REV3 : (U == 1 ? RS_NREG_F_REV1 : RS_NREG_F_REV2)));
 }
-// The largest CTA such a kernel can be launched with: whole warps of the 65,536 registers of
-// an SM, a thread's registers allocated in units of 8.
-constexpr int step_max_threads(bool fp32, bool rev, int U) {
-    return 32 * (65536 / (32 * ((step_nreg(fp32, rev, U) + 7) / 8 * 8)));
-}
-// Half-shell pair kernels (k_water_half): forward 128, reverse 184 registers (at most 352
-// threads per CTA in reverse).
+// The largest CTA a kernel of nreg registers per thread can be launched with: a CTA's warps
+// are spread over the SM's four schedulers, each with a quarter (16,384) of the registers, a
+// thread's registers allocated in units of 8.  128 registers: 512 threads; 168: 384; 200 or
+// 255: 256.
+constexpr int max_threads_for(int nreg) { return 32 * 4 * (16384 / (32 * ((nreg + 7) / 8 * 8))); }
+constexpr int step_max_threads(bool fp32, bool rev, int U) { return max_threads_for(step_nreg(fp32, rev, U)); }
+// Half-shell pair kernels (k_water_half): forward 128, reverse 168 registers.
 #ifndef RS_NREG_HALF_REV
-#define RS_NREG_HALF_REV 184
+#define RS_NREG_HALF_REV 168
 #endif
 constexpr int half_nreg(bool rev) { return rev ? RS_NREG_HALF_REV : RS_NREG_F_FWD; }
-constexpr int half_max_threads(bool rev) { return 32 * (65536 / (32 * ((half_nreg(rev) + 7) / 8 * 8))); }
+constexpr int half_max_threads(bool rev) { return max_threads_for(half_nreg(rev)); }
 
 // Everything the step kernels read or write.
 struct StepArgs {
