@@ -95,9 +95,9 @@ __global__ void k_cell_sort(NlistArgs a) {
     a.cell_sorted[s + rank] = I;
 }
 
-// Rows of the molecules of one home cell (up to eight CTAs of eight warps per cell, so that
-// a warp has at most one home molecule in all but the fullest cells: the build's time is
-// that of its slowest warp).  The CTA stages the neighbourhood -- the members of the
+// Rows of the molecules of one home cell (up to eight CTAs of sixteen warps per cell, so
+// that a warp has at most one home molecule in all but the fullest cells: the build's time
+// is that of its slowest warp).  The CTA stages the neighbourhood -- the members of the
 // surrounding cells, in the canonical cell order and index order within a cell -- with all
 // three atoms in FP32 in shared memory, in chunks of up to kRowChunk molecules.  Each warp
 // takes one home molecule at a time: an FP32 O-O test against the candidate radius (with a
@@ -108,7 +108,8 @@ __global__ void k_cell_sort(NlistArgs a) {
 //
 // Periodic images.  The FP64 test takes each atom pair's own minimum image.  The FP32 test
 // sees whole molecules (each H placed at its O plus the O-H minimum image, as the step
-// kernels' gather buffer holds them; the state wraps every atom on its own).  When every O-H
+// kernels' gather buffer holds them; the state wraps every atom on its own): the home
+// molecule made whole in FP64, the staged candidates in FP32 (within 1e-6 nm of that).  When every O-H
 // distance is at most r_near (counted by k_cell_count) and the box side L exceeds
 // 2 (rc_nl + 2 r_near) + 0.02 nm, the FP32 test shifts all three atoms of the candidate by
 // the image of the O-O vector instead: an atom pair whose own image differs has a component
@@ -116,18 +117,18 @@ __global__ void k_cell_sort(NlistArgs a) {
 // the pair is outside either way; every other pair gets the same vector up to FP32 rounding
 // (|d^2 error| < 5e-6 L/4.5 nm, a quarter of `band`).  The rows are the same bits with
 // either form; the shifted form saves the 27 per-component image selections.
-constexpr int kRowChunk = 1024;
+constexpr int kRowChunk = 2048;
 constexpr int kCandBatch = 256;
 
 __device__ __forceinline__ float mi_f(float d, float L, float hL) {
     return d > hL ? d - L : (d < -hL ? d + L : d);
 }
 
-__global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
+__global__ void __launch_bounds__(512) k_rows(NlistArgs a) {
     extern __shared__ float s_c[];              // [9][kRowChunk] coordinates
     int *s_idx = (int *)(s_c + 9 * kRowChunk);   // [kRowChunk] molecule ids
     __shared__ int s_off[126], s_start[125];
-    __shared__ int s_kbuf[8 * kCandBatch];       // per warp: candidates passing the O-O test
+    __shared__ int s_kbuf[16 * kCandBatch];      // per warp: candidates passing the O-O test
     const int c_home = blockIdx.x;
     const int r = a.cell_rep[c_home];
     const int nc = a.rep_nc[r];
@@ -195,7 +196,13 @@ __global__ void __launch_bounds__(256) k_rows(NlistArgs a) {
                 s_idx[k] = J;
                 const double *xj = a.x + 9 * (size_t)J;
 #pragma unroll
-                for (int u = 0; u < 9; u++) s_c[u * kRowChunk + k] = (float)gather_coord(xj[u % 3], xj[u], u >= 3, Ld);
+                for (int u = 0; u < 3; u++) {
+                    // whole molecule in FP32: H = O + minimum image of (H - O)
+                    const float o = (float)xj[u];
+                    s_c[u * kRowChunk + k] = o;
+                    s_c[(3 + u) * kRowChunk + k] = o + mi_f((float)xj[3 + u] - o, L, hL);
+                    s_c[(6 + u) * kRowChunk + k] = o + mi_f((float)xj[6 + u] - o, L, hL);
+                }
             }
             __syncthreads();
 #pragma unroll 1
@@ -428,12 +435,12 @@ cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
     k_cell_sort<<<b, t, 0, st>>>(a);
     const size_t smem = (9 * sizeof(float) + sizeof(int)) * kRowChunk;
     cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // home molecules per cell over the 8 warps of a CTA: split a cell over up to 8 CTAs,
+    // home molecules per cell over the 16 warps of a CTA: split a cell over up to 8 CTAs,
     // with warps for twice the mean count, so that the fullest cells of a Poisson-like
     // occupancy still give a warp one home molecule (CTAs beyond a cell's count exit at once)
     const int per_cell = (a.M + a.n_cells - 1) / a.n_cells;
-    const int split = std::min(8, std::max(1, (2 * per_cell + 7) / 8));
-    k_rows<<<dim3(a.n_cells, split), 256, smem, st>>>(a);
+    const int split = std::min(8, std::max(1, (2 * per_cell + 15) / 16));
+    k_rows<<<dim3(a.n_cells, split), 512, smem, st>>>(a);
     if (a.split) {
         const int wb = (a.M + 7) / 8;   // one warp per row, eight per CTA
         k_split_own<<<wb, 256, 0, st>>>(a);
