@@ -223,18 +223,23 @@ __global__ void __launch_bounds__(512) k_rows(NlistArgs a) {
                 for (int b0 = 0; b0 < cn; b0 += kCandBatch) {
                     const int b1 = min(b0 + kCandBatch, cn);
                     int nk = 0;
-                    for (int base = b0; base < b1; base += 32) {
-                        const int k = base + lane;
-                        bool pass = false;
-                        if (k < b1) {
-                            const float ox = mi_f(s_c[k] - xi[0], L, hL);
-                            const float oy = mi_f(s_c[kRowChunk + k] - xi[1], L, hL);
-                            const float oz = mi_f(s_c[2 * kRowChunk + k] - xi[2], L, hL);
-                            pass = k != kself && ox * ox + oy * oy + oz * oz <= rcand2;
-                        }
-                        const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                        if (pass) s_k[nk + __popc(bal & ((1u << lane) - 1u))] = k;
-                        nk += __popc(bal);
+                    auto oo_pass = [&](int k) {
+                        if (k >= b1) return false;
+                        const float ox = mi_f(s_c[k] - xi[0], L, hL);
+                        const float oy = mi_f(s_c[kRowChunk + k] - xi[1], L, hL);
+                        const float oz = mi_f(s_c[2 * kRowChunk + k] - xi[2], L, hL);
+                        return k != kself && ox * ox + oy * oy + oz * oz <= rcand2;
+                    };
+                    // two candidates per lane per step (independent chains), compacted in order
+                    const unsigned below = (1u << lane) - 1u;
+                    for (int base = b0; base < b1; base += 64) {
+                        const bool p0 = oo_pass(base + lane), p1 = oo_pass(base + 32 + lane);
+                        const unsigned bal0 = __ballot_sync(0xffffffffu, p0);
+                        const unsigned bal1 = __ballot_sync(0xffffffffu, p1);
+                        if (p0) s_k[nk + __popc(bal0 & below)] = base + lane;
+                        nk += __popc(bal0);
+                        if (p1) s_k[nk + __popc(bal1 & below)] = base + 32 + lane;
+                        nk += __popc(bal1);
                     }
                     __syncwarp();
                     for (int base = 0; base < nk; base += 32) {
@@ -243,7 +248,7 @@ __global__ void __launch_bounds__(512) k_rows(NlistArgs a) {
                         if (idx < nk) {
                             const int k = s_k[idx];
                             const int J = s_idx[k];
-                            uint32_t mask = 0;
+                            uint32_t mask = 0, near = 0;
                             float cb[9];
                             if (one_image) {
 #pragma unroll
@@ -270,12 +275,18 @@ __global__ void __launch_bounds__(512) k_rows(NlistArgs a) {
                                         dz = mi_f(s_c[(3 * kb + 2) * kRowChunk + k] - xi[3 * ka + 2], L, hL);
                                     }
                                     const float d2 = dx * dx + dy * dy + dz * dz;
-                                    bool in = d2 < rc2f;
-                                    if (fabsf(d2 - rc2f) <= band)
-                                        in = dist2_fp64(a.x + 9 * (size_t)I + 3 * ka,
-                                                        a.x + 9 * (size_t)J + 3 * kb, Ld) <= a.rc_nl2;
-                                    if (in) mask |= 1u << (3 * ka + kb);
+                                    mask |= (d2 < rc2f ? 1u : 0u) << (3 * ka + kb);
+                                    near |= (fabsf(d2 - rc2f) <= band ? 1u : 0u) << (3 * ka + kb);
                                 }
+                            // the nine tests above are straight-line code; the rare pairs
+                            // within `band` of the cutoff are decided here in FP64
+                            while (near) {
+                                const int b = __ffs(near) - 1;
+                                near &= near - 1u;
+                                const bool in = dist2_fp64(a.x + 9 * (size_t)I + 3 * (b / 3),
+                                                           a.x + 9 * (size_t)J + 3 * (b % 3), Ld) <= a.rc_nl2;
+                                mask = in ? (mask | (1u << b)) : (mask & ~(1u << b));
+                            }
                             if (mask) ent = (uint32_t)J | (mask << 23);
                         }
                         const unsigned bal = __ballot_sync(0xffffffffu, ent != 0);
