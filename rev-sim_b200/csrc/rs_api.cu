@@ -537,6 +537,7 @@ int build_nlist(revsim_handle *h, const double *xsrc, uint32_t *nbr = nullptr, i
     a.rcand2 = rcand * rcand;
     a.rext2 = kRext * kRext;
     a.rnear2 = kRnear * kRnear;
+    a.rcand_near2 = (h->rc_nl + 2 * kRnear) * (h->rc_nl + 2 * kRnear);
     a.shift_box = 2 * (h->rc_nl + 2 * kRnear) + 0.02;
     a.status = h->d_status;
     a.max_cnt = h->d_maxcnt;

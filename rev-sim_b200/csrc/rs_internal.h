@@ -163,6 +163,7 @@ struct NlistArgs {
     int cap;
     double rc_nl2;     // neighbour-list cutoff^2
     double rcand2;     // O-O candidate radius^2
+    double rcand_near2;   // the same with the tighter O-H bound rnear (every O-H within it)
     double rext2;      // max intramolecular O-H distance^2
     double rnear2;     // O-H distance^2 bound under which one image shift per molecule pair holds
     double shift_box;  // boxes above this side may use one image shift per molecule pair

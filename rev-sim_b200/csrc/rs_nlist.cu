@@ -169,7 +169,8 @@ __global__ void __launch_bounds__(512) k_rows(NlistArgs a) {
     const int lane = threadIdx.x & 31;
     const int nwarp = (int)gridDim.y * (int)(blockDim.x >> 5);               // warps per home cell
     const int warp = (int)blockIdx.y * (int)(blockDim.x >> 5) + (threadIdx.x >> 5);
-    const float rcand2 = (float)a.rcand2 + 1e-3f;
+    // an atom pair within rc_nl needs an O-O distance within rc_nl + 2 (largest O-H)
+    const float rcand2 = (float)(a.max_cnt[1] == 0 ? a.rcand_near2 : a.rcand2) + 1e-3f;
     const float rc2f = (float)a.rc_nl2;
     const float band = a.band;
     // per home molecule state kept across chunks (a warp owns the same molecules in
