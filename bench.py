@@ -1655,6 +1655,10 @@ def run_ours_diamond(a):
     eng.set_state(x0, v0)
     eng.set_kernel_timing(True)
     gradient()
+    # the reverse pass ends at the start state, rebuilt over the first loss block
+    recon = {a.precision: recon_error(eng.get_state()[0], x0, np.repeat(np.asarray(boxes), n)),
+             "steps_reconstructed": NL, "gamma_per_ps": SW_GAMMA,
+             "integrator": "the reference's step arithmetic"}
     rt_ms, rt_n = eng.kernel_time(0)
     ft_ms, ft_n = eng.kernel_time(1)
     rg_ms, rg_n = eng.kernel_time(2)
@@ -1744,7 +1748,7 @@ def run_ours_diamond(a):
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-               "clocks": clocks,
+               "clocks": clocks, "recon": recon,
                "loss": {"forward": float(lf.mean()), "reverse": float(lr.mean())}}
         out.update(extra)
         print(json.dumps(out), flush=True)
@@ -1775,7 +1779,7 @@ def mlp_config(a, extra=None):
                      "reference's scaled Adam), MLP lr 1e-3; target: the O-O RDF of a teacher "
                      "(default LJ + a fixed MLP correction, seeded init + N(0, 0.05)), outside "
                      "the classical family",
-         "mlp_precision": a.mlp_precision,
+         "mlp_precision": a.mlp_precision, "integrator": a.integrator,
          "precision": a.precision, "l2": "flushed (256 MiB write) between timed steps"}
     if extra:
         c.update(extra)
@@ -1799,7 +1803,7 @@ def run_ours_mlp(a):
     a.n_mol, a.box, a.form = 895, 3.0, "lj"
     x0, v0, p, target = prepare(a, local, a.equil_ps)
     theta0 = np.concatenate([p, mlp.init_params(3)])
-    eng = Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=True)
+    eng = integ(Engine(895, 3.0, inter_type="lj", precision=a.precision, device=local, mlp=True), a)
     eng.set_mlp_precision(a.mlp_precision)
     eng.set_params(theta0)
     eng.set_loss([oo_l2_term(target)])
@@ -1853,6 +1857,8 @@ def run_ours_mlp(a):
     eng.set_kernel_timing(False)
     launch_ms = kt_ms / max(kt_n, 1)
     xs, _ = eng.get_state()
+    recon = {a.precision: recon_error(xs, x0, 3.0), "steps_reconstructed": 1000,
+             "integrator": a.integrator}
     pairs = eng.neighbor_pairs(0)
     ipairs, _ = count_ipairs(xs, 3.0, pairs)
     flops_launch = (FLOPS_REV_IPAIR + MLP_FLOPS_REV_EXTRA) * ipairs
@@ -1970,7 +1976,7 @@ def run_ours_mlp(a):
            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None,
            "clocks": clocks, "loss": {"forward": float(lf[0]), "reverse": float(lr[0])},
            "grad_rel_err_vs_fp64_first_100_steps": {"classical": err_cl, "mlp": err_mlp},
-           "training": train, "network_per_pair_vs_table": network,
+           "training": train, "network_per_pair_vs_table": network, "recon": recon,
            "e2e_note": "every timed gradient starts from host arrays (set_state), so value is "
                        "end to end"}
     if rank == 0:
@@ -2115,6 +2121,9 @@ def run_ours_replicas(a):
     eng.set_kernel_timing(False)
     launch_ms = kt_ms / max(kt_n, 1)
     xs, _ = eng.get_state()
+    # the reverse pass ends at the start state, rebuilt over the first 1,000-step block
+    recon = {a.precision: recon_error(xs, x0, np.repeat(np.asarray(boxes, dtype=np.float64), 3 * np.asarray(n_mol))),
+             "steps_reconstructed": 1000, "gamma_per_ps": 1.0, "integrator": a.integrator}
     ipairs = 0
     for r in range(R):
         sl = slice(int(3 * n_mol[:r].sum()), int(3 * n_mol[:r + 1].sum()))
@@ -2146,7 +2155,7 @@ def run_ours_replicas(a):
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": None, "clocks": clocks,
            "loss": {"forward_mean": float(lf.mean()), "reverse_mean": float(lr.mean())},
-           "mean_gradient": [float(t) for t in g],
+           "recon": recon, "mean_gradient": [float(t) for t in g],
            "e2e_note": "every timed gradient starts from host arrays (set_state), so value is end to end"}
     if rank == 0:
         print(json.dumps(out), flush=True)
