@@ -2006,8 +2006,11 @@ def replicas_config(a, n_mol, extra=None):
          "n_steps_loss": 1000, "n_steps_trunc": 1000, "dt_ps": 0.001, "gamma_per_ps": 1.0,
          "loss": "O-O smoothed RDF, 200 bins 0-1 nm, squared error vs the replica-mean RDF of a "
                  "sigma x1.02 / eps x0.95 run; per-replica gradients averaged",
-         "launch": "all replicas in one launch per step (per-CTA replica table); not captured "
-                   "in a CUDA graph (the step kernels are GPU-bound)",
+         "launch": "all replicas in one launch per step (per-CTA replica table), step launches "
+                   "chained (programmatic dependent launch); the CUDA-graph mode "
+                   "(revsim_set_graph_mode) is not used here: each step kernel runs ~0.6 ms, so "
+                   "the launch queue never drains",
+         "integrator": a.integrator,
          "precision": a.precision, "l2": "inputs larger than L2 are not guaranteed; flushed "
                                          "(256 MiB write) between timed steps"}
     if extra:
