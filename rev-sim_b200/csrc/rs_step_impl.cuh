@@ -792,14 +792,23 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                     entry2(ex, ey, pbx, wbx, pby, wby);
                 }
             } else {
+                // U entry pairs per lane per iteration: all their loads are issued first, and
+                // the next iteration's row entries are loaded one iteration ahead
+                constexpr int UP = U == 3 ? 1 : U;
+                uint32_t nx[UP], ny[UP];
+#pragma unroll
+                for (int q = 0; q < UP; q++) {
+                    nx[q] = ent_at(lane + 2 * q * G);
+                    ny[q] = ent_at(lane + (2 * q + 1) * G);
+                }
                 for (int e0 = lane; e0 < cnt; e0 += 2 * U * G) {
-                    // U entry pairs per lane per iteration: all their loads are issued first
-                    constexpr int UP = U == 3 ? 1 : U;
                     uint32_t ex[UP], ey[UP];
 #pragma unroll
                     for (int q = 0; q < UP; q++) {
-                        ex[q] = ent_at(e0 + 2 * q * G);
-                        ey[q] = ent_at(e0 + (2 * q + 1) * G);
+                        ex[q] = nx[q];
+                        ey[q] = ny[q];
+                        nx[q] = ent_at(e0 + 2 * U * G + 2 * q * G);
+                        ny[q] = ent_at(e0 + 2 * U * G + (2 * q + 1) * G);
                     }
                     V4 pbx[UP][3], wbx[UP][3], pby[UP][3], wby[UP][3];
 #pragma unroll
@@ -845,12 +854,19 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                     entry(ent, pbq, wbq);
                 }
             } else {
+                // U entries per lane per iteration: all their loads are issued first, and the
+                // next iteration's row entries are loaded one iteration ahead
+                constexpr int UE = U == 3 ? 1 : U;
+                uint32_t nxt[UE];
+#pragma unroll
+                for (int q = 0; q < UE; q++) nxt[q] = ent_at(lane + q * G);
                 for (int e0 = lane; e0 < cnt; e0 += U * G) {
-                    // U entries per lane per iteration: all their loads are issued first
-                    constexpr int UE = U == 3 ? 1 : U;
                     uint32_t ent[UE];
 #pragma unroll
-                    for (int q = 0; q < UE; q++) ent[q] = ent_at(e0 + q * G);
+                    for (int q = 0; q < UE; q++) {
+                        ent[q] = nxt[q];
+                        nxt[q] = ent_at(e0 + U * G + q * G);
+                    }
                     V4 pb[UE][3], wb[UE][3];
 #pragma unroll
                     for (int q = 0; q < UE; q++) fetch(ent[q], pb[q], wb[q]);
