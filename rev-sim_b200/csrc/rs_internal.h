@@ -100,6 +100,10 @@ constexpr int step_nreg(bool fp32, bool rev, int U) {
 // 255: 256.
 constexpr int max_threads_for(int nreg) { return 32 * 4 * (16384 / (32 * ((nreg + 7) / 8 * 8))); }
 constexpr int step_max_threads(bool fp32, bool rev, int U) { return max_threads_for(step_nreg(fp32, rev, U)); }
+// Row entries of the FP32 step kernels' neighbour loop are loaded this many iterations ahead.
+#ifndef RS_ROW_AHEAD
+#define RS_ROW_AHEAD 1
+#endif
 // Half-shell pair kernels (k_water_half): forward 128, reverse 168 registers.
 #ifndef RS_NREG_HALF_REV
 #define RS_NREG_HALF_REV 168

@@ -709,6 +709,15 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 for (int u = 0; u < 3; u++) ca[k][u] = (R)__dmul_rn(a.A[9 * (size_t)I + 3 * k + u], sc);
             }
         }
+        const uint32_t *__restrict__ row = a.nbr + (size_t)I * a.cap;
+        const int cnt = min(a.nbr_cnt[I], a.cap);
+        // padding entries (past the row end) read molecule 0 with an empty mask
+        auto ent_at = [&](int e) { return e < cnt ? __ldg(row + e) : 0u; };
+        // the lane's first row entries, loaded before the bonded terms so that their latency
+        // overlaps lane 0's bonded arithmetic (entries lane + q G, q < 4 covers every loop form)
+        uint32_t first[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) first[q] = ent_at(lane + q * G);
         if (lane == 0) {
             double xm[9];
 #pragma unroll
@@ -732,8 +741,6 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
 #pragma unroll
             for (int q = 0; q < 4; q++) s_bond[18 + q] = tb[q];
         }
-        const uint32_t *__restrict__ row = a.nbr + (size_t)I * a.cap;
-        const int cnt = min(a.nbr_cnt[I], a.cap);
         const R hL = xmul(L, R(0.5));
         auto fetch = [&](uint32_t ent, V4 pbq[3], V4 wbq[3]) {
             const int J = (int)(ent & 0x7FFFFFu);
@@ -743,8 +750,6 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 if (REV) wbq[k] = wgt[3 * J + k];
             }
         };
-        // padding entries (past the row end) read molecule 0 with an empty mask
-        auto ent_at = [&](int e) { return e < cnt ? __ldg(row + e) : 0u; };
         if constexpr (PACKED) {
             // Entries e and e + G of the row as one pair (halves x and y); a lane takes the
             // pairs starting at lane, lane + 2G, lane + 4G, ...
@@ -767,7 +772,7 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
             if (U == 3) {
                 // one entry pair per iteration, the next pair's indices and coordinates
                 // loaded while the current pair is computed
-                uint32_t nx = ent_at(lane), ny = ent_at(lane + G);
+                uint32_t nx = first[0], ny = first[1];
                 V4 pnx[3], wnx[3], pny[3], wny[3];
                 fetch(nx, pnx, wnx);
                 fetch(ny, pny, wny);
@@ -793,22 +798,31 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 }
             } else {
                 // U entry pairs per lane per iteration: all their loads are issued first, and
-                // the next iteration's row entries are loaded one iteration ahead
+                // the row entries are loaded RS_ROW_AHEAD iterations ahead
                 constexpr int UP = U == 3 ? 1 : U;
-                uint32_t nx[UP], ny[UP];
+                constexpr int D = RS_ROW_AHEAD;
+                constexpr int STEP = 2 * U * G;
+                uint32_t nx[D][UP], ny[D][UP];
 #pragma unroll
-                for (int q = 0; q < UP; q++) {
-                    nx[q] = ent_at(lane + 2 * q * G);
-                    ny[q] = ent_at(lane + (2 * q + 1) * G);
-                }
-                for (int e0 = lane; e0 < cnt; e0 += 2 * U * G) {
+                for (int d = 0; d < D; d++)
+#pragma unroll
+                    for (int q = 0; q < UP; q++) {
+                        nx[d][q] = d == 0 ? first[2 * q] : ent_at(lane + d * STEP + 2 * q * G);
+                        ny[d][q] = d == 0 ? first[2 * q + 1] : ent_at(lane + d * STEP + (2 * q + 1) * G);
+                    }
+                for (int e0 = lane; e0 < cnt; e0 += STEP) {
                     uint32_t ex[UP], ey[UP];
 #pragma unroll
                     for (int q = 0; q < UP; q++) {
-                        ex[q] = nx[q];
-                        ey[q] = ny[q];
-                        nx[q] = ent_at(e0 + 2 * U * G + 2 * q * G);
-                        ny[q] = ent_at(e0 + 2 * U * G + (2 * q + 1) * G);
+                        ex[q] = nx[0][q];
+                        ey[q] = ny[0][q];
+#pragma unroll
+                        for (int d = 0; d + 1 < D; d++) {
+                            nx[d][q] = nx[d + 1][q];
+                            ny[d][q] = ny[d + 1][q];
+                        }
+                        nx[D - 1][q] = ent_at(e0 + D * STEP + 2 * q * G);
+                        ny[D - 1][q] = ent_at(e0 + D * STEP + (2 * q + 1) * G);
                     }
                     V4 pbx[UP][3], wbx[UP][3], pby[UP][3], wby[UP][3];
 #pragma unroll
@@ -838,7 +852,7 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                                                   g[2], th, madj);
             };
             if (U == 3) {
-                uint32_t ent_n = ent_at(lane);
+                uint32_t ent_n = first[0];
                 V4 pbn[3], wbn[3];
                 fetch(ent_n, pbn, wbn);
                 for (int e = lane; e < cnt; e += G) {
@@ -859,7 +873,7 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 constexpr int UE = U == 3 ? 1 : U;
                 uint32_t nxt[UE];
 #pragma unroll
-                for (int q = 0; q < UE; q++) nxt[q] = ent_at(lane + q * G);
+                for (int q = 0; q < UE; q++) nxt[q] = first[q];
                 for (int e0 = lane; e0 < cnt; e0 += U * G) {
                     uint32_t ent[UE];
 #pragma unroll
