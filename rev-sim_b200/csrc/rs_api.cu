@@ -549,10 +549,10 @@ int build_nlist(revsim_handle *h, const double *xsrc, uint32_t *nbr = nullptr, i
         a.cnt_own = a.nbr_cnt + h->M;
         a.cnt_inc = a.nbr_cnt + 2 * (size_t)h->M;
         a.ownpos = h->d_ownpos;
-        h->launches += 2;
     }
-    cudaError_t e = launch_nlist(a, h->st);
-    h->launches += 6;
+    int nk = 0;
+    cudaError_t e = launch_nlist(a, h->st, &nk);
+    h->launches += nk;
     if (e != cudaSuccess) return fail(h, REVSIM_ERR_CUDA, std::string("nlist: ") + cudaGetErrorString(e));
     return REVSIM_OK;
 }

@@ -203,7 +203,7 @@ inline bool rdf_term_recurrence_ok(double step, double width, double exp_cutoff)
 }
 
 // Launchers (return cudaError_t of the launch).
-cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st);
+cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st, int *n_kernels);
 cudaError_t launch_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap, int mol0,
                                 int nmol, int32_t *pairs, unsigned long long *count,
                                 long long max_pairs, cudaStream_t st);

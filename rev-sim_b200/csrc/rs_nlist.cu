@@ -26,10 +26,9 @@ __device__ __forceinline__ double dist2_fp64(const double *xa, const double *xb,
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-// Cell of each molecule (by its O atom) and the per-cell counts.
-__global__ void k_cell_count(NlistArgs a) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x;
-    if (I >= a.M) return;
+// Cell of molecule I (by its O atom), written to cell_of_mol, with the O-H checks:
+// molecules are matched by O-O distance with a margin of two O-H lengths.
+__device__ __forceinline__ int mol_cell(const NlistArgs &a, int I) {
     const int r = a.mol_rep[I];
     const int nc = a.rep_nc[r];
     const double L = a.rep_box[r];
@@ -42,11 +41,75 @@ __global__ void k_cell_count(NlistArgs a) {
     }
     const int cell = a.rep_cell_off[r] + (ci[2] * nc + ci[1]) * nc + ci[0];
     a.cell_of_mol[I] = cell;
-    atomicAdd(a.cell_cnt + cell, 1);
-    // Molecules are matched by O-O distance with a margin of two O-H lengths.
     const double d1 = dist2_fp64(xo, xo + 3, L), d2 = dist2_fp64(xo, xo + 6, L);
     if (d1 > a.rext2 || d2 > a.rext2) atomicOr(a.status, ST_GEOMETRY);
     if (!(d1 <= a.rnear2 && d2 <= a.rnear2)) atomicAdd(a.max_cnt + 1, 1);
+    return cell;
+}
+
+// Cell of each molecule and the per-cell counts.
+__global__ void k_cell_count(NlistArgs a) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= a.M) return;
+    atomicAdd(a.cell_cnt + mol_cell(a, I), 1);
+}
+
+// The four cell passes (count, scan, fill, sort) in one CTA, for systems of up to
+// kCellsOneM molecules in up to kCellsOneC cells: counts, starts and fill cursors in shared
+// memory, each pass separated by a barrier.  Same cells, starts and order as the four kernels.
+constexpr int kCellsOneM = 8192, kCellsOneC = 4096;
+
+__global__ void __launch_bounds__(1024) k_cells_one(NlistArgs a) {
+    extern __shared__ int s_cell[];   // [3][n_cells]: counts, starts, fill cursors
+    __shared__ int s_part[1024];
+    int *s_cnt = s_cell, *s_start = s_cell + a.n_cells, *s_fill = s_cell + 2 * a.n_cells;
+    const int t = threadIdx.x, nt = blockDim.x;
+    for (int c = t; c < a.n_cells; c += nt) {
+        s_cnt[c] = 0;
+        s_fill[c] = 0;
+    }
+    if (t == 0) a.max_cnt[1] = 0;
+    __syncthreads();
+    for (int I = t; I < a.M; I += nt) atomicAdd(s_cnt + mol_cell(a, I), 1);
+    __syncthreads();
+    // exclusive scan: thread t takes the k consecutive cells from t k
+    const int k = (a.n_cells + nt - 1) / nt;
+    int sum = 0;
+    for (int j = 0; j < k; j++) {
+        const int c = t * k + j;
+        if (c < a.n_cells) sum += s_cnt[c];
+    }
+    s_part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < nt; off <<= 1) {
+        const int v = t >= off ? s_part[t - off] : 0;
+        __syncthreads();
+        s_part[t] += v;
+        __syncthreads();
+    }
+    int run = s_part[t] - sum;
+    for (int j = 0; j < k; j++) {
+        const int c = t * k + j;
+        if (c < a.n_cells) {
+            s_start[c] = run;
+            a.cell_start[c] = run;
+            a.cell_cnt[c] = s_cnt[c];
+            run += s_cnt[c];
+        }
+    }
+    __syncthreads();
+    for (int I = t; I < a.M; I += nt) {
+        const int c = a.cell_of_mol[I];
+        a.cell_tmp[s_start[c] + atomicAdd(s_fill + c, 1)] = I;
+    }
+    __syncthreads();
+    for (int I = t; I < a.M; I += nt) {
+        const int c = a.cell_of_mol[I];
+        const int s0 = s_start[c], n = s_cnt[c];
+        int rank = 0;
+        for (int q = 0; q < n; q++) rank += a.cell_tmp[s0 + q] < I;
+        a.cell_sorted[s0 + rank] = I;
+    }
 }
 
 // Exclusive scan of the cell counts (one CTA; cells are few).
@@ -437,14 +500,21 @@ __global__ void k_export_pairs(const uint32_t *nbr, const int *nbr_cnt, int cap,
 
 }  // namespace
 
-cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
-    cudaMemsetAsync(a.cell_cnt, 0, sizeof(int) * a.n_cells, st);
-    cudaMemsetAsync(a.max_cnt + 1, 0, sizeof(int), st);
-    const int t = 256, b = (a.M + t - 1) / t;
-    k_cell_count<<<b, t, 0, st>>>(a);
-    k_cell_scan<<<1, 1024, 0, st>>>(a);
-    k_cell_fill<<<b, t, 0, st>>>(a);
-    k_cell_sort<<<b, t, 0, st>>>(a);
+cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st, int *n_kernels) {
+    int nk = 0;
+    if (a.M <= kCellsOneM && a.n_cells <= kCellsOneC) {
+        k_cells_one<<<1, 1024, 3 * sizeof(int) * a.n_cells, st>>>(a);
+        nk += 1;
+    } else {
+        cudaMemsetAsync(a.cell_cnt, 0, sizeof(int) * a.n_cells, st);
+        cudaMemsetAsync(a.max_cnt + 1, 0, sizeof(int), st);
+        const int t = 256, b = (a.M + t - 1) / t;
+        k_cell_count<<<b, t, 0, st>>>(a);
+        k_cell_scan<<<1, 1024, 0, st>>>(a);
+        k_cell_fill<<<b, t, 0, st>>>(a);
+        k_cell_sort<<<b, t, 0, st>>>(a);
+        nk += 4;
+    }
     const size_t smem = (9 * sizeof(float) + sizeof(int)) * kRowChunk;
     cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // home molecules per cell over the 16 warps of a CTA: split a cell over up to 8 CTAs,
@@ -453,11 +523,14 @@ cudaError_t launch_nlist(const NlistArgs &a, cudaStream_t st) {
     const int per_cell = (a.M + a.n_cells - 1) / a.n_cells;
     const int split = std::min(8, std::max(1, (2 * per_cell + 15) / 16));
     k_rows<<<dim3(a.n_cells, split), 512, smem, st>>>(a);
+    nk += 1;
     if (a.split) {
         const int wb = (a.M + 7) / 8;   // one warp per row, eight per CTA
         k_split_own<<<wb, 256, 0, st>>>(a);
         k_split_inc<<<wb, 256, 0, st>>>(a);
+        nk += 2;
     }
+    if (n_kernels) *n_kernels = nk;
     return cudaGetLastError();
 }
 
