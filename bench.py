@@ -718,7 +718,7 @@ def cfg1_cpu_sample(x0, v0, p, target, box, n_s=10):
 
 
 def run_target_cfg1(a, device, reps=3, with_cpu=True):
-    """BASELINE configs[0] as the target of the engine: the 895-water box, 1,000 steps forward
+    """The target configuration of the engine: the 895-water box, 1,000 steps forward
     + 1,000 reverse (velocity Verlet, gamma = 0), loss = O-O RDF L2 (200 bins, 0-1 nm) against
     the sigma x 1.02 / eps x 0.95 target; R replicas of it batched in one handle (one launch
     per step), mixed precision against the same engine in FP64 and against the FP64 oracle on
@@ -1862,7 +1862,7 @@ def mlp_training_comparison(a, local, n_mol=400, box=2.48, R=4, n_steps=400, n_l
 
 
 def run_ours_mlp(a):
-    """Config 4: the 895-water system with the learned pair correction.  Timed: the full
+    """The 895-water system with the learned pair correction.  Timed: the full
     gradient (1,000 forward + 1,000 reverse steps) with the MLP on.  Then a training
     comparison, wall-clock timed: the classical + MLP model and the classical model alone,
     each trained for the same number of Adam updates from the same start."""
@@ -2008,7 +2008,7 @@ def run_ours_mlp(a):
 
 # ------------------------------------------------------------ replicas workload
 def replica_systems(n_rep, seed=2):
-    """Config 3: molecule counts log-uniform in [300, 3000] and temperatures uniform in
+    """64 water boxes: molecule counts log-uniform in [300, 3000] and temperatures uniform in
     [280, 320] K from a seed; boxes at liquid density, at least 2.45 nm (the minimum image
     of the 1.2 nm neighbour cutoff needs a side above 2.4 nm, so replicas under ~480
     molecules are less dense)."""
@@ -2041,7 +2041,7 @@ def replicas_config(a, n_mol, extra=None):
 
 
 def run_ours_replicas(a):
-    """Config 3: 64 water boxes of uneven size and temperature in one handle; one bench step
+    """64 water boxes of uneven size and temperature in one handle; one bench step
     = one batched gradient (forward + reverse) whose per-replica gradients are averaged."""
     import ctypes
     import torch

@@ -3,9 +3,8 @@
 The reversible-simulation gradient does not shard within a replica; independent replicas
 (batched water boxes, diamond replicas) spread across ranks with no collective on the data
 path.  The one exchange is the parameter update of a batch: the per-replica gradients of
-every rank are averaged into one update (config 3: "per-replica gradients averaged into one
-parameter update"), one all-reduce of P + 1 doubles over the process group (NCCL over NVLink
-on GPUs, gloo on CPU).
+every rank are averaged into one parameter update, one all-reduce of P + 1 doubles over the
+process group (NCCL over NVLink on GPUs, gloo on CPU).
 """
 
 import numpy as np
