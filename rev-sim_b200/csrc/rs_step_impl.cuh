@@ -239,16 +239,6 @@ __device__ __forceinline__ void mlp_adjoint(double *madj, int QI, int gi, R na, 
     atomicAdd(adj + 2, 2.0 * s1 * v);
     atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
 }
-// The same into a CTA's FP32 table in shared memory ([MLP_NT][MLP_NG][3]: c1, c2, c3), added
-// to the replica's FP64 accumulator once, at the end of the kernel (mlp_flush).
-template <typename R>
-__device__ __forceinline__ void mlp_adjoint(float *madj, int QI, int gi, R na, R sm, R hinv) {
-    const double v = (double)na * (double)hinv, s1 = (double)sm;
-    float *adj = madj + (QI * MLP_NG + gi) * 3;
-    atomicAdd(adj, (float)v);
-    atomicAdd(adj + 1, (float)(2.0 * s1 * v));
-    atomicAdd(adj + 2, (float)(3.0 * s1 * s1 * v));
-}
 
 // Two-entry form (FP32 kernels).  One (own atom KA, neighbour atom KB) slot of two neighbour
 // entries at once: the .x halves of the displacement (dx, dy, dz), of the VJP differences
@@ -256,14 +246,14 @@ __device__ __forceinline__ void mlp_adjoint(float *madj, int QI, int gi, R na, R
 // "x", the .y halves to entry "y" (rs_pack.cuh).  Evaluated unconditionally: pairs outside the
 // neighbour mask or the cutoff contribute exact zeros, so the nine slots of an entry pair run
 // as straight-line code with no divergence between the lanes of a warp.
-template <typename R, int FORM, bool REV, int KA, int KB, typename MA>
+template <typename R, int FORM, bool REV, int KA, int KB>
 __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>::T dx,
                                           typename PkT<R>::T dy, typename PkT<R>::T dz,
                                           typename PkT<R>::T ex, typename PkT<R>::T ey,
                                           typename PkT<R>::T ez, const R ca[3],
                                           const NbConsts<R> &nb, typename PkT<R>::T f[3],
                                           typename PkT<R>::T g[3], typename PkT<R>::T *th,
-                                          MA *madj) {
+                                          double *madj) {
     using P = typename PkT<R>::T;
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
@@ -358,7 +348,7 @@ __device__ __forceinline__ R image_shift(R d, R L, R hL) {
 
 // The three slots of own atom KA against the three atoms of the two neighbour molecules
 // (entry x: pbx, wbx; entry y: pby, wby).
-template <typename R, int FORM, bool REV, bool SHIFT, int KA, typename MA>
+template <typename R, int FORM, bool REV, bool SHIFT, int KA>
 __device__ __forceinline__ void pair_row(uint32_t maskx, uint32_t masky, const typename V4T<R>::T &pa,
                                          const typename V4T<R>::T pbx[3],
                                          const typename V4T<R>::T pby[3],
@@ -368,7 +358,7 @@ __device__ __forceinline__ void pair_row(uint32_t maskx, uint32_t masky, const t
                                          const typename PkT<R>::T sh[3], R L, R invL,
                                          const NbConsts<R> &nb, typename PkT<R>::T f[3],
                                          typename PkT<R>::T g[3], typename PkT<R>::T *th,
-                                         MA *madj) {
+                                         double *madj) {
     using P = typename PkT<R>::T;
 #define RS_SLOT(KB)                                                                               \
     {                                                                                             \
@@ -676,22 +666,10 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     const R invL = (R)(1.0 / Ld);
     const V4 *__restrict__ pos = (const V4 *)a.pos_in;
     const V4 *__restrict__ wgt = (const V4 *)a.wgt_in;
-    // this replica's accumulator of the learned term's interval-coefficient adjoints; the
-    // FP32 kernels sum a CTA's pairs into a table in shared memory first (after the bonded
-    // results), so that each interval costs one global FP64 atomic per CTA, not one per pair
+    // this replica's accumulator of the learned term's interval-coefficient adjoints
     double *madj = FORM == F_LJ_MLP && REV
                        ? nb.mlp_adj + ((size_t)rep * MLP_NCOPY + (blk % MLP_NCOPY)) * MLP_NT * MLP_NG * 4
                        : nullptr;
-    constexpr bool MLP_SMEM = FORM == F_LJ_MLP && REV && sizeof(R) == 4;
-    float *s_madj = MLP_SMEM ? (float *)((R *)(s_th + ngrp * (a.P + 1)) + 22 * ngrp) : nullptr;
-    if constexpr (MLP_SMEM) {
-        for (int i = threadIdx.x; i < MLP_NT * MLP_NG * 3; i += blockDim.x) s_madj[i] = 0.f;
-        __syncthreads();
-    }
-    auto *mlp_acc = [&]() {
-        if constexpr (MLP_SMEM) return s_madj;
-        else return madj;
-    }();
 
     // FP32: two entries per lane step in packed arithmetic (rs_pack.cuh), accumulated in
     // the halves of f2, g2, th2 and combined after the row loop; FP64: one entry per step
@@ -785,11 +763,11 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 }
                 const uint32_t mx = ex >> 23, my = ey >> 23;
                 pair_row<R, FORM, REV, SHIFT, 0>(mx, my, pa[0], pbx, pby, wa[0], wbx, wby, ca[0], sh, L, invL, nb,
-                                                 f2[0], g2[0], th2, mlp_acc);
+                                                 f2[0], g2[0], th2, madj);
                 pair_row<R, FORM, REV, SHIFT, 1>(mx, my, pa[1], pbx, pby, wa[1], wbx, wby, ca[1], sh, L, invL, nb,
-                                                 f2[1], g2[1], th2, mlp_acc);
+                                                 f2[1], g2[1], th2, madj);
                 pair_row<R, FORM, REV, SHIFT, 2>(mx, my, pa[2], pbx, pby, wa[2], wbx, wby, ca[2], sh, L, invL, nb,
-                                                 f2[2], g2[2], th2, mlp_acc);
+                                                 f2[2], g2[2], th2, madj);
             };
             if (U == 3) {
                 // one entry pair per iteration, the next pair's indices and coordinates
@@ -1000,14 +978,6 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
             for (int q = 0; q < ngrp; q++) s = __dadd_rn(s, sn2[q]);
             a.norm2[blk] = s;
         }
-        if constexpr (MLP_SMEM) {
-            // every lane's pairs are in the table (the barrier above): one FP64 atomic per
-            // touched coefficient into this CTA's copy of the replica's accumulator
-            for (int i = threadIdx.x; i < MLP_NT * MLP_NG * 3; i += blockDim.x) {
-                const float v = s_madj[i];
-                if (v != 0.f) atomicAdd(madj + (i / 3) * 4 + 1 + i % 3, (double)v);
-            }
-        }
     }
 }
 
@@ -1017,8 +987,7 @@ template <typename R, int FORM, int G, bool SHIFT, int U>
 cudaError_t launch_one(bool rev, int n_blk, int threads, const StepArgs &a, const NbConsts<R> &nb,
                        const BondConsts &bc, cudaStream_t st) {
     const int ngrp = threads / G;
-    const size_t smem = sizeof(double) * (size_t)ngrp * (a.P + 1) + sizeof(R) * 22 * (size_t)ngrp +
-                        (FORM == F_LJ_MLP && rev && sizeof(R) == 4 ? sizeof(float) * MLP_NT * MLP_NG * 3 : 0);
+    const size_t smem = sizeof(double) * (size_t)ngrp * (a.P + 1) + sizeof(R) * 22 * (size_t)ngrp;
     if (rev)
         return launch_chained(k_water_step<R, FORM, G, true, SHIFT, U>, dim3(n_blk), dim3(threads), smem,
                               st, a, nb, bc);
