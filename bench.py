@@ -804,6 +804,27 @@ def run_ours_cfg1(a):
     torch.cuda.set_device(local)
     import build as _build
     _build.build()
+    if a.profile:
+        # one batched gradient between cudaProfilerStart/Stop at the launch shapes the
+        # autotuner picks for it (8 lanes x 16 molecules per CTA for both step kernels)
+        from revsim import Engine, oo_l2_term, systems
+        R = a.cfg1_replicas
+        x0, v0, p, target, box = cfg1_start(R, local)
+        e = integ(Engine([895] * R, [box] * R, precision="mixed", device=local), a)
+        e.set_params(p)
+        e.set_loss([oo_l2_term(target)])
+        e.set_launch_shape(8, 16, 1, which=-1)
+        e.set_state(x0, v0)
+        seeds = systems.noise_seeds(1000 * R, seed=42).reshape(1000, R)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        e.forward(seeds, 0.0, 1000, 1000, 0.001)
+        e.reverse(seeds, 0.0, 1000, 1000, 1000, 0.001)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profiled_shape": e.launch_shape(0), "forward_shape": e.launch_shape(1)}))
+        e.close()
+        return
     with Clocks(local) as clk:
         t = run_target_cfg1(a, local, reps=max(a.steps, 1))
     if rank != 0:
