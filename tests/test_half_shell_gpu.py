@@ -185,3 +185,64 @@ def test_mode_rules():
     with pytest.raises(RevsimError):
         e.reverse(seeds, 1.0, 10, 10, 10, 0.001)
     e.close()
+
+
+def _mlp_theta(scale):
+    from revsim import mlp
+    th = mlp.init_params(3) + np.random.default_rng(4).normal(scale=scale, size=mlp.N_PARAMS)
+    return np.concatenate([C.default_params("lj"), th])
+
+
+def test_learned_term_forces_vjp_and_contraction(cfg1_water):
+    """The learned pair correction in the owner kernel: its coefficient adjoints are taken
+    once per pair against ca_a - ca_b.  Forces, VJP and the contraction over all 15,946
+    parameters against the FP64 oracle at the mixed bars, and against the both-sides
+    kernels of the same handle."""
+    n_mol, box, x, v = cfg1_water
+    theta = _mlp_theta(0.05)
+    rng = np.random.default_rng(7)
+    w, ac = rng.normal(size=x.shape), rng.normal(size=x.shape)
+    s = orc.make_system(n_mol, box, "lj", mlp=True)
+    pairs = orc.neighbor_pairs(s, x)
+    Fo, Go, _ = orc.forces_grads(s, theta, x, pairs, w, jac=False)
+    tho = orc.contract(s, theta, x, pairs, ac)
+    out = {}
+    for mode in ("both_sides", "half_shell"):
+        e = Engine(n_mol, box, inter_type="lj", precision="mixed", mlp=True)
+        e.set_params(theta)
+        e.set_pair_mode(mode)
+        assert e.pair_mode()[1] == mode
+        e.set_state(x, v)
+        out[mode] = e.force_vjp(w, ac)
+        e.close()
+    F, G, th = out["half_shell"]
+    assert nrel(F, Fo) < 1e-5
+    assert nrel(G, Go) < 1e-4
+    cl = slice(0, 7)
+    sc = np.abs(tho[cl] * theta[cl])
+    assert np.all(np.abs((th[0][cl] - tho[cl]) * theta[cl]) / np.maximum(sc, 0.01 * sc.max()) < 1e-4)
+    assert np.abs(th[0][7:] - tho[7:]).max() < 1e-4 * np.abs(tho[7:]).max()
+    Fb, Gb, thb = out["both_sides"]
+    assert nrel(F, Fb) < 1e-5
+    assert np.abs(th[0][7:] - thb[0][7:]).max() < 1e-4 * np.abs(thb[0][7:]).max()
+
+
+def test_buffered_14_7_forces(cfg1_water):
+    """The buffered 14-7 pair form (not among the trained parameter sets) in the owner
+    kernel: forces and VJP against the oracle."""
+    n_mol, box, x, v = cfg1_water
+    p = np.array(C.default_params("buff"))
+    rng = np.random.default_rng(9)
+    w, ac = rng.normal(size=x.shape), rng.normal(size=x.shape)
+    s = orc.make_system(n_mol, box, "buff")
+    Fo, Go, J = orc.forces_grads(s, p, x, orc.neighbor_pairs(s, x), w)
+    e = Engine(n_mol, box, inter_type="buff", precision="mixed")
+    e.set_params(p)
+    e.set_pair_mode("half_shell")
+    assert e.pair_mode()[1] == "half_shell"
+    e.set_state(x, v)
+    F, G, th = e.force_vjp(w, ac)
+    e.close()
+    assert nrel(F, Fo) < 1e-5
+    assert nrel(G, Go) < 1e-4
+    assert np.all(scaled_err(th[0], ac.ravel() @ J, p) < 1e-4)
