@@ -5,6 +5,8 @@ pair evaluated once by its owner, the partner's share gathered by a second kerne
   oracle at the mixed-precision bars (1e-5 / 1e-4), for every trained parameter set, and
   against the both-sides kernels of the same handle (1e-5: the same FP32 pair arithmetic
   summed in another order);
+* the learned pair correction (coefficient adjoints taken once per pair) and the buffered
+  14-7 form against the oracle at the mixed bars;
 * a 20-step gradient (gamma = 1/ps) against the oracle at the mixed bar (1e-4, 3e-4 for the
   exponential forms), on the tip3p box and on a 4.5 nm box of 3,000 molecules;
 * with the exactly reversible integrator the reverse pass rebuilds 1,000 steps at gamma = 0 bit
