@@ -240,12 +240,39 @@ __device__ __forceinline__ void mlp_adjoint(double *madj, int QI, int gi, R na, 
     atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
 }
 
+// The O-O Lennard-Jones form of pair_form on both halves of a register pair at once (the
+// packed instructions round each half as the scalar ones do, so the halves carry the bits of
+// pair_form<R, F_LJ>).  c[0] = sigma^2, c[1] = 24 eps, c[2] = 144 eps / sigma, c[3] = 1/eps.
+template <typename R, bool GRAD>
+__device__ __forceinline__ void lj_form2(const FormConsts<R> &fc, typename PkT<R>::T rinv,
+                                         typename PkT<R>::T invr2, typename PkT<R>::T &F,
+                                         typename PkT<R>::T &dF, typename PkT<R>::T g[2]) {
+    using P = typename PkT<R>::T;
+    P six = xmul(pk1(fc.c[0]), invr2);
+    six = xmul(xmul(six, six), six);
+    const P twelve = xmul(six, six);
+    F = xmul(xmul(pk1(fc.c[1]), rinv), xsub(xadd(twelve, twelve), six));
+    if (GRAD) {
+        dF = xneg(xmul(xmul(pk1(fc.c[1]), invr2), xsub(xmul(pk1(R(26)), twelve), xmul(pk1(R(7)), six))));
+        g[0] = xmul(xmul(pk1(fc.c[2]), rinv), xsub(xmul(pk1(R(4)), twelve), six));
+        g[1] = xmul(F, pk1(fc.c[3]));
+    }
+}
+
 // Two-entry form (FP32 kernels).  One (own atom KA, neighbour atom KB) slot of two neighbour
 // entries at once: the .x halves of the displacement (dx, dy, dz), of the VJP differences
 // (ex, ey, ez) = w_b - w_a, of the accumulators and of every intermediate belong to entry
 // "x", the .y halves to entry "y" (rs_pack.cuh).  Evaluated unconditionally: pairs outside the
 // neighbour mask or the cutoff contribute exact zeros, so the nine slots of an entry pair run
 // as straight-line code with no divergence between the lanes of a warp.
+//
+// The slot works with A = F/r and B = (dF/dr - F/r) / r^2 of the radial force F(r): the force
+// on the own atom is -A d, the force Jacobian is M = -(B d d^T + A I), so the VJP adds
+// -(B (d . e) d + A e), and the contraction of dF/dtheta with the adjoint a is
+// -(dF/dtheta / r) (d . a).  For the reaction-field Coulomb term F = qq (1/r^2 - 2 k_rf r),
+// A = qq (1/r^3 - 2 k_rf) and B = -3 qq / r^5 in closed form (no separate r, dF or 1/r
+// scaling of the dot products); the O-O form and the learned term add their own A and B.
+// The accumulators receive -A and -B times the vectors ("mA", "mB").
 template <typename R, int FORM, bool REV, int KA, int KB>
 __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>::T dx,
                                           typename PkT<R>::T dy, typename PkT<R>::T dz,
@@ -257,70 +284,89 @@ __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>:
     using P = typename PkT<R>::T;
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
+    constexpr int QI = (KA > 0) + (KB > 0);
+    constexpr bool OO = KA == 0 && KB == 0;
     const P r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
     const bool onx = bitx && r2.x <= nb.rc2;
     const bool ony = bity && r2.y <= nb.rc2;
-    const P z = pk(onx ? R(1) : R(0), ony ? R(1) : R(0));
-    const P r2s = pk(onx ? r2.x : R(1), ony ? r2.y : R(1));
-    const P rinv = xrsqrt(r2s);
-    const P r = xmul(r2s, rinv);
-    const P invr2 = xmul(rinv, rinv);
-    constexpr int QI = (KA > 0) + (KB > 0);
     const R qq = nb.qq[QI];
-    const P Fc = xmul(pk1(qq), xsub(invr2, xmul(pk1(nb.krf2), r)));
-    P F = Fc;
-    P dF = pk1(R(0));
+    // dead slots: 1/r of r = 1 (finite) and a zero charge product
+    const P rinv = xrsqrt(pk(onx ? r2.x : R(1), ony ? r2.y : R(1)));
+    const P qz = pk(onx ? qq : R(0), ony ? qq : R(0));
+    const P invr2 = xmul(rinv, rinv);
+    const P rinv3 = xmul(invr2, rinv);
+    const P mAc = xmul(qz, xsub(pk1(nb.krf2), rinv3));   // -A of the Coulomb term
+    P mA = mAc;
+    P mB = pk1(R(0));
+    if (REV) mB = xmul(xmul(qz, pk1(R(3))), xmul(rinv3, invr2));   // 3 qq / r^5 = -B
     P gf[4];
-    if (REV) dF = xneg(xmul(pk1(xadd(qq, qq)), xadd(xmul(invr2, rinv), pk1(nb.krf))));
-    if (KA == 0 && KB == 0) {
-        if (nb.fc.on) {
-            // one O-O slot in nine: the pair form runs per half with the scalar code
-            R Fx, Fy, dFx = R(0), dFy = R(0), gx[4], gy[4];
-            pair_form<R, PF, REV>(nb.fc, r.x, rinv.x, invr2.x, Fx, dFx, gx);
-            pair_form<R, PF, REV>(nb.fc, r.y, rinv.y, invr2.y, Fy, dFy, gy);
-            F = xadd(F, pk(Fx, Fy));
-            if (REV) {
-                dF = xadd(dF, pk(dFx, dFy));
+    if (OO || FORM == F_LJ_MLP) {
+        const P z = pk(onx ? R(1) : R(0), ony ? R(1) : R(0));
+        const P r = xmul(pk(onx ? r2.x : R(1), ony ? r2.y : R(1)), rinv);
+        P Ff = pk1(R(0)), dFf = pk1(R(0));
+        bool have = false;
+        if (OO && nb.fc.on) {
+            have = true;
+            if constexpr (PF == F_LJ) {
+                lj_form2<R, REV>(nb.fc, rinv, invr2, Ff, dFf, gf);
+            } else {
+                // the other O-O forms per half with the scalar code
+                R Fx, Fy, dFx = R(0), dFy = R(0), gx[4], gy[4];
+                pair_form<R, PF, REV>(nb.fc, r.x, rinv.x, invr2.x, Fx, dFx, gx);
+                pair_form<R, PF, REV>(nb.fc, r.y, rinv.y, invr2.y, Fy, dFy, gy);
+                Ff = pk(Fx, Fy);
+                if (REV) {
+                    dFf = pk(dFx, dFy);
 #pragma unroll
-                for (int p = 0; p < NF; p++) gf[p] = pk(gx[p], gy[p]);
+                    for (int p = 0; p < NF; p++) gf[p] = pk(gx[p], gy[p]);
+                }
             }
         }
-    }
-    int gix = 0, giy = 0;
-    R smx = R(0), smy = R(0);
-    if constexpr (FORM == F_LJ_MLP) {
-        R d1x, d1y, d2x, d2y;
-        mlp_segment<R, REV>(nb, QI, r.x, gix, smx, d1x, d2x);
-        mlp_segment<R, REV>(nb, QI, r.y, giy, smy, d1y, d2y);
-        F = xsub(F, pk(d1x, d1y));
-        if (REV) dF = xsub(dF, pk(d2x, d2y));
-    }
-    const P Fr = xmul(xmul(F, rinv), z);
-    // force on the own atom: -F n = -(F/r) dr
-    const P mFr = xneg(Fr);
-    f[0] = xfma(mFr, dx, f[0]);
-    f[1] = xfma(mFr, dy, f[1]);
-    f[2] = xfma(mFr, dz, f[2]);
-    if (REV) {
-        // VJP: M delta, delta = (ex, ey, ez), M = -[F' n n + (F/r)(I - n n)]
-        const P s = xmul(rinv, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
-        const P k1 = xmul(xmul(xsub(xmul(dF, z), Fr), s), rinv);
-        g[0] = xsub(g[0], xfma(k1, dx, xmul(Fr, ex)));
-        g[1] = xsub(g[1], xfma(k1, dy, xmul(Fr, ey)));
-        g[2] = xsub(g[2], xfma(k1, dz, xmul(Fr, ez)));
-        // dtheta: acoef_a . dF_a/dtheta_p = -(dF/dtheta_p) (n . acoef_a)
-        const P na = xmul(xmul(rinv, xfma(dz, pk1(ca[2]), xfma(dy, pk1(ca[1]), xmul(dx, pk1(ca[0]))))), z);
-        th[NF] = xfma(xneg(xmul(Fc, pk1(nb.twoinvq))), na, th[NF]);
-        if (KA == 0 && KB == 0) {
-            if (nb.fc.on) {
+        int gix = 0, giy = 0;
+        R smx = R(0), smy = R(0);
+        if constexpr (FORM == F_LJ_MLP) {
+            // the learned correction: F -= u'(r), dF/dr -= u''(r)
+            R d1x, d1y, d2x, d2y;
+            mlp_segment<R, REV>(nb, QI, r.x, gix, smx, d1x, d2x);
+            mlp_segment<R, REV>(nb, QI, r.y, giy, smy, d1y, d2y);
+            Ff = xsub(Ff, pk(d1x, d1y));
+            if (REV) dFf = xsub(dFf, pk(d2x, d2y));
+            have = true;
+        }
+        if (have) {
+            Ff = xmul(Ff, z);
+            const P Af = xmul(Ff, rinv);
+            mA = xsub(mA, Af);
+            if (REV) mB = xfma(xsub(Af, xmul(dFf, z)), invr2, mB);
+        }
+        if (REV) {
+            const P dca = xfma(dz, pk1(ca[2]), xfma(dy, pk1(ca[1]), xmul(dx, pk1(ca[0]))));
+            const P na = xmul(xmul(rinv, dca), z);   // n . a
+            if (OO && nb.fc.on) {
 #pragma unroll
                 for (int p = 0; p < NF; p++) th[p] = xfma(xneg(gf[p]), na, th[p]);
             }
+            if constexpr (FORM == F_LJ_MLP) {
+                if (onx) mlp_adjoint<R>(madj, QI, gix, na.x, smx, nb.mlp_hinv);
+                if (ony) mlp_adjoint<R>(madj, QI, giy, na.y, smy, nb.mlp_hinv);
+            }
+            // charge: acoef . dF/dq_O = (2 / q_O) (-A_c) (d . a)
+            th[NF] = xfma(xmul(mAc, pk1(nb.twoinvq)), dca, th[NF]);
         }
-        if constexpr (FORM == F_LJ_MLP) {
-            if (onx) mlp_adjoint<R>(madj, QI, gix, na.x, smx, nb.mlp_hinv);
-            if (ony) mlp_adjoint<R>(madj, QI, giy, na.y, smy, nb.mlp_hinv);
-        }
+    } else if (REV) {
+        const P dca = xfma(dz, pk1(ca[2]), xfma(dy, pk1(ca[1]), xmul(dx, pk1(ca[0]))));
+        th[NF] = xfma(xmul(mAc, pk1(nb.twoinvq)), dca, th[NF]);
+    }
+    // force on the own atom: -A d
+    f[0] = xfma(mA, dx, f[0]);
+    f[1] = xfma(mA, dy, f[1]);
+    f[2] = xfma(mA, dz, f[2]);
+    if (REV) {
+        // VJP: -(B (d . e) d + A e)
+        const P mt = xmul(mB, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
+        g[0] = xfma(mt, dx, xfma(mA, ex, g[0]));
+        g[1] = xfma(mt, dy, xfma(mA, ey, g[1]));
+        g[2] = xfma(mt, dz, xfma(mA, ez, g[2]));
     }
 }
 
@@ -386,6 +432,7 @@ __device__ __forceinline__ void pair_row(uint32_t maskx, uint32_t masky, const t
 // evaluated unconditionally: pairs outside the neighbour mask or the cutoff
 // contribute exact zeros, so the nine slots of an entry run as straight-line code with
 // no divergence between the lanes of a warp (each lane holds a different neighbour).
+// Same A / B formulation as the two-entry form.
 template <typename R, int FORM, bool REV, int KA, int KB>
 __device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
                                           const typename V4T<R>::T &wa,
@@ -394,77 +441,85 @@ __device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
                                           double *madj) {
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
+    constexpr int QI = (KA > 0) + (KB > 0);
+    constexpr bool OO = KA == 0 && KB == 0;
     const R r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
     const bool on = bit && r2 <= nb.rc2;
-    const R z = on ? R(1) : R(0);
     const R r2s = on ? r2 : R(1);
     const R rinv = xrsqrt(r2s);
-    const R r = xmul(r2s, rinv);
+    const R qz = on ? nb.qq[QI] : R(0);
     const R invr2 = xmul(rinv, rinv);
-    constexpr int QI = (KA > 0) + (KB > 0);
-    const R qq = nb.qq[QI];
-    const R Fc = xmul(qq, xsub(invr2, xmul(nb.krf2, r)));
-    R F = Fc;
-    R dF = R(0);
-    R gf[4];
-    if (REV) dF = -xmul(xadd(qq, qq), xadd(xmul(invr2, rinv), nb.krf));
-    if (KA == 0 && KB == 0) {
-        if (nb.fc.on) {
-            R Ff, dFf = R(0);
+    const R rinv3 = xmul(invr2, rinv);
+    const R mAc = xmul(qz, xsub(nb.krf2, rinv3));   // -A of the Coulomb term
+    R mA = mAc;
+    R mB = R(0);
+    if (REV) mB = xmul(xmul(qz, R(3)), xmul(rinv3, invr2));   // 3 qq / r^5 = -B
+    R dca = R(0);
+    if (REV) dca = xfma(dz, ca[2], xfma(dy, ca[1], xmul(dx, ca[0])));
+    if (OO || FORM == F_LJ_MLP) {
+        const R z = on ? R(1) : R(0);
+        const R r = xmul(r2s, rinv);
+        R Ff = R(0), dFf = R(0), gf[4];
+        bool have = false;
+        if (OO && nb.fc.on) {
+            have = true;
             pair_form<R, PF, REV>(nb.fc, r, rinv, invr2, Ff, dFf, gf);
-            F = xadd(F, Ff);
-            if (REV) dF = xadd(dF, dFf);
         }
-    }
-    // Learned pair correction: the cubic segment of interval gi of type QI (O-O, O-H,
-    // H-H), F = -u'(r) = -(c1 + 2 c2 s + 3 c3 s^2) / h, dF/dr = -(2 c2 + 6 c3 s) / h^2.
-    int gi = 0;
-    R sm = R(0);
-    if constexpr (FORM == F_LJ_MLP) {
-        using V4m = typename V4T<R>::T;
-        const R q = xmul(r, nb.mlp_hinv);
-        gi = min((int)q, MLP_NG - 1);
-        sm = xsub(q, (R)gi);
-        const V4m cf = reinterpret_cast<const V4m *>(nb.mlp_tab)[QI * MLP_NG + gi];
-        const R d1 = xmul(xfma(sm, xfma(xmul(R(3), sm), cf.w, xmul(R(2), cf.z)), cf.y), nb.mlp_hinv);
-        F = xsub(F, d1);
+        // Learned pair correction: the cubic segment of interval gi of type QI (O-O, O-H,
+        // H-H), F -= u'(r) = (c1 + 2 c2 s + 3 c3 s^2) / h, dF/dr -= (2 c2 + 6 c3 s) / h^2.
+        int gi = 0;
+        R sm = R(0);
+        if constexpr (FORM == F_LJ_MLP) {
+            using V4m = typename V4T<R>::T;
+            const R q = xmul(r, nb.mlp_hinv);
+            gi = min((int)q, MLP_NG - 1);
+            sm = xsub(q, (R)gi);
+            const V4m cf = reinterpret_cast<const V4m *>(nb.mlp_tab)[QI * MLP_NG + gi];
+            const R d1 = xmul(xfma(sm, xfma(xmul(R(3), sm), cf.w, xmul(R(2), cf.z)), cf.y), nb.mlp_hinv);
+            Ff = xsub(Ff, d1);
+            if (REV) {
+                const R d2 = xmul(xmul(xfma(xmul(R(6), sm), cf.w, xmul(R(2), cf.z)), nb.mlp_hinv), nb.mlp_hinv);
+                dFf = xsub(dFf, d2);
+            }
+            have = true;
+        }
+        if (have) {
+            Ff = xmul(Ff, z);
+            const R Af = xmul(Ff, rinv);
+            mA = xsub(mA, Af);
+            if (REV) mB = xfma(xsub(Af, xmul(dFf, z)), invr2, mB);
+        }
         if (REV) {
-            const R d2 = xmul(xmul(xfma(xmul(R(6), sm), cf.w, xmul(R(2), cf.z)), nb.mlp_hinv), nb.mlp_hinv);
-            dF = xsub(dF, d2);
-        }
-    }
-    const R Fr = xmul(xmul(F, rinv), z);
-    // force on the own atom: -F n = -(F/r) dr
-    f[0] = xfma(-Fr, dx, f[0]);
-    f[1] = xfma(-Fr, dy, f[1]);
-    f[2] = xfma(-Fr, dz, f[2]);
-    if (REV) {
-        // VJP: M delta, delta = w_b - w_a, M = -[F' n n + (F/r)(I - n n)]
-        const R ex = xsub(wb.x, wa.x), ey = xsub(wb.y, wa.y), ez = xsub(wb.z, wa.z);
-        const R s = xmul(rinv, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
-        const R k1 = xmul(xmul(xsub(xmul(dF, z), Fr), s), rinv);
-        g[0] = xsub(g[0], xfma(k1, dx, xmul(Fr, ex)));
-        g[1] = xsub(g[1], xfma(k1, dy, xmul(Fr, ey)));
-        g[2] = xsub(g[2], xfma(k1, dz, xmul(Fr, ez)));
-        // dtheta: acoef_a . dF_a/dtheta_p = -(dF/dtheta_p) (n . acoef_a)
-        const R na = xmul(xmul(rinv, xfma(dz, ca[2], xfma(dy, ca[1], xmul(dx, ca[0])))), z);
-        th[NF] = xfma(-xmul(Fc, nb.twoinvq), na, th[NF]);
-        if (KA == 0 && KB == 0) {
-            if (nb.fc.on) {
+            const R na = xmul(xmul(rinv, dca), z);   // n . a
+            if (OO && nb.fc.on) {
 #pragma unroll
                 for (int p = 0; p < NF; p++) th[p] = xfma(-gf[p], na, th[p]);
             }
-        }
-        if constexpr (FORM == F_LJ_MLP) {
-            // -(dF/dc_k) (n . acoef_a) for the interval's coefficients c1, c2, c3
-            if (on) {
-                const double v = (double)na * (double)nb.mlp_hinv, s1 = (double)sm;
-                double *adj = madj + ((size_t)QI * MLP_NG + gi) * 4;
-                atomicAdd(adj + 1, v);
-                atomicAdd(adj + 2, 2.0 * s1 * v);
-                atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
+            if constexpr (FORM == F_LJ_MLP) {
+                // -(dF/dc_k) (n . acoef_a) for the interval's coefficients c1, c2, c3
+                if (on) {
+                    const double v = (double)na * (double)nb.mlp_hinv, s1 = (double)sm;
+                    double *adj = madj + ((size_t)QI * MLP_NG + gi) * 4;
+                    atomicAdd(adj + 1, v);
+                    atomicAdd(adj + 2, 2.0 * s1 * v);
+                    atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
+                }
             }
         }
+    }
+    // force on the own atom: -A d
+    f[0] = xfma(mA, dx, f[0]);
+    f[1] = xfma(mA, dy, f[1]);
+    f[2] = xfma(mA, dz, f[2]);
+    if (REV) {
+        // VJP: -(B (d . e) d + A e), e = w_b - w_a
+        const R ex = xsub(wb.x, wa.x), ey = xsub(wb.y, wa.y), ez = xsub(wb.z, wa.z);
+        const R mt = xmul(mB, xfma(dz, ez, xfma(dy, ey, xmul(dx, ex))));
+        g[0] = xfma(mt, dx, xfma(mA, ex, g[0]));
+        g[1] = xfma(mt, dy, xfma(mA, ey, g[1]));
+        g[2] = xfma(mt, dz, xfma(mA, ez, g[2]));
+        // charge: acoef . dF/dq_O = (2 / q_O) (-A_c) (d . a)
+        th[NF] = xfma(xmul(mAc, nb.twoinvq), dca, th[NF]);
     }
 }
 
