@@ -915,6 +915,10 @@ int forward_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     if (h->ev_on) CK(cudaMemsetAsync(h->d_ev_acc, 0, sizeof(double) * R, h->st));
     StepArgs a = base_args(h, false);
     a.dt = dt;
+    a.dtm_O = dt / h->mO;
+    a.dtm_H = dt / h->mH;
+    a.invm_O = 1.0 / h->mO;
+    a.invm_H = 1.0 / h->mH;
     a.c = c;
     a.s = s;
     for (int step = 1; step <= n_steps; step++) {
@@ -980,6 +984,10 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
 
     StepArgs a = base_args(h, true);
     a.dt = dt;
+    a.dtm_O = dt / h->mO;
+    a.dtm_H = dt / h->mH;
+    a.invm_O = 1.0 / h->mO;
+    a.invm_H = 1.0 / h->mH;
     a.c = c;
     a.s = s;
     const double dt2 = dt * dt;

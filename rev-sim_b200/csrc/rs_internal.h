@@ -128,6 +128,7 @@ struct StepArgs {
     int *status;
     double *F_out;     // forces-only mode
     double dt, c, s, mO, mH, acoefO, acoefH;
+    double dtm_O, dtm_H, invm_O, invm_H;   // dt / m and 1 / m of O and H (the exact integrator)
     const uint64_t *seed_cur, *seed_next;   // [n_replicas]
     // Caller-supplied noise of the current / next step, [3N] each (host_noise entry points);
     // when set it replaces the Philox draw of seed_cur / seed_next.

@@ -240,6 +240,13 @@ __device__ __forceinline__ void mlp_adjoint(double *madj, int QI, int gi, R na, 
     atomicAdd(adj + 3, 3.0 * s1 * s1 * v);
 }
 
+// The reverse kernels' charge contraction sum_slots (2 / q_O) (-A_c) (d . a) equals, per own
+// atom, (2 / q_O) a . (F - F_form): the Coulomb share of the atom's pair force, known once the
+// row is done.  So the slots only accumulate the O-O form's share F_form (one slot in nine), and
+// the contraction is formed after the row -- except with the learned term, whose share is on
+// every slot and which needs n . a per slot anyway.
+__host__ __device__ constexpr bool charge_from_forces(int form) { return form != F_LJ_MLP; }
+
 // The O-O Lennard-Jones form of pair_form on both halves of a register pair at once (the
 // packed instructions round each half as the scalar ones do, so the halves carry the bits of
 // pair_form<R, F_LJ>).  c[0] = sigma^2, c[1] = 24 eps, c[2] = 144 eps / sigma, c[3] = 1/eps.
@@ -280,12 +287,13 @@ __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>:
                                           typename PkT<R>::T ez, const R ca[3],
                                           const NbConsts<R> &nb, typename PkT<R>::T f[3],
                                           typename PkT<R>::T g[3], typename PkT<R>::T *th,
-                                          double *madj) {
+                                          typename PkT<R>::T fnc[3], double *madj) {
     using P = typename PkT<R>::T;
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
     constexpr int QI = (KA > 0) + (KB > 0);
     constexpr bool OO = KA == 0 && KB == 0;
+    constexpr bool CHG_F = charge_from_forces(FORM);
     const P r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
     const bool onx = bitx && r2.x <= nb.rc2;
     const bool ony = bity && r2.y <= nb.rc2;
@@ -338,6 +346,13 @@ __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>:
             const P Af = xmul(Ff, rinv);
             mA = xsub(mA, Af);
             if (REV) mB = xfma(xsub(Af, xmul(dFf, z)), invr2, mB);
+            if (REV && CHG_F) {
+                // the O-O form's share of the own-atom force, so that the Coulomb share is
+                // known after the row (charge_contraction)
+                fnc[0] = xfma(Af, dx, fnc[0]);
+                fnc[1] = xfma(Af, dy, fnc[1]);
+                fnc[2] = xfma(Af, dz, fnc[2]);
+            }
         }
         if (REV) {
             const P dca = xfma(dz, pk1(ca[2]), xfma(dy, pk1(ca[1]), xmul(dx, pk1(ca[0]))));
@@ -350,12 +365,9 @@ __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>:
                 if (onx) mlp_adjoint<R>(madj, QI, gix, na.x, smx, nb.mlp_hinv);
                 if (ony) mlp_adjoint<R>(madj, QI, giy, na.y, smy, nb.mlp_hinv);
             }
-            // charge: acoef . dF/dq_O = (2 / q_O) (-A_c) (d . a)
-            th[NF] = xfma(xmul(mAc, pk1(nb.twoinvq)), dca, th[NF]);
+            // charge, per slot when the learned term is on: acoef . dF/dq_O = (2 / q_O) (-A_c) (d . a)
+            if (!CHG_F) th[NF] = xfma(xmul(mAc, pk1(nb.twoinvq)), dca, th[NF]);
         }
-    } else if (REV) {
-        const P dca = xfma(dz, pk1(ca[2]), xfma(dy, pk1(ca[1]), xmul(dx, pk1(ca[0]))));
-        th[NF] = xfma(xmul(mAc, pk1(nb.twoinvq)), dca, th[NF]);
     }
     // force on the own atom: -A d
     f[0] = xfma(mA, dx, f[0]);
@@ -404,7 +416,7 @@ __device__ __forceinline__ void pair_row(uint32_t maskx, uint32_t masky, const t
                                          const typename PkT<R>::T sh[3], R L, R invL,
                                          const NbConsts<R> &nb, typename PkT<R>::T f[3],
                                          typename PkT<R>::T g[3], typename PkT<R>::T *th,
-                                         double *madj) {
+                                         typename PkT<R>::T fnc[3], double *madj) {
     using P = typename PkT<R>::T;
 #define RS_SLOT(KB)                                                                               \
     {                                                                                             \
@@ -418,7 +430,7 @@ __device__ __forceinline__ void pair_row(uint32_t maskx, uint32_t masky, const t
                                         slot_d<R, SHIFT>(pa.x, pbx[KB].x, pby[KB].x, sh[0], L, invL), \
                                         slot_d<R, SHIFT>(pa.y, pbx[KB].y, pby[KB].y, sh[1], L, invL), \
                                         slot_d<R, SHIFT>(pa.z, pbx[KB].z, pby[KB].z, sh[2], L, invL), \
-                                        ex, ey, ez, ca, nb, f, g, th, madj);                      \
+                                        ex, ey, ez, ca, nb, f, g, th, fnc, madj);                 \
     }
     RS_SLOT(0);
     RS_SLOT(1);
@@ -438,11 +450,12 @@ __device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
                                           const typename V4T<R>::T &wa,
                                           const typename V4T<R>::T &wb, const R ca[3],
                                           const NbConsts<R> &nb, R f[3], R g[3], R *th,
-                                          double *madj) {
+                                          R fnc[3], double *madj) {
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int PF = FORM == F_LJ_MLP ? F_LJ : FORM;   // the O-O pair form
     constexpr int QI = (KA > 0) + (KB > 0);
     constexpr bool OO = KA == 0 && KB == 0;
+    constexpr bool CHG_F = charge_from_forces(FORM);
     const R r2 = xfma(dz, dz, xfma(dy, dy, xmul(dx, dx)));
     const bool on = bit && r2 <= nb.rc2;
     const R r2s = on ? r2 : R(1);
@@ -455,7 +468,7 @@ __device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
     R mB = R(0);
     if (REV) mB = xmul(xmul(qz, R(3)), xmul(rinv3, invr2));   // 3 qq / r^5 = -B
     R dca = R(0);
-    if (REV) dca = xfma(dz, ca[2], xfma(dy, ca[1], xmul(dx, ca[0])));
+    if (REV && (OO || !CHG_F)) dca = xfma(dz, ca[2], xfma(dy, ca[1], xmul(dx, ca[0])));
     if (OO || FORM == F_LJ_MLP) {
         const R z = on ? R(1) : R(0);
         const R r = xmul(r2s, rinv);
@@ -488,6 +501,11 @@ __device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
             const R Af = xmul(Ff, rinv);
             mA = xsub(mA, Af);
             if (REV) mB = xfma(xsub(Af, xmul(dFf, z)), invr2, mB);
+            if (REV && CHG_F) {
+                fnc[0] = xfma(Af, dx, fnc[0]);
+                fnc[1] = xfma(Af, dy, fnc[1]);
+                fnc[2] = xfma(Af, dz, fnc[2]);
+            }
         }
         if (REV) {
             const R na = xmul(xmul(rinv, dca), z);   // n . a
@@ -518,8 +536,8 @@ __device__ __forceinline__ void pair_term1(bool bit, R dx, R dy, R dz,
         g[0] = xfma(mt, dx, xfma(mA, ex, g[0]));
         g[1] = xfma(mt, dy, xfma(mA, ey, g[1]));
         g[2] = xfma(mt, dz, xfma(mA, ez, g[2]));
-        // charge: acoef . dF/dq_O = (2 / q_O) (-A_c) (d . a)
-        th[NF] = xfma(xmul(mAc, nb.twoinvq), dca, th[NF]);
+        // charge, per slot when the learned term is on: acoef . dF/dq_O = (2 / q_O) (-A_c) (d . a)
+        if (!CHG_F) th[NF] = xfma(xmul(mAc, nb.twoinvq), dca, th[NF]);
     }
 }
 
@@ -544,13 +562,13 @@ __device__ __forceinline__ void pair_row1(uint32_t mask, const typename V4T<R>::
                                          const typename V4T<R>::T &wa,
                                          const typename V4T<R>::T wb[3], const R ca[3],
                                          const R sh[3], R L, R invL, const NbConsts<R> &nb,
-                                         R f[3], R g[3], R *th, double *madj) {
+                                         R f[3], R g[3], R *th, R fnc[3], double *madj) {
 #define RS_SLOT(KB)                                                                             \
     pair_term1<R, FORM, REV, KA, KB>((mask >> (3 * KA + KB)) & 1u,                               \
                                     slot_d1<R, SHIFT>(pa.x, pb[KB].x, sh[0], L, invL),           \
                                     slot_d1<R, SHIFT>(pa.y, pb[KB].y, sh[1], L, invL),           \
                                     slot_d1<R, SHIFT>(pa.z, pb[KB].z, sh[2], L, invL), wa, wb[KB], \
-                                    ca, nb, f, g, th, madj)
+                                    ca, nb, f, g, th, fnc, madj)
     RS_SLOT(0);
     RS_SLOT(1);
     RS_SLOT(2);
@@ -568,6 +586,10 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
     using V4 = typename V4T<R>::T;
     const size_t ia = 3 * (size_t)I + k;
     const double m = k == 0 ? a.mO : a.mH;
+    // The exact integrator multiplies by dt / m and 1 / m (its increments are rounded to the
+    // grid, and forward and reverse use the same expression); the reference's arithmetic
+    // divides as water.jl does.
+    const double dtm = k == 0 ? a.dtm_O : a.dtm_H, invm = k == 0 ? a.invm_O : a.invm_H;
     if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) atomicOr(a.status, ST_NAN);
     const double xk[3] = {a.x[3 * ia], a.x[3 * ia + 1], a.x[3 * ia + 2]};
     if (a.mode & MODE_FORCES_ONLY) {
@@ -595,7 +617,7 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
 #pragma unroll
         for (int u = 0; u < 3; u++) {
             double v = vk[u], x = xk[u];
-            const double kick = __ddiv_rn(__dmul_rn(F[u], a.dt), m);
+            const double kick = ex ? __dmul_rn(F[u], dtm) : __ddiv_rn(__dmul_rn(F[u], a.dt), m);
             v = __dadd_rn(v, ex ? qgrid(kick) : kick);
             const double h1 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
             x = __dadd_rn(x, ex ? qgrid(h1) : h1);
@@ -645,7 +667,7 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
             a.G[e] = Gv[u];
             n2 = __dadd_rn(n2, __dmul_rn(Gv[u], Gv[u]));
             // v_{n-1} = v' - F dt / m (water.jl:1516)
-            const double kick = __ddiv_rn(__dmul_rn(F[u], a.dt), m);
+            const double kick = a.exact ? __dmul_rn(F[u], dtm) : __ddiv_rn(__dmul_rn(F[u], a.dt), m);
             double v = __dsub_rn(vk[u], a.exact ? qgrid(kick) : kick);
             if (!defer) {
                 // water.jl:1520-1521
@@ -658,21 +680,21 @@ __device__ __forceinline__ void atom_update(const StepArgs &a, int I, int k, int
                 double x = xk[u];
                 const double h2 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
                 x = __dsub_rn(x, a.exact ? qgrid(h2) : h2);
-                v = __ddiv_rn(__dsub_rn(v, __dmul_rn(xi[u], a.s)), a.c);
+                v = __dsub_rn(v, __dmul_rn(xi[u], a.s));
+                if (a.c != 1.0) v = __ddiv_rn(v, a.c);   // v / 1 is v: the same bits at gamma = 0
                 if (a.exact) v = qgrid(v);
                 const double h1 = __dmul_rn(__dmul_rn(v, a.dt), 0.5);
                 x = __dsub_rn(x, a.exact ? qgrid(h1) : h1);
                 x = a.exact ? wrap_exact(x, Ld) : wrap1d(x, Ld);
+                // (dt^2 G (1 + c)) / 2, the halving as the (exact) product with 0.5
                 const double D = __dadd_rn(__dmul_rn(a.c, Dk[u]),
-                                           __ddiv_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]),
-                                                               __dadd_rn(1.0, a.c)),
-                                                     2.0));
+                                           __dmul_rn(__dmul_rn(__dmul_rn(dt2, Gv[u]), __dadd_rn(1.0, a.c)), 0.5));
                 const double C = __dadd_rn(Ck[u], D);
                 a.D[e] = D;
                 a.C[e] = C;
                 a.x[e] = x;
                 xn[u] = x;
-                Cm[u] = __ddiv_rn(C, m);
+                Cm[u] = a.exact ? __dmul_rn(C, invm) : __ddiv_rn(C, m);
             }
             a.v[e] = v;
         }
@@ -731,8 +753,8 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     // into f, g, th.
     constexpr bool PACKED = sizeof(R) == 4;
     using P = typename PkT<R>::T;
-    P f2[3][3], g2[3][3], th2[NTH];
-    R f[3][3], g[3][3], th[NTH];
+    P f2[3][3], g2[3][3], th2[NTH], fnc2[3];
+    R f[3][3], g[3][3], th[NTH], fnc[3];
 #pragma unroll
     for (int k = 0; k < 3; k++)
 #pragma unroll
@@ -746,6 +768,11 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     for (int p = 0; p < NTH; p++) {
         th2[p] = pk1(R(0));
         th[p] = R(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        fnc2[u] = pk1(R(0));
+        fnc[u] = R(0);
     }
 
     V4 pa[3], wa[3];
@@ -818,11 +845,11 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                 }
                 const uint32_t mx = ex >> 23, my = ey >> 23;
                 pair_row<R, FORM, REV, SHIFT, 0>(mx, my, pa[0], pbx, pby, wa[0], wbx, wby, ca[0], sh, L, invL, nb,
-                                                 f2[0], g2[0], th2, madj);
+                                                 f2[0], g2[0], th2, fnc2, madj);
                 pair_row<R, FORM, REV, SHIFT, 1>(mx, my, pa[1], pbx, pby, wa[1], wbx, wby, ca[1], sh, L, invL, nb,
-                                                 f2[1], g2[1], th2, madj);
+                                                 f2[1], g2[1], th2, fnc2, madj);
                 pair_row<R, FORM, REV, SHIFT, 2>(mx, my, pa[2], pbx, pby, wa[2], wbx, wby, ca[2], sh, L, invL, nb,
-                                                 f2[2], g2[2], th2, madj);
+                                                 f2[2], g2[2], th2, fnc2, madj);
             };
             if (U == 3) {
                 // one entry pair per iteration, the next pair's indices and coordinates
@@ -900,11 +927,11 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
                     sh[2] = image_shift1<R, SHIFT>(xsub(pbq[0].z, pa[0].z), L, hL);
                 }
                 pair_row1<R, FORM, REV, SHIFT, 0>(mask, pa[0], pbq, wa[0], wbq, ca[0], sh, L, invL, nb, f[0],
-                                                  g[0], th, madj);
+                                                  g[0], th, fnc, madj);
                 pair_row1<R, FORM, REV, SHIFT, 1>(mask, pa[1], pbq, wa[1], wbq, ca[1], sh, L, invL, nb, f[1],
-                                                  g[1], th, madj);
+                                                  g[1], th, fnc, madj);
                 pair_row1<R, FORM, REV, SHIFT, 2>(mask, pa[2], pbq, wa[2], wbq, ca[2], sh, L, invL, nb, f[2],
-                                                  g[2], th, madj);
+                                                  g[2], th, fnc, madj);
             };
             if (U == 3) {
                 uint32_t ent_n = first[0];
@@ -942,6 +969,30 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
 #pragma unroll
                     for (int q = 0; q < UE; q++) entry(ent[q], pb[q], wb[q]);
                 }
+            }
+        }
+    }
+
+    // The charge contraction from the forces (charge_from_forces), per lane on its partial
+    // sums: (2 / q_O) sum_k a_k . (F_k - F_form,k), F_form only on the O atom.
+    if constexpr (REV && charge_from_forces(FORM)) {
+        if (active) {
+            if constexpr (PACKED) {
+                P q = pk1(R(0));
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+#pragma unroll
+                    for (int u = 0; u < 3; u++)
+                        q = xfma(pk1(ca[k][u]), k == 0 ? xadd(f2[0][u], fnc2[u]) : f2[k][u], q);
+                th2[NF] = xfma(pk1(nb.twoinvq), q, th2[NF]);
+            } else {
+                R q = R(0);
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+#pragma unroll
+                    for (int u = 0; u < 3; u++)
+                        q = xfma(ca[k][u], k == 0 ? xadd(f[0][u], fnc[u]) : f[k][u], q);
+                th[NF] = xfma(nb.twoinvq, q, th[NF]);
             }
         }
     }
