@@ -120,6 +120,7 @@ struct revsim_handle {
            *d_D = nullptr, *d_G = nullptr, *d_F = nullptr, *d_x0 = nullptr, *d_v0 = nullptr;
     void *d_pos[2] = {nullptr, nullptr}, *d_wgt[2] = {nullptr, nullptr};
     double *d_part = nullptr, *d_norm2 = nullptr, *d_scale = nullptr;
+    std::vector<int> mol_rep_h;     // replica of each molecule (host copy)
     int *d_status = nullptr, *d_maxcnt = nullptr;
     unsigned long long *d_count = nullptr;
     // trajectory store
@@ -371,6 +372,23 @@ size_t cnts_set(const revsim_handle *h) { return (size_t)h->M * (split_rows(h) ?
 // per molecule pair in every box, and no barostat (whose box moves could end that).
 bool half_eff(const revsim_handle *h) { return h->half_req && split_rows(h) && h->shift_ok && !h->baro_on; }
 
+// The step kernels' dtheta partials and |dl_dfi|^2 sums (d_part, d_norm2): one slot per
+// molecule for the both-sides kernels, one per CTA of the reverse block table for the
+// half-shell kernels.  part_slots: the slots to clear; slot_owner: each slot's replica.
+size_t part_slots(const revsim_handle *h) { return std::max((size_t)h->shp[0].n_blk, (size_t)h->M); }
+
+int slot_owner(revsim_handle *h, std::vector<int> &owner) {
+    if (!half_eff(h)) {
+        owner = h->mol_rep_h;
+        return REVSIM_OK;
+    }
+    owner.resize(h->shp[0].n_blk);
+    if (cudaMemcpy(owner.data(), h->shp[0].d_blk_rep, sizeof(int) * owner.size(), cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return REVSIM_ERR_CUDA;
+    return REVSIM_OK;
+}
+
 void free_half(revsim_handle *h) {
     dfree(h->d_ownpos);
     dfree(h->d_slot_f);
@@ -466,8 +484,10 @@ int build_block_table(revsim_handle *h, int dir) {
         dfree(h->d_part);
         dfree(h->d_norm2);
         h->d_part = h->d_norm2 = nullptr;
-        CK(dalloc(&h->d_part, br.size() * (size_t)std::max(h->P, 1)));
-        CK(dalloc(&h->d_norm2, br.size()));
+        // per molecule (both-sides kernels) or per CTA (half-shell kernels)
+        const size_t slots = std::max(br.size(), (size_t)h->M);
+        CK(dalloc(&h->d_part, slots * (size_t)std::max(h->P, 1)));
+        CK(dalloc(&h->d_norm2, slots));
     }
     return REVSIM_OK;
 }
@@ -971,7 +991,7 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
     // the reverse pass must evaluate pairs as the forward pass did (same force bits)
     if (half_eff(h) != h->fwd_half)
         return fail(h, REVSIM_ERR_STATE, "the pair evaluation mode changed since the forward pass");
-    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * part_slots(h) * h->P, h->st));
     if (int rc_ = mlp_zero_adj(h)) return rc_;
     CK(cudaMemsetAsync(h->d_loss_acc, 0, sizeof(double) * R, h->st));
     if (h->ev_on) {
@@ -1049,14 +1069,14 @@ int reverse_impl(revsim_handle *h, double gamma, int n_steps, int n_steps_loss, 
             a.mode = (fuse ? MODE_FUSE_NEXT : 0) | (clipping ? MODE_DEFER_BA : 0);
             if ((rc = launch_step_k(h, true, a))) return rc;
             if (clipping) {
-                // Per-replica norm of dl_dfi from the block partials (fixed order).
-                std::vector<double> n2(h->shp[0].n_blk);
-                std::vector<int> br(h->shp[0].n_blk);
-                CK(cudaMemcpyAsync(n2.data(), h->d_norm2, sizeof(double) * h->shp[0].n_blk, cudaMemcpyDeviceToHost, h->st));
-                CK(cudaMemcpyAsync(br.data(), h->shp[0].d_blk_rep, sizeof(int) * h->shp[0].n_blk, cudaMemcpyDeviceToHost, h->st));
+                // Per-replica norm of dl_dfi from the per-slot sums (fixed order).
+                std::vector<int> br;
+                if ((rc = slot_owner(h, br))) return fail(h, rc, "block table copy failed");
+                std::vector<double> n2(br.size());
+                CK(cudaMemcpyAsync(n2.data(), h->d_norm2, sizeof(double) * n2.size(), cudaMemcpyDeviceToHost, h->st));
                 CK(cudaStreamSynchronize(h->st));
                 std::vector<double> acc(R, 0.0);
-                for (int b = 0; b < h->shp[0].n_blk; b++) acc[br[b]] += n2[b];
+                for (size_t b = 0; b < br.size(); b++) acc[br[b]] += n2[b];
                 for (int r = 0; r < R; r++) {
                     scale[2 * r] = std::sqrt(acc[r]);
                     scale[2 * r + 1] = clip;
@@ -1103,16 +1123,16 @@ int collect_kernel_times(revsim_handle *h) {
     return REVSIM_OK;
 }
 
-// Sum the dtheta block partials per replica (FP64, block order).
+// Sum the dtheta partials per replica (FP64, in slot order).
 int reduce_part(revsim_handle *h, std::vector<double> &out) {
-    std::vector<double> part((size_t)h->shp[0].n_blk * h->P);
-    std::vector<int> br(h->shp[0].n_blk);
+    std::vector<int> owner;
+    if (int rc = slot_owner(h, owner)) return fail(h, rc, "block table copy failed");
+    std::vector<double> part(owner.size() * h->P);
     CK(cudaMemcpyAsync(part.data(), h->d_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaMemcpyAsync(br.data(), h->shp[0].d_blk_rep, sizeof(int) * h->shp[0].n_blk, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     out.assign((size_t)h->R * h->P, 0.0);
-    for (int b = 0; b < h->shp[0].n_blk; b++)
-        for (int p = 0; p < h->P; p++) out[(size_t)br[b] * h->P + p] += part[(size_t)b * h->P + p];
+    for (size_t b = 0; b < owner.size(); b++)
+        for (int p = 0; p < h->P; p++) out[(size_t)owner[b] * h->P + p] += part[b * h->P + p];
     return REVSIM_OK;
 }
 
@@ -1254,6 +1274,7 @@ int32_t revsim_create(const revsim_system_desc *d, revsim_handle **out) {
     h->band = (float)(2e-5 * std::max(1.0, lmax / 4.0));
     const size_t n3 = 3 * (size_t)h->N;
     const size_t v4 = h->prec == REVSIM_MIXED ? sizeof(float4) : sizeof(double4);
+    h->mol_rep_h = mol_rep;
     bool ok = dalloc(&h->d_mol_rep, h->M) == cudaSuccess && dalloc(&h->d_atom_rep, h->N) == cudaSuccess &&
               dalloc(&h->d_rep_atom0, h->R) == cudaSuccess && dalloc(&h->d_rep_nmol, h->R) == cudaSuccess &&
               dalloc(&h->d_rep_box, h->R) == cudaSuccess && dalloc(&h->d_rep_sdO, h->R) == cudaSuccess &&
@@ -1531,7 +1552,7 @@ int32_t revsim_force_vjp(revsim_handle *h, const double *w, const double *acoef,
     CK(cudaMemcpyAsync(h->d_A, acoef, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
     if ((rc = build_nlist_checked(h, h->d_x))) return rc;
     if ((rc = pack(h, 0, true))) return rc;
-    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * (size_t)h->shp[0].n_blk * h->P, h->st));
+    CK(cudaMemsetAsync(h->d_part, 0, sizeof(double) * part_slots(h) * h->P, h->st));
     if ((rc = mlp_zero_adj(h))) return rc;
     StepArgs a = base_args(h, true);
     a.pos_in = h->d_pos[0];

@@ -107,6 +107,25 @@ __device__ __forceinline__ double gather_coord(double xo, double xa, bool is_h, 
     return is_h ? __dadd_rn(xo, vec1d(xo, xa, L)) : xa;
 }
 
+// FP32 gather coordinates (the mixed-precision step kernels): each molecule's coordinates as
+// FP32 offsets from an origin on a 0.5 nm grid (its O's cell), the origin's x, y, z in the
+// w component of the molecule's O, H1, H2 entries.  An offset is at most ~0.6 nm, so it
+// rounds to FP32 with an error of ~3e-8 nm where an absolute coordinate in a 4.5 nm box
+// rounds with up to 2.4e-7 nm; two molecules' origins differ by an exact multiple of 0.5 nm.
+// gather_origin: the grid point below the (wrapped) O coordinate xo, exactly.
+__device__ __forceinline__ double gather_origin(double xo) { return __dmul_rn(floor(__dmul_rn(xo, 2.0)), 0.5); }
+
+// Entry k (0: O, 1: H1, 2: H2) of a molecule whose O is at xo, the atom at xa.
+__device__ __forceinline__ float4 gather_f32(const double xo[3], const double xa[3], int k, double L) {
+    float4 r;
+    const double o0 = gather_origin(xo[0]), o1 = gather_origin(xo[1]), o2 = gather_origin(xo[2]);
+    r.x = (float)__dsub_rn(gather_coord(xo[0], xa[0], k != 0, L), o0);
+    r.y = (float)__dsub_rn(gather_coord(xo[1], xa[1], k != 0, L), o1);
+    r.z = (float)__dsub_rn(gather_coord(xo[2], xa[2], k != 0, L), o2);
+    r.w = (float)(k == 0 ? o0 : (k == 1 ? o1 : o2));
+    return r;
+}
+
 // ------------------------------------------------------------------ Philox
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, SC'11).
 __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {

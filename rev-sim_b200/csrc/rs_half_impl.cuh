@@ -242,9 +242,15 @@ __global__ void __maxnreg__((half_nreg(REV))) k_water_half(StepArgs a, NbConsts<
             // the partner atoms' coordinates, weights and coefficients are loaded per partner
             // atom (RS_HCOL), the O coordinates first for the image shift
             const V4 pox = pos[3 * Jx], poy = pos[3 * Jy];
-            const P sh[3] = {pk(image_shift(xsub(pox.x, pa[0].x), L, hL), image_shift(xsub(poy.x, pa[0].x), L, hL)),
-                             pk(image_shift(xsub(pox.y, pa[0].y), L, hL), image_shift(xsub(poy.y, pa[0].y), L, hL)),
-                             pk(image_shift(xsub(pox.z, pa[0].z), L, hL), image_shift(xsub(poy.z, pa[0].z), L, hL))};
+            // cell-origin differences (exact; gather_f32) plus the image shift from the O-O vector
+            const R ox[3] = {xsub(pox.w, pa[0].w), xsub(pos[3 * Jx + 1].w, pa[1].w), xsub(pos[3 * Jx + 2].w, pa[2].w)};
+            const R oy[3] = {xsub(poy.w, pa[0].w), xsub(pos[3 * Jy + 1].w, pa[1].w), xsub(pos[3 * Jy + 2].w, pa[2].w)};
+            const P sh[3] = {pk(xadd(ox[0], image_shift(xadd(xsub(pox.x, pa[0].x), ox[0]), L, hL)),
+                                xadd(oy[0], image_shift(xadd(xsub(poy.x, pa[0].x), oy[0]), L, hL))),
+                             pk(xadd(ox[1], image_shift(xadd(xsub(pox.y, pa[0].y), ox[1]), L, hL)),
+                                xadd(oy[1], image_shift(xadd(xsub(poy.y, pa[0].y), oy[1]), L, hL))),
+                             pk(xadd(ox[2], image_shift(xadd(xsub(pox.z, pa[0].z), ox[2]), L, hL)),
+                                xadd(oy[2], image_shift(xadd(xsub(poy.z, pa[0].z), oy[2]), L, hL)))};
             const uint32_t mx = ex >> 23, my = ey >> 23;
 #define RS_HCOL(KB)                                                                                    \
     {                                                                                                  \
@@ -406,10 +412,15 @@ __global__ void __launch_bounds__(512) k_water_gather(StepArgs a) {
         if (wpos) {
             const bool is_h = lane != 0;
             V4 po;
-            po.x = (R)gather_coord(o0, xn[0], is_h, Ld);
-            po.y = (R)gather_coord(o1, xn[1], is_h, Ld);
-            po.z = (R)gather_coord(o2, xn[2], is_h, Ld);
-            po.w = R(0);
+            if constexpr (sizeof(R) == 4) {
+                const double xo[3] = {o0, o1, o2};
+                po = gather_f32(xo, xn, lane, Ld);   // offsets from the molecule's cell origin
+            } else {
+                po.x = (R)gather_coord(o0, xn[0], is_h, Ld);
+                po.y = (R)gather_coord(o1, xn[1], is_h, Ld);
+                po.z = (R)gather_coord(o2, xn[2], is_h, Ld);
+                po.w = R(0);
+            }
             ((V4 *)a.pos_out)[3 * (size_t)I + lane] = po;
         }
     }

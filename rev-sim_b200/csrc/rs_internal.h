@@ -122,8 +122,9 @@ struct StepArgs {
     double *x, *v, *A, *B, *C, *D, *G;
     const void *pos_in, *wgt_in;
     void *pos_out, *wgt_out;
-    double *part;      // [n_blk * P] dtheta partials (accumulated)
-    double *norm2;     // [n_blk] sum of dl_dfi^2 (deferred / clipped mode)
+    double *part;      // [M * P] dtheta partials per molecule (accumulated); [n_blk * P] per
+                       // CTA in the half-shell kernels
+    double *norm2;     // [M] (half-shell: [n_blk]) sum of dl_dfi^2 (deferred / clipped mode)
     int P;
     int *status;
     double *F_out;     // forces-only mode

@@ -17,9 +17,7 @@ __global__ void k_pack_f(int N, const double *x, const double *C, double mO, dou
     const double m = is_h ? mH : mO;
     const double L = rep_box[atom_rep[i]];
     const double *xo = x + 9 * (size_t)(i / 3);
-    pos[i] = make_float4((float)gather_coord(xo[0], x[3 * i], is_h, L),
-                         (float)gather_coord(xo[1], x[3 * i + 1], is_h, L),
-                         (float)gather_coord(xo[2], x[3 * i + 2], is_h, L), 0.f);
+    pos[i] = gather_f32(xo, x + 3 * (size_t)i, i % 3, L);
     if (C)
         wgt[i] = make_float4((float)__ddiv_rn(C[3 * i], m), (float)__ddiv_rn(C[3 * i + 1], m),
                              (float)__ddiv_rn(C[3 * i + 2], m), 0.f);
@@ -98,10 +96,14 @@ __global__ void k_unintegrate(int M, StepArgs a, const int *mol_rep) {
     for (int k = 0; k < 3; k++) {
         using R = decltype(V4::x);
         V4 po;
-        po.x = (R)gather_coord(xn[0], xn[3 * k], k != 0, Ld);
-        po.y = (R)gather_coord(xn[1], xn[3 * k + 1], k != 0, Ld);
-        po.z = (R)gather_coord(xn[2], xn[3 * k + 2], k != 0, Ld);
-        po.w = R(0);
+        if constexpr (sizeof(R) == 4) {
+            po = gather_f32(xn, xn + 3 * k, k, Ld);
+        } else {
+            po.x = (R)gather_coord(xn[0], xn[3 * k], k != 0, Ld);
+            po.y = (R)gather_coord(xn[1], xn[3 * k + 1], k != 0, Ld);
+            po.z = (R)gather_coord(xn[2], xn[3 * k + 2], k != 0, Ld);
+            po.w = R(0);
+        }
         ((V4 *)a.pos_out)[3 * I + k] = po;
     }
 }

@@ -382,21 +382,22 @@ __device__ __forceinline__ void pair_term(bool bitx, bool bity, typename PkT<R>:
     }
 }
 
-// Displacement of one slot for both entries: cx / cy = the neighbour atom's coordinate in
-// entry x / y, c = the own atom's; formed per half (the two results land in one register
-// pair) and packed from there on.  SHIFT: one periodic image per molecule pair (chosen from
-// the O-O vector) is applied to all nine atom pairs; d + s rounds exactly as Molly's
-// (c2 - c1) -/+ L, and the image is the minimum one for every pair within the cutoff whenever
-// L > 2 (cutoff + 2 * max O-H distance).  Otherwise per slot d - L rint(d / L), which for every
-// pair within the cutoff gives the same bits as Molly's rule (vec1d); it differs only for
-// pairs near L/2, far outside the cutoff.
+// Displacement of one slot for both entries (FP32 kernels): cx / cy = the neighbour atom's
+// gather coordinate in entry x / y, c = the own atom's; formed per half (the two results land
+// in one register pair) and packed from there on.  The gather coordinates are offsets from
+// per-molecule cell origins (gather_f32) and s carries the entries' origin differences (exact
+// multiples of 0.5 nm).  SHIFT: s also carries one periodic image per molecule pair (chosen
+// from the O-O vector) for all nine atom pairs, the minimum one for every pair within the
+// cutoff whenever L > 2 (cutoff + 2 * max O-H distance); s stays exact, so d + s is the one
+// rounding of a vector within the cutoff.  Otherwise the image is chosen per slot from d + s
+// and applied to s first (s - L rint((d + s) / L), exact), then added to d.
 template <typename R, bool SHIFT>
 __device__ __forceinline__ typename PkT<R>::T slot_d(R c, R cx, R cy, typename PkT<R>::T s, R L, R invL) {
     using P = typename PkT<R>::T;
     const P d = pk(xsub(cx, c), xsub(cy, c));
     if (SHIFT) return xadd(d, s);
-    const P q = xmul(d, pk1(invL));
-    return xfma(pk(-r_rint(q.x), -r_rint(q.y)), pk1(L), d);
+    const P q = xmul(xadd(d, s), pk1(invL));
+    return xadd(d, xfma(pk(-r_rint(q.x), -r_rint(q.y)), pk1(L), s));
 }
 
 template <typename R>
@@ -726,14 +727,12 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     using V4 = typename V4T<R>::T;
     constexpr int NF = FormInfo<FORM>::NP;
     constexpr int NTH = NF + 1;
-    // dynamic shared memory: [groups][P] dtheta (double), [groups] |dl_dfi|^2 (double),
-    // then [groups][22] bonded results (R): forces (9), VJP (9), dtheta (4)
-    extern __shared__ double s_th[];
+    // dynamic shared memory: [groups][22] bonded results (R): forces (9), VJP (9), dtheta (4)
+    extern __shared__ double s_dyn[];
     chain_enter();
 
     const int grp = threadIdx.x / G;
     const int lane = threadIdx.x % G;
-    const int ngrp = blockDim.x / G;
     const int blk = blockIdx.x;
     const int rep = a.blk_rep[blk];
     const int I = a.blk_mol0[blk] + grp;
@@ -779,7 +778,7 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
     R ca[3][3];
     // Bonded terms first, by lane 0 of each group into shared memory, so that their
     // latency overlaps the neighbour loops of the other lanes and warps.
-    R *s_bond = (R *)(s_th + ngrp * (a.P + 1)) + 22 * grp;
+    R *s_bond = (R *)s_dyn + 22 * grp;
     if (active) {
 #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -837,11 +836,23 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
             // pairs starting at lane, lane + 2G, lane + 4G, ...
             auto entry2 = [&](uint32_t ex, uint32_t ey, const V4 pbx[3], const V4 wbx[3], const V4 pby[3],
                               const V4 wby[3]) {
-                P sh[3] = {pk1(R(0)), pk1(R(0)), pk1(R(0))};
+                // the entries' cell origins relative to the own molecule's (exact multiples of
+                // 0.5 nm, gather_f32) and, with SHIFT, the periodic image from the O-O vector:
+                // s = origin difference + image shift, exact, added to each slot's offset difference
+                R ox[3], oy[3];
+#pragma unroll
+                for (int u = 0; u < 3; u++) {
+                    ox[u] = xsub(pbx[u].w, pa[u].w);
+                    oy[u] = xsub(pby[u].w, pa[u].w);
+                }
+                P sh[3] = {pk(ox[0], oy[0]), pk(ox[1], oy[1]), pk(ox[2], oy[2])};
                 if (SHIFT) {
-                    sh[0] = pk(image_shift(xsub(pbx[0].x, pa[0].x), L, hL), image_shift(xsub(pby[0].x, pa[0].x), L, hL));
-                    sh[1] = pk(image_shift(xsub(pbx[0].y, pa[0].y), L, hL), image_shift(xsub(pby[0].y, pa[0].y), L, hL));
-                    sh[2] = pk(image_shift(xsub(pbx[0].z, pa[0].z), L, hL), image_shift(xsub(pby[0].z, pa[0].z), L, hL));
+                    sh[0] = pk(xadd(ox[0], image_shift(xadd(xsub(pbx[0].x, pa[0].x), ox[0]), L, hL)),
+                               xadd(oy[0], image_shift(xadd(xsub(pby[0].x, pa[0].x), oy[0]), L, hL)));
+                    sh[1] = pk(xadd(ox[1], image_shift(xadd(xsub(pbx[0].y, pa[0].y), ox[1]), L, hL)),
+                               xadd(oy[1], image_shift(xadd(xsub(pby[0].y, pa[0].y), oy[1]), L, hL)));
+                    sh[2] = pk(xadd(ox[2], image_shift(xadd(xsub(pbx[0].z, pa[0].z), ox[2]), L, hL)),
+                               xadd(oy[2], image_shift(xadd(xsub(pby[0].z, pa[0].z), oy[2]), L, hL)));
                 }
                 const uint32_t mx = ex >> 23, my = ey >> 23;
                 pair_row<R, FORM, REV, SHIFT, 0>(mx, my, pa[0], pbx, pby, wa[0], wbx, wby, ca[0], sh, L, invL, nb,
@@ -1050,39 +1061,33 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
         if (wpos) {
             const bool is_h = lane != 0;
             V4 po;
-            po.x = (R)gather_coord(o0, xn[0], is_h, Ld);
-            po.y = (R)gather_coord(o1, xn[1], is_h, Ld);
-            po.z = (R)gather_coord(o2, xn[2], is_h, Ld);
-            po.w = R(0);
+            if constexpr (sizeof(R) == 4) {
+                const double xo[3] = {o0, o1, o2};
+                po = gather_f32(xo, xn, lane, Ld);   // offsets from the molecule's cell origin
+            } else {
+                po.x = (R)gather_coord(o0, xn[0], is_h, Ld);
+                po.y = (R)gather_coord(o1, xn[1], is_h, Ld);
+                po.z = (R)gather_coord(o2, xn[2], is_h, Ld);
+                po.w = R(0);
+            }
             ((V4 *)a.pos_out)[3 * (size_t)I + lane] = po;
         }
     }
 
     if (REV) {
-        // Block reduction of the dtheta contributions (fixed order) and of |dl_dfi|^2.
+        // This molecule's dtheta contributions and |dl_dfi|^2, into its own slots: one group
+        // per molecule and step, so every slot sums its steps in step order.
         const int P = a.P;
-        double *sth = s_th;
-        double *sn2 = s_th + ngrp * P;
-        if (lane == 0) {
-#pragma unroll
-            for (int p = 0; p < NTH; p++) sth[grp * P + p] = active ? (double)th[p] : 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) sth[grp * P + NF + 1 + q] = active ? (double)s_bond[18 + q] : 0.0;
-        }
-        // lanes 0..2 hold per-atom |G|^2; fold them into lane 0's slot in order
+        // lanes 0..2 hold per-atom |G|^2; fold them into lane 0's in order
         const double n2a = __shfl_sync(0xffffffffu, n2, (threadIdx.x & 31) - lane + 1);
         const double n2b = __shfl_sync(0xffffffffu, n2, (threadIdx.x & 31) - lane + 2);
-        if (lane == 0) sn2[grp] = __dadd_rn(__dadd_rn(n2, n2a), n2b);
-        __syncthreads();
-        if (threadIdx.x < P) {
-            double s = 0.0;
-            for (int q = 0; q < ngrp; q++) s = __dadd_rn(s, sth[q * P + threadIdx.x]);
-            a.part[(size_t)blk * P + threadIdx.x] = __dadd_rn(a.part[(size_t)blk * P + threadIdx.x], s);
-        }
-        if (threadIdx.x == 0 && a.norm2) {
-            double s = 0.0;
-            for (int q = 0; q < ngrp; q++) s = __dadd_rn(s, sn2[q]);
-            a.norm2[blk] = s;
+        if (active && lane == 0) {
+            double *pm = a.part + (size_t)I * P;
+#pragma unroll
+            for (int p = 0; p < NTH; p++) pm[p] = __dadd_rn(pm[p], (double)th[p]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) pm[NF + 1 + q] = __dadd_rn(pm[NF + 1 + q], (double)s_bond[18 + q]);
+            if (a.norm2) a.norm2[I] = __dadd_rn(__dadd_rn(n2, n2a), n2b);
         }
     }
 }
@@ -1092,8 +1097,7 @@ __global__ void __maxnreg__((step_maxnreg<R, REV, U>())) k_water_step(StepArgs a
 template <typename R, int FORM, int G, bool SHIFT, int U>
 cudaError_t launch_one(bool rev, int n_blk, int threads, const StepArgs &a, const NbConsts<R> &nb,
                        const BondConsts &bc, cudaStream_t st) {
-    const int ngrp = threads / G;
-    const size_t smem = sizeof(double) * (size_t)ngrp * (a.P + 1) + sizeof(R) * 22 * (size_t)ngrp;
+    const size_t smem = sizeof(R) * 22 * (size_t)(threads / G);
     if (rev)
         return launch_chained(k_water_step<R, FORM, G, true, SHIFT, U>, dim3(n_blk), dim3(threads), smem,
                               st, a, nb, bc);
