@@ -44,8 +44,8 @@ UNIT = "atom-steps/s"
 FLOPS_FWD_IPAIR, FLOPS_FWD_OO_EXTRA, FLOPS_REV_IPAIR = 40, 15, 170
 # DRAM traffic per reverse-step launch of the default workload: dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture of that kernel on the same 9,000-atom system
-# (5.395 MB read, 0 written).
-REV_STEP_DRAM_BYTES = 5.395e6
+# (5.546 MB read, 0 written).
+REV_STEP_DRAM_BYTES = 5.546e6
 # DRAM traffic per forward-step launch of the gas-in-water engine (2,675 atoms), from one ncu
 # capture with cold caches (8.11 MB read, 0.11 MB written).
 GAS_FWD_STEP_DRAM_BYTES = 8.22e6
